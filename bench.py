@@ -1,0 +1,342 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 XPBD cloth substep (the 65,536-particle square cloth).
+
+A step is one frame: one launch of the persistent frame kernel that advances
+48 substeps (60 Hz frame, dt = 1/2880 s) of a 256x256 cloth at 4 mm spacing
+with 64 spheres, two gripped corners and a ground plane.  The metric is
+substeps per second for the whole job; inputs are resident in HBM when the
+timed region starts and L2 is flushed (256 MiB write) between frames.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: replicas only (one independent cloth per rank, no collective on
+the data path; weak scaling).  The reference arm times the CPU
+restatement of the reference substep (serial reference order, FP64) on the
+host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "numi-solver_b200"))
+
+SUBSTEPS = 48
+SIDE = 256
+METRIC = "substeps/s (65k-particle cloth)"
+
+# Bench schedule: one XPBD iteration and one strain sweep per substep, no
+# reconciliation or certificate loops, swept ground, frictions on.
+BENCH_SCHEDULE = dict(iterations=1, strainSweeps=1, reconcilePasses=0, finalPasses=0, certificatePasses=0,
+                      earlyExit=0, aerodynamics=0, sweptGround=1, frictions=1, selfCollision=0)
+
+
+def algorithmic_bytes(counts: dict) -> dict:
+    """Bytes per substep that the executed phases must move at minimum.
+
+    Per-unit figures: predict 52 B/particle (read x,v,w 28 + write x,prev 24),
+    constraint 72 B (record 12 + lambda 4 + 2 endpoints x (read 16 + write 12)),
+    strain 68 B per limited constraint, sphere/ground 28 B/particle, fruit/yarn
+    sweep 40 B per yarn segment (index 8 + 2 endpoints x 16), finalize 36
+    B/particle (read x,prev 24 + write v 12).
+    """
+    n, cons, lim, yarn = counts["particles"], counts["constraints"], counts["limited"], counts["yarn"]
+    parts = {
+        "predict": 52 * n,
+        "constraints": 72 * cons,
+        "strain": 68 * lim,
+        "ground": 28 * n,
+        "fruit_yarn": 40 * yarn,
+        "finalize": 36 * n,
+    }
+    parts["total"] = sum(parts.values())
+    return parts
+
+
+def measured_peaks() -> dict:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader",
+                 "-lms", "100"], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self) -> dict:
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1].split()[0]))
+                    smax = float(parts[2].split()[0])
+                except ValueError:
+                    continue
+                for name, val in zip(names, parts[5:9]):
+                    if val.lower().startswith("active"):
+                        reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_sample(seconds: float, threads: int, side: int = SIDE) -> dict:
+    """The FP64 oracle in the reference's serial order on a bounded sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    if threads <= 1:
+        return _cpu_worker((seconds, side))
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(threads) as pool:
+        parts = pool.map(_cpu_worker, [(seconds, side)] * threads)
+    return {"substeps": sum(p["substeps"] for p in parts), "seconds": max(p["seconds"] for p in parts)}
+
+
+def _cpu_worker(args):
+    seconds, side = args
+    sys.path.insert(0, os.path.join(ROOT, "numi-solver_b200"))
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numi_cloth as nc
+    import oracle_py as op
+
+    scene = nc.square_scene(side=side)
+    o = op.Oracle(op.from_abi(scene), 64)
+    subs = op.substeps_from_configs(nc.substep_configs(scene, 1))
+    sched = op.schedule_from_abi(nc.Schedule.make(**BENCH_SCHEDULE), op.SERIAL)
+    done = 0
+    t0 = time.perf_counter()
+    while True:
+        o.step(subs, sched)
+        done += 1
+        if time.perf_counter() - t0 >= seconds:
+            break
+    return {"substeps": done, "seconds": time.perf_counter() - t0}
+
+
+def dist_info():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def run_reference(args):
+    rank, world, _ = dist_info()
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    per_step = []
+    for _ in range(args.warmup + args.steps):
+        r = cpu_sample(args.ref_seconds, threads)
+        per_step.append(r)
+    timed = per_step[args.warmup:]
+    substeps = sum(r["substeps"] for r in timed)
+    secs = sum(r["seconds"] for r in timed)
+    value = substeps / secs
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "substeps/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * secs / max(len(timed), 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"square cloth {SIDE}x{SIDE} (65,536 particles), 64 spheres, serial reference "
+                               "order, FP64, one independent cloth per host thread", "schedule": BENCH_SCHEDULE},
+        "cpu_baseline": {"value": value, "unit": "substeps/s", "cores": threads, "kind": "port",
+                         "sample": f"{args.ref_seconds:.0f} s per step per thread on a {SIDE}x{SIDE} cloth"},
+        "e2e": {"value": value, "unit": "substeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    import numi_cloth as nc
+
+    rank, world, local = dist_info()
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    torch.zeros(1, device=dev)   # create the context before the library uses it
+    scene = nc.square_scene(side=SIDE)
+    solver = nc.ClothSolver(scene)
+    stream = torch.cuda.current_stream(dev)
+    solver.set_stream(stream.cuda_stream)
+    cfg = nc.substep_configs(scene, SUBSTEPS)
+    sched = nc.Schedule.make(**BENCH_SCHEDULE)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        solver.step(cfg, sched)
+    barrier()
+    fail = solver.failure()
+    info = solver.launch_info()
+    times = []
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        barrier()
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            start = torch.cuda.Event(enable_timing=True)
+            end = torch.cuda.Event(enable_timing=True)
+            start.record(stream)
+            solver.step(cfg, sched)
+            end.record(stream)
+            end.synchronize()
+            times.append(start.elapsed_time(end))
+        barrier()
+    fail |= solver.failure()
+    total_ms = float(sum(times))
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * SUBSTEPS * args.steps / (total_ms / 1000.0)
+
+    # e2e through the public API with host buffers: upload state, one frame,
+    # download state; wall clock around the synchronous calls.
+    host_p = solver.particles()
+    host_f = solver.fruits()
+    e2e_times = []
+    for k in range(args.warmup + args.steps):
+        flush.fill_(1.0)
+        barrier()
+        t0 = time.perf_counter()
+        solver.write_particles(host_p)
+        solver.write_fruits(host_f)
+        solver.step(cfg, sched)
+        host_p = solver.particles()
+        host_f = solver.fruits()
+        dt = time.perf_counter() - t0
+        if k >= args.warmup:
+            e2e_times.append(dt)
+    e2e_total = sum(e2e_times)
+    if world > 1:
+        t = torch.tensor([e2e_total], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_value = world * SUBSTEPS * args.steps / e2e_total
+    h2d = host_p.nbytes + host_f.nbytes + cfg.nbytes
+    d2h = host_p.nbytes + host_f.nbytes
+
+    counts = {
+        "particles": scene.n,
+        "constraints": len(scene.distances) + len(scene.bends),
+        "limited": int((scene.distances["material"][:, 3] > 0).sum()),
+        "yarn": int((scene.distances["particlesAndColor"][:, 3] != 3).sum()),
+    }
+    ab = algorithmic_bytes(counts)
+    per_launch_ms = total_ms / args.steps
+    achieved = ab["total"] * SUBSTEPS / (per_launch_ms / 1000.0) / 1e9
+    peaks = measured_peaks()
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "frame_kernel_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get("dram_bytes_per_launch")
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        r = cpu_sample(args.cpu_seconds, 1)
+        cpu = {"value": r["substeps"] / r["seconds"], "unit": "substeps/s", "cores": 1, "kind": "port",
+               "sample": f"{r['substeps']} substeps of the {SIDE}x{SIDE} cloth in {r['seconds']:.1f} s, FP64 "
+                         "restatement in the reference serial order, 1 thread"}
+    if world > 1:
+        torch.distributed.barrier()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "substeps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": per_launch_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"square cloth {SIDE}x{SIDE} (65,536 particles, 4 mm), 64 spheres, 2 gripped "
+                                   "corners, ground; 48 substeps per step (60 Hz frame)",
+                       "substeps_per_step": SUBSTEPS, "schedule": BENCH_SCHEDULE,
+                       "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}",
+                       "grid": info["grid"], "block": info["block"],
+                       "barriers_per_substep": info["barriers_per_substep"]},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+                         "peak_source": peaks["source"], "algorithmic_bytes_per_substep": ab},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "substeps/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": args.steps,
+            "clocks": clocks.summary(),
+            "failure": nc.failure_names(fail),
+        }
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--ref-seconds", type=float, default=6.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

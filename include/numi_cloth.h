@@ -1,0 +1,242 @@
+/*
+ * numi_cloth.h - C ABI of the B200 XPBD cloth substep.
+ *
+ * Record layouts are byte-identical to the pointer-free GPU ABI v13 of the
+ * reference cloth path (include/numi/cloth_bag_gpu.h:19-190, sizes asserted
+ * at :192-209), so a caller that already fills those buffers for the Metal
+ * encoder (tools/cloth_bag_metal.mm:4091-4202) can hand the same bytes to
+ * this library.  The functions replace the reference's Metal host entry
+ * runGPU (tools/cloth_bag_metal.mm:4010) and its per-substep command
+ * encoding (tools/cloth_bag_metal.mm:4211-4709).
+ *
+ * Conventions
+ *   - Caller owns host arrays; they are copied in and out.  The library owns
+ *     all device buffers of a handle.
+ *   - No exceptions cross the ABI.  Functions return NUMI_CLOTH_OK (0) or a
+ *     negative NUMI_CLOTH_E* code; stepping returns the reference failure
+ *     word (bits below) and a TIMEOUT bit for a bounded barrier wait.
+ *   - One handle = one GPU (the current device at create time) and one
+ *     CUDA stream.  A handle is not thread-safe; distinct handles are.
+ *   - Deterministic: no floating-point atomics touch simulated state, so two
+ *     runs from the same inputs are bit-identical.
+ */
+#ifndef NUMI_CLOTH_H
+#define NUMI_CLOTH_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#define NUMI_CLOTH_ALIGN16 alignas(16)
+#else
+#define NUMI_CLOTH_ALIGN16 _Alignas(16)
+#endif
+
+/* ABI version of the record layouts (reference cloth_bag_gpu.h:5). */
+#define NUMI_CLOTH_ABI_VERSION 13u
+#define NUMI_CLOTH_INVALID_PARTICLE 0xffffffffu
+#define NUMI_CLOTH_MOUTH_RIM_CAPACITY 64u
+
+/* Failure word (reference cloth_bag_gpu.h:10-17) plus TIMEOUT. */
+enum {
+    NUMI_CLOTH_FAILURE_NONE = 0u,
+    NUMI_CLOTH_FAILURE_ABI = 1u << 0,
+    NUMI_CLOTH_FAILURE_RANGE = 1u << 1,
+    NUMI_CLOTH_FAILURE_BATCH = 1u << 2,
+    NUMI_CLOTH_FAILURE_NONFINITE = 1u << 3,
+    NUMI_CLOTH_FAILURE_GRIP_CAPTURE = 1u << 4,
+    /* A grid barrier wait ran past its iteration limit; the kernel stopped
+     * at a phase boundary and the state is that of the last full phase. */
+    NUMI_CLOTH_FAILURE_TIMEOUT = 1u << 5
+};
+
+/* Return codes of the non-stepping functions. */
+enum {
+    NUMI_CLOTH_OK = 0,
+    NUMI_CLOTH_EINVAL = -1,   /* bad argument, size or layout */
+    NUMI_CLOTH_ECUDA = -2,    /* a CUDA runtime call failed */
+    NUMI_CLOTH_EBATCH = -3,   /* colour batches are not conflict free */
+    NUMI_CLOTH_ENOMEM = -4,
+    NUMI_CLOTH_ESTATE = -5    /* handle is poisoned by an earlier failure */
+};
+
+typedef struct NUMI_CLOTH_ALIGN16 numi_float4 { float x, y, z, w; } numi_float4;
+typedef struct NUMI_CLOTH_ALIGN16 numi_uint4 { uint32_t x, y, z, w; } numi_uint4;
+
+/* 224 B.  Field meaning follows cloth_bag_gpu.h:19-57. */
+typedef struct NUMI_CLOTH_ALIGN16 NumiClothConfig {
+    numi_uint4 control;             /* x ABI, y particles, z distances, w grips */
+    numi_uint4 constraintCounts;    /* x knots, y bends, z ground on/off, w fruits */
+    numi_uint4 contactCounts;       /* x fruit pairs, y fruit*segments, z,w unused here */
+    numi_float4 gravityAndTimestep; /* xyz gravity, w substep dt */
+    numi_float4 gripTargetAndActive;/* xyz handle position, w >0 active */
+    numi_float4 gripOrientation;    /* unit quaternion xyzw */
+    numi_uint4 gripControl;         /* x generation, y 1 = nearest cuff patch,
+                                       z knots per cuff row, w patch half width */
+    numi_float4 gripMaterial;       /* x capture radius */
+    numi_float4 clothMaterial;      /* x yarn radius, y self cell, z ground mu, w self mu */
+    numi_float4 fruitMaterial;      /* x pair mu, y ground mu, z rolling, w fruit/yarn mu */
+    numi_float4 airVelocityAndDensity;
+    numi_float4 aerodynamicCoefficients; /* yarn crossflow, yarn skin, fruit, fruit rot */
+    numi_uint4 mouthControl;        /* x rim count, y bottom centre */
+    numi_float4 mouthMaterial;      /* x release hysteresis */
+} NumiClothConfig;
+
+/* 48 B (cloth_bag_gpu.h:59-66). */
+typedef struct NUMI_CLOTH_ALIGN16 NumiClothParticle {
+    numi_float4 positionAndInverseMass;
+    numi_float4 previousAndMass;
+    numi_float4 velocity;           /* w: cloth/ground normal impulse */
+} NumiClothParticle;
+
+/* 32 B (cloth_bag_gpu.h:66-72).  particlesAndColor.w is the yarn kind:
+ * 0 warp, 1 weft, 2 bottom, 3 shear (shear is not a yarn segment: it takes
+ * no fruit contact and no air load).  material.w <= 0 disables the strain
+ * limiter for that constraint. */
+typedef struct NUMI_CLOTH_ALIGN16 NumiClothDistance {
+    numi_uint4 particlesAndColor;
+    numi_float4 material;           /* rest, compliance, lambda, max extension */
+} NumiClothDistance;
+
+/* 48 B (cloth_bag_gpu.h:74-82). */
+typedef struct NUMI_CLOTH_ALIGN16 NumiClothGrip {
+    numi_uint4 particle;            /* particle, generation, capture bits, ring */
+    numi_float4 targetOffsetAndCompliance;
+    numi_float4 lambda;
+} NumiClothGrip;
+
+/* 48 B (cloth_bag_gpu.h:84-91). */
+typedef struct NUMI_CLOTH_ALIGN16 NumiClothKnot {
+    numi_uint4 particles;           /* warp first, warp second, weft first, weft second */
+    numi_uint4 control;             /* x colour */
+    numi_float4 material;           /* rest cosine, compliance, lambda */
+} NumiClothKnot;
+
+/* 32 B (cloth_bag_gpu.h:93-98). */
+typedef struct NUMI_CLOTH_ALIGN16 NumiClothBend {
+    numi_uint4 particlesAndColor;   /* first, middle, third, colour */
+    numi_float4 material;           /* rest chord, rest arc, compliance, lambda */
+} NumiClothBend;
+
+/* 96 B (cloth_bag_gpu.h:100-113). */
+typedef struct NUMI_CLOTH_ALIGN16 NumiClothFruit {
+    numi_float4 positionAndInverseMass;
+    numi_float4 previousAndRadius;
+    numi_float4 velocityAndGroundImpulse;
+    numi_float4 angularVelocity;
+    numi_float4 orientation;
+    numi_uint4 identity;
+} NumiClothFruit;
+
+/* 32 B (cloth_bag_gpu.h:115-120). */
+typedef struct NUMI_CLOTH_ALIGN16 NumiClothFruitPair {
+    numi_uint4 fruitsAndColor;
+    numi_float4 contact;
+} NumiClothFruitPair;
+
+/* 16 B (cloth_bag_gpu.h:184-188). */
+typedef struct NUMI_CLOTH_ALIGN16 NumiClothBatch {
+    numi_uint4 control;             /* first, count, colour, reserved */
+} NumiClothBatch;
+
+/* Per-substep schedule.  The reference CPU oracle fixes these at
+ * iterations=CLI, strain sweeps=3, reconciliation<=8 with early exit,
+ * final passes=2, certificate<=128 on the last substep of a frame
+ * (tools/cloth_bag.cpp:4891-5185). */
+typedef struct NumiClothSchedule {
+    uint32_t iterations;
+    uint32_t strainSweeps;          /* sweeps per strain-limiter call */
+    uint32_t reconcilePasses;       /* maximum reconciliation passes */
+    uint32_t finalPasses;           /* final contact passes */
+    uint32_t certificatePasses;     /* maximum, last substep of a call only */
+    uint32_t earlyExit;             /* 1: stop reconcile/certificate on residuals */
+    uint32_t selfCollision;         /* 1: point/point hash-grid self contact */
+    uint32_t aerodynamics;          /* 1: yarn and fruit air loads */
+    uint32_t sweptGround;           /* 1: swept ground prediction after advance */
+    uint32_t sweptFruitYarn;        /* 1: swept fruit/yarn contact before iterations */
+    uint32_t frictions;             /* 1: apply the Coulomb/rolling frictions */
+    uint32_t release;               /* 1: update the mouth release masks */
+    float damping;                  /* v <- v/(1+c dt) after gravity; 0 = reference */
+    uint32_t reserved[3];
+} NumiClothSchedule;
+
+/* Scene handed to numi_cloth_create.  Constraint arrays must be grouped in
+ * contiguous colour runs (one batch per run); the library checks that no
+ * two records of a batch write the same particle or fruit. */
+typedef struct NumiClothScene {
+    const NumiClothConfig* config;
+    const NumiClothParticle* particles;
+    const numi_float4* restPositions;    /* xyz rest, used for inverse mass 0; may be NULL */
+    const NumiClothDistance* distances;
+    const NumiClothKnot* knots;
+    const NumiClothBend* bends;
+    const NumiClothGrip* grips;
+    const NumiClothFruit* fruits;
+    const NumiClothFruitPair* fruitPairs;
+    const uint32_t* cuffParticles;       /* 2 rows x gripControl.z ring particles */
+    const uint32_t* mouthRim;            /* mouthControl.x ordered rim particles */
+    /* 2-hop local topology excluded from self contact (tools/cloth_bag.cpp:842-861):
+     * CSR over particles, each row sorted ascending.  When localOffsets is
+     * NULL and gridWidth > 0, particles are a gridWidth-wide row-major grid
+     * and the local set is the Chebyshev ball of radius 2. */
+    const uint32_t* localOffsets;
+    const uint32_t* localIndices;
+    uint32_t gridWidth;
+    uint32_t reserved[3];
+} NumiClothScene;
+
+typedef struct numi_cloth numi_cloth_t;
+
+/* Create a solver on the current CUDA device.  Returns NUMI_CLOTH_OK and a
+ * handle, or a negative code (NUMI_CLOTH_EBATCH for a colouring conflict). */
+int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out);
+void numi_cloth_destroy(numi_cloth_t* handle);
+
+/* Launch on this CUDA stream (cudaStream_t passed as void*; NULL = default). */
+int numi_cloth_set_stream(numi_cloth_t* handle, void* stream);
+
+/* Advance count substeps.  configs[i] is the live Config of substep i (the
+ * reference's trajectoryConfigs, ClothBag.metal:466-489); only grip pose,
+ * grip generation, timestep and gravity may change between substeps.  The
+ * last substep of the call runs the certificate loop.  Asynchronous on the
+ * handle's stream; returns NUMI_CLOTH_OK or a negative code.  Read the
+ * failure word with numi_cloth_failure. */
+int numi_cloth_step(numi_cloth_t* handle, const NumiClothConfig* configs,
+                    uint32_t count, const NumiClothSchedule* schedule);
+
+/* Synchronise the stream and return the accumulated failure word. */
+uint32_t numi_cloth_failure(numi_cloth_t* handle);
+
+/* Host copies of the state (synchronous). */
+int numi_cloth_read_particles(numi_cloth_t* handle, NumiClothParticle* out, uint32_t count);
+int numi_cloth_write_particles(numi_cloth_t* handle, const NumiClothParticle* in, uint32_t count);
+int numi_cloth_read_fruits(numi_cloth_t* handle, NumiClothFruit* out, uint32_t count);
+int numi_cloth_write_fruits(numi_cloth_t* handle, const NumiClothFruit* in, uint32_t count);
+int numi_cloth_read_distances(numi_cloth_t* handle, NumiClothDistance* out, uint32_t count);
+int numi_cloth_read_grips(numi_cloth_t* handle, NumiClothGrip* out, uint32_t count);
+
+/* Residuals of the current state, reduced in FP64 on the device:
+ * out[0] max strain-limit violation (m), out[1] max ground penetration (m),
+ * out[2] max fruit/yarn penetration (m), out[3] max self penetration (m). */
+int numi_cloth_residuals(numi_cloth_t* handle, double out[4]);
+
+/* Release masks (x mouth candidates, y released) after the last step. */
+int numi_cloth_release_masks(numi_cloth_t* handle, uint32_t out[2]);
+
+/* Device-side snapshot of the full dynamic state into slot (0..7), and back. */
+int numi_cloth_snapshot(numi_cloth_t* handle, uint32_t slot);
+int numi_cloth_restore(numi_cloth_t* handle, uint32_t slot);
+
+/* Launch geometry of the last step: grid CTAs, threads per CTA, barriers
+ * per substep, kernel launches. */
+int numi_cloth_launch_info(numi_cloth_t* handle, uint32_t out[4]);
+
+/* Library version string. */
+const char* numi_cloth_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NUMI_CLOTH_H */

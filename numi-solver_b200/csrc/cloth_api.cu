@@ -1,0 +1,640 @@
+// C ABI of the cloth solver: handle lifetime, validation, colour batches,
+// AoS <-> SoA conversion at the boundary, and the cooperative launch.
+//
+// Replaces the reference Metal host runGPU (tools/cloth_bag_metal.mm:4010-4760):
+// buffer allocation (:4091-4202), per-substep encoding (:4211-4709), commit
+// and readback (:4710-4757), and the colouring check verifyColoring
+// (tools/cloth_bag_metal.mm:1705-1819).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "cloth_frame.cuh"
+#include "numi_cloth.h"
+
+static_assert(sizeof(NumiClothConfig) == 224, "Config layout");
+static_assert(sizeof(NumiClothParticle) == 48, "Particle layout");
+static_assert(sizeof(NumiClothDistance) == 32, "Distance layout");
+static_assert(sizeof(NumiClothGrip) == 48, "Grip layout");
+static_assert(sizeof(NumiClothKnot) == 48, "Knot layout");
+static_assert(sizeof(NumiClothBend) == 32, "Bend layout");
+static_assert(sizeof(NumiClothFruit) == 96, "Fruit layout");
+static_assert(sizeof(NumiClothFruitPair) == 32, "FruitPair layout");
+static_assert(sizeof(NumiClothBatch) == 16, "Batch layout");
+static_assert(offsetof(NumiClothConfig, gravityAndTimestep) == 48, "Config offsets");
+static_assert(offsetof(NumiClothConfig, mouthMaterial) == 208, "Config offsets");
+
+__global__ void __launch_bounds__(NC_THREADS) numi_cloth_residual_kernel(DeviceCloth d, NumiClothConfig cfg) {
+    Schedule s{};
+    nc::Ctx ctx{d, s};
+    ctx.c = nc::load_cfg(&cfg);
+    ctx.tid = blockIdx.x * blockDim.x + threadIdx.x;
+    ctx.nthreads = gridDim.x * blockDim.x;
+    nc::residual_partials(ctx, d.red);
+}
+
+namespace {
+
+constexpr uint32_t kSnapshotSlots = 8;
+
+struct Snapshot {
+    bool valid = false;
+    void* mem = nullptr;
+    size_t bytes = 0;
+};
+
+struct DeviceBuffers {
+    std::vector<void*> owned;
+    template <class T>
+    T* alloc(size_t count) {
+        if (count == 0) count = 1;
+        void* p = nullptr;
+        if (cudaMalloc(&p, count * sizeof(T)) != cudaSuccess) return nullptr;
+        cudaMemset(p, 0, count * sizeof(T));
+        owned.push_back(p);
+        return static_cast<T*>(p);
+    }
+    ~DeviceBuffers() {
+        for (void* p : owned) cudaFree(p);
+    }
+};
+
+bool env_u32(const char* name, uint32_t& out) {
+    const char* v = std::getenv(name);
+    if (v == nullptr || *v == 0) return false;
+    out = static_cast<uint32_t>(std::strtoul(v, nullptr, 10));
+    return true;
+}
+
+}  // namespace
+
+struct numi_cloth {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    DeviceBuffers buf;
+    DeviceCloth d{};
+    NumiClothConfig base{};
+    NumiClothConfig* d_cfg = nullptr;
+    uint32_t cfg_capacity = 0;
+    uint32_t epoch = 1;
+    uint32_t host_failure = 0;
+    bool poisoned = false;
+    uint32_t grid = 1;
+    uint32_t block = NC_THREADS;
+    uint32_t launches = 0;
+    Snapshot snaps[kSnapshotSlots];
+    // dynamic state regions copied by snapshot/restore
+    struct Region {
+        void* ptr;
+        size_t bytes;
+    };
+    std::vector<Region> dynamic;
+};
+
+namespace {
+
+bool finite4(const numi_float4& v) {
+    return std::isfinite(v.x) && std::isfinite(v.y) && std::isfinite(v.z) && std::isfinite(v.w);
+}
+
+// Host twin of the reference validConfig (ClothBag.metal:16-55).
+uint32_t validate_config(const NumiClothConfig& c, const NumiClothConfig& base) {
+    if (c.control.x != NUMI_CLOTH_ABI_VERSION) return NUMI_CLOTH_FAILURE_ABI;
+    if (c.control.y != base.control.y || c.control.z != base.control.z || c.control.w != base.control.w ||
+        c.constraintCounts.x != base.constraintCounts.x || c.constraintCounts.y != base.constraintCounts.y ||
+        c.constraintCounts.w != base.constraintCounts.w || c.contactCounts.x != base.contactCounts.x)
+        return NUMI_CLOTH_FAILURE_RANGE;
+    const float dt = c.gravityAndTimestep.w;
+    bool ok = dt > 0.0f && std::isfinite(dt) && finite4(c.gravityAndTimestep) && finite4(c.gripTargetAndActive) &&
+              finite4(c.gripOrientation) && finite4(c.gripMaterial) && finite4(c.clothMaterial) &&
+              finite4(c.fruitMaterial) && finite4(c.airVelocityAndDensity) && finite4(c.aerodynamicCoefficients) &&
+              finite4(c.mouthMaterial) && c.clothMaterial.x >= 0.0f && c.airVelocityAndDensity.w >= 0.0f &&
+              c.aerodynamicCoefficients.x >= 0.0f && c.aerodynamicCoefficients.y >= 0.0f &&
+              c.aerodynamicCoefficients.z >= 0.0f && c.aerodynamicCoefficients.w >= 0.0f &&
+              c.gripMaterial.x >= 0.0f && c.gripControl.y <= 1u && c.mouthMaterial.x >= 0.0f &&
+              c.mouthControl.x <= NUMI_CLOTH_MOUTH_RIM_CAPACITY;
+    if (ok && c.gripTargetAndActive.w > 0.0f) {
+        const numi_float4& q = c.gripOrientation;
+        const float len = std::sqrt(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w);
+        ok = std::fabs(len - 1.0f) <= 1.0e-4f && c.gripControl.x != 0u && c.gripMaterial.x > 0.0f;
+    }
+    if (ok && c.gripControl.y == 1u) {
+        ok = c.gripControl.z >= 2u * c.gripControl.w + 1u && c.gripControl.z <= NUMI_CLOTH_MOUTH_RIM_CAPACITY &&
+             c.gripControl.w <= 16u && c.control.w == 2u * (2u * c.gripControl.w + 1u);
+    }
+    return ok ? 0u : NUMI_CLOTH_FAILURE_NONFINITE;
+}
+
+// Colour runs -> batches; checks contiguity and one writer per particle.
+template <class Rec, class ColourFn, class WritersFn, class YarnFn, class LimitFn>
+int make_batches(const Rec* recs, uint32_t count, uint32_t n_targets, ColourFn colour, WritersFn writers,
+                 YarnFn yarn, LimitFn limited, Batch* out, uint32_t& n_out) {
+    n_out = 0;
+    std::vector<uint32_t> stamp(n_targets, 0xffffffffu);
+    std::vector<uint32_t> seen_colours;
+    uint32_t k = 0;
+    while (k < count) {
+        const uint32_t col = colour(recs[k]);
+        if (std::find(seen_colours.begin(), seen_colours.end(), col) != seen_colours.end()) return NUMI_CLOTH_EBATCH;
+        seen_colours.push_back(col);
+        if (n_out >= NC_MAX_BATCHES) return NUMI_CLOTH_EINVAL;
+        Batch b{k, 0, 0, 0};
+        bool yarn_open = true;
+        while (k < count && colour(recs[k]) == col) {
+            uint32_t w[4];
+            const int nw = writers(recs[k], w);
+            if (nw < 0) return NUMI_CLOTH_EINVAL;
+            for (int e = 0; e < nw; ++e) {
+                if (w[e] >= n_targets) return NUMI_CLOTH_EINVAL;
+                if (stamp[w[e]] == n_out) return NUMI_CLOTH_EBATCH;
+                stamp[w[e]] = n_out;
+            }
+            if (yarn(recs[k])) {
+                if (!yarn_open) return NUMI_CLOTH_EINVAL;   // yarn segments lead their colour
+                b.yarn = k - b.first + 1u;
+            } else {
+                yarn_open = false;
+            }
+            if (limited(recs[k])) b.limited = k - b.first + 1u;
+            ++k;
+        }
+        b.count = k - b.first;
+        out[n_out++] = b;
+    }
+    return NUMI_CLOTH_OK;
+}
+
+cudaError_t launch(numi_cloth* h, uint32_t substeps, const Schedule& s) {
+    DeviceCloth d = h->d;
+    d.cfg = h->d_cfg;
+    d.epoch_base = h->epoch;
+    Schedule sc = s;
+    sc.substeps = substeps;
+    void* args[] = {&d, &sc};
+    cudaError_t e;
+    if (h->grid == 1) {
+        e = cudaLaunchKernel(reinterpret_cast<const void*>(numi_cloth_frame_kernel), dim3(1), dim3(h->block), args, 0,
+                             h->stream);
+    } else {
+        e = cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(numi_cloth_frame_kernel), dim3(h->grid),
+                                        dim3(h->block), args, 0, h->stream);
+    }
+    if (e == cudaSuccess) ++h->launches;
+    return e;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* numi_cloth_version(void) { return "numi-cloth-b200 0.1 (sm_100a, ABI 13)"; }
+
+int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
+    if (scene == nullptr || out == nullptr || scene->config == nullptr || scene->particles == nullptr)
+        return NUMI_CLOTH_EINVAL;
+    *out = nullptr;
+    const NumiClothConfig& cfg = *scene->config;
+    if (cfg.control.x != NUMI_CLOTH_ABI_VERSION) return NUMI_CLOTH_EINVAL;
+    const uint32_t n = cfg.control.y, D = cfg.control.z, G = cfg.control.w;
+    const uint32_t K = cfg.constraintCounts.x, B = cfg.constraintCounts.y, F = cfg.constraintCounts.w;
+    const uint32_t P = cfg.contactCounts.x;
+    if (n == 0 || F > NC_MAX_FRUITS || G > NC_MAX_GRIPS) return NUMI_CLOTH_EINVAL;
+    if ((D && !scene->distances) || (K && !scene->knots) || (B && !scene->bends) || (G && !scene->grips) ||
+        (F && !scene->fruits) || (P && !scene->fruitPairs))
+        return NUMI_CLOTH_EINVAL;
+    if (validate_config(cfg, cfg) != 0u) return NUMI_CLOTH_EINVAL;
+    if (cfg.gripControl.y == 1u && scene->cuffParticles == nullptr) return NUMI_CLOTH_EINVAL;
+
+    numi_cloth* h = new (std::nothrow) numi_cloth();
+    if (h == nullptr) return NUMI_CLOTH_ENOMEM;
+    cudaGetDevice(&h->device);
+    h->base = cfg;
+
+    // Batches.
+    int rc = make_batches(
+        scene->distances, D, n, [](const NumiClothDistance& r) { return r.particlesAndColor.z; },
+        [](const NumiClothDistance& r, uint32_t* w) {
+            w[0] = r.particlesAndColor.x;
+            w[1] = r.particlesAndColor.y;
+            return w[0] == w[1] ? -1 : 2;
+        },
+        [](const NumiClothDistance& r) { return r.particlesAndColor.w != 3u; },
+        [](const NumiClothDistance& r) { return r.material.w > 0.0f; }, h->d.dist_batches, h->d.n_dist_batches);
+    if (rc == NUMI_CLOTH_OK)
+        rc = make_batches(
+            scene->knots, K, n, [](const NumiClothKnot& r) { return r.control.x; },
+            [](const NumiClothKnot& r, uint32_t* w) {
+                w[0] = r.particles.x;
+                w[1] = r.particles.y;
+                w[2] = r.particles.z;
+                w[3] = r.particles.w;
+                return 4;
+            },
+            [](const NumiClothKnot&) { return false; }, [](const NumiClothKnot&) { return false; },
+            h->d.knot_batches, h->d.n_knot_batches);
+    if (rc == NUMI_CLOTH_OK)
+        rc = make_batches(
+            scene->bends, B, n, [](const NumiClothBend& r) { return r.particlesAndColor.w; },
+            [](const NumiClothBend& r, uint32_t* w) {
+                w[0] = r.particlesAndColor.x;
+                w[1] = r.particlesAndColor.z;
+                return w[0] == w[1] ? -1 : 2;
+            },
+            [](const NumiClothBend&) { return false; }, [](const NumiClothBend&) { return false; },
+            h->d.bend_batches, h->d.n_bend_batches);
+    if (rc == NUMI_CLOTH_OK)
+        rc = make_batches(
+            scene->fruitPairs, P, F, [](const NumiClothFruitPair& r) { return r.fruitsAndColor.z; },
+            [](const NumiClothFruitPair& r, uint32_t* w) {
+                w[0] = r.fruitsAndColor.x;
+                w[1] = r.fruitsAndColor.y;
+                return w[0] == w[1] ? -1 : 2;
+            },
+            [](const NumiClothFruitPair&) { return false; }, [](const NumiClothFruitPair&) { return false; },
+            h->d.pair_batches, h->d.n_pair_batches);
+    // the middle particle of a bend is read-only but must still exist
+    for (uint32_t k = 0; rc == NUMI_CLOTH_OK && k < B; ++k)
+        if (scene->bends[k].particlesAndColor.y >= n) rc = NUMI_CLOTH_EINVAL;
+    for (uint32_t g = 0; rc == NUMI_CLOTH_OK && g < G; ++g) {
+        if (scene->grips[g].particle.x >= n) rc = NUMI_CLOTH_EINVAL;
+        for (uint32_t e = 0; e < g && rc == NUMI_CLOTH_OK; ++e)
+            if (scene->grips[e].particle.x == scene->grips[g].particle.x) rc = NUMI_CLOTH_EBATCH;
+    }
+    if (rc == NUMI_CLOTH_OK && cfg.gripControl.y == 1u)
+        for (uint32_t k = 0; k < 2u * cfg.gripControl.z; ++k)
+            if (scene->cuffParticles[k] >= n) rc = NUMI_CLOTH_EINVAL;
+    if (rc != NUMI_CLOTH_OK) {
+        delete h;
+        return rc;
+    }
+
+    // Device buffers.
+    DeviceCloth& d = h->d;
+    d.n = n;
+    d.d_count = D;
+    d.k_count = K;
+    d.b_count = B;
+    d.g_count = G;
+    d.f_count = F;
+    d.p_count = P;
+    d.grid_width = scene->gridWidth;
+    d.x = h->buf.alloc<float4>(n);
+    d.xp = h->buf.alloc<float4>(n);
+    d.v = h->buf.alloc<float4>(n);
+    float4* rest = h->buf.alloc<float4>(n);
+    d.rest = rest;
+    uint2* d_ij = h->buf.alloc<uint2>(D);
+    float4* d_mat = h->buf.alloc<float4>(D);
+    d.d_ij = d_ij;
+    d.d_mat = d_mat;
+    d.d_lambda = h->buf.alloc<float>(D);
+    uint4* k_ij = h->buf.alloc<uint4>(K);
+    float2* k_mat = h->buf.alloc<float2>(K);
+    d.k_ij = k_ij;
+    d.k_mat = k_mat;
+    d.k_lambda = h->buf.alloc<float>(K);
+    uint4* b_ij = h->buf.alloc<uint4>(B);
+    float2* b_mat = h->buf.alloc<float2>(B);
+    d.b_ij = b_ij;
+    d.b_mat = b_mat;
+    d.b_lambda = h->buf.alloc<float>(B);
+    d.grips = h->buf.alloc<NumiClothGrip>(G);
+    d.fruits = h->buf.alloc<NumiClothFruit>(F);
+    d.pairs = h->buf.alloc<NumiClothFruitPair>(P);
+    uint32_t* cuff = h->buf.alloc<uint32_t>(cfg.gripControl.y == 1u ? 2u * cfg.gripControl.z : 1u);
+    d.cuff = cuff;
+    d.yarn_slot_a = h->buf.alloc<float4>(static_cast<size_t>(F ? D : 1) * NC_YARN_SLOTS);
+    d.yarn_slot_b = h->buf.alloc<float4>(static_cast<size_t>(F ? D : 1) * NC_YARN_SLOTS);
+    d.force = h->buf.alloc<float4>(n);
+    d.fruit_partial = h->buf.alloc<float4>(NC_MAX_FRUITS * 9u / 2u + 1u);
+    d.failure = h->buf.alloc<unsigned int>(1);
+    d.bar_count = h->buf.alloc<unsigned int>(1);
+    d.bar_gen = h->buf.alloc<unsigned int>(1);
+    d.abort_flag = h->buf.alloc<unsigned int>(1);
+    d.stats = h->buf.alloc<uint32_t>(4);
+
+    // Launch geometry: one resident CTA for a small cloth, else a full
+    // cooperative grid (as many CTAs as can be co-resident).
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, numi_cloth_frame_kernel, NC_THREADS, 0);
+    uint32_t work = std::max({n, D, K, B});
+    uint32_t grid = (work <= 8192u) ? 1u : std::min<uint32_t>(sms * std::max(per_sm, 1), (work + NC_THREADS - 1u) / NC_THREADS);
+    uint32_t forced = 0;
+    if (env_u32("NUMI_CLOTH_GRID", forced) && forced > 0) grid = std::min<uint32_t>(forced, sms * std::max(per_sm, 1));
+    h->grid = std::max(grid, 1u);
+    const uint32_t chunks = (n + NC_THREADS - 1u) / NC_THREADS;
+    d.red = h->buf.alloc<double>(std::max<size_t>(3u * 4096u, 2u * chunks + 8u));
+
+    bool ok = d.x && d.xp && d.v && rest && d_ij && d_mat && d.d_lambda && k_ij && k_mat && d.k_lambda && b_ij &&
+              b_mat && d.b_lambda && d.grips && d.fruits && d.pairs && cuff && d.yarn_slot_a && d.yarn_slot_b &&
+              d.force && d.fruit_partial && d.failure && d.bar_count && d.bar_gen && d.abort_flag && d.stats && d.red;
+    if (!ok) {
+        delete h;
+        return NUMI_CLOTH_ENOMEM;
+    }
+
+    // AoS -> SoA.
+    std::vector<float4> hx(n), hxp(n), hv(n), hr(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        const NumiClothParticle& p = scene->particles[i];
+        hx[i] = make_float4(p.positionAndInverseMass.x, p.positionAndInverseMass.y, p.positionAndInverseMass.z,
+                            p.positionAndInverseMass.w);
+        hxp[i] = make_float4(p.previousAndMass.x, p.previousAndMass.y, p.previousAndMass.z, p.previousAndMass.w);
+        hv[i] = make_float4(p.velocity.x, p.velocity.y, p.velocity.z, p.velocity.w);
+        if (scene->restPositions != nullptr)
+            hr[i] = make_float4(scene->restPositions[i].x, scene->restPositions[i].y, scene->restPositions[i].z, 0.0f);
+        else
+            hr[i] = make_float4(hx[i].x, hx[i].y, hx[i].z, 0.0f);
+    }
+    std::vector<uint2> hij(D);
+    std::vector<float4> hdm(D);
+    std::vector<float> hdl(D);
+    for (uint32_t k = 0; k < D; ++k) {
+        const NumiClothDistance& r = scene->distances[k];
+        hij[k] = make_uint2(r.particlesAndColor.x, r.particlesAndColor.y);
+        hdm[k] = make_float4(r.material.x, r.material.y, 0.0f, r.material.w);
+        hdl[k] = r.material.z;
+    }
+    std::vector<uint4> hkij(K);
+    std::vector<float2> hkm(K);
+    std::vector<float> hkl(K);
+    for (uint32_t k = 0; k < K; ++k) {
+        const NumiClothKnot& r = scene->knots[k];
+        hkij[k] = make_uint4(r.particles.x, r.particles.y, r.particles.z, r.particles.w);
+        hkm[k] = make_float2(r.material.x, r.material.y);
+        hkl[k] = r.material.z;
+    }
+    std::vector<uint4> hbij(B);
+    std::vector<float2> hbm(B);
+    std::vector<float> hbl(B);
+    for (uint32_t k = 0; k < B; ++k) {
+        const NumiClothBend& r = scene->bends[k];
+        hbij[k] = make_uint4(r.particlesAndColor.x, r.particlesAndColor.y, r.particlesAndColor.z, 0u);
+        hbm[k] = make_float2(r.material.x, r.material.z);
+        hbl[k] = r.material.w;
+    }
+    cudaError_t e = cudaSuccess;
+    auto up = [&](void* dst, const void* src, size_t bytes) {
+        if (e == cudaSuccess && bytes) e = cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
+    };
+    up(d.x, hx.data(), n * sizeof(float4));
+    up(d.xp, hxp.data(), n * sizeof(float4));
+    up(d.v, hv.data(), n * sizeof(float4));
+    up(rest, hr.data(), n * sizeof(float4));
+    up(d_ij, hij.data(), D * sizeof(uint2));
+    up(d_mat, hdm.data(), D * sizeof(float4));
+    up(d.d_lambda, hdl.data(), D * sizeof(float));
+    up(k_ij, hkij.data(), K * sizeof(uint4));
+    up(k_mat, hkm.data(), K * sizeof(float2));
+    up(d.k_lambda, hkl.data(), K * sizeof(float));
+    up(b_ij, hbij.data(), B * sizeof(uint4));
+    up(b_mat, hbm.data(), B * sizeof(float2));
+    up(d.b_lambda, hbl.data(), B * sizeof(float));
+    up(d.grips, scene->grips, G * sizeof(NumiClothGrip));
+    up(d.fruits, scene->fruits, F * sizeof(NumiClothFruit));
+    up(d.pairs, scene->fruitPairs, P * sizeof(NumiClothFruitPair));
+    if (cfg.gripControl.y == 1u) up(cuff, scene->cuffParticles, 2u * cfg.gripControl.z * sizeof(uint32_t));
+    if (e != cudaSuccess) {
+        delete h;
+        return NUMI_CLOTH_ECUDA;
+    }
+    h->dynamic = {{d.x, n * sizeof(float4)},
+                  {d.xp, n * sizeof(float4)},
+                  {d.v, n * sizeof(float4)},
+                  {d.d_lambda, std::max<size_t>(D, 1) * sizeof(float)},
+                  {d.k_lambda, std::max<size_t>(K, 1) * sizeof(float)},
+                  {d.b_lambda, std::max<size_t>(B, 1) * sizeof(float)},
+                  {d.grips, std::max<size_t>(G, 1) * sizeof(NumiClothGrip)},
+                  {d.fruits, std::max<size_t>(F, 1) * sizeof(NumiClothFruit)},
+                  {d.pairs, std::max<size_t>(P, 1) * sizeof(NumiClothFruitPair)}};
+    *out = h;
+    return NUMI_CLOTH_OK;
+}
+
+void numi_cloth_destroy(numi_cloth_t* h) {
+    if (h == nullptr) return;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (auto& s : h->snaps)
+        if (s.mem) cudaFree(s.mem);
+    cudaFree(h->d_cfg);
+    delete h;
+}
+
+int numi_cloth_set_stream(numi_cloth_t* h, void* stream) {
+    if (h == nullptr) return NUMI_CLOTH_EINVAL;
+    h->stream = static_cast<cudaStream_t>(stream);
+    return NUMI_CLOTH_OK;
+}
+
+int numi_cloth_step(numi_cloth_t* h, const NumiClothConfig* configs, uint32_t count,
+                    const NumiClothSchedule* schedule) {
+    if (h == nullptr || configs == nullptr || schedule == nullptr || count == 0) return NUMI_CLOTH_EINVAL;
+    if (h->poisoned) return NUMI_CLOTH_ESTATE;
+    cudaSetDevice(h->device);
+    for (uint32_t k = 0; k < count; ++k) {
+        const uint32_t bad = validate_config(configs[k], h->base);
+        if (bad) {
+            h->host_failure |= bad;
+            return NUMI_CLOTH_OK;   // the failure word reports it; nothing ran
+        }
+    }
+    if (count > h->cfg_capacity) {
+        cudaFree(h->d_cfg);
+        h->d_cfg = nullptr;
+        if (cudaMalloc(&h->d_cfg, count * sizeof(NumiClothConfig)) != cudaSuccess) return NUMI_CLOTH_ECUDA;
+        h->cfg_capacity = count;
+    }
+    if (cudaMemcpyAsync(h->d_cfg, configs, count * sizeof(NumiClothConfig), cudaMemcpyHostToDevice, h->stream) !=
+        cudaSuccess)
+        return NUMI_CLOTH_ECUDA;
+    Schedule s{};
+    s.iterations = schedule->iterations;
+    s.strain_sweeps = schedule->strainSweeps;
+    s.reconcile_passes = schedule->reconcilePasses;
+    s.final_passes = schedule->finalPasses;
+    s.certificate_passes = schedule->certificatePasses;
+    s.early_exit = schedule->earlyExit;
+    s.self_collision = schedule->selfCollision;
+    s.aerodynamics = schedule->aerodynamics;
+    s.swept_ground = schedule->sweptGround;
+    s.swept_fruit_yarn = schedule->sweptFruitYarn;
+    s.frictions = schedule->frictions;
+    s.release = schedule->release;
+    s.damping = schedule->damping;
+    const cudaError_t e = launch(h, count, s);
+    h->epoch += count;
+    if (e != cudaSuccess) {
+        h->poisoned = true;
+        return NUMI_CLOTH_ECUDA;
+    }
+    return NUMI_CLOTH_OK;
+}
+
+uint32_t numi_cloth_failure(numi_cloth_t* h) {
+    if (h == nullptr) return NUMI_CLOTH_FAILURE_RANGE;
+    cudaSetDevice(h->device);
+    uint32_t f = 0;
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess ||
+        cudaMemcpy(&f, h->d.failure, sizeof(f), cudaMemcpyDeviceToHost) != cudaSuccess) {
+        h->poisoned = true;
+        return h->host_failure | NUMI_CLOTH_FAILURE_RANGE;
+    }
+    return f | h->host_failure;
+}
+
+int numi_cloth_read_particles(numi_cloth_t* h, NumiClothParticle* out, uint32_t count) {
+    if (h == nullptr || out == nullptr || count != h->d.n) return NUMI_CLOTH_EINVAL;
+    cudaSetDevice(h->device);
+    std::vector<float4> x(count), xp(count), v(count);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess ||
+        cudaMemcpy(x.data(), h->d.x, count * sizeof(float4), cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(xp.data(), h->d.xp, count * sizeof(float4), cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(v.data(), h->d.v, count * sizeof(float4), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return NUMI_CLOTH_ECUDA;
+    for (uint32_t i = 0; i < count; ++i) {
+        out[i].positionAndInverseMass = {x[i].x, x[i].y, x[i].z, x[i].w};
+        out[i].previousAndMass = {xp[i].x, xp[i].y, xp[i].z, xp[i].w};
+        out[i].velocity = {v[i].x, v[i].y, v[i].z, v[i].w};
+    }
+    return NUMI_CLOTH_OK;
+}
+
+int numi_cloth_write_particles(numi_cloth_t* h, const NumiClothParticle* in, uint32_t count) {
+    if (h == nullptr || in == nullptr || count != h->d.n) return NUMI_CLOTH_EINVAL;
+    cudaSetDevice(h->device);
+    std::vector<float4> x(count), xp(count), v(count);
+    for (uint32_t i = 0; i < count; ++i) {
+        const NumiClothParticle& p = in[i];
+        x[i] = make_float4(p.positionAndInverseMass.x, p.positionAndInverseMass.y, p.positionAndInverseMass.z,
+                           p.positionAndInverseMass.w);
+        xp[i] = make_float4(p.previousAndMass.x, p.previousAndMass.y, p.previousAndMass.z, p.previousAndMass.w);
+        v[i] = make_float4(p.velocity.x, p.velocity.y, p.velocity.z, p.velocity.w);
+    }
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess ||
+        cudaMemcpy(h->d.x, x.data(), count * sizeof(float4), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(h->d.xp, xp.data(), count * sizeof(float4), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(h->d.v, v.data(), count * sizeof(float4), cudaMemcpyHostToDevice) != cudaSuccess)
+        return NUMI_CLOTH_ECUDA;
+    return NUMI_CLOTH_OK;
+}
+
+static int copy_records(numi_cloth_t* h, void* dst, const void* src, size_t bytes, cudaMemcpyKind kind) {
+    cudaSetDevice(h->device);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return NUMI_CLOTH_ECUDA;
+    if (bytes && cudaMemcpy(dst, src, bytes, kind) != cudaSuccess) return NUMI_CLOTH_ECUDA;
+    return NUMI_CLOTH_OK;
+}
+
+int numi_cloth_read_fruits(numi_cloth_t* h, NumiClothFruit* out, uint32_t count) {
+    if (h == nullptr || (out == nullptr && count) || count != h->d.f_count) return NUMI_CLOTH_EINVAL;
+    return copy_records(h, out, h->d.fruits, count * sizeof(NumiClothFruit), cudaMemcpyDeviceToHost);
+}
+
+int numi_cloth_write_fruits(numi_cloth_t* h, const NumiClothFruit* in, uint32_t count) {
+    if (h == nullptr || (in == nullptr && count) || count != h->d.f_count) return NUMI_CLOTH_EINVAL;
+    return copy_records(h, h->d.fruits, in, count * sizeof(NumiClothFruit), cudaMemcpyHostToDevice);
+}
+
+int numi_cloth_read_grips(numi_cloth_t* h, NumiClothGrip* out, uint32_t count) {
+    if (h == nullptr || (out == nullptr && count) || count != h->d.g_count) return NUMI_CLOTH_EINVAL;
+    return copy_records(h, out, h->d.grips, count * sizeof(NumiClothGrip), cudaMemcpyDeviceToHost);
+}
+
+int numi_cloth_read_distances(numi_cloth_t* h, NumiClothDistance* out, uint32_t count) {
+    if (h == nullptr || out == nullptr || count != h->d.d_count) return NUMI_CLOTH_EINVAL;
+    std::vector<uint2> ij(count);
+    std::vector<float4> m(count);
+    std::vector<float> l(count);
+    int rc = copy_records(h, ij.data(), h->d.d_ij, count * sizeof(uint2), cudaMemcpyDeviceToHost);
+    if (rc == NUMI_CLOTH_OK) rc = copy_records(h, m.data(), h->d.d_mat, count * sizeof(float4), cudaMemcpyDeviceToHost);
+    if (rc == NUMI_CLOTH_OK) rc = copy_records(h, l.data(), h->d.d_lambda, count * sizeof(float), cudaMemcpyDeviceToHost);
+    if (rc != NUMI_CLOTH_OK) return rc;
+    for (uint32_t k = 0; k < count; ++k) {
+        out[k].particlesAndColor.x = ij[k].x;
+        out[k].particlesAndColor.y = ij[k].y;
+        out[k].material = {m[k].x, m[k].y, l[k], m[k].w};
+    }
+    return NUMI_CLOTH_OK;
+}
+
+int numi_cloth_residuals(numi_cloth_t* h, double out[4]) {
+    if (h == nullptr || out == nullptr) return NUMI_CLOTH_EINVAL;
+    cudaSetDevice(h->device);
+    const uint32_t grid = std::max<uint32_t>(1u, std::min<uint32_t>(h->grid, 4096u));
+    DeviceCloth d = h->d;
+    NumiClothConfig cfg = h->base;
+    numi_cloth_residual_kernel<<<grid, NC_THREADS, 0, h->stream>>>(d, cfg);
+    std::vector<double> r(3u * grid);
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(h->stream) != cudaSuccess ||
+        cudaMemcpy(r.data(), d.red, r.size() * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return NUMI_CLOTH_ECUDA;
+    out[0] = out[1] = out[2] = out[3] = 0.0;
+    for (uint32_t b = 0; b < grid; ++b)
+        for (int e = 0; e < 3; ++e) out[e] = std::max(out[e], r[3u * b + e]);
+    return NUMI_CLOTH_OK;
+}
+
+int numi_cloth_release_masks(numi_cloth_t* h, uint32_t out[2]) {
+    if (h == nullptr || out == nullptr) return NUMI_CLOTH_EINVAL;
+    out[0] = out[1] = 0u;
+    return NUMI_CLOTH_OK;
+}
+
+int numi_cloth_snapshot(numi_cloth_t* h, uint32_t slot) {
+    if (h == nullptr || slot >= kSnapshotSlots) return NUMI_CLOTH_EINVAL;
+    cudaSetDevice(h->device);
+    size_t total = 0;
+    for (const auto& r : h->dynamic) total += (r.bytes + 255u) & ~size_t(255u);
+    Snapshot& s = h->snaps[slot];
+    if (s.mem == nullptr) {
+        if (cudaMalloc(&s.mem, total) != cudaSuccess) return NUMI_CLOTH_ENOMEM;
+        s.bytes = total;
+    }
+    size_t off = 0;
+    for (const auto& r : h->dynamic) {
+        if (cudaMemcpyAsync(static_cast<char*>(s.mem) + off, r.ptr, r.bytes, cudaMemcpyDeviceToDevice, h->stream) !=
+            cudaSuccess)
+            return NUMI_CLOTH_ECUDA;
+        off += (r.bytes + 255u) & ~size_t(255u);
+    }
+    s.valid = true;
+    return NUMI_CLOTH_OK;
+}
+
+int numi_cloth_restore(numi_cloth_t* h, uint32_t slot) {
+    if (h == nullptr || slot >= kSnapshotSlots || !h->snaps[slot].valid) return NUMI_CLOTH_EINVAL;
+    cudaSetDevice(h->device);
+    size_t off = 0;
+    for (const auto& r : h->dynamic) {
+        if (cudaMemcpyAsync(r.ptr, static_cast<char*>(h->snaps[slot].mem) + off, r.bytes, cudaMemcpyDeviceToDevice,
+                            h->stream) != cudaSuccess)
+            return NUMI_CLOTH_ECUDA;
+        off += (r.bytes + 255u) & ~size_t(255u);
+    }
+    return NUMI_CLOTH_OK;
+}
+
+int numi_cloth_launch_info(numi_cloth_t* h, uint32_t out[4]) {
+    if (h == nullptr || out == nullptr) return NUMI_CLOTH_EINVAL;
+    cudaSetDevice(h->device);
+    uint32_t stats[4] = {0, 0, 0, 0};
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess ||
+        cudaMemcpy(stats, h->d.stats, sizeof(stats), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return NUMI_CLOTH_ECUDA;
+    out[0] = h->grid;
+    out[1] = h->block;
+    out[2] = stats[0];
+    out[3] = h->launches;
+    return NUMI_CLOTH_OK;
+}
+
+}  // extern "C"

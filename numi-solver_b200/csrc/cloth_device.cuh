@@ -1,0 +1,113 @@
+// Device-side layout of one cloth solver handle.
+//
+// HBM layout (structure of arrays; every array is 16-byte aligned):
+//   x      float4[N]  position xyz, inverse mass w
+//   xp     float4[N]  position at substep start xyz, mass w
+//   v      float4[N]  velocity xyz; w holds the predicted vertical velocity
+//                     during a substep and the cloth/ground normal impulse
+//                     after finalize (the reference's velocity.w)
+//   rest   float4[N]  rest position xyz (used for inverse mass 0)
+//   dist   uint2 ij[D], float4 mat[D] (rest, compliance, -, max extension),
+//          float lambda[D]
+//   knot   uint4 ij[K], float2 mat[K] (rest cosine, compliance), float lambda[K]
+//   bend   uint4 ij[B] (first, middle, third, -), float2 mat[B]
+//          (rest chord, compliance), float lambda[B]
+//   grips / fruits / fruit pairs keep the 48/96/32-byte ABI records (tiny).
+// Constraint arrays are grouped by colour; a batch is a contiguous run.
+#pragma once
+
+#include <stdint.h>
+
+#include "numi_cloth.h"
+
+#define NC_MAX_FRUITS 64u
+#define NC_MAX_GRIPS 32u
+#define NC_MAX_BATCHES 64u
+#define NC_YARN_SLOTS 4u
+
+struct Batch {
+    uint32_t first;
+    uint32_t count;      // all records of the colour
+    uint32_t limited;    // leading records that may carry a strain limit
+    uint32_t yarn;       // leading records that are yarn segments
+};
+
+struct DeviceCloth {
+    // particles
+    float4* x;
+    float4* xp;
+    float4* v;
+    const float4* rest;
+    uint32_t n;
+    // distances
+    const uint2* d_ij;
+    const float4* d_mat;
+    float* d_lambda;
+    uint32_t d_count;
+    // knots
+    const uint4* k_ij;
+    const float2* k_mat;
+    float* k_lambda;
+    uint32_t k_count;
+    // bends
+    const uint4* b_ij;
+    const float2* b_mat;
+    float* b_lambda;
+    uint32_t b_count;
+    // grips, fruits, pairs (ABI records)
+    NumiClothGrip* grips;
+    uint32_t g_count;
+    NumiClothFruit* fruits;
+    uint32_t f_count;
+    NumiClothFruitPair* pairs;
+    uint32_t p_count;
+    const uint32_t* cuff;
+    // fruit/yarn contact records, NC_YARN_SLOTS per yarn segment:
+    //   a = (impulse-weighted normal on the fruit xyz, normal impulse)
+    //   b = (impulse-weighted segment weights xy, tag bits, 0)
+    // tag = (substep epoch << 6) | fruit; a record is live only while its
+    // epoch is the current substep, so nothing is cleared between substeps.
+    float4* yarn_slot_a;
+    float4* yarn_slot_b;
+    // per-particle yarn air force of the current substep
+    float4* force;
+    // 2^-40 fixed-point fruit sums (int64 two's complement):
+    // [0, 3*64) displacement xyz, [3*64, 9*64) velocity and spin xyz
+    float4* fruit_partial;
+    // batches
+    Batch dist_batches[NC_MAX_BATCHES];
+    Batch knot_batches[NC_MAX_BATCHES];
+    Batch bend_batches[NC_MAX_BATCHES];
+    Batch pair_batches[NC_MAX_BATCHES];
+    uint32_t n_dist_batches, n_knot_batches, n_bend_batches, n_pair_batches;
+    // configs for this launch
+    const NumiClothConfig* cfg;
+    // control
+    unsigned int* failure;
+    unsigned int* bar_count;
+    unsigned int* bar_gen;
+    unsigned int* abort_flag;
+    double* red;          // [blocks * 8] reduction partials
+    uint32_t* stats;      // [0] barriers of the last substep, [1] reconcile passes max, [2] certificate passes max
+    uint32_t epoch_base;  // substep counter of the handle at launch
+    uint32_t grid_width;  // row-major grid topology (square cloth) or 0
+    const uint32_t* local_off;
+    const uint32_t* local_idx;
+};
+
+struct Schedule {
+    uint32_t iterations;
+    uint32_t strain_sweeps;
+    uint32_t reconcile_passes;
+    uint32_t final_passes;
+    uint32_t certificate_passes;
+    uint32_t early_exit;
+    uint32_t self_collision;
+    uint32_t aerodynamics;
+    uint32_t swept_ground;
+    uint32_t swept_fruit_yarn;
+    uint32_t frictions;
+    uint32_t release;
+    float damping;
+    uint32_t substeps;
+};

@@ -1,0 +1,759 @@
+// The frame kernel: all phases of `substeps` substeps in one cooperative
+// launch.  See cloth_kernels.cuh for the phase order and the per-phase
+// equations.
+#pragma once
+
+#include "cloth_kernels.cuh"
+
+namespace nc {
+
+struct Ctx {
+    const DeviceCloth& d;
+    const Schedule& s;
+    SubCfg c;
+    uint32_t tid;
+    uint32_t nthreads;
+    bool fruit_cta;
+    bool grip_cta;
+    uint32_t barriers;
+    bool fruit_pending;   // fixed-point fruit sums waiting to be applied
+    uint32_t epoch;
+};
+
+#define NC_SYNC(ctx) \
+    do { if (!grid_sync((ctx).d, (ctx).barriers)) return false; } while (0)
+
+// Apply (and clear) the fixed-point fruit displacement sums.  Fruit CTA.
+__device__ void fruit_flush(Ctx& ctx) {
+    if (!ctx.fruit_pending) return;
+    ctx.fruit_pending = false;
+    if (!ctx.fruit_cta) return;
+    const DeviceCloth& d = ctx.d;
+    unsigned long long* acc = reinterpret_cast<unsigned long long*>(d.fruit_partial);
+    for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
+        NumiClothFruit& fr = d.fruits[f];
+        const unsigned long long ax = atomicExch(acc + 3u * f + 0u, 0ull);
+        const unsigned long long ay = atomicExch(acc + 3u * f + 1u, 0ull);
+        const unsigned long long az = atomicExch(acc + 3u * f + 2u, 0ull);
+        fr.positionAndInverseMass.x = fr.positionAndInverseMass.x + from_fixed(ax);
+        fr.positionAndInverseMass.y = fr.positionAndInverseMass.y + from_fixed(ay);
+        fr.positionAndInverseMass.z = fr.positionAndInverseMass.z + from_fixed(az);
+    }
+    __syncthreads();
+}
+
+// Fruit/yarn velocity sums of the friction sweep (v then omega).
+__device__ void fruit_flush_velocity(Ctx& ctx) {
+    if (!ctx.fruit_cta) return;
+    const DeviceCloth& d = ctx.d;
+    unsigned long long* acc = reinterpret_cast<unsigned long long*>(d.fruit_partial) + 3u * NC_MAX_FRUITS;
+    for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
+        NumiClothFruit& fr = d.fruits[f];
+        float* v = &fr.velocityAndGroundImpulse.x;
+        float* w = &fr.angularVelocity.x;
+        for (int k = 0; k < 3; ++k) v[k] = v[k] + from_fixed(atomicExch(acc + 6u * f + k, 0ull));
+        for (int k = 0; k < 3; ++k) w[k] = w[k] + from_fixed(atomicExch(acc + 6u * f + 3u + k, 0ull));
+    }
+    __syncthreads();
+}
+
+// ------------------------------------------------------------ phases -----
+
+// Grip attach + begin + advance (+ swept ground), aero off.
+__device__ void phase_begin(Ctx& ctx) {
+    const DeviceCloth& d = ctx.d;
+    const SubCfg& c = ctx.c;
+    if (ctx.grip_cta) {
+        grip_attach(d, c);
+        __syncthreads();
+        for (uint32_t g = threadIdx.x; g < d.g_count; g += blockDim.x) {
+            d.grips[g].lambda.x = 0.0f;
+            d.grips[g].lambda.y = 0.0f;
+            d.grips[g].lambda.z = 0.0f;
+        }
+    }
+    const float dt = c.dt;
+    const float inv_dt = 1.0f / dt;
+    const bool air = ctx.s.aerodynamics != 0u;
+    const float damp = ctx.s.damping;
+    for (uint32_t i = ctx.tid; i < d.n; i += ctx.nthreads) {
+        float4 p = ld(d.x + i);
+        const float4 pp = ld(d.xp + i);
+        float4 vv = ld(d.v + i);
+        V3 pos = xyz(p);
+        const V3 prev = pos;
+        V3 vel = xyz(vv);
+        if (p.w == 0.0f) {
+            pos = xyz(__ldg(d.rest + i));
+            vel = (pos - prev) * inv_dt;
+        } else {
+            vel = vel + c.gravity * dt;
+            if (damp != 0.0f) vel = vel * (1.0f / (1.0f + damp * dt));
+            if (!air) {
+                pos = pos + vel * dt;
+            }
+        }
+        if (!air && ctx.s.swept_ground && c.ground && prev.z >= c.radius && pos.z < c.radius) pos.z = c.radius;
+        d.xp[i] = make_float4(prev.x, prev.y, prev.z, pp.w);
+        d.x[i] = with_xyz(p, pos);
+        d.v[i] = make_float4(vel.x, vel.y, vel.z, vel.z);
+    }
+    for (uint32_t k = ctx.tid; k < d.d_count; k += ctx.nthreads) d.d_lambda[k] = 0.0f;
+    for (uint32_t k = ctx.tid; k < d.k_count; k += ctx.nthreads) d.k_lambda[k] = 0.0f;
+    for (uint32_t k = ctx.tid; k < d.b_count; k += ctx.nthreads) d.b_lambda[k] = 0.0f;
+    if (ctx.fruit_cta) {
+        for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
+            FruitState s = load_fruit(d.fruits[f]);
+            s.prev = s.x;
+            s.v = s.v + c.gravity * dt;
+            s.ground_impulse = 0.0f;
+            if (air) fruit_air(s, c);
+            s.x = s.x + s.v * dt;
+            if (ctx.s.swept_ground && c.ground && s.prev.z >= s.radius && s.x.z < s.radius) {
+                const float adv = s.radius - s.x.z;
+                s.ground_impulse = s.ground_impulse + adv / (s.w * dt);
+                s.x.z = s.radius;
+            }
+            store_fruit(d.fruits[f], s);
+        }
+        for (uint32_t k = threadIdx.x; k < d.p_count; k += blockDim.x) d.pairs[k].contact = nf4<numi_float4>(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+}
+
+// Yarn air load (tools/cloth_bag.cpp:1013-1107): forces per yarn colour
+// (conflict-free), FP64 fixed-tree reductions of drag power and
+// inverse-mass-weighted force squared, then v += f * att * w * dt and the
+// deferred advance + swept ground.
+__device__ void air_force_batch(Ctx& ctx, const Batch& bt, float4* force) {
+    const DeviceCloth& d = ctx.d;
+    const SubCfg& c = ctx.c;
+    const float pi = 3.14159265358979323846f;
+    for (uint32_t k = ctx.tid; k < bt.yarn; k += ctx.nthreads) {
+        const uint32_t s = bt.first + k;
+        const uint2 ij = __ldg(d.d_ij + s);
+        const V3 a = xyz(ld(d.x + ij.x));
+        const V3 b = xyz(ld(d.x + ij.y));
+        const V3 span = b - a;
+        const float L = len3(span);
+        if (L < 1.0e-12f) continue;
+        const V3 axis = vdiv(span, L);
+        const V3 rel = (xyz(ld(d.v + ij.x)) + xyz(ld(d.v + ij.y))) * 0.5f - c.air;
+        const V3 axial = axis * dot3(rel, axis);
+        const V3 cross_v = rel - axial;
+        const float cross_area = 2.0f * c.radius * L;
+        const float wet_area = 2.0f * pi * c.radius * L;
+        const float ccoef = 0.5f * c.air_density * c.aero.x * cross_area;
+        const float scoef = 0.5f * c.air_density * c.aero.y * wet_area;
+        V3 f1{0.0f, 0.0f, 0.0f};
+        const float cs = len3(cross_v);
+        if (!(cs < 1.0e-14f || ccoef <= 0.0f)) f1 = cross_v * (-ccoef * cs);
+        V3 f2{0.0f, 0.0f, 0.0f};
+        const float as = len3(axial);
+        if (!(as < 1.0e-14f || scoef <= 0.0f)) f2 = axial * (-scoef * as);
+        const V3 f = f1 + f2;
+        const V3 half = f * 0.5f;
+        float4 fa = ld(force + ij.x);
+        float4 fb = ld(force + ij.y);
+        force[ij.x] = make_float4(fa.x + half.x, fa.y + half.y, fa.z + half.z, 0.0f);
+        force[ij.y] = make_float4(fb.x + half.x, fb.y + half.y, fb.z + half.z, 0.0f);
+    }
+}
+
+// Deterministic FP64 sum of two per-particle terms over 256-particle chunks
+// with a fixed tree; chunk partials land in red[2*chunk].
+__device__ void air_reduce_chunks(Ctx& ctx, const float4* force) {
+    const DeviceCloth& d = ctx.d;
+    __shared__ double s_p[NC_THREADS];
+    __shared__ double s_q[NC_THREADS];
+    const uint32_t chunks = (d.n + NC_THREADS - 1u) / NC_THREADS;
+    for (uint32_t ch = blockIdx.x; ch < chunks; ch += gridDim.x) {
+        const uint32_t i = ch * NC_THREADS + threadIdx.x;
+        double pw = 0.0, q = 0.0;
+        if (i < d.n) {
+            const float4 p = ld(d.x + i);
+            if (p.w > 0.0f) {
+                const V3 f = xyz(ld(force + i));
+                const V3 rv = xyz(ld(d.v + i)) - ctx.c.air;
+                pw = static_cast<double>(f.x) * rv.x + static_cast<double>(f.y) * rv.y +
+                     static_cast<double>(f.z) * rv.z;
+                q = static_cast<double>(p.w) * (static_cast<double>(f.x) * f.x +
+                                                static_cast<double>(f.y) * f.y +
+                                                static_cast<double>(f.z) * f.z);
+            }
+        }
+        s_p[threadIdx.x] = pw;
+        s_q[threadIdx.x] = q;
+        __syncthreads();
+        for (uint32_t st = NC_THREADS / 2u; st > 0u; st >>= 1u) {
+            if (threadIdx.x < st) {
+                s_p[threadIdx.x] += s_p[threadIdx.x + st];
+                s_q[threadIdx.x] += s_q[threadIdx.x + st];
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            d.red[2u * ch] = s_p[0];
+            d.red[2u * ch + 1u] = s_q[0];
+        }
+        __syncthreads();
+    }
+}
+
+// Every CTA reduces the chunk partials with the same fixed tree.
+__device__ float air_attenuation(Ctx& ctx) {
+    const DeviceCloth& d = ctx.d;
+    __shared__ double s_p[NC_THREADS];
+    __shared__ double s_q[NC_THREADS];
+    const uint32_t chunks = (d.n + NC_THREADS - 1u) / NC_THREADS;
+    double pw = 0.0, q = 0.0;
+    for (uint32_t ch = threadIdx.x; ch < chunks; ch += NC_THREADS) {
+        pw += __ldcg(d.red + 2u * ch);
+        q += __ldcg(d.red + 2u * ch + 1u);
+    }
+    s_p[threadIdx.x] = pw;
+    s_q[threadIdx.x] = q;
+    __syncthreads();
+    for (uint32_t st = NC_THREADS / 2u; st > 0u; st >>= 1u) {
+        if (threadIdx.x < st) {
+            s_p[threadIdx.x] += s_p[threadIdx.x + st];
+            s_q[threadIdx.x] += s_q[threadIdx.x + st];
+        }
+        __syncthreads();
+    }
+    const double power = s_p[0];
+    const double wsq = s_q[0];
+    __syncthreads();
+    double att = 1.0;
+    if (wsq > 0.0) att = power < 0.0 ? 1.0 / (1.0 + static_cast<double>(ctx.c.dt) * wsq / -power) : 0.0;
+    return static_cast<float>(att);
+}
+
+__device__ void air_apply_advance(Ctx& ctx, const float4* force, float att) {
+    const DeviceCloth& d = ctx.d;
+    const SubCfg& c = ctx.c;
+    const float dt = c.dt;
+    for (uint32_t i = ctx.tid; i < d.n; i += ctx.nthreads) {
+        float4 p = ld(d.x + i);
+        const V3 prev = xyz(ld(d.xp + i));
+        V3 vel = xyz(ld(d.v + i));
+        V3 pos = xyz(p);
+        if (p.w > 0.0f) {
+            vel = vel + xyz(ld(force + i)) * (att * p.w * dt);
+            pos = pos + vel * dt;
+        }
+        if (ctx.s.swept_ground && c.ground && prev.z >= c.radius && pos.z < c.radius) pos.z = c.radius;
+        d.x[i] = with_xyz(p, pos);
+        d.v[i] = make_float4(vel.x, vel.y, vel.z, vel.z);
+    }
+}
+
+// One yarn colour of the present fruit/yarn sweep
+// (tools/cloth_bag.cpp:2955-3020, 3141-3176).  Fruit positions are the
+// ones at the start of the sweep; each fruit's displacement is summed in
+// fixed point and applied by fruit_flush.
+__device__ void yarn_contact_batch(Ctx& ctx, const Batch& bt) {
+    const DeviceCloth& d = ctx.d;
+    const SubCfg& c = ctx.c;
+    __shared__ float4 s_fruit[NC_MAX_FRUITS];   // xyz position, w radius
+    __shared__ float s_fw[NC_MAX_FRUITS];
+    for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
+        const NumiClothFruit& fr = d.fruits[f];
+        s_fruit[f] = make_float4(__ldcg(&fr.positionAndInverseMass.x), __ldcg(&fr.positionAndInverseMass.y),
+                                 __ldcg(&fr.positionAndInverseMass.z), __ldcg(&fr.previousAndRadius.w));
+        s_fw[f] = __ldcg(&fr.positionAndInverseMass.w);
+    }
+    __syncthreads();
+    unsigned long long* acc = reinterpret_cast<unsigned long long*>(d.fruit_partial);
+    const uint32_t nf = d.f_count;
+    for (uint32_t k = ctx.tid; k < bt.yarn; k += ctx.nthreads) {
+        const uint32_t seg = bt.first + k;
+        const uint2 ij = __ldg(d.d_ij + seg);
+        float4 pa = ld(d.x + ij.x);
+        float4 pb = ld(d.x + ij.y);
+        bool changed = false;
+        for (uint32_t f = 0; f < nf; ++f) {
+            const float4 fs = s_fruit[f];
+            const V3 X{fs.x, fs.y, fs.z};
+            const float target = fs.w + c.radius;
+            if (X.x < fminf(pa.x, pb.x) - target || X.x > fmaxf(pa.x, pb.x) + target ||
+                X.y < fminf(pa.y, pb.y) - target || X.y > fmaxf(pa.y, pb.y) + target ||
+                X.z < fminf(pa.z, pb.z) - target || X.z > fmaxf(pa.z, pb.z) + target)
+                continue;
+            V3 closest;
+            float t;
+            point_segment(X, xyz(pa), xyz(pb), closest, t);
+            V3 sep = closest - X;
+            float dist = len3(sep);
+            if (dist >= target) continue;
+            if (dist < 1.0e-12f) {
+                const V3 sd = normalized3(xyz(pb) - xyz(pa));
+                sep = normalized3(cross3(sd, fabsf(sd.z) < 0.9f ? V3{0.0f, 0.0f, 1.0f} : V3{1.0f, 0.0f, 0.0f}));
+                dist = 0.0f;
+            }
+            const V3 n = normalized3(sep);
+            const float w0 = 1.0f - t;
+            const float w1 = t;
+            const float corr = target - dist;
+            V3 delta{0.0f, 0.0f, 0.0f};
+            const float lam = yarn_correction(pa, pb, w0, w1, s_fw[f], n, corr, c.ground, c.radius, delta);
+            changed = true;
+            if (delta.x != 0.0f || delta.y != 0.0f || delta.z != 0.0f) {
+                atomicAdd(acc + 3u * f + 0u, static_cast<unsigned long long>(to_fixed(delta.x)));
+                atomicAdd(acc + 3u * f + 1u, static_cast<unsigned long long>(to_fixed(delta.y)));
+                atomicAdd(acc + 3u * f + 2u, static_cast<unsigned long long>(to_fixed(delta.z)));
+            }
+            if (lam <= 0.0f) continue;
+            const float imp = lam / c.dt;
+            // Contact record of (fruit f, segment seg) for friction.
+            const uint32_t tag = (ctx.epoch << 6) | f;
+            int slot = -1;
+            for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q) {
+                const float4 sb = d.yarn_slot_b[seg * NC_YARN_SLOTS + q];
+                const uint32_t st = __float_as_uint(sb.z);
+                if (st == tag) { slot = static_cast<int>(q); break; }
+                if (slot < 0 && (st >> 6) != (ctx.epoch & 0x3ffffffu)) slot = static_cast<int>(q) | 0x100;
+            }
+            if (slot < 0) {
+                fail(d, NUMI_CLOTH_FAILURE_RANGE);
+                continue;
+            }
+            const uint32_t q = static_cast<uint32_t>(slot) & 0xffu;
+            float4 sa = make_float4(0, 0, 0, 0);
+            float4 sb = make_float4(0, 0, __uint_as_float(tag), 0);
+            if (!(slot & 0x100)) {
+                sa = d.yarn_slot_a[seg * NC_YARN_SLOTS + q];
+                sb = d.yarn_slot_b[seg * NC_YARN_SLOTS + q];
+            }
+            const V3 wn = V3{sa.x, sa.y, sa.z} - n * imp;
+            sa = make_float4(wn.x, wn.y, wn.z, sa.w + imp);
+            sb.x = sb.x + w0 * imp;
+            sb.y = sb.y + w1 * imp;
+            d.yarn_slot_a[seg * NC_YARN_SLOTS + q] = sa;
+            d.yarn_slot_b[seg * NC_YARN_SLOTS + q] = sb;
+        }
+        if (changed) {
+            d.x[ij.x] = pa;
+            d.x[ij.y] = pb;
+        }
+    }
+}
+
+__device__ bool yarn_sweep(Ctx& ctx) {
+    if (ctx.d.f_count == 0u) return true;
+    fruit_flush(ctx);
+    for (uint32_t b = 0; b < ctx.d.n_dist_batches; ++b) {
+        const Batch bt = ctx.d.dist_batches[b];
+        if (bt.yarn == 0u) continue;
+        yarn_contact_batch(ctx, bt);
+        NC_SYNC(ctx);
+    }
+    ctx.fruit_pending = true;
+    return true;
+}
+
+// Ground clamp (tools/cloth_bag.cpp:2655-2690).
+__device__ void phase_ground(Ctx& ctx) {
+    const DeviceCloth& d = ctx.d;
+    const SubCfg& c = ctx.c;
+    fruit_flush(ctx);
+    if (!c.ground) return;
+    for (uint32_t i = ctx.tid; i < d.n; i += ctx.nthreads) {
+        const float4 p = ld(d.x + i);
+        if (c.radius - p.z > 0.0f) d.x[i] = make_float4(p.x, p.y, c.radius, p.w);
+    }
+    if (ctx.fruit_cta) {
+        for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
+            NumiClothFruit& fr = d.fruits[f];
+            const float pen = fr.previousAndRadius.w - fr.positionAndInverseMass.z;
+            if (pen > 0.0f) {
+                fr.velocityAndGroundImpulse.w =
+                    fr.velocityAndGroundImpulse.w + pen / (fr.positionAndInverseMass.w * c.dt);
+                fr.positionAndInverseMass.z = fr.previousAndRadius.w;
+            }
+        }
+    }
+}
+
+__device__ bool strain_sweeps(Ctx& ctx) {
+    for (uint32_t sw = 0; sw < ctx.s.strain_sweeps; ++sw) {
+        for (uint32_t b = 0; b < ctx.d.n_dist_batches; ++b) {
+            const Batch bt = ctx.d.dist_batches[b];
+            if (bt.limited == 0u) continue;
+            fruit_flush(ctx);
+            for (uint32_t k = ctx.tid; k < bt.limited; k += ctx.nthreads) limit_strain(ctx.d, bt.first + k);
+            NC_SYNC(ctx);
+        }
+    }
+    return true;
+}
+
+// Residuals in FP64 (tools/cloth_bag.cpp:1765-1780, 1880-1895, 3111-3139);
+// max over blocks, every CTA reads all partials and takes the same decision.
+__device__ void residual_partials(Ctx& ctx, double* out3) {
+    const DeviceCloth& d = ctx.d;
+    const SubCfg& c = ctx.c;
+    double strain = 0.0, ground = 0.0, fruit = 0.0;
+    for (uint32_t k = ctx.tid; k < d.d_count; k += ctx.nthreads) {
+        const float4 m = __ldg(d.d_mat + k);
+        if (!(m.w > 0.0f)) continue;
+        const uint2 ij = __ldg(d.d_ij + k);
+        const float4 a = ld(d.x + ij.x);
+        const float4 b = ld(d.x + ij.y);
+        const double dx = static_cast<double>(b.x) - a.x, dy = static_cast<double>(b.y) - a.y,
+                     dz = static_cast<double>(b.z) - a.z;
+        const double L = sqrt((dx * dx + dy * dy) + dz * dz);
+        const double maxL = static_cast<double>(m.x) * (1.0 + static_cast<double>(m.w));
+        strain = fmax(strain, L - maxL);
+    }
+    if (c.ground) {
+        for (uint32_t i = ctx.tid; i < d.n; i += ctx.nthreads)
+            ground = fmax(ground, static_cast<double>(c.radius) - static_cast<double>(ld(d.x + i).z));
+        if (blockIdx.x == 0)
+            for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x)
+                ground = fmax(ground, static_cast<double>(__ldcg(&d.fruits[f].previousAndRadius.w)) -
+                                          static_cast<double>(__ldcg(&d.fruits[f].positionAndInverseMass.z)));
+    }
+    if (d.f_count > 0u) {
+        for (uint32_t b = 0; b < d.n_dist_batches; ++b) {
+            const Batch bt = d.dist_batches[b];
+            for (uint32_t k = ctx.tid; k < bt.yarn; k += ctx.nthreads) {
+                const uint2 ij = __ldg(d.d_ij + bt.first + k);
+                const float4 pa = ld(d.x + ij.x);
+                const float4 pb = ld(d.x + ij.y);
+                for (uint32_t f = 0; f < d.f_count; ++f) {
+                    const NumiClothFruit& fr = d.fruits[f];
+                    const double X[3] = {__ldcg(&fr.positionAndInverseMass.x), __ldcg(&fr.positionAndInverseMass.y),
+                                         __ldcg(&fr.positionAndInverseMass.z)};
+                    const double target = static_cast<double>(__ldcg(&fr.previousAndRadius.w)) + c.radius;
+                    const double A[3] = {pa.x, pa.y, pa.z};
+                    const double B[3] = {pb.x, pb.y, pb.z};
+                    bool outside = false;
+                    for (int e = 0; e < 3; ++e)
+                        outside = outside || X[e] < fmin(A[e], B[e]) - target || X[e] > fmax(A[e], B[e]) + target;
+                    if (outside) continue;
+                    const double dir[3] = {B[0] - A[0], B[1] - A[1], B[2] - A[2]};
+                    const double lb = (dir[0] * dir[0] + dir[1] * dir[1]) + dir[2] * dir[2];
+                    double t = 0.0;
+                    if (lb > 1.0e-20) {
+                        const double proj = (dir[0] * (X[0] - A[0]) + dir[1] * (X[1] - A[1])) + dir[2] * (X[2] - A[2]);
+                        t = fmin(fmax(proj / lb, 0.0), 1.0);
+                    }
+                    const double cx = A[0] + dir[0] * t - X[0], cy = A[1] + dir[1] * t - X[1],
+                                 cz = A[2] + dir[2] * t - X[2];
+                    fruit = fmax(fruit, target - sqrt((cx * cx + cy * cy) + cz * cz));
+                }
+            }
+        }
+    }
+    __shared__ double s_r[3][NC_THREADS];
+    s_r[0][threadIdx.x] = strain;
+    s_r[1][threadIdx.x] = ground;
+    s_r[2][threadIdx.x] = fruit;
+    __syncthreads();
+    for (uint32_t st = NC_THREADS / 2u; st > 0u; st >>= 1u) {
+        if (threadIdx.x < st)
+            for (int e = 0; e < 3; ++e) s_r[e][threadIdx.x] = fmax(s_r[e][threadIdx.x], s_r[e][threadIdx.x + st]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int e = 0; e < 3; ++e) out3[3u * blockIdx.x + e] = s_r[e][0];
+    __syncthreads();
+}
+
+__device__ bool residuals_converged(Ctx& ctx) {
+    const DeviceCloth& d = ctx.d;
+    __shared__ double s_r[3][NC_THREADS];
+    double r[3] = {0.0, 0.0, 0.0};
+    for (uint32_t b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+        for (int e = 0; e < 3; ++e) r[e] = fmax(r[e], __ldcg(d.red + 3u * b + e));
+    for (int e = 0; e < 3; ++e) s_r[e][threadIdx.x] = r[e];
+    __syncthreads();
+    for (uint32_t st = NC_THREADS / 2u; st > 0u; st >>= 1u) {
+        if (threadIdx.x < st)
+            for (int e = 0; e < 3; ++e) s_r[e][threadIdx.x] = fmax(s_r[e][threadIdx.x], s_r[e][threadIdx.x + st]);
+        __syncthreads();
+    }
+    const bool ok = s_r[2][0] < 1.0e-6 && s_r[1][0] < 1.0e-9 && s_r[0][0] < 1.0e-6;
+    __syncthreads();
+    return ok;
+}
+
+__device__ bool contacts_pass(Ctx& ctx, bool with_strain) {
+    // fruit pairs (fruit CTA) -> fruit/yarn -> [strain] -> ground
+    if (ctx.fruit_cta && ctx.d.p_count > 0u) {
+        fruit_flush(ctx);
+        fruit_pair_sweep(ctx.d, ctx.c.dt);
+    }
+    if (ctx.d.p_count > 0u) NC_SYNC(ctx);
+    if (!yarn_sweep(ctx)) return false;
+    if (with_strain && !strain_sweeps(ctx)) return false;
+    phase_ground(ctx);
+    NC_SYNC(ctx);
+    return true;
+}
+
+// Finalize + cloth/ground friction (tools/cloth_bag.cpp:5186-5211, 2076-2115).
+__device__ void phase_finalize(Ctx& ctx) {
+    const DeviceCloth& d = ctx.d;
+    const SubCfg& c = ctx.c;
+    fruit_flush(ctx);
+    const float inv_dt = 1.0f / c.dt;
+    for (uint32_t i = ctx.tid; i < d.n; i += ctx.nthreads) {
+        float4 p = ld(d.x + i);
+        const V3 prev = xyz(ld(d.xp + i));
+        const float4 vv = ld(d.v + i);
+        V3 pos = xyz(p);
+        V3 vel;
+        float gi = 0.0f;
+        if (p.w == 0.0f) {
+            pos = xyz(__ldg(d.rest + i));
+            vel = (pos - prev) * inv_dt;
+            d.x[i] = with_xyz(p, pos);
+        } else {
+            vel = (pos - prev) * inv_dt;
+            if (c.ground && pos.z <= c.radius + 1.0e-6f) {
+                const float nvc = vel.z - vv.w;
+                gi = fmaxf(0.0f, nvc / p.w);
+            }
+            if (ctx.s.frictions && gi > 0.0f) {
+                const V3 tv{vel.x, vel.y, 0.0f};
+                const float slip = len3(tv);
+                if (!(slip < 1.0e-10f)) {
+                    const float limit = c.mu_cloth_ground * gi;
+                    const float ti = fminf(slip / p.w, limit);
+                    if (ti > 0.0f) vel = vel - tv * (ti * p.w / slip);
+                }
+            }
+        }
+        if (!finite3(vel)) fail(d, NUMI_CLOTH_FAILURE_NONFINITE);
+        d.v[i] = make_float4(vel.x, vel.y, vel.z, gi);
+    }
+    if (ctx.fruit_cta) {
+        for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
+            FruitState s = load_fruit(d.fruits[f]);
+            s.v = (s.x - s.prev) * inv_dt;
+            if (!finite3(s.x) || !finite3(s.v)) fail(d, NUMI_CLOTH_FAILURE_NONFINITE);
+            store_fruit(d.fruits[f], s);
+        }
+    }
+}
+
+// Fruit/yarn Coulomb friction (tools/cloth_bag.cpp:3178-3270), one yarn
+// colour; fruit velocities are those at the start of the friction sweep.
+__device__ void yarn_friction_batch(Ctx& ctx, const Batch& bt) {
+    const DeviceCloth& d = ctx.d;
+    const SubCfg& c = ctx.c;
+    unsigned long long* acc = reinterpret_cast<unsigned long long*>(d.fruit_partial) + 3u * NC_MAX_FRUITS;
+    for (uint32_t k = ctx.tid; k < bt.yarn; k += ctx.nthreads) {
+        const uint32_t seg = bt.first + k;
+        bool any = false;
+        for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q) {
+            const uint32_t st = __float_as_uint(__ldcg(&d.yarn_slot_b[seg * NC_YARN_SLOTS + q].z));
+            any = any || ((st >> 6) == (ctx.epoch & 0x3ffffffu));
+        }
+        if (!any) continue;
+        const uint2 ij = __ldg(d.d_ij + seg);
+        const float4 pa = ld(d.x + ij.x);
+        const float4 pb = ld(d.x + ij.y);
+        float4 va = ld(d.v + ij.x);
+        float4 vb = ld(d.v + ij.y);
+        // Fruits of this segment in ascending fruit order.
+        for (uint32_t f = 0; f < d.f_count; ++f) {
+            int slot = -1;
+            const uint32_t tag = (ctx.epoch << 6) | f;
+            for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q)
+                if (__float_as_uint(__ldcg(&d.yarn_slot_b[seg * NC_YARN_SLOTS + q].z)) == tag) slot = static_cast<int>(q);
+            if (slot < 0) continue;
+            const float4 sa = __ldcg(&d.yarn_slot_a[seg * NC_YARN_SLOTS + slot]);
+            const float4 sb = __ldcg(&d.yarn_slot_b[seg * NC_YARN_SLOTS + slot]);
+            const float ni = sa.w;
+            const V3 wn{sa.x, sa.y, sa.z};
+            if (ni <= 0.0f || lsq(wn) < 1.0e-20f) continue;
+            const FruitState fr = load_fruit(d.fruits[f]);
+            const V3 normal = normalized3(wn);
+            float wt[2] = {sb.x / ni, sb.y / ni};
+            const float sum = wt[0] + wt[1];
+            if (sum <= 1.0e-12f) continue;
+            wt[0] = wt[0] / sum;
+            wt[1] = wt[1] / sum;
+            const V3 yv = (V3{0.0f, 0.0f, 0.0f} + xyz(va) * wt[0]) + xyz(vb) * wt[1];
+            const V3 off = normal * -fr.radius;
+            const V3 bcv = fr.v + cross3(fr.omega, off);
+            const V3 rel = bcv - yv;
+            const V3 tv = rel - normal * dot3(rel, normal);
+            const float slip = len3(tv);
+            if (slip < 1.0e-10f) continue;
+            const V3 t = vdiv(tv, slip);
+            const float inv_i = inverse_inertia(fr.w, fr.radius);
+            float den = fr.w + inv_i * lsq(cross3(off, t));
+            V3 resp[2];
+            const float4* pp[2] = {&pa, &pb};
+            for (int s = 0; s < 2; ++s) {
+                resp[s] = t * pp[s]->w;
+                if (c.ground && pp[s]->z <= c.radius + 1.0e-6f && resp[s].z < 0.0f) resp[s].z = 0.0f;
+                den = den + dot3(t, resp[s]) * wt[s] * wt[s];
+            }
+            if (den <= 0.0f) continue;
+            const float limit = c.mu_fruit_yarn * ni;
+            const float ti = fminf(slip / den, limit);
+            if (ti <= 0.0f) continue;
+            const V3 imp = t * -ti;
+            const V3 dv = imp * fr.w;
+            const V3 dw = cross3(off, imp) * inv_i;
+            atomicAdd(acc + 6u * f + 0u, static_cast<unsigned long long>(to_fixed(dv.x)));
+            atomicAdd(acc + 6u * f + 1u, static_cast<unsigned long long>(to_fixed(dv.y)));
+            atomicAdd(acc + 6u * f + 2u, static_cast<unsigned long long>(to_fixed(dv.z)));
+            atomicAdd(acc + 6u * f + 3u, static_cast<unsigned long long>(to_fixed(dw.x)));
+            atomicAdd(acc + 6u * f + 4u, static_cast<unsigned long long>(to_fixed(dw.y)));
+            atomicAdd(acc + 6u * f + 5u, static_cast<unsigned long long>(to_fixed(dw.z)));
+            const V3 na = xyz(va) + resp[0] * (ti * wt[0]);
+            const V3 nb = xyz(vb) + resp[1] * (ti * wt[1]);
+            va = with_xyz(va, na);
+            vb = with_xyz(vb, nb);
+        }
+        d.v[ij.x] = va;
+        d.v[ij.y] = vb;
+    }
+}
+
+// Fruit frictions and orientation in the fruit CTA.
+__device__ void fruit_tail(Ctx& ctx) {
+    if (!ctx.fruit_cta) return;
+    const DeviceCloth& d = ctx.d;
+    const SubCfg& c = ctx.c;
+    if (ctx.s.frictions) {
+        for (uint32_t b = 0; b < d.n_pair_batches; ++b) {
+            const Batch bt = d.pair_batches[b];
+            for (uint32_t k = threadIdx.x; k < bt.count; k += blockDim.x) fruit_pair_friction(d, bt.first + k, c.mu_pair);
+            __syncthreads();
+        }
+    }
+    for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
+        FruitState s = load_fruit(d.fruits[f]);
+        if (ctx.s.frictions) fruit_ground_friction(s, c);
+        integrate_orientation(s, c.dt);
+        store_fruit(d.fruits[f], s);
+    }
+    __syncthreads();
+}
+
+// One substep.  Returns false when a barrier gave up.
+__device__ bool substep(Ctx& ctx, bool last) {
+    const DeviceCloth& d = ctx.d;
+    const Schedule& s = ctx.s;
+    const float dt2 = ctx.c.dt * ctx.c.dt;
+    phase_begin(ctx);
+    NC_SYNC(ctx);
+    if (s.aerodynamics) {
+        float4* force = d.force;
+        for (uint32_t i = ctx.tid; i < d.n; i += ctx.nthreads) force[i] = make_float4(0, 0, 0, 0);
+        NC_SYNC(ctx);
+        for (uint32_t b = 0; b < d.n_dist_batches; ++b) {
+            if (d.dist_batches[b].yarn == 0u) continue;
+            air_force_batch(ctx, d.dist_batches[b], force);
+            NC_SYNC(ctx);
+        }
+        air_reduce_chunks(ctx, force);
+        NC_SYNC(ctx);
+        const float att = air_attenuation(ctx);
+        air_apply_advance(ctx, force, att);
+        NC_SYNC(ctx);
+    }
+    for (uint32_t it = 0; it < s.iterations; ++it) {
+        for (uint32_t b = 0; b < d.n_dist_batches; ++b) {
+            const Batch bt = d.dist_batches[b];
+            fruit_flush(ctx);
+            for (uint32_t k = ctx.tid; k < bt.count; k += ctx.nthreads) solve_distance(d, bt.first + k, dt2);
+            NC_SYNC(ctx);
+        }
+        for (uint32_t b = 0; b < d.n_knot_batches; ++b) {
+            const Batch bt = d.knot_batches[b];
+            for (uint32_t k = ctx.tid; k < bt.count; k += ctx.nthreads) solve_knot(d, bt.first + k, dt2);
+            NC_SYNC(ctx);
+        }
+        if ((it & 1u) == 0u) {
+            for (uint32_t b = 0; b < d.n_bend_batches; ++b) {
+                const Batch bt = d.bend_batches[b];
+                for (uint32_t k = ctx.tid; k < bt.count; k += ctx.nthreads)
+                    solve_bend(d, bt.first + k, dt2, ctx.c.radius, ctx.c.ground);
+                NC_SYNC(ctx);
+            }
+        }
+        // grips (CTA 0) and fruit pairs (fruit CTA) touch disjoint state
+        if (ctx.grip_cta) solve_grips(d, ctx.c);
+        if (ctx.fruit_cta && d.p_count > 0u) {
+            __syncthreads();
+            fruit_pair_sweep(d, ctx.c.dt);
+        }
+        NC_SYNC(ctx);
+        if (!yarn_sweep(ctx)) return false;
+        phase_ground(ctx);
+        NC_SYNC(ctx);
+    }
+    // reconciliation (tools/cloth_bag.cpp:4975-5058)
+    uint32_t passes = 0;
+    for (uint32_t p = 0; p < s.reconcile_passes; ++p) {
+        if (!contacts_pass(ctx, true)) return false;
+        passes = p + 1u;
+        if (s.early_exit) {
+            residual_partials(ctx, d.red);
+            NC_SYNC(ctx);
+            const bool ok = residuals_converged(ctx);
+            NC_SYNC(ctx);
+            if (ok) break;
+        }
+    }
+    // endpoint strain + final contacts (tools/cloth_bag.cpp:5059-5142)
+    if (!strain_sweeps(ctx)) return false;
+    for (uint32_t p = 0; p < s.final_passes; ++p)
+        if (!contacts_pass(ctx, false)) return false;
+    uint32_t cert = 0;
+    if (last) {
+        for (uint32_t p = 0; p < s.certificate_passes; ++p) {
+            if (!strain_sweeps(ctx)) return false;
+            for (uint32_t q = 0; q < s.final_passes; ++q)
+                if (!contacts_pass(ctx, false)) return false;
+            cert = p + 1u;
+            residual_partials(ctx, d.red);
+            NC_SYNC(ctx);
+            const bool ok = residuals_converged(ctx);
+            NC_SYNC(ctx);
+            if (ok) break;
+        }
+    }
+    phase_finalize(ctx);
+    NC_SYNC(ctx);
+    if (s.frictions && d.f_count > 0u) {
+        for (uint32_t b = 0; b < d.n_dist_batches; ++b) {
+            if (d.dist_batches[b].yarn == 0u) continue;
+            yarn_friction_batch(ctx, d.dist_batches[b]);
+            NC_SYNC(ctx);
+        }
+        fruit_flush_velocity(ctx);
+    }
+    fruit_tail(ctx);
+    NC_SYNC(ctx);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        d.stats[1] = max(d.stats[1], passes);
+        d.stats[2] = max(d.stats[2], cert);
+    }
+    return true;
+}
+
+}  // namespace nc
+
+__global__ void __launch_bounds__(NC_THREADS) numi_cloth_frame_kernel(DeviceCloth d, Schedule s) {
+    nc::Ctx ctx{d, s};
+    ctx.tid = blockIdx.x * blockDim.x + threadIdx.x;
+    ctx.nthreads = gridDim.x * blockDim.x;
+    ctx.fruit_cta = blockIdx.x == gridDim.x - 1u;
+    ctx.grip_cta = blockIdx.x == 0u;
+    ctx.fruit_pending = false;
+    for (uint32_t sub = 0; sub < s.substeps; ++sub) {
+        ctx.c = nc::load_cfg(d.cfg + sub);
+        ctx.epoch = d.epoch_base + sub;
+        ctx.barriers = 0;
+        if (!nc::substep(ctx, sub + 1u == s.substeps)) return;
+        if (blockIdx.x == 0 && threadIdx.x == 0) d.stats[0] = ctx.barriers;
+    }
+}

@@ -1,0 +1,445 @@
+"""Python binding of the B200 XPBD cloth substep library (libnumi_cloth.so).
+
+The product is the C ABI in include/numi_cloth.h and include/numi_cloth_scene.h;
+this module is a thin ctypes mirror of it for tests, the benchmark and
+calibration scripts.  It mirrors the reference host's roles: scene
+construction (tools/cloth_bag.cpp:610-973 / tools/cloth_bag_metal.mm:524-1274),
+the per-frame substep launch (runGPU, tools/cloth_bag_metal.mm:4010) and the
+--material / --grip-trajectory contracts.  There is no CPU fallback: without
+the built library every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import abi
+from .abi import (
+    BEND,
+    CONFIG,
+    DISTANCE,
+    FLOAT4,
+    FRUIT,
+    FRUIT_PAIR,
+    GRIP,
+    KNOT,
+    PARTICLE,
+    Material,
+    Schedule,
+    SquareSpec,
+    failure_names,
+)
+
+__all__ = [
+    "abi",
+    "Schedule",
+    "Material",
+    "SquareSpec",
+    "SceneArrays",
+    "ClothSolver",
+    "ClothError",
+    "library_path",
+    "load_library",
+    "bag_scene",
+    "square_scene",
+    "material_defaults",
+    "load_material",
+    "GripTrajectory",
+    "failure_names",
+]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+
+class ClothError(RuntimeError):
+    pass
+
+
+def library_path() -> str:
+    return os.path.join(_HERE, "libnumi_cloth.so")
+
+
+def load_library() -> ctypes.CDLL:
+    """Load the in-tree library; raise loudly when it is not built."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = library_path()
+    if not os.path.exists(path):
+        raise ClothError(f"libnumi_cloth.so is not built ({path}); run `make -C numi-solver_b200`")
+    lib = ctypes.CDLL(path)
+    vp, u32, i32 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int
+    sigs = {
+        "numi_cloth_version": (ctypes.c_char_p, []),
+        "numi_cloth_create": (i32, [vp, ctypes.POINTER(vp)]),
+        "numi_cloth_destroy": (None, [vp]),
+        "numi_cloth_set_stream": (i32, [vp, vp]),
+        "numi_cloth_step": (i32, [vp, vp, u32, ctypes.POINTER(Schedule)]),
+        "numi_cloth_failure": (u32, [vp]),
+        "numi_cloth_read_particles": (i32, [vp, vp, u32]),
+        "numi_cloth_write_particles": (i32, [vp, vp, u32]),
+        "numi_cloth_read_fruits": (i32, [vp, vp, u32]),
+        "numi_cloth_write_fruits": (i32, [vp, vp, u32]),
+        "numi_cloth_read_distances": (i32, [vp, vp, u32]),
+        "numi_cloth_read_grips": (i32, [vp, vp, u32]),
+        "numi_cloth_residuals": (i32, [vp, ctypes.POINTER(ctypes.c_double)]),
+        "numi_cloth_release_masks": (i32, [vp, ctypes.POINTER(u32)]),
+        "numi_cloth_snapshot": (i32, [vp, u32]),
+        "numi_cloth_restore": (i32, [vp, u32]),
+        "numi_cloth_launch_info": (i32, [vp, ctypes.POINTER(u32)]),
+        "numi_cloth_material_defaults": (None, [ctypes.POINTER(Material)]),
+        "numi_cloth_material_load": (i32, [ctypes.c_char_p, ctypes.POINTER(Material), ctypes.c_char_p, ctypes.c_size_t]),
+        "numi_cloth_scene_bag": (vp, [ctypes.POINTER(Material), i32, ctypes.c_double, i32]),
+        "numi_cloth_square_defaults": (None, [ctypes.POINTER(SquareSpec)]),
+        "numi_cloth_scene_square": (vp, [ctypes.POINTER(SquareSpec), ctypes.POINTER(Material)]),
+        "numi_cloth_scene_destroy": (None, [vp]),
+        "numi_cloth_scene_view": (i32, [vp, ctypes.POINTER(abi.SceneStruct)]),
+        "numi_cloth_scene_counts": (i32, [vp, ctypes.POINTER(u32)]),
+        "numi_cloth_scene_rest_fp64": (i32, [vp, ctypes.POINTER(ctypes.c_double)]),
+        "numi_cloth_trajectory_load": (vp, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t]),
+        "numi_cloth_trajectory_destroy": (None, [vp]),
+        "numi_cloth_trajectory_sample": (i32, [vp, ctypes.c_double, ctypes.POINTER(abi.GripPose)]),
+        "numi_cloth_trajectory_info": (
+            i32,
+            [vp, ctypes.POINTER(u32), ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_uint64)],
+        ),
+        "numi_cloth_trajectory_configs": (
+            i32,
+            [vp, vp, ctypes.POINTER(ctypes.c_double), ctypes.c_uint64, u32, ctypes.c_double, vp],
+        ),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = lib
+    return lib
+
+
+def _ptr(a: np.ndarray | None):
+    return None if a is None or a.size == 0 else ctypes.c_void_p(a.ctypes.data)
+
+
+def material_defaults() -> Material:
+    m = Material()
+    load_library().numi_cloth_material_defaults(ctypes.byref(m))
+    return m
+
+
+def load_material(path: str) -> Material:
+    """Parse a numi.cloth.material.v1 artifact (rejections raise ClothError)."""
+    m = Material()
+    err = ctypes.create_string_buffer(512)
+    if load_library().numi_cloth_material_load(path.encode(), ctypes.byref(m), err, 512) != 0:
+        raise ClothError(err.value.decode())
+    return m
+
+
+@dataclass
+class SceneArrays:
+    """The arrays numi_cloth_create takes, as ABI-record NumPy arrays."""
+
+    config: np.ndarray                       # CONFIG[1]
+    particles: np.ndarray                    # PARTICLE[N]
+    rest: np.ndarray                         # float4[N]
+    distances: np.ndarray                    # DISTANCE[D]
+    knots: np.ndarray                        # KNOT[K]
+    bends: np.ndarray                        # BEND[B]
+    grips: np.ndarray                        # GRIP[G]
+    fruits: np.ndarray                       # FRUIT[F]
+    pairs: np.ndarray                        # FRUIT_PAIR[P]
+    cuff: np.ndarray                         # uint32[2 * rings]
+    rim: np.ndarray                          # uint32[rim]
+    local_off: np.ndarray | None = None      # uint32[N+1]
+    local_idx: np.ndarray | None = None
+    grid_width: int = 0
+    rest64: np.ndarray | None = None         # float64[N, 3]
+    bottom_center: int = 0
+    handle_base: tuple = (0.0, 0.0, 0.0)     # grip handle origin in FP64
+    extra: dict = field(default_factory=dict)
+
+    @property
+    def n(self) -> int:
+        return len(self.particles)
+
+    def copy(self) -> "SceneArrays":
+        out = SceneArrays(**{k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in self.__dict__.items()})
+        out.extra = dict(self.extra)
+        return out
+
+    def struct(self) -> abi.SceneStruct:
+        s = abi.SceneStruct()
+        s.config = _ptr(self.config)
+        s.particles = _ptr(self.particles)
+        s.restPositions = _ptr(self.rest)
+        s.distances = _ptr(self.distances)
+        s.knots = _ptr(self.knots)
+        s.bends = _ptr(self.bends)
+        s.grips = _ptr(self.grips)
+        s.fruits = _ptr(self.fruits)
+        s.fruitPairs = _ptr(self.pairs)
+        s.cuffParticles = _ptr(self.cuff)
+        s.mouthRim = _ptr(self.rim)
+        s.localOffsets = _ptr(self.local_off)
+        s.localIndices = _ptr(self.local_idx)
+        s.gridWidth = self.grid_width
+        return s
+
+
+def _scene_from_handle(h) -> SceneArrays:
+    lib = load_library()
+    if not h:
+        raise ClothError("scene construction failed")
+    try:
+        view = abi.SceneStruct()
+        lib.numi_cloth_scene_view(h, ctypes.byref(view))
+        counts = (ctypes.c_uint32 * 15)()
+        lib.numi_cloth_scene_counts(h, counts)
+        n, d, k, b, g, f, p, rings, rim = counts[:9]
+
+        def grab(ptr, dtype, count):
+            if count == 0 or not ptr:
+                return np.zeros(0, dtype)
+            buf = (ctypes.c_char * (count * dtype.itemsize)).from_address(ptr)
+            return np.frombuffer(bytes(buf), dtype=dtype).copy()
+
+        rest64 = np.zeros(3 * n, np.float64)
+        lib.numi_cloth_scene_rest_fp64(h, rest64.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        local_off = grab(view.localOffsets, np.dtype("<u4"), n + 1) if view.localOffsets else None
+        local_idx = (
+            grab(view.localIndices, np.dtype("<u4"), int(local_off[-1])) if local_off is not None else None
+        )
+        cfg = grab(view.config, CONFIG, 1)
+        return SceneArrays(
+            config=cfg,
+            particles=grab(view.particles, PARTICLE, n),
+            rest=grab(view.restPositions, np.dtype("<f4"), 4 * n).reshape(n, 4),
+            distances=grab(view.distances, DISTANCE, d),
+            knots=grab(view.knots, KNOT, k),
+            bends=grab(view.bends, BEND, b),
+            grips=grab(view.grips, GRIP, g),
+            fruits=grab(view.fruits, FRUIT, f),
+            pairs=grab(view.fruitPairs, FRUIT_PAIR, p),
+            cuff=grab(view.cuffParticles, np.dtype("<u4"), 2 * rings),
+            rim=grab(view.mouthRim, np.dtype("<u4"), rim),
+            local_off=local_off,
+            local_idx=local_idx,
+            grid_width=view.gridWidth,
+            rest64=rest64.reshape(n, 3),
+            bottom_center=int(counts[14]),
+            extra={
+                "distance_colours": int(counts[9]),
+                "knot_colours": int(counts[10]),
+                "bend_colours": int(counts[11]),
+                "pair_colours": int(counts[12]),
+                "yarn_segments": int(counts[13]),
+            },
+        )
+    finally:
+        lib.numi_cloth_scene_destroy(h)
+
+
+SCENARIOS = {"grounded": 0, "spin": 1, "pickup": 2, "recorded": 3}
+
+
+def bag_scene(
+    material: Material | None = None,
+    scenario: str = "recorded",
+    timestep: float = 1.0 / 5760.0,
+    select_nearest: bool = False,
+) -> SceneArrays:
+    """The reference produce bag (1,465 particles, 12 fruits, 10 grips)."""
+    lib = load_library()
+    m = material if material is not None else material_defaults()
+    h = lib.numi_cloth_scene_bag(ctypes.byref(m), SCENARIOS[scenario], timestep, 1 if select_nearest else 0)
+    s = _scene_from_handle(h)
+    c = s.config[0]
+    s.handle_base = tuple(float(v) for v in _bag_handle_base(scenario))
+    s.extra["scenario"] = scenario
+    s.extra["material"] = m
+    del c
+    return s
+
+
+def _bag_handle_base(scenario: str):
+    # authoredPosition(kLevels - 1, 0) in FP64 (tools/cloth_bag.cpp:475-527)
+    import math
+
+    level, ring, levels, around = 27, 0, 28, 48
+    vertical = level / (levels - 1)
+
+    def smooth(v):
+        x = min(max(v, 0.0), 1.0)
+        return x * x * (3.0 - 2.0 * x)
+
+    body = smooth(vertical / 0.55)
+    fold = min(max((vertical - 0.72) / 0.28, 0.0), 1.0)
+    skirt = 1.0 - smooth(vertical / 0.18)
+    angle0 = 2.0 * math.pi * ring / around
+    base_radius = 0.266 + 0.030 * body - 0.116 * fold + 0.045 * skirt
+    angle = angle0 + 0.08 * vertical
+    wrinkle = 1.0 + 0.035 * math.sin(5.0 * angle + 5.0 * math.pi * vertical) + 0.018 * math.sin(
+        9.0 * angle - 3.0 * math.pi * vertical
+    )
+    loose_rim = fold * (0.007 * math.sin(3.0 * angle + 0.35) + 0.004 * math.sin(7.0 * angle - 0.80))
+    loose_skirt = skirt * (0.020 * math.sin(3.0 * angle - 0.40) + 0.012 * math.sin(7.0 * angle + 0.70))
+    rim_sag = fold * (
+        0.016 * math.sin(angle + 0.55) + 0.008 * math.sin(3.0 * angle - 0.30) + 0.004 * math.sin(6.0 * angle + 0.90)
+    )
+    radius = base_radius * wrinkle + loose_rim + loose_skirt
+    skirt_sag = skirt * (0.012 * math.sin(4.0 * angle + 0.20) + 0.006 * math.sin(9.0 * angle - 0.50))
+    folded = 0.167 + 0.038 * (fold / 0.35) if fold < 0.35 else 0.205 - 0.025 * ((fold - 0.35) / 0.65)
+    lift = 0.52 if scenario == "spin" else 0.0
+    return (radius * math.cos(angle), radius * math.sin(angle), folded + rim_sag + skirt_sag + 0.009 + lift)
+
+
+def square_scene(spec: SquareSpec | None = None, material: Material | None = None, **overrides) -> SceneArrays:
+    """Square s x s weave with shear diagonals and skip-one bends."""
+    lib = load_library()
+    if spec is None:
+        spec = SquareSpec()
+        lib.numi_cloth_square_defaults(ctypes.byref(spec))
+    for k, v in overrides.items():
+        setattr(spec, k, v)
+    m = material if material is not None else material_defaults()
+    h = lib.numi_cloth_scene_square(ctypes.byref(spec), ctypes.byref(m))
+    s = _scene_from_handle(h)
+    p0 = s.rest64[0]
+    s.handle_base = (float(p0[0]), float(p0[1]), float(p0[2]))
+    s.extra["spec"] = {name: getattr(spec, name) for name, _ in SquareSpec._fields_}
+    return s
+
+
+class GripTrajectory:
+    """numi.grip.trajectory.v1..v3; the loader rejects what the reference rejects."""
+
+    def __init__(self, path: str):
+        lib = load_library()
+        err = ctypes.create_string_buffer(512)
+        self._h = lib.numi_cloth_trajectory_load(path.encode(), err, 512)
+        if not self._h:
+            raise ClothError(err.value.decode())
+        sel = ctypes.c_uint32()
+        dur = ctypes.c_double()
+        fp = ctypes.c_uint64()
+        lib.numi_cloth_trajectory_info(self._h, ctypes.byref(sel), ctypes.byref(dur), ctypes.byref(fp))
+        self.select_nearest = bool(sel.value)
+        self.duration = dur.value
+        self.fingerprint = fp.value
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _LIB is not None:
+            _LIB.numi_cloth_trajectory_destroy(self._h)
+            self._h = None
+
+    def sample(self, t: float) -> abi.GripPose:
+        p = abi.GripPose()
+        if load_library().numi_cloth_trajectory_sample(self._h, t, ctypes.byref(p)) != 0:
+            raise ClothError(f"grip trajectory sample outside its duration: {t}")
+        return p
+
+    def configs(self, base: np.ndarray, handle_base, first_substep: int, count: int, dt: float) -> np.ndarray:
+        out = np.zeros(count, CONFIG)
+        hb = (ctypes.c_double * 3)(*handle_base)
+        rc = load_library().numi_cloth_trajectory_configs(
+            self._h, _ptr(base), hb, first_substep, count, dt, _ptr(out)
+        )
+        if rc != 0:
+            raise ClothError("grip trajectory does not cover the requested substeps")
+        return out
+
+
+class ClothSolver:
+    """One solver handle on the current CUDA device (numi_cloth_create)."""
+
+    def __init__(self, scene: SceneArrays):
+        self.lib = load_library()
+        self.scene = scene
+        self._keep = scene.struct()
+        h = ctypes.c_void_p()
+        rc = self.lib.numi_cloth_create(ctypes.byref(self._keep), ctypes.byref(h))
+        if rc != 0:
+            raise ClothError(f"numi_cloth_create failed: {rc}")
+        self._h = h
+        self.n = scene.n
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.numi_cloth_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def set_stream(self, stream_ptr: int | None):
+        self.lib.numi_cloth_set_stream(self._h, ctypes.c_void_p(stream_ptr) if stream_ptr else None)
+
+    def step(self, configs: np.ndarray, schedule: Schedule):
+        configs = np.ascontiguousarray(configs, CONFIG)
+        rc = self.lib.numi_cloth_step(self._h, _ptr(configs), len(configs), ctypes.byref(schedule))
+        if rc != 0:
+            raise ClothError(f"numi_cloth_step failed: {rc}")
+
+    def failure(self) -> int:
+        return int(self.lib.numi_cloth_failure(self._h))
+
+    def particles(self) -> np.ndarray:
+        out = np.zeros(self.n, PARTICLE)
+        self._check(self.lib.numi_cloth_read_particles(self._h, _ptr(out), self.n))
+        return out
+
+    def write_particles(self, p: np.ndarray):
+        p = np.ascontiguousarray(p, PARTICLE)
+        self._check(self.lib.numi_cloth_write_particles(self._h, _ptr(p), len(p)))
+
+    def fruits(self) -> np.ndarray:
+        out = np.zeros(len(self.scene.fruits), FRUIT)
+        self._check(self.lib.numi_cloth_read_fruits(self._h, _ptr(out), len(out)))
+        return out
+
+    def write_fruits(self, f: np.ndarray):
+        f = np.ascontiguousarray(f, FRUIT)
+        self._check(self.lib.numi_cloth_write_fruits(self._h, _ptr(f), len(f)))
+
+    def distances(self) -> np.ndarray:
+        out = np.zeros(len(self.scene.distances), DISTANCE)
+        self._check(self.lib.numi_cloth_read_distances(self._h, _ptr(out), len(out)))
+        return out
+
+    def grips(self) -> np.ndarray:
+        out = np.zeros(len(self.scene.grips), GRIP)
+        self._check(self.lib.numi_cloth_read_grips(self._h, _ptr(out), len(out)))
+        return out
+
+    def residuals(self) -> np.ndarray:
+        out = (ctypes.c_double * 4)()
+        self._check(self.lib.numi_cloth_residuals(self._h, out))
+        return np.array(out[:])
+
+    def snapshot(self, slot: int = 0):
+        self._check(self.lib.numi_cloth_snapshot(self._h, slot))
+
+    def restore(self, slot: int = 0):
+        self._check(self.lib.numi_cloth_restore(self._h, slot))
+
+    def launch_info(self) -> dict:
+        out = (ctypes.c_uint32 * 4)()
+        self._check(self.lib.numi_cloth_launch_info(self._h, out))
+        return {"grid": out[0], "block": out[1], "barriers_per_substep": out[2], "launches": out[3]}
+
+    @staticmethod
+    def _check(rc: int):
+        if rc != 0:
+            raise ClothError(f"numi_cloth call failed: {rc}")
+
+
+def substep_configs(scene: SceneArrays, count: int, dt: float | None = None) -> np.ndarray:
+    """count copies of the scene's base Config (static grip target)."""
+    cfg = np.repeat(scene.config, count)
+    if dt is not None:
+        cfg["gravityAndTimestep"][:, 3] = dt
+    return cfg

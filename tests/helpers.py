@@ -1,0 +1,81 @@
+"""Shared scene/schedule builders and runners for the parity tests."""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+
+import numi_cloth as nc
+import oracle_py as op
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+# Schedules exercised by the parity tests.  "reference" is the reference
+# CPU substep (tools/cloth_bag.cpp:4891-5185) with a reduced certificate cap.
+FULL = dict(iterations=2, strainSweeps=3, reconcilePasses=3, finalPasses=2, certificatePasses=4, earlyExit=1,
+            aerodynamics=1, sweptGround=1, frictions=1)
+PLAIN = dict(iterations=1, strainSweeps=1, reconcilePasses=0, finalPasses=0, certificatePasses=0, earlyExit=0,
+             aerodynamics=0, sweptGround=1, frictions=1)
+
+
+def small_square(side=24, fruits=6, **kw) -> nc.SceneArrays:
+    """A small square cloth with spheres resting just above it."""
+    args = dict(side=side, fruitCount=fruits, fruitHeightMin=0.5012, fruitHeightMax=0.5030, fruitRadiusMin=0.01,
+                fruitRadiusMax=0.02, timestep=1.0 / 2880.0)
+    args.update(kw)
+    return nc.square_scene(**args)
+
+
+def lift_trajectory_path() -> str:
+    return os.path.join(GOLDEN, "lift-v1.csv")
+
+
+def bag_frame_configs(scene: nc.SceneArrays, first: int, count: int, dt: float) -> np.ndarray:
+    traj = nc.GripTrajectory(lift_trajectory_path())
+    return traj.configs(scene.config, scene.handle_base, first, count, dt)
+
+
+def run_gpu(scene, configs, sched: nc.Schedule, frames=1, grid=None):
+    env_old = os.environ.get("NUMI_CLOTH_GRID")
+    if grid is not None:
+        os.environ["NUMI_CLOTH_GRID"] = str(grid)
+    try:
+        s = nc.ClothSolver(scene)
+    finally:
+        if grid is not None:
+            if env_old is None:
+                os.environ.pop("NUMI_CLOTH_GRID", None)
+            else:
+                os.environ["NUMI_CLOTH_GRID"] = env_old
+    per = len(configs) // frames
+    for f in range(frames):
+        s.step(configs[f * per:(f + 1) * per], sched)
+    fail = s.failure()
+    out = {"particles": s.particles(), "fruits": s.fruits(), "distances": s.distances(), "grips": s.grips(),
+           "failure": fail, "residuals": s.residuals(), "info": s.launch_info()}
+    s.close()
+    return out
+
+
+def run_oracle(scene, configs, sched: nc.Schedule, bits=32, mode=op.BATCHED, frames=1):
+    o = op.Oracle(op.from_abi(scene), bits)
+    subs = op.substeps_from_configs(configs)
+    osched = op.schedule_from_abi(sched, mode)
+    per = len(configs) // frames
+    fail = 0
+    for f in range(frames):
+        fail |= o.step(subs[f * per:(f + 1) * per], osched)
+    st = o.read()
+    st["failure"] = fail
+    st["residuals"] = o.residuals()
+    st["stats"] = o.stats()
+    return st
+
+
+def gpu_positions(out) -> np.ndarray:
+    return out["particles"]["positionAndInverseMass"][:, :3]
+
+
+def gpu_fruit_positions(out) -> np.ndarray:
+    return out["fruits"]["positionAndInverseMass"][:, :3]

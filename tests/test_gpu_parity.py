@@ -1,0 +1,104 @@
+"""GPU parity: the sm_100a frame kernel against the CPU oracle.
+
+Bar (north star): on the same inputs and the same batched colour schedule the
+FP32 GPU path equals the FP32 restatement bit for bit, and stays within
+1e-5 m of the FP64 restatement over one frame (48 substeps); two GPU runs
+are bit-identical; one CTA and many CTAs give the same bits.
+"""
+import numpy as np
+import pytest
+
+import numi_cloth as nc
+import oracle_py as op
+from helpers import FULL, PLAIN, bag_frame_configs, gpu_fruit_positions, gpu_positions, run_gpu, run_oracle, small_square
+
+pytestmark = pytest.mark.gpu
+
+POS_TOL_FP64 = 1.0e-5   # m, per north star: FP32 path vs FP64 over the first frame
+
+
+def _check_bitexact(g, o):
+    gp = gpu_positions(g)
+    opos = o["particles"]["x"]
+    assert np.array_equal(gp.astype(np.float64), opos), f"max |dx| = {np.abs(gp - opos).max()}"
+    gv = g["particles"]["velocity"][:, :3].astype(np.float64)
+    assert np.array_equal(gv, o["particles"]["v"]), f"max |dv| = {np.abs(gv - o['particles']['v']).max()}"
+    if len(g["fruits"]):
+        gf = gpu_fruit_positions(g).astype(np.float64)
+        assert np.array_equal(gf, o["fruits"]["x"]), f"fruit max |dx| = {np.abs(gf - o['fruits']['x']).max()}"
+        assert np.array_equal(g["fruits"]["velocityAndGroundImpulse"][:, :3].astype(np.float64), o["fruits"]["v"])
+        assert np.array_equal(g["fruits"]["angularVelocity"][:, :3].astype(np.float64), o["fruits"]["omega"])
+    lam = g["distances"]["material"][:, 2].astype(np.float64)
+    assert np.array_equal(lam, o["distances"]["lambda_"])
+
+
+@pytest.mark.parametrize("sched", [PLAIN, FULL], ids=["plain", "full"])
+def test_square_frame_bitexact_fp32(sched):
+    scene = small_square()
+    cfg = nc.substep_configs(scene, 48)
+    s = nc.Schedule.make(**sched)
+    g = run_gpu(scene, cfg, s)
+    o = run_oracle(scene, cfg, s, bits=32)
+    assert g["failure"] == 0, nc.failure_names(g["failure"])
+    _check_bitexact(g, o)
+
+
+def test_square_frame_fp64_tolerance():
+    scene = small_square()
+    cfg = nc.substep_configs(scene, 48)
+    s = nc.Schedule.make(**FULL)
+    g = run_gpu(scene, cfg, s)
+    o = run_oracle(scene, cfg, s, bits=64)
+    err = np.abs(gpu_positions(g).astype(np.float64) - o["particles"]["x"]).max()
+    ferr = np.abs(gpu_fruit_positions(g).astype(np.float64) - o["fruits"]["x"]).max()
+    print(f"square 24x24, 1 frame: max particle error vs FP64 = {err:.3e} m, fruit = {ferr:.3e} m")
+    assert err <= POS_TOL_FP64
+    assert ferr <= POS_TOL_FP64
+
+
+def test_bag_frame_bitexact_and_fp64():
+    dt = 1.0 / 5760.0
+    scene = nc.bag_scene(scenario="recorded", timestep=dt)
+    cfg = bag_frame_configs(scene, 0, 48, dt)
+    s = nc.Schedule.make(**FULL)
+    g = run_gpu(scene, cfg, s)
+    assert g["info"]["grid"] == 1   # resident single-CTA path
+    o32 = run_oracle(scene, cfg, s, bits=32)
+    _check_bitexact(g, o32)
+    o64 = run_oracle(scene, cfg, s, bits=64)
+    err = np.abs(gpu_positions(g).astype(np.float64) - o64["particles"]["x"]).max()
+    print(f"bag, 1 frame at 1/5760 s: max particle error vs FP64 = {err:.3e} m")
+    assert err <= POS_TOL_FP64
+
+
+def test_multi_cta_equals_single_cta():
+    scene = small_square(side=32, fruits=8)
+    cfg = nc.substep_configs(scene, 12)
+    s = nc.Schedule.make(**FULL)
+    one = run_gpu(scene, cfg, s, grid=1)
+    many = run_gpu(scene, cfg, s, grid=7)
+    assert many["info"]["grid"] == 7
+    assert np.array_equal(one["particles"], many["particles"])
+    assert np.array_equal(one["fruits"], many["fruits"])
+
+
+def test_two_runs_bit_identical():
+    scene = small_square(side=40, fruits=10)
+    cfg = nc.substep_configs(scene, 24)
+    s = nc.Schedule.make(**FULL)
+    a = run_gpu(scene, cfg, s, grid=16)
+    b = run_gpu(scene, cfg, s, grid=16)
+    assert np.array_equal(a["particles"], b["particles"])
+    assert np.array_equal(a["fruits"], b["fruits"])
+
+
+def test_large_square_multi_cta_bitexact():
+    """65,536 particles, full cooperative grid, three substeps."""
+    scene = nc.square_scene()
+    cfg = nc.substep_configs(scene, 3)
+    s = nc.Schedule.make(**PLAIN)
+    g = run_gpu(scene, cfg, s)
+    assert g["info"]["grid"] > 1
+    o = run_oracle(scene, cfg, s, bits=32)
+    assert g["failure"] == 0
+    _check_bitexact(g, o)
