@@ -232,6 +232,16 @@ int numi_cloth_restore(numi_cloth_t* handle, uint32_t slot);
  * per substep, kernel launches. */
 int numi_cloth_launch_info(numi_cloth_t* handle, uint32_t out[4]);
 
+/* Per-phase device timestamps of the last step (profiling aid).  Enabled
+ * when the handle was created with NUMI_CLOTH_TRACE=<substeps> in the
+ * environment; out receives substeps x slots (slots must be 128) globaltimer
+ * values in ns, one per grid barrier in program order, 0 where unused.
+ * Returns NUMI_CLOTH_ESTATE when tracing is off.  No reference counterpart:
+ * the reference records only command-buffer GPU start/end times
+ * (tools/cloth_bag_metal.mm:4758-4760). */
+int numi_cloth_trace(numi_cloth_t* handle, unsigned long long* out,
+                     uint32_t substeps, uint32_t slots);
+
 /* Library version string. */
 const char* numi_cloth_version(void);
 

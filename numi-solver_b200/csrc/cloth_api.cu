@@ -88,6 +88,8 @@ struct numi_cloth {
     uint32_t grid = 1;
     uint32_t block = NC_THREADS;
     uint32_t launches = 0;
+    uint32_t trace_capacity = 0;   // substeps the trace buffer holds
+    uint32_t last_substeps = 0;
     Snapshot snaps[kSnapshotSlots];
     // dynamic state regions copied by snapshot/restore
     struct Region {
@@ -177,7 +179,10 @@ cudaError_t launch(numi_cloth* h, uint32_t substeps, const Schedule& s) {
     Schedule sc = s;
     sc.substeps = substeps;
     void* args[] = {&d, &sc};
-    cudaError_t e;
+    if (d.trace != nullptr && substeps > h->trace_capacity) d.trace = nullptr;
+    cudaError_t e = cudaMemsetAsync(h->d.bar_count, 0, 2 * sizeof(unsigned long long), h->stream);
+    if (e != cudaSuccess) return e;
+    h->last_substeps = substeps;
     if (h->grid == 1) {
         e = cudaLaunchKernel(reinterpret_cast<const void*>(numi_cloth_frame_kernel), dim3(1), dim3(h->block), args, 0,
                              h->stream);
@@ -314,9 +319,10 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
     d.force = h->buf.alloc<float4>(n);
     d.fruit_partial = h->buf.alloc<float4>(NC_MAX_FRUITS * 9u / 2u + 1u);
     d.failure = h->buf.alloc<unsigned int>(1);
-    d.bar_count = h->buf.alloc<unsigned int>(1);
-    d.bar_gen = h->buf.alloc<unsigned int>(1);
-    d.abort_flag = h->buf.alloc<unsigned int>(1);
+    // barrier counter (u64) and abort flag share one 16-byte block so one
+    // memset resets both before a launch
+    d.bar_count = h->buf.alloc<unsigned long long>(2);
+    d.abort_flag = reinterpret_cast<unsigned int*>(d.bar_count + 1);
     d.stats = h->buf.alloc<uint32_t>(4);
 
     // Launch geometry: one resident CTA for a small cloth, else a full
@@ -330,12 +336,17 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
     uint32_t forced = 0;
     if (env_u32("NUMI_CLOTH_GRID", forced) && forced > 0) grid = std::min<uint32_t>(forced, sms * std::max(per_sm, 1));
     h->grid = std::max(grid, 1u);
+    uint32_t trace_substeps = 0;
+    if (env_u32("NUMI_CLOTH_TRACE", trace_substeps) && trace_substeps > 0) {
+        d.trace = h->buf.alloc<unsigned long long>(static_cast<size_t>(trace_substeps) * NC_TRACE_SLOTS);
+        h->trace_capacity = d.trace ? trace_substeps : 0u;
+    }
     const uint32_t chunks = (n + NC_THREADS - 1u) / NC_THREADS;
     d.red = h->buf.alloc<double>(std::max<size_t>(3u * 4096u, 2u * chunks + 8u));
 
     bool ok = d.x && d.xp && d.v && rest && d_ij && d_mat && d.d_lambda && k_ij && k_mat && d.k_lambda && b_ij &&
               b_mat && d.b_lambda && d.grips && d.fruits && d.pairs && cuff && d.yarn_slot_a && d.yarn_slot_b &&
-              d.force && d.fruit_partial && d.failure && d.bar_count && d.bar_gen && d.abort_flag && d.stats && d.red;
+              d.force && d.fruit_partial && d.failure && d.bar_count && d.abort_flag && d.stats && d.red;
     if (!ok) {
         delete h;
         return NUMI_CLOTH_ENOMEM;
@@ -620,6 +631,17 @@ int numi_cloth_restore(numi_cloth_t* h, uint32_t slot) {
             return NUMI_CLOTH_ECUDA;
         off += (r.bytes + 255u) & ~size_t(255u);
     }
+    return NUMI_CLOTH_OK;
+}
+
+int numi_cloth_trace(numi_cloth_t* h, unsigned long long* out, uint32_t substeps, uint32_t slots) {
+    if (h == nullptr || out == nullptr || slots != NC_TRACE_SLOTS) return NUMI_CLOTH_EINVAL;
+    if (h->d.trace == nullptr || substeps > h->trace_capacity) return NUMI_CLOTH_ESTATE;
+    cudaSetDevice(h->device);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess ||
+        cudaMemcpy(out, h->d.trace, static_cast<size_t>(substeps) * NC_TRACE_SLOTS * sizeof(unsigned long long),
+                   cudaMemcpyDeviceToHost) != cudaSuccess)
+        return NUMI_CLOTH_ECUDA;
     return NUMI_CLOTH_OK;
 }
 

@@ -24,6 +24,8 @@
 #define NC_MAX_GRIPS 32u
 #define NC_MAX_BATCHES 64u
 #define NC_YARN_SLOTS 4u
+#define NC_MAX_PAIRS 2016u
+#define NC_TRACE_SLOTS 128u
 
 struct Batch {
     uint32_t first;
@@ -84,9 +86,12 @@ struct DeviceCloth {
     const NumiClothConfig* cfg;
     // control
     unsigned int* failure;
-    unsigned int* bar_count;
-    unsigned int* bar_gen;
+    // grid barrier: monotonically increasing arrival counter (reset to 0 by
+    // the host before every launch) and a sticky abort flag
+    unsigned long long* bar_count;
     unsigned int* abort_flag;
+    // optional per-barrier globaltimer trace: [substep][NC_TRACE_SLOTS]
+    unsigned long long* trace;
     double* red;          // [blocks * 8] reduction partials
     uint32_t* stats;      // [0] barriers of the last substep, [1] reconcile passes max, [2] certificate passes max
     uint32_t epoch_base;  // substep counter of the handle at launch

@@ -18,10 +18,57 @@ struct Ctx {
     uint32_t barriers;
     bool fruit_pending;   // fixed-point fruit sums waiting to be applied
     uint32_t epoch;
+    uint32_t sub;
+    unsigned long long seq;   // barriers passed in this launch
 };
 
+// Grid-wide barrier with a bounded wait.  Arrival adds 1 to a counter the
+// host zeroes before each launch; barrier number s of the launch completes
+// when the counter reaches s * gridDim.x.  A CTA that waits past the limit
+// raises TIMEOUT and the abort flag, and every CTA leaves at its next
+// barrier (or as soon as it sees the flag while waiting).
+__device__ bool grid_sync(Ctx& ctx) {
+    const DeviceCloth& d = ctx.d;
+    ++ctx.barriers;
+    ++ctx.seq;
+    if (gridDim.x == 1) {
+        __syncthreads();
+        if (d.trace && threadIdx.x == 0 && ctx.barriers <= NC_TRACE_SLOTS)
+            d.trace[static_cast<size_t>(ctx.sub) * NC_TRACE_SLOTS + ctx.barriers - 1u] = globaltimer();
+        return true;
+    }
+    __shared__ unsigned s_abort;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned long long target = ctx.seq * gridDim.x;
+        __threadfence();
+        atomicAdd(d.bar_count, 1ull);
+        unsigned ab = 0u;
+        unsigned spins = 0u;
+        while (ld_acquire_u64(d.bar_count) < target) {
+            ++spins;
+            if ((spins & 63u) == 0u && ld_acquire(d.abort_flag) != 0u) {
+                ab = 1u;
+                break;
+            }
+            if (spins > NC_BARRIER_SPIN_LIMIT) {
+                atomicOr(d.failure, NUMI_CLOTH_FAILURE_TIMEOUT);
+                atomicExch(d.abort_flag, 1u);
+                ab = 1u;
+                break;
+            }
+        }
+        __threadfence();
+        s_abort = ab;
+        if (d.trace && blockIdx.x == 0 && ctx.barriers <= NC_TRACE_SLOTS)
+            d.trace[static_cast<size_t>(ctx.sub) * NC_TRACE_SLOTS + ctx.barriers - 1u] = globaltimer();
+    }
+    __syncthreads();
+    return s_abort == 0u;
+}
+
 #define NC_SYNC(ctx) \
-    do { if (!grid_sync((ctx).d, (ctx).barriers)) return false; } while (0)
+    do { if (!grid_sync(ctx)) return false; } while (0)
 
 // Apply (and clear) the fixed-point fruit displacement sums.  Fruit CTA.
 __device__ void fruit_flush(Ctx& ctx) {
@@ -616,20 +663,48 @@ __device__ void yarn_friction_batch(Ctx& ctx, const Batch& bt) {
     }
 }
 
-// Fruit frictions and orientation in the fruit CTA.
+// Fruit frictions and orientation in the fruit CTA: pair friction on
+// fruit velocities staged in shared memory (one warp walks the colours),
+// then ground friction, rolling resistance and orientation per fruit.
 __device__ void fruit_tail(Ctx& ctx) {
     if (!ctx.fruit_cta) return;
     const DeviceCloth& d = ctx.d;
     const SubCfg& c = ctx.c;
+    __shared__ float4 s_v[NC_MAX_FRUITS];
+    __shared__ float4 s_o[NC_MAX_FRUITS];
+    __shared__ float s_ni[NC_MAX_PAIRS];
+    __shared__ unsigned short s_ab[NC_MAX_PAIRS];
+    for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
+        const NumiClothFruit& fr = d.fruits[f];
+        s_v[f] = make_float4(fr.velocityAndGroundImpulse.x, fr.velocityAndGroundImpulse.y,
+                             fr.velocityAndGroundImpulse.z, fr.positionAndInverseMass.w);
+        s_o[f] = make_float4(fr.angularVelocity.x, fr.angularVelocity.y, fr.angularVelocity.z,
+                             fr.previousAndRadius.w);
+    }
     if (ctx.s.frictions) {
-        for (uint32_t b = 0; b < d.n_pair_batches; ++b) {
-            const Batch bt = d.pair_batches[b];
-            for (uint32_t k = threadIdx.x; k < bt.count; k += blockDim.x) fruit_pair_friction(d, bt.first + k, c.mu_pair);
-            __syncthreads();
+        for (uint32_t k = threadIdx.x; k < d.p_count; k += blockDim.x) {
+            s_ni[k] = d.pairs[k].contact.w;
+            s_ab[k] = static_cast<unsigned short>(d.pairs[k].fruitsAndColor.x | (d.pairs[k].fruitsAndColor.y << 8));
         }
     }
+    __syncthreads();
+    if (ctx.s.frictions && threadIdx.x < 32u) {
+        for (uint32_t b = 0; b < d.n_pair_batches; ++b) {
+            const Batch bt = d.pair_batches[b];
+            for (uint32_t k = bt.first + threadIdx.x; k < bt.first + bt.count; k += 32u) {
+                const float ni = s_ni[k];
+                if (ni <= 0.0f) continue;
+                const numi_float4 cw = d.pairs[k].contact;
+                pair_friction_smem(s_v, s_o, s_ab[k] & 0xffu, s_ab[k] >> 8, V3{cw.x, cw.y, cw.z}, ni, c.mu_pair);
+            }
+            __syncwarp();
+        }
+    }
+    __syncthreads();
     for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
         FruitState s = load_fruit(d.fruits[f]);
+        s.v = xyz(s_v[f]);
+        s.omega = xyz(s_o[f]);
         if (ctx.s.frictions) fruit_ground_friction(s, c);
         integrate_orientation(s, c.dt);
         store_fruit(d.fruits[f], s);
@@ -749,7 +824,9 @@ __global__ void __launch_bounds__(NC_THREADS) numi_cloth_frame_kernel(DeviceClot
     ctx.fruit_cta = blockIdx.x == gridDim.x - 1u;
     ctx.grip_cta = blockIdx.x == 0u;
     ctx.fruit_pending = false;
+    ctx.seq = 0;
     for (uint32_t sub = 0; sub < s.substeps; ++sub) {
+        ctx.sub = sub;
         ctx.c = nc::load_cfg(d.cfg + sub);
         ctx.epoch = d.epoch_base + sub;
         ctx.barriers = 0;

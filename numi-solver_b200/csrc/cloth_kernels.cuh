@@ -51,40 +51,15 @@ __device__ __forceinline__ float from_fixed(unsigned long long v) {
     return static_cast<float>(static_cast<double>(static_cast<long long>(v)) * (1.0 / NC_FIXED_SCALE));
 }
 
-// Grid-wide barrier with a bounded wait.  Returns false when any CTA gave up
-// (timeout), after which every CTA leaves the kernel at its next barrier.
-__device__ bool grid_sync(const DeviceCloth& d, uint32_t& barriers) {
-    ++barriers;
-    if (gridDim.x == 1) {
-        __syncthreads();
-        return true;
-    }
-    __shared__ unsigned s_abort;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const unsigned gen = ld_acquire(d.bar_gen);
-        __threadfence();
-        const unsigned arrived = atomicAdd(d.bar_count, 1u);
-        if (arrived == gridDim.x - 1u) {
-            atomicExch(d.bar_count, 0u);
-            __threadfence();
-            st_release(d.bar_gen, gen + 1u);
-        } else {
-            unsigned spins = 0;
-            while (ld_acquire(d.bar_gen) == gen) {
-                if (++spins > NC_BARRIER_SPIN_LIMIT) {
-                    atomicOr(d.failure, NUMI_CLOTH_FAILURE_TIMEOUT);
-                    atomicExch(d.abort_flag, 1u);
-                    break;
-                }
-                __nanosleep(64);
-            }
-        }
-        __threadfence();
-        s_abort = ld_acquire(d.abort_flag);
-    }
-    __syncthreads();
-    return s_abort == 0u;
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned long long globaltimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
 }
 
 struct SubCfg {
@@ -419,42 +394,56 @@ __device__ void fruit_air(FruitState& f, const SubCfg& c) {
 }
 
 // Sphere/sphere separation (tools/cloth_bag.cpp:1897-1919).
-__device__ __forceinline__ void solve_fruit_pair(const DeviceCloth& d, uint32_t k, float dt) {
-    NumiClothFruitPair pr = d.pairs[k];
-    NumiClothFruit& fa = d.fruits[pr.fruitsAndColor.x];
-    NumiClothFruit& fb = d.fruits[pr.fruitsAndColor.y];
-    const V3 a{fa.positionAndInverseMass.x, fa.positionAndInverseMass.y, fa.positionAndInverseMass.z};
-    const V3 b{fb.positionAndInverseMass.x, fb.positionAndInverseMass.y, fb.positionAndInverseMass.z};
-    const float wa = fa.positionAndInverseMass.w;
-    const float wb = fb.positionAndInverseMass.w;
-    const V3 diff = b - a;
-    const float L = len3(diff);
-    const float target = fa.previousAndRadius.w + fb.previousAndRadius.w;
-    if (L >= target || L < 1.0e-12f) return;
-    const float den = wa + wb;
-    const float lambda = (target - L) / den;
-    const V3 normal = vdiv(diff, L);
-    const V3 corr = normal * lambda;
-    const V3 na = a - corr * wa;
-    const V3 nb = b + corr * wb;
-    fa.positionAndInverseMass.x = na.x;
-    fa.positionAndInverseMass.y = na.y;
-    fa.positionAndInverseMass.z = na.z;
-    fb.positionAndInverseMass.x = nb.x;
-    fb.positionAndInverseMass.y = nb.y;
-    fb.positionAndInverseMass.z = nb.z;
-    const float imp = lambda / dt;
-    const V3 wn = V3{pr.contact.x, pr.contact.y, pr.contact.z} + normal * imp;
-    d.pairs[k].contact = nf4<numi_float4>(wn.x, wn.y, wn.z, pr.contact.w + imp);
-}
-
-// All fruit-pair colours, in the fruit CTA.
+// All fruit-pair colours, in the fruit CTA: fruit positions and pair
+// indices staged in shared memory, one warp walks the colours (a colour's
+// pairs are disjoint, so its lanes never touch the same fruit).
 __device__ void fruit_pair_sweep(const DeviceCloth& d, float dt) {
-    for (uint32_t b = 0; b < d.n_pair_batches; ++b) {
-        const Batch bt = d.pair_batches[b];
-        for (uint32_t k = threadIdx.x; k < bt.count; k += blockDim.x) solve_fruit_pair(d, bt.first + k, dt);
-        __syncthreads();
+    __shared__ float4 s_fx[NC_MAX_FRUITS];
+    __shared__ float s_fr[NC_MAX_FRUITS];
+    __shared__ unsigned short s_ab[NC_MAX_PAIRS];
+    for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
+        const NumiClothFruit& fr = d.fruits[f];
+        s_fx[f] = make_float4(fr.positionAndInverseMass.x, fr.positionAndInverseMass.y,
+                              fr.positionAndInverseMass.z, fr.positionAndInverseMass.w);
+        s_fr[f] = fr.previousAndRadius.w;
     }
+    for (uint32_t k = threadIdx.x; k < d.p_count; k += blockDim.x)
+        s_ab[k] = static_cast<unsigned short>(d.pairs[k].fruitsAndColor.x | (d.pairs[k].fruitsAndColor.y << 8));
+    __syncthreads();
+    if (threadIdx.x < 32u) {
+        for (uint32_t b = 0; b < d.n_pair_batches; ++b) {
+            const Batch bt = d.pair_batches[b];
+            for (uint32_t k = bt.first + threadIdx.x; k < bt.first + bt.count; k += 32u) {
+                const uint32_t ia = s_ab[k] & 0xffu;
+                const uint32_t ib = s_ab[k] >> 8;
+                const float4 A = s_fx[ia];
+                const float4 B = s_fx[ib];
+                const V3 diff = xyz(B) - xyz(A);
+                const float L = len3(diff);
+                const float target = s_fr[ia] + s_fr[ib];
+                if (L >= target || L < 1.0e-12f) continue;
+                const float den = A.w + B.w;
+                const float lambda = (target - L) / den;
+                const V3 normal = vdiv(diff, L);
+                const V3 corr = normal * lambda;
+                s_fx[ia] = with_xyz(A, xyz(A) - corr * A.w);
+                s_fx[ib] = with_xyz(B, xyz(B) + corr * B.w);
+                const float imp = lambda / dt;
+                const numi_float4 c = d.pairs[k].contact;
+                const V3 wn = V3{c.x, c.y, c.z} + normal * imp;
+                d.pairs[k].contact = nf4<numi_float4>(wn.x, wn.y, wn.z, c.w + imp);
+            }
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
+        NumiClothFruit& fr = d.fruits[f];
+        fr.positionAndInverseMass.x = s_fx[f].x;
+        fr.positionAndInverseMass.y = s_fx[f].y;
+        fr.positionAndInverseMass.z = s_fx[f].z;
+    }
+    __syncthreads();
 }
 
 __device__ __forceinline__ void apply_fruit_impulse(FruitState& f, V3 impulse, V3 offset) {
@@ -462,35 +451,35 @@ __device__ __forceinline__ void apply_fruit_impulse(FruitState& f, V3 impulse, V
     f.omega = f.omega + cross3(offset, impulse) * inverse_inertia(f.w, f.radius);
 }
 
-// Coulomb pair friction (tools/cloth_bag.cpp:1921-1983).
-__device__ void fruit_pair_friction(const DeviceCloth& d, uint32_t k, float mu) {
-    const NumiClothFruitPair pr = d.pairs[k];
-    const float ni = pr.contact.w;
-    const V3 wn{pr.contact.x, pr.contact.y, pr.contact.z};
+// Coulomb pair friction (tools/cloth_bag.cpp:1921-1983) on fruit states
+// staged in shared memory (v.xyz + inverse mass, omega.xyz + radius).
+__device__ __forceinline__ void pair_friction_smem(float4* sv, float4* so, uint32_t ia, uint32_t ib, V3 wn,
+                                                   float ni, float mu) {
     if (ni <= 0.0f || lsq(wn) < 1.0e-20f) return;
-    FruitState a = load_fruit(d.fruits[pr.fruitsAndColor.x]);
-    FruitState b = load_fruit(d.fruits[pr.fruitsAndColor.y]);
+    const float4 va = sv[ia], vb = sv[ib], oa4 = so[ia], ob4 = so[ib];
     const V3 normal = normalized3(wn);
-    const V3 oa = normal * a.radius;
-    const V3 ob = normal * -b.radius;
-    const V3 ca = a.v + cross3(a.omega, oa);
-    const V3 cb = b.v + cross3(b.omega, ob);
+    const V3 oa = normal * oa4.w;
+    const V3 ob = normal * -ob4.w;
+    const V3 ca = xyz(va) + cross3(xyz(oa4), oa);
+    const V3 cb = xyz(vb) + cross3(xyz(ob4), ob);
     const V3 rel = cb - ca;
     const V3 tv = rel - normal * dot3(rel, normal);
     const float slip = len3(tv);
     if (slip < 1.0e-10f) return;
     const V3 t = vdiv(tv, slip);
-    const float den = ((a.w + b.w) + inverse_inertia(a.w, a.radius) * lsq(cross3(oa, t))) +
-                      inverse_inertia(b.w, b.radius) * lsq(cross3(ob, t));
+    const float ia_inv = inverse_inertia(va.w, oa4.w);
+    const float ib_inv = inverse_inertia(vb.w, ob4.w);
+    const float den = ((va.w + vb.w) + ia_inv * lsq(cross3(oa, t))) + ib_inv * lsq(cross3(ob, t));
     if (den <= 0.0f) return;
     const float limit = mu * ni;
     const float ti = fminf(slip / den, limit);
     if (ti <= 0.0f) return;
     const V3 imp_b = t * -ti;
-    apply_fruit_impulse(b, imp_b, ob);
-    apply_fruit_impulse(a, imp_b * -1.0f, oa);
-    store_fruit(d.fruits[pr.fruitsAndColor.x], a);
-    store_fruit(d.fruits[pr.fruitsAndColor.y], b);
+    const V3 imp_a = imp_b * -1.0f;
+    sv[ib] = with_xyz(vb, xyz(vb) + imp_b * vb.w);
+    so[ib] = with_xyz(ob4, xyz(ob4) + cross3(ob, imp_b) * ib_inv);
+    sv[ia] = with_xyz(va, xyz(va) + imp_a * va.w);
+    so[ia] = with_xyz(oa4, xyz(oa4) + cross3(oa, imp_a) * ia_inv);
 }
 
 // Fruit/ground Coulomb friction and rolling resistance

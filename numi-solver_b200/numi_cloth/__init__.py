@@ -91,6 +91,7 @@ def load_library() -> ctypes.CDLL:
         "numi_cloth_snapshot": (i32, [vp, u32]),
         "numi_cloth_restore": (i32, [vp, u32]),
         "numi_cloth_launch_info": (i32, [vp, ctypes.POINTER(u32)]),
+        "numi_cloth_trace": (i32, [vp, ctypes.POINTER(ctypes.c_ulonglong), u32, u32]),
         "numi_cloth_material_defaults": (None, [ctypes.POINTER(Material)]),
         "numi_cloth_material_load": (i32, [ctypes.c_char_p, ctypes.POINTER(Material), ctypes.c_char_p, ctypes.c_size_t]),
         "numi_cloth_scene_bag": (vp, [ctypes.POINTER(Material), i32, ctypes.c_double, i32]),
@@ -430,6 +431,13 @@ class ClothSolver:
         out = (ctypes.c_uint32 * 4)()
         self._check(self.lib.numi_cloth_launch_info(self._h, out))
         return {"grid": out[0], "block": out[1], "barriers_per_substep": out[2], "launches": out[3]}
+
+    def trace(self, substeps: int) -> np.ndarray:
+        """Per-barrier globaltimer stamps (ns) of the last step, [substeps, 128]."""
+        out = np.zeros((substeps, 128), np.uint64)
+        self._check(self.lib.numi_cloth_trace(
+            self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_ulonglong)), substeps, 128))
+        return out
 
     @staticmethod
     def _check(rc: int):

@@ -79,3 +79,54 @@ def gpu_positions(out) -> np.ndarray:
 
 def gpu_fruit_positions(out) -> np.ndarray:
     return out["fruits"]["positionAndInverseMass"][:, :3]
+
+
+def oracle_state_to_abi(scene, st):
+    """GPU particle/fruit records (FP32) from an oracle state (FP64)."""
+    P = scene.particles.copy()
+    p = st["particles"]
+    P["positionAndInverseMass"][:, :3] = p["x"]
+    P["positionAndInverseMass"][:, 3] = p["w"]
+    P["previousAndMass"][:, :3] = p["prev"]
+    P["previousAndMass"][:, 3] = p["mass"]
+    P["velocity"][:, :3] = p["v"]
+    P["velocity"][:, 3] = p["vw"]
+    F = scene.fruits.copy()
+    f = st["fruits"]
+    if len(F):
+        F["positionAndInverseMass"][:, :3] = f["x"]
+        F["previousAndRadius"][:, :3] = f["prev"]
+        F["velocityAndGroundImpulse"][:, :3] = f["v"]
+        F["velocityAndGroundImpulse"][:, 3] = f["ground_impulse"]
+        F["angularVelocity"][:, :3] = f["omega"]
+        F["orientation"] = f["q"]
+    return P, F
+
+
+def per_substep_errors(scene, configs, sched):
+    """Max particle / fruit position error of one GPU substep started from
+    the FP64 trajectory's state (rounded to FP32), for every substep."""
+    o = op.Oracle(op.from_abi(scene), 64)
+    subs = op.substeps_from_configs(configs)
+    osched = op.schedule_from_abi(sched, op.BATCHED)
+    s = nc.ClothSolver(scene)
+    errs, ferrs = [], []
+    try:
+        for k in range(len(configs)):
+            st = o.read()
+            P, F = oracle_state_to_abi(scene, st)
+            s.write_particles(P)
+            if len(F):
+                s.write_fruits(F)
+            s.step(configs[k:k + 1], sched)
+            o.step(subs[k:k + 1], osched)
+            nxt = o.read()
+            errs.append(float(np.abs(s.particles()["positionAndInverseMass"][:, :3].astype(np.float64)
+                                     - nxt["particles"]["x"]).max()))
+            if len(F):
+                ferrs.append(float(np.abs(s.fruits()["positionAndInverseMass"][:, :3].astype(np.float64)
+                                          - nxt["fruits"]["x"]).max()))
+        assert s.failure() == 0
+    finally:
+        s.close()
+    return np.array(errs), np.array(ferrs) if ferrs else np.zeros(1)
