@@ -180,15 +180,16 @@ cudaError_t launch(numi_cloth* h, uint32_t substeps, const Schedule& s) {
     sc.substeps = substeps;
     void* args[] = {&d, &sc};
     if (d.trace != nullptr && substeps > h->trace_capacity) d.trace = nullptr;
-    cudaError_t e = cudaMemsetAsync(h->d.bar_count, 0, 2 * sizeof(unsigned long long), h->stream);
+    cudaError_t e = cudaMemsetAsync(h->d.bar_count, 0, 32 * sizeof(unsigned long long), h->stream);
     if (e != cudaSuccess) return e;
     h->last_substeps = substeps;
+    const size_t smem = sizeof(FruitShared);
     if (h->grid == 1) {
-        e = cudaLaunchKernel(reinterpret_cast<const void*>(numi_cloth_frame_kernel), dim3(1), dim3(h->block), args, 0,
-                             h->stream);
+        e = cudaLaunchKernel(reinterpret_cast<const void*>(numi_cloth_frame_kernel), dim3(1), dim3(h->block), args,
+                             smem, h->stream);
     } else {
         e = cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(numi_cloth_frame_kernel), dim3(h->grid),
-                                        dim3(h->block), args, 0, h->stream);
+                                        dim3(h->block), args, smem, h->stream);
     }
     if (e == cudaSuccess) ++h->launches;
     return e;
@@ -209,7 +210,7 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
     const uint32_t n = cfg.control.y, D = cfg.control.z, G = cfg.control.w;
     const uint32_t K = cfg.constraintCounts.x, B = cfg.constraintCounts.y, F = cfg.constraintCounts.w;
     const uint32_t P = cfg.contactCounts.x;
-    if (n == 0 || F > NC_MAX_FRUITS || G > NC_MAX_GRIPS) return NUMI_CLOTH_EINVAL;
+    if (n == 0 || F > NC_MAX_FRUITS || G > NC_MAX_GRIPS || P > NC_MAX_PAIRS) return NUMI_CLOTH_EINVAL;
     if ((D && !scene->distances) || (K && !scene->knots) || (B && !scene->bends) || (G && !scene->grips) ||
         (F && !scene->fruits) || (P && !scene->fruitPairs))
         return NUMI_CLOTH_EINVAL;
@@ -316,13 +317,15 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
     d.cuff = cuff;
     d.yarn_slot_a = h->buf.alloc<float4>(static_cast<size_t>(F ? D : 1) * NC_YARN_SLOTS);
     d.yarn_slot_b = h->buf.alloc<float4>(static_cast<size_t>(F ? D : 1) * NC_YARN_SLOTS);
+    d.yarn_live = h->buf.alloc<uint32_t>(F ? D : 1);
     d.force = h->buf.alloc<float4>(n);
     d.fruit_partial = h->buf.alloc<float4>(NC_MAX_FRUITS * 9u / 2u + 1u);
     d.failure = h->buf.alloc<unsigned int>(1);
     // barrier counter (u64) and abort flag share one 16-byte block so one
     // memset resets both before a launch
-    d.bar_count = h->buf.alloc<unsigned long long>(2);
+    d.bar_count = h->buf.alloc<unsigned long long>(32);
     d.abort_flag = reinterpret_cast<unsigned int*>(d.bar_count + 1);
+    d.bar_flag = d.bar_count + 16;   // 128 bytes away from the arrival counter
     d.stats = h->buf.alloc<uint32_t>(4);
 
     // Launch geometry: one resident CTA for a small cloth, else a full
@@ -330,7 +333,9 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, numi_cloth_frame_kernel, NC_THREADS, 0);
+    cudaFuncSetAttribute(numi_cloth_frame_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(sizeof(FruitShared)));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, numi_cloth_frame_kernel, NC_THREADS, sizeof(FruitShared));
     uint32_t work = std::max({n, D, K, B});
     uint32_t grid = (work <= 8192u) ? 1u : std::min<uint32_t>(sms * std::max(per_sm, 1), (work + NC_THREADS - 1u) / NC_THREADS);
     uint32_t forced = 0;
@@ -345,7 +350,7 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
     d.red = h->buf.alloc<double>(std::max<size_t>(3u * 4096u, 2u * chunks + 8u));
 
     bool ok = d.x && d.xp && d.v && rest && d_ij && d_mat && d.d_lambda && k_ij && k_mat && d.k_lambda && b_ij &&
-              b_mat && d.b_lambda && d.grips && d.fruits && d.pairs && cuff && d.yarn_slot_a && d.yarn_slot_b &&
+              b_mat && d.b_lambda && d.grips && d.fruits && d.pairs && cuff && d.yarn_slot_a && d.yarn_slot_b && d.yarn_live &&
               d.force && d.fruit_partial && d.failure && d.bar_count && d.abort_flag && d.stats && d.red;
     if (!ok) {
         delete h;

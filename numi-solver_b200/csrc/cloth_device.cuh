@@ -71,6 +71,8 @@ struct DeviceCloth {
     // epoch is the current substep, so nothing is cleared between substeps.
     float4* yarn_slot_a;
     float4* yarn_slot_b;
+    // substep epoch of the latest fruit/yarn contact record of each segment
+    uint32_t* yarn_live;
     // per-particle yarn air force of the current substep
     float4* force;
     // 2^-40 fixed-point fruit sums (int64 two's complement):
@@ -89,6 +91,7 @@ struct DeviceCloth {
     // grid barrier: monotonically increasing arrival counter (reset to 0 by
     // the host before every launch) and a sticky abort flag
     unsigned long long* bar_count;
+    unsigned long long* bar_flag;   // barrier number released last (own 128-byte line)
     unsigned int* abort_flag;
     // optional per-barrier globaltimer trace: [substep][NC_TRACE_SLOTS]
     unsigned long long* trace;
@@ -115,4 +118,17 @@ struct Schedule {
     uint32_t release;
     float damping;
     uint32_t substeps;
+};
+
+// Fruit-side state kept in the shared memory of the fruit CTA for a whole
+// launch: compact pair indices (loaded once) and the pair contact impulses
+// of the current substep (the only readers and writers are fruit-CTA
+// phases), plus staging for the fruit sweeps.
+struct FruitShared {
+    unsigned short ab[NC_MAX_PAIRS];       // fruit a | fruit b << 8, colour order
+    float4 contact[NC_MAX_PAIRS];          // weighted normal xyz, normal impulse
+    float4 fx[NC_MAX_FRUITS];              // position xyz, inverse mass
+    float fr[NC_MAX_FRUITS];               // radius
+    float4 v[NC_MAX_FRUITS];               // velocity xyz, inverse mass
+    float4 o[NC_MAX_FRUITS];               // spin xyz, radius
 };

@@ -20,11 +20,13 @@ struct Ctx {
     uint32_t epoch;
     uint32_t sub;
     unsigned long long seq;   // barriers passed in this launch
+    FruitShared* fs;          // fruit-CTA shared state (valid in the fruit CTA)
 };
 
 // Grid-wide barrier with a bounded wait.  Arrival adds 1 to a counter the
-// host zeroes before each launch; barrier number s of the launch completes
-// when the counter reaches s * gridDim.x.  A CTA that waits past the limit
+// host zeroes before each launch; the CTA whose arrival brings it to
+// s * gridDim.x (barrier number s of the launch) releases barrier s through
+// a separate flag that the others poll.  A CTA that waits past the limit
 // raises TIMEOUT and the abort flag, and every CTA leaves at its next
 // barrier (or as soon as it sees the flag while waiting).
 __device__ bool grid_sync(Ctx& ctx) {
@@ -42,10 +44,14 @@ __device__ bool grid_sync(Ctx& ctx) {
     if (threadIdx.x == 0) {
         const unsigned long long target = ctx.seq * gridDim.x;
         __threadfence();
-        atomicAdd(d.bar_count, 1ull);
+        const unsigned long long arrived = atomicAdd(d.bar_count, 1ull) + 1ull;
         unsigned ab = 0u;
         unsigned spins = 0u;
-        while (ld_acquire_u64(d.bar_count) < target) {
+        if (arrived == target) {
+            __threadfence();
+            atomicMax(d.bar_flag, ctx.seq);
+        }
+        while (ld_acquire_u64(d.bar_flag) < ctx.seq) {
             ++spins;
             if ((spins & 63u) == 0u && ld_acquire(d.abort_flag) != 0u) {
                 ab = 1u;
@@ -163,7 +169,7 @@ __device__ void phase_begin(Ctx& ctx) {
             }
             store_fruit(d.fruits[f], s);
         }
-        for (uint32_t k = threadIdx.x; k < d.p_count; k += blockDim.x) d.pairs[k].contact = nf4<numi_float4>(0.0f, 0.0f, 0.0f, 0.0f);
+        for (uint32_t k = threadIdx.x; k < d.p_count; k += blockDim.x) ctx.fs->contact[k] = make_float4(0, 0, 0, 0);
     }
 }
 
@@ -298,6 +304,12 @@ __device__ void air_apply_advance(Ctx& ctx, const float4* force, float att) {
 // (tools/cloth_bag.cpp:2955-3020, 3141-3176).  Fruit positions are the
 // ones at the start of the sweep; each fruit's displacement is summed in
 // fixed point and applied by fruit_flush.
+//
+// Warp broadphase: a warp bounds its 32 segments and keeps only the fruits
+// whose centre lies inside that box grown by the contact distance.  Float
+// subtraction is monotone, so a fruit outside the warp box also fails every
+// per-segment box test; once a contact moves a segment its thread tests all
+// remaining fruits again.  The result is identical to testing every fruit.
 __device__ void yarn_contact_batch(Ctx& ctx, const Batch& bt) {
     const DeviceCloth& d = ctx.d;
     const SubCfg& c = ctx.c;
@@ -312,13 +324,48 @@ __device__ void yarn_contact_batch(Ctx& ctx, const Batch& bt) {
     __syncthreads();
     unsigned long long* acc = reinterpret_cast<unsigned long long*>(d.fruit_partial);
     const uint32_t nf = d.f_count;
-    for (uint32_t k = ctx.tid; k < bt.yarn; k += ctx.nthreads) {
-        const uint32_t seg = bt.first + k;
-        const uint2 ij = __ldg(d.d_ij + seg);
-        float4 pa = ld(d.x + ij.x);
-        float4 pb = ld(d.x + ij.y);
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t base = ctx.tid - lane; base < bt.yarn; base += ctx.nthreads) {
+        const uint32_t k = base + lane;
+        const bool valid = k < bt.yarn;
+        const uint32_t seg = bt.first + (valid ? k : 0u);
+        uint2 ij = make_uint2(0u, 0u);
+        float4 pa = make_float4(0, 0, 0, 0), pb = pa;
+        V3 lo{INFINITY, INFINITY, INFINITY}, hi{-INFINITY, -INFINITY, -INFINITY};
+        if (valid) {
+            ij = __ldg(d.d_ij + seg);
+            pa = ld(d.x + ij.x);
+            pb = ld(d.x + ij.y);
+            lo = V3{fminf(pa.x, pb.x), fminf(pa.y, pb.y), fminf(pa.z, pb.z)};
+            hi = V3{fmaxf(pa.x, pb.x), fmaxf(pa.y, pb.y), fmaxf(pa.z, pb.z)};
+        }
+        V3 wlo = lo, whi = hi;
+        for (int o = 16; o > 0; o >>= 1) {
+            wlo.x = fminf(wlo.x, __shfl_xor_sync(0xffffffffu, wlo.x, o));
+            wlo.y = fminf(wlo.y, __shfl_xor_sync(0xffffffffu, wlo.y, o));
+            wlo.z = fminf(wlo.z, __shfl_xor_sync(0xffffffffu, wlo.z, o));
+            whi.x = fmaxf(whi.x, __shfl_xor_sync(0xffffffffu, whi.x, o));
+            whi.y = fmaxf(whi.y, __shfl_xor_sync(0xffffffffu, whi.y, o));
+            whi.z = fmaxf(whi.z, __shfl_xor_sync(0xffffffffu, whi.z, o));
+        }
+        unsigned long long mask = 0ull;
+        for (uint32_t f0 = 0; f0 < nf; f0 += 32u) {
+            const uint32_t f = f0 + lane;
+            bool near = false;
+            if (f < nf) {
+                const float4 fs = s_fruit[f];
+                const float target = fs.w + c.radius;
+                near = !(fs.x < wlo.x - target || fs.x > whi.x + target || fs.y < wlo.y - target ||
+                         fs.y > whi.y + target || fs.z < wlo.z - target || fs.z > whi.z + target);
+            }
+            mask |= static_cast<unsigned long long>(__ballot_sync(0xffffffffu, near)) << f0;
+        }
+        if (!valid || mask == 0ull) continue;
+        const unsigned long long all = nf == 64u ? ~0ull : ((1ull << nf) - 1ull);
         bool changed = false;
-        for (uint32_t f = 0; f < nf; ++f) {
+        while (mask != 0ull) {
+            const uint32_t f = static_cast<uint32_t>(__ffsll(static_cast<long long>(mask)) - 1);
+            mask &= mask - 1ull;
             const float4 fs = s_fruit[f];
             const V3 X{fs.x, fs.y, fs.z};
             const float target = fs.w + c.radius;
@@ -343,7 +390,10 @@ __device__ void yarn_contact_batch(Ctx& ctx, const Batch& bt) {
             const float corr = target - dist;
             V3 delta{0.0f, 0.0f, 0.0f};
             const float lam = yarn_correction(pa, pb, w0, w1, s_fw[f], n, corr, c.ground, c.radius, delta);
-            changed = true;
+            if (!changed) {
+                changed = true;
+                mask |= all & ~((2ull << f) - 1ull);   // the segment moved: test every later fruit
+            }
             if (delta.x != 0.0f || delta.y != 0.0f || delta.z != 0.0f) {
                 atomicAdd(acc + 3u * f + 0u, static_cast<unsigned long long>(to_fixed(delta.x)));
                 atomicAdd(acc + 3u * f + 1u, static_cast<unsigned long long>(to_fixed(delta.y)));
@@ -377,6 +427,7 @@ __device__ void yarn_contact_batch(Ctx& ctx, const Batch& bt) {
             sb.y = sb.y + w1 * imp;
             d.yarn_slot_a[seg * NC_YARN_SLOTS + q] = sa;
             d.yarn_slot_b[seg * NC_YARN_SLOTS + q] = sb;
+            d.yarn_live[seg] = ctx.epoch;
         }
         if (changed) {
             d.x[ij.x] = pa;
@@ -529,7 +580,7 @@ __device__ bool contacts_pass(Ctx& ctx, bool with_strain) {
     // fruit pairs (fruit CTA) -> fruit/yarn -> [strain] -> ground
     if (ctx.fruit_cta && ctx.d.p_count > 0u) {
         fruit_flush(ctx);
-        fruit_pair_sweep(ctx.d, ctx.c.dt);
+        fruit_pair_sweep(ctx.d, *ctx.fs, ctx.c.dt);
     }
     if (ctx.d.p_count > 0u) NC_SYNC(ctx);
     if (!yarn_sweep(ctx)) return false;
@@ -593,12 +644,7 @@ __device__ void yarn_friction_batch(Ctx& ctx, const Batch& bt) {
     unsigned long long* acc = reinterpret_cast<unsigned long long*>(d.fruit_partial) + 3u * NC_MAX_FRUITS;
     for (uint32_t k = ctx.tid; k < bt.yarn; k += ctx.nthreads) {
         const uint32_t seg = bt.first + k;
-        bool any = false;
-        for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q) {
-            const uint32_t st = __float_as_uint(__ldcg(&d.yarn_slot_b[seg * NC_YARN_SLOTS + q].z));
-            any = any || ((st >> 6) == (ctx.epoch & 0x3ffffffu));
-        }
-        if (!any) continue;
+        if (__ldcg(d.yarn_live + seg) != ctx.epoch) continue;
         const uint2 ij = __ldg(d.d_ij + seg);
         const float4 pa = ld(d.x + ij.x);
         const float4 pb = ld(d.x + ij.y);
@@ -665,37 +711,28 @@ __device__ void yarn_friction_batch(Ctx& ctx, const Batch& bt) {
 
 // Fruit frictions and orientation in the fruit CTA: pair friction on
 // fruit velocities staged in shared memory (one warp walks the colours),
-// then ground friction, rolling resistance and orientation per fruit.
+// then ground friction, rolling resistance and orientation per fruit; the
+// substep's pair impulses are published to global memory for readback.
 __device__ void fruit_tail(Ctx& ctx) {
     if (!ctx.fruit_cta) return;
     const DeviceCloth& d = ctx.d;
     const SubCfg& c = ctx.c;
-    __shared__ float4 s_v[NC_MAX_FRUITS];
-    __shared__ float4 s_o[NC_MAX_FRUITS];
-    __shared__ float s_ni[NC_MAX_PAIRS];
-    __shared__ unsigned short s_ab[NC_MAX_PAIRS];
+    FruitShared& fs = *ctx.fs;
     for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
         const NumiClothFruit& fr = d.fruits[f];
-        s_v[f] = make_float4(fr.velocityAndGroundImpulse.x, fr.velocityAndGroundImpulse.y,
-                             fr.velocityAndGroundImpulse.z, fr.positionAndInverseMass.w);
-        s_o[f] = make_float4(fr.angularVelocity.x, fr.angularVelocity.y, fr.angularVelocity.z,
-                             fr.previousAndRadius.w);
-    }
-    if (ctx.s.frictions) {
-        for (uint32_t k = threadIdx.x; k < d.p_count; k += blockDim.x) {
-            s_ni[k] = d.pairs[k].contact.w;
-            s_ab[k] = static_cast<unsigned short>(d.pairs[k].fruitsAndColor.x | (d.pairs[k].fruitsAndColor.y << 8));
-        }
+        fs.v[f] = make_float4(fr.velocityAndGroundImpulse.x, fr.velocityAndGroundImpulse.y,
+                              fr.velocityAndGroundImpulse.z, fr.positionAndInverseMass.w);
+        fs.o[f] = make_float4(fr.angularVelocity.x, fr.angularVelocity.y, fr.angularVelocity.z,
+                              fr.previousAndRadius.w);
     }
     __syncthreads();
     if (ctx.s.frictions && threadIdx.x < 32u) {
         for (uint32_t b = 0; b < d.n_pair_batches; ++b) {
             const Batch bt = d.pair_batches[b];
             for (uint32_t k = bt.first + threadIdx.x; k < bt.first + bt.count; k += 32u) {
-                const float ni = s_ni[k];
-                if (ni <= 0.0f) continue;
-                const numi_float4 cw = d.pairs[k].contact;
-                pair_friction_smem(s_v, s_o, s_ab[k] & 0xffu, s_ab[k] >> 8, V3{cw.x, cw.y, cw.z}, ni, c.mu_pair);
+                const float4 cw = fs.contact[k];
+                if (cw.w <= 0.0f) continue;
+                pair_friction_smem(fs.v, fs.o, fs.ab[k] & 0xffu, fs.ab[k] >> 8, xyz(cw), cw.w, c.mu_pair);
             }
             __syncwarp();
         }
@@ -703,11 +740,15 @@ __device__ void fruit_tail(Ctx& ctx) {
     __syncthreads();
     for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
         FruitState s = load_fruit(d.fruits[f]);
-        s.v = xyz(s_v[f]);
-        s.omega = xyz(s_o[f]);
+        s.v = xyz(fs.v[f]);
+        s.omega = xyz(fs.o[f]);
         if (ctx.s.frictions) fruit_ground_friction(s, c);
         integrate_orientation(s, c.dt);
         store_fruit(d.fruits[f], s);
+    }
+    for (uint32_t k = threadIdx.x; k < d.p_count; k += blockDim.x) {
+        const float4 cw = fs.contact[k];
+        d.pairs[k].contact = nf4<numi_float4>(cw.x, cw.y, cw.z, cw.w);
     }
     __syncthreads();
 }
@@ -758,7 +799,7 @@ __device__ bool substep(Ctx& ctx, bool last) {
         if (ctx.grip_cta) solve_grips(d, ctx.c);
         if (ctx.fruit_cta && d.p_count > 0u) {
             __syncthreads();
-            fruit_pair_sweep(d, ctx.c.dt);
+            fruit_pair_sweep(d, *ctx.fs, ctx.c.dt);
         }
         NC_SYNC(ctx);
         if (!yarn_sweep(ctx)) return false;
@@ -818,7 +859,16 @@ __device__ bool substep(Ctx& ctx, bool last) {
 }  // namespace nc
 
 __global__ void __launch_bounds__(NC_THREADS) numi_cloth_frame_kernel(DeviceCloth d, Schedule s) {
+    extern __shared__ __align__(16) unsigned char nc_dynamic_smem[];
+    FruitShared& fruit_shared = *reinterpret_cast<FruitShared*>(nc_dynamic_smem);
     nc::Ctx ctx{d, s};
+    ctx.fs = &fruit_shared;
+    if (blockIdx.x == gridDim.x - 1u) {
+        for (uint32_t k = threadIdx.x; k < d.p_count; k += blockDim.x)
+            fruit_shared.ab[k] =
+                static_cast<unsigned short>(d.pairs[k].fruitsAndColor.x | (d.pairs[k].fruitsAndColor.y << 8));
+        __syncthreads();
+    }
     ctx.tid = blockIdx.x * blockDim.x + threadIdx.x;
     ctx.nthreads = gridDim.x * blockDim.x;
     ctx.fruit_cta = blockIdx.x == gridDim.x - 1u;

@@ -394,44 +394,40 @@ __device__ void fruit_air(FruitState& f, const SubCfg& c) {
 }
 
 // Sphere/sphere separation (tools/cloth_bag.cpp:1897-1919).
-// All fruit-pair colours, in the fruit CTA: fruit positions and pair
-// indices staged in shared memory, one warp walks the colours (a colour's
-// pairs are disjoint, so its lanes never touch the same fruit).
-__device__ void fruit_pair_sweep(const DeviceCloth& d, float dt) {
-    __shared__ float4 s_fx[NC_MAX_FRUITS];
-    __shared__ float s_fr[NC_MAX_FRUITS];
-    __shared__ unsigned short s_ab[NC_MAX_PAIRS];
+// All fruit-pair colours, in the fruit CTA: fruit positions staged in
+// shared memory, one warp walks the colours (a colour's pairs are disjoint,
+// so its lanes never touch the same fruit); pair impulses accumulate in
+// shared memory.
+__device__ void fruit_pair_sweep(const DeviceCloth& d, FruitShared& fs, float dt) {
     for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
         const NumiClothFruit& fr = d.fruits[f];
-        s_fx[f] = make_float4(fr.positionAndInverseMass.x, fr.positionAndInverseMass.y,
-                              fr.positionAndInverseMass.z, fr.positionAndInverseMass.w);
-        s_fr[f] = fr.previousAndRadius.w;
+        fs.fx[f] = make_float4(fr.positionAndInverseMass.x, fr.positionAndInverseMass.y,
+                               fr.positionAndInverseMass.z, fr.positionAndInverseMass.w);
+        fs.fr[f] = fr.previousAndRadius.w;
     }
-    for (uint32_t k = threadIdx.x; k < d.p_count; k += blockDim.x)
-        s_ab[k] = static_cast<unsigned short>(d.pairs[k].fruitsAndColor.x | (d.pairs[k].fruitsAndColor.y << 8));
     __syncthreads();
     if (threadIdx.x < 32u) {
         for (uint32_t b = 0; b < d.n_pair_batches; ++b) {
             const Batch bt = d.pair_batches[b];
             for (uint32_t k = bt.first + threadIdx.x; k < bt.first + bt.count; k += 32u) {
-                const uint32_t ia = s_ab[k] & 0xffu;
-                const uint32_t ib = s_ab[k] >> 8;
-                const float4 A = s_fx[ia];
-                const float4 B = s_fx[ib];
+                const uint32_t ia = fs.ab[k] & 0xffu;
+                const uint32_t ib = fs.ab[k] >> 8;
+                const float4 A = fs.fx[ia];
+                const float4 B = fs.fx[ib];
                 const V3 diff = xyz(B) - xyz(A);
                 const float L = len3(diff);
-                const float target = s_fr[ia] + s_fr[ib];
+                const float target = fs.fr[ia] + fs.fr[ib];
                 if (L >= target || L < 1.0e-12f) continue;
                 const float den = A.w + B.w;
                 const float lambda = (target - L) / den;
                 const V3 normal = vdiv(diff, L);
                 const V3 corr = normal * lambda;
-                s_fx[ia] = with_xyz(A, xyz(A) - corr * A.w);
-                s_fx[ib] = with_xyz(B, xyz(B) + corr * B.w);
+                fs.fx[ia] = with_xyz(A, xyz(A) - corr * A.w);
+                fs.fx[ib] = with_xyz(B, xyz(B) + corr * B.w);
                 const float imp = lambda / dt;
-                const numi_float4 c = d.pairs[k].contact;
-                const V3 wn = V3{c.x, c.y, c.z} + normal * imp;
-                d.pairs[k].contact = nf4<numi_float4>(wn.x, wn.y, wn.z, c.w + imp);
+                const float4 c = fs.contact[k];
+                const V3 wn = xyz(c) + normal * imp;
+                fs.contact[k] = make_float4(wn.x, wn.y, wn.z, c.w + imp);
             }
             __syncwarp();
         }
@@ -439,16 +435,11 @@ __device__ void fruit_pair_sweep(const DeviceCloth& d, float dt) {
     __syncthreads();
     for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
         NumiClothFruit& fr = d.fruits[f];
-        fr.positionAndInverseMass.x = s_fx[f].x;
-        fr.positionAndInverseMass.y = s_fx[f].y;
-        fr.positionAndInverseMass.z = s_fx[f].z;
+        fr.positionAndInverseMass.x = fs.fx[f].x;
+        fr.positionAndInverseMass.y = fs.fx[f].y;
+        fr.positionAndInverseMass.z = fs.fx[f].z;
     }
     __syncthreads();
-}
-
-__device__ __forceinline__ void apply_fruit_impulse(FruitState& f, V3 impulse, V3 offset) {
-    f.v = f.v + impulse * f.w;
-    f.omega = f.omega + cross3(offset, impulse) * inverse_inertia(f.w, f.radius);
 }
 
 // Coulomb pair friction (tools/cloth_bag.cpp:1921-1983) on fruit states
@@ -480,6 +471,11 @@ __device__ __forceinline__ void pair_friction_smem(float4* sv, float4* so, uint3
     so[ib] = with_xyz(ob4, xyz(ob4) + cross3(ob, imp_b) * ib_inv);
     sv[ia] = with_xyz(va, xyz(va) + imp_a * va.w);
     so[ia] = with_xyz(oa4, xyz(oa4) + cross3(oa, imp_a) * ia_inv);
+}
+
+__device__ __forceinline__ void apply_fruit_impulse(FruitState& f, V3 impulse, V3 offset) {
+    f.v = f.v + impulse * f.w;
+    f.omega = f.omega + cross3(offset, impulse) * inverse_inertia(f.w, f.radius);
 }
 
 // Fruit/ground Coulomb friction and rolling resistance
