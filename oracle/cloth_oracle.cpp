@@ -601,8 +601,10 @@ struct Sim {
 
     // applyBallYarnCorrection (tools/cloth_bag.cpp:2863-2953); the fruit
     // displacement is returned in delta rather than applied.
+    // direct != nullptr: move that fruit position after every step, as the
+    // reference does (serial order); else sum the steps into delta.
     R yarn_correction(V<R>& pa, V<R>& pb, R wa, R wb, R w0, R w1, R wf, V<R> n, R correction, bool ground,
-                      V<R>& delta) {
+                      V<R>& delta, V<R>* direct = nullptr) {
         const R wt[2] = {w0, w1};
         V<R>* p[2] = {&pa, &pb};
         const R pw[2] = {wa, wb};
@@ -634,7 +636,10 @@ struct Sim {
                     step = rmin(step, dg / -vr);
                 }
             }
-            delta = delta - n * (wf * step);
+            if (direct)
+                *direct = *direct - n * (wf * step);
+            else
+                delta = delta - n * (wf * step);
             for (int s = 0; s < 2; ++s) *p[s] = *p[s] + resp[s] * (wt[s] * step);
             total = total + step;
             remaining = rmax(R(0), remaining - den * step);
@@ -655,7 +660,7 @@ struct Sim {
     // solveBallYarn (tools/cloth_bag.cpp:2955-3020) against fruit position X.
     // Returns the multiplier; pa/pb/delta updated.
     R yarn_contact(uint32_t seg, uint32_t f, V<R> X, V<R>& pa, V<R>& pb, bool ground, R dt, V<R>& delta,
-                   bool& touched) {
+                   bool& touched, V<R>* direct = nullptr) {
         const Fruit& fr = fruits[f];
         const R target = fr.radius + radius;
         if (X.x < rmin(pa.x, pb.x) - target || X.x > rmax(pa.x, pb.x) + target || X.y < rmin(pa.y, pb.y) - target ||
@@ -676,7 +681,7 @@ struct Sim {
         const R w0 = R(1) - t;
         const R w1 = t;
         const R corr = target - dist;
-        const R lam = yarn_correction(pa, pb, w[di[seg]], w[dj[seg]], w0, w1, fr.w, n, corr, ground, delta);
+        const R lam = yarn_correction(pa, pb, w[di[seg]], w[dj[seg]], w0, w1, fr.w, n, corr, ground, delta, direct);
         touched = true;
         if (lam > R(0)) {
             const R imp = lam / dt;
@@ -721,11 +726,10 @@ struct Sim {
                     V<R> pa = x[di[seg]], pb = x[dj[seg]];
                     V<R> delta{};
                     bool touched = false;
-                    yarn_contact(seg, f, fruits[f].x, pa, pb, ground, dt, delta, touched);
+                    yarn_contact(seg, f, fruits[f].x, pa, pb, ground, dt, delta, touched, &fruits[f].x);
                     if (touched) {
                         x[di[seg]] = pa;
                         x[dj[seg]] = pb;
-                        fruits[f].x = fruits[f].x + delta;
                     }
                 }
             return;
@@ -806,10 +810,9 @@ struct Sim {
                 if (removed <= R(0)) continue;
                 V<R> pa = x[ia], pb = x[ib];
                 V<R> delta{};
-                const R lam = yarn_correction(pa, pb, w[ia], w[ib], w0, w1, fr.w, n, removed, ground, delta);
+                const R lam = yarn_correction(pa, pb, w[ia], w[ib], w0, w1, fr.w, n, removed, ground, delta, &fr.x);
                 x[ia] = pa;
                 x[ib] = pb;
-                fr.x = fr.x + delta;
                 if (lam <= R(0)) continue;
                 const R imp = lam / dt;
                 YarnRecord& r = yarn[{seg, f}];

@@ -1,0 +1,26 @@
+# Recipe for the compiled reference checker (test infrastructure only).
+# Builds, from the reference sources where they lie, into oracle/_ref/:
+#   cloth_bag      the reference FP64 CPU cloth executable (tools/cloth_bag.cpp)
+#   libref_shim.so the same source behind the C API of ref_shim.cpp
+# Nothing here is copied into the repository; _ref/ is git-ignored.
+REFERENCE ?= /root/reference
+CXX ?= g++
+HERE := $(abspath $(dir $(lastword $(MAKEFILE_LIST))))
+OUT := $(HERE)/_ref
+FLAGS := -std=c++23 -O3 -I$(REFERENCE)/include -I$(REFERENCE)
+
+all: $(OUT)/cloth_bag $(OUT)/libref_shim.so
+
+$(OUT)/cloth_bag: $(REFERENCE)/tools/cloth_bag.cpp
+	@mkdir -p $(OUT)
+	$(CXX) $(FLAGS) $< -o $@
+
+# Linked against the shared libstdc++ so that it can share a process with
+# Python extension modules that already loaded it.
+LIBSTDCXX ?= $(shell $(CXX) -print-file-name=libstdc++.so.6)
+
+$(OUT)/libref_shim.so: $(HERE)/ref_shim.cpp $(HERE)/oracle.h $(REFERENCE)/tools/cloth_bag.cpp
+	@mkdir -p $(OUT)
+	$(CXX) $(FLAGS) -I$(HERE) -fPIC -shared $(HERE)/ref_shim.cpp $(LIBSTDCXX) -o $@
+
+.PHONY: all
