@@ -206,7 +206,7 @@ def run_ours(args):
         torch.cuda.set_device(0)
     dev = torch.device("cuda", torch.cuda.current_device())
     torch.zeros(1, device=dev)   # create the context before the library uses it
-    scene = nc.square_scene(side=SIDE)
+    scene = nc.square_scene(side=args.side)
     solver = nc.ClothSolver(scene)
     stream = torch.cuda.current_stream(dev)
     solver.set_stream(stream.cuda_stream)
@@ -250,7 +250,7 @@ def run_ours(args):
     host_p = solver.particles()
     host_f = solver.fruits()
     e2e_times = []
-    for k in range(args.warmup + args.steps):
+    for k in range(0 if args.no_e2e else args.warmup + args.steps):
         flush.fill_(1.0)
         barrier()
         t0 = time.perf_counter()
@@ -262,7 +262,7 @@ def run_ours(args):
         dt = time.perf_counter() - t0
         if k >= args.warmup:
             e2e_times.append(dt)
-    e2e_total = sum(e2e_times)
+    e2e_total = sum(e2e_times) if e2e_times else float("nan")
     if world > 1:
         t = torch.tensor([e2e_total], device=dev, dtype=torch.float64)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -331,6 +331,10 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-seconds", type=float, default=6.0)
     ap.add_argument("--no-cpu", action="store_true")
+    # profiling aids (small cases for ncu captures); the bench line is only
+    # valid at the default side
+    ap.add_argument("--side", type=int, default=SIDE)
+    ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -242,6 +242,10 @@ int numi_cloth_launch_info(numi_cloth_t* handle, uint32_t out[4]);
 int numi_cloth_trace(numi_cloth_t* handle, unsigned long long* out,
                      uint32_t substeps, uint32_t slots);
 
+/* Per-CTA barrier arrival stamps of the last step, [substeps][128][grid CTAs]
+ * (ns), when the handle was also created with NUMI_CLOTH_TRACE_CTA=1. */
+int numi_cloth_trace_cta(numi_cloth_t* handle, unsigned long long* out, uint32_t substeps);
+
 /* Library version string. */
 const char* numi_cloth_version(void);
 

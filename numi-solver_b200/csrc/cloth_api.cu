@@ -87,6 +87,7 @@ struct numi_cloth {
     bool poisoned = false;
     uint32_t grid = 1;
     uint32_t block = NC_THREADS;
+    uint32_t cluster = 0;   // > 0: the grid is one cluster of this many CTAs
     uint32_t launches = 0;
     uint32_t trace_capacity = 0;   // substeps the trace buffer holds
     uint32_t last_substeps = 0;
@@ -180,11 +181,27 @@ cudaError_t launch(numi_cloth* h, uint32_t substeps, const Schedule& s) {
     sc.substeps = substeps;
     void* args[] = {&d, &sc};
     if (d.trace != nullptr && substeps > h->trace_capacity) d.trace = nullptr;
+    if (d.trace == nullptr) d.trace_cta = nullptr;
     cudaError_t e = cudaMemsetAsync(h->d.bar_count, 0, 32 * sizeof(unsigned long long), h->stream);
     if (e != cudaSuccess) return e;
     h->last_substeps = substeps;
     const size_t smem = sizeof(FruitShared);
-    if (h->grid == 1) {
+    if (h->cluster > 0) {
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3(h->cluster);
+        cfg.blockDim = dim3(h->block);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = h->stream;
+        cudaLaunchAttribute attr{};
+        attr.id = cudaLaunchAttributeClusterDimension;
+        attr.val.clusterDim.x = h->cluster;
+        attr.val.clusterDim.y = 1;
+        attr.val.clusterDim.z = 1;
+        cfg.attrs = &attr;
+        cfg.numAttrs = 1;
+        d.cluster_barrier = 1u;
+        e = cudaLaunchKernelEx(&cfg, numi_cloth_frame_kernel, d, sc);
+    } else if (h->grid == 1) {
         e = cudaLaunchKernel(reinterpret_cast<const void*>(numi_cloth_frame_kernel), dim3(1), dim3(h->block), args,
                              smem, h->stream);
     } else {
@@ -341,10 +358,45 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
     uint32_t forced = 0;
     if (env_u32("NUMI_CLOTH_GRID", forced) && forced > 0) grid = std::min<uint32_t>(forced, sms * std::max(per_sm, 1));
     h->grid = std::max(grid, 1u);
+    // NUMI_CLOTH_CLUSTER=8 or =16 runs a large cloth as one thread-block
+    // cluster (hardware cluster barrier) when the device can place it; the
+    // default is the cooperative grid.
+    uint32_t want_cluster = 0;
+    env_u32("NUMI_CLOTH_CLUSTER", want_cluster);
+    if (h->grid > 1 && want_cluster > 0 && forced == 0) {
+        cudaFuncSetAttribute(numi_cloth_frame_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        for (uint32_t c : {want_cluster, 8u}) {
+            if (c > 16u || c < 2u) continue;
+            cudaLaunchConfig_t cfg{};
+            cfg.gridDim = dim3(c);
+            cfg.blockDim = dim3(NC_BLOCK_MAX);
+            cfg.dynamicSmemBytes = sizeof(FruitShared);
+            cudaLaunchAttribute attr{};
+            attr.id = cudaLaunchAttributeClusterDimension;
+            attr.val.clusterDim.x = c;
+            attr.val.clusterDim.y = 1;
+            attr.val.clusterDim.z = 1;
+            cfg.attrs = &attr;
+            cfg.numAttrs = 1;
+            int clusters = 0;
+            if (cudaOccupancyMaxActiveClusters(&clusters, numi_cloth_frame_kernel, &cfg) == cudaSuccess &&
+                clusters >= 1) {
+                h->cluster = c;
+                h->grid = c;
+                h->block = NC_BLOCK_MAX;
+                break;
+            }
+        }
+        cudaGetLastError();
+    }
     uint32_t trace_substeps = 0;
     if (env_u32("NUMI_CLOTH_TRACE", trace_substeps) && trace_substeps > 0) {
         d.trace = h->buf.alloc<unsigned long long>(static_cast<size_t>(trace_substeps) * NC_TRACE_SLOTS);
         h->trace_capacity = d.trace ? trace_substeps : 0u;
+        uint32_t per_cta = 0;
+        if (env_u32("NUMI_CLOTH_TRACE_CTA", per_cta) && per_cta > 0)
+            d.trace_cta = h->buf.alloc<unsigned long long>(static_cast<size_t>(trace_substeps) * NC_TRACE_SLOTS *
+                                                           std::max<uint32_t>(h->grid, 1u));
     }
     const uint32_t chunks = (n + NC_THREADS - 1u) / NC_THREADS;
     d.red = h->buf.alloc<double>(std::max<size_t>(3u * 4096u, 2u * chunks + 8u));
@@ -645,6 +697,18 @@ int numi_cloth_trace(numi_cloth_t* h, unsigned long long* out, uint32_t substeps
     cudaSetDevice(h->device);
     if (cudaStreamSynchronize(h->stream) != cudaSuccess ||
         cudaMemcpy(out, h->d.trace, static_cast<size_t>(substeps) * NC_TRACE_SLOTS * sizeof(unsigned long long),
+                   cudaMemcpyDeviceToHost) != cudaSuccess)
+        return NUMI_CLOTH_ECUDA;
+    return NUMI_CLOTH_OK;
+}
+
+int numi_cloth_trace_cta(numi_cloth_t* h, unsigned long long* out, uint32_t substeps) {
+    if (h == nullptr || out == nullptr) return NUMI_CLOTH_EINVAL;
+    if (h->d.trace_cta == nullptr || substeps > h->trace_capacity) return NUMI_CLOTH_ESTATE;
+    cudaSetDevice(h->device);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess ||
+        cudaMemcpy(out, h->d.trace_cta,
+                   static_cast<size_t>(substeps) * NC_TRACE_SLOTS * h->grid * sizeof(unsigned long long),
                    cudaMemcpyDeviceToHost) != cudaSuccess)
         return NUMI_CLOTH_ECUDA;
     return NUMI_CLOTH_OK;

@@ -95,6 +95,11 @@ struct DeviceCloth {
     unsigned int* abort_flag;
     // optional per-barrier globaltimer trace: [substep][NC_TRACE_SLOTS]
     unsigned long long* trace;
+    // optional per-CTA barrier arrival stamps: [substep][NC_TRACE_SLOTS][grid]
+    unsigned long long* trace_cta;
+    // 1: the grid is one thread-block cluster and phases are separated by
+    // the hardware cluster barrier instead of the global-memory barrier
+    uint32_t cluster_barrier;
     double* red;          // [blocks * 8] reduction partials
     uint32_t* stats;      // [0] barriers of the last substep, [1] reconcile passes max, [2] certificate passes max
     uint32_t epoch_base;  // substep counter of the handle at launch

@@ -23,16 +23,27 @@ struct Ctx {
     FruitShared* fs;          // fruit-CTA shared state (valid in the fruit CTA)
 };
 
-// Grid-wide barrier with a bounded wait.  Arrival adds 1 to a counter the
-// host zeroes before each launch; the CTA whose arrival brings it to
-// s * gridDim.x (barrier number s of the launch) releases barrier s through
-// a separate flag that the others poll.  A CTA that waits past the limit
+// Grid-wide barrier with a bounded wait.  Arrival is a release-add of 1 to
+// a counter the host zeroes before each launch; barrier number s of the
+// launch completes when an acquire load sees s * gridDim.x.  A CTA that waits past the limit
 // raises TIMEOUT and the abort flag, and every CTA leaves at its next
 // barrier (or as soon as it sees the flag while waiting).
 __device__ bool grid_sync(Ctx& ctx) {
     const DeviceCloth& d = ctx.d;
     ++ctx.barriers;
     ++ctx.seq;
+    if (d.trace_cta && ctx.barriers <= NC_TRACE_SLOTS) {
+        __syncthreads();
+        if (threadIdx.x == 0)
+            d.trace_cta[(static_cast<size_t>(ctx.sub) * NC_TRACE_SLOTS + ctx.barriers - 1u) * gridDim.x + blockIdx.x] =
+                globaltimer();
+    }
+    if (d.cluster_barrier) {
+        cooperative_groups::this_cluster().sync();
+        if (d.trace && blockIdx.x == 0 && threadIdx.x == 0 && ctx.barriers <= NC_TRACE_SLOTS)
+            d.trace[static_cast<size_t>(ctx.sub) * NC_TRACE_SLOTS + ctx.barriers - 1u] = globaltimer();
+        return true;
+    }
     if (gridDim.x == 1) {
         __syncthreads();
         if (d.trace && threadIdx.x == 0 && ctx.barriers <= NC_TRACE_SLOTS)
@@ -43,15 +54,10 @@ __device__ bool grid_sync(Ctx& ctx) {
     __syncthreads();
     if (threadIdx.x == 0) {
         const unsigned long long target = ctx.seq * gridDim.x;
-        __threadfence();
-        const unsigned long long arrived = atomicAdd(d.bar_count, 1ull) + 1ull;
+        red_release_add_u64(d.bar_count, 1ull);
         unsigned ab = 0u;
         unsigned spins = 0u;
-        if (arrived == target) {
-            __threadfence();
-            atomicMax(d.bar_flag, ctx.seq);
-        }
-        while (ld_acquire_u64(d.bar_flag) < ctx.seq) {
+        while (ld_acquire_u64(d.bar_count) < target) {
             ++spins;
             if ((spins & 63u) == 0u && ld_acquire(d.abort_flag) != 0u) {
                 ab = 1u;
@@ -213,16 +219,21 @@ __device__ void air_force_batch(Ctx& ctx, const Batch& bt, float4* force) {
 }
 
 // Deterministic FP64 sum of two per-particle terms over 256-particle chunks
-// with a fixed tree; chunk partials land in red[2*chunk].
+// with a fixed 256-wide tree (a 512-thread CTA reduces two chunks at once,
+// each with the same tree); chunk partials land in red[2*chunk].
 __device__ void air_reduce_chunks(Ctx& ctx, const float4* force) {
     const DeviceCloth& d = ctx.d;
-    __shared__ double s_p[NC_THREADS];
-    __shared__ double s_q[NC_THREADS];
+    __shared__ double s_p[NC_BLOCK_MAX];
+    __shared__ double s_q[NC_BLOCK_MAX];
     const uint32_t chunks = (d.n + NC_THREADS - 1u) / NC_THREADS;
-    for (uint32_t ch = blockIdx.x; ch < chunks; ch += gridDim.x) {
-        const uint32_t i = ch * NC_THREADS + threadIdx.x;
+    const uint32_t groups = blockDim.x / NC_THREADS;
+    const uint32_t t = threadIdx.x % NC_THREADS;
+    const uint32_t base = threadIdx.x - t;
+    for (uint32_t first = blockIdx.x * groups; first < chunks; first += gridDim.x * groups) {
+        const uint32_t ch = first + threadIdx.x / NC_THREADS;
+        const uint32_t i = ch * NC_THREADS + t;
         double pw = 0.0, q = 0.0;
-        if (i < d.n) {
+        if (ch < chunks && i < d.n) {
             const float4 p = ld(d.x + i);
             if (p.w > 0.0f) {
                 const V3 f = xyz(ld(force + i));
@@ -238,33 +249,36 @@ __device__ void air_reduce_chunks(Ctx& ctx, const float4* force) {
         s_q[threadIdx.x] = q;
         __syncthreads();
         for (uint32_t st = NC_THREADS / 2u; st > 0u; st >>= 1u) {
-            if (threadIdx.x < st) {
-                s_p[threadIdx.x] += s_p[threadIdx.x + st];
-                s_q[threadIdx.x] += s_q[threadIdx.x + st];
+            if (t < st) {
+                s_p[base + t] += s_p[base + t + st];
+                s_q[base + t] += s_q[base + t + st];
             }
             __syncthreads();
         }
-        if (threadIdx.x == 0) {
-            d.red[2u * ch] = s_p[0];
-            d.red[2u * ch + 1u] = s_q[0];
+        if (t == 0 && ch < chunks) {
+            d.red[2u * ch] = s_p[base];
+            d.red[2u * ch + 1u] = s_q[base];
         }
         __syncthreads();
     }
 }
 
-// Every CTA reduces the chunk partials with the same fixed tree.
+// Every CTA reduces the chunk partials with the same fixed tree (the first
+// 256 threads; the tree shape does not depend on the launch).
 __device__ float air_attenuation(Ctx& ctx) {
     const DeviceCloth& d = ctx.d;
     __shared__ double s_p[NC_THREADS];
     __shared__ double s_q[NC_THREADS];
     const uint32_t chunks = (d.n + NC_THREADS - 1u) / NC_THREADS;
-    double pw = 0.0, q = 0.0;
-    for (uint32_t ch = threadIdx.x; ch < chunks; ch += NC_THREADS) {
-        pw += __ldcg(d.red + 2u * ch);
-        q += __ldcg(d.red + 2u * ch + 1u);
+    if (threadIdx.x < NC_THREADS) {
+        double pw = 0.0, q = 0.0;
+        for (uint32_t ch = threadIdx.x; ch < chunks; ch += NC_THREADS) {
+            pw += __ldcg(d.red + 2u * ch);
+            q += __ldcg(d.red + 2u * ch + 1u);
+        }
+        s_p[threadIdx.x] = pw;
+        s_q[threadIdx.x] = q;
     }
-    s_p[threadIdx.x] = pw;
-    s_q[threadIdx.x] = q;
     __syncthreads();
     for (uint32_t st = NC_THREADS / 2u; st > 0u; st >>= 1u) {
         if (threadIdx.x < st) {
@@ -401,25 +415,39 @@ __device__ void yarn_contact_batch(Ctx& ctx, const Batch& bt) {
             }
             if (lam <= 0.0f) continue;
             const float imp = lam / c.dt;
-            // Contact record of (fruit f, segment seg) for friction.
+            // Contact record of (fruit f, segment seg) for friction.  The
+            // first record of the substep takes slot 0 without a search.
             const uint32_t tag = (ctx.epoch << 6) | f;
+            const float4* slot_b = d.yarn_slot_b + seg * NC_YARN_SLOTS;
             int slot = -1;
-            for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q) {
-                const float4 sb = d.yarn_slot_b[seg * NC_YARN_SLOTS + q];
-                const uint32_t st = __float_as_uint(sb.z);
-                if (st == tag) { slot = static_cast<int>(q); break; }
-                if (slot < 0 && (st >> 6) != (ctx.epoch & 0x3ffffffu)) slot = static_cast<int>(q) | 0x100;
+            bool fresh = true;
+            if (__ldcg(d.yarn_live + seg) != ctx.epoch) {
+                slot = 0;
+            } else {
+                uint32_t st[NC_YARN_SLOTS];
+#pragma unroll
+                for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q) st[q] = __float_as_uint(__ldcg(&slot_b[q].z));
+#pragma unroll
+                for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q) {
+                    if (st[q] == tag && fresh) {
+                        slot = static_cast<int>(q);
+                        fresh = false;
+                    }
+                }
+                if (fresh)
+                    for (uint32_t q = 0; q < NC_YARN_SLOTS && slot < 0; ++q)
+                        if ((st[q] >> 6) != (ctx.epoch & 0x3ffffffu)) slot = static_cast<int>(q);
             }
             if (slot < 0) {
                 fail(d, NUMI_CLOTH_FAILURE_RANGE);
                 continue;
             }
-            const uint32_t q = static_cast<uint32_t>(slot) & 0xffu;
+            const uint32_t q = static_cast<uint32_t>(slot);
             float4 sa = make_float4(0, 0, 0, 0);
             float4 sb = make_float4(0, 0, __uint_as_float(tag), 0);
-            if (!(slot & 0x100)) {
-                sa = d.yarn_slot_a[seg * NC_YARN_SLOTS + q];
-                sb = d.yarn_slot_b[seg * NC_YARN_SLOTS + q];
+            if (!fresh) {
+                sa = __ldcg(&d.yarn_slot_a[seg * NC_YARN_SLOTS + q]);
+                sb = __ldcg(&d.yarn_slot_b[seg * NC_YARN_SLOTS + q]);
             }
             const V3 wn = V3{sa.x, sa.y, sa.z} - n * imp;
             sa = make_float4(wn.x, wn.y, wn.z, sa.w + imp);
@@ -427,6 +455,10 @@ __device__ void yarn_contact_batch(Ctx& ctx, const Batch& bt) {
             sb.y = sb.y + w1 * imp;
             d.yarn_slot_a[seg * NC_YARN_SLOTS + q] = sa;
             d.yarn_slot_b[seg * NC_YARN_SLOTS + q] = sb;
+            if (q == 0u && fresh) {
+                // a new substep claims the segment: retire the older records
+                for (uint32_t r = 1; r < NC_YARN_SLOTS; ++r) d.yarn_slot_b[seg * NC_YARN_SLOTS + r].z = __uint_as_float(0u);
+            }
             d.yarn_live[seg] = ctx.epoch;
         }
         if (changed) {
@@ -543,12 +575,12 @@ __device__ void residual_partials(Ctx& ctx, double* out3) {
             }
         }
     }
-    __shared__ double s_r[3][NC_THREADS];
+    __shared__ double s_r[3][NC_BLOCK_MAX];
     s_r[0][threadIdx.x] = strain;
     s_r[1][threadIdx.x] = ground;
     s_r[2][threadIdx.x] = fruit;
     __syncthreads();
-    for (uint32_t st = NC_THREADS / 2u; st > 0u; st >>= 1u) {
+    for (uint32_t st = blockDim.x / 2u; st > 0u; st >>= 1u) {
         if (threadIdx.x < st)
             for (int e = 0; e < 3; ++e) s_r[e][threadIdx.x] = fmax(s_r[e][threadIdx.x], s_r[e][threadIdx.x + st]);
         __syncthreads();
@@ -560,13 +592,13 @@ __device__ void residual_partials(Ctx& ctx, double* out3) {
 
 __device__ bool residuals_converged(Ctx& ctx) {
     const DeviceCloth& d = ctx.d;
-    __shared__ double s_r[3][NC_THREADS];
+    __shared__ double s_r[3][NC_BLOCK_MAX];
     double r[3] = {0.0, 0.0, 0.0};
     for (uint32_t b = threadIdx.x; b < gridDim.x; b += blockDim.x)
         for (int e = 0; e < 3; ++e) r[e] = fmax(r[e], __ldcg(d.red + 3u * b + e));
     for (int e = 0; e < 3; ++e) s_r[e][threadIdx.x] = r[e];
     __syncthreads();
-    for (uint32_t st = NC_THREADS / 2u; st > 0u; st >>= 1u) {
+    for (uint32_t st = blockDim.x / 2u; st > 0u; st >>= 1u) {
         if (threadIdx.x < st)
             for (int e = 0; e < 3; ++e) s_r[e][threadIdx.x] = fmax(s_r[e][threadIdx.x], s_r[e][threadIdx.x + st]);
         __syncthreads();
@@ -650,13 +682,24 @@ __device__ void yarn_friction_batch(Ctx& ctx, const Batch& bt) {
         const float4 pb = ld(d.x + ij.y);
         float4 va = ld(d.v + ij.x);
         float4 vb = ld(d.v + ij.y);
-        // Fruits of this segment in ascending fruit order.
-        for (uint32_t f = 0; f < d.f_count; ++f) {
+        // Live records of this segment, visited in ascending fruit order.
+        const uint32_t live = ctx.epoch & 0x3ffffffu;
+        uint32_t fruit_of[NC_YARN_SLOTS];
+        uint32_t nlive = 0;
+        for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q) {
+            const uint32_t st = __float_as_uint(__ldcg(&d.yarn_slot_b[seg * NC_YARN_SLOTS + q].z));
+            fruit_of[q] = ((st >> 6) == live) ? (st & 63u) : 0xffffffffu;
+            nlive += fruit_of[q] != 0xffffffffu ? 1u : 0u;
+        }
+        for (uint32_t visit = 0; visit < nlive; ++visit) {
             int slot = -1;
-            const uint32_t tag = (ctx.epoch << 6) | f;
+            uint32_t f = 0xffffffffu;
             for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q)
-                if (__float_as_uint(__ldcg(&d.yarn_slot_b[seg * NC_YARN_SLOTS + q].z)) == tag) slot = static_cast<int>(q);
-            if (slot < 0) continue;
+                if (fruit_of[q] < f) {
+                    f = fruit_of[q];
+                    slot = static_cast<int>(q);
+                }
+            fruit_of[slot] = 0xffffffffu;
             const float4 sa = __ldcg(&d.yarn_slot_a[seg * NC_YARN_SLOTS + slot]);
             const float4 sb = __ldcg(&d.yarn_slot_b[seg * NC_YARN_SLOTS + slot]);
             const float ni = sa.w;
@@ -725,8 +768,10 @@ __device__ void fruit_tail(Ctx& ctx) {
         fs.o[f] = make_float4(fr.angularVelocity.x, fr.angularVelocity.y, fr.angularVelocity.z,
                               fr.previousAndRadius.w);
     }
-    __syncthreads();
-    if (ctx.s.frictions && threadIdx.x < 32u) {
+    bool loaded = false;
+    for (uint32_t k = threadIdx.x; k < d.p_count; k += blockDim.x) loaded = loaded || fs.contact[k].w > 0.0f;
+    const bool any_pair = __syncthreads_or(loaded) != 0;
+    if (ctx.s.frictions && any_pair && threadIdx.x < 32u) {
         for (uint32_t b = 0; b < d.n_pair_batches; ++b) {
             const Batch bt = d.pair_batches[b];
             for (uint32_t k = bt.first + threadIdx.x; k < bt.first + bt.count; k += 32u) {
@@ -858,7 +903,7 @@ __device__ bool substep(Ctx& ctx, bool last) {
 
 }  // namespace nc
 
-__global__ void __launch_bounds__(NC_THREADS) numi_cloth_frame_kernel(DeviceCloth d, Schedule s) {
+__global__ void __launch_bounds__(NC_BLOCK_MAX) numi_cloth_frame_kernel(DeviceCloth d, Schedule s) {
     extern __shared__ __align__(16) unsigned char nc_dynamic_smem[];
     FruitShared& fruit_shared = *reinterpret_cast<FruitShared*>(nc_dynamic_smem);
     nc::Ctx ctx{d, s};

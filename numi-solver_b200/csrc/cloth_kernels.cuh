@@ -27,7 +27,10 @@
 #include "cloth_device.cuh"
 #include "vec.cuh"
 
-#define NC_THREADS 256
+#include <cooperative_groups.h>
+
+#define NC_THREADS 256      /* threads of a CTA in the cooperative-grid launch; width of the fixed reduction trees */
+#define NC_BLOCK_MAX 512    /* largest CTA (cluster launch) */
 #define NC_FIXED_SCALE 1099511627776.0   /* 2^40 */
 #define NC_BARRIER_SPIN_LIMIT (1u << 22)
 
@@ -55,6 +58,9 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long
     unsigned long long v;
     asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return v;
+}
+__device__ __forceinline__ void red_release_add_u64(unsigned long long* p, unsigned long long v) {
+    asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 __device__ __forceinline__ unsigned long long globaltimer() {
     unsigned long long t;
@@ -406,6 +412,16 @@ __device__ void fruit_pair_sweep(const DeviceCloth& d, FruitShared& fs, float dt
         fs.fr[f] = fr.previousAndRadius.w;
     }
     __syncthreads();
+    // Fruits move only through pair contacts, so when no pair touches at the
+    // start of the sweep none touches at any point of it: skip the walk.
+    bool touching = false;
+    for (uint32_t k = threadIdx.x; k < d.p_count; k += blockDim.x) {
+        const uint32_t ia = fs.ab[k] & 0xffu;
+        const uint32_t ib = fs.ab[k] >> 8;
+        const float L = len3(xyz(fs.fx[ib]) - xyz(fs.fx[ia]));
+        touching = touching || !(L >= fs.fr[ia] + fs.fr[ib] || L < 1.0e-12f);
+    }
+    if (!__syncthreads_or(touching)) return;
     if (threadIdx.x < 32u) {
         for (uint32_t b = 0; b < d.n_pair_batches; ++b) {
             const Batch bt = d.pair_batches[b];

@@ -92,6 +92,7 @@ def load_library() -> ctypes.CDLL:
         "numi_cloth_restore": (i32, [vp, u32]),
         "numi_cloth_launch_info": (i32, [vp, ctypes.POINTER(u32)]),
         "numi_cloth_trace": (i32, [vp, ctypes.POINTER(ctypes.c_ulonglong), u32, u32]),
+        "numi_cloth_trace_cta": (i32, [vp, ctypes.POINTER(ctypes.c_ulonglong), u32]),
         "numi_cloth_material_defaults": (None, [ctypes.POINTER(Material)]),
         "numi_cloth_material_load": (i32, [ctypes.c_char_p, ctypes.POINTER(Material), ctypes.c_char_p, ctypes.c_size_t]),
         "numi_cloth_scene_bag": (vp, [ctypes.POINTER(Material), i32, ctypes.c_double, i32]),
@@ -437,6 +438,14 @@ class ClothSolver:
         out = np.zeros((substeps, 128), np.uint64)
         self._check(self.lib.numi_cloth_trace(
             self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_ulonglong)), substeps, 128))
+        return out
+
+    def trace_cta(self, substeps: int) -> np.ndarray:
+        """Per-CTA barrier arrival stamps (ns), [substeps, 128, grid]."""
+        grid = self.launch_info()["grid"]
+        out = np.zeros((substeps, 128, grid), np.uint64)
+        self._check(self.lib.numi_cloth_trace_cta(
+            self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_ulonglong)), substeps))
         return out
 
     @staticmethod

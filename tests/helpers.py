@@ -36,18 +36,25 @@ def bag_frame_configs(scene: nc.SceneArrays, first: int, count: int, dt: float) 
     return traj.configs(scene.config, scene.handle_base, first, count, dt)
 
 
-def run_gpu(scene, configs, sched: nc.Schedule, frames=1, grid=None):
-    env_old = os.environ.get("NUMI_CLOTH_GRID")
+def make_solver(scene, grid=None, env=None):
+    """A solver created under temporary launch-policy environment variables."""
+    env = dict(env or {})
     if grid is not None:
-        os.environ["NUMI_CLOTH_GRID"] = str(grid)
+        env["NUMI_CLOTH_GRID"] = str(grid)
+    old = {k: os.environ.get(k) for k in env}
+    os.environ.update({k: str(v) for k, v in env.items()})
     try:
-        s = nc.ClothSolver(scene)
+        return nc.ClothSolver(scene)
     finally:
-        if grid is not None:
-            if env_old is None:
-                os.environ.pop("NUMI_CLOTH_GRID", None)
+        for k, v in old.items():
+            if v is None:
+                os.environ.pop(k, None)
             else:
-                os.environ["NUMI_CLOTH_GRID"] = env_old
+                os.environ[k] = v
+
+
+def run_gpu(scene, configs, sched: nc.Schedule, frames=1, grid=None, env=None):
+    s = make_solver(scene, grid, env)
     per = len(configs) // frames
     for f in range(frames):
         s.step(configs[f * per:(f + 1) * per], sched)

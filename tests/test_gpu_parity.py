@@ -100,6 +100,22 @@ def test_multi_cta_equals_single_cta():
     assert np.array_equal(one["fruits"], many["fruits"])
 
 
+def test_cluster_equals_cooperative_grid():
+    """One thread-block cluster (hardware cluster barrier) and the
+    cooperative grid (global-memory barrier) give the same bits."""
+    scene = small_square(side=96, fruits=16)
+    cfg = nc.substep_configs(scene, 12)
+    s = nc.Schedule.make(**FULL)
+    grid = run_gpu(scene, cfg, s, env={"NUMI_CLOTH_CLUSTER": "0"})
+    clus = run_gpu(scene, cfg, s, env={"NUMI_CLOTH_CLUSTER": "16"})
+    assert grid["info"]["grid"] > 16
+    assert clus["info"]["grid"] in (8, 16)
+    assert np.array_equal(grid["particles"], clus["particles"])
+    assert np.array_equal(grid["fruits"], clus["fruits"])
+    o = run_oracle(scene, cfg, s, bits=32)
+    _check_bitexact(clus, o)
+
+
 def test_two_runs_bit_identical():
     scene = small_square(side=40, fruits=10)
     cfg = nc.substep_configs(scene, 24)
