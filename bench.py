@@ -282,7 +282,7 @@ def run_ours(args):
     achieved = ab["total"] * SUBSTEPS / (per_launch_ms / 1000.0) / 1e9
     peaks = measured_peaks()
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "frame_kernel_traffic.json")
+    tpath = os.path.join(ROOT, "profiles", f"frame_kernel_square{args.side}_traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
             traffic = json.load(f).get("dram_bytes_per_launch")
@@ -325,7 +325,7 @@ def run_ours(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
