@@ -246,6 +246,74 @@ int numi_cloth_trace(numi_cloth_t* handle, unsigned long long* out,
  * (ns), when the handle was also created with NUMI_CLOTH_TRACE_CTA=1. */
 int numi_cloth_trace_cta(numi_cloth_t* handle, unsigned long long* out, uint32_t substeps);
 
+/* ---------------------------------------------------------------------------
+ * Allocation-free stepping.  No counterpart in the reference: its Metal host
+ * always allocates its own buffers (tools/cloth_bag_metal.mm:4091-4202).
+ *
+ * For callers that cannot let the library allocate GPU memory: hosts that
+ * own every device byte through their own pool or arena, and code that steps
+ * the cloth from inside a stream capture, where a cudaMalloc would break the
+ * capture (and elsewhere synchronises the whole device).  The caller passes
+ * every input and output as device buffers in the library's structure-of-
+ * arrays layout; the library's own scratch (contact records, air forces,
+ * fixed-point fruit sums, reduction partials, the substep Configs) lives in
+ * one statically allocated device array of about 1.2 MB that every GPU that
+ * loads the library keeps until the process exits.
+ *
+ * Limits: at most NUMI_CLOTH_NOALLOC_MAX_PARTICLES particles,
+ * NUMI_CLOTH_NOALLOC_MAX_DISTANCES distances, 64 fruits and
+ * NUMI_CLOTH_NOALLOC_MAX_SUBSTEPS substeps per call; larger inputs are
+ * rejected with NUMI_CLOTH_EINVAL.  The cloth runs on one CTA (the resident
+ * small-cloth path).
+ *
+ * The first call on a device looks up the scratch array's device address
+ * (once per device, with that device current); make that first call before
+ * any stream capture begins.  All calls share the one scratch array and
+ * every call clears the parts that must start at zero, so calls whose
+ * kernels overlap on the GPU (different streams, no ordering between them)
+ * race on it: order them on one stream or with events.
+ * ------------------------------------------------------------------------ */
+#define NUMI_CLOTH_NOALLOC_MAX_PARTICLES 4096u
+#define NUMI_CLOTH_NOALLOC_MAX_DISTANCES 8192u
+#define NUMI_CLOTH_NOALLOC_MAX_SUBSTEPS 256u
+
+/* Device buffers of one cloth, library layout (float4 = 4 floats). */
+typedef struct NumiClothDeviceState {
+    float* positions;              /* float4[N] xyz, inverse mass        (in/out) */
+    float* previous;               /* float4[N] xyz, mass                (in/out) */
+    float* velocities;             /* float4[N] xyz, ground impulse      (in/out) */
+    const float* rest;             /* float4[N] rest positions           (in) */
+    const uint32_t* distanceIJ;    /* uint2[D] particle pair, colour-run order (in) */
+    const float* distanceMaterial; /* float4[D] rest, compliance, 0, max extension (in) */
+    float* distanceLambda;         /* float[D]                           (out) */
+    const uint32_t* knotIJ;        /* uint4[K]                           (in) */
+    const float* knotMaterial;     /* float2[K] rest cosine, compliance  (in) */
+    float* knotLambda;             /* float[K]                           (out) */
+    const uint32_t* bendIJ;        /* uint4[B] first, middle, third, 0   (in) */
+    const float* bendMaterial;     /* float2[B] rest chord, compliance   (in) */
+    float* bendLambda;             /* float[B]                           (out) */
+    NumiClothGrip* grips;          /* [G]                                (in/out) */
+    NumiClothFruit* fruits;        /* [F]                                (in/out) */
+    NumiClothFruitPair* fruitPairs;/* [P]                                (in/out) */
+    const uint32_t* cuffParticles; /* 2 x ring count, or NULL            (in) */
+    uint32_t* failure;             /* one word: zeroed, then failure bits (out) */
+} NumiClothDeviceState;
+
+/* Advance count substeps of the cloth described by base (counts, material)
+ * and state, on stream (cudaStream_t as void*), without allocating.
+ * batches holds the distance, knot, bend and fruit-pair colour runs, in that
+ * order, batchCounts[4] of each; control = (first, count, colour, x) where for
+ * distance runs x = yarn-prefix count | strain-limited-prefix count << 16.
+ * configs (host) are validated as by numi_cloth_step; an invalid one sets
+ * its failure bit in the host-visible return value and nothing runs.
+ * Returns NUMI_CLOTH_OK, NUMI_CLOTH_EINVAL (size over a limit, bad
+ * argument, with a message on stderr) or NUMI_CLOTH_ECUDA; a rejected Config
+ * returns its failure bit as a positive value. */
+int numi_cloth_step_noalloc(const NumiClothConfig* base, const NumiClothDeviceState* state,
+                            const NumiClothBatch* batches, const uint32_t batchCounts[4],
+                            const NumiClothConfig* configs, uint32_t count,
+                            const NumiClothSchedule* schedule, void* stream);
+
 /* Library version string. */
 const char* numi_cloth_version(void);
 

@@ -729,3 +729,172 @@ int numi_cloth_launch_info(numi_cloth_t* h, uint32_t out[4]) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------
+// Allocation-free stepping (numi_cloth_step_noalloc in numi_cloth.h).  The
+// array below is the only device memory this path uses besides the
+// caller's buffers: contact records, air forces, fixed-point fruit sums,
+// reduction partials and the substep Configs of one call.
+namespace {
+
+struct NoAllocScratch {
+    float4 slot_a[NUMI_CLOTH_NOALLOC_MAX_DISTANCES * NC_YARN_SLOTS];
+    float4 slot_b[NUMI_CLOTH_NOALLOC_MAX_DISTANCES * NC_YARN_SLOTS];
+    uint32_t live[NUMI_CLOTH_NOALLOC_MAX_DISTANCES];
+    float4 force[NUMI_CLOTH_NOALLOC_MAX_PARTICLES];
+    unsigned long long fruit_sums[9u * NC_MAX_FRUITS + 8u];
+    double red[256];
+    NumiClothConfig configs[NUMI_CLOTH_NOALLOC_MAX_SUBSTEPS];
+    unsigned long long barrier[32];
+    uint32_t stats[4];
+};
+
+// File-scope device array.  In host code this name is only a stand-in for
+// the symbol, never a device address; the address comes from
+// cudaGetSymbolAddress, once per device.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocScratch)];
+
+constexpr int kMaxDevices = 64;
+NoAllocScratch* g_noalloc_ptr[kMaxDevices] = {};
+
+NoAllocScratch* noalloc_scratch(int device) {
+    if (device < 0 || device >= kMaxDevices) return nullptr;
+    if (g_noalloc_ptr[device] == nullptr) {
+        void* ptr = nullptr;
+        if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || ptr == nullptr) return nullptr;
+        g_noalloc_ptr[device] = static_cast<NoAllocScratch*>(ptr);
+    }
+    return g_noalloc_ptr[device];
+}
+
+int noalloc_reject(const char* what) {
+    std::fprintf(stderr, "numi_cloth_step_noalloc: %s\n", what);
+    return NUMI_CLOTH_EINVAL;
+}
+
+}  // namespace
+
+extern "C" int numi_cloth_step_noalloc(const NumiClothConfig* base, const NumiClothDeviceState* st,
+                                       const NumiClothBatch* batches, const uint32_t batchCounts[4],
+                                       const NumiClothConfig* configs, uint32_t count,
+                                       const NumiClothSchedule* schedule, void* stream_ptr) {
+    if (base == nullptr || st == nullptr || configs == nullptr || schedule == nullptr || batchCounts == nullptr ||
+        count == 0)
+        return noalloc_reject("null argument or zero substeps");
+    const uint32_t n = base->control.y, D = base->control.z, G = base->control.w;
+    const uint32_t K = base->constraintCounts.x, B = base->constraintCounts.y, F = base->constraintCounts.w;
+    const uint32_t P = base->contactCounts.x;
+    if (n == 0 || n > NUMI_CLOTH_NOALLOC_MAX_PARTICLES)
+        return noalloc_reject("particle count is zero or above NUMI_CLOTH_NOALLOC_MAX_PARTICLES (4096)");
+    if (D > NUMI_CLOTH_NOALLOC_MAX_DISTANCES)
+        return noalloc_reject("distance count above NUMI_CLOTH_NOALLOC_MAX_DISTANCES (8192)");
+    if (count > NUMI_CLOTH_NOALLOC_MAX_SUBSTEPS)
+        return noalloc_reject("substeps per call above NUMI_CLOTH_NOALLOC_MAX_SUBSTEPS (256)");
+    if (F > NC_MAX_FRUITS || G > NC_MAX_GRIPS || P > NC_MAX_PAIRS)
+        return noalloc_reject("fruit, grip or fruit-pair count above its limit");
+    for (int k = 0; k < 4; ++k)
+        if (batchCounts[k] > NC_MAX_BATCHES) return noalloc_reject("more than 64 colour runs in one family");
+    if ((batchCounts[0] + batchCounts[1] + batchCounts[2] + batchCounts[3]) != 0u && batches == nullptr)
+        return noalloc_reject("null batches");
+    if (!st->positions || !st->previous || !st->velocities || !st->rest || !st->failure ||
+        (D && (!st->distanceIJ || !st->distanceMaterial || !st->distanceLambda)) ||
+        (K && (!st->knotIJ || !st->knotMaterial || !st->knotLambda)) ||
+        (B && (!st->bendIJ || !st->bendMaterial || !st->bendLambda)) || (G && !st->grips) || (F && !st->fruits) ||
+        (P && !st->fruitPairs) || (base->gripControl.y == 1u && !st->cuffParticles))
+        return noalloc_reject("null device buffer");
+    uint32_t bad = 0;
+    for (uint32_t k = 0; k < count && bad == 0u; ++k) bad = validate_config(configs[k], *base);
+    if (bad != 0u) return static_cast<int>(bad);
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) return NUMI_CLOTH_ECUDA;
+    NoAllocScratch* scratch = noalloc_scratch(device);
+    if (scratch == nullptr) return NUMI_CLOTH_ECUDA;
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+
+    DeviceCloth d{};
+    d.x = reinterpret_cast<float4*>(st->positions);
+    d.xp = reinterpret_cast<float4*>(st->previous);
+    d.v = reinterpret_cast<float4*>(st->velocities);
+    d.rest = reinterpret_cast<const float4*>(st->rest);
+    d.n = n;
+    d.d_ij = reinterpret_cast<const uint2*>(st->distanceIJ);
+    d.d_mat = reinterpret_cast<const float4*>(st->distanceMaterial);
+    d.d_lambda = st->distanceLambda;
+    d.d_count = D;
+    d.k_ij = reinterpret_cast<const uint4*>(st->knotIJ);
+    d.k_mat = reinterpret_cast<const float2*>(st->knotMaterial);
+    d.k_lambda = st->knotLambda;
+    d.k_count = K;
+    d.b_ij = reinterpret_cast<const uint4*>(st->bendIJ);
+    d.b_mat = reinterpret_cast<const float2*>(st->bendMaterial);
+    d.b_lambda = st->bendLambda;
+    d.b_count = B;
+    d.grips = st->grips;
+    d.g_count = G;
+    d.fruits = st->fruits;
+    d.f_count = F;
+    d.pairs = st->fruitPairs;
+    d.p_count = P;
+    d.cuff = st->cuffParticles;
+    d.failure = st->failure;
+    d.yarn_slot_a = scratch->slot_a;
+    d.yarn_slot_b = scratch->slot_b;
+    d.yarn_live = scratch->live;
+    d.force = scratch->force;
+    d.fruit_partial = reinterpret_cast<float4*>(scratch->fruit_sums);
+    d.red = scratch->red;
+    d.bar_count = scratch->barrier;
+    d.abort_flag = reinterpret_cast<unsigned int*>(scratch->barrier + 1);
+    d.bar_flag = scratch->barrier + 16;
+    d.stats = scratch->stats;
+    d.cfg = scratch->configs;
+    d.epoch_base = 1u;   // contact records are cleared below, so epochs restart at 1
+    Batch* families[4] = {d.dist_batches, d.knot_batches, d.bend_batches, d.pair_batches};
+    uint32_t* family_counts[4] = {&d.n_dist_batches, &d.n_knot_batches, &d.n_bend_batches, &d.n_pair_batches};
+    const NumiClothBatch* b = batches;
+    for (int fam = 0; fam < 4; ++fam) {
+        *family_counts[fam] = batchCounts[fam];
+        for (uint32_t k = 0; k < batchCounts[fam]; ++k, ++b) {
+            Batch& o = families[fam][k];
+            o.first = b->control.x;
+            o.count = b->control.y;
+            o.yarn = fam == 0 ? (b->control.w & 0xffffu) : 0u;
+            o.limited = fam == 0 ? (b->control.w >> 16) : 0u;
+        }
+    }
+    // Every call shares the scratch: clear what must start at zero (contact
+    // records and their live epochs, fixed-point fruit sums, barrier words,
+    // stats) and the caller's failure word.
+    cudaError_t e = cudaMemsetAsync(scratch->slot_b, 0, sizeof(scratch->slot_b), stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(scratch->live, 0, sizeof(scratch->live), stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(scratch->fruit_sums, 0, sizeof(scratch->fruit_sums), stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(scratch->barrier, 0, sizeof(scratch->barrier), stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(scratch->stats, 0, sizeof(scratch->stats), stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(st->failure, 0, sizeof(uint32_t), stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(scratch->configs, configs, count * sizeof(NumiClothConfig), cudaMemcpyHostToDevice,
+                            stream);
+    if (e != cudaSuccess) return NUMI_CLOTH_ECUDA;
+    Schedule s{};
+    s.iterations = schedule->iterations;
+    s.strain_sweeps = schedule->strainSweeps;
+    s.reconcile_passes = schedule->reconcilePasses;
+    s.final_passes = schedule->finalPasses;
+    s.certificate_passes = schedule->certificatePasses;
+    s.early_exit = schedule->earlyExit;
+    s.self_collision = schedule->selfCollision;
+    s.aerodynamics = schedule->aerodynamics;
+    s.swept_ground = schedule->sweptGround;
+    s.swept_fruit_yarn = schedule->sweptFruitYarn;
+    s.frictions = schedule->frictions;
+    s.release = schedule->release;
+    s.damping = schedule->damping;
+    s.substeps = count;
+    void* args[] = {&d, &s};
+    e = cudaFuncSetAttribute(numi_cloth_frame_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(sizeof(FruitShared)));
+    if (e == cudaSuccess)
+        e = cudaLaunchKernel(reinterpret_cast<const void*>(numi_cloth_frame_kernel), dim3(1), dim3(NC_THREADS), args,
+                             sizeof(FruitShared), stream);
+    return e == cudaSuccess ? NUMI_CLOTH_OK : NUMI_CLOTH_ECUDA;
+}

@@ -93,6 +93,9 @@ def load_library() -> ctypes.CDLL:
         "numi_cloth_launch_info": (i32, [vp, ctypes.POINTER(u32)]),
         "numi_cloth_trace": (i32, [vp, ctypes.POINTER(ctypes.c_ulonglong), u32, u32]),
         "numi_cloth_trace_cta": (i32, [vp, ctypes.POINTER(ctypes.c_ulonglong), u32]),
+        "numi_cloth_step_noalloc": (
+            i32, [vp, ctypes.POINTER(abi.DeviceState), vp, ctypes.POINTER(u32), vp, u32, ctypes.POINTER(Schedule), vp],
+        ),
         "numi_cloth_material_defaults": (None, [ctypes.POINTER(Material)]),
         "numi_cloth_material_load": (i32, [ctypes.c_char_p, ctypes.POINTER(Material), ctypes.c_char_p, ctypes.c_size_t]),
         "numi_cloth_scene_bag": (vp, [ctypes.POINTER(Material), i32, ctypes.c_double, i32]),
@@ -460,3 +463,57 @@ def substep_configs(scene: SceneArrays, count: int, dt: float | None = None) -> 
     if dt is not None:
         cfg["gravityAndTimestep"][:, 3] = dt
     return cfg
+
+
+def colour_runs(scene: SceneArrays):
+    """NumiClothBatch records of the scene's colour runs (distance, knot,
+    bend, fruit pair) and the count of each family; distance runs carry the
+    yarn-prefix | strain-limited-prefix << 16 word."""
+    from .abi import KIND_SHEAR
+
+    def runs(colours, extra=None):
+        out = []
+        k = 0
+        while k < len(colours):
+            first = k
+            while k < len(colours) and colours[k] == colours[first]:
+                k += 1
+            w = extra(first, k) if extra else 0
+            out.append((first, k - first, int(colours[first]), w))
+        return out
+
+    d = scene.distances
+
+    def dist_extra(first, end):
+        yarn = limited = 0
+        for i in range(first, end):
+            if d["particlesAndColor"][i, 3] != KIND_SHEAR:
+                yarn = i - first + 1
+            if d["material"][i, 3] > 0:
+                limited = i - first + 1
+        return yarn | (limited << 16)
+
+    fams = [
+        runs(d["particlesAndColor"][:, 2], dist_extra),
+        runs(scene.knots["control"][:, 0]) if len(scene.knots) else [],
+        runs(scene.bends["particlesAndColor"][:, 3]) if len(scene.bends) else [],
+        runs(scene.pairs["fruitsAndColor"][:, 2]) if len(scene.pairs) else [],
+    ]
+    flat = [r for f in fams for r in f]
+    recs = np.zeros((max(len(flat), 1), 4), np.uint32)
+    for i, r in enumerate(flat):
+        recs[i] = r
+    return recs, np.array([len(f) for f in fams], np.uint32)
+
+
+def step_noalloc(scene: SceneArrays, state: abi.DeviceState, batches: np.ndarray, counts: np.ndarray,
+                 configs: np.ndarray, schedule: Schedule, stream_ptr: int | None = None) -> int:
+    """numi_cloth_step_noalloc: step device buffers the caller owns; returns
+    the ABI return code (0 ok, <0 error, >0 a rejected Config's failure bit)."""
+    configs = np.ascontiguousarray(configs, CONFIG)
+    batches = np.ascontiguousarray(batches, np.uint32)
+    counts = np.ascontiguousarray(counts, np.uint32)
+    return int(load_library().numi_cloth_step_noalloc(
+        _ptr(scene.config), ctypes.byref(state), _ptr(batches),
+        counts.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), _ptr(configs), len(configs),
+        ctypes.byref(schedule), ctypes.c_void_p(stream_ptr) if stream_ptr else None))

@@ -219,3 +219,21 @@ class GripPose(ctypes.Structure):
 
 def failure_names(word: int) -> list[str]:
     return [name for bit, name in FAILURE_NAMES.items() if word & bit]
+
+
+class DeviceState(ctypes.Structure):
+    """NumiClothDeviceState: device buffers of one cloth, library layout."""
+
+    _fields_ = [
+        (name, ctypes.c_void_p)
+        for name in (
+            "positions", "previous", "velocities", "rest", "distanceIJ", "distanceMaterial", "distanceLambda",
+            "knotIJ", "knotMaterial", "knotLambda", "bendIJ", "bendMaterial", "bendLambda", "grips", "fruits",
+            "fruitPairs", "cuffParticles", "failure",
+        )
+    ]
+
+
+NOALLOC_MAX_PARTICLES = 4096
+NOALLOC_MAX_DISTANCES = 8192
+NOALLOC_MAX_SUBSTEPS = 256
