@@ -305,7 +305,8 @@ def run_ours(args):
                        "substeps_per_step": SUBSTEPS, "schedule": BENCH_SCHEDULE,
                        "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}",
                        "grid": info["grid"], "block": info["block"],
-                       "barriers_per_substep": info["barriers_per_substep"]},
+                       "barriers_per_substep": info["barriers_per_substep"], "cluster": info["cluster"],
+                       "particles_resident_in_smem": info["resident"]},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                          "peak_source": peaks["source"], "algorithmic_bytes_per_substep": ab},

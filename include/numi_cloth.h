@@ -229,8 +229,9 @@ int numi_cloth_snapshot(numi_cloth_t* handle, uint32_t slot);
 int numi_cloth_restore(numi_cloth_t* handle, uint32_t slot);
 
 /* Launch geometry of the last step: grid CTAs, threads per CTA, barriers
- * per substep, kernel launches. */
-int numi_cloth_launch_info(numi_cloth_t* handle, uint32_t out[4]);
+ * per substep, kernel launches, cluster size (0: no cluster), and 1 when the
+ * particles are resident in (distributed) shared memory. */
+int numi_cloth_launch_info(numi_cloth_t* handle, uint32_t out[6]);
 
 /* Per-phase device timestamps of the last step (profiling aid).  Enabled
  * when the handle was created with NUMI_CLOTH_TRACE=<substeps> in the

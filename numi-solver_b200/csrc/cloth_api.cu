@@ -42,6 +42,7 @@ __global__ void __launch_bounds__(NC_THREADS) numi_cloth_residual_kernel(DeviceC
 namespace {
 
 constexpr uint32_t kSnapshotSlots = 8;
+constexpr uint32_t kResidentChunk = 4096;   // particles a CTA holds in resident mode
 
 struct Snapshot {
     bool valid = false;
@@ -88,6 +89,7 @@ struct numi_cloth {
     uint32_t grid = 1;
     uint32_t block = NC_THREADS;
     uint32_t cluster = 0;   // > 0: the grid is one cluster of this many CTAs
+    size_t smem = sizeof(FruitShared);   // dynamic shared memory of a frame launch
     uint32_t launches = 0;
     uint32_t trace_capacity = 0;   // substeps the trace buffer holds
     uint32_t last_substeps = 0;
@@ -101,6 +103,18 @@ struct numi_cloth {
 };
 
 namespace {
+
+// cudaFuncAttributeMaxDynamicSharedMemorySize is per function, not per
+// launch, and cloths with different launch modes share the frame kernel: only
+// ever raise it, so that creating one cloth never breaks another's launch.
+cudaError_t raise_frame_smem(size_t bytes) {
+    cudaFuncAttributes fa{};
+    cudaError_t e = cudaFuncGetAttributes(&fa, numi_cloth_frame_kernel);
+    if (e != cudaSuccess) return e;
+    if (static_cast<size_t>(fa.maxDynamicSharedSizeBytes) >= bytes) return cudaSuccess;
+    return cudaFuncSetAttribute(numi_cloth_frame_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(bytes));
+}
 
 bool finite4(const numi_float4& v) {
     return std::isfinite(v.x) && std::isfinite(v.y) && std::isfinite(v.z) && std::isfinite(v.w);
@@ -185,7 +199,7 @@ cudaError_t launch(numi_cloth* h, uint32_t substeps, const Schedule& s) {
     cudaError_t e = cudaMemsetAsync(h->d.bar_count, 0, 32 * sizeof(unsigned long long), h->stream);
     if (e != cudaSuccess) return e;
     h->last_substeps = substeps;
-    const size_t smem = sizeof(FruitShared);
+    const size_t smem = h->smem;
     if (h->cluster > 0) {
         cudaLaunchConfig_t cfg{};
         cfg.gridDim = dim3(h->cluster);
@@ -350,8 +364,7 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
     int per_sm = 0;
-    cudaFuncSetAttribute(numi_cloth_frame_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         static_cast<int>(sizeof(FruitShared)));
+    raise_frame_smem(sizeof(FruitShared));
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, numi_cloth_frame_kernel, NC_THREADS, sizeof(FruitShared));
     uint32_t work = std::max({n, D, K, B});
     uint32_t grid = (work <= 8192u) ? 1u : std::min<uint32_t>(sms * std::max(per_sm, 1), (work + NC_THREADS - 1u) / NC_THREADS);
@@ -363,6 +376,59 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
     // default is the cooperative grid.
     uint32_t want_cluster = 0;
     env_u32("NUMI_CLOTH_CLUSTER", want_cluster);
+    // Resident mode: particle positions and velocities stay in the shared
+    // memory of one CTA (n <= 4096, the default) or, with
+    // NUMI_CLOTH_RESIDENT=2, of one thread-block cluster of up to 16 CTAs
+    // holding 4096 particles each (n <= 65536) for the whole frame, where
+    // accesses to another CTA's particles go through distributed shared
+    // memory.  NUMI_CLOTH_RESIDENT=0 keeps them in global memory.  The
+    // cluster form is off by default: 16 CTAs leave too few threads to hide
+    // the latency of a 65,536-particle cloth's colour batches, and it
+    // measured slower than the cooperative grid.
+    uint32_t want_resident = 1;
+    env_u32("NUMI_CLOTH_RESIDENT", want_resident);
+    const uint32_t resident_limit = want_resident >= 2u ? 16u * kResidentChunk : kResidentChunk;
+    if (want_resident != 0u && forced == 0 && n > 0u && n <= resident_limit) {
+        uint32_t shift = 4u;
+        while ((1u << shift) < std::min(n, kResidentChunk)) ++shift;
+        const uint32_t ranks = (n + (1u << shift) - 1u) >> shift;
+        const size_t smem = nc_resident_offset() + 2u * (static_cast<size_t>(1u) << shift) * sizeof(float4);
+        int max_optin = 0;
+        cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
+        cudaFuncAttributes fa{};
+        cudaFuncGetAttributes(&fa, numi_cloth_frame_kernel);
+        bool ok = smem + fa.sharedSizeBytes <= static_cast<size_t>(max_optin) &&
+                  raise_frame_smem(smem) == cudaSuccess;
+        if (ok && ranks > 1u) {
+            cudaFuncSetAttribute(numi_cloth_frame_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+            cudaLaunchConfig_t cfg{};
+            cfg.gridDim = dim3(ranks);
+            cfg.blockDim = dim3(NC_BLOCK_MAX);
+            cfg.dynamicSmemBytes = smem;
+            cudaLaunchAttribute attr{};
+            attr.id = cudaLaunchAttributeClusterDimension;
+            attr.val.clusterDim.x = ranks;
+            attr.val.clusterDim.y = 1;
+            attr.val.clusterDim.z = 1;
+            cfg.attrs = &attr;
+            cfg.numAttrs = 1;
+            int clusters = 0;
+            ok = cudaOccupancyMaxActiveClusters(&clusters, numi_cloth_frame_kernel, &cfg) == cudaSuccess &&
+                 clusters >= 1;
+        }
+        cudaGetLastError();
+        if (ok) {
+            d.resident = 1u;
+            d.resident_shift = shift;
+            h->smem = smem;
+            h->grid = ranks;
+            if (ranks > 1u) {
+                h->cluster = ranks;
+                h->block = NC_BLOCK_MAX;
+            }
+            want_cluster = 0;
+        }
+    }
     if (h->grid > 1 && want_cluster > 0 && forced == 0) {
         cudaFuncSetAttribute(numi_cloth_frame_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
         for (uint32_t c : {want_cluster, 8u}) {
@@ -714,7 +780,7 @@ int numi_cloth_trace_cta(numi_cloth_t* h, unsigned long long* out, uint32_t subs
     return NUMI_CLOTH_OK;
 }
 
-int numi_cloth_launch_info(numi_cloth_t* h, uint32_t out[4]) {
+int numi_cloth_launch_info(numi_cloth_t* h, uint32_t out[6]) {
     if (h == nullptr || out == nullptr) return NUMI_CLOTH_EINVAL;
     cudaSetDevice(h->device);
     uint32_t stats[4] = {0, 0, 0, 0};
@@ -725,6 +791,8 @@ int numi_cloth_launch_info(numi_cloth_t* h, uint32_t out[4]) {
     out[1] = h->block;
     out[2] = stats[0];
     out[3] = h->launches;
+    out[4] = h->cluster;
+    out[5] = h->d.resident;
     return NUMI_CLOTH_OK;
 }
 
@@ -891,8 +959,7 @@ extern "C" int numi_cloth_step_noalloc(const NumiClothConfig* base, const NumiCl
     s.damping = schedule->damping;
     s.substeps = count;
     void* args[] = {&d, &s};
-    e = cudaFuncSetAttribute(numi_cloth_frame_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(sizeof(FruitShared)));
+    e = raise_frame_smem(sizeof(FruitShared));
     if (e == cudaSuccess)
         e = cudaLaunchKernel(reinterpret_cast<const void*>(numi_cloth_frame_kernel), dim3(1), dim3(NC_THREADS), args,
                              sizeof(FruitShared), stream);

@@ -100,6 +100,11 @@ struct DeviceCloth {
     // 1: the grid is one thread-block cluster and phases are separated by
     // the hardware cluster barrier instead of the global-memory barrier
     uint32_t cluster_barrier;
+    // resident mode: 1 when particle positions and velocities live in the
+    // (distributed) shared memory of the grid's CTAs for the whole launch;
+    // CTA r owns particles [r << resident_shift, (r + 1) << resident_shift)
+    uint32_t resident;
+    uint32_t resident_shift;
     double* red;          // [blocks * 8] reduction partials
     uint32_t* stats;      // [0] barriers of the last substep, [1] reconcile passes max, [2] certificate passes max
     uint32_t epoch_base;  // substep counter of the handle at launch

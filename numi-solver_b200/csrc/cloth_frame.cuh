@@ -7,22 +7,6 @@
 
 namespace nc {
 
-struct Ctx {
-    const DeviceCloth& d;
-    const Schedule& s;
-    SubCfg c;
-    uint32_t tid;
-    uint32_t nthreads;
-    bool fruit_cta;
-    bool grip_cta;
-    uint32_t barriers;
-    bool fruit_pending;   // fixed-point fruit sums waiting to be applied
-    uint32_t epoch;
-    uint32_t sub;
-    unsigned long long seq;   // barriers passed in this launch
-    FruitShared* fs;          // fruit-CTA shared state (valid in the fruit CTA)
-};
-
 // Grid-wide barrier with a bounded wait.  Arrival is a release-add of 1 to
 // a counter the host zeroes before each launch; barrier number s of the
 // launch completes when an acquire load sees s * gridDim.x.  A CTA that waits past the limit
@@ -123,7 +107,7 @@ __device__ void phase_begin(Ctx& ctx) {
     const DeviceCloth& d = ctx.d;
     const SubCfg& c = ctx.c;
     if (ctx.grip_cta) {
-        grip_attach(d, c);
+        grip_attach(ctx);
         __syncthreads();
         for (uint32_t g = threadIdx.x; g < d.g_count; g += blockDim.x) {
             d.grips[g].lambda.x = 0.0f;
@@ -135,10 +119,11 @@ __device__ void phase_begin(Ctx& ctx) {
     const float inv_dt = 1.0f / dt;
     const bool air = ctx.s.aerodynamics != 0u;
     const float damp = ctx.s.damping;
-    for (uint32_t i = ctx.tid; i < d.n; i += ctx.nthreads) {
-        float4 p = ld(d.x + i);
+    for (Range r = particle_range(ctx); r.i < r.end; r.i += r.stride) {
+        const uint32_t i = r.i;
+        float4 p = px(ctx, i);
         const float4 pp = ld(d.xp + i);
-        float4 vv = ld(d.v + i);
+        float4 vv = pv(ctx, i);
         V3 pos = xyz(p);
         const V3 prev = pos;
         V3 vel = xyz(vv);
@@ -154,8 +139,8 @@ __device__ void phase_begin(Ctx& ctx) {
         }
         if (!air && ctx.s.swept_ground && c.ground && prev.z >= c.radius && pos.z < c.radius) pos.z = c.radius;
         d.xp[i] = make_float4(prev.x, prev.y, prev.z, pp.w);
-        d.x[i] = with_xyz(p, pos);
-        d.v[i] = make_float4(vel.x, vel.y, vel.z, vel.z);
+        px_set(ctx, i, with_xyz(p, pos));
+        pv_set(ctx, i, make_float4(vel.x, vel.y, vel.z, vel.z));
     }
     for (uint32_t k = ctx.tid; k < d.d_count; k += ctx.nthreads) d.d_lambda[k] = 0.0f;
     for (uint32_t k = ctx.tid; k < d.k_count; k += ctx.nthreads) d.k_lambda[k] = 0.0f;
@@ -187,16 +172,16 @@ __device__ void air_force_batch(Ctx& ctx, const Batch& bt, float4* force) {
     const DeviceCloth& d = ctx.d;
     const SubCfg& c = ctx.c;
     const float pi = 3.14159265358979323846f;
-    for (uint32_t k = ctx.tid; k < bt.yarn; k += ctx.nthreads) {
-        const uint32_t s = bt.first + k;
+    for (Range r = item_range(ctx, bt.yarn); r.i < r.end; r.i += r.stride) {
+        const uint32_t s = bt.first + r.i;
         const uint2 ij = __ldg(d.d_ij + s);
-        const V3 a = xyz(ld(d.x + ij.x));
-        const V3 b = xyz(ld(d.x + ij.y));
+        const V3 a = xyz(px(ctx, ij.x));
+        const V3 b = xyz(px(ctx, ij.y));
         const V3 span = b - a;
         const float L = len3(span);
         if (L < 1.0e-12f) continue;
         const V3 axis = vdiv(span, L);
-        const V3 rel = (xyz(ld(d.v + ij.x)) + xyz(ld(d.v + ij.y))) * 0.5f - c.air;
+        const V3 rel = (xyz(pv(ctx, ij.x)) + xyz(pv(ctx, ij.y))) * 0.5f - c.air;
         const V3 axial = axis * dot3(rel, axis);
         const V3 cross_v = rel - axial;
         const float cross_area = 2.0f * c.radius * L;
@@ -234,10 +219,10 @@ __device__ void air_reduce_chunks(Ctx& ctx, const float4* force) {
         const uint32_t i = ch * NC_THREADS + t;
         double pw = 0.0, q = 0.0;
         if (ch < chunks && i < d.n) {
-            const float4 p = ld(d.x + i);
+            const float4 p = px(ctx, i);
             if (p.w > 0.0f) {
                 const V3 f = xyz(ld(force + i));
-                const V3 rv = xyz(ld(d.v + i)) - ctx.c.air;
+                const V3 rv = xyz(pv(ctx, i)) - ctx.c.air;
                 pw = static_cast<double>(f.x) * rv.x + static_cast<double>(f.y) * rv.y +
                      static_cast<double>(f.z) * rv.z;
                 q = static_cast<double>(p.w) * (static_cast<double>(f.x) * f.x +
@@ -299,18 +284,19 @@ __device__ void air_apply_advance(Ctx& ctx, const float4* force, float att) {
     const DeviceCloth& d = ctx.d;
     const SubCfg& c = ctx.c;
     const float dt = c.dt;
-    for (uint32_t i = ctx.tid; i < d.n; i += ctx.nthreads) {
-        float4 p = ld(d.x + i);
+    for (Range r = particle_range(ctx); r.i < r.end; r.i += r.stride) {
+        const uint32_t i = r.i;
+        float4 p = px(ctx, i);
         const V3 prev = xyz(ld(d.xp + i));
-        V3 vel = xyz(ld(d.v + i));
+        V3 vel = xyz(pv(ctx, i));
         V3 pos = xyz(p);
         if (p.w > 0.0f) {
             vel = vel + xyz(ld(force + i)) * (att * p.w * dt);
             pos = pos + vel * dt;
         }
         if (ctx.s.swept_ground && c.ground && prev.z >= c.radius && pos.z < c.radius) pos.z = c.radius;
-        d.x[i] = with_xyz(p, pos);
-        d.v[i] = make_float4(vel.x, vel.y, vel.z, vel.z);
+        px_set(ctx, i, with_xyz(p, pos));
+        pv_set(ctx, i, make_float4(vel.x, vel.y, vel.z, vel.z));
     }
 }
 
@@ -339,17 +325,18 @@ __device__ void yarn_contact_batch(Ctx& ctx, const Batch& bt) {
     unsigned long long* acc = reinterpret_cast<unsigned long long*>(d.fruit_partial);
     const uint32_t nf = d.f_count;
     const uint32_t lane = threadIdx.x & 31u;
-    for (uint32_t base = ctx.tid - lane; base < bt.yarn; base += ctx.nthreads) {
+    const Range rg = item_range(ctx, bt.yarn);
+    for (uint32_t base = rg.i - lane; base < rg.end; base += rg.stride) {
         const uint32_t k = base + lane;
-        const bool valid = k < bt.yarn;
+        const bool valid = k < rg.end;
         const uint32_t seg = bt.first + (valid ? k : 0u);
         uint2 ij = make_uint2(0u, 0u);
         float4 pa = make_float4(0, 0, 0, 0), pb = pa;
         V3 lo{INFINITY, INFINITY, INFINITY}, hi{-INFINITY, -INFINITY, -INFINITY};
         if (valid) {
             ij = __ldg(d.d_ij + seg);
-            pa = ld(d.x + ij.x);
-            pb = ld(d.x + ij.y);
+            pa = px(ctx, ij.x);
+            pb = px(ctx, ij.y);
             lo = V3{fminf(pa.x, pb.x), fminf(pa.y, pb.y), fminf(pa.z, pb.z)};
             hi = V3{fmaxf(pa.x, pb.x), fmaxf(pa.y, pb.y), fmaxf(pa.z, pb.z)};
         }
@@ -462,8 +449,8 @@ __device__ void yarn_contact_batch(Ctx& ctx, const Batch& bt) {
             d.yarn_live[seg] = ctx.epoch;
         }
         if (changed) {
-            d.x[ij.x] = pa;
-            d.x[ij.y] = pb;
+            px_set(ctx, ij.x, pa);
+            px_set(ctx, ij.y, pb);
         }
     }
 }
@@ -487,9 +474,9 @@ __device__ void phase_ground(Ctx& ctx) {
     const SubCfg& c = ctx.c;
     fruit_flush(ctx);
     if (!c.ground) return;
-    for (uint32_t i = ctx.tid; i < d.n; i += ctx.nthreads) {
-        const float4 p = ld(d.x + i);
-        if (c.radius - p.z > 0.0f) d.x[i] = make_float4(p.x, p.y, c.radius, p.w);
+    for (Range r = particle_range(ctx); r.i < r.end; r.i += r.stride) {
+        const float4 p = px(ctx, r.i);
+        if (c.radius - p.z > 0.0f) px_set(ctx, r.i, make_float4(p.x, p.y, c.radius, p.w));
     }
     if (ctx.fruit_cta) {
         for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
@@ -510,7 +497,7 @@ __device__ bool strain_sweeps(Ctx& ctx) {
             const Batch bt = ctx.d.dist_batches[b];
             if (bt.limited == 0u) continue;
             fruit_flush(ctx);
-            for (uint32_t k = ctx.tid; k < bt.limited; k += ctx.nthreads) limit_strain(ctx.d, bt.first + k);
+            for (Range r = item_range(ctx, bt.limited); r.i < r.end; r.i += r.stride) limit_strain(ctx, bt.first + r.i);
             NC_SYNC(ctx);
         }
     }
@@ -523,12 +510,13 @@ __device__ void residual_partials(Ctx& ctx, double* out3) {
     const DeviceCloth& d = ctx.d;
     const SubCfg& c = ctx.c;
     double strain = 0.0, ground = 0.0, fruit = 0.0;
-    for (uint32_t k = ctx.tid; k < d.d_count; k += ctx.nthreads) {
+    for (Range r = item_range(ctx, d.d_count); r.i < r.end; r.i += r.stride) {
+        const uint32_t k = r.i;
         const float4 m = __ldg(d.d_mat + k);
         if (!(m.w > 0.0f)) continue;
         const uint2 ij = __ldg(d.d_ij + k);
-        const float4 a = ld(d.x + ij.x);
-        const float4 b = ld(d.x + ij.y);
+        const float4 a = px(ctx, ij.x);
+        const float4 b = px(ctx, ij.y);
         const double dx = static_cast<double>(b.x) - a.x, dy = static_cast<double>(b.y) - a.y,
                      dz = static_cast<double>(b.z) - a.z;
         const double L = sqrt((dx * dx + dy * dy) + dz * dz);
@@ -536,8 +524,8 @@ __device__ void residual_partials(Ctx& ctx, double* out3) {
         strain = fmax(strain, L - maxL);
     }
     if (c.ground) {
-        for (uint32_t i = ctx.tid; i < d.n; i += ctx.nthreads)
-            ground = fmax(ground, static_cast<double>(c.radius) - static_cast<double>(ld(d.x + i).z));
+        for (Range r = particle_range(ctx); r.i < r.end; r.i += r.stride)
+            ground = fmax(ground, static_cast<double>(c.radius) - static_cast<double>(px(ctx, r.i).z));
         if (blockIdx.x == 0)
             for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x)
                 ground = fmax(ground, static_cast<double>(__ldcg(&d.fruits[f].previousAndRadius.w)) -
@@ -546,10 +534,10 @@ __device__ void residual_partials(Ctx& ctx, double* out3) {
     if (d.f_count > 0u) {
         for (uint32_t b = 0; b < d.n_dist_batches; ++b) {
             const Batch bt = d.dist_batches[b];
-            for (uint32_t k = ctx.tid; k < bt.yarn; k += ctx.nthreads) {
-                const uint2 ij = __ldg(d.d_ij + bt.first + k);
-                const float4 pa = ld(d.x + ij.x);
-                const float4 pb = ld(d.x + ij.y);
+            for (Range r = item_range(ctx, bt.yarn); r.i < r.end; r.i += r.stride) {
+                const uint2 ij = __ldg(d.d_ij + bt.first + r.i);
+                const float4 pa = px(ctx, ij.x);
+                const float4 pb = px(ctx, ij.y);
                 for (uint32_t f = 0; f < d.f_count; ++f) {
                     const NumiClothFruit& fr = d.fruits[f];
                     const double X[3] = {__ldcg(&fr.positionAndInverseMass.x), __ldcg(&fr.positionAndInverseMass.y),
@@ -628,17 +616,18 @@ __device__ void phase_finalize(Ctx& ctx) {
     const SubCfg& c = ctx.c;
     fruit_flush(ctx);
     const float inv_dt = 1.0f / c.dt;
-    for (uint32_t i = ctx.tid; i < d.n; i += ctx.nthreads) {
-        float4 p = ld(d.x + i);
+    for (Range r = particle_range(ctx); r.i < r.end; r.i += r.stride) {
+        const uint32_t i = r.i;
+        float4 p = px(ctx, i);
         const V3 prev = xyz(ld(d.xp + i));
-        const float4 vv = ld(d.v + i);
+        const float4 vv = pv(ctx, i);
         V3 pos = xyz(p);
         V3 vel;
         float gi = 0.0f;
         if (p.w == 0.0f) {
             pos = xyz(__ldg(d.rest + i));
             vel = (pos - prev) * inv_dt;
-            d.x[i] = with_xyz(p, pos);
+            px_set(ctx, i, with_xyz(p, pos));
         } else {
             vel = (pos - prev) * inv_dt;
             if (c.ground && pos.z <= c.radius + 1.0e-6f) {
@@ -656,7 +645,7 @@ __device__ void phase_finalize(Ctx& ctx) {
             }
         }
         if (!finite3(vel)) fail(d, NUMI_CLOTH_FAILURE_NONFINITE);
-        d.v[i] = make_float4(vel.x, vel.y, vel.z, gi);
+        pv_set(ctx, i, make_float4(vel.x, vel.y, vel.z, gi));
     }
     if (ctx.fruit_cta) {
         for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
@@ -674,14 +663,14 @@ __device__ void yarn_friction_batch(Ctx& ctx, const Batch& bt) {
     const DeviceCloth& d = ctx.d;
     const SubCfg& c = ctx.c;
     unsigned long long* acc = reinterpret_cast<unsigned long long*>(d.fruit_partial) + 3u * NC_MAX_FRUITS;
-    for (uint32_t k = ctx.tid; k < bt.yarn; k += ctx.nthreads) {
-        const uint32_t seg = bt.first + k;
+    for (Range r = item_range(ctx, bt.yarn); r.i < r.end; r.i += r.stride) {
+        const uint32_t seg = bt.first + r.i;
         if (__ldcg(d.yarn_live + seg) != ctx.epoch) continue;
         const uint2 ij = __ldg(d.d_ij + seg);
-        const float4 pa = ld(d.x + ij.x);
-        const float4 pb = ld(d.x + ij.y);
-        float4 va = ld(d.v + ij.x);
-        float4 vb = ld(d.v + ij.y);
+        const float4 pa = px(ctx, ij.x);
+        const float4 pb = px(ctx, ij.y);
+        float4 va = pv(ctx, ij.x);
+        float4 vb = pv(ctx, ij.y);
         // Live records of this segment, visited in ascending fruit order.
         const uint32_t live = ctx.epoch & 0x3ffffffu;
         uint32_t fruit_of[NC_YARN_SLOTS];
@@ -747,8 +736,8 @@ __device__ void yarn_friction_batch(Ctx& ctx, const Batch& bt) {
             va = with_xyz(va, na);
             vb = with_xyz(vb, nb);
         }
-        d.v[ij.x] = va;
-        d.v[ij.y] = vb;
+        pv_set(ctx, ij.x, va);
+        pv_set(ctx, ij.y, vb);
     }
 }
 
@@ -824,24 +813,24 @@ __device__ bool substep(Ctx& ctx, bool last) {
         for (uint32_t b = 0; b < d.n_dist_batches; ++b) {
             const Batch bt = d.dist_batches[b];
             fruit_flush(ctx);
-            for (uint32_t k = ctx.tid; k < bt.count; k += ctx.nthreads) solve_distance(d, bt.first + k, dt2);
+            for (Range r = item_range(ctx, bt.count); r.i < r.end; r.i += r.stride) solve_distance(ctx, bt.first + r.i, dt2);
             NC_SYNC(ctx);
         }
         for (uint32_t b = 0; b < d.n_knot_batches; ++b) {
             const Batch bt = d.knot_batches[b];
-            for (uint32_t k = ctx.tid; k < bt.count; k += ctx.nthreads) solve_knot(d, bt.first + k, dt2);
+            for (Range r = item_range(ctx, bt.count); r.i < r.end; r.i += r.stride) solve_knot(ctx, bt.first + r.i, dt2);
             NC_SYNC(ctx);
         }
         if ((it & 1u) == 0u) {
             for (uint32_t b = 0; b < d.n_bend_batches; ++b) {
                 const Batch bt = d.bend_batches[b];
-                for (uint32_t k = ctx.tid; k < bt.count; k += ctx.nthreads)
-                    solve_bend(d, bt.first + k, dt2, ctx.c.radius, ctx.c.ground);
+                for (Range r = item_range(ctx, bt.count); r.i < r.end; r.i += r.stride)
+                    solve_bend(ctx, bt.first + r.i, dt2, ctx.c.radius, ctx.c.ground);
                 NC_SYNC(ctx);
             }
         }
         // grips (CTA 0) and fruit pairs (fruit CTA) touch disjoint state
-        if (ctx.grip_cta) solve_grips(d, ctx.c);
+        if (ctx.grip_cta) solve_grips(ctx);
         if (ctx.fruit_cta && d.p_count > 0u) {
             __syncthreads();
             fruit_pair_sweep(d, *ctx.fs, ctx.c.dt);
@@ -903,23 +892,46 @@ __device__ bool substep(Ctx& ctx, bool last) {
 
 }  // namespace nc
 
+// Byte offset of the resident particle arrays in dynamic shared memory.
+__host__ __device__ constexpr size_t nc_resident_offset() { return (sizeof(FruitShared) + 255u) & ~size_t(255u); }
+
 __global__ void __launch_bounds__(NC_BLOCK_MAX) numi_cloth_frame_kernel(DeviceCloth d, Schedule s) {
     extern __shared__ __align__(16) unsigned char nc_dynamic_smem[];
     FruitShared& fruit_shared = *reinterpret_cast<FruitShared*>(nc_dynamic_smem);
     nc::Ctx ctx{d, s};
     ctx.fs = &fruit_shared;
-    if (blockIdx.x == gridDim.x - 1u) {
-        for (uint32_t k = threadIdx.x; k < d.p_count; k += blockDim.x)
-            fruit_shared.ab[k] =
-                static_cast<unsigned short>(d.pairs[k].fruitsAndColor.x | (d.pairs[k].fruitsAndColor.y << 8));
-        __syncthreads();
-    }
     ctx.tid = blockIdx.x * blockDim.x + threadIdx.x;
     ctx.nthreads = gridDim.x * blockDim.x;
     ctx.fruit_cta = blockIdx.x == gridDim.x - 1u;
     ctx.grip_cta = blockIdx.x == 0u;
     ctx.fruit_pending = false;
     ctx.seq = 0;
+    ctx.resident = d.resident != 0u;
+    ctx.rank = blockIdx.x;
+    ctx.ranks = gridDim.x;
+    ctx.shift = d.resident_shift;
+    uint32_t own_first = 0, own_end = 0;
+    if (ctx.resident) {
+        // Stage this CTA's particles into shared memory for the whole launch.
+        ctx.xs = reinterpret_cast<float4*>(nc_dynamic_smem + nc_resident_offset());
+        ctx.vs = ctx.xs + (1u << ctx.shift);
+        own_first = ctx.rank << ctx.shift;
+        own_end = min(own_first + (1u << ctx.shift), d.n);
+        for (uint32_t i = own_first + threadIdx.x; i < own_end; i += blockDim.x) {
+            ctx.xs[i - own_first] = __ldcg(d.x + i);
+            ctx.vs[i - own_first] = __ldcg(d.v + i);
+        }
+        if (gridDim.x > 1u)
+            cooperative_groups::this_cluster().sync();
+        else
+            __syncthreads();
+    }
+    if (blockIdx.x == gridDim.x - 1u) {
+        for (uint32_t k = threadIdx.x; k < d.p_count; k += blockDim.x)
+            fruit_shared.ab[k] =
+                static_cast<unsigned short>(d.pairs[k].fruitsAndColor.x | (d.pairs[k].fruitsAndColor.y << 8));
+        __syncthreads();
+    }
     for (uint32_t sub = 0; sub < s.substeps; ++sub) {
         ctx.sub = sub;
         ctx.c = nc::load_cfg(d.cfg + sub);
@@ -927,5 +939,13 @@ __global__ void __launch_bounds__(NC_BLOCK_MAX) numi_cloth_frame_kernel(DeviceCl
         ctx.barriers = 0;
         if (!nc::substep(ctx, sub + 1u == s.substeps)) return;
         if (blockIdx.x == 0 && threadIdx.x == 0) d.stats[0] = ctx.barriers;
+    }
+    if (ctx.resident) {
+        // Every remote access ended at the last barrier: write the CTA's own
+        // particles back.
+        for (uint32_t i = own_first + threadIdx.x; i < own_end; i += blockDim.x) {
+            d.x[i] = ctx.xs[i - own_first];
+            d.v[i] = ctx.vs[i - own_first];
+        }
     }
 }

@@ -119,10 +119,87 @@ __device__ __forceinline__ float inverse_inertia(float w, float radius) {
     return 2.5f * w / (radius * radius);
 }
 
+// Per-thread view of a launch.  In resident mode (one thread-block cluster,
+// particles kept in distributed shared memory for the whole launch) particle
+// i lives in the shared memory of cluster rank i >> shift at offset
+// i & (chunk - 1); otherwise it lives in global memory.
+struct Ctx {
+    const DeviceCloth& d;
+    const Schedule& s;
+    SubCfg c;
+    uint32_t tid;
+    uint32_t nthreads;
+    bool fruit_cta;
+    bool grip_cta;
+    uint32_t barriers;
+    bool fruit_pending;       // fixed-point fruit sums waiting to be applied
+    uint32_t epoch;
+    uint32_t sub;
+    unsigned long long seq;   // barriers passed in this launch
+    FruitShared* fs;          // fruit-CTA shared state (valid in the fruit CTA)
+    bool resident;
+    uint32_t rank;            // cluster rank (resident) or 0
+    uint32_t ranks;           // CTAs that own particles (resident) or 1
+    uint32_t shift;           // log2 of the particles each CTA owns
+    float4* xs;               // this CTA's positions in shared memory
+    float4* vs;               // this CTA's velocities in shared memory
+};
+
+__device__ __forceinline__ float4* resident_ptr(const Ctx& c, float4* local_base, uint32_t i) {
+    const uint32_t r = i >> c.shift;
+    float4* p = local_base + (i & ((1u << c.shift) - 1u));
+    return r == c.rank ? p : static_cast<float4*>(__cluster_map_shared_rank(p, r));
+}
+// Particle position (xyz, inverse mass) and velocity accessors.
+__device__ __forceinline__ float4 px(const Ctx& c, uint32_t i) {
+    return c.resident ? *resident_ptr(c, c.xs, i) : __ldcg(c.d.x + i);
+}
+__device__ __forceinline__ void px_set(const Ctx& c, uint32_t i, float4 v) {
+    if (c.resident)
+        *resident_ptr(c, c.xs, i) = v;
+    else
+        c.d.x[i] = v;
+}
+__device__ __forceinline__ float4 pv(const Ctx& c, uint32_t i) {
+    return c.resident ? *resident_ptr(c, c.vs, i) : __ldcg(c.d.v + i);
+}
+__device__ __forceinline__ void pv_set(const Ctx& c, uint32_t i, float4 v) {
+    if (c.resident)
+        *resident_ptr(c, c.vs, i) = v;
+    else
+        c.d.v[i] = v;
+}
+
+// Loop range of this thread over count items: grid-stride in the global
+// modes; in resident mode each CTA takes one contiguous slice (constraint
+// arrays follow particle order, so a slice touches mostly its own particles).
+struct Range {
+    uint32_t i, end, stride;
+};
+__device__ __forceinline__ Range item_range(const Ctx& c, uint32_t count) {
+    if (c.resident) {
+        const uint32_t lo = static_cast<uint32_t>(static_cast<unsigned long long>(count) * c.rank / c.ranks);
+        const uint32_t hi = static_cast<uint32_t>(static_cast<unsigned long long>(count) * (c.rank + 1u) / c.ranks);
+        return Range{lo + threadIdx.x, hi, blockDim.x};
+    }
+    return Range{c.tid, count, c.nthreads};
+}
+// Particles: resident mode walks the CTA's own particles.
+__device__ __forceinline__ Range particle_range(const Ctx& c) {
+    if (c.resident) {
+        const uint32_t first = c.rank << c.shift;
+        const uint32_t end = min(first + (1u << c.shift), c.d.n);
+        return Range{first + threadIdx.x, end, blockDim.x};
+    }
+    return Range{c.tid, c.d.n, c.nthreads};
+}
+
 // ---------------------------------------------------------------- grip ----
 // Re-attachment on a generation change (tools/cloth_bag.cpp:1520-1611;
 // ClothBag.metal:577-673).  Block 0, one thread per grip.
-__device__ void grip_attach(const DeviceCloth& d, const SubCfg& c) {
+__device__ void grip_attach(const Ctx& ctx) {
+    const DeviceCloth& d = ctx.d;
+    const SubCfg& c = ctx.c;
     const uint32_t g = threadIdx.x;
     if (g >= d.g_count || !c.grip_active) return;
     NumiClothGrip grip = d.grips[g];
@@ -137,7 +214,7 @@ __device__ void grip_attach(const DeviceCloth& d, const SubCfg& c) {
         float nearest = INFINITY;
         for (uint32_t ring = 0u; ring < c.ring_count; ++ring) {
             const uint32_t cand = d.cuff[c.ring_count + ring];
-            const V3 sep = xyz(ld(d.x + cand)) - c.grip_target;
+            const V3 sep = xyz(px(ctx, cand)) - c.grip_target;
             const float dsq = lsq(sep);
             if (dsq < nearest) {
                 nearest = dsq;
@@ -152,7 +229,7 @@ __device__ void grip_attach(const DeviceCloth& d, const SubCfg& c) {
         grip.particle.x = particle;
         grip.particle.w = center;
     }
-    const V3 position = xyz(ld(d.x + particle));
+    const V3 position = xyz(px(ctx, particle));
     const V3 sep = position - c.grip_target;
     const float capture = len3(sep);
     if (!finite3(position) || !isfinite(capture)) {
@@ -179,13 +256,15 @@ __device__ void grip_attach(const DeviceCloth& d, const SubCfg& c) {
 }
 
 // Compliant vector attachment (tools/cloth_bag.cpp:1630-1647).
-__device__ void solve_grips(const DeviceCloth& d, const SubCfg& c) {
+__device__ void solve_grips(const Ctx& ctx) {
+    const DeviceCloth& d = ctx.d;
+    const SubCfg& c = ctx.c;
     const uint32_t g = threadIdx.x;
     if (g >= d.g_count || !c.grip_active) return;
     NumiClothGrip grip = d.grips[g];
     if (grip.particle.y != c.grip_gen) return;
     const uint32_t i = grip.particle.x;
-    float4 p = ld(d.x + i);
+    float4 p = px(ctx, i);
     const float alpha = grip.targetOffsetAndCompliance.w / (c.dt * c.dt);
     const float den = p.w + alpha;
     if (den <= 0.0f) return;
@@ -198,7 +277,7 @@ __device__ void solve_grips(const DeviceCloth& d, const SubCfg& c) {
     const V3 nl = lambda + dl;
     const V3 np = xyz(p) + dl * p.w;
     if (!finite3(np)) fail(d, NUMI_CLOTH_FAILURE_NONFINITE);
-    d.x[i] = with_xyz(p, np);
+    px_set(ctx, i, with_xyz(p, np));
     grip.lambda.x = nl.x;
     grip.lambda.y = nl.y;
     grip.lambda.z = nl.z;
@@ -207,11 +286,12 @@ __device__ void solve_grips(const DeviceCloth& d, const SubCfg& c) {
 
 // ---------------------------------------------------------- constraints ---
 // XPBD distance (tools/cloth_bag.cpp:1649-1673).
-__device__ __forceinline__ void solve_distance(const DeviceCloth& d, uint32_t k, float dt2) {
+__device__ __forceinline__ void solve_distance(const Ctx& ctx, uint32_t k, float dt2) {
+    const DeviceCloth& d = ctx.d;
     const uint2 ij = __ldg(d.d_ij + k);
     const float4 m = __ldg(d.d_mat + k);
-    float4 a = ld(d.x + ij.x);
-    float4 b = ld(d.x + ij.y);
+    float4 a = px(ctx, ij.x);
+    float4 b = px(ctx, ij.y);
     const V3 diff = xyz(b) - xyz(a);
     const float L = len3(diff);
     if (L < 1.0e-12f) return;
@@ -224,19 +304,20 @@ __device__ __forceinline__ void solve_distance(const DeviceCloth& d, uint32_t k,
     const V3 corr = diff * (dl / L);
     const V3 na = xyz(a) - corr * a.w;
     const V3 nb = xyz(b) + corr * b.w;
-    d.x[ij.x] = with_xyz(a, na);
-    d.x[ij.y] = with_xyz(b, nb);
+    px_set(ctx, ij.x, with_xyz(a, na));
+    px_set(ctx, ij.y, with_xyz(b, nb));
     d.d_lambda[k] = lam + dl;
 }
 
 // Crossing-angle knot (tools/cloth_bag.cpp:1675-1725).
-__device__ __forceinline__ void solve_knot(const DeviceCloth& d, uint32_t k, float dt2) {
+__device__ __forceinline__ void solve_knot(const Ctx& ctx, uint32_t k, float dt2) {
+    const DeviceCloth& d = ctx.d;
     const uint4 q = __ldg(d.k_ij + k);
     const float2 m = __ldg(d.k_mat + k);
-    const float4 p0 = ld(d.x + q.x);
-    const float4 p1 = ld(d.x + q.y);
-    const float4 p2 = ld(d.x + q.z);
-    const float4 p3 = ld(d.x + q.w);
+    const float4 p0 = px(ctx, q.x);
+    const float4 p1 = px(ctx, q.y);
+    const float4 p2 = px(ctx, q.z);
+    const float4 p3 = px(ctx, q.w);
     const V3 warpv = xyz(p1) - xyz(p0);
     const V3 weftv = xyz(p3) - xyz(p2);
     const float wl = len3(warpv);
@@ -260,19 +341,19 @@ __device__ __forceinline__ void solve_knot(const DeviceCloth& d, uint32_t k, flo
     const float lam = ldf(d.k_lambda + k);
     const float dl = (-value - alpha * lam) / den;
     d.k_lambda[k] = lam + dl;
-    d.x[q.x] = with_xyz(p0, xyz(p0) + g0 * (p0.w * dl));
-    d.x[q.y] = with_xyz(p1, xyz(p1) + gw * (p1.w * dl));
-    d.x[q.z] = with_xyz(p2, xyz(p2) + g2 * (p2.w * dl));
-    d.x[q.w] = with_xyz(p3, xyz(p3) + gf * (p3.w * dl));
+    px_set(ctx, q.x, with_xyz(p0, xyz(p0) + g0 * (p0.w * dl)));
+    px_set(ctx, q.y, with_xyz(p1, xyz(p1) + gw * (p1.w * dl)));
+    px_set(ctx, q.z, with_xyz(p2, xyz(p2) + g2 * (p2.w * dl)));
+    px_set(ctx, q.w, with_xyz(p3, xyz(p3) + gf * (p3.w * dl)));
 }
 
 // Skip-one chord bend with the ground active set (tools/cloth_bag.cpp:1782-1863).
-__device__ __forceinline__ void solve_bend(const DeviceCloth& d, uint32_t k, float dt2,
-                                           float radius, bool ground) {
+__device__ __forceinline__ void solve_bend(const Ctx& ctx, uint32_t k, float dt2, float radius, bool ground) {
+    const DeviceCloth& d = ctx.d;
     const uint4 q = __ldg(d.b_ij + k);
     const float2 m = __ldg(d.b_mat + k);
     const uint32_t idx[2] = {q.x, q.z};
-    float4 p[2] = {ld(d.x + q.x), ld(d.x + q.z)};
+    float4 p[2] = {px(ctx, q.x), px(ctx, q.z)};
     const V3 diff = xyz(p[1]) - xyz(p[0]);
     const float chord = len3(diff);
     if (chord < 1.0e-12f) return;
@@ -311,18 +392,19 @@ __device__ __forceinline__ void solve_bend(const DeviceCloth& d, uint32_t k, flo
         if (active[s]) corr.z = 0.0f;
         V3 np = xyz(p[s]) + corr;
         if (ground && np.z < radius) np.z = radius;
-        d.x[idx[s]] = with_xyz(p[s], np);
+        px_set(ctx, idx[s], with_xyz(p[s], np));
     }
 }
 
 // Unilateral strain limit (tools/cloth_bag.cpp:1732-1763); returns nothing,
 // the correction is not published.
-__device__ __forceinline__ void limit_strain(const DeviceCloth& d, uint32_t k) {
+__device__ __forceinline__ void limit_strain(const Ctx& ctx, uint32_t k) {
+    const DeviceCloth& d = ctx.d;
     const float4 m = __ldg(d.d_mat + k);
     if (!(m.w > 0.0f)) return;
     const uint2 ij = __ldg(d.d_ij + k);
-    float4 a = ld(d.x + ij.x);
-    float4 b = ld(d.x + ij.y);
+    float4 a = px(ctx, ij.x);
+    float4 b = px(ctx, ij.y);
     const V3 diff = xyz(b) - xyz(a);
     const float L = len3(diff);
     const float maxL = m.x * (1.0f + m.w);
@@ -331,8 +413,8 @@ __device__ __forceinline__ void limit_strain(const DeviceCloth& d, uint32_t k) {
     if (den <= 0.0f) return;
     const float cm = L - maxL;
     const V3 dir = vdiv(diff, L);
-    d.x[ij.x] = with_xyz(a, xyz(a) + dir * (a.w * cm / den));
-    d.x[ij.y] = with_xyz(b, xyz(b) - dir * (b.w * cm / den));
+    px_set(ctx, ij.x, with_xyz(a, xyz(a) + dir * (a.w * cm / den)));
+    px_set(ctx, ij.y, with_xyz(b, xyz(b) - dir * (b.w * cm / den)));
 }
 
 // ------------------------------------------------------------- fruits -----

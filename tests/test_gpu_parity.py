@@ -106,14 +106,34 @@ def test_cluster_equals_cooperative_grid():
     scene = small_square(side=96, fruits=16)
     cfg = nc.substep_configs(scene, 12)
     s = nc.Schedule.make(**FULL)
-    grid = run_gpu(scene, cfg, s, env={"NUMI_CLOTH_CLUSTER": "0"})
-    clus = run_gpu(scene, cfg, s, env={"NUMI_CLOTH_CLUSTER": "16"})
-    assert grid["info"]["grid"] > 16
-    assert clus["info"]["grid"] in (8, 16)
+    grid = run_gpu(scene, cfg, s, env={"NUMI_CLOTH_CLUSTER": "0", "NUMI_CLOTH_RESIDENT": "0"})
+    clus = run_gpu(scene, cfg, s, env={"NUMI_CLOTH_CLUSTER": "16", "NUMI_CLOTH_RESIDENT": "0"})
+    assert grid["info"]["grid"] > 16 and not grid["info"]["resident"]
+    assert clus["info"]["grid"] in (8, 16) and clus["info"]["cluster"] == clus["info"]["grid"]
     assert np.array_equal(grid["particles"], clus["particles"])
     assert np.array_equal(grid["fruits"], clus["fruits"])
     o = run_oracle(scene, cfg, s, bits=32)
     _check_bitexact(clus, o)
+
+
+@pytest.mark.parametrize("side,ranks", [(40, 1), (96, 3), (128, 4)])
+def test_resident_equals_global(side, ranks):
+    """Particles resident in the shared memory of one CTA or spread over a
+    cluster's distributed shared memory give the same bits as particles in
+    global memory, and as the oracle."""
+    scene = small_square(side=side, fruits=12)
+    cfg = nc.substep_configs(scene, 12)
+    s = nc.Schedule.make(**FULL)
+    res = run_gpu(scene, cfg, s, env={"NUMI_CLOTH_RESIDENT": "1" if ranks == 1 else "2"})
+    glob = run_gpu(scene, cfg, s, env={"NUMI_CLOTH_RESIDENT": "0"})
+    assert res["info"]["resident"] and res["info"]["grid"] == ranks
+    assert not glob["info"]["resident"]
+    assert res["failure"] == 0
+    assert np.array_equal(res["particles"], glob["particles"])
+    assert np.array_equal(res["fruits"], glob["fruits"])
+    assert np.array_equal(res["distances"], glob["distances"])
+    o = run_oracle(scene, cfg, s, bits=32)
+    _check_bitexact(res, o)
 
 
 def test_two_runs_bit_identical():
@@ -126,13 +146,16 @@ def test_two_runs_bit_identical():
     assert np.array_equal(a["fruits"], b["fruits"])
 
 
-def test_large_square_multi_cta_bitexact():
-    """65,536 particles, full cooperative grid, three substeps."""
+@pytest.mark.parametrize("resident", ["2", "0"], ids=["resident-cluster", "global-grid"])
+def test_large_square_multi_cta_bitexact(resident):
+    """65,536 particles, three substeps: a 16-CTA cluster holding the
+    particles in distributed shared memory, and the full cooperative grid."""
     scene = nc.square_scene()
     cfg = nc.substep_configs(scene, 3)
     s = nc.Schedule.make(**PLAIN)
-    g = run_gpu(scene, cfg, s)
+    g = run_gpu(scene, cfg, s, env={"NUMI_CLOTH_RESIDENT": resident})
     assert g["info"]["grid"] > 1
+    assert g["info"]["resident"] == (resident == "2")
     o = run_oracle(scene, cfg, s, bits=32)
     assert g["failure"] == 0
     _check_bitexact(g, o)
