@@ -365,9 +365,15 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
     int per_sm = 0;
     raise_frame_smem(sizeof(FruitShared));
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, numi_cloth_frame_kernel, NC_THREADS, sizeof(FruitShared));
+    // NUMI_CLOTH_BLOCK=512 runs the cooperative grid with 512-thread CTAs
+    // (one per SM) instead of 256 (two per SM).
+    uint32_t block = NC_THREADS;
+    if (env_u32("NUMI_CLOTH_BLOCK", block) && block != NC_BLOCK_MAX) block = NC_THREADS;
+    h->block = block;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, numi_cloth_frame_kernel, static_cast<int>(block),
+                                                  sizeof(FruitShared));
     uint32_t work = std::max({n, D, K, B});
-    uint32_t grid = (work <= 8192u) ? 1u : std::min<uint32_t>(sms * std::max(per_sm, 1), (work + NC_THREADS - 1u) / NC_THREADS);
+    uint32_t grid = (work <= 8192u) ? 1u : std::min<uint32_t>(sms * std::max(per_sm, 1), (work + block - 1u) / block);
     uint32_t forced = 0;
     if (env_u32("NUMI_CLOTH_GRID", forced) && forced > 0) grid = std::min<uint32_t>(forced, sms * std::max(per_sm, 1));
     h->grid = std::max(grid, 1u);

@@ -310,18 +310,58 @@ __device__ void air_apply_advance(Ctx& ctx, const float4* force, float att) {
 // subtraction is monotone, so a fruit outside the warp box also fails every
 // per-segment box test; once a contact moves a segment its thread tests all
 // remaining fruits again.  The result is identical to testing every fruit.
-__device__ void yarn_contact_batch(Ctx& ctx, const Batch& bt) {
+// CTA-level fixed-point fruit sums.  Integer addition is exact and
+// associative, so adding a CTA's contributions in shared memory first and
+// then its total once to the global sum gives the same bits as one global
+// atomic per contribution, without hundreds of segments queueing on the
+// same few addresses when a fruit rests on the cloth.
+__device__ __forceinline__ void cta_sums_clear(unsigned long long* s, uint32_t count) {
+    for (uint32_t k = threadIdx.x; k < count; k += blockDim.x) s[k] = 0ull;
+}
+
+__device__ __forceinline__ void cta_sums_add(unsigned long long* s, float v) {
+    if (v != 0.0f) atomicAdd(s, static_cast<unsigned long long>(to_fixed(v)));
+}
+
+__device__ __forceinline__ void cta_sums_flush(unsigned long long* s, unsigned long long* g, uint32_t count) {
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < count; k += blockDim.x) {
+        const unsigned long long v = s[k];
+        if (v != 0ull) atomicAdd(g + k, v);
+    }
+}
+
+// Box test of a fruit against a yarn segment (the broadphase of the
+// reference's per-fruit segment loop).
+__device__ __forceinline__ bool fruit_near_segment(const float4& fs, const float4& pa, const float4& pb,
+                                                   float radius) {
+    const float target = fs.w + radius;
+    return !(fs.x < fminf(pa.x, pb.x) - target || fs.x > fmaxf(pa.x, pb.x) + target ||
+             fs.y < fminf(pa.y, pb.y) - target || fs.y > fmaxf(pa.y, pb.y) + target ||
+             fs.z < fminf(pa.z, pb.z) - target || fs.z > fmaxf(pa.z, pb.z) + target);
+}
+
+// One yarn colour of the fruit/yarn sweep.  Fruits do not move during a
+// sweep (their summed displacements are applied after it), so the first
+// colour stages them in shared memory for all colours, the CTA's
+// displacement sums accumulate over the sweep, and the last colour adds
+// them to the global sums.
+__device__ void yarn_contact_batch(Ctx& ctx, const Batch& bt, bool first, bool last) {
     const DeviceCloth& d = ctx.d;
     const SubCfg& c = ctx.c;
     __shared__ float4 s_fruit[NC_MAX_FRUITS];   // xyz position, w radius
     __shared__ float s_fw[NC_MAX_FRUITS];
-    for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
-        const NumiClothFruit& fr = d.fruits[f];
-        s_fruit[f] = make_float4(__ldcg(&fr.positionAndInverseMass.x), __ldcg(&fr.positionAndInverseMass.y),
-                                 __ldcg(&fr.positionAndInverseMass.z), __ldcg(&fr.previousAndRadius.w));
-        s_fw[f] = __ldcg(&fr.positionAndInverseMass.w);
+    __shared__ unsigned long long s_sum[3u * NC_MAX_FRUITS];
+    if (first) {
+        cta_sums_clear(s_sum, 3u * d.f_count);
+        for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
+            const NumiClothFruit& fr = d.fruits[f];
+            const float4 xw = __ldcg(reinterpret_cast<const float4*>(&fr.positionAndInverseMass));
+            s_fruit[f] = make_float4(xw.x, xw.y, xw.z, __ldcg(&fr.previousAndRadius.w));
+            s_fw[f] = xw.w;
+        }
+        __syncthreads();
     }
-    __syncthreads();
     unsigned long long* acc = reinterpret_cast<unsigned long long*>(d.fruit_partial);
     const uint32_t nf = d.f_count;
     const uint32_t lane = threadIdx.x & 31u;
@@ -362,18 +402,27 @@ __device__ void yarn_contact_batch(Ctx& ctx, const Batch& bt) {
             mask |= static_cast<unsigned long long>(__ballot_sync(0xffffffffu, near)) << f0;
         }
         if (!valid || mask == 0ull) continue;
-        const unsigned long long all = nf == 64u ? ~0ull : ((1ull << nf) - 1ull);
+        // this segment's own candidates among the warp's: the box test the
+        // loop applies, so the loop visits only fruits it would not skip
+        {
+            unsigned long long own = 0ull;
+            for (unsigned long long m = mask; m != 0ull; m &= m - 1ull) {
+                const uint32_t f = static_cast<uint32_t>(__ffsll(static_cast<long long>(m)) - 1);
+                if (fruit_near_segment(s_fruit[f], pa, pb, c.radius)) own |= 1ull << f;
+            }
+            mask = own;
+        }
         bool changed = false;
+        // contact-record tags of this segment, loaded at its first contact
+        bool rec_loaded = false, seg_live = false, recorded = false;
+        uint32_t rtag[NC_YARN_SLOTS] = {};
         while (mask != 0ull) {
             const uint32_t f = static_cast<uint32_t>(__ffsll(static_cast<long long>(mask)) - 1);
             mask &= mask - 1ull;
             const float4 fs = s_fruit[f];
             const V3 X{fs.x, fs.y, fs.z};
             const float target = fs.w + c.radius;
-            if (X.x < fminf(pa.x, pb.x) - target || X.x > fmaxf(pa.x, pb.x) + target ||
-                X.y < fminf(pa.y, pb.y) - target || X.y > fmaxf(pa.y, pb.y) + target ||
-                X.z < fminf(pa.z, pb.z) - target || X.z > fmaxf(pa.z, pb.z) + target)
-                continue;
+            if (!fruit_near_segment(fs, pa, pb, c.radius)) continue;
             V3 closest;
             float t;
             point_segment(X, xyz(pa), xyz(pb), closest, t);
@@ -391,39 +440,46 @@ __device__ void yarn_contact_batch(Ctx& ctx, const Batch& bt) {
             const float corr = target - dist;
             V3 delta{0.0f, 0.0f, 0.0f};
             const float lam = yarn_correction(pa, pb, w0, w1, s_fw[f], n, corr, c.ground, c.radius, delta);
-            if (!changed) {
-                changed = true;
-                mask |= all & ~((2ull << f) - 1ull);   // the segment moved: test every later fruit
-            }
-            if (delta.x != 0.0f || delta.y != 0.0f || delta.z != 0.0f) {
-                atomicAdd(acc + 3u * f + 0u, static_cast<unsigned long long>(to_fixed(delta.x)));
-                atomicAdd(acc + 3u * f + 1u, static_cast<unsigned long long>(to_fixed(delta.y)));
-                atomicAdd(acc + 3u * f + 2u, static_cast<unsigned long long>(to_fixed(delta.z)));
-            }
+            // the segment moved: its candidates are the later fruits near its
+            // new box
+            changed = true;
+            mask = 0ull;
+            for (uint32_t g = f + 1u; g < nf; ++g)
+                if (fruit_near_segment(s_fruit[g], pa, pb, c.radius)) mask |= 1ull << g;
+            cta_sums_add(s_sum + 3u * f + 0u, delta.x);
+            cta_sums_add(s_sum + 3u * f + 1u, delta.y);
+            cta_sums_add(s_sum + 3u * f + 2u, delta.z);
             if (lam <= 0.0f) continue;
             const float imp = lam / c.dt;
-            // Contact record of (fruit f, segment seg) for friction.  The
-            // first record of the substep takes slot 0 without a search.
+            // Contact record of (fruit f, segment seg) for friction, kept in
+            // registers until the segment is done.  The first record of the
+            // substep takes slot 0 without a search and retires the others.
+            if (!rec_loaded) {
+                rec_loaded = true;
+                seg_live = __ldcg(d.yarn_live + seg) == ctx.epoch;
+                if (seg_live) {
+#pragma unroll
+                    for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q)
+                        rtag[q] = __float_as_uint(__ldcg(&d.yarn_slot_b[seg * NC_YARN_SLOTS + q].z));
+                }
+            }
             const uint32_t tag = (ctx.epoch << 6) | f;
-            const float4* slot_b = d.yarn_slot_b + seg * NC_YARN_SLOTS;
             int slot = -1;
             bool fresh = true;
-            if (__ldcg(d.yarn_live + seg) != ctx.epoch) {
+            if (!seg_live) {
                 slot = 0;
             } else {
-                uint32_t st[NC_YARN_SLOTS];
-#pragma unroll
-                for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q) st[q] = __float_as_uint(__ldcg(&slot_b[q].z));
 #pragma unroll
                 for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q) {
-                    if (st[q] == tag && fresh) {
+                    if (rtag[q] == tag && fresh) {
                         slot = static_cast<int>(q);
                         fresh = false;
                     }
                 }
                 if (fresh)
-                    for (uint32_t q = 0; q < NC_YARN_SLOTS && slot < 0; ++q)
-                        if ((st[q] >> 6) != (ctx.epoch & 0x3ffffffu)) slot = static_cast<int>(q);
+#pragma unroll
+                    for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q)
+                        if (slot < 0 && (rtag[q] >> 6) != (ctx.epoch & 0x3ffffffu)) slot = static_cast<int>(q);
             }
             if (slot < 0) {
                 fail(d, NUMI_CLOTH_FAILURE_RANGE);
@@ -442,26 +498,42 @@ __device__ void yarn_contact_batch(Ctx& ctx, const Batch& bt) {
             sb.y = sb.y + w1 * imp;
             d.yarn_slot_a[seg * NC_YARN_SLOTS + q] = sa;
             d.yarn_slot_b[seg * NC_YARN_SLOTS + q] = sb;
+#pragma unroll
+            for (uint32_t r = 0; r < NC_YARN_SLOTS; ++r)
+                if (r == q) rtag[r] = tag;
             if (q == 0u && fresh) {
                 // a new substep claims the segment: retire the older records
-                for (uint32_t r = 1; r < NC_YARN_SLOTS; ++r) d.yarn_slot_b[seg * NC_YARN_SLOTS + r].z = __uint_as_float(0u);
+#pragma unroll
+                for (uint32_t r = 1; r < NC_YARN_SLOTS; ++r) {
+                    d.yarn_slot_b[seg * NC_YARN_SLOTS + r].z = __uint_as_float(0u);
+                    rtag[r] = 0u;
+                }
             }
-            d.yarn_live[seg] = ctx.epoch;
+            seg_live = true;
+            recorded = true;
         }
         if (changed) {
             px_set(ctx, ij.x, pa);
             px_set(ctx, ij.y, pb);
         }
+        if (recorded) d.yarn_live[seg] = ctx.epoch;
     }
+    if (last) cta_sums_flush(s_sum, acc, 3u * nf);
 }
 
 __device__ bool yarn_sweep(Ctx& ctx) {
     if (ctx.d.f_count == 0u) return true;
     fruit_flush(ctx);
-    for (uint32_t b = 0; b < ctx.d.n_dist_batches; ++b) {
+    uint32_t first = NC_MAX_BATCHES, last = 0;
+    for (uint32_t b = 0; b < ctx.d.n_dist_batches; ++b)
+        if (ctx.d.dist_batches[b].yarn != 0u) {
+            first = min(first, b);
+            last = b;
+        }
+    for (uint32_t b = first; b <= last && b < ctx.d.n_dist_batches; ++b) {
         const Batch bt = ctx.d.dist_batches[b];
         if (bt.yarn == 0u) continue;
-        yarn_contact_batch(ctx, bt);
+        yarn_contact_batch(ctx, bt, b == first, b == last);
         NC_SYNC(ctx);
     }
     ctx.fruit_pending = true;
@@ -659,14 +731,33 @@ __device__ void phase_finalize(Ctx& ctx) {
 
 // Fruit/yarn Coulomb friction (tools/cloth_bag.cpp:3178-3270), one yarn
 // colour; fruit velocities are those at the start of the friction sweep.
-__device__ void yarn_friction_batch(Ctx& ctx, const Batch& bt) {
+__device__ void yarn_friction_batch(Ctx& ctx, const Batch& bt, bool first, bool last) {
     const DeviceCloth& d = ctx.d;
     const SubCfg& c = ctx.c;
     unsigned long long* acc = reinterpret_cast<unsigned long long*>(d.fruit_partial) + 3u * NC_MAX_FRUITS;
+    __shared__ unsigned long long s_sum[6u * NC_MAX_FRUITS];
+    // fruit velocities are frozen over the sweep: stage them once per CTA
+    __shared__ float4 s_vw[NC_MAX_FRUITS];   // velocity xyz, inverse mass
+    __shared__ float4 s_or[NC_MAX_FRUITS];   // spin xyz, radius
+    if (first) {
+        cta_sums_clear(s_sum, 6u * d.f_count);
+        for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
+            const NumiClothFruit& fr = d.fruits[f];
+            const float4 vg = __ldcg(reinterpret_cast<const float4*>(&fr.velocityAndGroundImpulse));
+            const float4 om = __ldcg(reinterpret_cast<const float4*>(&fr.angularVelocity));
+            s_vw[f] = make_float4(vg.x, vg.y, vg.z, __ldcg(&fr.positionAndInverseMass.w));
+            s_or[f] = make_float4(om.x, om.y, om.z, __ldcg(&fr.previousAndRadius.w));
+        }
+        __syncthreads();
+    }
     for (Range r = item_range(ctx, bt.yarn); r.i < r.end; r.i += r.stride) {
         const uint32_t seg = bt.first + r.i;
         if (__ldcg(d.yarn_live + seg) != ctx.epoch) continue;
         const uint2 ij = __ldg(d.d_ij + seg);
+        uint32_t st[NC_YARN_SLOTS];
+#pragma unroll
+        for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q)
+            st[q] = __float_as_uint(__ldcg(&d.yarn_slot_b[seg * NC_YARN_SLOTS + q].z));
         const float4 pa = px(ctx, ij.x);
         const float4 pb = px(ctx, ij.y);
         float4 va = pv(ctx, ij.x);
@@ -675,26 +766,37 @@ __device__ void yarn_friction_batch(Ctx& ctx, const Batch& bt) {
         const uint32_t live = ctx.epoch & 0x3ffffffu;
         uint32_t fruit_of[NC_YARN_SLOTS];
         uint32_t nlive = 0;
+#pragma unroll
         for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q) {
-            const uint32_t st = __float_as_uint(__ldcg(&d.yarn_slot_b[seg * NC_YARN_SLOTS + q].z));
-            fruit_of[q] = ((st >> 6) == live) ? (st & 63u) : 0xffffffffu;
+            fruit_of[q] = ((st[q] >> 6) == live) ? (st[q] & 63u) : 0xffffffffu;
             nlive += fruit_of[q] != 0xffffffffu ? 1u : 0u;
         }
         for (uint32_t visit = 0; visit < nlive; ++visit) {
-            int slot = -1;
+            uint32_t slot = 0;
             uint32_t f = 0xffffffffu;
+#pragma unroll
             for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q)
                 if (fruit_of[q] < f) {
                     f = fruit_of[q];
-                    slot = static_cast<int>(q);
+                    slot = q;
                 }
-            fruit_of[slot] = 0xffffffffu;
+#pragma unroll
+            for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q)
+                if (q == slot) fruit_of[q] = 0xffffffffu;
             const float4 sa = __ldcg(&d.yarn_slot_a[seg * NC_YARN_SLOTS + slot]);
             const float4 sb = __ldcg(&d.yarn_slot_b[seg * NC_YARN_SLOTS + slot]);
             const float ni = sa.w;
             const V3 wn{sa.x, sa.y, sa.z};
             if (ni <= 0.0f || lsq(wn) < 1.0e-20f) continue;
-            const FruitState fr = load_fruit(d.fruits[f]);
+            FruitState fr;
+            {
+                const float4 vw = s_vw[f];
+                const float4 orr = s_or[f];
+                fr.v = V3{vw.x, vw.y, vw.z};
+                fr.w = vw.w;
+                fr.omega = V3{orr.x, orr.y, orr.z};
+                fr.radius = orr.w;
+            }
             const V3 normal = normalized3(wn);
             float wt[2] = {sb.x / ni, sb.y / ni};
             const float sum = wt[0] + wt[1];
@@ -725,12 +827,12 @@ __device__ void yarn_friction_batch(Ctx& ctx, const Batch& bt) {
             const V3 imp = t * -ti;
             const V3 dv = imp * fr.w;
             const V3 dw = cross3(off, imp) * inv_i;
-            atomicAdd(acc + 6u * f + 0u, static_cast<unsigned long long>(to_fixed(dv.x)));
-            atomicAdd(acc + 6u * f + 1u, static_cast<unsigned long long>(to_fixed(dv.y)));
-            atomicAdd(acc + 6u * f + 2u, static_cast<unsigned long long>(to_fixed(dv.z)));
-            atomicAdd(acc + 6u * f + 3u, static_cast<unsigned long long>(to_fixed(dw.x)));
-            atomicAdd(acc + 6u * f + 4u, static_cast<unsigned long long>(to_fixed(dw.y)));
-            atomicAdd(acc + 6u * f + 5u, static_cast<unsigned long long>(to_fixed(dw.z)));
+            cta_sums_add(s_sum + 6u * f + 0u, dv.x);
+            cta_sums_add(s_sum + 6u * f + 1u, dv.y);
+            cta_sums_add(s_sum + 6u * f + 2u, dv.z);
+            cta_sums_add(s_sum + 6u * f + 3u, dw.x);
+            cta_sums_add(s_sum + 6u * f + 4u, dw.y);
+            cta_sums_add(s_sum + 6u * f + 5u, dw.z);
             const V3 na = xyz(va) + resp[0] * (ti * wt[0]);
             const V3 nb = xyz(vb) + resp[1] * (ti * wt[1]);
             va = with_xyz(va, na);
@@ -739,6 +841,7 @@ __device__ void yarn_friction_batch(Ctx& ctx, const Batch& bt) {
         pv_set(ctx, ij.x, va);
         pv_set(ctx, ij.y, vb);
     }
+    if (last) cta_sums_flush(s_sum, acc, 6u * d.f_count);
 }
 
 // Fruit frictions and orientation in the fruit CTA: pair friction on
@@ -757,11 +860,25 @@ __device__ void fruit_tail(Ctx& ctx) {
         fs.o[f] = make_float4(fr.angularVelocity.x, fr.angularVelocity.y, fr.angularVelocity.z,
                               fr.previousAndRadius.w);
     }
-    bool loaded = false;
-    for (uint32_t k = threadIdx.x; k < d.p_count; k += blockDim.x) loaded = loaded || fs.contact[k].w > 0.0f;
-    const bool any_pair = __syncthreads_or(loaded) != 0;
-    if (ctx.s.frictions && any_pair && threadIdx.x < 32u) {
-        for (uint32_t b = 0; b < d.n_pair_batches; ++b) {
+    // Colours holding at least one loaded pair (one warp per colour); the
+    // friction walk visits only those, in colour order.
+    __shared__ unsigned long long s_loaded;
+    if (threadIdx.x == 0) s_loaded = 0ull;
+    __syncthreads();
+    {
+        const uint32_t lane = threadIdx.x & 31u;
+        for (uint32_t b = threadIdx.x >> 5; b < d.n_pair_batches; b += blockDim.x >> 5) {
+            const Batch bt = d.pair_batches[b];
+            bool loaded = false;
+            for (uint32_t k = bt.first + lane; k < bt.first + bt.count; k += 32u) loaded = loaded || fs.contact[k].w > 0.0f;
+            if (__any_sync(0xffffffffu, loaded) && lane == 0u) atomicOr(&s_loaded, 1ull << b);
+        }
+    }
+    __syncthreads();
+    const unsigned long long loaded_colours = s_loaded;
+    if (ctx.s.frictions && loaded_colours != 0ull && threadIdx.x < 32u) {
+        for (unsigned long long m = loaded_colours; m != 0ull; m &= m - 1ull) {
+            const uint32_t b = static_cast<uint32_t>(__ffsll(static_cast<long long>(m)) - 1);
             const Batch bt = d.pair_batches[b];
             for (uint32_t k = bt.first + threadIdx.x; k < bt.first + bt.count; k += 32u) {
                 const float4 cw = fs.contact[k];
@@ -874,9 +991,15 @@ __device__ bool substep(Ctx& ctx, bool last) {
     phase_finalize(ctx);
     NC_SYNC(ctx);
     if (s.frictions && d.f_count > 0u) {
-        for (uint32_t b = 0; b < d.n_dist_batches; ++b) {
+        uint32_t first = NC_MAX_BATCHES, last = 0;
+        for (uint32_t b = 0; b < d.n_dist_batches; ++b)
+            if (d.dist_batches[b].yarn != 0u) {
+                first = min(first, b);
+                last = b;
+            }
+        for (uint32_t b = first; b <= last && b < d.n_dist_batches; ++b) {
             if (d.dist_batches[b].yarn == 0u) continue;
-            yarn_friction_batch(ctx, d.dist_batches[b]);
+            yarn_friction_batch(ctx, d.dist_batches[b], b == first, b == last);
             NC_SYNC(ctx);
         }
         fruit_flush_velocity(ctx);
