@@ -33,9 +33,10 @@ SIDE = 256
 METRIC = "substeps/s (65k-particle cloth)"
 
 # Bench schedule: one XPBD iteration and one strain sweep per substep, no
-# reconciliation or certificate loops, swept ground, frictions on.
+# reconciliation or certificate loops, swept ground, frictions on, hash-grid
+# point self contact (contact distance 2r = 2 mm) on.
 BENCH_SCHEDULE = dict(iterations=1, strainSweeps=1, reconcilePasses=0, finalPasses=0, certificatePasses=0,
-                      earlyExit=0, aerodynamics=0, sweptGround=1, frictions=1, selfCollision=0)
+                      earlyExit=0, aerodynamics=0, sweptGround=1, frictions=1, selfCollision=1)
 
 
 def algorithmic_bytes(counts: dict) -> dict:
@@ -44,8 +45,9 @@ def algorithmic_bytes(counts: dict) -> dict:
     Per-unit figures: predict 52 B/particle (read x,v,w 28 + write x,prev 24),
     constraint 72 B (record 12 + lambda 4 + 2 endpoints x (read 16 + write 12)),
     strain 68 B per limited constraint, sphere/ground 28 B/particle, fruit/yarn
-    sweep 40 B per yarn segment (index 8 + 2 endpoints x 16), finalize 36
-    B/particle (read x,prev 24 + write v 12).
+    sweep 40 B per yarn segment (index 8 + 2 endpoints x 16), point
+    self-contact hash grid 60 B/particle (build 20 + sort 16 + query
+    read/write 24), finalize 36 B/particle (read x,prev 24 + write v 12).
     """
     n, cons, lim, yarn = counts["particles"], counts["constraints"], counts["limited"], counts["yarn"]
     parts = {
@@ -54,6 +56,7 @@ def algorithmic_bytes(counts: dict) -> dict:
         "strain": 68 * lim,
         "ground": 28 * n,
         "fruit_yarn": 40 * yarn,
+        "hash_grid": 60 * n if counts.get("self_collision", 1) else 0,
         "finalize": 36 * n,
     }
     parts["total"] = sum(parts.values())
@@ -301,7 +304,7 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": per_launch_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"square cloth {SIDE}x{SIDE} (65,536 particles, 4 mm), 64 spheres, 2 gripped "
-                                   "corners, ground; 48 substeps per step (60 Hz frame)",
+                                   "corners, ground, hash-grid self contact; 48 substeps per step (60 Hz frame)",
                        "substeps_per_step": SUBSTEPS, "schedule": BENCH_SCHEDULE,
                        "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}",
                        "grid": info["grid"], "block": info["block"],

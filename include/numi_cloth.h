@@ -221,6 +221,12 @@ int numi_cloth_read_grips(numi_cloth_t* handle, NumiClothGrip* out, uint32_t cou
  * out[2] max fruit/yarn penetration (m), out[3] max self penetration (m). */
 int numi_cloth_residuals(numi_cloth_t* handle, double out[4]);
 
+/* Point self-contact counters since create: pairs resolved and the largest
+ * penetration resolved (m), the reference's metrics.selfContacts and
+ * maximumSelfPenetration (tools/cloth_bag.cpp:4949-4958).  Zero until a
+ * step ran with selfCollision. */
+int numi_cloth_self_contacts(numi_cloth_t* handle, unsigned long long* contacts, double* max_penetration);
+
 /* Release masks (x mouth candidates, y released) after the last step. */
 int numi_cloth_release_masks(numi_cloth_t* handle, uint32_t out[2]);
 
@@ -264,8 +270,9 @@ int numi_cloth_trace_cta(numi_cloth_t* handle, unsigned long long* out, uint32_t
  * Limits: at most NUMI_CLOTH_NOALLOC_MAX_PARTICLES particles,
  * NUMI_CLOTH_NOALLOC_MAX_DISTANCES distances, 64 fruits and
  * NUMI_CLOTH_NOALLOC_MAX_SUBSTEPS substeps per call; larger inputs are
- * rejected with NUMI_CLOTH_EINVAL.  The cloth runs on one CTA (the resident
- * small-cloth path).
+ * rejected with NUMI_CLOTH_EINVAL, and so is a schedule with selfCollision
+ * (the point self-contact hash grid is not part of the static scratch).
+ * The cloth runs on one CTA (the resident small-cloth path).
  *
  * The first call on a device looks up the scratch array's device address
  * (once per device, with that device current); make that first call before

@@ -542,6 +542,20 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
     up(d.fruits, scene->fruits, F * sizeof(NumiClothFruit));
     up(d.pairs, scene->fruitPairs, P * sizeof(NumiClothFruitPair));
     if (cfg.gripControl.y == 1u) up(cuff, scene->cuffParticles, 2u * cfg.gripControl.z * sizeof(uint32_t));
+    if (scene->localOffsets != nullptr && scene->localIndices != nullptr) {
+        // 2-hop topology CSR of the point self-contact exclusion
+        const uint32_t entries = scene->localOffsets[n];
+        uint32_t* off = h->buf.alloc<uint32_t>(n + 1u);
+        uint32_t* idx = h->buf.alloc<uint32_t>(entries);
+        if (off == nullptr || idx == nullptr) {
+            delete h;
+            return NUMI_CLOTH_ENOMEM;
+        }
+        up(off, scene->localOffsets, (n + 1u) * sizeof(uint32_t));
+        up(idx, scene->localIndices, entries * sizeof(uint32_t));
+        d.local_off = off;
+        d.local_idx = idx;
+    }
     if (e != cudaSuccess) {
         delete h;
         return NUMI_CLOTH_ECUDA;
@@ -610,6 +624,26 @@ int numi_cloth_step(numi_cloth_t* h, const NumiClothConfig* configs, uint32_t co
     s.frictions = schedule->frictions;
     s.release = schedule->release;
     s.damping = schedule->damping;
+    if (s.self_collision && h->d.hash_head == nullptr) {
+        // point self-contact grid, on first use: about two buckets per particle
+        uint32_t buckets = 1024u;
+        while (buckets < 2u * h->d.n) buckets <<= 1;
+        DeviceCloth& d = h->d;
+        d.hash_head = h->buf.alloc<unsigned long long>(buckets);
+        d.hash = h->buf.alloc<HashSlot>(static_cast<size_t>(buckets) * NC_HASH_CAP);
+        d.self_stats = h->buf.alloc<unsigned long long>(2);
+        if (d.hash_head == nullptr || d.hash == nullptr || d.self_stats == nullptr) {
+            d.hash_head = nullptr;
+            return NUMI_CLOTH_ENOMEM;
+        }
+        d.hash_mask = buckets - 1u;
+    }
+    if (h->d.hash_head != nullptr && ((h->epoch + count) >> 26) != (h->epoch >> 26)) {
+        // bucket tags hold 26 bits of the substep counter: clear on wrap
+        if (cudaMemsetAsync(h->d.hash_head, 0, (static_cast<size_t>(h->d.hash_mask) + 1u) * sizeof(unsigned long long),
+                            h->stream) != cudaSuccess)
+            return NUMI_CLOTH_ECUDA;
+    }
     const cudaError_t e = launch(h, count, s);
     h->epoch += count;
     if (e != cudaSuccess) {
@@ -720,6 +754,24 @@ int numi_cloth_residuals(numi_cloth_t* h, double out[4]) {
     out[0] = out[1] = out[2] = out[3] = 0.0;
     for (uint32_t b = 0; b < grid; ++b)
         for (int e = 0; e < 3; ++e) out[e] = std::max(out[e], r[3u * b + e]);
+    return NUMI_CLOTH_OK;
+}
+
+int numi_cloth_self_contacts(numi_cloth_t* h, unsigned long long* contacts, double* max_penetration) {
+    if (h == nullptr || contacts == nullptr || max_penetration == nullptr) return NUMI_CLOTH_EINVAL;
+    *contacts = 0ull;
+    *max_penetration = 0.0;
+    if (h->d.self_stats == nullptr) return NUMI_CLOTH_OK;
+    cudaSetDevice(h->device);
+    unsigned long long st[2] = {0ull, 0ull};
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess ||
+        cudaMemcpy(st, h->d.self_stats, sizeof(st), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return NUMI_CLOTH_ECUDA;
+    *contacts = st[0];
+    float pen = 0.0f;
+    const uint32_t bits = static_cast<uint32_t>(st[1]);
+    std::memcpy(&pen, &bits, sizeof(pen));
+    *max_penetration = pen;
     return NUMI_CLOTH_OK;
 }
 
@@ -870,6 +922,8 @@ extern "C" int numi_cloth_step_noalloc(const NumiClothConfig* base, const NumiCl
         if (batchCounts[k] > NC_MAX_BATCHES) return noalloc_reject("more than 64 colour runs in one family");
     if ((batchCounts[0] + batchCounts[1] + batchCounts[2] + batchCounts[3]) != 0u && batches == nullptr)
         return noalloc_reject("null batches");
+    if (schedule->selfCollision)
+        return noalloc_reject("selfCollision needs the point self-contact hash grid, which this path does not hold");
     if (!st->positions || !st->previous || !st->velocities || !st->rest || !st->failure ||
         (D && (!st->distanceIJ || !st->distanceMaterial || !st->distanceLambda)) ||
         (K && (!st->knotIJ || !st->knotMaterial || !st->knotLambda)) ||

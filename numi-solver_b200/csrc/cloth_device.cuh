@@ -26,12 +26,19 @@
 #define NC_YARN_SLOTS 4u
 #define NC_MAX_PAIRS 2016u
 #define NC_TRACE_SLOTS 128u
+#define NC_HASH_CAP 8u      /* particles one self-contact bucket holds */
 
 struct Batch {
     uint32_t first;
     uint32_t count;      // all records of the colour
     uint32_t limited;    // leading records that may carry a strain limit
     uint32_t yarn;       // leading records that are yarn segments
+};
+
+// One particle in the self-contact grid: one 32-byte sector.
+struct __align__(32) HashSlot {
+    float4 pos;     // start-of-pass position xyz, inverse mass
+    uint4 meta;     // particle index, 0, 0, 0
 };
 
 struct DeviceCloth {
@@ -111,6 +118,17 @@ struct DeviceCloth {
     uint32_t grid_width;  // row-major grid topology (square cloth) or 0
     const uint32_t* local_off;
     const uint32_t* local_idx;
+    // point self-contact hash grid: cells of twice the contact distance,
+    // hashed into hash_mask + 1 buckets (about two per particle) of
+    // NC_HASH_CAP slots; a bucket head is (pass tag << 32) | count, so
+    // buckets of older passes read as empty and nothing is cleared between
+    // passes
+    unsigned long long* hash_head;
+    HashSlot* hash;       // [buckets * NC_HASH_CAP]
+    uint32_t hash_mask;
+    // [0] self contacts (a < b pairs resolved), [1] max self penetration
+    // (float bits; non-negative so unsigned max orders them)
+    unsigned long long* self_stats;
 };
 
 struct Schedule {

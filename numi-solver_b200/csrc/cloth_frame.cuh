@@ -540,6 +540,201 @@ __device__ bool yarn_sweep(Ctx& ctx) {
     return true;
 }
 
+// ------------------------------------------------------- self contact ---
+// Point/point self contact (tools/cloth_bag.cpp:4249-4315), batched: every
+// particle resolves all its pairs closer than 2r against the positions at
+// the start of the pass and applies the sum of its corrections once.  The
+// reference pushes each pair apart in particle order (Gauss-Seidel); here
+// the pair set and the per-pair correction are the reference's, the sums
+// are 2^-40 fixed point so their order does not matter, and the two sides
+// of a pair compute exactly opposite corrections.
+
+// Not-a-neighbour test of the reference's localTopologyPair
+// (tools/cloth_bag.cpp:2723-2730): the 2-hop topology list, or for a
+// row-major grid cloth the 5 x 5 block around the particle.
+__device__ __forceinline__ bool local_pair(const DeviceCloth& d, uint32_t a, uint32_t b) {
+    if (d.local_off != nullptr) {
+        uint32_t lo = __ldg(d.local_off + a), hi = __ldg(d.local_off + a + 1u);
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            const uint32_t v = __ldg(d.local_idx + mid);
+            if (v == b) return true;
+            if (v < b) lo = mid + 1u;
+            else hi = mid;
+        }
+        return false;
+    }
+    if (d.grid_width == 0u) return a == b;
+    const int ra = static_cast<int>(a / d.grid_width), ca = static_cast<int>(a % d.grid_width);
+    const int rb = static_cast<int>(b / d.grid_width), cb = static_cast<int>(b % d.grid_width);
+    return abs(ra - rb) <= 2 && abs(ca - cb) <= 2;
+}
+
+// Bucket of a hash cell: the cell key with 21 biased bits per axis (as the
+// reference's spatialKey, tools/cloth_bag.cpp:2732-2738) through the
+// SplitMix64 finalizer (Steele, Lea and Flood 2014), so that neighbouring
+// cells of a flat cloth spread over the buckets.
+__device__ __forceinline__ uint32_t cell_bucket(int x, int y, int z, uint32_t mask) {
+    unsigned long long k = (static_cast<unsigned long long>(x + (1 << 20)) & 0x1fffffull) |
+                           ((static_cast<unsigned long long>(y + (1 << 20)) & 0x1fffffull) << 21) |
+                           ((static_cast<unsigned long long>(z + (1 << 20)) & 0x1fffffull) << 42);
+    k = (k ^ (k >> 30)) * 0xbf58476d1ce4e5b9ull;
+    k = (k ^ (k >> 27)) * 0x94d049bb133111ebull;
+    return static_cast<uint32_t>(k ^ (k >> 31)) & mask;
+}
+
+__device__ __forceinline__ uint32_t self_pass_tag(const Ctx& ctx, uint32_t it) { return (ctx.epoch << 6) | (it & 63u); }
+
+// Insert every particle at its start-of-pass position.  Tags only grow (the
+// host clears the heads when the substep counter wraps), so a max with
+// (tag, 0) resets a bucket of an older pass and leaves a current one alone;
+// the add after it, in the same thread's order on the same address, takes
+// the next slot.
+__device__ void self_insert(Ctx& ctx, uint32_t it) {
+    const DeviceCloth& d = ctx.d;
+    const float inv_cell = 1.0f / (4.0f * ctx.c.radius);
+    const unsigned long long tag = self_pass_tag(ctx, it);
+    for (Range r = particle_range(ctx); r.i < r.end; r.i += r.stride) {
+        const uint32_t i = r.i;
+        const float4 p = px(ctx, i);
+        const uint32_t bucket = cell_bucket(static_cast<int>(floorf(p.x * inv_cell)),
+                                            static_cast<int>(floorf(p.y * inv_cell)),
+                                            static_cast<int>(floorf(p.z * inv_cell)), d.hash_mask);
+        unsigned long long* head = d.hash_head + bucket;
+        atomicMax(head, tag << 32);
+        const uint32_t slot = static_cast<uint32_t>(atomicAdd(head, 1ull));
+        if (slot >= NC_HASH_CAP) {
+            fail(d, NUMI_CLOTH_FAILURE_RANGE);
+            continue;
+        }
+        HashSlot& e = d.hash[bucket * NC_HASH_CAP + slot];
+        e.pos = p;
+        e.meta = make_uint4(i, 0u, 0u, 0u);
+    }
+}
+
+// Resolve every particle's pairs.  A cell is twice the contact distance,
+// so the 2 x 2 x 2 cells on the particle's side of its own cell's centre
+// hold every particle closer than the contact distance.  The eight bucket
+// heads are read together, then the candidates in batches of eight, every
+// load of a batch issued before any is used.  The grid is read-only in this
+// phase and the grid barrier before it is a gpu-scope acquire, so the reads
+// may go through L1, where neighbouring particles of a CTA share cells;
+// under the cluster barrier (cluster-scope acquire) they stay L2 reads.
+#define NC_SELF_BATCH 8u
+__device__ void self_solve(Ctx& ctx, uint32_t it) {
+    const DeviceCloth& d = ctx.d;
+    const float target = 2.0f * ctx.c.radius;
+    const float inv_cell = 1.0f / (4.0f * ctx.c.radius);
+    const uint32_t tag = self_pass_tag(ctx, it);
+    const bool l1 = d.cluster_barrier == 0u;
+    unsigned long long contacts = 0ull;
+    float max_pen = 0.0f;
+    for (Range r = particle_range(ctx); r.i < r.end; r.i += r.stride) {
+        const uint32_t a = r.i;
+        const float4 p = px(ctx, a);
+        int base[3], step[3];
+        float gap2[3];   // squared distance to the probed neighbour cell, in cell units
+        const float coord[3] = {p.x * inv_cell, p.y * inv_cell, p.z * inv_cell};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const float c0 = floorf(coord[k]);
+            const float frac = coord[k] - c0;
+            base[k] = static_cast<int>(c0);
+            step[k] = frac < 0.5f ? -1 : 1;
+            const float gap = frac < 0.5f ? frac : 1.0f - frac;
+            gap2[k] = gap * gap;
+        }
+        uint32_t bk[8];
+        unsigned long long hd[8];
+#pragma unroll
+        for (uint32_t q = 0; q < 8u; ++q)
+            bk[q] = cell_bucket(base[0] + ((q & 1u) ? step[0] : 0), base[1] + ((q & 2u) ? step[1] : 0),
+                                base[2] + ((q & 4u) ? step[2] : 0), d.hash_mask);
+#pragma unroll
+        for (uint32_t q = 0; q < 8u; ++q) hd[q] = l1 ? __ldca(d.hash_head + bk[q]) : __ldcg(d.hash_head + bk[q]);
+        // candidates per bucket (a bucket met twice counts once)
+        uint32_t pre[9];
+        pre[0] = 0u;
+#pragma unroll
+        // A neighbour cell farther than the contact distance (half a cell)
+        // cannot hold a contact.  The margin covers the rounding of the cell
+        // coordinates: 1e-3 cells plus a few ulps of the largest coordinate.
+        const float slack =
+            0.5f + 1.0e-3f + 2.4e-7f * fmaxf(fabsf(coord[0]), fmaxf(fabsf(coord[1]), fabsf(coord[2])));
+        const float reach2 = slack * slack;
+        bool near[8];
+#pragma unroll
+        for (uint32_t q = 0; q < 8u; ++q) {
+            const float g2 = ((q & 1u) ? gap2[0] : 0.0f) + ((q & 2u) ? gap2[1] : 0.0f) + ((q & 4u) ? gap2[2] : 0.0f);
+            near[q] = q == 0u || g2 < reach2;
+            bool repeat = false;
+#pragma unroll
+            for (uint32_t e = 0; e < q; ++e) repeat = repeat || (near[e] && bk[e] == bk[q]);
+            const uint32_t cnt = (near[q] && !repeat && static_cast<uint32_t>(hd[q] >> 32) == tag)
+                                     ? min(static_cast<uint32_t>(hd[q]), NC_HASH_CAP)
+                                     : 0u;
+            pre[q + 1u] = pre[q] + cnt;
+        }
+        const uint32_t total = pre[8];
+        long long sum[3] = {0, 0, 0};
+        bool touched = false;
+        for (uint32_t t0 = 0; t0 < total; t0 += NC_SELF_BATCH) {
+            uint32_t slot[NC_SELF_BATCH];
+#pragma unroll
+            for (uint32_t j = 0; j < NC_SELF_BATCH; ++j) {
+                const uint32_t t = min(t0 + j, total - 1u);   // past the end: repeat the last
+                uint32_t bq = bk[0], pq = 0u;
+#pragma unroll
+                for (uint32_t k = 1; k < 8u; ++k)
+                    if (t >= pre[k]) {
+                        bq = bk[k];
+                        pq = pre[k];
+                    }
+                slot[j] = bq * NC_HASH_CAP + (t - pq);
+            }
+            float4 e[NC_SELF_BATCH];
+            uint32_t bidx[NC_SELF_BATCH];
+#pragma unroll
+            for (uint32_t j = 0; j < NC_SELF_BATCH; ++j) {
+                e[j] = l1 ? __ldca(&d.hash[slot[j]].pos) : __ldcg(&d.hash[slot[j]].pos);
+                bidx[j] = l1 ? __ldca(&d.hash[slot[j]].meta.x) : __ldcg(&d.hash[slot[j]].meta.x);
+            }
+#pragma unroll
+            for (uint32_t j = 0; j < NC_SELF_BATCH; ++j) {
+                if (t0 + j >= total) continue;
+                const uint32_t b = bidx[j];
+                if (b == a) continue;
+                const V3 diff = xyz(e[j]) - xyz(p);
+                const float L = len3(diff);
+                if (L >= target || L < 1.0e-12f) continue;
+                const float den = p.w + e[j].w;
+                if (den <= 0.0f) continue;
+                if (local_pair(d, a, b)) continue;
+                const V3 corr = diff * ((target - L) / (L * den));
+                sum[0] += to_fixed(-(corr.x * p.w));
+                sum[1] += to_fixed(-(corr.y * p.w));
+                sum[2] += to_fixed(-(corr.z * p.w));
+                touched = true;
+                if (a < b) {
+                    ++contacts;
+                    max_pen = fmaxf(max_pen, target - L);
+                }
+            }
+        }
+        if (touched) {
+            const float dx = from_fixed(static_cast<unsigned long long>(sum[0]));
+            const float dy = from_fixed(static_cast<unsigned long long>(sum[1]));
+            const float dz = from_fixed(static_cast<unsigned long long>(sum[2]));
+            px_set(ctx, a, make_float4(p.x + dx, p.y + dy, p.z + dz, p.w));
+        }
+    }
+    if (contacts != 0ull) {
+        atomicAdd(d.self_stats, contacts);
+        atomicMax(d.self_stats + 1, static_cast<unsigned long long>(__float_as_uint(max_pen)));
+    }
+}
+
 // Ground clamp (tools/cloth_bag.cpp:2655-2690).
 __device__ void phase_ground(Ctx& ctx) {
     const DeviceCloth& d = ctx.d;
@@ -954,6 +1149,12 @@ __device__ bool substep(Ctx& ctx, bool last) {
         }
         NC_SYNC(ctx);
         if (!yarn_sweep(ctx)) return false;
+        if (s.self_collision && d.hash_head != nullptr) {
+            fruit_flush(ctx);
+            self_insert(ctx, it);
+            NC_SYNC(ctx);
+            self_solve(ctx, it);   // same particle ranges as the ground clamp below
+        }
         phase_ground(ctx);
         NC_SYNC(ctx);
     }

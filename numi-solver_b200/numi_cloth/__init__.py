@@ -91,6 +91,7 @@ def load_library() -> ctypes.CDLL:
         "numi_cloth_snapshot": (i32, [vp, u32]),
         "numi_cloth_restore": (i32, [vp, u32]),
         "numi_cloth_launch_info": (i32, [vp, ctypes.POINTER(u32)]),
+        "numi_cloth_self_contacts": (i32, [vp, ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(ctypes.c_double)]),
         "numi_cloth_trace": (i32, [vp, ctypes.POINTER(ctypes.c_ulonglong), u32, u32]),
         "numi_cloth_trace_cta": (i32, [vp, ctypes.POINTER(ctypes.c_ulonglong), u32]),
         "numi_cloth_step_noalloc": (
@@ -430,6 +431,13 @@ class ClothSolver:
 
     def restore(self, slot: int = 0):
         self._check(self.lib.numi_cloth_restore(self._h, slot))
+
+    def self_contacts(self) -> tuple[int, float]:
+        """(pairs resolved, largest penetration resolved in m) since create."""
+        n = ctypes.c_ulonglong()
+        pen = ctypes.c_double()
+        self._check(self.lib.numi_cloth_self_contacts(self._h, ctypes.byref(n), ctypes.byref(pen)))
+        return int(n.value), float(pen.value)
 
     def launch_info(self) -> dict:
         out = (ctypes.c_uint32 * 6)()

@@ -975,6 +975,77 @@ struct Sim {
         return maxpen;
     }
 
+    // Point self contact in the kernel's batched order (restates
+    // solveSelfCollision, tools/cloth_bag.cpp:4249-4315): every non-local
+    // pair closer than 2r at the start of the pass, each particle's
+    // corrections summed (2^-40 fixed point in FP32, FP64 sums in FP64) and
+    // applied once.
+    R self_batched() {
+        const R target = R(2) * radius;
+        const R inv_cell = R(1) / target;
+        const uint32_t n = static_cast<uint32_t>(x.size());
+        const std::vector<V<R>> x0 = x;
+        std::unordered_map<uint64_t, std::vector<uint32_t>> cells;
+        auto cell = [&](const V<R>& p, int k[3]) {
+            k[0] = static_cast<int>(std::floor(p.x * inv_cell));
+            k[1] = static_cast<int>(std::floor(p.y * inv_cell));
+            k[2] = static_cast<int>(std::floor(p.z * inv_cell));
+        };
+        for (uint32_t i = 0; i < n; ++i) {
+            int k[3];
+            cell(x0[i], k);
+            cells[spatial_key(k[0], k[1], k[2])].push_back(i);
+        }
+        R maxpen = R(0);
+        for (uint32_t a = 0; a < n; ++a) {
+            int k[3];
+            cell(x0[a], k);
+            long long fs[3] = {0, 0, 0};
+            double ds[3] = {0.0, 0.0, 0.0};
+            std::vector<uint32_t> near;
+            for (int dz = -1; dz <= 1; ++dz)
+                for (int dy = -1; dy <= 1; ++dy)
+                    for (int dx = -1; dx <= 1; ++dx) {
+                        const auto it = cells.find(spatial_key(k[0] + dx, k[1] + dy, k[2] + dz));
+                        if (it != cells.end()) near.insert(near.end(), it->second.begin(), it->second.end());
+                    }
+            std::sort(near.begin(), near.end());
+            bool touched = false;
+            for (uint32_t b : near) {
+                if (b == a) continue;
+                const V<R> diff = x0[b] - x0[a];
+                const R L = len(diff);
+                if (L >= target || L < R(1.0e-12)) continue;
+                const R den = w[a] + w[b];
+                if (den <= R(0)) continue;
+                if (local_pair(a, b)) continue;
+                const V<R> corr = diff * ((target - L) / (L * den));
+                const R c3[3] = {-(corr.x * w[a]), -(corr.y * w[a]), -(corr.z * w[a])};
+                for (int e = 0; e < 3; ++e) {
+                    if constexpr (kF32)
+                        fs[e] += std::llrint(static_cast<double>(c3[e]) * kFixedScale);
+                    else
+                        ds[e] += static_cast<double>(c3[e]);
+                }
+                touched = true;
+                if (a < b) {
+                    ++self_contacts;
+                    maxpen = rmax(maxpen, target - L);
+                }
+            }
+            if (!touched) continue;
+            if constexpr (kF32) {
+                x[a] = V<R>{x[a].x + static_cast<R>(static_cast<double>(fs[0]) * (1.0 / kFixedScale)),
+                            x[a].y + static_cast<R>(static_cast<double>(fs[1]) * (1.0 / kFixedScale)),
+                            x[a].z + static_cast<R>(static_cast<double>(fs[2]) * (1.0 / kFixedScale))};
+            } else {
+                x[a] = V<R>{x[a].x + static_cast<R>(ds[0]), x[a].y + static_cast<R>(ds[1]),
+                            x[a].z + static_cast<R>(ds[2])};
+            }
+        }
+        return maxpen;
+    }
+
     // applyClothGroundFriction for one particle (tools/cloth_bag.cpp:2076-2115).
     static void cloth_ground_friction(V<R>& vel, R wi, R gi, R mu) {
         if (gi <= R(0) || wi <= R(0)) return;
@@ -1318,7 +1389,12 @@ struct Sim {
             solve_grips(sub, dt);
             pair_sweep(dt, serial);
             yarn_sweep(serial, ground_on, dt);
-            if (s.self_collision && serial) self_serial();
+            if (s.self_collision) {
+                if (serial)
+                    self_serial();
+                else
+                    self_batched();
+            }
             if (ground_on) ground(dt);
         }
         auto contacts = [&](bool with_strain) {
@@ -1523,6 +1599,12 @@ void oracle_residuals(void* p, double out[4]) {
         h->f->residuals(h->f->prm.ground != 0u, out);
     else
         h->d->residuals(h->d->prm.ground != 0u, out);
+}
+
+double oracle_self_pass(void* p, int serial) {
+    auto* h = static_cast<Handle*>(p);
+    if (h->f) return static_cast<double>(serial ? h->f->self_serial() : h->f->self_batched());
+    return serial ? h->d->self_serial() : h->d->self_batched();
 }
 
 void oracle_stats(void* p, uint64_t out[6]) {

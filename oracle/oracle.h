@@ -139,6 +139,10 @@ void oracle_residuals(void* h, double out[4]);
  * out[0..1] masks, out[2] max reconcile passes, out[3] max certificate passes,
  * out[4] fruit/yarn contacts, out[5] self contacts. */
 void oracle_stats(void* h, uint64_t out[6]);
+/* One point self-contact pass on the current state (serial = the
+ * reference's Gauss-Seidel order, else the batched order); returns the
+ * largest penetration it resolved. */
+double oracle_self_pass(void* h, int serial);
 /* Restated probes with known answers; returns 1 on pass and fills values. */
 int oracle_probe_strain(double out[4]);
 int oracle_probe_cloth_ground_friction(double out[4]);

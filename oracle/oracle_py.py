@@ -124,6 +124,8 @@ def lib() -> ctypes.CDLL:
         L.oracle_write.argtypes = [vp, vp, vp]
         L.oracle_residuals.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
         L.oracle_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64)]
+        L.oracle_self_pass.restype = ctypes.c_double
+        L.oracle_self_pass.argtypes = [vp, ctypes.c_int]
         for name, n in (("oracle_probe_strain", 4), ("oracle_probe_cloth_ground_friction", 4),
                         ("oracle_probe_rolling", 4), ("oracle_probe_aerodynamics", 8)):
             fn = getattr(L, name)
@@ -322,6 +324,10 @@ class Oracle:
         out = (ctypes.c_double * 4)()
         lib().oracle_residuals(self._h, out)
         return np.array(out[:])
+
+    def self_pass(self, serial: bool) -> float:
+        """One point self-contact pass on the current state."""
+        return float(lib().oracle_self_pass(self._h, 1 if serial else 0))
 
     def stats(self) -> dict:
         out = (ctypes.c_uint64 * 6)()

@@ -1,0 +1,110 @@
+"""Point/point self contact (tools/cloth_bag.cpp:4249-4315): the batched
+restatement in the oracle, and the GPU hash grid against it.
+
+The batched order resolves every non-local pair closer than 2r against the
+positions at the start of the pass and applies each particle's summed
+corrections once.  Where every particle is in at most one pair the reference's
+Gauss-Seidel pass and the batched pass make the same moves, bit for bit in
+FP64; that pins the batched pair set and per-pair correction to the
+reference's serial pass, which is itself pinned to the compiled reference by
+the golden runs.
+"""
+import numpy as np
+import pytest
+
+import numi_cloth as nc
+import oracle_py as op
+from helpers import FULL, gpu_positions, run_gpu, run_oracle, small_square
+
+
+def folded_square(side=24, gap=0.0015, fruits=0):
+    """A square folded in half over its middle row: the upper layer lies
+    `gap` above the lower one, so every upper particle is within 2r = 2 mm of
+    the lower particle under it (rows more than two apart: not local)."""
+    scene = small_square(side=side, fruits=fruits)
+    pos = scene.particles["positionAndInverseMass"]
+    prev = scene.particles["previousAndMass"]
+    half = side // 2
+    for r in range(half, side):
+        mirror = side - 1 - r
+        for c in range(side):
+            i, j = r * side + c, mirror * side + c
+            pos[i, 0], pos[i, 1] = pos[j, 0], pos[j, 1]
+            pos[i, 2] = pos[j, 2] + np.float32(gap)
+    prev[:, :3] = pos[:, :3]
+    scene.particles["velocity"][:] = 0.0
+    return scene
+
+
+def _oracle(scene, bits):
+    return op.Oracle(op.from_abi(scene), bits)
+
+
+def test_isolated_pairs_batched_equals_serial_fp64():
+    """Isolated overlapping pairs: the batched pass moves every particle
+    exactly as the reference's serial pass does."""
+    scene = small_square(side=24, fruits=0)
+    pos = scene.particles["positionAndInverseMass"]
+    side = 24
+    # five far-apart pairs, each particle 1.2-1.8 mm above another one
+    for k, (src, dst) in enumerate([(30, 200), (60, 330), (100, 460), (140, 520), (170, 560)]):
+        pos[dst, :3] = pos[src, :3] + np.array([0.0002 * k, -0.0001, 0.0012 + 0.00015 * k], np.float32)
+        assert abs(src // side - dst // side) > 2
+    a, b = _oracle(scene, 64), _oracle(scene, 64)
+    pen_a = a.self_pass(serial=True)
+    pen_b = b.self_pass(serial=False)
+    assert pen_a == pen_b and pen_a > 0.0
+    xa, xb = a.read()["particles"]["x"], b.read()["particles"]["x"]
+    assert np.array_equal(xa, xb)
+    moved = np.flatnonzero(np.any(xa != pos[:, :3].astype(np.float64), axis=1))
+    assert len(moved) == 10
+    assert a.stats()["self_contacts"] == b.stats()["self_contacts"] == 5
+
+
+def test_batched_pass_separates_folded_layers():
+    """On a folded cloth one batched pass resolves every overlapping pair
+    (each particle has exactly one partner across the fold), and both orders
+    find the same pairs."""
+    scene = folded_square()
+    o_ser, o_bat = _oracle(scene, 64), _oracle(scene, 64)
+    pen_s = o_ser.self_pass(serial=True)
+    pen_b = o_bat.self_pass(serial=False)
+    assert pen_b == pytest.approx(0.0005, rel=1e-3) and pen_s == pen_b
+    assert o_bat.stats()["self_contacts"] == o_ser.stats()["self_contacts"] > 0
+    x = o_bat.read()["particles"]["x"]
+    side, half = 24, 12
+    up = np.array([r * side + c for r in range(half + 3, side) for c in range(side)])
+    lo = np.array([(side - 1 - r) * side + c for r in range(half + 3, side) for c in range(side)])
+    gaps = np.linalg.norm(x[up] - x[lo], axis=1)
+    # pairs whose particles carry no other contact end exactly 2r apart
+    assert np.all(gaps >= 0.002 - 1e-9)
+
+
+@pytest.mark.gpu
+def test_gpu_self_contact_bitexact_fp32():
+    """The hash-grid kernel phases give the FP32 batched oracle's bits over
+    a frame with the folded cloth, and the same contact count."""
+    scene = folded_square(fruits=4)
+    cfg = nc.substep_configs(scene, 12)
+    s = nc.Schedule.make(**dict(FULL, selfCollision=1))
+    solver_out = run_gpu(scene, cfg, s)
+    o = run_oracle(scene, cfg, s, bits=32)
+    assert solver_out["failure"] == 0, nc.failure_names(solver_out["failure"])
+    gp = gpu_positions(solver_out).astype(np.float64)
+    assert np.array_equal(gp, o["particles"]["x"]), f"max |dx| = {np.abs(gp - o['particles']['x']).max()}"
+    assert np.array_equal(solver_out["particles"]["velocity"][:, :3].astype(np.float64), o["particles"]["v"])
+    assert solver_out["self_contacts"][0] == o["stats"]["self_contacts"] > 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("resident", ["0", "1"], ids=["global", "resident"])
+def test_gpu_self_contact_launch_modes(resident):
+    """Same bits with particles in global memory and resident in shared
+    memory, and from a multi-CTA cooperative grid."""
+    scene = folded_square(side=32)
+    cfg = nc.substep_configs(scene, 6)
+    s = nc.Schedule.make(**dict(FULL, selfCollision=1))
+    a = run_gpu(scene, cfg, s, env={"NUMI_CLOTH_RESIDENT": resident})
+    b = run_gpu(scene, cfg, s, grid=5)
+    assert a["failure"] == 0 and b["failure"] == 0
+    assert np.array_equal(a["particles"], b["particles"])
