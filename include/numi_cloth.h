@@ -227,7 +227,10 @@ int numi_cloth_residuals(numi_cloth_t* handle, double out[4]);
  * step ran with selfCollision. */
 int numi_cloth_self_contacts(numi_cloth_t* handle, unsigned long long* contacts, double* max_penetration);
 
-/* Release masks (x mouth candidates, y released) after the last step. */
+/* Release masks after the last step: out[0] fruits that entered the mouth
+ * (candidates), out[1] fruits released, one bit per fruit, sticky since
+ * create (updateReleasedFruit, tools/cloth_bag.cpp:4545-4597).  Updated
+ * every substep of a step whose schedule has release = 1. */
 int numi_cloth_release_masks(numi_cloth_t* handle, uint32_t out[2]);
 
 /* Device-side snapshot of the full dynamic state into slot (0..7), and back. */
@@ -271,7 +274,8 @@ int numi_cloth_trace_cta(numi_cloth_t* handle, unsigned long long* out, uint32_t
  * NUMI_CLOTH_NOALLOC_MAX_DISTANCES distances, 64 fruits and
  * NUMI_CLOTH_NOALLOC_MAX_SUBSTEPS substeps per call; larger inputs are
  * rejected with NUMI_CLOTH_EINVAL, and so is a schedule with selfCollision
- * (the point self-contact hash grid is not part of the static scratch).
+ * (the point self-contact hash grid is not part of the static scratch) or
+ * with release (the state carries no mouth rim).
  * The cloth runs on one CTA (the resident small-cloth path).
  *
  * The first call on a device looks up the scratch array's device address

@@ -346,6 +346,10 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
     d.pairs = h->buf.alloc<NumiClothFruitPair>(P);
     uint32_t* cuff = h->buf.alloc<uint32_t>(cfg.gripControl.y == 1u ? 2u * cfg.gripControl.z : 1u);
     d.cuff = cuff;
+    const uint32_t rim_count = scene->mouthRim != nullptr ? cfg.mouthControl.x : 0u;
+    uint32_t* rim = h->buf.alloc<uint32_t>(rim_count);
+    d.rim = rim_count >= 3u ? rim : nullptr;
+    d.release = h->buf.alloc<uint32_t>(2);
     d.yarn_slot_a = h->buf.alloc<float4>(static_cast<size_t>(F ? D : 1) * NC_YARN_SLOTS);
     d.yarn_slot_b = h->buf.alloc<float4>(static_cast<size_t>(F ? D : 1) * NC_YARN_SLOTS);
     d.yarn_live = h->buf.alloc<uint32_t>(F ? D : 1);
@@ -475,7 +479,8 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
 
     bool ok = d.x && d.xp && d.v && rest && d_ij && d_mat && d.d_lambda && k_ij && k_mat && d.k_lambda && b_ij &&
               b_mat && d.b_lambda && d.grips && d.fruits && d.pairs && cuff && d.yarn_slot_a && d.yarn_slot_b && d.yarn_live &&
-              d.force && d.fruit_partial && d.failure && d.bar_count && d.abort_flag && d.stats && d.red;
+              d.force && d.fruit_partial && d.failure && d.bar_count && d.abort_flag && d.stats && d.red && rim &&
+              d.release;
     if (!ok) {
         delete h;
         return NUMI_CLOTH_ENOMEM;
@@ -542,6 +547,7 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
     up(d.fruits, scene->fruits, F * sizeof(NumiClothFruit));
     up(d.pairs, scene->fruitPairs, P * sizeof(NumiClothFruitPair));
     if (cfg.gripControl.y == 1u) up(cuff, scene->cuffParticles, 2u * cfg.gripControl.z * sizeof(uint32_t));
+    if (rim_count > 0u) up(rim, scene->mouthRim, rim_count * sizeof(uint32_t));
     if (scene->localOffsets != nullptr && scene->localIndices != nullptr) {
         // 2-hop topology CSR of the point self-contact exclusion
         const uint32_t entries = scene->localOffsets[n];
@@ -568,7 +574,8 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
                   {d.b_lambda, std::max<size_t>(B, 1) * sizeof(float)},
                   {d.grips, std::max<size_t>(G, 1) * sizeof(NumiClothGrip)},
                   {d.fruits, std::max<size_t>(F, 1) * sizeof(NumiClothFruit)},
-                  {d.pairs, std::max<size_t>(P, 1) * sizeof(NumiClothFruitPair)}};
+                  {d.pairs, std::max<size_t>(P, 1) * sizeof(NumiClothFruitPair)},
+                  {d.release, 2u * sizeof(uint32_t)}};
     *out = h;
     return NUMI_CLOTH_OK;
 }
@@ -778,6 +785,10 @@ int numi_cloth_self_contacts(numi_cloth_t* h, unsigned long long* contacts, doub
 int numi_cloth_release_masks(numi_cloth_t* h, uint32_t out[2]) {
     if (h == nullptr || out == nullptr) return NUMI_CLOTH_EINVAL;
     out[0] = out[1] = 0u;
+    cudaSetDevice(h->device);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess ||
+        cudaMemcpy(out, h->d.release, 2u * sizeof(uint32_t), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return NUMI_CLOTH_ECUDA;
     return NUMI_CLOTH_OK;
 }
 
@@ -924,6 +935,8 @@ extern "C" int numi_cloth_step_noalloc(const NumiClothConfig* base, const NumiCl
         return noalloc_reject("null batches");
     if (schedule->selfCollision)
         return noalloc_reject("selfCollision needs the point self-contact hash grid, which this path does not hold");
+    if (schedule->release)
+        return noalloc_reject("release needs the mouth rim, which NumiClothDeviceState does not carry");
     if (!st->positions || !st->previous || !st->velocities || !st->rest || !st->failure ||
         (D && (!st->distanceIJ || !st->distanceMaterial || !st->distanceLambda)) ||
         (K && (!st->knotIJ || !st->knotMaterial || !st->knotLambda)) ||

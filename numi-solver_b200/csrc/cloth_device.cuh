@@ -71,6 +71,8 @@ struct DeviceCloth {
     NumiClothFruitPair* pairs;
     uint32_t p_count;
     const uint32_t* cuff;
+    const uint32_t* rim;           // ordered mouth-rim particles (Config mouthControl.x of them)
+    uint32_t* release;             // [0] mouth candidates, [1] released fruits (sticky bit masks)
     // fruit/yarn contact records, NC_YARN_SLOTS per yarn segment:
     //   a = (impulse-weighted normal on the fruit xyz, normal impulse)
     //   b = (impulse-weighted segment weights xy, tag bits, 0)

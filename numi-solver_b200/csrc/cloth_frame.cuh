@@ -1039,6 +1039,124 @@ __device__ void yarn_friction_batch(Ctx& ctx, const Batch& bt, bool first, bool 
     if (last) cta_sums_flush(s_sum, acc, 6u * d.f_count);
 }
 
+// ---------------------------------------------------------- release ----
+// Released-fruit masks (updateReleasedFruit, tools/cloth_bag.cpp:4545-4597):
+// the mouth frame from the ordered rim, a fruit's projection tested against
+// the rim polygon, and the 0.025 m hysteresis on leaving through the mouth
+// or around it.  FP64 throughout, in the reference's operation order, on
+// the fruit CTA (one thread per fruit; the frame by one thread).
+struct D3 {
+    double x, y, z;
+};
+__device__ __forceinline__ D3 operator+(D3 a, D3 b) { return D3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ D3 operator-(D3 a, D3 b) { return D3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ D3 operator*(D3 a, double s) { return D3{a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ double dot_d(D3 a, D3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+__device__ __forceinline__ D3 cross_d(D3 a, D3 b) {
+    return D3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ D3 vdiv_d(D3 a, double s) { return a * (1.0 / s); }
+__device__ __forceinline__ D3 normalized_d(D3 a) {
+    const double m = sqrt(dot_d(a, a));
+    return m > 1.0e-14 ? vdiv_d(a, m) : D3{1.0, 0.0, 0.0};
+}
+__device__ __forceinline__ double clamp01_d(double v) { return v < 0.0 ? 0.0 : (1.0 < v ? 1.0 : v); }
+__device__ __forceinline__ double min_d(double a, double b) { return b < a ? b : a; }
+__device__ __forceinline__ D3 to_d3(float4 p) { return D3{static_cast<double>(p.x), static_cast<double>(p.y), static_cast<double>(p.z)}; }
+
+__device__ void release_masks(Ctx& ctx) {
+    const DeviceCloth& d = ctx.d;
+    const NumiClothConfig& cf = d.cfg[ctx.sub];
+    const uint32_t m = cf.mouthControl.x;
+    if (!ctx.s.release || d.rim == nullptr || m < 3u || m > NUMI_CLOTH_MOUTH_RIM_CAPACITY) return;
+    __shared__ D3 s_ring[NUMI_CLOTH_MOUTH_RIM_CAPACITY];
+    __shared__ D3 s_frame[4];   // centre, normal, tangent, bitangent
+    __shared__ int s_ok;
+    __shared__ unsigned s_mask[2];
+    for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) s_ring[k] = to_d3(px(ctx, __ldg(d.rim + k)));
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        D3 center{0.0, 0.0, 0.0};
+        for (uint32_t k = 0; k < m; ++k) center = center + s_ring[k];
+        center = vdiv_d(center, static_cast<double>(m));
+        D3 area{0.0, 0.0, 0.0};
+        for (uint32_t k = 0; k < m; ++k) area = area + cross_d(s_ring[k] - center, s_ring[(k + 1u) % m] - center);
+        s_ok = dot_d(area, area) < 1.0e-16 ? 0 : 1;
+        if (s_ok) {
+            D3 normal = normalized_d(area);
+            const D3 bc = to_d3(px(ctx, cf.mouthControl.y));
+            if (dot_d(normal, center - bc) < 0.0) normal = normal * -1.0;
+            D3 tangent = s_ring[0] - center;
+            tangent = tangent - normal * dot_d(tangent, normal);
+            if (dot_d(tangent, tangent) < 1.0e-16)
+                tangent = cross_d(normal, fabs(normal.z) < 0.9 ? D3{0.0, 0.0, 1.0} : D3{1.0, 0.0, 0.0});
+            tangent = normalized_d(tangent);
+            s_frame[0] = center;
+            s_frame[1] = normal;
+            s_frame[2] = tangent;
+            s_frame[3] = normalized_d(cross_d(normal, tangent));
+        }
+        s_mask[0] = d.release[0];
+        s_mask[1] = d.release[1];
+    }
+    __syncthreads();
+    if (!s_ok) return;
+    const D3 center = s_frame[0], normal = s_frame[1], tangent = s_frame[2], bitangent = s_frame[3];
+    const double hysteresis = static_cast<double>(cf.mouthMaterial.x);
+    for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
+        const NumiClothFruit& fr = d.fruits[f];
+        const D3 p{static_cast<double>(fr.positionAndInverseMass.x), static_cast<double>(fr.positionAndInverseMass.y),
+                   static_cast<double>(fr.positionAndInverseMass.z)};
+        const double need = static_cast<double>(fr.previousAndRadius.w) + static_cast<double>(ctx.c.radius);
+        // projection inside the rim polygon, and its squared distance to it
+        const D3 rel = p - center;
+        const double qx = dot_d(rel, tangent), qy = dot_d(rel, bitangent);
+        bool in = false;
+        double best = INFINITY;
+        for (uint32_t a = 0, b = m - 1u; a < m; b = a++) {
+            const D3 ra = s_ring[a] - center, rb = s_ring[b] - center;
+            const double ax = dot_d(ra, tangent), ay = dot_d(ra, bitangent);
+            const double bx = dot_d(rb, tangent), by = dot_d(rb, bitangent);
+            const double ex = bx - ax, ey = by - ay;
+            const double el = ex * ex + ey * ey;
+            const double t = el > 1.0e-20 ? clamp01_d(((qx - ax) * ex + (qy - ay) * ey) / el) : 0.0;
+            const double sx = qx - (ax + t * ex), sy = qy - (ay + t * ey);
+            best = min_d(best, sx * sx + sy * sy);
+            if ((ay > qy) != (by > qy)) {
+                const double cx = ax + (bx - ax) * (qy - ay) / (by - ay);
+                if (qx < cx) in = !in;
+            }
+        }
+        const bool in_proj = in || best <= 0.0;
+        const bool near_proj = in || best <= need * need;
+        // distance to the rim polyline in 3D
+        double rim_best = INFINITY;
+        for (uint32_t a = 0; a < m; ++a) {
+            const D3 st = s_ring[a];
+            const D3 e = s_ring[(a + 1u) % m] - st;
+            const double el = dot_d(e, e);
+            const double t = el > 1.0e-20 ? clamp01_d(dot_d(p - st, e) / el) : 0.0;
+            const D3 off = p - (st + e * t);
+            rim_best = min_d(rim_best, dot_d(off, off));
+        }
+        const double out = dot_d(p - center, normal);
+        const unsigned bit = 1u << f;
+        bool candidate = (s_mask[0] & bit) != 0u;
+        if (in_proj && out > 0.0) candidate = true;
+        const double axial = out - need;
+        const double rim_clear = sqrt(rim_best) - need;
+        const bool cap = near_proj && axial > hysteresis;
+        const bool around = candidate && !in_proj && out > 0.0 && rim_clear > hysteresis;
+        if (candidate) atomicOr(&s_mask[0], bit);
+        if (cap || around) atomicOr(&s_mask[1], bit);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        d.release[0] = s_mask[0];
+        d.release[1] = s_mask[1];
+    }
+}
+
 // Fruit frictions and orientation in the fruit CTA: pair friction on
 // fruit velocities staged in shared memory (one warp walks the colours),
 // then ground friction, rolling resistance and orientation per fruit; the
@@ -1084,6 +1202,7 @@ __device__ void fruit_tail(Ctx& ctx) {
         }
     }
     __syncthreads();
+    release_masks(ctx);
     for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
         FruitState s = load_fruit(d.fruits[f]);
         s.v = xyz(fs.v[f]);

@@ -432,6 +432,12 @@ class ClothSolver:
     def restore(self, slot: int = 0):
         self._check(self.lib.numi_cloth_restore(self._h, slot))
 
+    def release_masks(self) -> tuple[int, int]:
+        """(mouth candidates, released) fruit bit masks, sticky since create."""
+        out = (ctypes.c_uint32 * 2)()
+        self._check(self.lib.numi_cloth_release_masks(self._h, out))
+        return int(out[0]), int(out[1])
+
     def self_contacts(self) -> tuple[int, float]:
         """(pairs resolved, largest penetration resolved in m) since create."""
         n = ctypes.c_ulonglong()

@@ -60,7 +60,8 @@ def run_gpu(scene, configs, sched: nc.Schedule, frames=1, grid=None, env=None):
         s.step(configs[f * per:(f + 1) * per], sched)
     fail = s.failure()
     out = {"particles": s.particles(), "fruits": s.fruits(), "distances": s.distances(), "grips": s.grips(),
-           "failure": fail, "residuals": s.residuals(), "info": s.launch_info(), "self_contacts": s.self_contacts()}
+           "failure": fail, "residuals": s.residuals(), "info": s.launch_info(), "self_contacts": s.self_contacts(),
+           "release": s.release_masks()}
     s.close()
     return out
 
