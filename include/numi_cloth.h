@@ -326,6 +326,52 @@ int numi_cloth_step_noalloc(const NumiClothConfig* base, const NumiClothDeviceSt
                             const NumiClothConfig* configs, uint32_t count,
                             const NumiClothSchedule* schedule, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Batched stepping: many independent cloths (same device) advanced by one
+ * persistent kernel launch per step.  Every CTA takes the next cloth from a
+ * device work queue, largest first, and runs its whole frame alone.  No
+ * reference counterpart: the reference runs one cloth per process
+ * (tools/cloth_bag_metal.mm:4010-4760); this is the batched forward of the
+ * square-cloth instances and of calibration candidates.
+ *
+ * The batch borrows the handles: destroy it before them.  Each cloth's
+ * state stays in its handle, so numi_cloth_read_* / numi_cloth_failure /
+ * snapshot / restore work on batch members as on single cloths.
+ * ------------------------------------------------------------------------ */
+typedef struct numi_cloth_batch numi_cloth_batch_t;
+
+int numi_cloth_batch_create(numi_cloth_t* const* cloths, uint32_t count, numi_cloth_batch_t** out);
+void numi_cloth_batch_destroy(numi_cloth_batch_t* batch);
+int numi_cloth_batch_set_stream(numi_cloth_batch_t* batch, void* stream);
+
+/* Advance every cloth by `substeps` substeps.  configs holds count x
+ * substeps Configs, cloth-major in the order the cloths were given (cloth
+ * k's substeps start at k * substeps); each is validated against its
+ * cloth's creation Config as numi_cloth_step does. */
+int numi_cloth_batch_step(numi_cloth_batch_t* batch, const NumiClothConfig* configs, uint32_t substeps,
+                          const NumiClothSchedule* schedule);
+
+/* Launch shape: out[0] resident particle chunk (cloths with at most that
+ * many particles keep them in shared memory; 0 = none), out[1] threads per
+ * CTA, out[2] CTAs of the persistent launch. */
+int numi_cloth_batch_shape(numi_cloth_batch_t* batch, uint32_t out[3]);
+int numi_cloth_batch_set_shape(numi_cloth_batch_t* batch, uint32_t resident_chunk, uint32_t threads);
+
+/* Autotuner: times one step of every candidate shape (resident chunk 0,
+ * 256 ... 4096; 256 or 512 threads) on the current state, restores the
+ * state after each, and keeps the fastest; out (optional) receives it. */
+int numi_cloth_batch_tune(numi_cloth_batch_t* batch, const NumiClothConfig* configs, uint32_t substeps,
+                          const NumiClothSchedule* schedule, uint32_t out[3]);
+
+/* CUDA graph of one step: the copy of `configs` (PINNED host memory the
+ * caller keeps and may rewrite between replays; same layout as
+ * numi_cloth_batch_step), the work-queue reset, the frame launch and the
+ * substep-counter advance.  numi_cloth_batch_replay validates the current
+ * contents of configs on the host and launches the graph. */
+int numi_cloth_batch_capture(numi_cloth_batch_t* batch, const NumiClothConfig* configs, uint32_t substeps,
+                             const NumiClothSchedule* schedule);
+int numi_cloth_batch_replay(numi_cloth_batch_t* batch);
+
 /* Library version string. */
 const char* numi_cloth_version(void);
 

@@ -29,6 +29,7 @@ static_assert(sizeof(NumiClothFruitPair) == 32, "FruitPair layout");
 static_assert(sizeof(NumiClothBatch) == 16, "Batch layout");
 static_assert(offsetof(NumiClothConfig, gravityAndTimestep) == 48, "Config offsets");
 static_assert(offsetof(NumiClothConfig, mouthMaterial) == 208, "Config offsets");
+static_assert(sizeof(DeviceCloth) % 4u == 0u, "DeviceCloth is copied as 32-bit words");
 
 __global__ void __launch_bounds__(NC_THREADS) numi_cloth_residual_kernel(DeviceCloth d, NumiClothConfig cfg) {
     Schedule s{};
@@ -36,6 +37,8 @@ __global__ void __launch_bounds__(NC_THREADS) numi_cloth_residual_kernel(DeviceC
     ctx.c = nc::load_cfg(&cfg);
     ctx.tid = blockIdx.x * blockDim.x + threadIdx.x;
     ctx.nthreads = gridDim.x * blockDim.x;
+    ctx.rank = blockIdx.x;
+    ctx.ranks = gridDim.x;
     nc::residual_partials(ctx, d.red);
 }
 
@@ -89,7 +92,7 @@ struct numi_cloth {
     uint32_t grid = 1;
     uint32_t block = NC_THREADS;
     uint32_t cluster = 0;   // > 0: the grid is one cluster of this many CTAs
-    size_t smem = sizeof(FruitShared);   // dynamic shared memory of a frame launch
+    size_t smem = nc_resident_offset();   // dynamic shared memory of a frame launch
     uint32_t launches = 0;
     uint32_t trace_capacity = 0;   // substeps the trace buffer holds
     uint32_t last_substeps = 0;
@@ -224,6 +227,49 @@ cudaError_t launch(numi_cloth* h, uint32_t substeps, const Schedule& s) {
     }
     if (e == cudaSuccess) ++h->launches;
     return e;
+}
+
+Schedule device_schedule(const NumiClothSchedule& schedule) {
+    Schedule s{};
+    s.iterations = schedule.iterations;
+    s.strain_sweeps = schedule.strainSweeps;
+    s.reconcile_passes = schedule.reconcilePasses;
+    s.final_passes = schedule.finalPasses;
+    s.certificate_passes = schedule.certificatePasses;
+    s.early_exit = schedule.earlyExit;
+    s.self_collision = schedule.selfCollision;
+    s.aerodynamics = schedule.aerodynamics;
+    s.swept_ground = schedule.sweptGround;
+    s.swept_fruit_yarn = schedule.sweptFruitYarn;
+    s.frictions = schedule.frictions;
+    s.release = schedule.release;
+    s.damping = schedule.damping;
+    return s;
+}
+
+// Point self-contact grid of a cloth, allocated on first use (about two
+// buckets per particle); the bucket heads are cleared when the 26-bit
+// substep part of their tags wraps within the next `substeps`.
+int prepare_self_grid(numi_cloth* h, bool self_collision, uint32_t substeps) {
+    if (self_collision && h->d.hash_head == nullptr) {
+        uint32_t buckets = 1024u;
+        while (buckets < 2u * h->d.n) buckets <<= 1;
+        DeviceCloth& d = h->d;
+        d.hash_head = h->buf.alloc<unsigned long long>(buckets);
+        d.hash = h->buf.alloc<HashSlot>(static_cast<size_t>(buckets) * NC_HASH_CAP);
+        d.self_stats = h->buf.alloc<unsigned long long>(2);
+        if (d.hash_head == nullptr || d.hash == nullptr || d.self_stats == nullptr) {
+            d.hash_head = nullptr;
+            return NUMI_CLOTH_ENOMEM;
+        }
+        d.hash_mask = buckets - 1u;
+    }
+    if (h->d.hash_head != nullptr && ((h->epoch + substeps) >> 26) != (h->epoch >> 26)) {
+        if (cudaMemsetAsync(h->d.hash_head, 0, (static_cast<size_t>(h->d.hash_mask) + 1u) * sizeof(unsigned long long),
+                            h->stream) != cudaSuccess)
+            return NUMI_CLOTH_ECUDA;
+    }
+    return NUMI_CLOTH_OK;
 }
 
 }  // namespace
@@ -368,14 +414,14 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
     int per_sm = 0;
-    raise_frame_smem(sizeof(FruitShared));
+    raise_frame_smem(nc_resident_offset());
     // NUMI_CLOTH_BLOCK=512 runs the cooperative grid with 512-thread CTAs
     // (one per SM) instead of 256 (two per SM).
     uint32_t block = NC_THREADS;
     if (env_u32("NUMI_CLOTH_BLOCK", block) && block != NC_BLOCK_MAX) block = NC_THREADS;
     h->block = block;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, numi_cloth_frame_kernel, static_cast<int>(block),
-                                                  sizeof(FruitShared));
+                                                  nc_resident_offset());
     uint32_t work = std::max({n, D, K, B});
     uint32_t grid = (work <= 8192u) ? 1u : std::min<uint32_t>(sms * std::max(per_sm, 1), (work + block - 1u) / block);
     uint32_t forced = 0;
@@ -446,7 +492,7 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
             cudaLaunchConfig_t cfg{};
             cfg.gridDim = dim3(c);
             cfg.blockDim = dim3(NC_BLOCK_MAX);
-            cfg.dynamicSmemBytes = sizeof(FruitShared);
+            cfg.dynamicSmemBytes = nc_resident_offset();
             cudaLaunchAttribute attr{};
             attr.id = cudaLaunchAttributeClusterDimension;
             attr.val.clusterDim.x = c;
@@ -617,40 +663,9 @@ int numi_cloth_step(numi_cloth_t* h, const NumiClothConfig* configs, uint32_t co
     if (cudaMemcpyAsync(h->d_cfg, configs, count * sizeof(NumiClothConfig), cudaMemcpyHostToDevice, h->stream) !=
         cudaSuccess)
         return NUMI_CLOTH_ECUDA;
-    Schedule s{};
-    s.iterations = schedule->iterations;
-    s.strain_sweeps = schedule->strainSweeps;
-    s.reconcile_passes = schedule->reconcilePasses;
-    s.final_passes = schedule->finalPasses;
-    s.certificate_passes = schedule->certificatePasses;
-    s.early_exit = schedule->earlyExit;
-    s.self_collision = schedule->selfCollision;
-    s.aerodynamics = schedule->aerodynamics;
-    s.swept_ground = schedule->sweptGround;
-    s.swept_fruit_yarn = schedule->sweptFruitYarn;
-    s.frictions = schedule->frictions;
-    s.release = schedule->release;
-    s.damping = schedule->damping;
-    if (s.self_collision && h->d.hash_head == nullptr) {
-        // point self-contact grid, on first use: about two buckets per particle
-        uint32_t buckets = 1024u;
-        while (buckets < 2u * h->d.n) buckets <<= 1;
-        DeviceCloth& d = h->d;
-        d.hash_head = h->buf.alloc<unsigned long long>(buckets);
-        d.hash = h->buf.alloc<HashSlot>(static_cast<size_t>(buckets) * NC_HASH_CAP);
-        d.self_stats = h->buf.alloc<unsigned long long>(2);
-        if (d.hash_head == nullptr || d.hash == nullptr || d.self_stats == nullptr) {
-            d.hash_head = nullptr;
-            return NUMI_CLOTH_ENOMEM;
-        }
-        d.hash_mask = buckets - 1u;
-    }
-    if (h->d.hash_head != nullptr && ((h->epoch + count) >> 26) != (h->epoch >> 26)) {
-        // bucket tags hold 26 bits of the substep counter: clear on wrap
-        if (cudaMemsetAsync(h->d.hash_head, 0, (static_cast<size_t>(h->d.hash_mask) + 1u) * sizeof(unsigned long long),
-                            h->stream) != cudaSuccess)
-            return NUMI_CLOTH_ECUDA;
-    }
+    const Schedule s = device_schedule(*schedule);
+    const int rc = prepare_self_grid(h, s.self_collision != 0u, count);
+    if (rc != NUMI_CLOTH_OK) return rc;
     const cudaError_t e = launch(h, count, s);
     h->epoch += count;
     if (e != cudaSuccess) {
@@ -1032,9 +1047,380 @@ extern "C" int numi_cloth_step_noalloc(const NumiClothConfig* base, const NumiCl
     s.damping = schedule->damping;
     s.substeps = count;
     void* args[] = {&d, &s};
-    e = raise_frame_smem(sizeof(FruitShared));
+    e = raise_frame_smem(nc_resident_offset());
     if (e == cudaSuccess)
         e = cudaLaunchKernel(reinterpret_cast<const void*>(numi_cloth_frame_kernel), dim3(1), dim3(NC_THREADS), args,
-                             sizeof(FruitShared), stream);
+                             nc_resident_offset(), stream);
     return e == cudaSuccess ? NUMI_CLOTH_OK : NUMI_CLOTH_ECUDA;
 }
+
+// ------------------------------------------------------------------------
+// Batched stepping (numi_cloth_batch_* in numi_cloth.h): many independent
+// cloths in one persistent launch.  Each CTA takes the next cloth from a
+// device work queue (largest cloths first, so the last wave is short) and
+// runs its whole frame alone with CTA barriers; the cloths' device state is
+// their handles' own, so every per-handle read/write call still works.
+
+struct numi_cloth_batch {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<numi_cloth*> cloths;   // caller order
+    std::vector<uint32_t> order;       // launch position -> caller index
+    DeviceBuffers buf;
+    DeviceCloth* d_cloths = nullptr;   // launch order
+    NumiClothConfig* d_cfg = nullptr;  // caller order, cloth-major
+    uint32_t cfg_capacity = 0;         // substeps per cloth d_cfg holds
+    uint32_t layout_substeps = 0;      // substeps the uploaded descriptors assume
+    bool layout_valid = false;
+    unsigned int* queue = nullptr;
+    uint32_t* epoch = nullptr;         // device substep counter
+    uint32_t epoch_host = 1;
+    uint32_t block = NC_THREADS;
+    uint32_t chunk = 0;                // resident particle chunk (0: none)
+    uint32_t ctas = 0;
+    size_t smem = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    const NumiClothConfig* graph_cfg = nullptr;
+    uint32_t graph_substeps = 0;
+};
+
+namespace {
+
+uint32_t log2_pow2(uint32_t v) {
+    uint32_t s = 0;
+    while ((1u << s) < v) ++s;
+    return s;
+}
+
+// Launch shape: resident chunk (0 or a power of two), threads per CTA, and
+// as many CTAs as fit on the device (never more than the cloths).
+int batch_shape(numi_cloth_batch* b, uint32_t chunk, uint32_t block) {
+    const size_t smem = nc_resident_offset() + (chunk ? 2u * static_cast<size_t>(chunk) * sizeof(float4) : 0u);
+    cudaFuncAttributes fa{};
+    if (cudaFuncGetAttributes(&fa, numi_cloth_batch_kernel) != cudaSuccess) return NUMI_CLOTH_ECUDA;
+    int optin = 0, sms = 0;
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+    if (smem + fa.sharedSizeBytes > static_cast<size_t>(optin)) return NUMI_CLOTH_EINVAL;
+    if (static_cast<size_t>(fa.maxDynamicSharedSizeBytes) < smem &&
+        cudaFuncSetAttribute(numi_cloth_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem)) != cudaSuccess)
+        return NUMI_CLOTH_ECUDA;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, numi_cloth_batch_kernel, static_cast<int>(block), smem) !=
+            cudaSuccess ||
+        per_sm < 1)
+        return NUMI_CLOTH_EINVAL;
+    b->chunk = chunk;
+    b->block = block;
+    b->smem = smem;
+    b->ctas = std::min<uint32_t>(static_cast<uint32_t>(b->cloths.size()), static_cast<uint32_t>(sms * per_sm));
+    b->layout_valid = false;
+    return NUMI_CLOTH_OK;
+}
+
+// Descriptors of every cloth for a launch of `substeps` Configs each.
+int batch_layout(numi_cloth_batch* b, uint32_t substeps) {
+    if (b->layout_valid && b->layout_substeps == substeps) return NUMI_CLOTH_OK;
+    const uint32_t count = static_cast<uint32_t>(b->cloths.size());
+    std::vector<DeviceCloth> host(count);
+    for (uint32_t j = 0; j < count; ++j) {
+        const uint32_t k = b->order[j];
+        DeviceCloth d = b->cloths[k]->d;
+        d.cfg = b->d_cfg + static_cast<size_t>(k) * substeps;
+        d.trace = nullptr;
+        d.trace_cta = nullptr;
+        d.cluster_barrier = 0u;
+        d.resident = (b->chunk != 0u && d.n <= b->chunk) ? 1u : 0u;
+        d.resident_shift = b->chunk ? log2_pow2(b->chunk) : 0u;
+        host[j] = d;
+    }
+    if (cudaMemcpyAsync(b->d_cloths, host.data(), count * sizeof(DeviceCloth), cudaMemcpyHostToDevice, b->stream) !=
+        cudaSuccess)
+        return NUMI_CLOTH_ECUDA;
+    if (cudaStreamSynchronize(b->stream) != cudaSuccess) return NUMI_CLOTH_ECUDA;
+    b->layout_substeps = substeps;
+    b->layout_valid = true;
+    return NUMI_CLOTH_OK;
+}
+
+// Validate and stage one launch: Configs, self-contact grids, descriptors.
+int batch_prepare(numi_cloth_batch* b, const NumiClothConfig* configs, uint32_t substeps, const NumiClothSchedule& sched) {
+    const uint32_t count = static_cast<uint32_t>(b->cloths.size());
+    for (uint32_t k = 0; k < count; ++k) {
+        numi_cloth* h = b->cloths[k];
+        if (h->poisoned) return NUMI_CLOTH_ESTATE;
+        for (uint32_t q = 0; q < substeps; ++q) {
+            const uint32_t bad = validate_config(configs[static_cast<size_t>(k) * substeps + q], h->base);
+            if (bad) {
+                h->host_failure |= bad;
+                return static_cast<int>(bad);
+            }
+        }
+    }
+    if (substeps > b->cfg_capacity) {
+        NumiClothConfig* cfg = b->buf.alloc<NumiClothConfig>(static_cast<size_t>(count) * substeps);
+        if (cfg == nullptr) return NUMI_CLOTH_ENOMEM;
+        b->d_cfg = cfg;
+        b->cfg_capacity = substeps;
+        b->layout_valid = false;
+    }
+    for (numi_cloth* h : b->cloths) {
+        void* before = h->d.hash_head;
+        h->epoch = b->epoch_host;
+        const int rc = prepare_self_grid(h, sched.selfCollision != 0u, substeps);
+        if (rc != NUMI_CLOTH_OK) return rc;
+        if (h->d.hash_head != before) b->layout_valid = false;
+        if (h->stream != b->stream && h->stream != nullptr && cudaStreamSynchronize(h->stream) != cudaSuccess)
+            return NUMI_CLOTH_ECUDA;
+    }
+    return batch_layout(b, substeps);
+}
+
+cudaError_t batch_launch(numi_cloth_batch* b, const NumiClothConfig* configs, uint32_t substeps, const Schedule& s) {
+    const uint32_t count = static_cast<uint32_t>(b->cloths.size());
+    cudaError_t e = cudaMemcpyAsync(b->d_cfg, configs, static_cast<size_t>(count) * substeps * sizeof(NumiClothConfig),
+                                    cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->queue, 0, sizeof(unsigned int), b->stream);
+    if (e != cudaSuccess) return e;
+    Schedule sc = s;
+    sc.substeps = substeps;
+    sc.epoch_ptr = b->epoch;
+    numi_cloth_batch_kernel<<<b->ctas, b->block, b->smem, b->stream>>>(b->d_cloths, count, sc, b->queue);
+    numi_cloth_epoch_kernel<<<1, 1, 0, b->stream>>>(b->epoch, substeps);
+    return cudaGetLastError();
+}
+
+void batch_advance(numi_cloth_batch* b, uint32_t substeps) {
+    b->epoch_host += substeps;
+    for (numi_cloth* h : b->cloths) {
+        h->epoch = b->epoch_host;
+        h->last_substeps = substeps;
+        ++h->launches;
+    }
+}
+
+void batch_drop_graph(numi_cloth_batch* b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+    b->graph_cfg = nullptr;
+}
+
+}  // namespace
+
+extern "C" {
+
+int numi_cloth_batch_create(numi_cloth_t* const* cloths, uint32_t count, numi_cloth_batch_t** out) {
+    if (cloths == nullptr || out == nullptr || count == 0) return NUMI_CLOTH_EINVAL;
+    *out = nullptr;
+    auto* b = new numi_cloth_batch();
+    b->device = cloths[0] ? cloths[0]->device : 0;
+    for (uint32_t k = 0; k < count; ++k) {
+        if (cloths[k] == nullptr || cloths[k]->device != b->device) {
+            delete b;
+            return NUMI_CLOTH_EINVAL;
+        }
+        for (uint32_t j = 0; j < k; ++j)
+            if (cloths[j] == cloths[k]) {
+                delete b;
+                return NUMI_CLOTH_EINVAL;
+            }
+        b->cloths.push_back(cloths[k]);
+        b->epoch_host = std::max(b->epoch_host, cloths[k]->epoch);
+    }
+    cudaSetDevice(b->device);
+    // largest work first: particles plus constraints
+    b->order.resize(count);
+    for (uint32_t k = 0; k < count; ++k) b->order[k] = k;
+    auto work = [&](uint32_t k) {
+        const DeviceCloth& d = b->cloths[k]->d;
+        return static_cast<uint64_t>(d.n) + d.d_count + d.k_count + d.b_count;
+    };
+    std::stable_sort(b->order.begin(), b->order.end(), [&](uint32_t a, uint32_t c) { return work(a) > work(c); });
+    b->d_cloths = b->buf.alloc<DeviceCloth>(count);
+    b->queue = b->buf.alloc<unsigned int>(1);
+    b->epoch = b->buf.alloc<uint32_t>(1);
+    if (!b->d_cloths || !b->queue || !b->epoch ||
+        cudaMemcpy(b->epoch, &b->epoch_host, sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess) {
+        delete b;
+        return NUMI_CLOTH_ENOMEM;
+    }
+    // default shape: particles from global memory, 256 threads per CTA
+    const int rc = batch_shape(b, 0u, NC_THREADS);
+    if (rc != NUMI_CLOTH_OK) {
+        delete b;
+        return rc;
+    }
+    *out = b;
+    return NUMI_CLOTH_OK;
+}
+
+void numi_cloth_batch_destroy(numi_cloth_batch_t* b) {
+    if (b == nullptr) return;
+    cudaSetDevice(b->device);
+    cudaStreamSynchronize(b->stream);
+    batch_drop_graph(b);
+    delete b;
+}
+
+int numi_cloth_batch_set_stream(numi_cloth_batch_t* b, void* stream) {
+    if (b == nullptr) return NUMI_CLOTH_EINVAL;
+    b->stream = static_cast<cudaStream_t>(stream);
+    batch_drop_graph(b);
+    return NUMI_CLOTH_OK;
+}
+
+int numi_cloth_batch_set_shape(numi_cloth_batch_t* b, uint32_t resident_chunk, uint32_t threads) {
+    if (b == nullptr || (threads != NC_THREADS && threads != NC_BLOCK_MAX) ||
+        (resident_chunk != 0u && (resident_chunk & (resident_chunk - 1u)) != 0u) || resident_chunk > 4096u)
+        return NUMI_CLOTH_EINVAL;
+    cudaSetDevice(b->device);
+    batch_drop_graph(b);
+    return batch_shape(b, resident_chunk, threads);
+}
+
+int numi_cloth_batch_shape(numi_cloth_batch_t* b, uint32_t out[3]) {
+    if (b == nullptr || out == nullptr) return NUMI_CLOTH_EINVAL;
+    out[0] = b->chunk;
+    out[1] = b->block;
+    out[2] = b->ctas;
+    return NUMI_CLOTH_OK;
+}
+
+int numi_cloth_batch_step(numi_cloth_batch_t* b, const NumiClothConfig* configs, uint32_t substeps,
+                          const NumiClothSchedule* schedule) {
+    if (b == nullptr || configs == nullptr || schedule == nullptr || substeps == 0) return NUMI_CLOTH_EINVAL;
+    cudaSetDevice(b->device);
+    const int rc = batch_prepare(b, configs, substeps, *schedule);
+    if (rc > 0) return NUMI_CLOTH_OK;   // a rejected Config: its cloth's failure word reports it
+    if (rc != NUMI_CLOTH_OK) return rc;
+    const cudaError_t e = batch_launch(b, configs, substeps, device_schedule(*schedule));
+    batch_advance(b, substeps);
+    if (e != cudaSuccess) {
+        for (numi_cloth* h : b->cloths) h->poisoned = true;
+        return NUMI_CLOTH_ECUDA;
+    }
+    return NUMI_CLOTH_OK;
+}
+
+int numi_cloth_batch_tune(numi_cloth_batch_t* b, const NumiClothConfig* configs, uint32_t substeps,
+                          const NumiClothSchedule* schedule, uint32_t out[3]) {
+    if (b == nullptr || configs == nullptr || schedule == nullptr || substeps == 0) return NUMI_CLOTH_EINVAL;
+    cudaSetDevice(b->device);
+    batch_drop_graph(b);
+    uint32_t largest = 0;
+    for (numi_cloth* h : b->cloths) largest = std::max(largest, h->d.n);
+    const uint32_t slot = kSnapshotSlots - 1u;
+    for (numi_cloth* h : b->cloths) {
+        const int rc = numi_cloth_snapshot(h, slot);
+        if (rc != NUMI_CLOTH_OK) return rc;
+        if (h->stream && cudaStreamSynchronize(h->stream) != cudaSuccess) return NUMI_CLOTH_ECUDA;
+    }
+    if (cudaDeviceSynchronize() != cudaSuccess) return NUMI_CLOTH_ECUDA;
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    float best_ms = INFINITY;
+    uint32_t best_chunk = 0, best_block = NC_THREADS;
+    const uint32_t chunks[] = {0u, 256u, 512u, 1024u, 2048u, 4096u};
+    const uint32_t blocks[] = {NC_THREADS, NC_BLOCK_MAX};
+    const Schedule s = device_schedule(*schedule);
+    int rc = NUMI_CLOTH_OK;
+    for (uint32_t chunk : chunks) {
+        if (chunk > 0u && chunk / 2u >= largest) continue;   // same as a smaller chunk
+        for (uint32_t block : blocks) {
+            if (batch_shape(b, chunk, block) != NUMI_CLOTH_OK) continue;
+            rc = batch_prepare(b, configs, substeps, *schedule);
+            if (rc != NUMI_CLOTH_OK) break;
+            cudaEventRecord(t0, b->stream);
+            const cudaError_t e = batch_launch(b, configs, substeps, s);
+            cudaEventRecord(t1, b->stream);
+            if (e != cudaSuccess || cudaEventSynchronize(t1) != cudaSuccess) {
+                rc = NUMI_CLOTH_ECUDA;
+                break;
+            }
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, t0, t1);
+            batch_advance(b, substeps);
+            if (ms < best_ms) {
+                best_ms = ms;
+                best_chunk = chunk;
+                best_block = block;
+            }
+            for (numi_cloth* h : b->cloths) numi_cloth_restore(h, slot);
+            if (cudaDeviceSynchronize() != cudaSuccess) {
+                rc = NUMI_CLOTH_ECUDA;
+                break;
+            }
+        }
+        if (rc != NUMI_CLOTH_OK) break;
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    if (rc != NUMI_CLOTH_OK) return rc;
+    rc = batch_shape(b, best_chunk, best_block);
+    if (rc == NUMI_CLOTH_OK && out != nullptr) numi_cloth_batch_shape(b, out);
+    return rc;
+}
+
+int numi_cloth_batch_capture(numi_cloth_batch_t* b, const NumiClothConfig* configs, uint32_t substeps,
+                             const NumiClothSchedule* schedule) {
+    if (b == nullptr || configs == nullptr || schedule == nullptr || substeps == 0) return NUMI_CLOTH_EINVAL;
+    cudaSetDevice(b->device);
+    batch_drop_graph(b);
+    int rc = batch_prepare(b, configs, substeps, *schedule);
+    if (rc > 0) return NUMI_CLOTH_EINVAL;
+    if (rc != NUMI_CLOTH_OK) return rc;
+    cudaStream_t cap = nullptr;
+    if (cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) != cudaSuccess) return NUMI_CLOTH_ECUDA;
+    cudaStream_t saved = b->stream;
+    b->stream = cap;
+    cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        const cudaError_t le = batch_launch(b, configs, substeps, device_schedule(*schedule));
+        e = cudaStreamEndCapture(cap, &b->graph);
+        if (le != cudaSuccess) e = le;
+    }
+    b->stream = saved;
+    cudaStreamDestroy(cap);
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, b->graph, 0);
+    if (e != cudaSuccess) {
+        batch_drop_graph(b);
+        cudaGetLastError();
+        return NUMI_CLOTH_ECUDA;
+    }
+    b->graph_cfg = configs;
+    b->graph_substeps = substeps;
+    return NUMI_CLOTH_OK;
+}
+
+int numi_cloth_batch_replay(numi_cloth_batch_t* b) {
+    if (b == nullptr || b->exec == nullptr) return NUMI_CLOTH_ESTATE;
+    cudaSetDevice(b->device);
+    const uint32_t count = static_cast<uint32_t>(b->cloths.size());
+    for (uint32_t k = 0; k < count; ++k) {
+        numi_cloth* h = b->cloths[k];
+        if (h->poisoned) return NUMI_CLOTH_ESTATE;
+        for (uint32_t q = 0; q < b->graph_substeps; ++q) {
+            const uint32_t bad = validate_config(b->graph_cfg[static_cast<size_t>(k) * b->graph_substeps + q], h->base);
+            if (bad) {
+                h->host_failure |= bad;
+                return NUMI_CLOTH_OK;
+            }
+        }
+        if (h->d.hash_head != nullptr && ((b->epoch_host + b->graph_substeps) >> 26) != (b->epoch_host >> 26))
+            return NUMI_CLOTH_ESTATE;   // tag wrap: capture again after a plain step
+    }
+    const cudaError_t e = cudaGraphLaunch(b->exec, b->stream);
+    batch_advance(b, b->graph_substeps);
+    if (e != cudaSuccess) {
+        for (numi_cloth* h : b->cloths) h->poisoned = true;
+        return NUMI_CLOTH_ECUDA;
+    }
+    return NUMI_CLOTH_OK;
+}
+
+}  // extern "C"

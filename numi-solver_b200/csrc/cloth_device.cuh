@@ -148,6 +148,10 @@ struct Schedule {
     uint32_t release;
     float damping;
     uint32_t substeps;
+    // batch launches: the substep counter of the batch in device memory
+    // (advanced by a kernel after each launch, so a captured graph can be
+    // replayed); null: DeviceCloth::epoch_base
+    const uint32_t* epoch_ptr;
 };
 
 // Fruit-side state kept in the shared memory of the fruit CTA for a whole

@@ -9,7 +9,8 @@ namespace nc {
 
 // Grid-wide barrier with a bounded wait.  Arrival is a release-add of 1 to
 // a counter the host zeroes before each launch; barrier number s of the
-// launch completes when an acquire load sees s * gridDim.x.  A CTA that waits past the limit
+// launch completes when an acquire load sees s times the number of CTAs on
+// the cloth.  A CTA that waits past the limit
 // raises TIMEOUT and the abort flag, and every CTA leaves at its next
 // barrier (or as soon as it sees the flag while waiting).
 __device__ bool grid_sync(Ctx& ctx) {
@@ -19,16 +20,16 @@ __device__ bool grid_sync(Ctx& ctx) {
     if (d.trace_cta && ctx.barriers <= NC_TRACE_SLOTS) {
         __syncthreads();
         if (threadIdx.x == 0)
-            d.trace_cta[(static_cast<size_t>(ctx.sub) * NC_TRACE_SLOTS + ctx.barriers - 1u) * gridDim.x + blockIdx.x] =
+            d.trace_cta[(static_cast<size_t>(ctx.sub) * NC_TRACE_SLOTS + ctx.barriers - 1u) * ctx.ranks + ctx.rank] =
                 globaltimer();
     }
     if (d.cluster_barrier) {
         cooperative_groups::this_cluster().sync();
-        if (d.trace && blockIdx.x == 0 && threadIdx.x == 0 && ctx.barriers <= NC_TRACE_SLOTS)
+        if (d.trace && ctx.rank == 0 && threadIdx.x == 0 && ctx.barriers <= NC_TRACE_SLOTS)
             d.trace[static_cast<size_t>(ctx.sub) * NC_TRACE_SLOTS + ctx.barriers - 1u] = globaltimer();
         return true;
     }
-    if (gridDim.x == 1) {
+    if (ctx.ranks == 1) {
         __syncthreads();
         if (d.trace && threadIdx.x == 0 && ctx.barriers <= NC_TRACE_SLOTS)
             d.trace[static_cast<size_t>(ctx.sub) * NC_TRACE_SLOTS + ctx.barriers - 1u] = globaltimer();
@@ -37,7 +38,7 @@ __device__ bool grid_sync(Ctx& ctx) {
     __shared__ unsigned s_abort;
     __syncthreads();
     if (threadIdx.x == 0) {
-        const unsigned long long target = ctx.seq * gridDim.x;
+        const unsigned long long target = ctx.seq * ctx.ranks;
         red_release_add_u64(d.bar_count, 1ull);
         unsigned ab = 0u;
         unsigned spins = 0u;
@@ -56,7 +57,7 @@ __device__ bool grid_sync(Ctx& ctx) {
         }
         __threadfence();
         s_abort = ab;
-        if (d.trace && blockIdx.x == 0 && ctx.barriers <= NC_TRACE_SLOTS)
+        if (d.trace && ctx.rank == 0 && ctx.barriers <= NC_TRACE_SLOTS)
             d.trace[static_cast<size_t>(ctx.sub) * NC_TRACE_SLOTS + ctx.barriers - 1u] = globaltimer();
     }
     __syncthreads();
@@ -214,7 +215,7 @@ __device__ void air_reduce_chunks(Ctx& ctx, const float4* force) {
     const uint32_t groups = blockDim.x / NC_THREADS;
     const uint32_t t = threadIdx.x % NC_THREADS;
     const uint32_t base = threadIdx.x - t;
-    for (uint32_t first = blockIdx.x * groups; first < chunks; first += gridDim.x * groups) {
+    for (uint32_t first = ctx.rank * groups; first < chunks; first += ctx.ranks * groups) {
         const uint32_t ch = first + threadIdx.x / NC_THREADS;
         const uint32_t i = ch * NC_THREADS + t;
         double pw = 0.0, q = 0.0;
@@ -656,7 +657,6 @@ __device__ void self_solve(Ctx& ctx, uint32_t it) {
         // candidates per bucket (a bucket met twice counts once)
         uint32_t pre[9];
         pre[0] = 0u;
-#pragma unroll
         // A neighbour cell farther than the contact distance (half a cell)
         // cannot hold a contact.  The margin covers the rounding of the cell
         // coordinates: 1e-3 cells plus a few ulps of the largest coordinate.
@@ -793,7 +793,7 @@ __device__ void residual_partials(Ctx& ctx, double* out3) {
     if (c.ground) {
         for (Range r = particle_range(ctx); r.i < r.end; r.i += r.stride)
             ground = fmax(ground, static_cast<double>(c.radius) - static_cast<double>(px(ctx, r.i).z));
-        if (blockIdx.x == 0)
+        if (ctx.rank == 0)
             for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x)
                 ground = fmax(ground, static_cast<double>(__ldcg(&d.fruits[f].previousAndRadius.w)) -
                                           static_cast<double>(__ldcg(&d.fruits[f].positionAndInverseMass.z)));
@@ -841,7 +841,7 @@ __device__ void residual_partials(Ctx& ctx, double* out3) {
         __syncthreads();
     }
     if (threadIdx.x == 0)
-        for (int e = 0; e < 3; ++e) out3[3u * blockIdx.x + e] = s_r[e][0];
+        for (int e = 0; e < 3; ++e) out3[3u * ctx.rank + e] = s_r[e][0];
     __syncthreads();
 }
 
@@ -849,7 +849,7 @@ __device__ bool residuals_converged(Ctx& ctx) {
     const DeviceCloth& d = ctx.d;
     __shared__ double s_r[3][NC_BLOCK_MAX];
     double r[3] = {0.0, 0.0, 0.0};
-    for (uint32_t b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+    for (uint32_t b = threadIdx.x; b < ctx.ranks; b += blockDim.x)
         for (int e = 0; e < 3; ++e) r[e] = fmax(r[e], __ldcg(d.red + 3u * b + e));
     for (int e = 0; e < 3; ++e) s_r[e][threadIdx.x] = r[e];
     __syncthreads();
@@ -1219,7 +1219,7 @@ __device__ void fruit_tail(Ctx& ctx) {
 }
 
 // One substep.  Returns false when a barrier gave up.
-__device__ bool substep(Ctx& ctx, bool last) {
+__device__ __forceinline__ bool substep(Ctx& ctx, bool last) {
     const DeviceCloth& d = ctx.d;
     const Schedule& s = ctx.s;
     const float dt2 = ctx.c.dt * ctx.c.dt;
@@ -1326,7 +1326,7 @@ __device__ bool substep(Ctx& ctx, bool last) {
     }
     fruit_tail(ctx);
     NC_SYNC(ctx);
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (ctx.rank == 0 && threadIdx.x == 0) {
         d.stats[1] = max(d.stats[1], passes);
         d.stats[2] = max(d.stats[2], cert);
     }
@@ -1335,28 +1335,43 @@ __device__ bool substep(Ctx& ctx, bool last) {
 
 }  // namespace nc
 
-// Byte offset of the resident particle arrays in dynamic shared memory.
-__host__ __device__ constexpr size_t nc_resident_offset() { return (sizeof(FruitShared) + 255u) & ~size_t(255u); }
+// Dynamic shared memory of a frame: the cloth descriptor, the fruit CTA's
+// state, then (resident mode) the CTA's particle positions and velocities.
+__host__ __device__ constexpr size_t nc_round256(size_t b) { return (b + 255u) & ~size_t(255u); }
+__host__ __device__ constexpr size_t nc_fruit_offset() { return nc_round256(sizeof(DeviceCloth)); }
+__host__ __device__ constexpr size_t nc_resident_offset() { return nc_round256(nc_fruit_offset() + sizeof(FruitShared)); }
 
-__global__ void __launch_bounds__(NC_BLOCK_MAX) numi_cloth_frame_kernel(DeviceCloth d, Schedule s) {
-    extern __shared__ __align__(16) unsigned char nc_dynamic_smem[];
-    FruitShared& fruit_shared = *reinterpret_cast<FruitShared*>(nc_dynamic_smem);
+// One cloth's frame on `ranks` CTAs (this one is `rank`): all substeps of
+// the launch's Configs, particles optionally resident in (distributed)
+// shared memory.
+// The descriptor is copied into shared memory first, so both kernels run
+// the phases on the same (shared-memory) view of it.
+__device__ __forceinline__ void run_frame(const DeviceCloth& src, const Schedule& s, uint32_t rank, uint32_t ranks,
+                                          unsigned char* dynamic_smem) {
+    {
+        const uint32_t* from = reinterpret_cast<const uint32_t*>(&src);
+        uint32_t* to = reinterpret_cast<uint32_t*>(dynamic_smem);
+        for (uint32_t w = threadIdx.x; w < sizeof(DeviceCloth) / 4u; w += blockDim.x) to[w] = from[w];
+        __syncthreads();
+    }
+    const DeviceCloth& d = *reinterpret_cast<const DeviceCloth*>(dynamic_smem);
+    FruitShared& fruit_shared = *reinterpret_cast<FruitShared*>(dynamic_smem + nc_fruit_offset());
     nc::Ctx ctx{d, s};
     ctx.fs = &fruit_shared;
-    ctx.tid = blockIdx.x * blockDim.x + threadIdx.x;
-    ctx.nthreads = gridDim.x * blockDim.x;
-    ctx.fruit_cta = blockIdx.x == gridDim.x - 1u;
-    ctx.grip_cta = blockIdx.x == 0u;
+    ctx.tid = rank * blockDim.x + threadIdx.x;
+    ctx.nthreads = ranks * blockDim.x;
+    ctx.fruit_cta = rank == ranks - 1u;
+    ctx.grip_cta = rank == 0u;
     ctx.fruit_pending = false;
     ctx.seq = 0;
     ctx.resident = d.resident != 0u;
-    ctx.rank = blockIdx.x;
-    ctx.ranks = gridDim.x;
+    ctx.rank = rank;
+    ctx.ranks = ranks;
     ctx.shift = d.resident_shift;
     uint32_t own_first = 0, own_end = 0;
     if (ctx.resident) {
         // Stage this CTA's particles into shared memory for the whole launch.
-        ctx.xs = reinterpret_cast<float4*>(nc_dynamic_smem + nc_resident_offset());
+        ctx.xs = reinterpret_cast<float4*>(dynamic_smem + nc_resident_offset());
         ctx.vs = ctx.xs + (1u << ctx.shift);
         own_first = ctx.rank << ctx.shift;
         own_end = min(own_first + (1u << ctx.shift), d.n);
@@ -1364,24 +1379,25 @@ __global__ void __launch_bounds__(NC_BLOCK_MAX) numi_cloth_frame_kernel(DeviceCl
             ctx.xs[i - own_first] = __ldcg(d.x + i);
             ctx.vs[i - own_first] = __ldcg(d.v + i);
         }
-        if (gridDim.x > 1u)
+        if (ranks > 1u)
             cooperative_groups::this_cluster().sync();
         else
             __syncthreads();
     }
-    if (blockIdx.x == gridDim.x - 1u) {
+    if (ctx.fruit_cta) {
         for (uint32_t k = threadIdx.x; k < d.p_count; k += blockDim.x)
             fruit_shared.ab[k] =
                 static_cast<unsigned short>(d.pairs[k].fruitsAndColor.x | (d.pairs[k].fruitsAndColor.y << 8));
         __syncthreads();
     }
+    const uint32_t epoch_base = s.epoch_ptr != nullptr ? *s.epoch_ptr : d.epoch_base;
     for (uint32_t sub = 0; sub < s.substeps; ++sub) {
         ctx.sub = sub;
         ctx.c = nc::load_cfg(d.cfg + sub);
-        ctx.epoch = d.epoch_base + sub;
+        ctx.epoch = epoch_base + sub;
         ctx.barriers = 0;
         if (!nc::substep(ctx, sub + 1u == s.substeps)) return;
-        if (blockIdx.x == 0 && threadIdx.x == 0) d.stats[0] = ctx.barriers;
+        if (rank == 0 && threadIdx.x == 0) d.stats[0] = ctx.barriers;
     }
     if (ctx.resident) {
         // Every remote access ended at the last barrier: write the CTA's own
@@ -1392,3 +1408,29 @@ __global__ void __launch_bounds__(NC_BLOCK_MAX) numi_cloth_frame_kernel(DeviceCl
         }
     }
 }
+
+// One cloth on the whole grid (one CTA, a cooperative grid or a cluster).
+__global__ void __launch_bounds__(NC_BLOCK_MAX) numi_cloth_frame_kernel(DeviceCloth d, Schedule s) {
+    extern __shared__ __align__(16) unsigned char nc_dynamic_smem[];
+    run_frame(d, s, blockIdx.x, gridDim.x, nc_dynamic_smem);
+}
+
+// Many independent cloths in one persistent launch: every CTA takes the
+// next cloth from a device work queue (cloths ordered by work, largest
+// first) and runs its whole frame alone, until the queue is empty.
+__global__ void __launch_bounds__(NC_BLOCK_MAX) numi_cloth_batch_kernel(const DeviceCloth* cloths, uint32_t count,
+                                                                         Schedule s, unsigned int* queue) {
+    extern __shared__ __align__(16) unsigned char nc_dynamic_smem[];
+    __shared__ uint32_t s_next;
+    for (;;) {
+        if (threadIdx.x == 0) s_next = atomicAdd(queue, 1u);
+        __syncthreads();
+        const uint32_t k = s_next;
+        if (k >= count) break;
+        run_frame(cloths[k], s, 0u, 1u, nc_dynamic_smem);
+        __syncthreads();
+    }
+}
+
+// Advance the batch substep counter after a batch launch.
+__global__ void numi_cloth_epoch_kernel(uint32_t* epoch, uint32_t substeps) { *epoch += substeps; }

@@ -92,6 +92,15 @@ def load_library() -> ctypes.CDLL:
         "numi_cloth_restore": (i32, [vp, u32]),
         "numi_cloth_launch_info": (i32, [vp, ctypes.POINTER(u32)]),
         "numi_cloth_self_contacts": (i32, [vp, ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(ctypes.c_double)]),
+        "numi_cloth_batch_create": (i32, [ctypes.POINTER(vp), u32, ctypes.POINTER(vp)]),
+        "numi_cloth_batch_destroy": (None, [vp]),
+        "numi_cloth_batch_set_stream": (i32, [vp, vp]),
+        "numi_cloth_batch_step": (i32, [vp, vp, u32, ctypes.POINTER(Schedule)]),
+        "numi_cloth_batch_shape": (i32, [vp, ctypes.POINTER(u32)]),
+        "numi_cloth_batch_set_shape": (i32, [vp, u32, u32]),
+        "numi_cloth_batch_tune": (i32, [vp, vp, u32, ctypes.POINTER(Schedule), ctypes.POINTER(u32)]),
+        "numi_cloth_batch_capture": (i32, [vp, vp, u32, ctypes.POINTER(Schedule)]),
+        "numi_cloth_batch_replay": (i32, [vp]),
         "numi_cloth_trace": (i32, [vp, ctypes.POINTER(ctypes.c_ulonglong), u32, u32]),
         "numi_cloth_trace_cta": (i32, [vp, ctypes.POINTER(ctypes.c_ulonglong), u32]),
         "numi_cloth_step_noalloc": (
@@ -532,3 +541,71 @@ def step_noalloc(scene: SceneArrays, state: abi.DeviceState, batches: np.ndarray
         _ptr(scene.config), ctypes.byref(state), _ptr(batches),
         counts.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), _ptr(configs), len(configs),
         ctypes.byref(schedule), ctypes.c_void_p(stream_ptr) if stream_ptr else None))
+
+
+class ClothBatch:
+    """Many ClothSolvers stepped by one persistent launch (numi_cloth_batch_*).
+
+    The batch borrows the solvers; close it before them.  Configs are given
+    as one array of shape [cloths, substeps] (CONFIG records)."""
+
+    def __init__(self, solvers: list):
+        self.lib = load_library()
+        self.solvers = list(solvers)
+        handles = (ctypes.c_void_p * len(self.solvers))(*[sv._h for sv in self.solvers])
+        h = ctypes.c_void_p()
+        rc = self.lib.numi_cloth_batch_create(handles, len(self.solvers), ctypes.byref(h))
+        if rc != 0:
+            raise ClothError(f"numi_cloth_batch_create failed ({rc})")
+        self._h = h
+        self._graph_cfg = None
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.numi_cloth_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def _check(self, rc: int):
+        if rc != 0:
+            raise ClothError(f"cloth batch call failed ({rc})")
+
+    def _configs(self, configs: np.ndarray) -> tuple[np.ndarray, int]:
+        configs = np.ascontiguousarray(configs, abi.CONFIG)
+        if configs.ndim != 2 or configs.shape[0] != len(self.solvers):
+            raise ClothError("configs must be [cloths, substeps]")
+        return configs, configs.shape[1]
+
+    def set_stream(self, stream_ptr: int | None):
+        self._check(self.lib.numi_cloth_batch_set_stream(self._h, ctypes.c_void_p(stream_ptr or 0)))
+
+    def step(self, configs: np.ndarray, schedule: Schedule):
+        configs, n = self._configs(configs)
+        self._check(self.lib.numi_cloth_batch_step(self._h, configs.ctypes.data, n, ctypes.byref(schedule)))
+
+    def shape(self) -> dict:
+        out = (ctypes.c_uint32 * 3)()
+        self._check(self.lib.numi_cloth_batch_shape(self._h, out))
+        return {"resident_chunk": out[0], "threads": out[1], "ctas": out[2]}
+
+    def set_shape(self, resident_chunk: int, threads: int):
+        self._check(self.lib.numi_cloth_batch_set_shape(self._h, resident_chunk, threads))
+
+    def tune(self, configs: np.ndarray, schedule: Schedule) -> dict:
+        configs, n = self._configs(configs)
+        out = (ctypes.c_uint32 * 3)()
+        self._check(self.lib.numi_cloth_batch_tune(self._h, configs.ctypes.data, n, ctypes.byref(schedule), out))
+        return {"resident_chunk": out[0], "threads": out[1], "ctas": out[2]}
+
+    def capture(self, pinned_configs, substeps: int, schedule: Schedule):
+        """Capture one step as a CUDA graph reading `pinned_configs` (a pinned
+        host buffer, e.g. a pinned torch uint8 tensor, holding [cloths,
+        substeps] CONFIG records) at every replay."""
+        self._graph_cfg = pinned_configs
+        self._check(self.lib.numi_cloth_batch_capture(self._h, ctypes.c_void_p(pinned_configs.data_ptr()), substeps,
+                                                      ctypes.byref(schedule)))
+
+    def replay(self):
+        self._check(self.lib.numi_cloth_batch_replay(self._h))
