@@ -193,6 +193,12 @@ typedef struct numi_cloth numi_cloth_t;
 int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out);
 void numi_cloth_destroy(numi_cloth_t* handle);
 
+/* Velocity damping of this cloth, v <- v / (1 + c dt) after gravity, in
+ * place of the schedule's `damping` (c < 0 restores the schedule's).  Set it
+ * before adding the cloth to a batch.  No reference counterpart: the
+ * reference has no damping term (c = 0 is the reference). */
+int numi_cloth_set_damping(numi_cloth_t* handle, float damping);
+
 /* Launch on this CUDA stream (cudaStream_t passed as void*; NULL = default). */
 int numi_cloth_set_stream(numi_cloth_t* handle, void* stream);
 

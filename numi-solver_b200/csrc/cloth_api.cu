@@ -367,6 +367,7 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
     d.f_count = F;
     d.p_count = P;
     d.grid_width = scene->gridWidth;
+    d.damping = -1.0f;
     d.x = h->buf.alloc<float4>(n);
     d.xp = h->buf.alloc<float4>(n);
     d.v = h->buf.alloc<float4>(n);
@@ -634,6 +635,12 @@ void numi_cloth_destroy(numi_cloth_t* h) {
         if (s.mem) cudaFree(s.mem);
     cudaFree(h->d_cfg);
     delete h;
+}
+
+int numi_cloth_set_damping(numi_cloth_t* h, float damping) {
+    if (h == nullptr || !std::isfinite(damping)) return NUMI_CLOTH_EINVAL;
+    h->d.damping = damping < 0.0f ? -1.0f : damping;
+    return NUMI_CLOTH_OK;
 }
 
 int numi_cloth_set_stream(numi_cloth_t* h, void* stream) {

@@ -117,6 +117,7 @@ struct DeviceCloth {
     double* red;          // [blocks * 8] reduction partials
     uint32_t* stats;      // [0] barriers of the last substep, [1] reconcile passes max, [2] certificate passes max
     uint32_t epoch_base;  // substep counter of the handle at launch
+    float damping;        // velocity damping c of v <- v / (1 + c dt); < 0: the schedule's
     uint32_t grid_width;  // row-major grid topology (square cloth) or 0
     const uint32_t* local_off;
     const uint32_t* local_idx;

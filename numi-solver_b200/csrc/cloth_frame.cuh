@@ -119,7 +119,7 @@ __device__ void phase_begin(Ctx& ctx) {
     const float dt = c.dt;
     const float inv_dt = 1.0f / dt;
     const bool air = ctx.s.aerodynamics != 0u;
-    const float damp = ctx.s.damping;
+    const float damp = d.damping >= 0.0f ? d.damping : ctx.s.damping;
     for (Range r = particle_range(ctx); r.i < r.end; r.i += r.stride) {
         const uint32_t i = r.i;
         float4 p = px(ctx, i);

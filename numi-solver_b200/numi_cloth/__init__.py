@@ -92,6 +92,7 @@ def load_library() -> ctypes.CDLL:
         "numi_cloth_restore": (i32, [vp, u32]),
         "numi_cloth_launch_info": (i32, [vp, ctypes.POINTER(u32)]),
         "numi_cloth_self_contacts": (i32, [vp, ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(ctypes.c_double)]),
+        "numi_cloth_set_damping": (i32, [vp, ctypes.c_float]),
         "numi_cloth_batch_create": (i32, [ctypes.POINTER(vp), u32, ctypes.POINTER(vp)]),
         "numi_cloth_batch_destroy": (None, [vp]),
         "numi_cloth_batch_set_stream": (i32, [vp, vp]),
@@ -389,6 +390,10 @@ class ClothSolver:
 
     def __del__(self):
         self.close()
+
+    def set_damping(self, damping: float):
+        """Per-cloth velocity damping c (v <- v / (1 + c dt)); < 0: the schedule's."""
+        self._check(self.lib.numi_cloth_set_damping(self._h, damping))
 
     def set_stream(self, stream_ptr: int | None):
         self.lib.numi_cloth_set_stream(self._h, ctypes.c_void_p(stream_ptr) if stream_ptr else None)

@@ -112,3 +112,17 @@ def test_batch_graph_replay_equals_steps():
     assert a is not None
     batch.close()
     rb.close()
+
+
+def test_per_cloth_damping_equals_schedule_damping():
+    scene = small_square(side=24, fruits=2)
+    cfg = nc.substep_configs(scene, 8)
+    a = nc.ClothSolver(scene)
+    a.step(cfg, nc.Schedule.make(**dict(PLAIN, damping=40.0)))
+    b = nc.ClothSolver(scene)
+    b.set_damping(40.0)
+    b.step(cfg, nc.Schedule.make(**PLAIN))
+    c = nc.ClothSolver(scene)
+    c.step(cfg, nc.Schedule.make(**PLAIN))
+    assert np.array_equal(a.particles(), b.particles())
+    assert not np.array_equal(a.particles(), c.particles())
