@@ -1,0 +1,342 @@
+// Reverse-mode adjoint of the cloth substep (no reference counterpart: the
+// reference calibrates with external finite-difference sensitivities,
+// docs/CLOTH_SPECIMEN_CALIBRATION.md:52-82).
+//
+// The forward runs a segment of substeps on one CTA and records a tape: the
+// positions at the start of every substep and after every phase barrier,
+// and the velocities at the start of every substep.  This kernel walks the
+// segment's substeps and each substep's phases in reverse and applies the
+// vector-Jacobian product of every projection.  Branch decisions are
+// recomputed in FP32 from the tape exactly as the forward made them; the
+// derivatives are evaluated in FP64 at the FP32 state, and adjoints and
+// parameter gradients are accumulated in FP64.
+//
+// Differentiated: predict with gravity and damping, XPBD distance / shear /
+// bend projections (one iteration, so lambda starts at zero), compliant
+// grips, the ground clamp, unilateral strain limits, finalize.  The other
+// phases (fruit pairs, fruit/yarn contact and friction, cloth/ground
+// friction, swept ground, bend ground active sets) are non-smooth; where one
+// of them changes the cloth it is counted in `nonsmooth` and passed through
+// as the identity.
+#pragma once
+
+#include "cloth_kernels.cuh"
+
+enum AdjointPhase : uint32_t {
+    ADJ_BEGIN = 0,
+    ADJ_DIST = 1,
+    ADJ_BEND = 2,
+    ADJ_GRIP = 3,
+    ADJ_YARN = 4,
+    ADJ_GROUND = 5,
+    ADJ_STRAIN = 6,
+    ADJ_FINAL = 7,
+    ADJ_YFRIC = 8,
+    ADJ_TAIL = 9,
+};
+
+// Gradient slots: d loss / d log compliance of distance kinds warp, weft,
+// bottom, shear; of bends; of grips; d loss / d damping.
+#define ADJ_GRADS 7u
+
+struct AdjointArgs {
+    const DeviceCloth* cloth;        // device copy of the handle's descriptor
+    const NumiClothConfig* cfg;      // the segment's Configs
+    const float4* tape;              // [substeps][slots][n]
+    const float4* tape_v;            // [substeps][n]
+    const uint2* phases;             // [slots - 1] (type, batch) per barrier
+    uint32_t slots;
+    uint32_t substeps;               // substeps of the segment
+    uint32_t first_substep;          // rollout index of the segment's first substep
+    float damping;                   // the schedule's (or the cloth's) damping
+    const uint32_t* tracked;         // [n_tracked]
+    uint32_t n_tracked;
+    const double* targets;           // [losses][n_tracked][3]
+    uint32_t loss_every;             // loss after substeps s with (s + 1) % loss_every == 0
+    double4* gx;                     // [n] adjoint of positions (xyz; w unused)
+    double4* gv;                     // [n] adjoint of velocities
+    double4* gprev;                  // [n] scratch: adjoint of the substep's start positions via finalize
+    double* grads;                   // [ADJ_GRADS] accumulated
+    double* grip_grads;              // [rollout substeps][6] or null
+    double* loss;                    // [1] accumulated
+    unsigned int* nonsmooth;         // [1] count of non-smooth events met
+};
+
+namespace adj {
+
+struct D3v {
+    double x, y, z;
+};
+__device__ __forceinline__ D3v d3(const double4& a) { return D3v{a.x, a.y, a.z}; }
+__device__ __forceinline__ D3v d3f(const V3& a) { return D3v{a.x, a.y, a.z}; }
+__device__ __forceinline__ D3v d4f(const float4& a) { return D3v{a.x, a.y, a.z}; }
+__device__ __forceinline__ double dotd(D3v a, D3v b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ D3v addd(D3v a, D3v b) { return D3v{a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ D3v subd(D3v a, D3v b) { return D3v{a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ D3v muld(D3v a, double s) { return D3v{a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ D3v crossd(D3v a, D3v b) {
+    return D3v{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ void put(double4* g, uint32_t i, D3v v) { g[i] = make_double4(v.x, v.y, v.z, 0.0); }
+
+// VJP of x_a' = x_a - w_a dl n, x_b' = x_b + w_b dl n with
+// dl = -(L - rest) / (w_a + w_b + alpha) (lambda from zero), n = (x_b - x_a)/L,
+// at the FP32 state a, b (derivatives in FP64).  Returns d loss / d alpha.
+__device__ __forceinline__ double distance_vjp(double4* gx, uint32_t ia, uint32_t ib, const float4& a, const float4& b,
+                                               double rest, double alpha) {
+    const D3v dd = subd(d4f(b), d4f(a));
+    const double L = sqrt(dotd(dd, dd));
+    const D3v n = muld(dd, 1.0 / L);
+    const double den = (static_cast<double>(a.w) + b.w) + alpha;
+    const double dl = -(L - rest) / den;
+    const D3v ga = d3(gx[ia]), gb = d3(gx[ib]);
+    const D3v u = subd(muld(gb, b.w), muld(ga, a.w));
+    const double un = dotd(u, n);
+    const D3v gd = addd(muld(n, -un / den), muld(subd(u, muld(n, un)), dl / L));
+    put(gx, ia, subd(ga, gd));
+    put(gx, ib, addd(gb, gd));
+    return -un * dl / den;
+}
+
+}  // namespace adj
+
+__global__ void __launch_bounds__(NC_THREADS) numi_cloth_adjoint_kernel(AdjointArgs A) {
+    using namespace adj;
+    const DeviceCloth& d = *A.cloth;
+    const uint32_t n = d.n;
+    double acc[ADJ_GRADS] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    double loss = 0.0;
+    unsigned int rough = 0u;
+    __shared__ double s_grip[NC_MAX_GRIPS][6];
+    for (uint32_t si = A.substeps; si-- > 0u;) {
+        const NumiClothConfig& cf = A.cfg[si];
+        const float dt = cf.gravityAndTimestep.w;
+        const float dt2 = dt * dt;
+        const double dtd = dt;
+        const float radius = cf.clothMaterial.x;
+        const bool ground = cf.constraintCounts.z != 0u;
+        const float4* T = A.tape + static_cast<size_t>(si) * A.slots * n;
+        const uint32_t step = A.first_substep + si;
+        // loss seed at the end of the substep
+        if (A.loss_every != 0u && (step + 1u) % A.loss_every == 0u) {
+            const uint32_t li = (step + 1u) / A.loss_every - 1u;
+            const float4* xe = T + static_cast<size_t>(A.slots - 1u) * n;
+            for (uint32_t t = threadIdx.x; t < A.n_tracked; t += blockDim.x) {
+                const uint32_t i = A.tracked[t];
+                const double* tg = A.targets + (static_cast<size_t>(li) * A.n_tracked + t) * 3u;
+                const D3v diff{static_cast<double>(xe[i].x) - tg[0], static_cast<double>(xe[i].y) - tg[1],
+                               static_cast<double>(xe[i].z) - tg[2]};
+                loss += dotd(diff, diff);
+                put(A.gx, i, addd(d3(A.gx[i]), muld(diff, 2.0)));
+            }
+            __syncthreads();
+        }
+        for (uint32_t b = A.slots - 1u; b-- > 0u;) {
+            const uint2 ph = A.phases[b];
+            const float4* pre = T + static_cast<size_t>(b) * n;     // positions before the phase
+            const float4* post = pre + n;                            // after its barrier
+            switch (ph.x) {
+            case ADJ_TAIL:
+                break;
+            case ADJ_YARN:
+            case ADJ_YFRIC:
+                // fruit/yarn contact moved the cloth: not differentiated
+                for (uint32_t i = threadIdx.x; i < n; i += blockDim.x)
+                    if (pre[i].x != post[i].x || pre[i].y != post[i].y || pre[i].z != post[i].z) ++rough;
+                break;
+            case ADJ_FINAL: {
+                // v_end = (x - x_start) / dt; cloth/ground friction of a
+                // particle resting on the ground is not differentiated
+                for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+                    if (pre[i].w == 0.0f) {
+                        A.gx[i] = make_double4(0, 0, 0, 0);
+                        A.gv[i] = make_double4(0, 0, 0, 0);
+                        A.gprev[i] = make_double4(0, 0, 0, 0);
+                        continue;
+                    }
+                    if (ground && pre[i].z <= radius + 1.0e-6f) ++rough;
+                    const D3v gvv = d3(A.gv[i]);
+                    put(A.gx, i, addd(d3(A.gx[i]), muld(gvv, 1.0 / dtd)));
+                    put(A.gprev, i, muld(gvv, -1.0 / dtd));
+                    A.gv[i] = make_double4(0, 0, 0, 0);
+                }
+                break;
+            }
+            case ADJ_STRAIN:
+            case ADJ_DIST: {
+                const Batch bt = d.dist_batches[ph.y];
+                const uint32_t count = ph.x == ADJ_STRAIN ? bt.limited : bt.count;
+                for (uint32_t r = threadIdx.x; r < count; r += blockDim.x) {
+                    const uint32_t k = bt.first + r;
+                    const uint2 ij = d.d_ij[k];
+                    const float4 m = d.d_mat[k];
+                    const float4 a = pre[ij.x], bb = pre[ij.y];
+                    const V3 diff = xyz(bb) - xyz(a);
+                    const float L = len3(diff);
+                    if (ph.x == ADJ_STRAIN) {
+                        if (!(m.w > 0.0f)) continue;
+                        const float maxL = m.x * (1.0f + m.w);
+                        if (L <= maxL || L < 1.0e-12f) continue;
+                        if (a.w + bb.w <= 0.0f) continue;
+                        // x_a += dir w_a (L - maxL)/den: the distance form with rest maxL, alpha 0
+                        distance_vjp(A.gx, ij.x, ij.y, a, bb, static_cast<double>(maxL), 0.0);
+                    } else {
+                        if (L < 1.0e-12f) continue;
+                        const float alpha = m.y / dt2;
+                        if ((a.w + bb.w) + alpha <= 0.0f) continue;
+                        const double alphad = static_cast<double>(m.y) / (dtd * dtd);
+                        const double galpha =
+                            distance_vjp(A.gx, ij.x, ij.y, a, bb, static_cast<double>(m.x), alphad);
+                        const uint32_t kind = d.d_kind == nullptr ? 0u : min(static_cast<uint32_t>(d.d_kind[k]), 3u);
+                        acc[kind] += galpha * alphad;
+                    }
+                }
+                break;
+            }
+            case ADJ_BEND: {
+                const Batch bt = d.bend_batches[ph.y];
+                for (uint32_t r = threadIdx.x; r < bt.count; r += blockDim.x) {
+                    const uint32_t k = bt.first + r;
+                    const uint4 q = d.b_ij[k];
+                    const float2 m = d.b_mat[k];
+                    const float4 p0 = pre[q.x], p2 = pre[q.z];
+                    const V3 diff = xyz(p2) - xyz(p0);
+                    const float chord = len3(diff);
+                    if (chord < 1.0e-12f) continue;
+                    const float value = chord - m.x;
+                    const V3 dir = vdiv(diff, chord);
+                    const float alpha = m.y / dt2;
+                    float free_den = alpha;
+                    free_den = free_den + p0.w * lsq(dir * -1.0f);
+                    free_den = free_den + p2.w * lsq(dir);
+                    if (free_den < 1.0e-16f) continue;
+                    const float free_dl = -value / free_den;
+                    const bool act0 = ground && p0.z <= radius + 1.0e-9f && -dir.z * free_dl < 0.0f;
+                    const bool act2 = ground && p2.z <= radius + 1.0e-9f && dir.z * free_dl < 0.0f;
+                    if (act0 || act2) {
+                        ++rough;   // ground active set: not differentiated
+                        continue;
+                    }
+                    if (ground) {
+                        const float vc0 = -dir.z * p0.w * free_dl, vc2 = dir.z * p2.w * free_dl;
+                        if ((vc0 < 0.0f && fmaxf(0.0f, p0.z - radius) < -vc0) ||
+                            (vc2 < 0.0f && fmaxf(0.0f, p2.z - radius) < -vc2))
+                            ++rough;   // fraction clamp: not differentiated
+                        if (p0.z + (-dir.z) * (p0.w * free_dl) < radius || p2.z + dir.z * (p2.w * free_dl) < radius)
+                            ++rough;   // clamped to the ground after the bend: not differentiated
+                    }
+                    const double alphad = static_cast<double>(m.y) / (dtd * dtd);
+                    const double galpha = distance_vjp(A.gx, q.x, q.z, p0, p2, static_cast<double>(m.x), alphad);
+                    acc[4] += galpha * alphad;
+                }
+                break;
+            }
+            case ADJ_GRIP: {
+                const bool active = cf.gripTargetAndActive.w > 0.0f;
+                const uint32_t g = threadIdx.x;
+                double gg[6] = {0, 0, 0, 0, 0, 0};
+                if (active && g < d.g_count) {
+                    const NumiClothGrip grip = d.grips[g];
+                    if (grip.particle.y == cf.gripControl.x) {
+                        const uint32_t i = grip.particle.x;
+                        const float4 p = pre[i];
+                        const float alpha = grip.targetOffsetAndCompliance.w / dt2;
+                        if (p.w + alpha > 0.0f) {
+                            const float4 qr = make_float4(cf.gripOrientation.x, cf.gripOrientation.y,
+                                                          cf.gripOrientation.z, cf.gripOrientation.w);
+                            const V3 ro = rotate_q(qr, V3{grip.targetOffsetAndCompliance.x,
+                                                          grip.targetOffsetAndCompliance.y,
+                                                          grip.targetOffsetAndCompliance.z});
+                            const D3v target = addd(D3v{cf.gripTargetAndActive.x, cf.gripTargetAndActive.y,
+                                                        cf.gripTargetAndActive.z},
+                                                    d3f(ro));
+                            const D3v gout = d3(A.gx[i]);
+                            const double w = p.w;
+                            const double al = static_cast<double>(grip.targetOffsetAndCompliance.w) / (dtd * dtd);
+                            const double dn = w + al;
+                            // x' = (alpha x + w T) / (w + alpha)
+                            put(A.gx, i, muld(gout, al / dn));
+                            const D3v gT = muld(gout, w / dn);
+                            const D3v xm = subd(d4f(p), target);
+                            acc[5] += dotd(gout, muld(xm, w / (dn * dn))) * al;
+                            const D3v rot = crossd(d3f(ro), gT);
+                            gg[0] = gT.x;
+                            gg[1] = gT.y;
+                            gg[2] = gT.z;
+                            gg[3] = rot.x;
+                            gg[4] = rot.y;
+                            gg[5] = rot.z;
+                        }
+                    }
+                }
+                if (g < NC_MAX_GRIPS)
+                    for (int e = 0; e < 6; ++e) s_grip[g][e] = gg[e];
+                __syncthreads();
+                if (threadIdx.x == 0 && A.grip_grads != nullptr) {
+                    double* out = A.grip_grads + static_cast<size_t>(step) * 6u;
+                    for (uint32_t k = 0; k < min(d.g_count, NC_MAX_GRIPS); ++k)
+                        for (int e = 0; e < 6; ++e) out[e] += s_grip[k][e];
+                }
+                break;
+            }
+            case ADJ_GROUND:
+                if (ground)
+                    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x)
+                        if (radius - pre[i].z > 0.0f) A.gx[i].z = 0.0;
+                break;
+            case ADJ_BEGIN: {
+                // x' = x_s + v' dt, v' = (v_s + g dt) / (1 + c dt)
+                const float4* vs = A.tape_v + static_cast<size_t>(si) * n;
+                const double c = A.damping;
+                const double kf = c != 0.0 ? 1.0 / (1.0 + c * dtd) : 1.0;
+                const double dk = -dtd / ((1.0 + c * dtd) * (1.0 + c * dtd));
+                const D3v grav{cf.gravityAndTimestep.x, cf.gravityAndTimestep.y, cf.gravityAndTimestep.z};
+                for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+                    if (pre[i].w == 0.0f) {
+                        A.gx[i] = make_double4(0, 0, 0, 0);
+                        A.gv[i] = make_double4(0, 0, 0, 0);
+                        continue;
+                    }
+                    D3v gpos = d3(A.gx[i]);
+                    if (ground && pre[i].z >= radius && post[i].z == radius) {
+                        ++rough;   // swept ground clamp: not differentiated
+                        gpos.z = 0.0;
+                    }
+                    const D3v gvp = muld(gpos, dtd);
+                    const D3v v0 = addd(D3v{vs[i].x, vs[i].y, vs[i].z}, muld(grav, dtd));
+                    acc[6] += dotd(gvp, v0) * dk;
+                    put(A.gv, i, muld(gvp, kf));
+                    put(A.gx, i, addd(gpos, d3(A.gprev[i])));
+                    A.gprev[i] = make_double4(0, 0, 0, 0);
+                }
+                break;
+            }
+            default:
+                break;
+            }
+            __syncthreads();
+        }
+    }
+    // fixed-order block reductions
+    __shared__ double s_red[NC_THREADS];
+    __shared__ unsigned int s_rough;
+    if (threadIdx.x == 0) s_rough = 0u;
+    __syncthreads();
+    if (rough) atomicAdd(&s_rough, rough);
+    for (uint32_t e = 0; e <= ADJ_GRADS; ++e) {
+        s_red[threadIdx.x] = e < ADJ_GRADS ? acc[e] : loss;
+        __syncthreads();
+        for (uint32_t st = blockDim.x / 2u; st > 0u; st >>= 1u) {
+            if (threadIdx.x < st) s_red[threadIdx.x] += s_red[threadIdx.x + st];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            if (e < ADJ_GRADS)
+                A.grads[e] += s_red[0];
+            else
+                *A.loss += s_red[0];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *A.nonsmooth += s_rough;
+}

@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "cloth_frame.cuh"
+#include "cloth_adjoint.cuh"
 #include "numi_cloth.h"
 
 static_assert(sizeof(NumiClothConfig) == 224, "Config layout");
@@ -190,9 +191,9 @@ int make_batches(const Rec* recs, uint32_t count, uint32_t n_targets, ColourFn c
     return NUMI_CLOTH_OK;
 }
 
-cudaError_t launch(numi_cloth* h, uint32_t substeps, const Schedule& s) {
+cudaError_t launch(numi_cloth* h, uint32_t substeps, const Schedule& s, uint32_t cfg_offset = 0) {
     DeviceCloth d = h->d;
-    d.cfg = h->d_cfg;
+    d.cfg = h->d_cfg + cfg_offset;
     d.epoch_base = h->epoch;
     Schedule sc = s;
     sc.substeps = substeps;
@@ -378,6 +379,8 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
     d.d_ij = d_ij;
     d.d_mat = d_mat;
     d.d_lambda = h->buf.alloc<float>(D);
+    uint8_t* d_kind = h->buf.alloc<uint8_t>(D);
+    d.d_kind = d_kind;
     uint4* k_ij = h->buf.alloc<uint4>(K);
     float2* k_mat = h->buf.alloc<float2>(K);
     d.k_ij = k_ij;
@@ -524,7 +527,7 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
     const uint32_t chunks = (n + NC_THREADS - 1u) / NC_THREADS;
     d.red = h->buf.alloc<double>(std::max<size_t>(3u * 4096u, 2u * chunks + 8u));
 
-    bool ok = d.x && d.xp && d.v && rest && d_ij && d_mat && d.d_lambda && k_ij && k_mat && d.k_lambda && b_ij &&
+    bool ok = d.x && d.xp && d.v && rest && d_ij && d_mat && d.d_lambda && d_kind && k_ij && k_mat && d.k_lambda && b_ij &&
               b_mat && d.b_lambda && d.grips && d.fruits && d.pairs && cuff && d.yarn_slot_a && d.yarn_slot_b && d.yarn_live &&
               d.force && d.fruit_partial && d.failure && d.bar_count && d.abort_flag && d.stats && d.red && rim &&
               d.release;
@@ -549,9 +552,11 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
     std::vector<uint2> hij(D);
     std::vector<float4> hdm(D);
     std::vector<float> hdl(D);
+    std::vector<uint8_t> hkind(D);
     for (uint32_t k = 0; k < D; ++k) {
         const NumiClothDistance& r = scene->distances[k];
         hij[k] = make_uint2(r.particlesAndColor.x, r.particlesAndColor.y);
+        hkind[k] = static_cast<uint8_t>(std::min<uint32_t>(r.particlesAndColor.w, 3u));
         hdm[k] = make_float4(r.material.x, r.material.y, 0.0f, r.material.w);
         hdl[k] = r.material.z;
     }
@@ -584,6 +589,7 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
     up(d_ij, hij.data(), D * sizeof(uint2));
     up(d_mat, hdm.data(), D * sizeof(float4));
     up(d.d_lambda, hdl.data(), D * sizeof(float));
+    up(d_kind, hkind.data(), D * sizeof(uint8_t));
     up(k_ij, hkij.data(), K * sizeof(uint4));
     up(k_mat, hkm.data(), K * sizeof(float2));
     up(d.k_lambda, hkl.data(), K * sizeof(float));
@@ -1431,3 +1437,232 @@ int numi_cloth_batch_replay(numi_cloth_batch_t* b) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------
+// Reverse-mode gradients of a rollout (numi_cloth_rollout_grad).
+
+namespace {
+
+// Barrier sequence of one substep for the schedules the adjoint supports
+// (one iteration, no reconciliation / final / certificate passes, no air
+// load, no self contact, no knots): mirrors nc::substep.
+std::vector<uint2> adjoint_phases(const DeviceCloth& d, const Schedule& s) {
+    std::vector<uint2> ph;
+    ph.push_back(make_uint2(ADJ_BEGIN, 0u));
+    for (uint32_t b = 0; b < d.n_dist_batches; ++b) ph.push_back(make_uint2(ADJ_DIST, b));
+    for (uint32_t b = 0; b < d.n_bend_batches; ++b) ph.push_back(make_uint2(ADJ_BEND, b));
+    ph.push_back(make_uint2(ADJ_GRIP, 0u));
+    if (d.f_count > 0u)
+        for (uint32_t b = 0; b < d.n_dist_batches; ++b)
+            if (d.dist_batches[b].yarn != 0u) ph.push_back(make_uint2(ADJ_YARN, b));
+    ph.push_back(make_uint2(ADJ_GROUND, 0u));
+    for (uint32_t sw = 0; sw < s.strain_sweeps; ++sw)
+        for (uint32_t b = 0; b < d.n_dist_batches; ++b)
+            if (d.dist_batches[b].limited != 0u) ph.push_back(make_uint2(ADJ_STRAIN, b));
+    ph.push_back(make_uint2(ADJ_FINAL, 0u));
+    if (s.frictions && d.f_count > 0u)
+        for (uint32_t b = 0; b < d.n_dist_batches; ++b)
+            if (d.dist_batches[b].yarn != 0u) ph.push_back(make_uint2(ADJ_YFRIC, b));
+    ph.push_back(make_uint2(ADJ_TAIL, 0u));
+    return ph;
+}
+
+// Device allocations of one rollout, freed on scope exit.
+struct Scratch {
+    std::vector<void*> owned;
+    template <class T>
+    T* get(size_t count) {
+        void* p = nullptr;
+        if (cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)) != cudaSuccess) return nullptr;
+        cudaMemset(p, 0, std::max<size_t>(count, 1) * sizeof(T));
+        owned.push_back(p);
+        return static_cast<T*>(p);
+    }
+    ~Scratch() {
+        for (void* p : owned) cudaFree(p);
+    }
+};
+
+}  // namespace
+
+extern "C" int numi_cloth_rollout_grad(numi_cloth_t* h, const NumiClothConfig* configs, uint32_t substeps,
+                                       const NumiClothSchedule* schedule, uint32_t checkpoint_every,
+                                       const uint32_t* tracked, uint32_t n_tracked, const double* targets,
+                                       uint32_t loss_every, double* loss, double grads[NUMI_CLOTH_GRADS],
+                                       double* grip_grads, uint32_t* nonsmooth) {
+    if (h == nullptr || configs == nullptr || schedule == nullptr || substeps == 0 || checkpoint_every == 0 ||
+        loss == nullptr || grads == nullptr || (n_tracked > 0 && (tracked == nullptr || targets == nullptr)) ||
+        loss_every == 0)
+        return NUMI_CLOTH_EINVAL;
+    if (h->poisoned) return NUMI_CLOTH_ESTATE;
+    const NumiClothSchedule& sc = *schedule;
+    if (sc.iterations != 1u || sc.reconcilePasses != 0u || sc.finalPasses != 0u || sc.certificatePasses != 0u ||
+        sc.aerodynamics != 0u || sc.selfCollision != 0u || h->d.k_count != 0u)
+        return NUMI_CLOTH_EINVAL;
+    for (uint32_t t = 0; t < n_tracked; ++t)
+        if (tracked[t] >= h->d.n) return NUMI_CLOTH_EINVAL;
+    cudaSetDevice(h->device);
+    for (uint32_t k = 0; k < substeps; ++k) {
+        const uint32_t bad = validate_config(configs[k], h->base);
+        if (bad) {
+            h->host_failure |= bad;
+            return static_cast<int>(bad);
+        }
+    }
+    if (substeps > h->cfg_capacity) {
+        cudaFree(h->d_cfg);
+        h->d_cfg = nullptr;
+        if (cudaMalloc(&h->d_cfg, substeps * sizeof(NumiClothConfig)) != cudaSuccess) return NUMI_CLOTH_ECUDA;
+        h->cfg_capacity = substeps;
+    }
+    if (cudaMemcpyAsync(h->d_cfg, configs, substeps * sizeof(NumiClothConfig), cudaMemcpyHostToDevice, h->stream) !=
+        cudaSuccess)
+        return NUMI_CLOTH_ECUDA;
+    const Schedule s = device_schedule(sc);
+    const std::vector<uint2> phases = adjoint_phases(h->d, s);
+    const uint32_t slots = static_cast<uint32_t>(phases.size()) + 1u;
+    const uint32_t n = h->d.n;
+    const uint32_t segs = (substeps + checkpoint_every - 1u) / checkpoint_every;
+    const uint32_t losses = substeps / loss_every;
+
+    Scratch mem;
+    size_t state_bytes = 0;
+    for (const auto& r : h->dynamic) state_bytes += (r.bytes + 255u) & ~size_t(255u);
+    char* ckpt = mem.get<char>((segs + 1u) * state_bytes);
+    float4* tape = mem.get<float4>(static_cast<size_t>(checkpoint_every) * slots * n);
+    float4* tape_v = mem.get<float4>(static_cast<size_t>(checkpoint_every) * n);
+    uint2* d_phases = mem.get<uint2>(phases.size());
+    DeviceCloth* d_cloth = mem.get<DeviceCloth>(1);
+    uint32_t* d_tracked = mem.get<uint32_t>(n_tracked);
+    double* d_targets = mem.get<double>(static_cast<size_t>(losses) * n_tracked * 3u);
+    double4* gx = mem.get<double4>(n);
+    double4* gv = mem.get<double4>(n);
+    double4* gprev = mem.get<double4>(n);
+    double* d_out = mem.get<double>(NUMI_CLOTH_GRADS + 1u);   // grads, loss
+    double* d_grip = mem.get<double>(static_cast<size_t>(substeps) * 6u);
+    unsigned int* d_rough = mem.get<unsigned int>(1);
+    if (!ckpt || !tape || !tape_v || !d_phases || !d_cloth || !d_tracked || !d_targets || !gx || !gv || !gprev ||
+        !d_out || !d_grip || !d_rough)
+        return NUMI_CLOTH_ENOMEM;
+    cudaError_t e = cudaMemcpyAsync(d_phases, phases.data(), phases.size() * sizeof(uint2), cudaMemcpyHostToDevice,
+                                    h->stream);
+    if (e == cudaSuccess && n_tracked)
+        e = cudaMemcpyAsync(d_tracked, tracked, n_tracked * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess && n_tracked && losses)
+        e = cudaMemcpyAsync(d_targets, targets, static_cast<size_t>(losses) * n_tracked * 3u * sizeof(double),
+                            cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_cloth, &h->d, sizeof(DeviceCloth), cudaMemcpyHostToDevice, h->stream);
+    if (e != cudaSuccess) return NUMI_CLOTH_ECUDA;
+
+    auto save = [&](uint32_t slot) {
+        size_t off = 0;
+        for (const auto& r : h->dynamic) {
+            if (cudaMemcpyAsync(ckpt + slot * state_bytes + off, r.ptr, r.bytes, cudaMemcpyDeviceToDevice, h->stream) !=
+                cudaSuccess)
+                return false;
+            off += (r.bytes + 255u) & ~size_t(255u);
+        }
+        return true;
+    };
+    auto load = [&](uint32_t slot) {
+        size_t off = 0;
+        for (const auto& r : h->dynamic) {
+            if (cudaMemcpyAsync(r.ptr, ckpt + slot * state_bytes + off, r.bytes, cudaMemcpyDeviceToDevice, h->stream) !=
+                cudaSuccess)
+                return false;
+            off += (r.bytes + 255u) & ~size_t(255u);
+        }
+        return true;
+    };
+
+    // forward in the handle's own launch shape, checkpointing every segment
+    std::vector<uint32_t> seg_epoch(segs);
+    for (uint32_t g = 0; g < segs; ++g) {
+        const uint32_t first = g * checkpoint_every;
+        const uint32_t count = std::min(checkpoint_every, substeps - first);
+        seg_epoch[g] = h->epoch;
+        if (!save(g)) return NUMI_CLOTH_ECUDA;
+        e = launch(h, count, s, first);
+        h->epoch += count;
+        if (e != cudaSuccess) {
+            h->poisoned = true;
+            return NUMI_CLOTH_ECUDA;
+        }
+    }
+    const uint32_t end_epoch = h->epoch;
+    if (!save(segs)) return NUMI_CLOTH_ECUDA;
+
+    // backward: replay each segment on one CTA with the tape, then reverse it
+    const float damping = h->d.damping >= 0.0f ? h->d.damping : s.damping;
+    const bool resident_one = h->d.resident != 0u && h->grid == 1u;
+    for (uint32_t g = segs; g-- > 0u;) {
+        const uint32_t first = g * checkpoint_every;
+        const uint32_t count = std::min(checkpoint_every, substeps - first);
+        if (!load(g)) return NUMI_CLOTH_ECUDA;
+        DeviceCloth d = h->d;
+        d.cfg = h->d_cfg + first;
+        d.epoch_base = seg_epoch[g];
+        d.trace = nullptr;
+        d.trace_cta = nullptr;
+        d.cluster_barrier = 0u;
+        d.resident = resident_one ? 1u : 0u;
+        d.tape = tape;
+        d.tape_v = tape_v;
+        d.tape_slots = slots;
+        Schedule st = s;
+        st.substeps = count;
+        const size_t smem = resident_one ? h->smem : nc_resident_offset();
+        numi_cloth_frame_kernel<<<1, h->block, smem, h->stream>>>(d, st);
+        AdjointArgs A{};
+        A.cloth = d_cloth;
+        A.cfg = h->d_cfg + first;
+        A.tape = tape;
+        A.tape_v = tape_v;
+        A.phases = d_phases;
+        A.slots = slots;
+        A.substeps = count;
+        A.first_substep = first;
+        A.damping = damping;
+        A.tracked = d_tracked;
+        A.n_tracked = n_tracked;
+        A.targets = d_targets;
+        A.loss_every = loss_every;
+        A.gx = gx;
+        A.gv = gv;
+        A.gprev = gprev;
+        A.grads = d_out;
+        A.loss = d_out + NUMI_CLOTH_GRADS;
+        A.grip_grads = d_grip;
+        A.nonsmooth = d_rough;
+        numi_cloth_adjoint_kernel<<<1, NC_THREADS, 0, h->stream>>>(A);
+        if (cudaGetLastError() != cudaSuccess) {
+            h->poisoned = true;
+            return NUMI_CLOTH_ECUDA;
+        }
+        uint32_t barriers = 0;
+        if (cudaMemcpyAsync(&barriers, h->d.stats, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
+            cudaStreamSynchronize(h->stream) != cudaSuccess) {
+            h->poisoned = true;
+            return NUMI_CLOTH_ECUDA;
+        }
+        if (barriers + 1u != slots) return NUMI_CLOTH_ESTATE;   // the phase list does not match the kernel
+    }
+    if (!load(segs)) return NUMI_CLOTH_ECUDA;
+    h->epoch = end_epoch;
+    double out[NUMI_CLOTH_GRADS + 1u];
+    unsigned int rough = 0;
+    e = cudaMemcpyAsync(out, d_out, sizeof(out), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&rough, d_rough, sizeof(rough), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess && grip_grads)
+        e = cudaMemcpyAsync(grip_grads, d_grip, static_cast<size_t>(substeps) * 6u * sizeof(double),
+                            cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) {
+        h->poisoned = true;
+        return NUMI_CLOTH_ECUDA;
+    }
+    for (uint32_t k = 0; k < NUMI_CLOTH_GRADS; ++k) grads[k] = out[k];
+    *loss = out[NUMI_CLOTH_GRADS];
+    if (nonsmooth) *nonsmooth = rough;
+    return NUMI_CLOTH_OK;
+}

@@ -51,6 +51,7 @@ struct DeviceCloth {
     // distances
     const uint2* d_ij;
     const float4* d_mat;
+    const uint8_t* d_kind;   // distance kind (warp, weft, bottom, shear) or null
     float* d_lambda;
     uint32_t d_count;
     // knots
@@ -132,6 +133,12 @@ struct DeviceCloth {
     // [0] self contacts (a < b pairs resolved), [1] max self penetration
     // (float bits; non-negative so unsigned max orders them)
     unsigned long long* self_stats;
+    // adjoint tape (one-CTA launches only): positions at the start of every
+    // substep and after every barrier, [substep][tape_slots][n], and
+    // velocities at the start of every substep, [substep][n]
+    float4* tape;
+    float4* tape_v;
+    uint32_t tape_slots;
 };
 
 struct Schedule {

@@ -31,6 +31,12 @@ __device__ bool grid_sync(Ctx& ctx) {
     }
     if (ctx.ranks == 1) {
         __syncthreads();
+        if (d.tape != nullptr && ctx.barriers < d.tape_slots) {
+            // adjoint tape: positions after this barrier
+            float4* slot = d.tape + (static_cast<size_t>(ctx.sub) * d.tape_slots + ctx.barriers) * d.n;
+            for (uint32_t i = threadIdx.x; i < d.n; i += blockDim.x) slot[i] = px(ctx, i);
+            __syncthreads();
+        }
         if (d.trace && threadIdx.x == 0 && ctx.barriers <= NC_TRACE_SLOTS)
             d.trace[static_cast<size_t>(ctx.sub) * NC_TRACE_SLOTS + ctx.barriers - 1u] = globaltimer();
         return true;
@@ -1396,6 +1402,15 @@ __device__ __forceinline__ void run_frame(const DeviceCloth& src, const Schedule
         ctx.c = nc::load_cfg(d.cfg + sub);
         ctx.epoch = epoch_base + sub;
         ctx.barriers = 0;
+        if (d.tape != nullptr && ranks == 1u) {
+            // adjoint tape: state at the start of the substep
+            float4* slot = d.tape + static_cast<size_t>(sub) * d.tape_slots * d.n;
+            for (uint32_t i = threadIdx.x; i < d.n; i += blockDim.x) {
+                slot[i] = px(ctx, i);
+                d.tape_v[static_cast<size_t>(sub) * d.n + i] = pv(ctx, i);
+            }
+            __syncthreads();
+        }
         if (!nc::substep(ctx, sub + 1u == s.substeps)) return;
         if (rank == 0 && threadIdx.x == 0) d.stats[0] = ctx.barriers;
     }
