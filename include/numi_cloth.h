@@ -338,33 +338,43 @@ int numi_cloth_step_noalloc(const NumiClothConfig* base, const NumiClothDeviceSt
  * outside the simulator (docs/CLOTH_SPECIMEN_CALIBRATION.md:52-82); this
  * feeds a gradient-based fitter.
  *
- * Advances the cloth by `substeps` substeps (configs as numi_cloth_step),
- * checkpointing the state every `checkpoint_every` substeps, and returns the
- * loss L = sum over the substeps s with (s + 1) % loss_every == 0 of
+ * Compliance groups are the distinct compliance values of each constraint
+ * family (family 0 distance, 1 knot, 2 bend, 3 grip), ascending, family by
+ * family: on the produce bag the axial body and cuff distances, the knots,
+ * the bend body and cuff, and the grips; on a square cloth the stretch and
+ * shear distances, the bends and the grips.  numi_cloth_compliance_groups
+ * lists them (at most NUMI_CLOTH_MAX_GROUPS); numi_cloth_replace_compliance
+ * sets every record of `family` whose compliance equals `from` to `to`
+ * (how a fitter applies a new group value).
+ *
+ * numi_cloth_rollout_grad advances the cloth by `substeps` substeps
+ * (configs as numi_cloth_step), checkpointing the state every
+ * `checkpoint_every` substeps, and returns the loss L = sum over the
+ * substeps s with (s + 1) % loss_every == 0 of
  * sum_t |x_tracked[t](s) - target(s, t)|^2 (targets: [substeps / loss_every]
  * [n_tracked][3], m) and its gradients, reduced in FP64:
- *   grads[0..3] dL / d log-compliance scale of the distance kinds warp,
- *               weft, bottom, shear (all records of the kind scaled together);
- *   grads[4]    dL / d log-compliance scale of the bends;
- *   grads[5]    dL / d log-compliance scale of the grips;
- *   grads[6]    dL / d damping c (v <- v / (1 + c dt));
- *   grip_grads  (optional, [substeps][6]) dL / d grip target position xyz
- *               and dL / d a small rotation (axis-angle, applied before the
- *               grip orientation) of each substep's Config.
+ *   grads[g]      dL / d log-scale of compliance group g (count + 1 entries);
+ *   grads[count]  dL / d damping c (v <- v / (1 + c dt));
+ *   grip_grads    (optional, [substeps][6]) dL / d grip target position xyz
+ *                 and dL / d a small rotation (axis-angle, applied before
+ *                 the grip orientation) of each substep's Config.
  * The state after the call is the state after the rollout.
  *
  * Supported schedules: iterations = 1, no reconciliation, final or
- * certificate passes, aerodynamics = 0, selfCollision = 0; cloths without
- * knots.  Fruit contacts, cloth/ground friction, the swept ground and bend
- * ground active sets are not differentiated: the number of such events met
- * is returned in *nonsmooth (0 = the gradient is exact for the discrete
- * forward).  Returns NUMI_CLOTH_EINVAL for unsupported schedules. */
-#define NUMI_CLOTH_GRADS 7u
+ * certificate passes, aerodynamics = 0, selfCollision = 0.  Fruit contacts,
+ * cloth/ground friction, the swept ground and bend ground active sets are
+ * not differentiated: the number of such events met is returned in
+ * *nonsmooth (0 = the gradient is exact for the discrete forward).  Returns
+ * NUMI_CLOTH_EINVAL for unsupported schedules. */
+#define NUMI_CLOTH_MAX_GROUPS 16u
+int numi_cloth_compliance_groups(numi_cloth_t* handle, uint32_t family[NUMI_CLOTH_MAX_GROUPS],
+                                 float compliance[NUMI_CLOTH_MAX_GROUPS], uint32_t* count);
+int numi_cloth_replace_compliance(numi_cloth_t* handle, uint32_t family, float from, float to);
 int numi_cloth_rollout_grad(numi_cloth_t* handle, const NumiClothConfig* configs, uint32_t substeps,
                             const NumiClothSchedule* schedule, uint32_t checkpoint_every,
                             const uint32_t* tracked, uint32_t n_tracked, const double* targets,
-                            uint32_t loss_every, double* loss, double grads[NUMI_CLOTH_GRADS],
-                            double* grip_grads, uint32_t* nonsmooth);
+                            uint32_t loss_every, double* loss, double* grads, double* grip_grads,
+                            uint32_t* nonsmooth);
 
 /* ------------------------------------------------------------------------
  * Batched stepping: many independent cloths (same device) advanced by one

@@ -12,7 +12,7 @@
 // parameter gradients are accumulated in FP64.
 //
 // Differentiated: predict with gravity and damping, XPBD distance / shear /
-// bend projections (one iteration, so lambda starts at zero), compliant
+// knot / bend projections (one iteration, so lambda starts at zero), compliant
 // grips, the ground clamp, unilateral strain limits, finalize.  The other
 // phases (fruit pairs, fruit/yarn contact and friction, cloth/ground
 // friction, swept ground, bend ground active sets) are non-smooth; where one
@@ -23,6 +23,7 @@
 #include "cloth_kernels.cuh"
 
 enum AdjointPhase : uint32_t {
+    ADJ_KNOT = 10,
     ADJ_BEGIN = 0,
     ADJ_DIST = 1,
     ADJ_BEND = 2,
@@ -35,9 +36,10 @@ enum AdjointPhase : uint32_t {
     ADJ_TAIL = 9,
 };
 
-// Gradient slots: d loss / d log compliance of distance kinds warp, weft,
-// bottom, shear; of bends; of grips; d loss / d damping.
-#define ADJ_GRADS 7u
+// Gradients: d loss / d log-scale of each compliance group (the distinct
+// compliance values of each constraint family, numbered by the host), then
+// d loss / d damping.
+#define ADJ_MAX_GROUPS 16u
 
 struct AdjointArgs {
     const DeviceCloth* cloth;        // device copy of the handle's descriptor
@@ -56,7 +58,12 @@ struct AdjointArgs {
     double4* gx;                     // [n] adjoint of positions (xyz; w unused)
     double4* gv;                     // [n] adjoint of velocities
     double4* gprev;                  // [n] scratch: adjoint of the substep's start positions via finalize
-    double* grads;                   // [ADJ_GRADS] accumulated
+    const uint8_t* d_group;          // [distances] compliance group
+    const uint8_t* k_group;          // [knots]
+    const uint8_t* b_group;          // [bends]
+    const uint8_t* g_group;          // [grips]
+    uint32_t groups;
+    double* grads;                   // [groups + 1] accumulated (groups, then damping)
     double* grip_grads;              // [rollout substeps][6] or null
     double* loss;                    // [1] accumulated
     unsigned int* nonsmooth;         // [1] count of non-smooth events met
@@ -98,13 +105,64 @@ __device__ __forceinline__ double distance_vjp(double4* gx, uint32_t ia, uint32_
     return -un * dl / den;
 }
 
+// Forward-mode dual number (value, one tangent) for the knot projection,
+// whose Jacobian involves the derivatives of its own gradients.
+struct Dual {
+    double v, d;
+};
+__device__ __forceinline__ Dual operator+(Dual a, Dual b) { return Dual{a.v + b.v, a.d + b.d}; }
+__device__ __forceinline__ Dual operator-(Dual a, Dual b) { return Dual{a.v - b.v, a.d - b.d}; }
+__device__ __forceinline__ Dual operator*(Dual a, Dual b) { return Dual{a.v * b.v, a.d * b.v + a.v * b.d}; }
+__device__ __forceinline__ Dual operator/(Dual a, Dual b) {
+    return Dual{a.v / b.v, (a.d * b.v - a.v * b.d) / (b.v * b.v)};
+}
+__device__ __forceinline__ Dual dsqrt(Dual a) {
+    const double r = sqrt(a.v);
+    return Dual{r, a.d / (2.0 * r)};
+}
+struct DV {
+    Dual x, y, z;
+};
+__device__ __forceinline__ DV operator-(DV a, DV b) { return DV{a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ DV operator*(DV a, Dual s) { return DV{a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ Dual ddot(DV a, DV b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+
+// Knot projection (nc::solve_knot with lambda from zero) on dual numbers:
+// positions p[4], inverse masses w[4], compliance alpha; writes out[4].
+__device__ __forceinline__ void knot_dual(const DV p[4], const double w[4], Dual alpha, double rest, DV out[4]) {
+    const DV warpv = p[1] - p[0];
+    const DV weftv = p[3] - p[2];
+    const Dual wl = dsqrt(ddot(warpv, warpv));
+    const Dual fl = dsqrt(ddot(weftv, weftv));
+    const Dual one{1.0, 0.0};
+    const DV warp = warpv * (one / wl);
+    const DV weft = weftv * (one / fl);
+    Dual cosine = ddot(warp, weft);
+    if (cosine.v > 1.0) cosine = Dual{1.0, 0.0};
+    if (cosine.v < -1.0) cosine = Dual{-1.0, 0.0};
+    const Dual value = cosine - Dual{rest, 0.0};
+    const DV gw = (weft - warp * cosine) * (one / wl);
+    const DV gf = (warp - weft * cosine) * (one / fl);
+    const Dual W[4] = {{w[0], 0.0}, {w[1], 0.0}, {w[2], 0.0}, {w[3], 0.0}};
+    const Dual den = alpha + W[0] * ddot(gw, gw) + W[1] * ddot(gw, gw) + W[2] * ddot(gf, gf) + W[3] * ddot(gf, gf);
+    const Dual dl = Dual{0.0, 0.0} - value / den;
+    const Dual zero{0.0, 0.0};
+    const DV g[4] = {DV{zero, zero, zero} - gw, gw, DV{zero, zero, zero} - gf, gf};
+    for (int q = 0; q < 4; ++q) {
+        const Dual s = W[q] * dl;
+        out[q] = DV{p[q].x + g[q].x * s, p[q].y + g[q].y * s, p[q].z + g[q].z * s};
+    }
+}
+
 }  // namespace adj
 
 __global__ void __launch_bounds__(NC_THREADS) numi_cloth_adjoint_kernel(AdjointArgs A) {
     using namespace adj;
     const DeviceCloth& d = *A.cloth;
     const uint32_t n = d.n;
-    double acc[ADJ_GRADS] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    double acc[ADJ_MAX_GROUPS + 1u];
+    for (uint32_t e = 0; e <= ADJ_MAX_GROUPS; ++e) acc[e] = 0.0;
+    const uint32_t damp_slot = A.groups;
     double loss = 0.0;
     unsigned int rough = 0u;
     __shared__ double s_grip[NC_MAX_GRIPS][6];
@@ -187,9 +245,63 @@ __global__ void __launch_bounds__(NC_THREADS) numi_cloth_adjoint_kernel(AdjointA
                         const double alphad = static_cast<double>(m.y) / (dtd * dtd);
                         const double galpha =
                             distance_vjp(A.gx, ij.x, ij.y, a, bb, static_cast<double>(m.x), alphad);
-                        const uint32_t kind = d.d_kind == nullptr ? 0u : min(static_cast<uint32_t>(d.d_kind[k]), 3u);
-                        acc[kind] += galpha * alphad;
+                        acc[A.d_group[k]] += galpha * alphad;
                     }
+                }
+                break;
+            }
+            case ADJ_KNOT: {
+                const Batch bt = d.knot_batches[ph.y];
+                for (uint32_t r = threadIdx.x; r < bt.count; r += blockDim.x) {
+                    const uint32_t k = bt.first + r;
+                    const uint4 q = d.k_ij[k];
+                    const float2 m = d.k_mat[k];
+                    const uint32_t idx[4] = {q.x, q.y, q.z, q.w};
+                    float4 p[4];
+                    for (int e = 0; e < 4; ++e) p[e] = pre[idx[e]];
+                    // the forward's own skip tests, in FP32
+                    const float wl = len3(xyz(p[1]) - xyz(p[0]));
+                    const float fl = len3(xyz(p[3]) - xyz(p[2]));
+                    if (wl < 1.0e-12f || fl < 1.0e-12f) continue;
+                    const V3 warp = vdiv(xyz(p[1]) - xyz(p[0]), wl);
+                    const V3 weft = vdiv(xyz(p[3]) - xyz(p[2]), fl);
+                    const float cosine = fminf(fmaxf(dot3(warp, weft), -1.0f), 1.0f);
+                    const V3 gw = vdiv(weft - warp * cosine, wl);
+                    const V3 gf = vdiv(warp - weft * cosine, fl);
+                    const float alpha = m.y / dt2;
+                    float den = alpha;
+                    den = den + p[0].w * lsq(gw * -1.0f);
+                    den = den + p[1].w * lsq(gw);
+                    den = den + p[2].w * lsq(gf * -1.0f);
+                    den = den + p[3].w * lsq(gf);
+                    if (den <= 0.0f) continue;
+                    // VJP by forward mode: one tangent per input (12 coordinates, alpha)
+                    double u[12];
+                    for (int e = 0; e < 4; ++e) {
+                        const double4 ge = A.gx[idx[e]];
+                        u[3 * e] = ge.x;
+                        u[3 * e + 1] = ge.y;
+                        u[3 * e + 2] = ge.z;
+                    }
+                    const double w[4] = {p[0].w, p[1].w, p[2].w, p[3].w};
+                    const double alphad = static_cast<double>(m.y) / (dtd * dtd);
+                    double gin[13];
+                    for (int dir = 0; dir < 13; ++dir) {
+                        DV pd[4];
+                        for (int e = 0; e < 4; ++e) {
+                            pd[e] = DV{Dual{p[e].x, dir == 3 * e ? 1.0 : 0.0}, Dual{p[e].y, dir == 3 * e + 1 ? 1.0 : 0.0},
+                                       Dual{p[e].z, dir == 3 * e + 2 ? 1.0 : 0.0}};
+                        }
+                        DV out[4];
+                        knot_dual(pd, w, Dual{alphad, dir == 12 ? 1.0 : 0.0}, static_cast<double>(m.x), out);
+                        double acc_dir = 0.0;
+                        for (int e = 0; e < 4; ++e)
+                            acc_dir += u[3 * e] * out[e].x.d + u[3 * e + 1] * out[e].y.d + u[3 * e + 2] * out[e].z.d;
+                        gin[dir] = acc_dir;
+                    }
+                    for (int e = 0; e < 4; ++e)
+                        A.gx[idx[e]] = make_double4(gin[3 * e], gin[3 * e + 1], gin[3 * e + 2], 0.0);
+                    acc[A.k_group[k]] += gin[12] * alphad;
                 }
                 break;
             }
@@ -227,7 +339,7 @@ __global__ void __launch_bounds__(NC_THREADS) numi_cloth_adjoint_kernel(AdjointA
                     }
                     const double alphad = static_cast<double>(m.y) / (dtd * dtd);
                     const double galpha = distance_vjp(A.gx, q.x, q.z, p0, p2, static_cast<double>(m.x), alphad);
-                    acc[4] += galpha * alphad;
+                    acc[A.b_group[k]] += galpha * alphad;
                 }
                 break;
             }
@@ -258,7 +370,7 @@ __global__ void __launch_bounds__(NC_THREADS) numi_cloth_adjoint_kernel(AdjointA
                             put(A.gx, i, muld(gout, al / dn));
                             const D3v gT = muld(gout, w / dn);
                             const D3v xm = subd(d4f(p), target);
-                            acc[5] += dotd(gout, muld(xm, w / (dn * dn))) * al;
+                            acc[A.g_group[g]] += dotd(gout, muld(xm, w / (dn * dn))) * al;
                             const D3v rot = crossd(d3f(ro), gT);
                             gg[0] = gT.x;
                             gg[1] = gT.y;
@@ -304,7 +416,7 @@ __global__ void __launch_bounds__(NC_THREADS) numi_cloth_adjoint_kernel(AdjointA
                     }
                     const D3v gvp = muld(gpos, dtd);
                     const D3v v0 = addd(D3v{vs[i].x, vs[i].y, vs[i].z}, muld(grav, dtd));
-                    acc[6] += dotd(gvp, v0) * dk;
+                    acc[damp_slot] += dotd(gvp, v0) * dk;
                     put(A.gv, i, muld(gvp, kf));
                     put(A.gx, i, addd(gpos, d3(A.gprev[i])));
                     A.gprev[i] = make_double4(0, 0, 0, 0);
@@ -323,15 +435,15 @@ __global__ void __launch_bounds__(NC_THREADS) numi_cloth_adjoint_kernel(AdjointA
     if (threadIdx.x == 0) s_rough = 0u;
     __syncthreads();
     if (rough) atomicAdd(&s_rough, rough);
-    for (uint32_t e = 0; e <= ADJ_GRADS; ++e) {
-        s_red[threadIdx.x] = e < ADJ_GRADS ? acc[e] : loss;
+    for (uint32_t e = 0; e <= A.groups + 1u; ++e) {
+        s_red[threadIdx.x] = e <= A.groups ? acc[e] : loss;
         __syncthreads();
         for (uint32_t st = blockDim.x / 2u; st > 0u; st >>= 1u) {
             if (threadIdx.x < st) s_red[threadIdx.x] += s_red[threadIdx.x + st];
             __syncthreads();
         }
         if (threadIdx.x == 0) {
-            if (e < ADJ_GRADS)
+            if (e <= A.groups)
                 A.grads[e] += s_red[0];
             else
                 *A.loss += s_red[0];

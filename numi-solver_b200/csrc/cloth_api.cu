@@ -379,8 +379,6 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
     d.d_ij = d_ij;
     d.d_mat = d_mat;
     d.d_lambda = h->buf.alloc<float>(D);
-    uint8_t* d_kind = h->buf.alloc<uint8_t>(D);
-    d.d_kind = d_kind;
     uint4* k_ij = h->buf.alloc<uint4>(K);
     float2* k_mat = h->buf.alloc<float2>(K);
     d.k_ij = k_ij;
@@ -527,7 +525,7 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
     const uint32_t chunks = (n + NC_THREADS - 1u) / NC_THREADS;
     d.red = h->buf.alloc<double>(std::max<size_t>(3u * 4096u, 2u * chunks + 8u));
 
-    bool ok = d.x && d.xp && d.v && rest && d_ij && d_mat && d.d_lambda && d_kind && k_ij && k_mat && d.k_lambda && b_ij &&
+    bool ok = d.x && d.xp && d.v && rest && d_ij && d_mat && d.d_lambda && k_ij && k_mat && d.k_lambda && b_ij &&
               b_mat && d.b_lambda && d.grips && d.fruits && d.pairs && cuff && d.yarn_slot_a && d.yarn_slot_b && d.yarn_live &&
               d.force && d.fruit_partial && d.failure && d.bar_count && d.abort_flag && d.stats && d.red && rim &&
               d.release;
@@ -552,11 +550,9 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
     std::vector<uint2> hij(D);
     std::vector<float4> hdm(D);
     std::vector<float> hdl(D);
-    std::vector<uint8_t> hkind(D);
     for (uint32_t k = 0; k < D; ++k) {
         const NumiClothDistance& r = scene->distances[k];
         hij[k] = make_uint2(r.particlesAndColor.x, r.particlesAndColor.y);
-        hkind[k] = static_cast<uint8_t>(std::min<uint32_t>(r.particlesAndColor.w, 3u));
         hdm[k] = make_float4(r.material.x, r.material.y, 0.0f, r.material.w);
         hdl[k] = r.material.z;
     }
@@ -589,7 +585,6 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
     up(d_ij, hij.data(), D * sizeof(uint2));
     up(d_mat, hdm.data(), D * sizeof(float4));
     up(d.d_lambda, hdl.data(), D * sizeof(float));
-    up(d_kind, hkind.data(), D * sizeof(uint8_t));
     up(k_ij, hkij.data(), K * sizeof(uint4));
     up(k_mat, hkm.data(), K * sizeof(float2));
     up(d.k_lambda, hkl.data(), K * sizeof(float));
@@ -1445,11 +1440,12 @@ namespace {
 
 // Barrier sequence of one substep for the schedules the adjoint supports
 // (one iteration, no reconciliation / final / certificate passes, no air
-// load, no self contact, no knots): mirrors nc::substep.
+// load, no self contact): mirrors nc::substep.
 std::vector<uint2> adjoint_phases(const DeviceCloth& d, const Schedule& s) {
     std::vector<uint2> ph;
     ph.push_back(make_uint2(ADJ_BEGIN, 0u));
     for (uint32_t b = 0; b < d.n_dist_batches; ++b) ph.push_back(make_uint2(ADJ_DIST, b));
+    for (uint32_t b = 0; b < d.n_knot_batches; ++b) ph.push_back(make_uint2(ADJ_KNOT, b));
     for (uint32_t b = 0; b < d.n_bend_batches; ++b) ph.push_back(make_uint2(ADJ_BEND, b));
     ph.push_back(make_uint2(ADJ_GRIP, 0u));
     if (d.f_count > 0u)
@@ -1483,13 +1479,112 @@ struct Scratch {
     }
 };
 
+// Compliance groups: the distinct compliance values of each constraint
+// family (distance, knot, bend, grip), ascending, numbered family by family.
+struct Groups {
+    std::vector<uint32_t> family;
+    std::vector<float> value;
+    std::vector<uint8_t> d, k, b, g;   // per record
+};
+
+int compliance_groups(numi_cloth* h, Groups& out) {
+    const DeviceCloth& d = h->d;
+    std::vector<float4> dm(d.d_count);
+    std::vector<float2> km(d.k_count), bm(d.b_count);
+    std::vector<NumiClothGrip> gr(d.g_count);
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e == cudaSuccess && d.d_count) e = cudaMemcpy(dm.data(), d.d_mat, d.d_count * sizeof(float4), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && d.k_count) e = cudaMemcpy(km.data(), d.k_mat, d.k_count * sizeof(float2), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && d.b_count) e = cudaMemcpy(bm.data(), d.b_mat, d.b_count * sizeof(float2), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && d.g_count)
+        e = cudaMemcpy(gr.data(), d.grips, d.g_count * sizeof(NumiClothGrip), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return NUMI_CLOTH_ECUDA;
+    auto assign = [&](uint32_t family, const std::vector<float>& values, std::vector<uint8_t>& ids) {
+        std::vector<float> distinct = values;
+        std::sort(distinct.begin(), distinct.end());
+        distinct.erase(std::unique(distinct.begin(), distinct.end()), distinct.end());
+        const uint32_t base = static_cast<uint32_t>(out.value.size());
+        for (float v : distinct) {
+            out.family.push_back(family);
+            out.value.push_back(v);
+        }
+        ids.resize(values.size());
+        for (size_t r = 0; r < values.size(); ++r)
+            ids[r] = static_cast<uint8_t>(
+                base + (std::lower_bound(distinct.begin(), distinct.end(), values[r]) - distinct.begin()));
+    };
+    std::vector<float> v;
+    v.clear();
+    for (const float4& m : dm) v.push_back(m.y);
+    assign(0u, v, out.d);
+    v.clear();
+    for (const float2& m : km) v.push_back(m.y);
+    assign(1u, v, out.k);
+    v.clear();
+    for (const float2& m : bm) v.push_back(m.y);
+    assign(2u, v, out.b);
+    v.clear();
+    for (const NumiClothGrip& g : gr) v.push_back(g.targetOffsetAndCompliance.w);
+    assign(3u, v, out.g);
+    return out.value.size() <= NUMI_CLOTH_MAX_GROUPS ? NUMI_CLOTH_OK : NUMI_CLOTH_EINVAL;
+}
+
+__global__ void numi_cloth_replace_compliance_kernel(DeviceCloth d, uint32_t family, float from, float to) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;; k += stride) {
+        bool any = false;
+        if (family == 0u && k < d.d_count) {
+            any = true;
+            float4* m = const_cast<float4*>(d.d_mat) + k;
+            if (m->y == from) m->y = to;
+        }
+        if (family == 1u && k < d.k_count) {
+            any = true;
+            float2* m = const_cast<float2*>(d.k_mat) + k;
+            if (m->y == from) m->y = to;
+        }
+        if (family == 2u && k < d.b_count) {
+            any = true;
+            float2* m = const_cast<float2*>(d.b_mat) + k;
+            if (m->y == from) m->y = to;
+        }
+        if (family == 3u && k < d.g_count) {
+            any = true;
+            if (d.grips[k].targetOffsetAndCompliance.w == from) d.grips[k].targetOffsetAndCompliance.w = to;
+        }
+        if (!any) break;
+    }
+}
+
 }  // namespace
+
+extern "C" int numi_cloth_compliance_groups(numi_cloth_t* h, uint32_t family[NUMI_CLOTH_MAX_GROUPS],
+                                            float compliance[NUMI_CLOTH_MAX_GROUPS], uint32_t* count) {
+    if (h == nullptr || family == nullptr || compliance == nullptr || count == nullptr) return NUMI_CLOTH_EINVAL;
+    cudaSetDevice(h->device);
+    Groups g;
+    const int rc = compliance_groups(h, g);
+    if (rc != NUMI_CLOTH_OK) return rc;
+    *count = static_cast<uint32_t>(g.value.size());
+    for (size_t k = 0; k < g.value.size(); ++k) {
+        family[k] = g.family[k];
+        compliance[k] = g.value[k];
+    }
+    return NUMI_CLOTH_OK;
+}
+
+extern "C" int numi_cloth_replace_compliance(numi_cloth_t* h, uint32_t family, float from, float to) {
+    if (h == nullptr || family > 3u || !(to >= 0.0f) || !std::isfinite(to)) return NUMI_CLOTH_EINVAL;
+    cudaSetDevice(h->device);
+    numi_cloth_replace_compliance_kernel<<<64, 256, 0, h->stream>>>(h->d, family, from, to);
+    return cudaGetLastError() == cudaSuccess ? NUMI_CLOTH_OK : NUMI_CLOTH_ECUDA;
+}
 
 extern "C" int numi_cloth_rollout_grad(numi_cloth_t* h, const NumiClothConfig* configs, uint32_t substeps,
                                        const NumiClothSchedule* schedule, uint32_t checkpoint_every,
                                        const uint32_t* tracked, uint32_t n_tracked, const double* targets,
-                                       uint32_t loss_every, double* loss, double grads[NUMI_CLOTH_GRADS],
-                                       double* grip_grads, uint32_t* nonsmooth) {
+                                       uint32_t loss_every, double* loss, double* grads, double* grip_grads,
+                                       uint32_t* nonsmooth) {
     if (h == nullptr || configs == nullptr || schedule == nullptr || substeps == 0 || checkpoint_every == 0 ||
         loss == nullptr || grads == nullptr || (n_tracked > 0 && (tracked == nullptr || targets == nullptr)) ||
         loss_every == 0)
@@ -1497,7 +1592,7 @@ extern "C" int numi_cloth_rollout_grad(numi_cloth_t* h, const NumiClothConfig* c
     if (h->poisoned) return NUMI_CLOTH_ESTATE;
     const NumiClothSchedule& sc = *schedule;
     if (sc.iterations != 1u || sc.reconcilePasses != 0u || sc.finalPasses != 0u || sc.certificatePasses != 0u ||
-        sc.aerodynamics != 0u || sc.selfCollision != 0u || h->d.k_count != 0u)
+        sc.aerodynamics != 0u || sc.selfCollision != 0u)
         return NUMI_CLOTH_EINVAL;
     for (uint32_t t = 0; t < n_tracked; ++t)
         if (tracked[t] >= h->d.n) return NUMI_CLOTH_EINVAL;
@@ -1525,6 +1620,12 @@ extern "C" int numi_cloth_rollout_grad(numi_cloth_t* h, const NumiClothConfig* c
     const uint32_t segs = (substeps + checkpoint_every - 1u) / checkpoint_every;
     const uint32_t losses = substeps / loss_every;
 
+    Groups groups;
+    {
+        const int rc = compliance_groups(h, groups);
+        if (rc != NUMI_CLOTH_OK) return rc;
+    }
+    const uint32_t ngroups = static_cast<uint32_t>(groups.value.size());
     Scratch mem;
     size_t state_bytes = 0;
     for (const auto& r : h->dynamic) state_bytes += (r.bytes + 255u) & ~size_t(255u);
@@ -1538,11 +1639,15 @@ extern "C" int numi_cloth_rollout_grad(numi_cloth_t* h, const NumiClothConfig* c
     double4* gx = mem.get<double4>(n);
     double4* gv = mem.get<double4>(n);
     double4* gprev = mem.get<double4>(n);
-    double* d_out = mem.get<double>(NUMI_CLOTH_GRADS + 1u);   // grads, loss
+    double* d_out = mem.get<double>(ngroups + 2u);   // group gradients, damping, loss
+    uint8_t* gd = mem.get<uint8_t>(groups.d.size());
+    uint8_t* gk = mem.get<uint8_t>(groups.k.size());
+    uint8_t* gb = mem.get<uint8_t>(groups.b.size());
+    uint8_t* gg = mem.get<uint8_t>(groups.g.size());
     double* d_grip = mem.get<double>(static_cast<size_t>(substeps) * 6u);
     unsigned int* d_rough = mem.get<unsigned int>(1);
     if (!ckpt || !tape || !tape_v || !d_phases || !d_cloth || !d_tracked || !d_targets || !gx || !gv || !gprev ||
-        !d_out || !d_grip || !d_rough)
+        !d_out || !d_grip || !d_rough || !gd || !gk || !gb || !gg)
         return NUMI_CLOTH_ENOMEM;
     cudaError_t e = cudaMemcpyAsync(d_phases, phases.data(), phases.size() * sizeof(uint2), cudaMemcpyHostToDevice,
                                     h->stream);
@@ -1552,6 +1657,11 @@ extern "C" int numi_cloth_rollout_grad(numi_cloth_t* h, const NumiClothConfig* c
         e = cudaMemcpyAsync(d_targets, targets, static_cast<size_t>(losses) * n_tracked * 3u * sizeof(double),
                             cudaMemcpyHostToDevice, h->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_cloth, &h->d, sizeof(DeviceCloth), cudaMemcpyHostToDevice, h->stream);
+    const std::vector<uint8_t>* lists[4] = {&groups.d, &groups.k, &groups.b, &groups.g};
+    uint8_t* dst[4] = {gd, gk, gb, gg};
+    for (int f = 0; f < 4 && e == cudaSuccess; ++f)
+        if (!lists[f]->empty())
+            e = cudaMemcpyAsync(dst[f], lists[f]->data(), lists[f]->size(), cudaMemcpyHostToDevice, h->stream);
     if (e != cudaSuccess) return NUMI_CLOTH_ECUDA;
 
     auto save = [&](uint32_t slot) {
@@ -1630,8 +1740,13 @@ extern "C" int numi_cloth_rollout_grad(numi_cloth_t* h, const NumiClothConfig* c
         A.gx = gx;
         A.gv = gv;
         A.gprev = gprev;
+        A.d_group = gd;
+        A.k_group = gk;
+        A.b_group = gb;
+        A.g_group = gg;
+        A.groups = ngroups;
         A.grads = d_out;
-        A.loss = d_out + NUMI_CLOTH_GRADS;
+        A.loss = d_out + ngroups + 1u;
         A.grip_grads = d_grip;
         A.nonsmooth = d_rough;
         numi_cloth_adjoint_kernel<<<1, NC_THREADS, 0, h->stream>>>(A);
@@ -1649,9 +1764,9 @@ extern "C" int numi_cloth_rollout_grad(numi_cloth_t* h, const NumiClothConfig* c
     }
     if (!load(segs)) return NUMI_CLOTH_ECUDA;
     h->epoch = end_epoch;
-    double out[NUMI_CLOTH_GRADS + 1u];
+    std::vector<double> out(ngroups + 2u);
     unsigned int rough = 0;
-    e = cudaMemcpyAsync(out, d_out, sizeof(out), cudaMemcpyDeviceToHost, h->stream);
+    e = cudaMemcpyAsync(out.data(), d_out, out.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&rough, d_rough, sizeof(rough), cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess && grip_grads)
         e = cudaMemcpyAsync(grip_grads, d_grip, static_cast<size_t>(substeps) * 6u * sizeof(double),
@@ -1661,8 +1776,8 @@ extern "C" int numi_cloth_rollout_grad(numi_cloth_t* h, const NumiClothConfig* c
         h->poisoned = true;
         return NUMI_CLOTH_ECUDA;
     }
-    for (uint32_t k = 0; k < NUMI_CLOTH_GRADS; ++k) grads[k] = out[k];
-    *loss = out[NUMI_CLOTH_GRADS];
+    for (uint32_t k = 0; k <= ngroups; ++k) grads[k] = out[k];
+    *loss = out[ngroups + 1u];
     if (nonsmooth) *nonsmooth = rough;
     return NUMI_CLOTH_OK;
 }

@@ -51,7 +51,6 @@ struct DeviceCloth {
     // distances
     const uint2* d_ij;
     const float4* d_mat;
-    const uint8_t* d_kind;   // distance kind (warp, weft, bottom, shear) or null
     float* d_lambda;
     uint32_t d_count;
     // knots

@@ -96,6 +96,9 @@ def load_library() -> ctypes.CDLL:
         "numi_cloth_rollout_grad": (i32, [vp, vp, u32, ctypes.POINTER(Schedule), u32, vp, u32, vp, u32,
                                           ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), vp,
                                           ctypes.POINTER(u32)]),
+        "numi_cloth_compliance_groups": (i32, [vp, ctypes.POINTER(u32), ctypes.POINTER(ctypes.c_float),
+                                               ctypes.POINTER(u32)]),
+        "numi_cloth_replace_compliance": (i32, [vp, u32, ctypes.c_float, ctypes.c_float]),
         "numi_cloth_batch_create": (i32, [ctypes.POINTER(vp), u32, ctypes.POINTER(vp)]),
         "numi_cloth_batch_destroy": (None, [vp]),
         "numi_cloth_batch_set_stream": (i32, [vp, vp]),
@@ -394,28 +397,43 @@ class ClothSolver:
     def __del__(self):
         self.close()
 
-    GRAD_NAMES = ("log_c_warp", "log_c_weft", "log_c_bottom", "log_c_shear", "log_c_bend", "log_c_grip", "damping")
+    FAMILIES = ("distance", "knot", "bend", "grip")
+
+    def compliance_groups(self) -> list[tuple[str, float]]:
+        """(family, compliance) of every compliance group, in gradient order."""
+        fam = (ctypes.c_uint32 * 16)()
+        val = (ctypes.c_float * 16)()
+        count = ctypes.c_uint32()
+        self._check(self.lib.numi_cloth_compliance_groups(self._h, fam, val, ctypes.byref(count)))
+        return [(self.FAMILIES[fam[k]], float(val[k])) for k in range(count.value)]
+
+    def replace_compliance(self, family: str, old: float, new: float):
+        """Set every record of `family` whose compliance is `old` to `new`."""
+        self._check(self.lib.numi_cloth_replace_compliance(self._h, self.FAMILIES.index(family), old, new))
 
     def rollout_grad(self, configs: np.ndarray, schedule: Schedule, tracked, targets, loss_every: int,
                      checkpoint_every: int = 8) -> dict:
         """Advance len(configs) substeps and return the tracked-particle
-        loss and its reverse-mode gradients (numi_cloth_rollout_grad)."""
+        loss and its reverse-mode gradients (numi_cloth_rollout_grad):
+        `grads[g]` per compliance group (see compliance_groups), `damping`,
+        and per-substep grip pose gradients `grip` [substeps, 6]."""
         configs = np.ascontiguousarray(configs, CONFIG)
         tracked = np.ascontiguousarray(tracked, np.uint32)
         targets = np.ascontiguousarray(targets, np.float64)
         n = len(configs)
         if targets.shape != (n // loss_every, len(tracked), 3):
             raise ClothError("targets must be [substeps // loss_every, tracked, 3]")
+        groups = self.compliance_groups()
         loss = ctypes.c_double()
-        grads = (ctypes.c_double * 7)()
+        grads = (ctypes.c_double * (len(groups) + 1))()
         grip = np.zeros((n, 6), np.float64)
         rough = ctypes.c_uint32()
         self._check(self.lib.numi_cloth_rollout_grad(
             self._h, configs.ctypes.data, n, ctypes.byref(schedule), checkpoint_every, tracked.ctypes.data,
             len(tracked), targets.ctypes.data, loss_every, ctypes.byref(loss), grads, grip.ctypes.data,
             ctypes.byref(rough)))
-        return {"loss": loss.value, "grads": dict(zip(self.GRAD_NAMES, grads[:])), "grip": grip,
-                "nonsmooth": int(rough.value)}
+        return {"loss": loss.value, "groups": groups, "grads": np.array(grads[:len(groups)]),
+                "damping": grads[len(groups)], "grip": grip, "nonsmooth": int(rough.value)}
 
     def set_damping(self, damping: float):
         """Per-cloth velocity damping c (v <- v / (1 + c dt)); < 0: the schedule's."""
