@@ -422,6 +422,22 @@ int numi_cloth_batch_capture(numi_cloth_batch_t* batch, const NumiClothConfig* c
                              const NumiClothSchedule* schedule);
 int numi_cloth_batch_replay(numi_cloth_batch_t* batch);
 
+/* Gradients of every cloth of a batch: numi_cloth_rollout_grad for all
+ * cloths at once, the forward of every cloth in one persistent launch per
+ * checkpoint segment, the taped replays likewise, and the adjoint of every
+ * cloth's segment in one grid (a CTA per cloth).  configs: count x substeps
+ * cloth-major; tracked: shared by the cloths; targets: [count][substeps /
+ * loss_every][n_tracked][3]; loss[count]; grads: [count][NUMI_CLOTH_MAX_GROUPS
+ * + 1], cloth k's group gradients first (groups_out[k] of them, in the order
+ * of numi_cloth_compliance_groups) then dL / d damping at index
+ * groups_out[k]; nonsmooth[count] (optional).  Same schedule limits as
+ * numi_cloth_rollout_grad. */
+int numi_cloth_batch_rollout_grad(numi_cloth_batch_t* batch, const NumiClothConfig* configs, uint32_t substeps,
+                                  const NumiClothSchedule* schedule, uint32_t checkpoint_every,
+                                  const uint32_t* tracked, uint32_t n_tracked, const double* targets,
+                                  uint32_t loss_every, double* loss, double* grads, uint32_t* groups_out,
+                                  uint32_t* nonsmooth);
+
 /* Library version string. */
 const char* numi_cloth_version(void);
 

@@ -156,7 +156,7 @@ __device__ __forceinline__ void knot_dual(const DV p[4], const double w[4], Dual
 
 }  // namespace adj
 
-__global__ void __launch_bounds__(NC_THREADS) numi_cloth_adjoint_kernel(AdjointArgs A) {
+__device__ __forceinline__ void adjoint_segment(const AdjointArgs& A) {
     using namespace adj;
     const DeviceCloth& d = *A.cloth;
     const uint32_t n = d.n;
@@ -451,4 +451,33 @@ __global__ void __launch_bounds__(NC_THREADS) numi_cloth_adjoint_kernel(AdjointA
         __syncthreads();
     }
     if (threadIdx.x == 0) *A.nonsmooth += s_rough;
+}
+
+// One cloth's segment on one CTA.
+__global__ void __launch_bounds__(NC_THREADS) numi_cloth_adjoint_kernel(AdjointArgs A) { adjoint_segment(A); }
+
+// Many cloths' segments, one CTA each.
+__global__ void __launch_bounds__(NC_THREADS) numi_cloth_adjoint_batch_kernel(const AdjointArgs* args) {
+    adjoint_segment(args[blockIdx.x]);
+}
+
+// Device-to-device copies of many regions in one launch, one CTA per
+// region (cloth state checkpoints of a batch).
+struct CopyOp {
+    const void* src;
+    void* dst;
+    unsigned long long bytes;
+};
+
+__global__ void numi_cloth_copy_kernel(const CopyOp* ops) {
+    const CopyOp op = ops[blockIdx.x];
+    if ((reinterpret_cast<uintptr_t>(op.src) | reinterpret_cast<uintptr_t>(op.dst) | op.bytes) % 16u == 0u) {
+        const float4* s = static_cast<const float4*>(op.src);
+        float4* d = static_cast<float4*>(op.dst);
+        for (unsigned long long k = threadIdx.x; k < op.bytes / 16u; k += blockDim.x) d[k] = s[k];
+    } else {
+        const unsigned char* s = static_cast<const unsigned char*>(op.src);
+        unsigned char* d = static_cast<unsigned char*>(op.dst);
+        for (unsigned long long k = threadIdx.x; k < op.bytes; k += blockDim.x) d[k] = s[k];
+    }
 }

@@ -1781,3 +1781,261 @@ extern "C" int numi_cloth_rollout_grad(numi_cloth_t* h, const NumiClothConfig* c
     if (nonsmooth) *nonsmooth = rough;
     return NUMI_CLOTH_OK;
 }
+
+// ------------------------------------------------------------------------
+// Batched rollout gradients (numi_cloth_batch_rollout_grad): the forward of
+// every cloth in one persistent launch per segment, the taped replays in one
+// launch per segment, and the adjoint of every cloth's segment in one grid
+// (a CTA per cloth).  Checkpoints are moved by one copy kernel per segment.
+
+extern "C" int numi_cloth_batch_rollout_grad(numi_cloth_batch_t* b, const NumiClothConfig* configs, uint32_t substeps,
+                                             const NumiClothSchedule* schedule, uint32_t checkpoint_every,
+                                             const uint32_t* tracked, uint32_t n_tracked, const double* targets,
+                                             uint32_t loss_every, double* loss, double* grads, uint32_t* groups_out,
+                                             uint32_t* nonsmooth) {
+    if (b == nullptr || configs == nullptr || schedule == nullptr || substeps == 0 || checkpoint_every == 0 ||
+        loss == nullptr || grads == nullptr || loss_every == 0 || (n_tracked > 0 && (tracked == nullptr || targets == nullptr)))
+        return NUMI_CLOTH_EINVAL;
+    const NumiClothSchedule& sc = *schedule;
+    if (sc.iterations != 1u || sc.reconcilePasses != 0u || sc.finalPasses != 0u || sc.certificatePasses != 0u ||
+        sc.aerodynamics != 0u || sc.selfCollision != 0u)
+        return NUMI_CLOTH_EINVAL;
+    cudaSetDevice(b->device);
+    batch_drop_graph(b);
+    const uint32_t count = static_cast<uint32_t>(b->cloths.size());
+    for (numi_cloth* h : b->cloths)
+        for (uint32_t t = 0; t < n_tracked; ++t)
+            if (tracked[t] >= h->d.n) return NUMI_CLOTH_EINVAL;
+    // Configs, descriptors (always rebuilt: damping and compliances may have
+    // changed since the last launch)
+    b->layout_valid = false;
+    {
+        const int rc = batch_prepare(b, configs, substeps, sc);
+        if (rc > 0) return rc;
+        if (rc != NUMI_CLOTH_OK) return rc;
+    }
+    cudaError_t e = cudaMemcpyAsync(b->d_cfg, configs, static_cast<size_t>(count) * substeps * sizeof(NumiClothConfig),
+                                    cudaMemcpyHostToDevice, b->stream);
+    if (e != cudaSuccess) return NUMI_CLOTH_ECUDA;
+    const Schedule s = device_schedule(sc);
+    const uint32_t segs = (substeps + checkpoint_every - 1u) / checkpoint_every;
+    const uint32_t losses = substeps / loss_every;
+
+    Scratch mem;
+    // per cloth: groups, phase list, tape, checkpoints, adjoint arrays
+    std::vector<Groups> groups(count);
+    std::vector<std::vector<uint2>> phases(count);
+    std::vector<size_t> state_bytes(count), tape_off(count), ckpt_off(count);
+    size_t tape_total = 0, ckpt_total = 0;
+    uint32_t max_slots = 0;
+    for (uint32_t k = 0; k < count; ++k) {
+        numi_cloth* h = b->cloths[k];
+        const int rc = compliance_groups(h, groups[k]);
+        if (rc != NUMI_CLOTH_OK) return rc;
+        phases[k] = adjoint_phases(h->d, s);
+        const uint32_t slots = static_cast<uint32_t>(phases[k].size()) + 1u;
+        max_slots = std::max(max_slots, slots);
+        tape_off[k] = tape_total;
+        tape_total += static_cast<size_t>(checkpoint_every) * (slots + 1u) * h->d.n;   // positions + velocities
+        size_t bytes = 0;
+        for (const auto& r : h->dynamic) bytes += (r.bytes + 255u) & ~size_t(255u);
+        state_bytes[k] = bytes;
+        ckpt_off[k] = ckpt_total;
+        ckpt_total += (segs + 1u) * bytes;
+    }
+    float4* tape = mem.get<float4>(tape_total);
+    char* ckpt = mem.get<char>(ckpt_total);
+    uint32_t* d_tracked = mem.get<uint32_t>(n_tracked);
+    double* d_targets = mem.get<double>(static_cast<size_t>(count) * losses * n_tracked * 3u);
+    double* d_out = mem.get<double>(static_cast<size_t>(count) * (NUMI_CLOTH_MAX_GROUPS + 2u));
+    unsigned int* d_rough = mem.get<unsigned int>(count);
+    DeviceCloth* d_replay = mem.get<DeviceCloth>(count);   // launch order, tape set
+    DeviceCloth* d_plain = mem.get<DeviceCloth>(count);    // caller order, for the adjoint
+    AdjointArgs* d_args = mem.get<AdjointArgs>(count);
+    CopyOp* d_save = mem.get<CopyOp>(static_cast<size_t>(count) * 16u);
+    if (!tape || !ckpt || !d_tracked || !d_targets || !d_out || !d_rough || !d_replay || !d_plain || !d_args || !d_save)
+        return NUMI_CLOTH_ENOMEM;
+    std::vector<AdjointArgs> args(count);
+    std::vector<DeviceCloth> replay(count), plain(count);
+    // one arena for every cloth's phase list, adjoint arrays and group ids
+    auto round256 = [](size_t v) { return (v + 255u) & ~size_t(255u); };
+    size_t arena_bytes = 0;
+    for (uint32_t k = 0; k < count; ++k)
+        arena_bytes += round256(phases[k].size() * sizeof(uint2)) + round256(3u * sizeof(double4) * b->cloths[k]->d.n) +
+                       round256(groups[k].d.size() + 1u) + round256(groups[k].k.size() + 1u) +
+                       round256(groups[k].b.size() + 1u) + round256(groups[k].g.size() + 1u);
+    char* arena = mem.get<char>(arena_bytes);
+    if (!arena) return NUMI_CLOTH_ENOMEM;
+    size_t cursor = 0;
+    auto carve = [&](size_t bytes) {
+        char* p = arena + cursor;
+        cursor += round256(bytes);
+        return p;
+    };
+    for (uint32_t k = 0; k < count; ++k) {
+        numi_cloth* h = b->cloths[k];
+        const uint32_t n = h->d.n;
+        const uint32_t slots = static_cast<uint32_t>(phases[k].size()) + 1u;
+        uint2* ph = reinterpret_cast<uint2*>(carve(phases[k].size() * sizeof(uint2)));
+        double4* gx = reinterpret_cast<double4*>(carve(3u * sizeof(double4) * n));
+        uint8_t* gd = reinterpret_cast<uint8_t*>(carve(groups[k].d.size() + 1u));
+        uint8_t* gk = reinterpret_cast<uint8_t*>(carve(groups[k].k.size() + 1u));
+        uint8_t* gb = reinterpret_cast<uint8_t*>(carve(groups[k].b.size() + 1u));
+        uint8_t* gg = reinterpret_cast<uint8_t*>(carve(groups[k].g.size() + 1u));
+        e = cudaMemcpyAsync(ph, phases[k].data(), phases[k].size() * sizeof(uint2), cudaMemcpyHostToDevice, b->stream);
+        const std::vector<uint8_t>* lists[4] = {&groups[k].d, &groups[k].k, &groups[k].b, &groups[k].g};
+        uint8_t* dst[4] = {gd, gk, gb, gg};
+        for (int f = 0; f < 4 && e == cudaSuccess; ++f)
+            if (!lists[f]->empty())
+                e = cudaMemcpyAsync(dst[f], lists[f]->data(), lists[f]->size(), cudaMemcpyHostToDevice, b->stream);
+        if (e != cudaSuccess) return NUMI_CLOTH_ECUDA;
+        plain[k] = h->d;
+        AdjointArgs& A = args[k];
+        A.cloth = d_plain + k;
+        A.tape = tape + tape_off[k];
+        A.tape_v = A.tape + static_cast<size_t>(checkpoint_every) * slots * n;
+        A.phases = ph;
+        A.slots = slots;
+        A.damping = h->d.damping >= 0.0f ? h->d.damping : s.damping;
+        A.tracked = d_tracked;
+        A.n_tracked = n_tracked;
+        A.targets = d_targets + static_cast<size_t>(k) * losses * n_tracked * 3u;
+        A.loss_every = loss_every;
+        A.gx = gx;
+        A.gv = gx + n;
+        A.gprev = gx + 2u * static_cast<size_t>(n);
+        A.d_group = gd;
+        A.k_group = gk;
+        A.b_group = gb;
+        A.g_group = gg;
+        A.groups = static_cast<uint32_t>(groups[k].value.size());
+        A.grads = d_out + static_cast<size_t>(k) * (NUMI_CLOTH_MAX_GROUPS + 2u);
+        A.loss = A.grads + NUMI_CLOTH_MAX_GROUPS + 1u;
+        A.grip_grads = nullptr;
+        A.nonsmooth = d_rough + k;
+    }
+    // replay descriptors: the batch's launch-order descriptors with tapes
+    {
+        std::vector<DeviceCloth> base(count);
+        e = cudaMemcpy(base.data(), b->d_cloths, count * sizeof(DeviceCloth), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return NUMI_CLOTH_ECUDA;
+        for (uint32_t j = 0; j < count; ++j) {
+            const uint32_t k = b->order[j];
+            replay[j] = base[j];
+            replay[j].tape = const_cast<float4*>(args[k].tape);
+            replay[j].tape_v = const_cast<float4*>(args[k].tape_v);
+            replay[j].tape_slots = args[k].slots;
+        }
+    }
+    e = cudaMemcpyAsync(d_replay, replay.data(), count * sizeof(DeviceCloth), cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_plain, plain.data(), count * sizeof(DeviceCloth), cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess && n_tracked)
+        e = cudaMemcpyAsync(d_tracked, tracked, n_tracked * sizeof(uint32_t), cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess && n_tracked && losses)
+        e = cudaMemcpyAsync(d_targets, targets, static_cast<size_t>(count) * losses * n_tracked * 3u * sizeof(double),
+                            cudaMemcpyHostToDevice, b->stream);
+    if (e != cudaSuccess) return NUMI_CLOTH_ECUDA;
+
+    // one copy kernel per checkpoint move: op tables for save (state ->
+    // checkpoint) and load (checkpoint -> state) of every slot
+    std::vector<CopyOp> save_ops, load_ops;
+    uint32_t regions = 0;
+    for (numi_cloth* h : b->cloths) regions += static_cast<uint32_t>(h->dynamic.size());
+    CopyOp* d_ops = mem.get<CopyOp>(2u * static_cast<size_t>(segs + 1u) * regions);
+    if (!d_ops) return NUMI_CLOTH_ENOMEM;
+    for (uint32_t g = 0; g <= segs; ++g) {
+        for (uint32_t k = 0; k < count; ++k) {
+            numi_cloth* h = b->cloths[k];
+            size_t off = 0;
+            for (const auto& r : h->dynamic) {
+                char* slot = ckpt + ckpt_off[k] + g * state_bytes[k] + off;
+                save_ops.push_back(CopyOp{r.ptr, slot, r.bytes});
+                load_ops.push_back(CopyOp{slot, r.ptr, r.bytes});
+                off += (r.bytes + 255u) & ~size_t(255u);
+            }
+        }
+    }
+    e = cudaMemcpyAsync(d_ops, save_ops.data(), save_ops.size() * sizeof(CopyOp), cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_ops + save_ops.size(), load_ops.data(), load_ops.size() * sizeof(CopyOp),
+                            cudaMemcpyHostToDevice, b->stream);
+    if (e != cudaSuccess) return NUMI_CLOTH_ECUDA;
+    auto move = [&](bool save, uint32_t g) {
+        const CopyOp* ops = d_ops + (save ? 0u : save_ops.size()) + static_cast<size_t>(g) * regions;
+        numi_cloth_copy_kernel<<<regions, 256, 0, b->stream>>>(ops);
+    };
+    auto set_epoch = [&](uint32_t value) {
+        return cudaMemcpyAsync(b->epoch, &value, sizeof(uint32_t), cudaMemcpyHostToDevice, b->stream) == cudaSuccess &&
+               cudaStreamSynchronize(b->stream) == cudaSuccess;
+    };
+
+    // forward
+    std::vector<uint32_t> seg_epoch(segs);
+    const uint32_t epoch0 = b->epoch_host;
+    if (!set_epoch(epoch0)) return NUMI_CLOTH_ECUDA;
+    for (uint32_t g = 0; g < segs; ++g) {
+        const uint32_t first = g * checkpoint_every;
+        const uint32_t cnt = std::min(checkpoint_every, substeps - first);
+        seg_epoch[g] = epoch0 + first;
+        move(true, g);
+        Schedule st = s;
+        st.substeps = cnt;
+        st.cfg_offset = first;
+        st.epoch_ptr = b->epoch;
+        cudaMemsetAsync(b->queue, 0, sizeof(unsigned int), b->stream);
+        numi_cloth_batch_kernel<<<b->ctas, b->block, b->smem, b->stream>>>(b->d_cloths, count, st, b->queue);
+        numi_cloth_epoch_kernel<<<1, 1, 0, b->stream>>>(b->epoch, cnt);
+    }
+    move(true, segs);
+    // backward
+    for (uint32_t g = segs; g-- > 0u;) {
+        const uint32_t first = g * checkpoint_every;
+        const uint32_t cnt = std::min(checkpoint_every, substeps - first);
+        move(false, g);
+        if (!set_epoch(seg_epoch[g])) return NUMI_CLOTH_ECUDA;
+        Schedule st = s;
+        st.substeps = cnt;
+        st.cfg_offset = first;
+        st.epoch_ptr = b->epoch;
+        cudaMemsetAsync(b->queue, 0, sizeof(unsigned int), b->stream);
+        numi_cloth_batch_kernel<<<b->ctas, b->block, b->smem, b->stream>>>(d_replay, count, st, b->queue);
+        for (uint32_t k = 0; k < count; ++k) {
+            args[k].cfg = b->d_cfg + static_cast<size_t>(k) * substeps + first;
+            args[k].substeps = cnt;
+            args[k].first_substep = first;
+        }
+        e = cudaMemcpyAsync(d_args, args.data(), count * sizeof(AdjointArgs), cudaMemcpyHostToDevice, b->stream);
+        if (e != cudaSuccess) return NUMI_CLOTH_ECUDA;
+        numi_cloth_adjoint_batch_kernel<<<count, NC_THREADS, 0, b->stream>>>(d_args);
+        // args is rewritten next segment: wait for this copy to be consumed
+        if (cudaStreamSynchronize(b->stream) != cudaSuccess) {
+            for (numi_cloth* h : b->cloths) h->poisoned = true;
+            return NUMI_CLOTH_ECUDA;
+        }
+    }
+    move(false, segs);
+    const uint32_t end_epoch = epoch0 + substeps;
+    if (!set_epoch(end_epoch)) return NUMI_CLOTH_ECUDA;
+    b->epoch_host = end_epoch;
+    for (numi_cloth* h : b->cloths) {
+        h->epoch = end_epoch;
+        h->last_substeps = substeps;
+    }
+    std::vector<double> out(static_cast<size_t>(count) * (NUMI_CLOTH_MAX_GROUPS + 2u));
+    std::vector<unsigned int> rough(count);
+    e = cudaMemcpyAsync(out.data(), d_out, out.size() * sizeof(double), cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(rough.data(), d_rough, count * sizeof(unsigned int), cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) {
+        for (numi_cloth* h : b->cloths) h->poisoned = true;
+        return NUMI_CLOTH_ECUDA;
+    }
+    for (uint32_t k = 0; k < count; ++k) {
+        const double* o = out.data() + static_cast<size_t>(k) * (NUMI_CLOTH_MAX_GROUPS + 2u);
+        for (uint32_t q = 0; q <= NUMI_CLOTH_MAX_GROUPS; ++q) grads[static_cast<size_t>(k) * (NUMI_CLOTH_MAX_GROUPS + 1u) + q] = o[q];
+        loss[k] = o[NUMI_CLOTH_MAX_GROUPS + 1u];
+        if (groups_out) groups_out[k] = static_cast<uint32_t>(groups[k].value.size());
+        if (nonsmooth) nonsmooth[k] = rough[k];
+    }
+    return NUMI_CLOTH_OK;
+}

@@ -159,6 +159,8 @@ struct Schedule {
     // (advanced by a kernel after each launch, so a captured graph can be
     // replayed); null: DeviceCloth::epoch_base
     const uint32_t* epoch_ptr;
+    // first Config of the launch within DeviceCloth::cfg
+    uint32_t cfg_offset;
 };
 
 // Fruit-side state kept in the shared memory of the fruit CTA for a whole

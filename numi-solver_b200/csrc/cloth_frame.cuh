@@ -1072,7 +1072,7 @@ __device__ __forceinline__ D3 to_d3(float4 p) { return D3{static_cast<double>(p.
 
 __device__ void release_masks(Ctx& ctx) {
     const DeviceCloth& d = ctx.d;
-    const NumiClothConfig& cf = d.cfg[ctx.sub];
+    const NumiClothConfig& cf = d.cfg[ctx.s.cfg_offset + ctx.sub];
     const uint32_t m = cf.mouthControl.x;
     if (!ctx.s.release || d.rim == nullptr || m < 3u || m > NUMI_CLOTH_MOUTH_RIM_CAPACITY) return;
     __shared__ D3 s_ring[NUMI_CLOTH_MOUTH_RIM_CAPACITY];
@@ -1399,7 +1399,7 @@ __device__ __forceinline__ void run_frame(const DeviceCloth& src, const Schedule
     const uint32_t epoch_base = s.epoch_ptr != nullptr ? *s.epoch_ptr : d.epoch_base;
     for (uint32_t sub = 0; sub < s.substeps; ++sub) {
         ctx.sub = sub;
-        ctx.c = nc::load_cfg(d.cfg + sub);
+        ctx.c = nc::load_cfg(d.cfg + s.cfg_offset + sub);
         ctx.epoch = epoch_base + sub;
         ctx.barriers = 0;
         if (d.tape != nullptr && ranks == 1u) {

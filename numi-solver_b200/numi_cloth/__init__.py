@@ -108,6 +108,8 @@ def load_library() -> ctypes.CDLL:
         "numi_cloth_batch_tune": (i32, [vp, vp, u32, ctypes.POINTER(Schedule), ctypes.POINTER(u32)]),
         "numi_cloth_batch_capture": (i32, [vp, vp, u32, ctypes.POINTER(Schedule)]),
         "numi_cloth_batch_replay": (i32, [vp]),
+        "numi_cloth_batch_rollout_grad": (i32, [vp, vp, u32, ctypes.POINTER(Schedule), u32, vp, u32, vp, u32, vp, vp,
+                                                vp, vp]),
         "numi_cloth_trace": (i32, [vp, ctypes.POINTER(ctypes.c_ulonglong), u32, u32]),
         "numi_cloth_trace_cta": (i32, [vp, ctypes.POINTER(ctypes.c_ulonglong), u32]),
         "numi_cloth_step_noalloc": (
@@ -658,3 +660,24 @@ class ClothBatch:
 
     def replay(self):
         self._check(self.lib.numi_cloth_batch_replay(self._h))
+
+    def rollout_grad(self, configs: np.ndarray, schedule: Schedule, tracked, targets, loss_every: int,
+                     checkpoint_every: int = 8) -> dict:
+        """numi_cloth_batch_rollout_grad: loss [cloths], group gradients
+        [cloths, groups], damping gradient [cloths], non-smooth counts."""
+        configs, n = self._configs(configs)
+        count = len(self.solvers)
+        tracked = np.ascontiguousarray(tracked, np.uint32)
+        targets = np.ascontiguousarray(targets, np.float64)
+        if targets.shape != (count, n // loss_every, len(tracked), 3):
+            raise ClothError("targets must be [cloths, substeps // loss_every, tracked, 3]")
+        loss = np.zeros(count, np.float64)
+        grads = np.zeros((count, 17), np.float64)
+        groups = np.zeros(count, np.uint32)
+        rough = np.zeros(count, np.uint32)
+        self._check(self.lib.numi_cloth_batch_rollout_grad(
+            self._h, configs.ctypes.data, n, ctypes.byref(schedule), checkpoint_every, tracked.ctypes.data,
+            len(tracked), targets.ctypes.data, loss_every, loss.ctypes.data, grads.ctypes.data, groups.ctypes.data,
+            rough.ctypes.data))
+        return {"loss": loss, "grads": [grads[k, :int(groups[k])] for k in range(count)],
+                "damping": grads[np.arange(count), groups.astype(np.int64)], "groups": groups, "nonsmooth": rough}

@@ -246,3 +246,38 @@ def test_bag_knot_gradients_match_fp64_finite_differences():
     scale = max(abs(v) for v in fd.values())
     for k, v in fd.items():
         assert _close(adj[k], v, scale), (k, adj[k], v)
+
+
+def test_batched_gradients_equal_single_cloth_gradients():
+    """The batched forward + adjoint (one launch per segment for all cloths,
+    one CTA per cloth for the adjoint) gives each cloth the gradients of its
+    own rollout."""
+    scenes = [_scene(), small_square(side=9, fruits=0, gripCorners=1, stretchCompliance=3e-5, shearCompliance=4e-5,
+                                     bendCompliance=1e-4, height=0.0, groundEnabled=0, seed=3), _bag_without_fruits()]
+    cfgs = [_configs(s) for s in scenes]
+    tracked = np.array([0, 5, 17, 40, 77], np.uint32)
+    rng = np.random.default_rng(11)
+    targets, singles = [], []
+    for s, c in zip(scenes, cfgs):
+        sv = nc.ClothSolver(s)
+        x = sv.particles()["positionAndInverseMass"][tracked, :3].astype(np.float64)
+        tg = np.stack([x + rng.uniform(-2e-3, 2e-3, size=x.shape) for _ in range(SUBSTEPS // LOSS_EVERY)])
+        targets.append(tg)
+        singles.append(sv.rollout_grad(c, nc.Schedule.make(**SCHED), tracked, tg, LOSS_EVERY, checkpoint_every=8))
+        sv.close()
+    solvers = [nc.ClothSolver(s) for s in scenes]
+    batch = nc.ClothBatch(solvers)
+    r = batch.rollout_grad(np.stack(cfgs), nc.Schedule.make(**SCHED), tracked, np.stack(targets), LOSS_EVERY,
+                           checkpoint_every=8)
+    for k, one in enumerate(singles):
+        assert int(r["groups"][k]) == len(one["groups"])
+        assert r["loss"][k] == pytest.approx(one["loss"], rel=1e-12)
+        assert np.allclose(r["grads"][k], one["grads"], rtol=1e-10, atol=0.0)
+        assert np.allclose(r["damping"][k], one["damping"], rtol=1e-10, atol=0.0)
+        assert r["nonsmooth"][k] == one["nonsmooth"] == 0
+    # the state after the call is the rollout's end state
+    for sv, s, c in zip(solvers, scenes, cfgs):
+        ref = nc.ClothSolver(s)
+        ref.step(c, nc.Schedule.make(**SCHED))
+        assert np.array_equal(sv.particles(), ref.particles())
+    batch.close()
