@@ -1,0 +1,144 @@
+"""Gradient-based calibration of cloth compliances and damping.
+
+The reference fits its material artifact by a linearised least-squares step
+on sensitivities measured outside the simulator by central finite
+differences (tools/cloth_calibration.cpp:542-683,
+docs/CLOTH_SPECIMEN_CALIBRATION.md:52-82).  Here the sensitivities come from
+the adjoint: every candidate parameter set is a cloth of one batch, the
+batch runs its forward and adjoint together (numi_cloth_batch_rollout_grad),
+and Adam descends on the log-compliances and the damping of every
+candidate at once.
+"""
+from __future__ import annotations
+
+import time
+
+import numpy as np
+
+from . import ClothBatch, ClothSolver, Schedule
+
+# Calibrated parameters of the produce bag: (constraint family, material
+# field); the bag's records of a family carry one of these compliances.
+BAG_PARAMS = (
+    ("distance", "axialBodyComplianceMPerN"),
+    ("distance", "axialCuffComplianceMPerN"),
+    ("knot", "knotCompliance"),
+    ("bend", "bendBodyComplianceMPerN"),
+    ("bend", "bendCuffComplianceMPerN"),
+    ("grip", "gripComplianceMPerN"),
+)
+FAMILIES = ("distance", "knot", "bend", "grip")
+
+
+def group_index(values: np.ndarray, params=BAG_PARAMS) -> list[int]:
+    """Gradient slot of each parameter: groups are the distinct compliance
+    values of each family, ascending, family by family (the order of
+    numi_cloth_compliance_groups)."""
+    slots, base = [], 0
+    order = {}
+    for fam in FAMILIES:
+        vals = sorted({float(values[p]) for p, (f, _) in enumerate(params) if f == fam})
+        for k, v in enumerate(vals):
+            order[(fam, v)] = base + k
+        base += len(vals)
+    for p, (fam, _) in enumerate(params):
+        slots.append(order[(fam, float(values[p]))])
+    return slots
+
+
+class Adam:
+    """Adam (Kingma and Ba 2015) on an array of parameters."""
+
+    def __init__(self, shape, lr: float, beta1: float = 0.9, beta2: float = 0.999, eps: float = 1e-12):
+        self.lr, self.b1, self.b2, self.eps = lr, beta1, beta2, eps
+        self.m = np.zeros(shape)
+        self.v = np.zeros(shape)
+        self.t = 0
+
+    def step(self, x: np.ndarray, g: np.ndarray) -> np.ndarray:
+        self.t += 1
+        self.m = self.b1 * self.m + (1 - self.b1) * g
+        self.v = self.b2 * self.v + (1 - self.b2) * g * g
+        mh = self.m / (1 - self.b1 ** self.t)
+        vh = self.v / (1 - self.b2 ** self.t)
+        return x - self.lr * mh / (np.sqrt(vh) + self.eps)
+
+
+class Calibration:
+    """Candidates of one scene as a batch; every evaluation restores the
+    initial state, applies each candidate's parameters and runs the batched
+    forward + adjoint."""
+
+    def __init__(self, scenes, configs: np.ndarray, schedule: Schedule, tracked, targets, loss_every: int,
+                 base_values: np.ndarray, params=BAG_PARAMS, checkpoint_every: int = 8, stream: int | None = None):
+        self.params = params
+        self.solvers = [ClothSolver(s) for s in scenes]
+        for sv in self.solvers:
+            if stream is not None:
+                sv.set_stream(stream)
+            sv.snapshot(0)
+        self.batch = ClothBatch(self.solvers)
+        if stream is not None:
+            self.batch.set_stream(stream)
+        n = len(self.solvers)
+        self.configs = np.ascontiguousarray(np.broadcast_to(configs, (n,) + configs.shape))
+        self.schedule = schedule
+        self.tracked = np.ascontiguousarray(tracked, np.uint32)
+        self.targets = np.ascontiguousarray(np.broadcast_to(targets, (n,) + targets.shape))
+        self.loss_every = loss_every
+        self.checkpoint_every = checkpoint_every
+        self.values = np.tile(np.asarray(base_values, np.float32), (n, 1))   # current float32 compliances
+        self.rollout_seconds = 0.0
+        self.rollouts = 0
+
+    def close(self):
+        self.batch.close()
+        for sv in self.solvers:
+            sv.close()
+
+    def _apply(self, logc: np.ndarray, damping: np.ndarray):
+        for k, sv in enumerate(self.solvers):
+            new = np.exp(logc[k]).astype(np.float32)
+            for p, (fam, _) in enumerate(self.params):
+                if new[p] == self.values[k, p]:
+                    continue
+                # a value shared with another parameter of the family would
+                # merge their records: step one ulp away
+                others = [self.values[k, q] for q, (f, _) in enumerate(self.params) if f == fam and q != p]
+                while new[p] in others:
+                    new[p] = np.nextafter(new[p], np.float32(np.inf))
+                sv.replace_compliance(fam, float(self.values[k, p]), float(new[p]))
+                self.values[k, p] = new[p]
+            sv.set_damping(float(damping[k]))
+
+    def evaluate(self, logc: np.ndarray, damping: np.ndarray) -> tuple[np.ndarray, np.ndarray, np.ndarray, np.ndarray]:
+        """Loss, d loss / d log-compliance [n, params], d loss / d damping, and
+        the non-smooth event counts of every candidate."""
+        for sv in self.solvers:
+            sv.restore(0)
+        self._apply(logc, damping)
+        t0 = time.perf_counter()
+        r = self.batch.rollout_grad(self.configs, self.schedule, self.tracked, self.targets, self.loss_every,
+                                    self.checkpoint_every)
+        self.rollout_seconds += time.perf_counter() - t0
+        self.rollouts += 1
+        g = np.zeros_like(logc)
+        for k in range(len(self.solvers)):
+            slots = group_index(self.values[k], self.params)
+            g[k] = [r["grads"][k][s] for s in slots]
+        return r["loss"], g, r["damping"], r["nonsmooth"]
+
+    def fit(self, logc0: np.ndarray, damping0: np.ndarray, steps: int, lr: float = 0.1, lr_damping: float = 0.005,
+            damping_max: float = 1.0) -> dict:
+        logc, damp = logc0.astype(np.float64).copy(), damping0.astype(np.float64).copy()
+        opt_c, opt_d = Adam(logc.shape, lr), Adam(damp.shape, lr_damping)
+        history = []
+        loss = None
+        for _ in range(steps):
+            loss, g, gd, rough = self.evaluate(logc, damp)
+            history.append(loss.copy())
+            logc = opt_c.step(logc, g)
+            damp = np.clip(opt_d.step(damp, gd), 0.0, damping_max)
+        final, _, _, rough = self.evaluate(logc, damp)
+        history.append(final.copy())
+        return {"logc": logc, "damping": damp, "loss": final, "history": np.array(history), "nonsmooth": rough}
