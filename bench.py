@@ -236,6 +236,83 @@ def batched_leg(nc, torch, stream, frames: int, warmup: int, plain_frames: int) 
             "inputs_vs_l2": "working set of all cloths above L2 (126 MB)", "failure": nc.failure_names(fail)}
 
 
+CALIB_SCHEDULE = dict(iterations=1, strainSweeps=3, reconcilePasses=0, finalPasses=0, certificatePasses=0,
+                      earlyExit=0, aerodynamics=0, sweptGround=1, frictions=1, selfCollision=0)
+
+
+def calibration_leg(nc, torch, stream, candidates: int, steps: int, plain_sample: int) -> dict:
+    """Batched calibration: candidates of the produce bag (1,465 particles, 12
+    fruits, lift trajectory, 48 substeps at 1/2880 s) with log-compliances
+    drawn +-1 decade around the authored defaults and damping in [0, 0.05];
+    each Adam step runs every candidate's forward and adjoint as one batch
+    against 40 tracked cuff and bottom knots of a target trajectory made at
+    hidden seeded parameters.  The plain path runs the same forward + adjoint
+    one cloth at a time (numi_cloth_rollout_grad)."""
+    import numpy as np
+
+    from numi_cloth import calibrate as cal
+
+    dt = 1.0 / 2880.0
+    scene = nc.bag_scene(scenario="recorded", timestep=dt)
+    traj = nc.GripTrajectory(os.path.join(ROOT, "tests", "golden", "lift-v1.csv"))
+    cfg = traj.configs(scene.config, scene.handle_base, 0, SUBSTEPS, dt)
+    sched = nc.Schedule.make(**CALIB_SCHEDULE)
+    m = nc.material_defaults()
+    base = np.array([getattr(m, field) for _, field in cal.BAG_PARAMS], np.float32)
+    z = scene.particles["positionAndInverseMass"][:, 2]
+    tracked = np.unique(np.concatenate([scene.cuff[:48:2][:20], np.argsort(z)[:20]])).astype(np.uint32)
+    rng = np.random.default_rng(424242)
+    hidden = base.astype(np.float64) * 10.0 ** rng.uniform(-0.5, 0.5, size=base.shape)
+    hidden_damping = 0.02
+    loss_every = 12
+    sv = nc.ClothSolver(scene)
+    sv.set_stream(stream.cuda_stream)
+    for p, (fam, _) in enumerate(cal.BAG_PARAMS):
+        sv.replace_compliance(fam, float(base[p]), float(np.float32(hidden[p])))
+    sv.set_damping(hidden_damping)
+    targets = []
+    for k in range(SUBSTEPS // loss_every):
+        sv.step(cfg[k * loss_every:(k + 1) * loss_every], sched)
+        targets.append(sv.particles()["positionAndInverseMass"][tracked, :3].astype(np.float64))
+    sv.close()
+    targets = np.stack(targets)
+    logc0 = np.log(base.astype(np.float64))[None, :] + rng.uniform(-np.log(10.0), np.log(10.0),
+                                                                    size=(candidates, len(base)))
+    d0 = rng.uniform(0.0, 0.05, size=candidates)
+    c = cal.Calibration([scene] * candidates, cfg, sched, tracked, targets, loss_every, base,
+                        stream=stream.cuda_stream)
+    out = c.fit(logc0, d0, steps, lr=0.1, lr_damping=0.005)
+    batched_s = c.rollout_seconds
+    rollouts = c.rollouts
+    c.close()
+    # plain path: one cloth per call
+    t_plain = 0.0
+    for k in range(plain_sample):
+        one = nc.ClothSolver(scene)
+        one.set_stream(stream.cuda_stream)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        one.rollout_grad(cfg, sched, tracked, targets, loss_every)
+        torch.cuda.synchronize()
+        t_plain += time.perf_counter() - t0
+        one.close()
+    best = int(np.argmin(out["loss"]))
+    err = np.abs(out["logc"][best] - np.log(hidden))
+    err0 = np.abs(logc0 - np.log(hidden)).mean(axis=0)
+    value = candidates * rollouts / batched_s
+    plain = plain_sample / t_plain
+    return {"metric": "calibration gradients/s (forward + adjoint, 48-substep bag rollouts)", "value": value,
+            "unit": "gradients/s", "candidates": candidates, "adam_steps": steps, "rollouts": rollouts,
+            "batched_seconds": batched_s, "plain_value": plain, "plain_sample": plain_sample,
+            "speedup_vs_plain": value / plain, "schedule": CALIB_SCHEDULE,
+            "params": [f for _, f in cal.BAG_PARAMS] + ["damping"],
+            "best_log_param_error": [float(v) for v in err] + [float(abs(out["damping"][best] - hidden_damping))],
+            "initial_mean_log_param_error": [float(v) for v in err0],
+            "best_loss": float(out["loss"][best]), "initial_best_loss": float(out["history"][0].min()),
+            "nonsmooth_events_best": int(out["nonsmooth"][best]),
+            "note": "fruit contact and cloth/ground friction are not differentiated; their events are counted"}
+
+
 def dist_info():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -371,6 +448,9 @@ def run_ours(args):
     batched = None
     if world == 1 and not args.no_batched:
         batched = batched_leg(nc, torch, stream, args.batch_frames, args.warmup, 2)
+    calibration = None
+    if world == 1 and not args.no_calibration:
+        calibration = calibration_leg(nc, torch, stream, args.calib_candidates, args.calib_steps, 4)
 
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -399,6 +479,7 @@ def run_ours(args):
             "e2e": {"value": e2e_value, "unit": "substeps/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "batched": batched,
+            "calibration": calibration,
             "gpu_launches": args.steps,
             "clocks": clocks.summary(),
             "failure": nc.failure_names(fail),
@@ -424,6 +505,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batch-frames", type=int, default=20)
+    ap.add_argument("--no-calibration", action="store_true")
+    ap.add_argument("--calib-candidates", type=int, default=256)
+    ap.add_argument("--calib-steps", type=int, default=50)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
