@@ -7,6 +7,11 @@
 
 namespace nc {
 
+// FP64 scratch of the CTA-wide reductions (air-load chunk sums, the air
+// attenuation, the residual maxima).  They run in different phases and each
+// ends with a CTA barrier, so they share one array.
+__shared__ double nc_red_smem[3][NC_BLOCK_MAX];
+
 // Grid-wide barrier with a bounded wait.  Arrival is a release-add of 1 to
 // a counter the host zeroes before each launch; barrier number s of the
 // launch completes when an acquire load sees s times the number of CTAs on
@@ -215,8 +220,8 @@ __device__ void air_force_batch(Ctx& ctx, const Batch& bt, float4* force) {
 // each with the same tree); chunk partials land in red[2*chunk].
 __device__ void air_reduce_chunks(Ctx& ctx, const float4* force) {
     const DeviceCloth& d = ctx.d;
-    __shared__ double s_p[NC_BLOCK_MAX];
-    __shared__ double s_q[NC_BLOCK_MAX];
+    double* s_p = nc_red_smem[0];
+    double* s_q = nc_red_smem[1];
     const uint32_t chunks = (d.n + NC_THREADS - 1u) / NC_THREADS;
     const uint32_t groups = blockDim.x / NC_THREADS;
     const uint32_t t = threadIdx.x % NC_THREADS;
@@ -259,8 +264,8 @@ __device__ void air_reduce_chunks(Ctx& ctx, const float4* force) {
 // 256 threads; the tree shape does not depend on the launch).
 __device__ float air_attenuation(Ctx& ctx) {
     const DeviceCloth& d = ctx.d;
-    __shared__ double s_p[NC_THREADS];
-    __shared__ double s_q[NC_THREADS];
+    double* s_p = nc_red_smem[0];
+    double* s_q = nc_red_smem[1];
     const uint32_t chunks = (d.n + NC_THREADS - 1u) / NC_THREADS;
     if (threadIdx.x < NC_THREADS) {
         double pw = 0.0, q = 0.0;
@@ -348,6 +353,86 @@ __device__ __forceinline__ bool fruit_near_segment(const float4& fs, const float
              fs.z < fminf(pa.z, pb.z) - target || fs.z > fmaxf(pa.z, pb.z) + target);
 }
 
+// Friction contact records of one yarn segment during a sweep (see
+// DeviceCloth::yarn_slot_a/b): the slot tags are loaded at the segment's
+// first contact and kept in registers; the first record of a substep takes
+// slot 0 without a search and retires the older ones.
+struct SegRecords {
+    uint32_t seg;
+    bool loaded, live, recorded;
+    uint32_t rtag[NC_YARN_SLOTS];
+
+    __device__ explicit SegRecords(uint32_t s) : seg(s), loaded(false), live(false), recorded(false) {
+#pragma unroll
+        for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q) rtag[q] = 0u;
+    }
+
+    // Add impulse imp along -n on fruit f with segment weights w0, w1.
+    __device__ void add(const Ctx& ctx, uint32_t f, V3 n, float imp, float w0, float w1) {
+        const DeviceCloth& d = ctx.d;
+        if (!loaded) {
+            loaded = true;
+            live = __ldcg(d.yarn_live + seg) == ctx.epoch;
+            if (live) {
+#pragma unroll
+                for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q)
+                    rtag[q] = __float_as_uint(__ldcg(&d.yarn_slot_b[seg * NC_YARN_SLOTS + q].z));
+            }
+        }
+        const uint32_t tag = (ctx.epoch << 6) | f;
+        int slot = -1;
+        bool fresh = true;
+        if (!live) {
+            slot = 0;
+        } else {
+#pragma unroll
+            for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q) {
+                if (rtag[q] == tag && fresh) {
+                    slot = static_cast<int>(q);
+                    fresh = false;
+                }
+            }
+            if (fresh)
+#pragma unroll
+                for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q)
+                    if (slot < 0 && (rtag[q] >> 6) != (ctx.epoch & 0x3ffffffu)) slot = static_cast<int>(q);
+        }
+        if (slot < 0) {
+            fail(d, NUMI_CLOTH_FAILURE_RANGE);
+            return;
+        }
+        const uint32_t q = static_cast<uint32_t>(slot);
+        float4 sa = make_float4(0, 0, 0, 0);
+        float4 sb = make_float4(0, 0, __uint_as_float(tag), 0);
+        if (!fresh) {
+            sa = __ldcg(&d.yarn_slot_a[seg * NC_YARN_SLOTS + q]);
+            sb = __ldcg(&d.yarn_slot_b[seg * NC_YARN_SLOTS + q]);
+        }
+        const V3 wn = V3{sa.x, sa.y, sa.z} - n * imp;
+        sa = make_float4(wn.x, wn.y, wn.z, sa.w + imp);
+        sb.x = sb.x + w0 * imp;
+        sb.y = sb.y + w1 * imp;
+        d.yarn_slot_a[seg * NC_YARN_SLOTS + q] = sa;
+        d.yarn_slot_b[seg * NC_YARN_SLOTS + q] = sb;
+#pragma unroll
+        for (uint32_t r = 0; r < NC_YARN_SLOTS; ++r)
+            if (r == q) rtag[r] = tag;
+        if (q == 0u && fresh) {
+#pragma unroll
+            for (uint32_t r = 1; r < NC_YARN_SLOTS; ++r) {
+                d.yarn_slot_b[seg * NC_YARN_SLOTS + r].z = __uint_as_float(0u);
+                rtag[r] = 0u;
+            }
+        }
+        live = true;
+        recorded = true;
+    }
+
+    __device__ void finish(const Ctx& ctx) const {
+        if (recorded) ctx.d.yarn_live[seg] = ctx.epoch;
+    }
+};
+
 // One yarn colour of the fruit/yarn sweep.  Fruits do not move during a
 // sweep (their summed displacements are applied after it), so the first
 // colour stages them in shared memory for all colours, the CTA's
@@ -420,9 +505,7 @@ __device__ void yarn_contact_batch(Ctx& ctx, const Batch& bt, bool first, bool l
             mask = own;
         }
         bool changed = false;
-        // contact-record tags of this segment, loaded at its first contact
-        bool rec_loaded = false, seg_live = false, recorded = false;
-        uint32_t rtag[NC_YARN_SLOTS] = {};
+        SegRecords rec(seg);
         while (mask != 0ull) {
             const uint32_t f = static_cast<uint32_t>(__ffsll(static_cast<long long>(mask)) - 1);
             mask &= mask - 1ull;
@@ -457,73 +540,115 @@ __device__ void yarn_contact_batch(Ctx& ctx, const Batch& bt, bool first, bool l
             cta_sums_add(s_sum + 3u * f + 1u, delta.y);
             cta_sums_add(s_sum + 3u * f + 2u, delta.z);
             if (lam <= 0.0f) continue;
-            const float imp = lam / c.dt;
-            // Contact record of (fruit f, segment seg) for friction, kept in
-            // registers until the segment is done.  The first record of the
-            // substep takes slot 0 without a search and retires the others.
-            if (!rec_loaded) {
-                rec_loaded = true;
-                seg_live = __ldcg(d.yarn_live + seg) == ctx.epoch;
-                if (seg_live) {
-#pragma unroll
-                    for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q)
-                        rtag[q] = __float_as_uint(__ldcg(&d.yarn_slot_b[seg * NC_YARN_SLOTS + q].z));
-                }
-            }
-            const uint32_t tag = (ctx.epoch << 6) | f;
-            int slot = -1;
-            bool fresh = true;
-            if (!seg_live) {
-                slot = 0;
-            } else {
-#pragma unroll
-                for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q) {
-                    if (rtag[q] == tag && fresh) {
-                        slot = static_cast<int>(q);
-                        fresh = false;
-                    }
-                }
-                if (fresh)
-#pragma unroll
-                    for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q)
-                        if (slot < 0 && (rtag[q] >> 6) != (ctx.epoch & 0x3ffffffu)) slot = static_cast<int>(q);
-            }
-            if (slot < 0) {
-                fail(d, NUMI_CLOTH_FAILURE_RANGE);
-                continue;
-            }
-            const uint32_t q = static_cast<uint32_t>(slot);
-            float4 sa = make_float4(0, 0, 0, 0);
-            float4 sb = make_float4(0, 0, __uint_as_float(tag), 0);
-            if (!fresh) {
-                sa = __ldcg(&d.yarn_slot_a[seg * NC_YARN_SLOTS + q]);
-                sb = __ldcg(&d.yarn_slot_b[seg * NC_YARN_SLOTS + q]);
-            }
-            const V3 wn = V3{sa.x, sa.y, sa.z} - n * imp;
-            sa = make_float4(wn.x, wn.y, wn.z, sa.w + imp);
-            sb.x = sb.x + w0 * imp;
-            sb.y = sb.y + w1 * imp;
-            d.yarn_slot_a[seg * NC_YARN_SLOTS + q] = sa;
-            d.yarn_slot_b[seg * NC_YARN_SLOTS + q] = sb;
-#pragma unroll
-            for (uint32_t r = 0; r < NC_YARN_SLOTS; ++r)
-                if (r == q) rtag[r] = tag;
-            if (q == 0u && fresh) {
-                // a new substep claims the segment: retire the older records
-#pragma unroll
-                for (uint32_t r = 1; r < NC_YARN_SLOTS; ++r) {
-                    d.yarn_slot_b[seg * NC_YARN_SLOTS + r].z = __uint_as_float(0u);
-                    rtag[r] = 0u;
-                }
-            }
-            seg_live = true;
-            recorded = true;
+            rec.add(ctx, f, n, lam / c.dt, w0, w1);
         }
         if (changed) {
             px_set(ctx, ij.x, pa);
             px_set(ctx, ij.y, pb);
         }
-        if (recorded) d.yarn_live[seg] = ctx.epoch;
+        rec.finish(ctx);
+    }
+    if (last) cta_sums_flush(s_sum, acc, 3u * nf);
+}
+
+// One yarn colour of the swept fruit/yarn sweep (solveSweptBallYarn,
+// tools/cloth_bag.cpp:3022-3109): conservative advancement of every fruit
+// against every segment over the substep's motion, at most 80 steps, then
+// the ground-aware correction of the approach left after the impact.  The
+// batched order is the present sweep's: segments of a colour in parallel,
+// fruits (positions and previous positions) frozen over the sweep, each
+// segment visiting the fruits in ascending order, fruit displacements summed.
+// A fruit whose swept box is farther than the contact distance from the
+// segment's swept box cannot be found by the advancement and is skipped.
+__device__ void swept_contact_batch(Ctx& ctx, const Batch& bt, bool first, bool last) {
+    const DeviceCloth& d = ctx.d;
+    const SubCfg& c = ctx.c;
+    __shared__ float4 s_fx[NC_MAX_FRUITS];   // position xyz, radius
+    __shared__ float4 s_fp[NC_MAX_FRUITS];   // previous position xyz, inverse mass
+    __shared__ unsigned long long s_sum[3u * NC_MAX_FRUITS];
+    const uint32_t nf = d.f_count;
+    if (first) {
+        cta_sums_clear(s_sum, 3u * nf);
+        for (uint32_t f = threadIdx.x; f < nf; f += blockDim.x) {
+            const NumiClothFruit& fr = d.fruits[f];
+            const float4 xw = __ldcg(reinterpret_cast<const float4*>(&fr.positionAndInverseMass));
+            const float4 pr = __ldcg(reinterpret_cast<const float4*>(&fr.previousAndRadius));
+            s_fx[f] = make_float4(xw.x, xw.y, xw.z, pr.w);
+            s_fp[f] = make_float4(pr.x, pr.y, pr.z, xw.w);
+        }
+        __syncthreads();
+    }
+    unsigned long long* acc = reinterpret_cast<unsigned long long*>(d.fruit_partial);
+    for (Range rg = item_range(ctx, bt.yarn); rg.i < rg.end; rg.i += rg.stride) {
+        const uint32_t seg = bt.first + rg.i;
+        const uint2 ij = __ldg(d.d_ij + seg);
+        float4 pa = px(ctx, ij.x), pb = px(ctx, ij.y);
+        const V3 qa = xyz(ld(d.xp + ij.x)), qb = xyz(ld(d.xp + ij.y));
+        bool changed = false;
+        SegRecords rec(seg);
+        for (uint32_t f = 0; f < nf; ++f) {
+            const float4 fx = s_fx[f], fp = s_fp[f];
+            const float target = fx.w + c.radius;
+            // swept boxes
+            const float slack = target + 1.0e-6f;
+            const V3 slo{fminf(fminf(pa.x, pb.x), fminf(qa.x, qb.x)), fminf(fminf(pa.y, pb.y), fminf(qa.y, qb.y)),
+                         fminf(fminf(pa.z, pb.z), fminf(qa.z, qb.z))};
+            const V3 shi{fmaxf(fmaxf(pa.x, pb.x), fmaxf(qa.x, qb.x)), fmaxf(fmaxf(pa.y, pb.y), fmaxf(qa.y, qb.y)),
+                         fmaxf(fmaxf(pa.z, pb.z), fmaxf(qa.z, qb.z))};
+            if (fmaxf(fx.x, fp.x) < slo.x - slack || fminf(fx.x, fp.x) > shi.x + slack ||
+                fmaxf(fx.y, fp.y) < slo.y - slack || fminf(fx.y, fp.y) > shi.y + slack ||
+                fmaxf(fx.z, fp.z) < slo.z - slack || fminf(fx.z, fp.z) > shi.z + slack)
+                continue;
+            const V3 X = xyz(fx), P = xyz(fp);
+            float bound = len3(X - P) + len3(xyz(pa) - qa);
+            bound = bound + len3(xyz(pb) - qb);
+            if (bound < 1.0e-14f) continue;
+            V3 bp, sa, sb, closest;
+            float weight, dist;
+            auto sample = [&](float time) {
+                bp = P + (X - P) * time;
+                sa = qa + (xyz(pa) - qa) * time;
+                sb = qb + (xyz(pb) - qb) * time;
+                point_segment(bp, sa, sb, closest, weight);
+                dist = len3(closest - bp);
+            };
+            float time = 0.0f;
+            sample(0.0f);
+            bool found = dist <= target + 1.0e-9f;
+            if (!found) {
+                for (int it = 0; it < 80; ++it) {
+                    sample(time);
+                    const float gap = dist - target;
+                    if (gap <= 1.0e-9f) {
+                        found = true;
+                        break;
+                    }
+                    const float advance = 0.9f * gap / bound;
+                    if (!isfinite(advance) || advance <= 0.0f || time + advance >= 1.0f) break;
+                    time = time + fmaxf(advance, 1.0e-10f);
+                }
+            }
+            if (!found || dist < 1.0e-12f) continue;
+            const V3 n = vdiv(closest - bp, dist);
+            const float w0 = 1.0f - weight, w1 = weight;
+            const V3 seg_rem = (xyz(pa) - sa) * w0 + (xyz(pb) - sb) * w1;
+            const V3 ball_rem = X - bp;
+            const float removed = dot3(ball_rem - seg_rem, n);
+            if (removed <= 0.0f) continue;
+            V3 delta{0.0f, 0.0f, 0.0f};
+            const float lam = yarn_correction(pa, pb, w0, w1, fp.w, n, removed, c.ground, c.radius, delta);
+            changed = true;
+            cta_sums_add(s_sum + 3u * f + 0u, delta.x);
+            cta_sums_add(s_sum + 3u * f + 1u, delta.y);
+            cta_sums_add(s_sum + 3u * f + 2u, delta.z);
+            if (lam <= 0.0f) continue;
+            rec.add(ctx, f, n, lam / c.dt, w0, w1);
+        }
+        if (changed) {
+            px_set(ctx, ij.x, pa);
+            px_set(ctx, ij.y, pb);
+        }
+        rec.finish(ctx);
     }
     if (last) cta_sums_flush(s_sum, acc, 3u * nf);
 }
@@ -836,7 +961,7 @@ __device__ void residual_partials(Ctx& ctx, double* out3) {
             }
         }
     }
-    __shared__ double s_r[3][NC_BLOCK_MAX];
+    double (*s_r)[NC_BLOCK_MAX] = nc_red_smem;
     s_r[0][threadIdx.x] = strain;
     s_r[1][threadIdx.x] = ground;
     s_r[2][threadIdx.x] = fruit;
@@ -853,7 +978,7 @@ __device__ void residual_partials(Ctx& ctx, double* out3) {
 
 __device__ bool residuals_converged(Ctx& ctx) {
     const DeviceCloth& d = ctx.d;
-    __shared__ double s_r[3][NC_BLOCK_MAX];
+    double (*s_r)[NC_BLOCK_MAX] = nc_red_smem;
     double r[3] = {0.0, 0.0, 0.0};
     for (uint32_t b = threadIdx.x; b < ctx.ranks; b += blockDim.x)
         for (int e = 0; e < 3; ++e) r[e] = fmax(r[e], __ldcg(d.red + 3u * b + e));
@@ -1245,6 +1370,20 @@ __device__ __forceinline__ bool substep(Ctx& ctx, bool last) {
         const float att = air_attenuation(ctx);
         air_apply_advance(ctx, force, att);
         NC_SYNC(ctx);
+    }
+    if (s.swept_fruit_yarn && d.f_count > 0u) {
+        uint32_t first = NC_MAX_BATCHES, last = 0;
+        for (uint32_t b = 0; b < d.n_dist_batches; ++b)
+            if (d.dist_batches[b].yarn != 0u) {
+                first = min(first, b);
+                last = b;
+            }
+        for (uint32_t b = first; b <= last && b < d.n_dist_batches; ++b) {
+            if (d.dist_batches[b].yarn == 0u) continue;
+            swept_contact_batch(ctx, d.dist_batches[b], b == first, b == last);
+            NC_SYNC(ctx);
+        }
+        ctx.fruit_pending = true;
     }
     for (uint32_t it = 0; it < s.iterations; ++it) {
         for (uint32_t b = 0; b < d.n_dist_batches; ++b) {

@@ -825,6 +825,90 @@ struct Sim {
         }
     }
 
+    // solveSweptBallYarn in the kernels' batched order: segments of a yarn
+    // colour in parallel, fruits (positions and previous positions) frozen
+    // over the sweep, each segment visiting the fruits in ascending order,
+    // the fruits' displacements summed and applied after the sweep.
+    void swept_yarn_batched(bool ground, R dt) {
+        if (fruits.empty()) return;
+        const uint32_t nf = static_cast<uint32_t>(fruits.size());
+        std::vector<V<R>> fx(nf), fp(nf);
+        for (uint32_t f = 0; f < nf; ++f) {
+            fx[f] = fruits[f].x;
+            fp[f] = fruits[f].prev;
+        }
+        for (const BatchInfo& b : dist_b) {
+            for (uint32_t seg = b.first; seg < b.first + b.yarn; ++seg) {
+                const uint32_t ia = di[seg], ib = dj[seg];
+                V<R> pa = x[ia], pb = x[ib];
+                bool changed = false;
+                for (uint32_t f = 0; f < nf; ++f) {
+                    const Fruit& fr = fruits[f];
+                    const R target = fr.radius + radius;
+                    R bound = len(fx[f] - fp[f]) + len(pa - xp[ia]);
+                    bound = bound + len(pb - xp[ib]);
+                    if (bound < R(1.0e-14)) continue;
+                    V<R> bp, sa, sb, closest;
+                    R weight, dist;
+                    auto sample = [&](R time) {
+                        bp = fp[f] + (fx[f] - fp[f]) * time;
+                        sa = xp[ia] + (pa - xp[ia]) * time;
+                        sb = xp[ib] + (pb - xp[ib]) * time;
+                        point_segment(bp, sa, sb, closest, weight);
+                        dist = len(closest - bp);
+                    };
+                    R time = R(0);
+                    sample(R(0));
+                    bool found = dist <= target + R(1.0e-9);
+                    if (!found) {
+                        for (int it = 0; it < 80; ++it) {
+                            sample(time);
+                            const R gap = dist - target;
+                            if (gap <= R(1.0e-9)) {
+                                found = true;
+                                break;
+                            }
+                            const R advance = R(0.9) * gap / bound;
+                            if (!std::isfinite(advance) || advance <= R(0) || time + advance >= R(1)) break;
+                            time = time + rmax(advance, R(1.0e-10));
+                        }
+                    }
+                    if (!found || dist < R(1.0e-12)) continue;
+                    const V<R> n = vdiv(closest - bp, dist);
+                    const R w0 = R(1) - weight, w1 = weight;
+                    const V<R> seg_rem = (pa - sa) * w0 + (pb - sb) * w1;
+                    const V<R> ball_rem = fx[f] - bp;
+                    const R removed = dot(ball_rem - seg_rem, n);
+                    if (removed <= R(0)) continue;
+                    V<R> delta{};
+                    const R lam = yarn_correction(pa, pb, w[ia], w[ib], w0, w1, fr.w, n, removed, ground, delta);
+                    changed = true;
+                    add_fruit_sum(3u * f + 0u, delta.x);
+                    add_fruit_sum(3u * f + 1u, delta.y);
+                    add_fruit_sum(3u * f + 2u, delta.z);
+                    if (lam <= R(0)) continue;
+                    const R imp = lam / dt;
+                    YarnRecord& r = yarn[{seg, f}];
+                    r.wn = r.wn - n * imp;
+                    r.ni = r.ni + imp;
+                    r.ws0 = r.ws0 + w0 * imp;
+                    r.ws1 = r.ws1 + w1 * imp;
+                    ++yarn_contacts;
+                }
+                if (changed) {
+                    x[ia] = pa;
+                    x[ib] = pb;
+                }
+            }
+        }
+        for (uint32_t f = 0; f < nf; ++f) {
+            const R dx = take_fruit_sum(3u * f + 0u);
+            const R dy = take_fruit_sum(3u * f + 1u);
+            const R dz = take_fruit_sum(3u * f + 2u);
+            fruits[f].x = V<R>{fruits[f].x.x + dx, fruits[f].x.y + dy, fruits[f].x.z + dz};
+        }
+    }
+
     // applyBallYarnFriction (tools/cloth_bag.cpp:3178-3270) for one record.
     void yarn_friction_one(uint32_t seg, uint32_t f, const YarnRecord& r, const Fruit& fr, V<R>& va, V<R>& vb,
                            bool ground, R mu, V<R>& dv, V<R>& dw) {
@@ -1355,7 +1439,12 @@ struct Sim {
         std::fill(dlam.begin(), dlam.end(), R(0));
         std::fill(klam.begin(), klam.end(), R(0));
         std::fill(blam.begin(), blam.end(), R(0));
-        if (s.swept_fruit_yarn && serial) swept_yarn_serial(ground_on, dt);
+        if (s.swept_fruit_yarn) {
+            if (serial)
+                swept_yarn_serial(ground_on, dt);
+            else
+                swept_yarn_batched(ground_on, dt);
+        }
         auto sweep_distance = [&] {
             if (serial)
                 for (uint32_t k = 0; k < di.size(); ++k) solve_distance(k, dt2);

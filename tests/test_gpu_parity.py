@@ -159,3 +159,37 @@ def test_large_square_multi_cta_bitexact(resident):
     o = run_oracle(scene, cfg, s, bits=32)
     assert g["failure"] == 0
     _check_bitexact(g, o)
+
+
+def _fast_fruits(side=24, fruits=6):
+    """Spheres a few mm above the cloth moving down at 6 m/s: 2 mm per substep,
+    so the swept (continuous) fruit/yarn test finds the impacts."""
+    scene = small_square(side=side, fruits=fruits)
+    scene.fruits["velocityAndGroundImpulse"][:, 2] = -6.0
+    return scene
+
+
+@pytest.mark.parametrize("sched", [PLAIN, FULL], ids=["plain", "full"])
+def test_swept_fruit_yarn_bitexact_fp32(sched):
+    """The swept fruit/yarn phase (solveSweptBallYarn, batched order) gives the
+    FP32 oracle's bits, and it changes the result (the impacts are found)."""
+    scene = _fast_fruits()
+    cfg = nc.substep_configs(scene, 12)
+    s = nc.Schedule.make(**dict(sched, sweptFruitYarn=1))
+    g = run_gpu(scene, cfg, s)
+    o = run_oracle(scene, cfg, s, bits=32)
+    assert g["failure"] == 0, nc.failure_names(g["failure"])
+    _check_bitexact(g, o)
+    plain = run_gpu(scene, cfg, nc.Schedule.make(**dict(sched, sweptFruitYarn=0)))
+    assert not np.array_equal(plain["particles"], g["particles"])
+
+
+def test_swept_fruit_yarn_launch_modes():
+    scene = _fast_fruits(side=40, fruits=10)
+    cfg = nc.substep_configs(scene, 8)
+    s = nc.Schedule.make(**dict(FULL, sweptFruitYarn=1))
+    a = run_gpu(scene, cfg, s, env={"NUMI_CLOTH_RESIDENT": "0"})
+    b = run_gpu(scene, cfg, s, grid=6)
+    c = run_gpu(scene, cfg, s)
+    assert np.array_equal(a["particles"], b["particles"]) and np.array_equal(a["particles"], c["particles"])
+    assert np.array_equal(a["fruits"], c["fruits"])
