@@ -257,9 +257,12 @@ int prepare_self_grid(numi_cloth* h, bool self_collision, uint32_t substeps) {
         while (buckets < 2u * h->d.n) buckets <<= 1;
         DeviceCloth& d = h->d;
         d.hash_head = h->buf.alloc<unsigned long long>(buckets);
+        d.hash_over_head = h->buf.alloc<unsigned long long>(1);
+        d.hash_over = h->buf.alloc<HashSlot>(h->d.n);
         d.hash = h->buf.alloc<HashSlot>(static_cast<size_t>(buckets) * NC_HASH_CAP);
         d.self_stats = h->buf.alloc<unsigned long long>(2);
-        if (d.hash_head == nullptr || d.hash == nullptr || d.self_stats == nullptr) {
+        if (d.hash_head == nullptr || d.hash == nullptr || d.self_stats == nullptr || d.hash_over_head == nullptr ||
+            d.hash_over == nullptr) {
             d.hash_head = nullptr;
             return NUMI_CLOTH_ENOMEM;
         }
@@ -267,7 +270,8 @@ int prepare_self_grid(numi_cloth* h, bool self_collision, uint32_t substeps) {
     }
     if (h->d.hash_head != nullptr && ((h->epoch + substeps) >> 26) != (h->epoch >> 26)) {
         if (cudaMemsetAsync(h->d.hash_head, 0, (static_cast<size_t>(h->d.hash_mask) + 1u) * sizeof(unsigned long long),
-                            h->stream) != cudaSuccess)
+                            h->stream) != cudaSuccess ||
+            cudaMemsetAsync(h->d.hash_over_head, 0, sizeof(unsigned long long), h->stream) != cudaSuccess)
             return NUMI_CLOTH_ECUDA;
     }
     return NUMI_CLOTH_OK;

@@ -128,6 +128,10 @@ struct DeviceCloth {
     // passes
     unsigned long long* hash_head;
     HashSlot* hash;       // [buckets * NC_HASH_CAP]
+    // particles whose bucket was full: (pass tag << 32) | count, and [n]
+    // slots, so no particle is ever dropped
+    unsigned long long* hash_over_head;
+    HashSlot* hash_over;
     uint32_t hash_mask;
     // [0] self contacts (a < b pairs resolved), [1] max self penetration
     // (float bits; non-negative so unsigned max orders them)

@@ -735,13 +735,22 @@ __device__ void self_insert(Ctx& ctx, uint32_t it) {
         unsigned long long* head = d.hash_head + bucket;
         atomicMax(head, tag << 32);
         const uint32_t slot = static_cast<uint32_t>(atomicAdd(head, 1ull));
-        if (slot >= NC_HASH_CAP) {
-            fail(d, NUMI_CLOTH_FAILURE_RANGE);
-            continue;
+        HashSlot* e;
+        if (slot < NC_HASH_CAP) {
+            e = d.hash + bucket * NC_HASH_CAP + slot;
+        } else {
+            // a full bucket (a crumpled cloth packs many particles into a
+            // cell): the particle goes to the overflow list every query scans
+            atomicMax(d.hash_over_head, tag << 32);
+            const uint32_t o = static_cast<uint32_t>(atomicAdd(d.hash_over_head, 1ull));
+            if (o >= d.n) {
+                fail(d, NUMI_CLOTH_FAILURE_RANGE);
+                continue;
+            }
+            e = d.hash_over + o;
         }
-        HashSlot& e = d.hash[bucket * NC_HASH_CAP + slot];
-        e.pos = p;
-        e.meta = make_uint4(i, 0u, 0u, 0u);
+        e->pos = p;
+        e->meta = make_uint4(i, 0u, 0u, 0u);
     }
 }
 
@@ -840,6 +849,31 @@ __device__ void self_solve(Ctx& ctx, uint32_t it) {
                 const float L = len3(diff);
                 if (L >= target || L < 1.0e-12f) continue;
                 const float den = p.w + e[j].w;
+                if (den <= 0.0f) continue;
+                if (local_pair(d, a, b)) continue;
+                const V3 corr = diff * ((target - L) / (L * den));
+                sum[0] += to_fixed(-(corr.x * p.w));
+                sum[1] += to_fixed(-(corr.y * p.w));
+                sum[2] += to_fixed(-(corr.z * p.w));
+                touched = true;
+                if (a < b) {
+                    ++contacts;
+                    max_pen = fmaxf(max_pen, target - L);
+                }
+            }
+        }
+        // the overflow list (particles of full buckets)
+        {
+            const unsigned long long oh = l1 ? __ldca(d.hash_over_head) : __ldcg(d.hash_over_head);
+            const uint32_t over = static_cast<uint32_t>(oh >> 32) == tag ? min(static_cast<uint32_t>(oh), d.n) : 0u;
+            for (uint32_t o = 0; o < over; ++o) {
+                const float4 e = __ldcg(&d.hash_over[o].pos);
+                const uint32_t b = __ldcg(&d.hash_over[o].meta.x);
+                if (b == a) continue;
+                const V3 diff = xyz(e) - xyz(p);
+                const float L = len3(diff);
+                if (L >= target || L < 1.0e-12f) continue;
+                const float den = p.w + e.w;
                 if (den <= 0.0f) continue;
                 if (local_pair(d, a, b)) continue;
                 const V3 corr = diff * ((target - L) / (L * den));

@@ -108,3 +108,23 @@ def test_gpu_self_contact_launch_modes(resident):
     b = run_gpu(scene, cfg, s, grid=5)
     assert a["failure"] == 0 and b["failure"] == 0
     assert np.array_equal(a["particles"], b["particles"])
+
+
+@pytest.mark.gpu
+def test_gpu_self_contact_full_buckets_use_the_overflow_list():
+    """A cloth squeezed into a couple of hash cells (far more particles per
+    cell than a bucket holds): the overflow list keeps every particle, the
+    pass stays bit-identical to the oracle and raises no failure."""
+    scene = small_square(side=10, fruits=0)
+    pos = scene.particles["positionAndInverseMass"]
+    centre = pos[:, :3].mean(axis=0)
+    pos[:, 0] = centre[0] + (pos[:, 0] - centre[0]) * np.float32(0.05)
+    pos[:, 1] = centre[1] + (pos[:, 1] - centre[1]) * np.float32(0.05)
+    scene.particles["previousAndMass"][:, :3] = pos[:, :3]
+    cfg = nc.substep_configs(scene, 2)
+    s = nc.Schedule.make(**dict(FULL, selfCollision=1))
+    g = run_gpu(scene, cfg, s)
+    o = run_oracle(scene, cfg, s, bits=32)
+    assert g["failure"] == 0, nc.failure_names(g["failure"])
+    assert np.array_equal(gpu_positions(g).astype(np.float64), o["particles"]["x"])
+    assert g["self_contacts"][0] == o["stats"]["self_contacts"] > 100
