@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <limits>
 #include <map>
 #include <numbers>
 #include <type_traits>
@@ -136,7 +137,22 @@ struct Sim {
     std::vector<double> acc;        // double mode: 9 per fruit
     uint32_t failure = 0;
     uint64_t reconcile_max = 0, cert_max = 0, yarn_contacts = 0, self_contacts = 0;
+    uint64_t edge_contacts = 0, self_friction_contacts = 0;
+    R self_cone = R(0);   // largest tangential / limit ratio of self friction
     uint32_t candidate_mask = 0, released_mask = 0;
+    // yarn segments: the distances that are not shear diagonals, in array
+    // order (the reference's yarnSegments, tools/cloth_bag.cpp:695-713)
+    std::vector<uint32_t> ya, yb;
+    // edge/edge contact impulses of the current substep, keyed
+    // (first segment << 32) | second segment (SelfEdgeEdgeContactImpulse,
+    // tools/cloth_bag.cpp:3962-3985)
+    struct EdgeRecord {
+        uint32_t a0{}, a1{}, b0{}, b1{};
+        V<R> wn;
+        R wf[2]{}, ws[2]{};
+        R ni{};
+    };
+    std::map<uint64_t, EdgeRecord> edge_rec;
 
     // ------------------------------------------------------------- set-up
     bool init(const OracleScene& s) {
@@ -162,6 +178,10 @@ struct Sim {
             di.push_back(d.i); dj.push_back(d.j); dcol.push_back(d.colour); dkind.push_back(d.kind);
             drest.push_back(R(d.rest)); dcomp.push_back(R(d.compliance)); dlam.push_back(R(d.lambda));
             dmax.push_back(R(d.maxext));
+            if (d.kind != 3u) {
+                ya.push_back(d.i);
+                yb.push_back(d.j);
+            }
         }
         for (uint32_t k = 0; k < s.k; ++k) {
             const OracleKnot& q = s.knots[k];
@@ -1130,6 +1150,422 @@ struct Sim {
         return maxpen;
     }
 
+    // ------------------------------------------------------ edge/edge self
+    // closestPointsOnSegments (tools/cloth_bag.cpp:2751-2824): closest points
+    // cp = p0 + (p1 - p0) s and cq = q0 + (q1 - q0) t.
+    static void segment_closest(V<R> p0, V<R> p1, V<R> q0, V<R> q1, V<R>& cp, V<R>& cq, R& s, R& t) {
+        const V<R> d1 = p1 - p0, d2 = q1 - q0, off = p0 - q0;
+        const R l1 = lsq(d1), l2 = lsq(d2), sp = dot(d2, off);
+        const R eps = R(1.0e-20);
+        s = R(0);
+        t = R(0);
+        if (l1 <= eps && l2 <= eps) {
+            cp = p0;
+            cq = q0;
+            return;
+        }
+        if (l1 <= eps) {
+            t = clamp01(sp / l2);
+        } else {
+            const R fp = dot(d1, off);
+            if (l2 <= eps) {
+                s = clamp01(-fp / l1);
+            } else {
+                const R c = dot(d1, d2);
+                const R den = l1 * l2 - c * c;
+                if (den > eps) s = clamp01((c * sp - fp * l2) / den);
+                t = (c * s + sp) / l2;
+                if (t < R(0)) {
+                    t = R(0);
+                    s = clamp01(-fp / l1);
+                } else if (t > R(1)) {
+                    t = R(1);
+                    s = clamp01((c - fp) / l1);
+                }
+            }
+        }
+        cp = p0 + d1 * s;
+        cq = q0 + d2 * t;
+    }
+
+    // selfContactNormal (tools/cloth_bag.cpp:3400-3414).
+    static V<R> contact_normal(V<R> sep, V<R> fa, V<R> fb, V<R> prev_off) {
+        const R L = len(sep);
+        if (L > R(1.0e-12)) return vdiv(sep, L);
+        V<R> nrm = normalized(cross(fa, fb));
+        if (dot(prev_off, nrm) > R(0)) nrm = nrm * R(-1);
+        return nrm;
+    }
+
+    struct Box {
+        V<R> lo{std::numeric_limits<R>::infinity(), std::numeric_limits<R>::infinity(),
+                std::numeric_limits<R>::infinity()};
+        V<R> hi{-std::numeric_limits<R>::infinity(), -std::numeric_limits<R>::infinity(),
+                -std::numeric_limits<R>::infinity()};
+        void add(V<R> p) {   // includePoint (tools/cloth_bag.cpp:3651-3658)
+            lo = {rmin(lo.x, p.x), rmin(lo.y, p.y), rmin(lo.z, p.z)};
+            hi = {rmax(hi.x, p.x), rmax(hi.y, p.y), rmax(hi.z, p.z)};
+        }
+        bool overlaps(const Box& o) const {   // overlapBounds (tools/cloth_bag.cpp:3758-3768)
+            return lo.x <= o.hi.x && hi.x >= o.lo.x && lo.y <= o.hi.y && hi.y >= o.lo.y && lo.z <= o.hi.z &&
+                   hi.z >= o.lo.z;
+        }
+        R centre(uint32_t axis) const {   // boundsCenterAxis (tools/cloth_bag.cpp:3770-3779)
+            return axis == 0u ? R(0.5) * (lo.x + hi.x) : axis == 1u ? R(0.5) * (lo.y + hi.y) : R(0.5) * (lo.z + hi.z);
+        }
+    };
+    struct Sphere {
+        V<R> c;
+        R r{};
+    };
+
+    // edgeBounds (tools/cloth_bag.cpp:3675-3691): the segment (and its
+    // substep-start copy when swept) grown by the expansion.
+    Box edge_box(uint32_t k, bool swept, R ex) const {
+        Box b;
+        b.add(x[ya[k]]);
+        if (swept) b.add(xp[ya[k]]);
+        b.add(x[yb[k]]);
+        if (swept) b.add(xp[yb[k]]);
+        b.lo = b.lo - V<R>{ex, ex, ex};
+        b.hi = b.hi + V<R>{ex, ex, ex};
+        return b;
+    }
+
+    // edgeCollisionSphere (tools/cloth_bag.cpp:3697-3720).
+    Sphere edge_sphere(uint32_t k, bool swept, R ex) const {
+        const V<R> pts[4] = {x[ya[k]], x[yb[k]], xp[ya[k]], xp[yb[k]]};
+        const uint32_t count = swept ? 4u : 2u;
+        V<R> c{};
+        for (uint32_t e = 0; e < count; ++e) c = c + pts[e];
+        c = vdiv(c, static_cast<R>(count));
+        R r = R(0);
+        for (uint32_t e = 0; e < count; ++e) r = rmax(r, len(pts[e] - c));
+        return {c, r + ex};
+    }
+
+    static bool spheres_overlap(const Sphere& a, const Sphere& b) {   // tools/cloth_bag.cpp:3722-3728
+        const R r = a.r + b.r;
+        return lsq(a.c - b.c) <= r * r;
+    }
+
+    bool edge_local(uint32_t i, uint32_t j) const {   // edgePairLocal (tools/cloth_bag.cpp:2740-2749)
+        return local_pair(ya[i], ya[j]) || local_pair(ya[i], yb[j]) || local_pair(yb[i], ya[j]) ||
+               local_pair(yb[i], yb[j]);
+    }
+
+    // Bounding-volume tree over segment boxes (makeCollisionBVH,
+    // buildCollisionBVHNode, gatherCollisionCandidates,
+    // tools/cloth_bag.cpp:3781-3878): leaves of at most 8 primitives; an
+    // inner node orders its primitives by box centre along the longest axis
+    // of the centres (ties by index) and splits them at the middle.  A query
+    // returns the primitives whose boxes overlap, left subtree first, which
+    // is the order of the reference's depth-first stack.
+    struct Tree {
+        struct Node {
+            Box b;
+            uint32_t begin, end, left, right;
+        };
+        std::vector<uint32_t> order;
+        std::vector<Node> nodes;
+        const std::vector<Box>* boxes = nullptr;
+
+        void build(const std::vector<Box>& bx) {
+            boxes = &bx;
+            order.resize(bx.size());
+            for (uint32_t k = 0; k < bx.size(); ++k) order[k] = k;
+            nodes.clear();
+            if (!bx.empty()) node(0u, static_cast<uint32_t>(bx.size()));
+        }
+        uint32_t node(uint32_t begin, uint32_t end) {
+            const uint32_t id = static_cast<uint32_t>(nodes.size());
+            nodes.push_back({});
+            Box all, centres;
+            for (uint32_t k = begin; k < end; ++k) {
+                const Box& b = (*boxes)[order[k]];
+                all.add(b.lo);
+                all.add(b.hi);
+                centres.add({b.centre(0), b.centre(1), b.centre(2)});
+            }
+            nodes[id] = {all, begin, end, ~0u, ~0u};
+            if (end - begin <= 8u) return id;
+            const V<R> e = centres.hi - centres.lo;
+            const uint32_t axis = e.y > e.x ? (e.z > e.y ? 2u : 1u) : (e.z > e.x ? 2u : 0u);
+            std::sort(order.begin() + begin, order.begin() + end, [&](uint32_t a, uint32_t b) {
+                const R ca = (*boxes)[a].centre(axis), cb = (*boxes)[b].centre(axis);
+                return ca < cb || (ca == cb && a < b);
+            });
+            const uint32_t mid = begin + (end - begin) / 2u;
+            const uint32_t l = node(begin, mid);
+            const uint32_t r = node(mid, end);
+            nodes[id].left = l;
+            nodes[id].right = r;
+            return id;
+        }
+        void query(const Box& q, std::vector<uint32_t>& out, uint32_t id = 0u) const {
+            if (id == 0u) out.clear();
+            if (nodes.empty()) return;
+            const Node& nd = nodes[id];
+            if (!nd.b.overlaps(q)) return;
+            if (nd.left == ~0u) {
+                for (uint32_t k = nd.begin; k < nd.end; ++k)
+                    if ((*boxes)[order[k]].overlaps(q)) out.push_back(order[k]);
+                return;
+            }
+            query(q, out, nd.left);
+            query(q, out, nd.right);
+        }
+    };
+
+    // Add one solve's impulse into the pair's record (tools/cloth_bag.cpp:3962-3985).
+    void edge_record(uint32_t i, uint32_t j, const EdgeRecord& local) {
+        const uint64_t key = (static_cast<uint64_t>(i) << 32) | j;
+        auto [it, inserted] = edge_rec.try_emplace(key);
+        EdgeRecord& r = it->second;
+        if (inserted) {
+            r.a0 = ya[i];
+            r.a1 = yb[i];
+            r.b0 = ya[j];
+            r.b1 = yb[j];
+        }
+        r.wn = r.wn + local.wn;
+        for (int e = 0; e < 2; ++e) {
+            r.wf[e] = r.wf[e] + local.wf[e];
+            r.ws[e] = r.ws[e] + local.ws[e];
+        }
+        r.ni = r.ni + local.ni;
+    }
+
+    // The impulse of one solve, as the reference's per-solve record
+    // (tools/cloth_bag.cpp:3545-3557, 3651-3663).
+    static void edge_impulse(EdgeRecord& rec, V<R> nrm, const R fw[2], const R sw[2], R lam, R dt) {
+        const R imp = lam / dt;
+        rec.wn = rec.wn - nrm * imp;
+        for (int e = 0; e < 2; ++e) {
+            rec.wf[e] = rec.wf[e] + fw[e] * imp;
+            rec.ws[e] = rec.ws[e] + sw[e] * imp;
+        }
+        rec.ni = rec.ni + imp;
+    }
+
+    // solveSweptEdgeEdge (tools/cloth_bag.cpp:3452-3567): conservative
+    // advancement of the closest distance from the substep start, then one
+    // position correction that takes back the approach after the impact.
+    R edge_swept(uint32_t i, uint32_t j, R dt, EdgeRecord* rec) {
+        const R target = R(2) * radius;
+        const R tol = R(1.0e-9);
+        const uint32_t id[4] = {ya[i], yb[i], ya[j], yb[j]};
+        R bound = R(0);
+        for (uint32_t e = 0; e < 4u; ++e) bound = bound + len(x[id[e]] - xp[id[e]]);
+        if (bound < R(1.0e-14)) return R(0);
+        V<R> P[4], cp, cq;
+        R s = R(0), t = R(0), dist = R(0);
+        auto sample = [&](R time) {
+            for (uint32_t e = 0; e < 4u; ++e) P[e] = xp[id[e]] + (x[id[e]] - xp[id[e]]) * time;
+            segment_closest(P[0], P[1], P[2], P[3], cp, cq, s, t);
+            dist = len(cq - cp);
+        };
+        R time = R(0);
+        sample(R(0));
+        bool found = dist <= target + tol;
+        if (!found) {
+            for (uint32_t k = 0; k < 80u; ++k) {
+                sample(time);
+                const R gap = dist - target;
+                if (gap <= tol) {
+                    found = true;
+                    break;
+                }
+                const R adv = R(0.9) * gap / bound;
+                if (!std::isfinite(adv) || adv <= R(0) || time + adv >= R(1)) break;
+                time = time + rmax(adv, R(1.0e-10));
+            }
+        }
+        if (!found) return R(0);
+        const R fw[2] = {R(1) - s, s}, sw[2] = {R(1) - t, t};
+        const V<R> fprev = xp[id[0]] * fw[0] + xp[id[1]] * fw[1];
+        const V<R> sprev = xp[id[2]] * sw[0] + xp[id[3]] * sw[1];
+        const V<R> nrm = contact_normal(cq - cp, P[1] - P[0], P[3] - P[2], fprev - sprev);
+        V<R> frem{}, srem{};
+        for (uint32_t e = 0; e < 2u; ++e) {
+            frem = frem + (x[id[e]] - P[e]) * fw[e];
+            srem = srem + (x[id[e + 2u]] - P[e + 2u]) * sw[e];
+        }
+        const R removed = dot(frem - srem, nrm);
+        if (removed <= R(0)) return R(0);
+        R den = R(0);
+        for (uint32_t e = 0; e < 2u; ++e) {
+            den = den + w[id[e]] * fw[e] * fw[e];
+            den = den + w[id[e + 2u]] * sw[e] * sw[e];
+        }
+        if (den <= R(0)) return R(0);
+        const R lam = removed / den;
+        for (uint32_t e = 0; e < 2u; ++e) {
+            x[id[e]] = x[id[e]] - nrm * (w[id[e]] * fw[e] * lam);
+            x[id[e + 2u]] = x[id[e + 2u]] + nrm * (w[id[e + 2u]] * sw[e] * lam);
+        }
+        if (rec) edge_impulse(*rec, nrm, fw, sw, lam, dt);
+        ++edge_contacts;
+        return removed;
+    }
+
+    // solveEdgeEdge (tools/cloth_bag.cpp:3569-3640): push two segments
+    // closer than the yarn diameter apart at their closest points.
+    R edge_present(uint32_t i, uint32_t j, R dt, EdgeRecord* rec) {
+        const R target = R(2) * radius;
+        const uint32_t id[4] = {ya[i], yb[i], ya[j], yb[j]};
+        V<R> cp, cq;
+        R s, t;
+        segment_closest(x[id[0]], x[id[1]], x[id[2]], x[id[3]], cp, cq, s, t);
+        const V<R> sep = cq - cp;
+        const R dist = len(sep);
+        if (dist >= target) return R(0);
+        const R fw[2] = {R(1) - s, s}, sw[2] = {R(1) - t, t};
+        const V<R> fprev = xp[id[0]] * fw[0] + xp[id[1]] * fw[1];
+        const V<R> sprev = xp[id[2]] * sw[0] + xp[id[3]] * sw[1];
+        const V<R> nrm = contact_normal(sep, x[id[1]] - x[id[0]], x[id[3]] - x[id[2]], fprev - sprev);
+        R den = R(0);
+        for (uint32_t e = 0; e < 2u; ++e) {
+            den = den + w[id[e]] * fw[e] * fw[e];
+            den = den + w[id[e + 2u]] * sw[e] * sw[e];
+        }
+        if (den <= R(0)) return target - dist;
+        const R lam = (target - dist) / den;
+        for (uint32_t e = 0; e < 2u; ++e) {
+            x[id[e]] = x[id[e]] - nrm * (w[id[e]] * fw[e] * lam);
+            x[id[e + 2u]] = x[id[e + 2u]] + nrm * (w[id[e + 2u]] * sw[e] * lam);
+        }
+        if (rec) edge_impulse(*rec, nrm, fw, sw, lam, dt);
+        ++edge_contacts;
+        return target - dist;
+    }
+
+    // solvePrimitiveSelfCollision (tools/cloth_bag.cpp:3880-3993), serial
+    // order: segment by segment, its candidates in tree order, boxes and
+    // spheres of the tree taken at the start of the pass and the query box
+    // at the segment's turn.
+    R edge_serial(bool swept, R dt, bool ascending = false) {
+        const R ex = R(0.5) * (R(2) * radius);
+        const uint32_t m = static_cast<uint32_t>(ya.size());
+        std::vector<Box> boxes(m);
+        std::vector<Sphere> sph(m);
+        for (uint32_t k = 0; k < m; ++k) {
+            boxes[k] = edge_box(k, swept, ex);
+            sph[k] = edge_sphere(k, swept, ex);
+        }
+        Tree tree;
+        tree.build(boxes);
+        std::vector<uint32_t> cand;
+        R maxc = R(0);
+        for (uint32_t i = 0; i < m; ++i) {
+            tree.query(edge_box(i, swept, ex), cand);
+            if (ascending) std::sort(cand.begin(), cand.end());
+            for (uint32_t j : cand) {
+                if (j <= i || !spheres_overlap(sph[i], sph[j]) || edge_local(i, j)) continue;
+                EdgeRecord local{};
+                const R c = swept ? edge_swept(i, j, dt, &local) : edge_present(i, j, dt, &local);
+                maxc = rmax(maxc, c);
+                if (local.ni > R(0)) edge_record(i, j, local);
+            }
+        }
+        return maxc;
+    }
+
+    // measurePrimitiveSelfPenetration (tools/cloth_bag.cpp:4182-4247): the
+    // deepest non-local segment pair.  Every pair closer than the yarn
+    // diameter passes the box and sphere filters, so the value is the
+    // maximum over all non-local pairs (and 0).
+    R edge_penetration() const {
+        const R target = R(2) * radius;
+        const R ex = R(0.5) * target;
+        const uint32_t m = static_cast<uint32_t>(ya.size());
+        std::vector<Box> boxes(m);
+        std::vector<Sphere> sph(m);
+        for (uint32_t k = 0; k < m; ++k) {
+            boxes[k] = edge_box(k, false, ex);
+            sph[k] = edge_sphere(k, false, ex);
+        }
+        Tree tree;
+        tree.build(boxes);
+        std::vector<uint32_t> cand;
+        R pen = R(0);
+        for (uint32_t i = 0; i < m; ++i) {
+            tree.query(boxes[i], cand);
+            for (uint32_t j : cand) {
+                if (j <= i || !spheres_overlap(sph[i], sph[j]) || edge_local(i, j)) continue;
+                V<R> cp, cq;
+                R s, t;
+                segment_closest(x[ya[i]], x[yb[i]], x[ya[j]], x[yb[j]], cp, cq, s, t);
+                pen = rmax(pen, target - len(cq - cp));
+            }
+        }
+        return pen;
+    }
+
+    // applyClothSelfFriction (tools/cloth_bag.cpp:3995-4090): Coulomb
+    // friction on every pair record in key order, at the record's
+    // impulse-weighted normal and barycentric weights.
+    void edge_friction_serial(R mu) {
+        for (const auto& [key, r] : edge_rec) {
+            if (r.ni <= R(0) || lsq(r.wn) < R(1.0e-20)) continue;
+            const V<R> nrm = normalized(r.wn);
+            R fw[2], sw[2];
+            R fsum = R(0), ssum = R(0);
+            for (int e = 0; e < 2; ++e) {
+                fw[e] = r.wf[e] / r.ni;
+                sw[e] = r.ws[e] / r.ni;
+                fsum = fsum + fw[e];
+                ssum = ssum + sw[e];
+            }
+            if (fsum <= R(1.0e-12) || ssum <= R(1.0e-12)) continue;
+            const uint32_t fi[2] = {r.a0, r.a1}, si[2] = {r.b0, r.b1};
+            V<R> fv{}, sv{};
+            for (int e = 0; e < 2; ++e) {
+                fw[e] = fw[e] / fsum;
+                sw[e] = sw[e] / ssum;
+                fv = fv + v[fi[e]] * fw[e];
+                sv = sv + v[si[e]] * sw[e];
+            }
+            const V<R> rel = fv - sv;
+            const V<R> tv = rel - nrm * dot(rel, nrm);
+            const R slip = len(tv);
+            if (slip < R(1.0e-10)) continue;
+            const V<R> tn = vdiv(tv, slip);
+            R den = R(0);
+            for (int e = 0; e < 2; ++e) {
+                den = den + w[fi[e]] * fw[e] * fw[e];
+                den = den + w[si[e]] * sw[e] * sw[e];
+            }
+            if (den <= R(0)) continue;
+            const R limit = mu * r.ni;
+            const R imp = rmin(slip / den, limit);
+            if (imp <= R(0)) continue;
+            const V<R> on_first = tn * (-imp);
+            for (int e = 0; e < 2; ++e) {
+                v[fi[e]] = v[fi[e]] + on_first * (w[fi[e]] * fw[e]);
+                v[si[e]] = v[si[e]] - on_first * (w[si[e]] * sw[e]);
+            }
+            if (limit > R(0)) self_cone = rmax(self_cone, imp / limit);   // tools/cloth_bag.cpp:1462-1474
+            ++self_friction_contacts;
+        }
+    }
+
+    // The kernels' order (restates solvePrimitiveSelfCollision,
+    // tools/cloth_bag.cpp:3880-3993): the same Gauss-Seidel sweep with the
+    // same pass-start spheres and current query boxes, but the candidates
+    // of a segment in ascending index order instead of the tree's leaf order.
+    R edge_batched(bool swept, R dt) { return edge_serial(swept, dt, true); }
+    // applyClothSelfFriction is already in key order, which the kernels keep.
+    void edge_friction_batched(R mu) { edge_friction_serial(mu); }
+
+    R edge_pass(bool serial, bool swept, R dt) { return serial ? edge_serial(swept, dt) : edge_batched(swept, dt); }
+    void edge_friction(bool serial, R mu) {
+        if (serial)
+            edge_friction_serial(mu);
+        else
+            edge_friction_batched(mu);
+    }
+
     // applyClothGroundFriction for one particle (tools/cloth_bag.cpp:2076-2115).
     static void cloth_ground_friction(V<R>& vel, R wi, R gi, R mu) {
         if (gi <= R(0) || wi <= R(0)) return;
@@ -1393,6 +1829,8 @@ struct Sim {
         const bool ground_on = prm.ground != 0u;
         const V<R> g{R(sub.gravity[0]), R(sub.gravity[1]), R(sub.gravity[2])};
         yarn.clear();
+        edge_rec.clear();
+        const bool prim = s.primitive_self != 0u;
         grip_attach(sub, serial);
         for (Grip& gr : grips) gr.lambda = {};
         const uint32_t n = static_cast<uint32_t>(x.size());
@@ -1439,6 +1877,7 @@ struct Sim {
         std::fill(dlam.begin(), dlam.end(), R(0));
         std::fill(klam.begin(), klam.end(), R(0));
         std::fill(blam.begin(), blam.end(), R(0));
+        if (prim) edge_pass(serial, true, dt);
         if (s.swept_fruit_yarn) {
             if (serial)
                 swept_yarn_serial(ground_on, dt);
@@ -1499,15 +1938,19 @@ struct Sim {
             if (s.early_exit && converged(ground_on)) break;
         }
         reconcile_max = std::max<uint64_t>(reconcile_max, passes);
+        // the endpoint: present edge/edge contacts, then the strain limit
+        // (tools/cloth_bag.cpp:5097-5110)
+        if (prim) edge_pass(serial, false, dt);
         sweep_strain();
         for (uint32_t p = 0; p < s.final_passes; ++p) contacts(false);
         if (last) {
             uint32_t cert = 0;
             for (uint32_t p = 0; p < s.certificate_passes; ++p) {
+                if (prim) edge_pass(serial, false, dt);
                 sweep_strain();
                 for (uint32_t q = 0; q < s.final_passes; ++q) contacts(false);
                 cert = p + 1u;
-                if (converged(ground_on)) break;
+                if (converged(ground_on) && (!prim || edge_penetration() < R(1.0e-6))) break;
             }
             cert_max = std::max<uint64_t>(cert_max, cert);
         }
@@ -1529,6 +1972,7 @@ struct Sim {
         }
         for (Fruit& f : fruits) f.v = (f.x - f.prev) * inv_dt;
         if (s.frictions) {
+            if (prim) edge_friction(serial, R(prm.mu_self));
             yarn_friction(serial, ground_on, R(prm.mu_fruit_yarn));
             if (serial) {
                 for (uint32_t k : serial_pairs) pair_friction(k, R(prm.mu_pair));
@@ -1696,7 +2140,7 @@ double oracle_self_pass(void* p, int serial) {
     return serial ? h->d->self_serial() : h->d->self_batched();
 }
 
-void oracle_stats(void* p, uint64_t out[6]) {
+void oracle_stats(void* p, uint64_t out[8]) {
     auto* h = static_cast<Handle*>(p);
     auto fill = [&](const auto& s) {
         out[0] = s.candidate_mask;
@@ -1705,6 +2149,8 @@ void oracle_stats(void* p, uint64_t out[6]) {
         out[3] = s.cert_max;
         out[4] = s.yarn_contacts;
         out[5] = s.self_contacts;
+        out[6] = s.edge_contacts;
+        out[7] = s.self_friction_contacts;
     };
     if (h->f)
         fill(*h->f);
@@ -1730,6 +2176,62 @@ int oracle_probe_strain(double out[4]) {
     out[2] = 0.5 * (s.x[0].x + s.x[1].x);
     out[3] = 0.0;
     return std::abs(out[0] - 0.285) < 1e-12 && std::abs(out[1] - 0.215) < 1e-12 && std::abs(out[2]) < 1e-12;
+}
+
+// --self-ccd-probe (tools/cloth_bag.cpp:2547-2603): a free segment falls
+// through a fixed crossing one in a single step; the swept solve stops it at
+// the yarn diameter above (yarn radius 4 mm, the authored material).
+int oracle_probe_self_ccd(double out[4]) {
+    Sim<double> s;
+    s.radius = 0.004;
+    s.x = {{-1.0, 0.0, 0.0}, {1.0, 0.0, 0.0}, {0.0, -1.0, -0.02}, {0.0, 1.0, -0.02}};
+    s.xp = {{-1.0, 0.0, 0.0}, {1.0, 0.0, 0.0}, {0.0, -1.0, 0.02}, {0.0, 1.0, 0.02}};
+    s.w = {0.0, 0.0, 1.0, 1.0};
+    s.ya = {0u, 2u};
+    s.yb = {1u, 3u};
+    const double removed = s.edge_swept(0u, 1u, 1.0, nullptr);
+    out[0] = 0.5 * (s.x[2].z + s.x[3].z);
+    out[1] = removed;
+    out[2] = static_cast<double>(s.edge_contacts);
+    out[3] = 0.0;
+    return s.edge_contacts == 1u && std::abs(out[0] - 0.008) < 2.0e-9 && out[1] > 0.027;
+}
+
+// --self-friction-probe (tools/cloth_bag.cpp:4102-4180): one edge/edge record
+// between a segment sliding at 1 m/s and a resting one, normal impulse 10
+// (sticks) and 1 (slides), friction 0.34 (the authored material).
+int oracle_probe_self_friction(double out[8]) {
+    auto run = [](double normal_impulse, double res[4]) {
+        Sim<double> s;
+        s.v = {{1.0, 0.0, 0.0}, {1.0, 0.0, 0.0}, {}, {}};
+        s.w = {1.0, 1.0, 1.0, 1.0};
+        Sim<double>::EdgeRecord r{};
+        r.a0 = 0u; r.a1 = 1u; r.b0 = 2u; r.b1 = 3u;
+        r.wn = {0.0, 0.0, normal_impulse};
+        r.wf[0] = r.wf[1] = r.ws[0] = r.ws[1] = normal_impulse / 2.0;
+        r.ni = normal_impulse;
+        s.edge_rec.emplace(0u, r);
+        s.edge_friction_serial(0.34);
+        const V<double> fv = vdiv(s.v[0] + s.v[1], 2.0), sv = vdiv(s.v[2] + s.v[3], 2.0);
+        double momentum = 0.0, energy = 0.0;
+        for (const V<double>& q : s.v) {
+            momentum += q.x;
+            energy += 0.5 * lsq(q);
+        }
+        res[0] = len(fv - sv);
+        res[1] = momentum;
+        res[2] = energy;
+        res[3] = s.self_cone;
+        return s.self_friction_contacts;
+    };
+    double stick[4], slide[4];
+    const uint64_t c0 = run(10.0, stick), c1 = run(1.0, slide);
+    out[0] = stick[0]; out[1] = stick[1]; out[2] = stick[2];
+    out[3] = slide[0]; out[4] = slide[1]; out[5] = slide[3];
+    out[6] = out[7] = 0.0;
+    return stick[0] < 1e-12 && std::abs(stick[1] - 2.0) < 1e-12 && std::abs(stick[2] - 0.5) < 1e-12 &&
+           slide[0] > 0.5 && std::abs(slide[1] - 2.0) < 1e-12 && std::abs(slide[3] - 1.0) < 1e-12 && c0 == 1u &&
+           c1 == 1u;
 }
 
 // --cloth-ground-friction-probe (tools/cloth_bag.cpp:2302-2368): unit

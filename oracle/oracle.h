@@ -103,7 +103,7 @@ typedef struct OracleSchedule {
     uint32_t self_collision, aerodynamics, swept_ground, swept_fruit_yarn, frictions, release;
     double damping;
     uint32_t mode;      /* 0 batched, 1 serial */
-    uint32_t pad;
+    uint32_t primitive_self;   /* edge/edge yarn self-collision and self friction */
 } OracleSchedule;
 
 typedef struct OracleScene {
@@ -137,8 +137,9 @@ void oracle_write(void* h, const OracleParticle* particles, const OracleFruit* f
 void oracle_residuals(void* h, double out[4]);
 /* Release masks (mouth candidates, released) and counters:
  * out[0..1] masks, out[2] max reconcile passes, out[3] max certificate passes,
- * out[4] fruit/yarn contacts, out[5] self contacts. */
-void oracle_stats(void* h, uint64_t out[6]);
+ * out[4] fruit/yarn contacts, out[5] self contacts, out[6] edge/edge
+ * contacts, out[7] self-friction contacts. */
+void oracle_stats(void* h, uint64_t out[8]);
 /* One point self-contact pass on the current state (serial = the
  * reference's Gauss-Seidel order, else the batched order); returns the
  * largest penetration it resolved. */
@@ -148,6 +149,8 @@ int oracle_probe_strain(double out[4]);
 int oracle_probe_cloth_ground_friction(double out[4]);
 int oracle_probe_rolling(double out[4]);
 int oracle_probe_aerodynamics(double out[8]);
+int oracle_probe_self_ccd(double out[4]);
+int oracle_probe_self_friction(double out[8]);
 
 #ifdef __cplusplus
 }

@@ -81,7 +81,7 @@ class OSchedule(ctypes.Structure):
             "iterations", "strain_sweeps", "reconcile_passes", "final_passes", "certificate_passes", "early_exit",
             "self_collision", "aerodynamics", "swept_ground", "swept_fruit_yarn", "frictions", "release",
         )
-    ] + [("damping", ctypes.c_double), ("mode", ctypes.c_uint32), ("pad", ctypes.c_uint32)]
+    ] + [("damping", ctypes.c_double), ("mode", ctypes.c_uint32), ("primitive_self", ctypes.c_uint32)]
 
 
 class OScene(ctypes.Structure):
@@ -127,7 +127,8 @@ def lib() -> ctypes.CDLL:
         L.oracle_self_pass.restype = ctypes.c_double
         L.oracle_self_pass.argtypes = [vp, ctypes.c_int]
         for name, n in (("oracle_probe_strain", 4), ("oracle_probe_cloth_ground_friction", 4),
-                        ("oracle_probe_rolling", 4), ("oracle_probe_aerodynamics", 8)):
+                        ("oracle_probe_rolling", 4), ("oracle_probe_aerodynamics", 8),
+                        ("oracle_probe_self_ccd", 4), ("oracle_probe_self_friction", 8)):
             fn = getattr(L, name)
             fn.restype = ctypes.c_int
             fn.argtypes = [ctypes.POINTER(ctypes.c_double)]
@@ -270,7 +271,7 @@ def schedule(mode=BATCHED, **kw) -> OSchedule:
     s = OSchedule()
     d = dict(iterations=1, strain_sweeps=3, reconcile_passes=8, final_passes=2, certificate_passes=128,
              early_exit=1, self_collision=0, aerodynamics=1, swept_ground=1, swept_fruit_yarn=0, frictions=1,
-             release=0, damping=0.0)
+             release=0, damping=0.0, primitive_self=0)
     d.update(kw)
     for k, v in d.items():
         setattr(s, k, v)
@@ -330,8 +331,8 @@ class Oracle:
         return float(lib().oracle_self_pass(self._h, 1 if serial else 0))
 
     def stats(self) -> dict:
-        out = (ctypes.c_uint64 * 6)()
+        out = (ctypes.c_uint64 * 8)()
         lib().oracle_stats(self._h, out)
         keys = ("candidate_mask", "released_mask", "reconcile_max", "certificate_max", "yarn_contacts",
-                "self_contacts")
+                "self_contacts", "edge_contacts", "self_friction_contacts")
         return dict(zip(keys, (int(v) for v in out)))

@@ -10,8 +10,9 @@ It builds oracle/_ref (oracle/ref.mk), then writes into tests/golden/:
                         trajectories v1-v3, material artifacts), copied as data
   ref_<case>.npz        reference scene (construction order, FP64), the grip
                         pose of every substep, and the reference's final
-                        particle/fruit state after the reference substep loop
-                        without the primitive (edge/edge) self-collision family
+                        particle/fruit state after the reference substep loop,
+                        without (final_*) and with (full_*) the primitive
+                        (edge/edge) self-collision family
   ref_probes.txt        stdout of the reference executable's analytic probes
   ref_hashes.json       reference simulate() state hashes (full substep) and
                         the shim loop's hash of the same runs
@@ -83,6 +84,8 @@ def main():
             local_off=scene.local_off, local_idx=scene.local_idx, params=params, substeps=run["substeps"],
             final_particles=run["particles"], final_fruits=run["fruits"],
             masks=np.array([run["released_mask"], run["candidate_mask"]], np.uint64),
+            full_particles=full["particles"], full_fruits=full["fruits"],
+            full_masks=np.array([full["released_mask"], full["candidate_mask"]], np.uint64),
             meta=np.array([steps, subs, its], np.uint32))
         print(name, hashes[name])
     with open(os.path.join(HERE, "ref_hashes.json"), "w") as f:

@@ -60,6 +60,35 @@ def test_oracle_serial_matches_reference(name):
         assert stats["candidate_mask"] == int(z["masks"][1])
 
 
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_serial_full_family_matches_reference(name):
+    """With the edge/edge yarn self-collision family and its self friction
+    switched on, the serial order reproduces the reference substep loop (as
+    the reference simulate() runs it) bit for bit."""
+    z, scene = load_case(name)
+    steps, subs, its = (int(v) for v in z["meta"])
+    grounded = name == "grounded"
+    o = op.Oracle(scene, 64)
+    sched = reference_schedule(its, 0 if grounded else 1)
+    sched.primitive_self = 1
+    fail = 0
+    for s in range(steps):
+        fail |= o.step(z["substeps"][s * subs:(s + 1) * subs], sched)
+    assert fail == 0
+    st = o.read()
+    ref_p, ref_f = z["full_particles"], z["full_fruits"]
+    for field in ("x", "v", "prev"):
+        assert np.array_equal(st["particles"][field], ref_p[field]), (
+            field, np.abs(st["particles"][field] - ref_p[field]).max())
+    for field in ("x", "v", "omega", "q"):
+        assert np.array_equal(st["fruits"][field], ref_f[field]), field
+    stats = o.stats()
+    assert stats["edge_contacts"] > 0 and stats["self_friction_contacts"] > 0
+    if not grounded:
+        assert stats["released_mask"] == int(z["full_masks"][0])
+        assert stats["candidate_mask"] == int(z["full_masks"][1])
+
+
 def test_oracle_batched_close_to_serial():
     """The batched (GPU) colour order is a different Gauss-Seidel order; over
     one short frame it stays close to the reference order."""
@@ -82,7 +111,7 @@ def test_restated_probes_known_answers():
 
     L = op.lib()
     for name, n in (("oracle_probe_strain", 4), ("oracle_probe_cloth_ground_friction", 4),
-                    ("oracle_probe_rolling", 4)):
+                    ("oracle_probe_rolling", 4), ("oracle_probe_self_ccd", 4), ("oracle_probe_self_friction", 8)):
         out = (ctypes.c_double * n)()
         assert getattr(L, name)(out) == 1, name
 
@@ -124,6 +153,16 @@ def test_probes_match_reference_printout():
     assert f"{a[4]:.12f}" == ref["fruit_speed"]
     assert f"{a[5]:.12f}" == ref["fruit_angular_speed"]
     assert abs(a[0] - a[2]) < 1e-12 and abs(a[1] - a[3]) < 1e-12   # refinement invariance
+    L.oracle_probe_self_ccd(out)
+    ref = vals["continuous_yarn_capsule_self_contact"]
+    assert f"{out[0]:.12f}" == ref["edge_contact_height"]
+    assert f"{out[1]:.12f}" == ref["edge_removed_advance"]
+    assert int(out[2]) == int(ref["edge_contacts"])
+    L.oracle_probe_self_friction(a)
+    ref = vals["cloth_self_coulomb_friction"]
+    for k, key in enumerate(("sticking_slip", "sticking_momentum", "sticking_energy", "sliding_slip",
+                             "sliding_momentum", "sliding_cone_ratio")):
+        assert f"{a[k]:.12f}" == ref[key], key
 
 
 def test_shim_loop_equals_reference_simulate():
