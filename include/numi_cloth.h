@@ -158,7 +158,11 @@ typedef struct NumiClothSchedule {
     uint32_t frictions;             /* 1: apply the Coulomb/rolling frictions */
     uint32_t release;               /* 1: update the mouth release masks */
     float damping;                  /* v <- v/(1+c dt) after gravity; 0 = reference */
-    uint32_t reserved[3];
+    uint32_t primitiveSelf;         /* 1: edge/edge yarn self-collision (swept before
+                                       the iterations, present at every endpoint),
+                                       its certificate test and yarn/yarn self
+                                       friction (tools/cloth_bag.cpp:3880-4247) */
+    uint32_t reserved[2];
 } NumiClothSchedule;
 
 /* Scene handed to numi_cloth_create.  Constraint arrays must be grouped in
@@ -232,6 +236,13 @@ int numi_cloth_residuals(numi_cloth_t* handle, double out[4]);
  * maximumSelfPenetration (tools/cloth_bag.cpp:4949-4958).  Zero until a
  * step ran with selfCollision. */
 int numi_cloth_self_contacts(numi_cloth_t* handle, unsigned long long* contacts, double* max_penetration);
+
+/* Edge/edge yarn self-collision counters since create: out[0] edge/edge
+ * solves that moved particles (the reference's edgeEdgeSelfContacts plus
+ * sweptEdgeEdgeSelfContacts), out[1] yarn/yarn self-friction contacts
+ * (clothSelfFrictionContacts), tools/cloth_bag.cpp:3986-3992, 4085.  Zero
+ * until a step ran with primitiveSelf. */
+int numi_cloth_edge_contacts(numi_cloth_t* handle, unsigned long long out[2]);
 
 /* Release masks after the last step: out[0] fruits that entered the mouth
  * (candidates), out[1] fruits released, one bit per fruit, sticky since

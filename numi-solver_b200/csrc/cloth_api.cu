@@ -97,6 +97,7 @@ struct numi_cloth {
     uint32_t launches = 0;
     uint32_t trace_capacity = 0;   // substeps the trace buffer holds
     uint32_t last_substeps = 0;
+    float yarn_rest_median = 0.0f;   // median yarn segment rest length
     Snapshot snaps[kSnapshotSlots];
     // dynamic state regions copied by snapshot/restore
     struct Region {
@@ -111,13 +112,41 @@ namespace {
 // cudaFuncAttributeMaxDynamicSharedMemorySize is per function, not per
 // launch, and cloths with different launch modes share the frame kernel: only
 // ever raise it, so that creating one cloth never breaks another's launch.
-cudaError_t raise_frame_smem(size_t bytes) {
+// The frame and batch kernels come in two builds: without and with the
+// edge/edge yarn self-collision phases (primitiveSelf).
+const void* frame_fn(bool edge) {
+    return edge ? reinterpret_cast<const void*>(numi_cloth_frame_edge_kernel)
+                : reinterpret_cast<const void*>(numi_cloth_frame_kernel);
+}
+const void* batch_fn(bool edge) {
+    return edge ? reinterpret_cast<const void*>(numi_cloth_batch_edge_kernel)
+                : reinterpret_cast<const void*>(numi_cloth_batch_kernel);
+}
+
+cudaError_t raise_smem(const void* fn, size_t bytes) {
     cudaFuncAttributes fa{};
-    cudaError_t e = cudaFuncGetAttributes(&fa, numi_cloth_frame_kernel);
+    cudaError_t e = cudaFuncGetAttributes(&fa, fn);
     if (e != cudaSuccess) return e;
     if (static_cast<size_t>(fa.maxDynamicSharedSizeBytes) >= bytes) return cudaSuccess;
-    return cudaFuncSetAttribute(numi_cloth_frame_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(bytes));
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+}
+cudaError_t raise_frame_smem(size_t bytes) {
+    cudaError_t e = raise_smem(frame_fn(false), bytes);
+    return e == cudaSuccess ? raise_smem(frame_fn(true), bytes) : e;
+}
+void allow_large_clusters() {
+    for (bool edge : {false, true})
+        cudaFuncSetAttribute(frame_fn(edge), cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+}
+// Clusters of cfg's shape that both frame kernels can place at once.
+int frame_clusters(const cudaLaunchConfig_t& cfg) {
+    int lo = 1 << 30;
+    for (bool edge : {false, true}) {
+        int clusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&clusters, frame_fn(edge), &cfg) != cudaSuccess) return 0;
+        lo = std::min(lo, clusters);
+    }
+    return lo;
 }
 
 bool finite4(const numi_float4& v) {
@@ -198,6 +227,7 @@ cudaError_t launch(numi_cloth* h, uint32_t substeps, const Schedule& s, uint32_t
     Schedule sc = s;
     sc.substeps = substeps;
     void* args[] = {&d, &sc};
+    const bool edge = sc.primitive_self != 0u && d.edge_head != nullptr;
     if (d.trace != nullptr && substeps > h->trace_capacity) d.trace = nullptr;
     if (d.trace == nullptr) d.trace_cta = nullptr;
     cudaError_t e = cudaMemsetAsync(h->d.bar_count, 0, 32 * sizeof(unsigned long long), h->stream);
@@ -218,13 +248,11 @@ cudaError_t launch(numi_cloth* h, uint32_t substeps, const Schedule& s, uint32_t
         cfg.attrs = &attr;
         cfg.numAttrs = 1;
         d.cluster_barrier = 1u;
-        e = cudaLaunchKernelEx(&cfg, numi_cloth_frame_kernel, d, sc);
+        e = cudaLaunchKernelExC(&cfg, frame_fn(edge), args);
     } else if (h->grid == 1) {
-        e = cudaLaunchKernel(reinterpret_cast<const void*>(numi_cloth_frame_kernel), dim3(1), dim3(h->block), args,
-                             smem, h->stream);
+        e = cudaLaunchKernel(frame_fn(edge), dim3(1), dim3(h->block), args, smem, h->stream);
     } else {
-        e = cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(numi_cloth_frame_kernel), dim3(h->grid),
-                                        dim3(h->block), args, smem, h->stream);
+        e = cudaLaunchCooperativeKernel(frame_fn(edge), dim3(h->grid), dim3(h->block), args, smem, h->stream);
     }
     if (e == cudaSuccess) ++h->launches;
     return e;
@@ -245,6 +273,7 @@ Schedule device_schedule(const NumiClothSchedule& schedule) {
     s.frictions = schedule.frictions;
     s.release = schedule.release;
     s.damping = schedule.damping;
+    s.primitive_self = schedule.primitiveSelf;
     return s;
 }
 
@@ -273,6 +302,66 @@ int prepare_self_grid(numi_cloth* h, bool self_collision, uint32_t substeps) {
                             h->stream) != cudaSuccess ||
             cudaMemsetAsync(h->d.hash_over_head, 0, sizeof(unsigned long long), h->stream) != cudaSuccess)
             return NUMI_CLOTH_ECUDA;
+    }
+    return NUMI_CLOTH_OK;
+}
+
+// Edge/edge buffers of a cloth, allocated on first use: a segment grid of
+// about two buckets per yarn segment, room for 32 listed pairs and 16
+// candidate pairs per segment.  The grid cell is four times the cover sphere
+// of a median yarn segment stretched by half (larger spheres go to the
+// list).  The bucket heads are cleared when the 23-bit substep part of their
+// tags wraps within the next `substeps`.
+int prepare_edge_grid(numi_cloth* h, bool primitive, uint32_t substeps, float radius) {
+    DeviceCloth& d = h->d;
+    if (primitive && d.edge_head == nullptr && d.y_count > 0u) {
+        uint32_t buckets = 1024u;
+        while (buckets < 2u * d.y_count) buckets <<= 1;
+        const uint32_t cap = std::max(1024u, 16u * d.y_count);
+        const uint32_t list_cap = std::max(2048u, 32u * d.y_count);
+        DeviceCloth e = d;
+        e.edge_head = h->buf.alloc<unsigned long long>(buckets);
+        e.edge_slot = h->buf.alloc<HashSlot>(static_cast<size_t>(buckets) * NC_HASH_CAP);
+        e.edge_list_head = h->buf.alloc<unsigned long long>(1);
+        e.edge_list = h->buf.alloc<HashSlot>(d.y_count);
+        e.edge_flag = h->buf.alloc<uint32_t>(d.y_count);
+        e.edge_pairs = h->buf.alloc<uint2>(list_cap);
+        e.edge_xb = h->buf.alloc<float4>(d.n);
+        e.edge_pb = h->buf.alloc<float4>(d.n);
+        e.edge_built_radius = h->buf.alloc<float>(1);
+        e.edge_sph = h->buf.alloc<float4>(d.y_count);
+        e.edge_x0 = h->buf.alloc<float4>(d.n);
+        e.edge_path = h->buf.alloc<float>(d.n);
+        e.edge_cand = h->buf.alloc<uint4>(cap);
+        e.edge_order = h->buf.alloc<unsigned long long>(cap);
+        e.edge_sorted = h->buf.alloc<unsigned long long>(cap);
+        e.edge_new = h->buf.alloc<EdgeRecord>(cap);
+        e.edge_rec = h->buf.alloc<EdgeRecord>(cap);
+        e.edge_ctl = h->buf.alloc<uint32_t>(8);
+        e.edge_stats = h->buf.alloc<unsigned long long>(2);
+        e.edge_red = h->buf.alloc<double>(2u * std::max<uint32_t>(h->grid, 1u));
+        if (!e.edge_head || !e.edge_slot || !e.edge_list_head || !e.edge_list || !e.edge_flag || !e.edge_pairs ||
+            !e.edge_xb || !e.edge_pb || !e.edge_built_radius || !e.edge_sph || !e.edge_x0 || !e.edge_path ||
+            !e.edge_cand || !e.edge_order || !e.edge_sorted || !e.edge_new || !e.edge_rec || !e.edge_ctl ||
+            !e.edge_stats || !e.edge_red)
+            return NUMI_CLOTH_ENOMEM;
+        e.edge_mask = buckets - 1u;
+        e.edge_cap = cap;
+        e.edge_list_cap = list_cap;
+        d = e;
+    }
+    if (d.edge_head != nullptr) {
+        d.edge_cell = 4.0f * (0.75f * h->yarn_rest_median + 2.0f * radius);
+        if (const char* v = std::getenv("NUMI_CLOTH_EDGE_CELL")) {
+            const float cell = std::strtof(v, nullptr);   // test hook: force the grid or the list path
+            if (cell > 0.0f) d.edge_cell = cell;
+        }
+        if (((h->epoch + substeps) >> 23) != (h->epoch >> 23)) {
+            if (cudaMemsetAsync(d.edge_head, 0, (static_cast<size_t>(d.edge_mask) + 1u) * sizeof(unsigned long long),
+                                h->stream) != cudaSuccess ||
+                cudaMemsetAsync(d.edge_list_head, 0, sizeof(unsigned long long), h->stream) != cudaSuccess)
+                return NUMI_CLOTH_ECUDA;
+        }
     }
     return NUMI_CLOTH_OK;
 }
@@ -426,8 +515,11 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
     uint32_t block = NC_THREADS;
     if (env_u32("NUMI_CLOTH_BLOCK", block) && block != NC_BLOCK_MAX) block = NC_THREADS;
     h->block = block;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, numi_cloth_frame_kernel, static_cast<int>(block),
-                                                  nc_resident_offset());
+    for (bool edge : {false, true}) {
+        int k = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, frame_fn(edge), static_cast<int>(block), nc_resident_offset());
+        per_sm = edge ? std::min(per_sm, k) : k;
+    }
     uint32_t work = std::max({n, D, K, B});
     uint32_t grid = (work <= 8192u) ? 1u : std::min<uint32_t>(sms * std::max(per_sm, 1), (work + block - 1u) / block);
     uint32_t forced = 0;
@@ -457,12 +549,13 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
         const size_t smem = nc_resident_offset() + 2u * (static_cast<size_t>(1u) << shift) * sizeof(float4);
         int max_optin = 0;
         cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
-        cudaFuncAttributes fa{};
-        cudaFuncGetAttributes(&fa, numi_cloth_frame_kernel);
-        bool ok = smem + fa.sharedSizeBytes <= static_cast<size_t>(max_optin) &&
+        cudaFuncAttributes fa{}, fe{};
+        cudaFuncGetAttributes(&fa, frame_fn(false));
+        cudaFuncGetAttributes(&fe, frame_fn(true));
+        bool ok = smem + std::max(fa.sharedSizeBytes, fe.sharedSizeBytes) <= static_cast<size_t>(max_optin) &&
                   raise_frame_smem(smem) == cudaSuccess;
         if (ok && ranks > 1u) {
-            cudaFuncSetAttribute(numi_cloth_frame_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+            allow_large_clusters();
             cudaLaunchConfig_t cfg{};
             cfg.gridDim = dim3(ranks);
             cfg.blockDim = dim3(NC_BLOCK_MAX);
@@ -474,9 +567,7 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
             attr.val.clusterDim.z = 1;
             cfg.attrs = &attr;
             cfg.numAttrs = 1;
-            int clusters = 0;
-            ok = cudaOccupancyMaxActiveClusters(&clusters, numi_cloth_frame_kernel, &cfg) == cudaSuccess &&
-                 clusters >= 1;
+            ok = frame_clusters(cfg) >= 1;
         }
         cudaGetLastError();
         if (ok) {
@@ -492,7 +583,7 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
         }
     }
     if (h->grid > 1 && want_cluster > 0 && forced == 0) {
-        cudaFuncSetAttribute(numi_cloth_frame_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        allow_large_clusters();
         for (uint32_t c : {want_cluster, 8u}) {
             if (c > 16u || c < 2u) continue;
             cudaLaunchConfig_t cfg{};
@@ -506,9 +597,7 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
             attr.val.clusterDim.z = 1;
             cfg.attrs = &attr;
             cfg.numAttrs = 1;
-            int clusters = 0;
-            if (cudaOccupancyMaxActiveClusters(&clusters, numi_cloth_frame_kernel, &cfg) == cudaSuccess &&
-                clusters >= 1) {
+            if (frame_clusters(cfg) >= 1) {
                 h->cluster = c;
                 h->grid = c;
                 h->block = NC_BLOCK_MAX;
@@ -587,6 +676,26 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
     up(d.v, hv.data(), n * sizeof(float4));
     up(rest, hr.data(), n * sizeof(float4));
     up(d_ij, hij.data(), D * sizeof(uint2));
+    {
+        // yarn segments: the distances that are not shear diagonals, in array order
+        std::vector<uint2> hy;
+        std::vector<float> rest_lengths;
+        for (uint32_t k = 0; k < D; ++k) {
+            const NumiClothDistance& r = scene->distances[k];
+            if (r.particlesAndColor.w == 3u) continue;
+            hy.push_back(make_uint2(r.particlesAndColor.x, r.particlesAndColor.y));
+            rest_lengths.push_back(r.material.x);
+        }
+        if (!rest_lengths.empty()) {
+            std::nth_element(rest_lengths.begin(), rest_lengths.begin() + rest_lengths.size() / 2, rest_lengths.end());
+            h->yarn_rest_median = rest_lengths[rest_lengths.size() / 2];
+        }
+        uint2* y_ij = h->buf.alloc<uint2>(hy.size());
+        if (y_ij == nullptr && e == cudaSuccess) e = cudaErrorMemoryAllocation;
+        d.y_ij = y_ij;
+        d.y_count = static_cast<uint32_t>(hy.size());
+        up(y_ij, hy.data(), hy.size() * sizeof(uint2));
+    }
     up(d_mat, hdm.data(), D * sizeof(float4));
     up(d.d_lambda, hdl.data(), D * sizeof(float));
     up(k_ij, hkij.data(), K * sizeof(uint4));
@@ -676,7 +785,8 @@ int numi_cloth_step(numi_cloth_t* h, const NumiClothConfig* configs, uint32_t co
         cudaSuccess)
         return NUMI_CLOTH_ECUDA;
     const Schedule s = device_schedule(*schedule);
-    const int rc = prepare_self_grid(h, s.self_collision != 0u, count);
+    int rc = prepare_self_grid(h, s.self_collision != 0u, count);
+    if (rc == NUMI_CLOTH_OK) rc = prepare_edge_grid(h, s.primitive_self != 0u, count, configs[0].clothMaterial.x);
     if (rc != NUMI_CLOTH_OK) return rc;
     const cudaError_t e = launch(h, count, s);
     h->epoch += count;
@@ -806,6 +916,17 @@ int numi_cloth_self_contacts(numi_cloth_t* h, unsigned long long* contacts, doub
     const uint32_t bits = static_cast<uint32_t>(st[1]);
     std::memcpy(&pen, &bits, sizeof(pen));
     *max_penetration = pen;
+    return NUMI_CLOTH_OK;
+}
+
+int numi_cloth_edge_contacts(numi_cloth_t* h, unsigned long long out[2]) {
+    if (h == nullptr || out == nullptr) return NUMI_CLOTH_EINVAL;
+    out[0] = out[1] = 0ull;
+    if (h->d.edge_stats == nullptr) return NUMI_CLOTH_OK;
+    cudaSetDevice(h->device);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess ||
+        cudaMemcpy(out, h->d.edge_stats, 2u * sizeof(unsigned long long), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return NUMI_CLOTH_ECUDA;
     return NUMI_CLOTH_OK;
 }
 
@@ -964,6 +1085,8 @@ extern "C" int numi_cloth_step_noalloc(const NumiClothConfig* base, const NumiCl
         return noalloc_reject("selfCollision needs the point self-contact hash grid, which this path does not hold");
     if (schedule->release)
         return noalloc_reject("release needs the mouth rim, which NumiClothDeviceState does not carry");
+    if (schedule->primitiveSelf)
+        return noalloc_reject("primitiveSelf needs the edge/edge pass buffers, which this path does not hold");
     if (!st->positions || !st->previous || !st->velocities || !st->rest || !st->failure ||
         (D && (!st->distanceIJ || !st->distanceMaterial || !st->distanceLambda)) ||
         (K && (!st->knotIJ || !st->knotMaterial || !st->knotLambda)) ||
@@ -1109,21 +1232,22 @@ uint32_t log2_pow2(uint32_t v) {
 // as many CTAs as fit on the device (never more than the cloths).
 int batch_shape(numi_cloth_batch* b, uint32_t chunk, uint32_t block) {
     const size_t smem = nc_resident_offset() + (chunk ? 2u * static_cast<size_t>(chunk) * sizeof(float4) : 0u);
-    cudaFuncAttributes fa{};
-    if (cudaFuncGetAttributes(&fa, numi_cloth_batch_kernel) != cudaSuccess) return NUMI_CLOTH_ECUDA;
     int optin = 0, sms = 0;
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
-    if (smem + fa.sharedSizeBytes > static_cast<size_t>(optin)) return NUMI_CLOTH_EINVAL;
-    if (static_cast<size_t>(fa.maxDynamicSharedSizeBytes) < smem &&
-        cudaFuncSetAttribute(numi_cloth_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(smem)) != cudaSuccess)
-        return NUMI_CLOTH_ECUDA;
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, numi_cloth_batch_kernel, static_cast<int>(block), smem) !=
-            cudaSuccess ||
-        per_sm < 1)
-        return NUMI_CLOTH_EINVAL;
+    int per_sm = 1 << 30;
+    for (bool edge : {false, true}) {
+        cudaFuncAttributes fa{};
+        if (cudaFuncGetAttributes(&fa, batch_fn(edge)) != cudaSuccess) return NUMI_CLOTH_ECUDA;
+        if (smem + fa.sharedSizeBytes > static_cast<size_t>(optin)) return NUMI_CLOTH_EINVAL;
+        if (raise_smem(batch_fn(edge), smem) != cudaSuccess) return NUMI_CLOTH_ECUDA;
+        int k = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, batch_fn(edge), static_cast<int>(block), smem) !=
+            cudaSuccess)
+            return NUMI_CLOTH_EINVAL;
+        per_sm = std::min(per_sm, k);
+    }
+    if (per_sm < 1) return NUMI_CLOTH_EINVAL;
     b->chunk = chunk;
     b->block = block;
     b->smem = smem;
@@ -1178,12 +1302,19 @@ int batch_prepare(numi_cloth_batch* b, const NumiClothConfig* configs, uint32_t 
         b->cfg_capacity = substeps;
         b->layout_valid = false;
     }
-    for (numi_cloth* h : b->cloths) {
+    for (size_t k = 0; k < b->cloths.size(); ++k) {
+        numi_cloth* h = b->cloths[k];
         void* before = h->d.hash_head;
+        void* edge_before = h->d.edge_head;
+        const float cell_before = h->d.edge_cell;
         h->epoch = b->epoch_host;
-        const int rc = prepare_self_grid(h, sched.selfCollision != 0u, substeps);
+        int rc = prepare_self_grid(h, sched.selfCollision != 0u, substeps);
+        if (rc == NUMI_CLOTH_OK)
+            rc = prepare_edge_grid(h, sched.primitiveSelf != 0u, substeps,
+                                   configs[k * substeps].clothMaterial.x);
         if (rc != NUMI_CLOTH_OK) return rc;
-        if (h->d.hash_head != before) b->layout_valid = false;
+        if (h->d.hash_head != before || h->d.edge_head != edge_before || h->d.edge_cell != cell_before)
+            b->layout_valid = false;
         if (h->stream != b->stream && h->stream != nullptr && cudaStreamSynchronize(h->stream) != cudaSuccess)
             return NUMI_CLOTH_ECUDA;
     }
@@ -1199,7 +1330,11 @@ cudaError_t batch_launch(numi_cloth_batch* b, const NumiClothConfig* configs, ui
     Schedule sc = s;
     sc.substeps = substeps;
     sc.epoch_ptr = b->epoch;
-    numi_cloth_batch_kernel<<<b->ctas, b->block, b->smem, b->stream>>>(b->d_cloths, count, sc, b->queue);
+    unsigned int* queue = b->queue;
+    const DeviceCloth* cloths = b->d_cloths;
+    void* args[] = {&cloths, const_cast<uint32_t*>(&count), &sc, &queue};
+    e = cudaLaunchKernel(batch_fn(sc.primitive_self != 0u), dim3(b->ctas), dim3(b->block), args, b->smem, b->stream);
+    if (e != cudaSuccess) return e;
     numi_cloth_epoch_kernel<<<1, 1, 0, b->stream>>>(b->epoch, substeps);
     return cudaGetLastError();
 }
@@ -1425,6 +1560,8 @@ int numi_cloth_batch_replay(numi_cloth_batch_t* b) {
         }
         if (h->d.hash_head != nullptr && ((b->epoch_host + b->graph_substeps) >> 26) != (b->epoch_host >> 26))
             return NUMI_CLOTH_ESTATE;   // tag wrap: capture again after a plain step
+        if (h->d.edge_head != nullptr && ((b->epoch_host + b->graph_substeps) >> 23) != (b->epoch_host >> 23))
+            return NUMI_CLOTH_ESTATE;
     }
     const cudaError_t e = cudaGraphLaunch(b->exec, b->stream);
     batch_advance(b, b->graph_substeps);
@@ -1596,7 +1733,7 @@ extern "C" int numi_cloth_rollout_grad(numi_cloth_t* h, const NumiClothConfig* c
     if (h->poisoned) return NUMI_CLOTH_ESTATE;
     const NumiClothSchedule& sc = *schedule;
     if (sc.iterations != 1u || sc.reconcilePasses != 0u || sc.finalPasses != 0u || sc.certificatePasses != 0u ||
-        sc.aerodynamics != 0u || sc.selfCollision != 0u)
+        sc.aerodynamics != 0u || sc.selfCollision != 0u || sc.primitiveSelf != 0u)
         return NUMI_CLOTH_EINVAL;
     for (uint32_t t = 0; t < n_tracked; ++t)
         if (tracked[t] >= h->d.n) return NUMI_CLOTH_EINVAL;
@@ -1802,7 +1939,7 @@ extern "C" int numi_cloth_batch_rollout_grad(numi_cloth_batch_t* b, const NumiCl
         return NUMI_CLOTH_EINVAL;
     const NumiClothSchedule& sc = *schedule;
     if (sc.iterations != 1u || sc.reconcilePasses != 0u || sc.finalPasses != 0u || sc.certificatePasses != 0u ||
-        sc.aerodynamics != 0u || sc.selfCollision != 0u)
+        sc.aerodynamics != 0u || sc.selfCollision != 0u || sc.primitiveSelf != 0u)
         return NUMI_CLOTH_EINVAL;
     cudaSetDevice(b->device);
     batch_drop_graph(b);

@@ -41,6 +41,17 @@ struct __align__(32) HashSlot {
     uint4 meta;     // particle index, 0, 0, 0
 };
 
+// One edge/edge pair record of a substep (SelfEdgeEdgeContactImpulse,
+// tools/cloth_bag.cpp:3962-3985): the two yarn segments and the sums of
+// their solves' impulse-weighted normal on the first segment, barycentric
+// weights and normal impulse.
+struct EdgeRecord {
+    uint32_t i, j;
+    float wn[3];
+    float wf[2], ws[2];
+    float ni;
+};
+
 struct DeviceCloth {
     // particles
     float4* x;
@@ -136,6 +147,51 @@ struct DeviceCloth {
     // [0] self contacts (a < b pairs resolved), [1] max self penetration
     // (float bits; non-negative so unsigned max orders them)
     unsigned long long* self_stats;
+    // edge/edge yarn self-collision.  Yarn segments: the distances that are
+    // not shear diagonals, in array order.  Buffers (allocated on first use):
+    //   pair list: every non-local segment pair (first < second) whose
+    //     present or swept spheres were within the skin when it was built,
+    //     the positions of the build, and for the build a hashed grid of
+    //     segment cover spheres (heads as the point grid's, pass tag = 23 bits
+    //     of the substep counter << 9 | pass) with a list for spheres too
+    //     large for a cell or met in a full bucket;
+    //   pass: the pass-start positions and spheres, each particle's path
+    //     length, the candidates (first, second, distance bound bits, ordered
+    //     flag), the keys (first << 32 | second) of the ordered pairs and
+    //     their sorted copy, the pass's records and the substep's records
+    //     (ascending keys)
+    const uint2* y_ij;
+    uint32_t y_count;
+    uint32_t edge_mask;
+    float edge_cell;
+    uint32_t edge_cap;            // candidates, ordered pairs, records
+    uint32_t edge_list_cap;       // pairs on the list
+    unsigned long long* edge_head;
+    HashSlot* edge_slot;          // [buckets * NC_HASH_CAP]
+    unsigned long long* edge_list_head;
+    HashSlot* edge_list;          // [y_count]
+    uint32_t* edge_flag;          // [y_count] 1: the segment's cover sphere is in the list
+    uint2* edge_pairs;            // [edge_list_cap]
+    float4* edge_xb;              // [n] positions at the build
+    float4* edge_pb;              // [n] substep-start positions at the build
+    float* edge_built_radius;     // yarn radius of the build
+    float4* edge_x0;              // [n]
+    float4* edge_sph;             // [y_count] pass spheres (centre, radius)
+    float* edge_path;             // [n]
+    uint4* edge_cand;             // [edge_cap]
+    unsigned long long* edge_order;    // [edge_cap]
+    unsigned long long* edge_sorted;   // [edge_cap]
+    EdgeRecord* edge_new;         // [edge_cap]
+    EdgeRecord* edge_rec;         // [edge_cap]
+    // [0] candidates, [1] ordered pairs, [2] violations found (only grows),
+    // [3] records of the substep, [4] records of the pass, [5] pairs on the
+    // list, [6] 1 once the list is built
+    uint32_t* edge_ctl;
+    // [0] edge/edge contacts resolved, [1] self-friction contacts
+    unsigned long long* edge_stats;
+    // [0, CTAs) deepest non-local pair of the last measure, [CTAs, 2 CTAs)
+    // largest displacement since the build
+    double* edge_red;
     // adjoint tape (one-CTA launches only): positions at the start of every
     // substep and after every barrier, [substep][tape_slots][n], and
     // velocities at the start of every substep, [substep][n]
@@ -159,6 +215,7 @@ struct Schedule {
     uint32_t release;
     float damping;
     uint32_t substeps;
+    uint32_t primitive_self;   // edge/edge yarn self-collision and self friction
     // batch launches: the substep counter of the batch in device memory
     // (advanced by a kernel after each launch, so a captured graph can be
     // replayed); null: DeviceCloth::epoch_base

@@ -6,6 +6,7 @@
 #include "cloth_kernels.cuh"
 
 namespace nc {
+namespace {   // internal linkage: the edge kernels' unit includes these too
 
 // FP64 scratch of the CTA-wide reductions (air-load chunk sums, the air
 // attenuation, the residual maxima).  They run in different phases and each
@@ -900,6 +901,14 @@ __device__ void self_solve(Ctx& ctx, uint32_t it) {
     }
 }
 
+}  // namespace
+}  // namespace nc
+
+#include "cloth_edge.cuh"
+
+namespace nc {
+namespace {   // internal linkage: the edge kernels' unit includes these too
+
 // Ground clamp (tools/cloth_bag.cpp:2655-2690).
 __device__ void phase_ground(Ctx& ctx) {
     const DeviceCloth& d = ctx.d;
@@ -1383,7 +1392,10 @@ __device__ void fruit_tail(Ctx& ctx) {
     __syncthreads();
 }
 
-// One substep.  Returns false when a barrier gave up.
+// One substep.  Returns false when a barrier gave up.  kEdge: the kernel
+// carries the edge/edge yarn self-collision phases (a separate kernel, so
+// that the kernel without them keeps its registers).
+template <bool kEdge>
 __device__ __forceinline__ bool substep(Ctx& ctx, bool last) {
     const DeviceCloth& d = ctx.d;
     const Schedule& s = ctx.s;
@@ -1405,6 +1417,8 @@ __device__ __forceinline__ bool substep(Ctx& ctx, bool last) {
         air_apply_advance(ctx, force, att);
         NC_SYNC(ctx);
     }
+    const bool prim = kEdge && s.primitive_self && d.edge_head != nullptr;
+    if (prim && !edge_sweep(ctx, true)) return false;   // swept edge/edge (tools/cloth_bag.cpp:4921)
     if (s.swept_fruit_yarn && d.f_count > 0u) {
         uint32_t first = NC_MAX_BATCHES, last = 0;
         for (uint32_t b = 0; b < d.n_dist_batches; ++b)
@@ -1469,26 +1483,34 @@ __device__ __forceinline__ bool substep(Ctx& ctx, bool last) {
             if (ok) break;
         }
     }
-    // endpoint strain + final contacts (tools/cloth_bag.cpp:5059-5142)
+    // endpoint: present edge/edge contacts, strain, final contacts
+    // (tools/cloth_bag.cpp:5059-5142)
+    if (prim && !edge_sweep(ctx, false)) return false;
     if (!strain_sweeps(ctx)) return false;
     for (uint32_t p = 0; p < s.final_passes; ++p)
         if (!contacts_pass(ctx, false)) return false;
     uint32_t cert = 0;
     if (last) {
         for (uint32_t p = 0; p < s.certificate_passes; ++p) {
+            if (prim && !edge_sweep(ctx, false)) return false;
             if (!strain_sweeps(ctx)) return false;
             for (uint32_t q = 0; q < s.final_passes; ++q)
                 if (!contacts_pass(ctx, false)) return false;
             cert = p + 1u;
+            if (prim && !edge_measure(ctx)) return false;
             residual_partials(ctx, d.red);
             NC_SYNC(ctx);
-            const bool ok = residuals_converged(ctx);
+            const bool ok = residuals_converged(ctx) && (!prim || edge_measured_clear(ctx));
             NC_SYNC(ctx);
             if (ok) break;
         }
     }
     phase_finalize(ctx);
     NC_SYNC(ctx);
+    if (prim && s.frictions) {
+        edge_friction(ctx);   // yarn/yarn self friction (tools/cloth_bag.cpp:3995-4090)
+        NC_SYNC(ctx);
+    }
     if (s.frictions && d.f_count > 0u) {
         uint32_t first = NC_MAX_BATCHES, last = 0;
         for (uint32_t b = 0; b < d.n_dist_batches; ++b)
@@ -1512,6 +1534,7 @@ __device__ __forceinline__ bool substep(Ctx& ctx, bool last) {
     return true;
 }
 
+}  // namespace
 }  // namespace nc
 
 // Dynamic shared memory of a frame: the cloth descriptor, the fruit CTA's
@@ -1525,6 +1548,7 @@ __host__ __device__ constexpr size_t nc_resident_offset() { return nc_round256(n
 // shared memory.
 // The descriptor is copied into shared memory first, so both kernels run
 // the phases on the same (shared-memory) view of it.
+template <bool kEdge>
 __device__ __forceinline__ void run_frame(const DeviceCloth& src, const Schedule& s, uint32_t rank, uint32_t ranks,
                                           unsigned char* dynamic_smem) {
     {
@@ -1575,6 +1599,7 @@ __device__ __forceinline__ void run_frame(const DeviceCloth& src, const Schedule
         ctx.c = nc::load_cfg(d.cfg + s.cfg_offset + sub);
         ctx.epoch = epoch_base + sub;
         ctx.barriers = 0;
+        ctx.edge_pass = 0;
         if (d.tape != nullptr && ranks == 1u) {
             // adjoint tape: state at the start of the substep
             float4* slot = d.tape + static_cast<size_t>(sub) * d.tape_slots * d.n;
@@ -1584,7 +1609,7 @@ __device__ __forceinline__ void run_frame(const DeviceCloth& src, const Schedule
             }
             __syncthreads();
         }
-        if (!nc::substep(ctx, sub + 1u == s.substeps)) return;
+        if (!nc::substep<kEdge>(ctx, sub + 1u == s.substeps)) return;
         if (rank == 0 && threadIdx.x == 0) d.stats[0] = ctx.barriers;
     }
     if (ctx.resident) {
@@ -1597,28 +1622,40 @@ __device__ __forceinline__ void run_frame(const DeviceCloth& src, const Schedule
     }
 }
 
-// One cloth on the whole grid (one CTA, a cooperative grid or a cluster).
-__global__ void __launch_bounds__(NC_BLOCK_MAX) numi_cloth_frame_kernel(DeviceCloth d, Schedule s) {
-    extern __shared__ __align__(16) unsigned char nc_dynamic_smem[];
-    run_frame(d, s, blockIdx.x, gridDim.x, nc_dynamic_smem);
-}
+// The frame and batch kernels with the edge/edge yarn self-collision phases
+// are defined in cloth_edge_kernels.cu, a translation unit of their own: with
+// them in the same unit the compiler inlines the shared phases differently
+// and the default kernels grow a call frame.
+__global__ void numi_cloth_frame_edge_kernel(DeviceCloth d, Schedule s);
+__global__ void numi_cloth_batch_edge_kernel(const DeviceCloth* cloths, uint32_t count, Schedule s,
+                                             unsigned int* queue);
 
 // Many independent cloths in one persistent launch: every CTA takes the
 // next cloth from a device work queue (cloths ordered by work, largest
 // first) and runs its whole frame alone, until the queue is empty.
+#define NC_BATCH_BODY(kEdge)                                                  \
+    extern __shared__ __align__(16) unsigned char nc_dynamic_smem[];          \
+    __shared__ uint32_t s_next;                                               \
+    for (;;) {                                                                \
+        if (threadIdx.x == 0) s_next = atomicAdd(queue, 1u);                  \
+        __syncthreads();                                                      \
+        const uint32_t k = s_next;                                            \
+        if (k >= count) break;                                                \
+        run_frame<kEdge>(cloths[k], s, 0u, 1u, nc_dynamic_smem);              \
+        __syncthreads();                                                      \
+    }
+
+#ifndef NC_EDGE_KERNELS
+// One cloth on the whole grid (one CTA, a cooperative grid or a cluster).
+__global__ void __launch_bounds__(NC_BLOCK_MAX) numi_cloth_frame_kernel(DeviceCloth d, Schedule s) {
+    extern __shared__ __align__(16) unsigned char nc_dynamic_smem[];
+    run_frame<false>(d, s, blockIdx.x, gridDim.x, nc_dynamic_smem);
+}
 __global__ void __launch_bounds__(NC_BLOCK_MAX) numi_cloth_batch_kernel(const DeviceCloth* cloths, uint32_t count,
                                                                          Schedule s, unsigned int* queue) {
-    extern __shared__ __align__(16) unsigned char nc_dynamic_smem[];
-    __shared__ uint32_t s_next;
-    for (;;) {
-        if (threadIdx.x == 0) s_next = atomicAdd(queue, 1u);
-        __syncthreads();
-        const uint32_t k = s_next;
-        if (k >= count) break;
-        run_frame(cloths[k], s, 0u, 1u, nc_dynamic_smem);
-        __syncthreads();
-    }
+    NC_BATCH_BODY(false)
 }
 
 // Advance the batch substep counter after a batch launch.
 __global__ void numi_cloth_epoch_kernel(uint32_t* epoch, uint32_t substeps) { *epoch += substeps; }
+#endif

@@ -35,6 +35,7 @@
 #define NC_BARRIER_SPIN_LIMIT (1u << 22)
 
 namespace nc {
+namespace {   // internal linkage: the edge kernels' unit includes these too
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
     unsigned v;
@@ -83,6 +84,7 @@ struct SubCfg {
     float4 grip_q;
     float mu_cloth_ground;
     float mu_pair, mu_fruit_ground, rolling, mu_fruit_yarn;
+    float mu_self;       // yarn/yarn self friction
     V3 air;
     float air_density;
     float4 aero;         // crossflow, skin, fruit drag, fruit rotational drag
@@ -108,6 +110,7 @@ __device__ __forceinline__ SubCfg load_cfg(const NumiClothConfig* c) {
     s.mu_fruit_ground = c->fruitMaterial.y;
     s.rolling = c->fruitMaterial.z;
     s.mu_fruit_yarn = c->fruitMaterial.w;
+    s.mu_self = c->clothMaterial.w;
     s.air = V3{c->airVelocityAndDensity.x, c->airVelocityAndDensity.y, c->airVelocityAndDensity.z};
     s.air_density = c->airVelocityAndDensity.w;
     s.aero = make_float4(c->aerodynamicCoefficients.x, c->aerodynamicCoefficients.y,
@@ -143,6 +146,7 @@ struct Ctx {
     uint32_t shift;           // log2 of the particles each CTA owns
     float4* xs;               // this CTA's positions in shared memory
     float4* vs;               // this CTA's velocities in shared memory
+    uint32_t edge_pass;       // edge/edge grid passes so far in this substep
 };
 
 __device__ __forceinline__ float4* resident_ptr(const Ctx& c, float4* local_base, uint32_t i) {
@@ -696,4 +700,5 @@ __device__ float yarn_correction(float4& pa, float4& pb, float wa_seg, float wb_
     return acc;
 }
 
+}  // namespace
 }  // namespace nc

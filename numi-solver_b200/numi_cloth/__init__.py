@@ -92,6 +92,7 @@ def load_library() -> ctypes.CDLL:
         "numi_cloth_restore": (i32, [vp, u32]),
         "numi_cloth_launch_info": (i32, [vp, ctypes.POINTER(u32)]),
         "numi_cloth_self_contacts": (i32, [vp, ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(ctypes.c_double)]),
+        "numi_cloth_edge_contacts": (i32, [vp, ctypes.POINTER(ctypes.c_ulonglong)]),
         "numi_cloth_set_damping": (i32, [vp, ctypes.c_float]),
         "numi_cloth_rollout_grad": (i32, [vp, vp, u32, ctypes.POINTER(Schedule), u32, vp, u32, vp, u32,
                                           ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), vp,
@@ -504,6 +505,13 @@ class ClothSolver:
         pen = ctypes.c_double()
         self._check(self.lib.numi_cloth_self_contacts(self._h, ctypes.byref(n), ctypes.byref(pen)))
         return int(n.value), float(pen.value)
+
+    def edge_contacts(self) -> tuple[int, int]:
+        """(edge/edge solves that moved particles, yarn/yarn self-friction
+        contacts) since create."""
+        out = (ctypes.c_ulonglong * 2)()
+        self._check(self.lib.numi_cloth_edge_contacts(self._h, out))
+        return int(out[0]), int(out[1])
 
     def launch_info(self) -> dict:
         out = (ctypes.c_uint32 * 6)()

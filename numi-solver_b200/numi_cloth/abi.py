@@ -99,7 +99,8 @@ class Schedule(ctypes.Structure):
         ("frictions", ctypes.c_uint32),
         ("release", ctypes.c_uint32),
         ("damping", ctypes.c_float),
-        ("reserved", ctypes.c_uint32 * 3),
+        ("primitiveSelf", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 2),
     ]
 
     @classmethod
@@ -119,6 +120,7 @@ class Schedule(ctypes.Structure):
             frictions=1,
             release=0,
             damping=0.0,
+            primitiveSelf=0,
         )
         defaults.update(kw)
         for k, v in defaults.items():

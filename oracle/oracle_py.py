@@ -286,7 +286,7 @@ def schedule_from_abi(sched, mode=BATCHED) -> OSchedule:
         final_passes=sched.finalPasses, certificate_passes=sched.certificatePasses, early_exit=sched.earlyExit,
         self_collision=sched.selfCollision, aerodynamics=sched.aerodynamics, swept_ground=sched.sweptGround,
         swept_fruit_yarn=sched.sweptFruitYarn, frictions=sched.frictions, release=sched.release,
-        damping=float(sched.damping),
+        damping=float(sched.damping), primitive_self=getattr(sched, "primitiveSelf", 0),
     )
 
 
