@@ -54,7 +54,9 @@ __device__ bool grid_sync(Ctx& ctx) {
         red_release_add_u64(d.bar_count, 1ull);
         unsigned ab = 0u;
         unsigned spins = 0u;
-        while (ld_acquire_u64(d.bar_count) < target) {
+        // poll relaxed; one acquire load once the count is reached (the
+        // count only grows)
+        while (ld_relaxed_u64(d.bar_count) < target) {
             ++spins;
             if ((spins & 63u) == 0u && ld_acquire(d.abort_flag) != 0u) {
                 ab = 1u;
@@ -67,7 +69,10 @@ __device__ bool grid_sync(Ctx& ctx) {
                 break;
             }
         }
-        __threadfence();
+        // no fence besides: the acquire load that sees the count orders this
+        // thread after every arrival's release, and the CTA barrier below
+        // orders the CTA's other threads after this thread
+        if (!ab) (void)ld_acquire_u64(d.bar_count);
         s_abort = ab;
         if (d.trace && ctx.rank == 0 && ctx.barriers <= NC_TRACE_SLOTS)
             d.trace[static_cast<size_t>(ctx.sub) * NC_TRACE_SLOTS + ctx.barriers - 1u] = globaltimer();
@@ -932,14 +937,27 @@ __device__ void phase_ground(Ctx& ctx) {
     }
 }
 
+template <bool kIlp>
 __device__ bool strain_sweeps(Ctx& ctx) {
+    const DeviceCloth& d = ctx.d;
     for (uint32_t sw = 0; sw < ctx.s.strain_sweeps; ++sw) {
-        for (uint32_t b = 0; b < ctx.d.n_dist_batches; ++b) {
-            const Batch bt = ctx.d.dist_batches[b];
-            if (bt.limited == 0u) continue;
-            fruit_flush(ctx);
-            for (Range r = item_range(ctx, bt.limited); r.i < r.end; r.i += r.stride) limit_strain(ctx, bt.first + r.i);
-            NC_SYNC(ctx);
+        if constexpr (kIlp) {
+            for (uint32_t b = 0; b < d.n_dist_batches; ++b) {
+                const Batch bt = d.dist_batches[b];
+                if (bt.limited == 0u) continue;
+                fruit_flush(ctx);
+                strain_colour(ctx, bt.first, bt.limited);
+                NC_SYNC(ctx);
+            }
+        } else {
+            for (uint32_t b = 0; b < d.n_dist_batches; ++b) {
+                const Batch bt = d.dist_batches[b];
+                if (bt.limited == 0u) continue;
+                fruit_flush(ctx);
+                for (Range r = item_range(ctx, bt.limited); r.i < r.end; r.i += r.stride)
+                    limit_strain(ctx, bt.first + r.i);
+                NC_SYNC(ctx);
+            }
         }
     }
     return true;
@@ -1037,6 +1055,7 @@ __device__ bool residuals_converged(Ctx& ctx) {
     return ok;
 }
 
+template <bool kIlp>
 __device__ bool contacts_pass(Ctx& ctx, bool with_strain) {
     // fruit pairs (fruit CTA) -> fruit/yarn -> [strain] -> ground
     if (ctx.fruit_cta && ctx.d.p_count > 0u) {
@@ -1045,7 +1064,7 @@ __device__ bool contacts_pass(Ctx& ctx, bool with_strain) {
     }
     if (ctx.d.p_count > 0u) NC_SYNC(ctx);
     if (!yarn_sweep(ctx)) return false;
-    if (with_strain && !strain_sweeps(ctx)) return false;
+    if (with_strain && !strain_sweeps<kIlp>(ctx)) return false;
     phase_ground(ctx);
     NC_SYNC(ctx);
     return true;
@@ -1394,8 +1413,12 @@ __device__ void fruit_tail(Ctx& ctx) {
 
 // One substep.  Returns false when a barrier gave up.  kEdge: the kernel
 // carries the edge/edge yarn self-collision phases (a separate kernel, so
-// that the kernel without them keeps its registers).
-template <bool kEdge>
+// that the kernel without them keeps its registers).  kIlp: the constraint
+// colours gather NC_ILP items per thread before computing them (the batched
+// engine, where a CTA holds a whole cloth and every thread several items of
+// a colour; with one item per thread, as on the cooperative grid, the wider
+// loops only cost registers).
+template <bool kEdge, bool kIlp>
 __device__ __forceinline__ bool substep(Ctx& ctx, bool last) {
     const DeviceCloth& d = ctx.d;
     const Schedule& s = ctx.s;
@@ -1434,11 +1457,21 @@ __device__ __forceinline__ bool substep(Ctx& ctx, bool last) {
         ctx.fruit_pending = true;
     }
     for (uint32_t it = 0; it < s.iterations; ++it) {
-        for (uint32_t b = 0; b < d.n_dist_batches; ++b) {
-            const Batch bt = d.dist_batches[b];
-            fruit_flush(ctx);
-            for (Range r = item_range(ctx, bt.count); r.i < r.end; r.i += r.stride) solve_distance(ctx, bt.first + r.i, dt2);
-            NC_SYNC(ctx);
+        if constexpr (kIlp) {
+            for (uint32_t b = 0; b < d.n_dist_batches; ++b) {
+                const Batch bt = d.dist_batches[b];
+                fruit_flush(ctx);
+                distance_colour(ctx, bt.first, bt.count, dt2);
+                NC_SYNC(ctx);
+            }
+        } else {
+            for (uint32_t b = 0; b < d.n_dist_batches; ++b) {
+                const Batch bt = d.dist_batches[b];
+                fruit_flush(ctx);
+                for (Range r = item_range(ctx, bt.count); r.i < r.end; r.i += r.stride)
+                    solve_distance(ctx, bt.first + r.i, dt2);
+                NC_SYNC(ctx);
+            }
         }
         for (uint32_t b = 0; b < d.n_knot_batches; ++b) {
             const Batch bt = d.knot_batches[b];
@@ -1446,11 +1479,19 @@ __device__ __forceinline__ bool substep(Ctx& ctx, bool last) {
             NC_SYNC(ctx);
         }
         if ((it & 1u) == 0u) {
-            for (uint32_t b = 0; b < d.n_bend_batches; ++b) {
-                const Batch bt = d.bend_batches[b];
-                for (Range r = item_range(ctx, bt.count); r.i < r.end; r.i += r.stride)
-                    solve_bend(ctx, bt.first + r.i, dt2, ctx.c.radius, ctx.c.ground);
-                NC_SYNC(ctx);
+            if constexpr (kIlp) {
+                for (uint32_t b = 0; b < d.n_bend_batches; ++b) {
+                    const Batch bt = d.bend_batches[b];
+                    bend_colour(ctx, bt.first, bt.count, dt2, ctx.c.radius, ctx.c.ground);
+                    NC_SYNC(ctx);
+                }
+            } else {
+                for (uint32_t b = 0; b < d.n_bend_batches; ++b) {
+                    const Batch bt = d.bend_batches[b];
+                    for (Range r = item_range(ctx, bt.count); r.i < r.end; r.i += r.stride)
+                        solve_bend(ctx, bt.first + r.i, dt2, ctx.c.radius, ctx.c.ground);
+                    NC_SYNC(ctx);
+                }
             }
         }
         // grips (CTA 0) and fruit pairs (fruit CTA) touch disjoint state
@@ -1473,7 +1514,7 @@ __device__ __forceinline__ bool substep(Ctx& ctx, bool last) {
     // reconciliation (tools/cloth_bag.cpp:4975-5058)
     uint32_t passes = 0;
     for (uint32_t p = 0; p < s.reconcile_passes; ++p) {
-        if (!contacts_pass(ctx, true)) return false;
+        if (!contacts_pass<kIlp>(ctx, true)) return false;
         passes = p + 1u;
         if (s.early_exit) {
             residual_partials(ctx, d.red);
@@ -1486,16 +1527,16 @@ __device__ __forceinline__ bool substep(Ctx& ctx, bool last) {
     // endpoint: present edge/edge contacts, strain, final contacts
     // (tools/cloth_bag.cpp:5059-5142)
     if (prim && !edge_sweep(ctx, false)) return false;
-    if (!strain_sweeps(ctx)) return false;
+    if (!strain_sweeps<kIlp>(ctx)) return false;
     for (uint32_t p = 0; p < s.final_passes; ++p)
-        if (!contacts_pass(ctx, false)) return false;
+        if (!contacts_pass<kIlp>(ctx, false)) return false;
     uint32_t cert = 0;
     if (last) {
         for (uint32_t p = 0; p < s.certificate_passes; ++p) {
             if (prim && !edge_sweep(ctx, false)) return false;
-            if (!strain_sweeps(ctx)) return false;
+            if (!strain_sweeps<kIlp>(ctx)) return false;
             for (uint32_t q = 0; q < s.final_passes; ++q)
-                if (!contacts_pass(ctx, false)) return false;
+                if (!contacts_pass<kIlp>(ctx, false)) return false;
             cert = p + 1u;
             if (prim && !edge_measure(ctx)) return false;
             residual_partials(ctx, d.red);
@@ -1548,7 +1589,7 @@ __host__ __device__ constexpr size_t nc_resident_offset() { return nc_round256(n
 // shared memory.
 // The descriptor is copied into shared memory first, so both kernels run
 // the phases on the same (shared-memory) view of it.
-template <bool kEdge>
+template <bool kEdge, bool kIlp>
 __device__ __forceinline__ void run_frame(const DeviceCloth& src, const Schedule& s, uint32_t rank, uint32_t ranks,
                                           unsigned char* dynamic_smem) {
     {
@@ -1609,7 +1650,7 @@ __device__ __forceinline__ void run_frame(const DeviceCloth& src, const Schedule
             }
             __syncthreads();
         }
-        if (!nc::substep<kEdge>(ctx, sub + 1u == s.substeps)) return;
+        if (!nc::substep<kEdge, kIlp>(ctx, sub + 1u == s.substeps)) return;
         if (rank == 0 && threadIdx.x == 0) d.stats[0] = ctx.barriers;
     }
     if (ctx.resident) {
@@ -1641,7 +1682,7 @@ __global__ void numi_cloth_batch_edge_kernel(const DeviceCloth* cloths, uint32_t
         __syncthreads();                                                      \
         const uint32_t k = s_next;                                            \
         if (k >= count) break;                                                \
-        run_frame<kEdge>(cloths[k], s, 0u, 1u, nc_dynamic_smem);              \
+        run_frame<kEdge, true>(cloths[k], s, 0u, 1u, nc_dynamic_smem);        \
         __syncthreads();                                                      \
     }
 
@@ -1649,7 +1690,7 @@ __global__ void numi_cloth_batch_edge_kernel(const DeviceCloth* cloths, uint32_t
 // One cloth on the whole grid (one CTA, a cooperative grid or a cluster).
 __global__ void __launch_bounds__(NC_BLOCK_MAX) numi_cloth_frame_kernel(DeviceCloth d, Schedule s) {
     extern __shared__ __align__(16) unsigned char nc_dynamic_smem[];
-    run_frame<false>(d, s, blockIdx.x, gridDim.x, nc_dynamic_smem);
+    run_frame<false, false>(d, s, blockIdx.x, gridDim.x, nc_dynamic_smem);
 }
 __global__ void __launch_bounds__(NC_BLOCK_MAX) numi_cloth_batch_kernel(const DeviceCloth* cloths, uint32_t count,
                                                                          Schedule s, unsigned int* queue) {

@@ -60,6 +60,11 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long
     asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
 __device__ __forceinline__ void red_release_add_u64(unsigned long long* p, unsigned long long v) {
     asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
@@ -289,28 +294,89 @@ __device__ void solve_grips(const Ctx& ctx) {
 }
 
 // ---------------------------------------------------------- constraints ---
-// XPBD distance (tools/cloth_bag.cpp:1649-1673).
+// XPBD distance (tools/cloth_bag.cpp:1649-1673) on loaded values: updates
+// the two particles and the multiplier; false when it changes nothing.
+__device__ __forceinline__ bool distance_core(float4& a, float4& b, const float4& m, float& lam, float dt2) {
+    const V3 diff = xyz(b) - xyz(a);
+    const float L = len3(diff);
+    if (L < 1.0e-12f) return false;
+    const float alpha = m.y / dt2;
+    const float den = (a.w + b.w) + alpha;
+    if (den <= 0.0f) return false;
+    const float value = L - m.x;
+    const float dl = (-value - alpha * lam) / den;
+    const V3 corr = diff * (dl / L);
+    const V3 na = xyz(a) - corr * a.w;
+    const V3 nb = xyz(b) + corr * b.w;
+    a = with_xyz(a, na);
+    b = with_xyz(b, nb);
+    lam = lam + dl;
+    return true;
+}
+
 __device__ __forceinline__ void solve_distance(const Ctx& ctx, uint32_t k, float dt2) {
     const DeviceCloth& d = ctx.d;
     const uint2 ij = __ldg(d.d_ij + k);
     const float4 m = __ldg(d.d_mat + k);
     float4 a = px(ctx, ij.x);
     float4 b = px(ctx, ij.y);
-    const V3 diff = xyz(b) - xyz(a);
-    const float L = len3(diff);
-    if (L < 1.0e-12f) return;
-    const float alpha = m.y / dt2;
-    const float den = (a.w + b.w) + alpha;
-    if (den <= 0.0f) return;
-    const float lam = ldf(d.d_lambda + k);
-    const float value = L - m.x;
-    const float dl = (-value - alpha * lam) / den;
-    const V3 corr = diff * (dl / L);
-    const V3 na = xyz(a) - corr * a.w;
-    const V3 nb = xyz(b) + corr * b.w;
-    px_set(ctx, ij.x, with_xyz(a, na));
-    px_set(ctx, ij.y, with_xyz(b, nb));
-    d.d_lambda[k] = lam + dl;
+    float lam = ldf(d.d_lambda + k);
+    if (!distance_core(a, b, m, lam, dt2)) return;
+    px_set(ctx, ij.x, a);
+    px_set(ctx, ij.y, b);
+    d.d_lambda[k] = lam;
+}
+
+// Items a thread gathers before it computes any of them.  The items of one
+// colour share no particle, so a thread may load all of its next NC_ILP
+// items first and overlap their latencies; every item's arithmetic is the
+// same as item by item.
+#define NC_ILP 4
+
+// Item j of a gathered group: its index within the batch (a dead slot
+// repeats the group's first item, loads it and stores nothing).
+struct IlpSlots {
+    uint32_t i[NC_ILP];
+    bool live[NC_ILP];
+};
+__device__ __forceinline__ IlpSlots ilp_slots(const Range& r) {
+    IlpSlots s;
+#pragma unroll
+    for (int j = 0; j < NC_ILP; ++j) {
+        const uint32_t i = r.i + static_cast<uint32_t>(j) * r.stride;
+        s.live[j] = i < r.end;
+        s.i[j] = s.live[j] ? i : r.i;
+    }
+    return s;
+}
+
+// One colour of distance constraints.
+__device__ __forceinline__ void distance_colour(const Ctx& ctx, uint32_t first, uint32_t count, float dt2) {
+    const DeviceCloth& d = ctx.d;
+    for (Range r = item_range(ctx, count); r.i < r.end; r.i += NC_ILP * r.stride) {
+        const IlpSlots sl = ilp_slots(r);
+        uint2 ij[NC_ILP];
+        float4 m[NC_ILP], a[NC_ILP], b[NC_ILP];
+        float lam[NC_ILP];
+#pragma unroll
+        for (int j = 0; j < NC_ILP; ++j) {
+            ij[j] = __ldg(d.d_ij + first + sl.i[j]);
+            m[j] = __ldg(d.d_mat + first + sl.i[j]);
+            lam[j] = ldf(d.d_lambda + first + sl.i[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < NC_ILP; ++j) {
+            a[j] = px(ctx, ij[j].x);
+            b[j] = px(ctx, ij[j].y);
+        }
+#pragma unroll
+        for (int j = 0; j < NC_ILP; ++j) {
+            if (!sl.live[j] || !distance_core(a[j], b[j], m[j], lam[j], dt2)) continue;
+            px_set(ctx, ij[j].x, a[j]);
+            px_set(ctx, ij[j].y, b[j]);
+            d.d_lambda[first + sl.i[j]] = lam[j];
+        }
+    }
 }
 
 // Crossing-angle knot (tools/cloth_bag.cpp:1675-1725).
@@ -351,16 +417,14 @@ __device__ __forceinline__ void solve_knot(const Ctx& ctx, uint32_t k, float dt2
     px_set(ctx, q.w, with_xyz(p3, xyz(p3) + gf * (p3.w * dl)));
 }
 
-// Skip-one chord bend with the ground active set (tools/cloth_bag.cpp:1782-1863).
-__device__ __forceinline__ void solve_bend(const Ctx& ctx, uint32_t k, float dt2, float radius, bool ground) {
-    const DeviceCloth& d = ctx.d;
-    const uint4 q = __ldg(d.b_ij + k);
-    const float2 m = __ldg(d.b_mat + k);
-    const uint32_t idx[2] = {q.x, q.z};
-    float4 p[2] = {px(ctx, q.x), px(ctx, q.z)};
+// Skip-one chord bend with the ground active set (tools/cloth_bag.cpp:1782-1863)
+// on loaded values: updates the two chord ends and the multiplier; false
+// when it changes nothing.
+__device__ __forceinline__ bool bend_core(float4 p[2], const float2& m, float& lam, float dt2, float radius,
+                                          bool ground) {
     const V3 diff = xyz(p[1]) - xyz(p[0]);
     const float chord = len3(diff);
-    if (chord < 1.0e-12f) return;
+    if (chord < 1.0e-12f) return false;
     const float value = chord - m.x;
     const V3 dir = vdiv(diff, chord);
     const V3 g[2] = {dir * -1.0f, dir};
@@ -368,8 +432,7 @@ __device__ __forceinline__ void solve_bend(const Ctx& ctx, uint32_t k, float dt2
     float free_den = alpha;
     free_den = free_den + p[0].w * lsq(g[0]);
     free_den = free_den + p[1].w * lsq(g[1]);
-    if (free_den < 1.0e-16f) return;
-    const float lam = ldf(d.b_lambda + k);
+    if (free_den < 1.0e-16f) return false;
     const float numerator = -value - alpha * lam;
     const float free_dl = numerator / free_den;
     bool active[2];
@@ -378,7 +441,7 @@ __device__ __forceinline__ void solve_bend(const Ctx& ctx, uint32_t k, float dt2
         active[s] = ground && p[s].z <= radius + 1.0e-9f && g[s].z * free_dl < 0.0f;
         den = den + p[s].w * (lsq(g[s]) - (active[s] ? g[s].z * g[s].z : 0.0f));
     }
-    if (den < 1.0e-16f) return;
+    if (den < 1.0e-16f) return false;
     const float dl = numerator / den;
     float fraction = 1.0f;
     if (ground) {
@@ -390,18 +453,77 @@ __device__ __forceinline__ void solve_bend(const Ctx& ctx, uint32_t k, float dt2
         }
     }
     const float applied = dl * fraction;
-    d.b_lambda[k] = lam + applied;
+    lam = lam + applied;
     for (int s = 0; s < 2; ++s) {
         V3 corr = g[s] * (p[s].w * applied);
         if (active[s]) corr.z = 0.0f;
         V3 np = xyz(p[s]) + corr;
         if (ground && np.z < radius) np.z = radius;
-        px_set(ctx, idx[s], with_xyz(p[s], np));
+        p[s] = with_xyz(p[s], np);
+    }
+    return true;
+}
+
+__device__ __forceinline__ void solve_bend(const Ctx& ctx, uint32_t k, float dt2, float radius, bool ground) {
+    const DeviceCloth& d = ctx.d;
+    const uint4 q = __ldg(d.b_ij + k);
+    const float2 m = __ldg(d.b_mat + k);
+    float4 p[2] = {px(ctx, q.x), px(ctx, q.z)};
+    float lam = ldf(d.b_lambda + k);
+    if (!bend_core(p, m, lam, dt2, radius, ground)) return;
+    d.b_lambda[k] = lam;
+    px_set(ctx, q.x, p[0]);
+    px_set(ctx, q.z, p[1]);
+}
+
+// One colour of bends.
+__device__ __forceinline__ void bend_colour(const Ctx& ctx, uint32_t first, uint32_t count, float dt2, float radius,
+                                            bool ground) {
+    const DeviceCloth& d = ctx.d;
+    for (Range r = item_range(ctx, count); r.i < r.end; r.i += NC_ILP * r.stride) {
+        const IlpSlots sl = ilp_slots(r);
+        uint4 q[NC_ILP];
+        float2 m[NC_ILP];
+        float lam[NC_ILP];
+        float4 p[NC_ILP][2];
+#pragma unroll
+        for (int j = 0; j < NC_ILP; ++j) {
+            q[j] = __ldg(d.b_ij + first + sl.i[j]);
+            m[j] = __ldg(d.b_mat + first + sl.i[j]);
+            lam[j] = ldf(d.b_lambda + first + sl.i[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < NC_ILP; ++j) {
+            p[j][0] = px(ctx, q[j].x);
+            p[j][1] = px(ctx, q[j].z);
+        }
+#pragma unroll
+        for (int j = 0; j < NC_ILP; ++j) {
+            if (!sl.live[j] || !bend_core(p[j], m[j], lam[j], dt2, radius, ground)) continue;
+            d.b_lambda[first + sl.i[j]] = lam[j];
+            px_set(ctx, q[j].x, p[j][0]);
+            px_set(ctx, q[j].z, p[j][1]);
+        }
     }
 }
 
-// Unilateral strain limit (tools/cloth_bag.cpp:1732-1763); returns nothing,
-// the correction is not published.
+// Unilateral strain limit (tools/cloth_bag.cpp:1732-1763) on loaded values;
+// false when it changes nothing.  The correction is not published.
+__device__ __forceinline__ bool strain_core(float4& a, float4& b, const float4& m) {
+    if (!(m.w > 0.0f)) return false;
+    const V3 diff = xyz(b) - xyz(a);
+    const float L = len3(diff);
+    const float maxL = m.x * (1.0f + m.w);
+    if (L <= maxL || L < 1.0e-12f) return false;
+    const float den = a.w + b.w;
+    if (den <= 0.0f) return false;
+    const float cm = L - maxL;
+    const V3 dir = vdiv(diff, L);
+    a = with_xyz(a, xyz(a) + dir * (a.w * cm / den));
+    b = with_xyz(b, xyz(b) - dir * (b.w * cm / den));
+    return true;
+}
+
 __device__ __forceinline__ void limit_strain(const Ctx& ctx, uint32_t k) {
     const DeviceCloth& d = ctx.d;
     const float4 m = __ldg(d.d_mat + k);
@@ -409,16 +531,35 @@ __device__ __forceinline__ void limit_strain(const Ctx& ctx, uint32_t k) {
     const uint2 ij = __ldg(d.d_ij + k);
     float4 a = px(ctx, ij.x);
     float4 b = px(ctx, ij.y);
-    const V3 diff = xyz(b) - xyz(a);
-    const float L = len3(diff);
-    const float maxL = m.x * (1.0f + m.w);
-    if (L <= maxL || L < 1.0e-12f) return;
-    const float den = a.w + b.w;
-    if (den <= 0.0f) return;
-    const float cm = L - maxL;
-    const V3 dir = vdiv(diff, L);
-    px_set(ctx, ij.x, with_xyz(a, xyz(a) + dir * (a.w * cm / den)));
-    px_set(ctx, ij.y, with_xyz(b, xyz(b) - dir * (b.w * cm / den)));
+    if (!strain_core(a, b, m)) return;
+    px_set(ctx, ij.x, a);
+    px_set(ctx, ij.y, b);
+}
+
+// One colour's strain-limited prefix.
+__device__ __forceinline__ void strain_colour(const Ctx& ctx, uint32_t first, uint32_t count) {
+    const DeviceCloth& d = ctx.d;
+    for (Range r = item_range(ctx, count); r.i < r.end; r.i += NC_ILP * r.stride) {
+        const IlpSlots sl = ilp_slots(r);
+        uint2 ij[NC_ILP];
+        float4 m[NC_ILP], a[NC_ILP], b[NC_ILP];
+#pragma unroll
+        for (int j = 0; j < NC_ILP; ++j) {
+            ij[j] = __ldg(d.d_ij + first + sl.i[j]);
+            m[j] = __ldg(d.d_mat + first + sl.i[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < NC_ILP; ++j) {
+            a[j] = px(ctx, ij[j].x);
+            b[j] = px(ctx, ij[j].y);
+        }
+#pragma unroll
+        for (int j = 0; j < NC_ILP; ++j) {
+            if (!sl.live[j] || !strain_core(a[j], b[j], m[j])) continue;
+            px_set(ctx, ij[j].x, a[j]);
+            px_set(ctx, ij[j].y, b[j]);
+        }
+    }
 }
 
 // ------------------------------------------------------------- fruits -----
