@@ -235,4 +235,5 @@ struct FruitShared {
     float fr[NC_MAX_FRUITS];               // radius
     float4 v[NC_MAX_FRUITS];               // velocity xyz, inverse mass
     float4 o[NC_MAX_FRUITS];               // spin xyz, radius
+    unsigned long long loaded;             // pair colours with an impulse this substep
 };

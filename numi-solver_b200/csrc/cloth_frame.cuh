@@ -90,15 +90,19 @@ __device__ void fruit_flush(Ctx& ctx) {
     ctx.fruit_pending = false;
     if (!ctx.fruit_cta) return;
     const DeviceCloth& d = ctx.d;
+    // the barrier before this phase completed every add: plain loads, and
+    // stores of zero for the next sweep
     unsigned long long* acc = reinterpret_cast<unsigned long long*>(d.fruit_partial);
     for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
         NumiClothFruit& fr = d.fruits[f];
-        const unsigned long long ax = atomicExch(acc + 3u * f + 0u, 0ull);
-        const unsigned long long ay = atomicExch(acc + 3u * f + 1u, 0ull);
-        const unsigned long long az = atomicExch(acc + 3u * f + 2u, 0ull);
-        fr.positionAndInverseMass.x = fr.positionAndInverseMass.x + from_fixed(ax);
-        fr.positionAndInverseMass.y = fr.positionAndInverseMass.y + from_fixed(ay);
-        fr.positionAndInverseMass.z = fr.positionAndInverseMass.z + from_fixed(az);
+        const unsigned long long ax = __ldcg(acc + 3u * f + 0u);
+        const unsigned long long ay = __ldcg(acc + 3u * f + 1u);
+        const unsigned long long az = __ldcg(acc + 3u * f + 2u);
+        const numi_float4 p = fr.positionAndInverseMass;
+        acc[3u * f + 0u] = 0ull;
+        acc[3u * f + 1u] = 0ull;
+        acc[3u * f + 2u] = 0ull;
+        fr.positionAndInverseMass = nf4<numi_float4>(p.x + from_fixed(ax), p.y + from_fixed(ay), p.z + from_fixed(az), p.w);
     }
     __syncthreads();
 }
@@ -110,10 +114,14 @@ __device__ void fruit_flush_velocity(Ctx& ctx) {
     unsigned long long* acc = reinterpret_cast<unsigned long long*>(d.fruit_partial) + 3u * NC_MAX_FRUITS;
     for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
         NumiClothFruit& fr = d.fruits[f];
-        float* v = &fr.velocityAndGroundImpulse.x;
-        float* w = &fr.angularVelocity.x;
-        for (int k = 0; k < 3; ++k) v[k] = v[k] + from_fixed(atomicExch(acc + 6u * f + k, 0ull));
-        for (int k = 0; k < 3; ++k) w[k] = w[k] + from_fixed(atomicExch(acc + 6u * f + 3u + k, 0ull));
+        unsigned long long s[6];
+        for (int k = 0; k < 6; ++k) s[k] = __ldcg(acc + 6u * f + k);
+        for (int k = 0; k < 6; ++k) acc[6u * f + k] = 0ull;
+        const numi_float4 v = fr.velocityAndGroundImpulse;
+        const numi_float4 w = fr.angularVelocity;
+        fr.velocityAndGroundImpulse =
+            nf4<numi_float4>(v.x + from_fixed(s[0]), v.y + from_fixed(s[1]), v.z + from_fixed(s[2]), v.w);
+        fr.angularVelocity = nf4<numi_float4>(w.x + from_fixed(s[3]), w.y + from_fixed(s[4]), w.z + from_fixed(s[5]), w.w);
     }
     __syncthreads();
 }
@@ -179,6 +187,7 @@ __device__ void phase_begin(Ctx& ctx) {
             store_fruit(d.fruits[f], s);
         }
         for (uint32_t k = threadIdx.x; k < d.p_count; k += blockDim.x) ctx.fs->contact[k] = make_float4(0, 0, 0, 0);
+        if (threadIdx.x == 0) ctx.fs->loaded = 0ull;
     }
 }
 
@@ -1353,8 +1362,9 @@ __device__ void release_masks(Ctx& ctx) {
 // Fruit frictions and orientation in the fruit CTA: pair friction on
 // fruit velocities staged in shared memory (one warp walks the colours),
 // then ground friction, rolling resistance and orientation per fruit; the
-// substep's pair impulses are published to global memory for readback.
-__device__ void fruit_tail(Ctx& ctx) {
+// pair impulses of a launch's last substep are published to global memory
+// for readback.
+__device__ void fruit_tail(Ctx& ctx, bool last) {
     if (!ctx.fruit_cta) return;
     const DeviceCloth& d = ctx.d;
     const SubCfg& c = ctx.c;
@@ -1366,22 +1376,10 @@ __device__ void fruit_tail(Ctx& ctx) {
         fs.o[f] = make_float4(fr.angularVelocity.x, fr.angularVelocity.y, fr.angularVelocity.z,
                               fr.previousAndRadius.w);
     }
-    // Colours holding at least one loaded pair (one warp per colour); the
-    // friction walk visits only those, in colour order.
-    __shared__ unsigned long long s_loaded;
-    if (threadIdx.x == 0) s_loaded = 0ull;
+    // Colours holding at least one loaded pair (marked by the pair sweeps);
+    // the friction walk visits only those, in colour order.
     __syncthreads();
-    {
-        const uint32_t lane = threadIdx.x & 31u;
-        for (uint32_t b = threadIdx.x >> 5; b < d.n_pair_batches; b += blockDim.x >> 5) {
-            const Batch bt = d.pair_batches[b];
-            bool loaded = false;
-            for (uint32_t k = bt.first + lane; k < bt.first + bt.count; k += 32u) loaded = loaded || fs.contact[k].w > 0.0f;
-            if (__any_sync(0xffffffffu, loaded) && lane == 0u) atomicOr(&s_loaded, 1ull << b);
-        }
-    }
-    __syncthreads();
-    const unsigned long long loaded_colours = s_loaded;
+    const unsigned long long loaded_colours = fs.loaded;
     if (ctx.s.frictions && loaded_colours != 0ull && threadIdx.x < 32u) {
         for (unsigned long long m = loaded_colours; m != 0ull; m &= m - 1ull) {
             const uint32_t b = static_cast<uint32_t>(__ffsll(static_cast<long long>(m)) - 1);
@@ -1404,9 +1402,11 @@ __device__ void fruit_tail(Ctx& ctx) {
         integrate_orientation(s, c.dt);
         store_fruit(d.fruits[f], s);
     }
-    for (uint32_t k = threadIdx.x; k < d.p_count; k += blockDim.x) {
-        const float4 cw = fs.contact[k];
-        d.pairs[k].contact = nf4<numi_float4>(cw.x, cw.y, cw.z, cw.w);
+    if (last) {   // the host reads the impulses of a launch's last substep
+        for (uint32_t k = threadIdx.x; k < d.p_count; k += blockDim.x) {
+            const float4 cw = fs.contact[k];
+            d.pairs[k].contact = nf4<numi_float4>(cw.x, cw.y, cw.z, cw.w);
+        }
     }
     __syncthreads();
 }
@@ -1566,7 +1566,7 @@ __device__ __forceinline__ bool substep(Ctx& ctx, bool last) {
         }
         fruit_flush_velocity(ctx);
     }
-    fruit_tail(ctx);
+    fruit_tail(ctx, last);
     NC_SYNC(ctx);
     if (ctx.rank == 0 && threadIdx.x == 0) {
         d.stats[1] = max(d.stats[1], passes);

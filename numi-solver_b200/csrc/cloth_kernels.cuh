@@ -652,6 +652,7 @@ __device__ void fruit_pair_sweep(const DeviceCloth& d, FruitShared& fs, float dt
     if (threadIdx.x < 32u) {
         for (uint32_t b = 0; b < d.n_pair_batches; ++b) {
             const Batch bt = d.pair_batches[b];
+            bool loaded = false;
             for (uint32_t k = bt.first + threadIdx.x; k < bt.first + bt.count; k += 32u) {
                 const uint32_t ia = fs.ab[k] & 0xffu;
                 const uint32_t ib = fs.ab[k] >> 8;
@@ -671,7 +672,9 @@ __device__ void fruit_pair_sweep(const DeviceCloth& d, FruitShared& fs, float dt
                 const float4 c = fs.contact[k];
                 const V3 wn = xyz(c) + normal * imp;
                 fs.contact[k] = make_float4(wn.x, wn.y, wn.z, c.w + imp);
+                loaded = loaded || c.w + imp > 0.0f;
             }
+            if (__any_sync(0xffffffffu, loaded) && threadIdx.x == 0) fs.loaded |= 1ull << b;
             __syncwarp();
         }
     }
