@@ -32,7 +32,6 @@ enum AdjointPhase : uint32_t {
     ADJ_GROUND = 5,
     ADJ_STRAIN = 6,
     ADJ_FINAL = 7,
-    ADJ_YFRIC = 8,
     ADJ_TAIL = 9,
 };
 
@@ -197,7 +196,6 @@ __device__ __forceinline__ void adjoint_segment(const AdjointArgs& A) {
             case ADJ_TAIL:
                 break;
             case ADJ_YARN:
-            case ADJ_YFRIC:
                 // fruit/yarn contact moved the cloth: not differentiated
                 for (uint32_t i = threadIdx.x; i < n; i += blockDim.x)
                     if (pre[i].x != post[i].x || pre[i].y != post[i].y || pre[i].z != post[i].z) ++rough;

@@ -494,6 +494,8 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
     d.yarn_slot_a = h->buf.alloc<float4>(static_cast<size_t>(F ? D : 1) * NC_YARN_SLOTS);
     d.yarn_slot_b = h->buf.alloc<float4>(static_cast<size_t>(F ? D : 1) * NC_YARN_SLOTS);
     d.yarn_live = h->buf.alloc<uint32_t>(F ? D : 1);
+    d.yarn_list = h->buf.alloc<uint32_t>(F ? D : 1);
+    d.yarn_list_n = h->buf.alloc<uint32_t>(1);
     d.force = h->buf.alloc<float4>(n);
     d.fruit_partial = h->buf.alloc<float4>(NC_MAX_FRUITS * 9u / 2u + 1u);
     d.failure = h->buf.alloc<unsigned int>(1);
@@ -619,7 +621,7 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
     d.red = h->buf.alloc<double>(std::max<size_t>(3u * 4096u, 2u * chunks + 8u));
 
     bool ok = d.x && d.xp && d.v && rest && d_ij && d_mat && d.d_lambda && k_ij && k_mat && d.k_lambda && b_ij &&
-              b_mat && d.b_lambda && d.grips && d.fruits && d.pairs && cuff && d.yarn_slot_a && d.yarn_slot_b && d.yarn_live &&
+              b_mat && d.b_lambda && d.grips && d.fruits && d.pairs && cuff && d.yarn_slot_a && d.yarn_slot_b && d.yarn_live && d.yarn_list && d.yarn_list_n &&
               d.force && d.fruit_partial && d.failure && d.bar_count && d.abort_flag && d.stats && d.red && rim &&
               d.release;
     if (!ok) {
@@ -1026,6 +1028,8 @@ struct NoAllocScratch {
     float4 slot_a[NUMI_CLOTH_NOALLOC_MAX_DISTANCES * NC_YARN_SLOTS];
     float4 slot_b[NUMI_CLOTH_NOALLOC_MAX_DISTANCES * NC_YARN_SLOTS];
     uint32_t live[NUMI_CLOTH_NOALLOC_MAX_DISTANCES];
+    uint32_t list[NUMI_CLOTH_NOALLOC_MAX_DISTANCES];
+    uint32_t list_n[4];
     float4 force[NUMI_CLOTH_NOALLOC_MAX_PARTICLES];
     unsigned long long fruit_sums[9u * NC_MAX_FRUITS + 8u];
     double red[256];
@@ -1131,6 +1135,8 @@ extern "C" int numi_cloth_step_noalloc(const NumiClothConfig* base, const NumiCl
     d.yarn_slot_a = scratch->slot_a;
     d.yarn_slot_b = scratch->slot_b;
     d.yarn_live = scratch->live;
+    d.yarn_list = scratch->list;
+    d.yarn_list_n = scratch->list_n;
     d.force = scratch->force;
     d.fruit_partial = reinterpret_cast<float4*>(scratch->fruit_sums);
     d.red = scratch->red;
@@ -1597,9 +1603,7 @@ std::vector<uint2> adjoint_phases(const DeviceCloth& d, const Schedule& s) {
         for (uint32_t b = 0; b < d.n_dist_batches; ++b)
             if (d.dist_batches[b].limited != 0u) ph.push_back(make_uint2(ADJ_STRAIN, b));
     ph.push_back(make_uint2(ADJ_FINAL, 0u));
-    if (s.frictions && d.f_count > 0u)
-        for (uint32_t b = 0; b < d.n_dist_batches; ++b)
-            if (d.dist_batches[b].yarn != 0u) ph.push_back(make_uint2(ADJ_YFRIC, b));
+    // fruit/yarn friction and the fruit tail share the substep's last phase
     ph.push_back(make_uint2(ADJ_TAIL, 0u));
     return ph;
 }

@@ -93,6 +93,10 @@ struct DeviceCloth {
     float4* yarn_slot_b;
     // substep epoch of the latest fruit/yarn contact record of each segment
     uint32_t* yarn_live;
+    // segments recorded this substep, each once, in no particular order (the
+    // friction sweep picks each colour's own), and their count
+    uint32_t* yarn_list;
+    uint32_t* yarn_list_n;
     // per-particle yarn air force of the current substep
     float4* force;
     // 2^-40 fixed-point fruit sums (int64 two's complement):

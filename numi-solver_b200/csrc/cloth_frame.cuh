@@ -107,25 +107,6 @@ __device__ void fruit_flush(Ctx& ctx) {
     __syncthreads();
 }
 
-// Fruit/yarn velocity sums of the friction sweep (v then omega).
-__device__ void fruit_flush_velocity(Ctx& ctx) {
-    if (!ctx.fruit_cta) return;
-    const DeviceCloth& d = ctx.d;
-    unsigned long long* acc = reinterpret_cast<unsigned long long*>(d.fruit_partial) + 3u * NC_MAX_FRUITS;
-    for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
-        NumiClothFruit& fr = d.fruits[f];
-        unsigned long long s[6];
-        for (int k = 0; k < 6; ++k) s[k] = __ldcg(acc + 6u * f + k);
-        for (int k = 0; k < 6; ++k) acc[6u * f + k] = 0ull;
-        const numi_float4 v = fr.velocityAndGroundImpulse;
-        const numi_float4 w = fr.angularVelocity;
-        fr.velocityAndGroundImpulse =
-            nf4<numi_float4>(v.x + from_fixed(s[0]), v.y + from_fixed(s[1]), v.z + from_fixed(s[2]), v.w);
-        fr.angularVelocity = nf4<numi_float4>(w.x + from_fixed(s[3]), w.y + from_fixed(s[4]), w.z + from_fixed(s[5]), w.w);
-    }
-    __syncthreads();
-}
-
 // ------------------------------------------------------------ phases -----
 
 // Grip attach + begin + advance (+ swept ground), aero off.
@@ -168,6 +149,7 @@ __device__ void phase_begin(Ctx& ctx) {
         px_set(ctx, i, with_xyz(p, pos));
         pv_set(ctx, i, make_float4(vel.x, vel.y, vel.z, vel.z));
     }
+    if (ctx.tid == 0u) *d.yarn_list_n = 0u;
     for (uint32_t k = ctx.tid; k < d.d_count; k += ctx.nthreads) d.d_lambda[k] = 0.0f;
     for (uint32_t k = ctx.tid; k < d.k_count; k += ctx.nthreads) d.k_lambda[k] = 0.0f;
     for (uint32_t k = ctx.tid; k < d.b_count; k += ctx.nthreads) d.b_lambda[k] = 0.0f;
@@ -374,10 +356,11 @@ __device__ __forceinline__ bool fruit_near_segment(const float4& fs, const float
 // slot 0 without a search and retires the older ones.
 struct SegRecords {
     uint32_t seg;
-    bool loaded, live, recorded;
+    bool loaded, live, was_live, recorded;
     uint32_t rtag[NC_YARN_SLOTS];
 
-    __device__ explicit SegRecords(uint32_t s) : seg(s), loaded(false), live(false), recorded(false) {
+    __device__ explicit SegRecords(uint32_t s)
+        : seg(s), loaded(false), live(false), was_live(false), recorded(false) {
 #pragma unroll
         for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q) rtag[q] = 0u;
     }
@@ -388,6 +371,7 @@ struct SegRecords {
         if (!loaded) {
             loaded = true;
             live = __ldcg(d.yarn_live + seg) == ctx.epoch;
+            was_live = live;
             if (live) {
 #pragma unroll
                 for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q)
@@ -444,7 +428,10 @@ struct SegRecords {
     }
 
     __device__ void finish(const Ctx& ctx) const {
-        if (recorded) ctx.d.yarn_live[seg] = ctx.epoch;
+        if (!recorded) return;
+        ctx.d.yarn_live[seg] = ctx.epoch;
+        // first record of the substep: the segment joins the friction list
+        if (!was_live) ctx.d.yarn_list[atomicAdd(ctx.d.yarn_list_n, 1u)] = seg;
     }
 };
 
@@ -1126,119 +1113,145 @@ __device__ void phase_finalize(Ctx& ctx) {
     }
 }
 
-// Fruit/yarn Coulomb friction (tools/cloth_bag.cpp:3178-3270), one yarn
-// colour; fruit velocities are those at the start of the friction sweep.
-__device__ void yarn_friction_batch(Ctx& ctx, const Batch& bt, bool first, bool last) {
+// Fruit/yarn Coulomb friction (tools/cloth_bag.cpp:3178-3270) of one
+// recorded segment, with fruit velocities frozen over the sweep; the fruit
+// velocity changes go into the CTA's fixed-point sums.
+__device__ __forceinline__ void yarn_friction_segment(const Ctx& ctx, uint32_t seg, const float4* s_vw,
+                                                      const float4* s_or, unsigned long long* s_sum) {
     const DeviceCloth& d = ctx.d;
     const SubCfg& c = ctx.c;
-    unsigned long long* acc = reinterpret_cast<unsigned long long*>(d.fruit_partial) + 3u * NC_MAX_FRUITS;
+    const uint2 ij = __ldg(d.d_ij + seg);
+    uint32_t st[NC_YARN_SLOTS];
+#pragma unroll
+    for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q)
+        st[q] = __float_as_uint(__ldcg(&d.yarn_slot_b[seg * NC_YARN_SLOTS + q].z));
+    const float4 pa = px(ctx, ij.x);
+    const float4 pb = px(ctx, ij.y);
+    float4 va = pv(ctx, ij.x);
+    float4 vb = pv(ctx, ij.y);
+    // Live records of this segment, visited in ascending fruit order.
+    const uint32_t live = ctx.epoch & 0x3ffffffu;
+    uint32_t fruit_of[NC_YARN_SLOTS];
+    uint32_t nlive = 0;
+#pragma unroll
+    for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q) {
+        fruit_of[q] = ((st[q] >> 6) == live) ? (st[q] & 63u) : 0xffffffffu;
+        nlive += fruit_of[q] != 0xffffffffu ? 1u : 0u;
+    }
+    for (uint32_t visit = 0; visit < nlive; ++visit) {
+        uint32_t slot = 0;
+        uint32_t f = 0xffffffffu;
+#pragma unroll
+        for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q)
+            if (fruit_of[q] < f) {
+                f = fruit_of[q];
+                slot = q;
+            }
+#pragma unroll
+        for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q)
+            if (q == slot) fruit_of[q] = 0xffffffffu;
+        const float4 sa = __ldcg(&d.yarn_slot_a[seg * NC_YARN_SLOTS + slot]);
+        const float4 sb = __ldcg(&d.yarn_slot_b[seg * NC_YARN_SLOTS + slot]);
+        const float ni = sa.w;
+        const V3 wn{sa.x, sa.y, sa.z};
+        if (ni <= 0.0f || lsq(wn) < 1.0e-20f) continue;
+        FruitState fr;
+        {
+            const float4 vw = s_vw[f];
+            const float4 orr = s_or[f];
+            fr.v = V3{vw.x, vw.y, vw.z};
+            fr.w = vw.w;
+            fr.omega = V3{orr.x, orr.y, orr.z};
+            fr.radius = orr.w;
+        }
+        const V3 normal = normalized3(wn);
+        float wt[2] = {sb.x / ni, sb.y / ni};
+        const float sum = wt[0] + wt[1];
+        if (sum <= 1.0e-12f) continue;
+        wt[0] = wt[0] / sum;
+        wt[1] = wt[1] / sum;
+        const V3 yv = (V3{0.0f, 0.0f, 0.0f} + xyz(va) * wt[0]) + xyz(vb) * wt[1];
+        const V3 off = normal * -fr.radius;
+        const V3 bcv = fr.v + cross3(fr.omega, off);
+        const V3 rel = bcv - yv;
+        const V3 tv = rel - normal * dot3(rel, normal);
+        const float slip = len3(tv);
+        if (slip < 1.0e-10f) continue;
+        const V3 t = vdiv(tv, slip);
+        const float inv_i = inverse_inertia(fr.w, fr.radius);
+        float den = fr.w + inv_i * lsq(cross3(off, t));
+        V3 resp[2];
+        const float4* pp[2] = {&pa, &pb};
+        for (int s = 0; s < 2; ++s) {
+            resp[s] = t * pp[s]->w;
+            if (c.ground && pp[s]->z <= c.radius + 1.0e-6f && resp[s].z < 0.0f) resp[s].z = 0.0f;
+            den = den + dot3(t, resp[s]) * wt[s] * wt[s];
+        }
+        if (den <= 0.0f) continue;
+        const float limit = c.mu_fruit_yarn * ni;
+        const float ti = fminf(slip / den, limit);
+        if (ti <= 0.0f) continue;
+        const V3 imp = t * -ti;
+        const V3 dv = imp * fr.w;
+        const V3 dw = cross3(off, imp) * inv_i;
+        cta_sums_add(s_sum + 6u * f + 0u, dv.x);
+        cta_sums_add(s_sum + 6u * f + 1u, dv.y);
+        cta_sums_add(s_sum + 6u * f + 2u, dv.z);
+        cta_sums_add(s_sum + 6u * f + 3u, dw.x);
+        cta_sums_add(s_sum + 6u * f + 4u, dw.y);
+        cta_sums_add(s_sum + 6u * f + 5u, dw.z);
+        const V3 na = xyz(va) + resp[0] * (ti * wt[0]);
+        const V3 nb = xyz(vb) + resp[1] * (ti * wt[1]);
+        va = with_xyz(va, na);
+        vb = with_xyz(vb, nb);
+    }
+    pv_set(ctx, ij.x, va);
+    pv_set(ctx, ij.y, vb);
+}
+
+// The fruit/yarn friction sweep on the fruit CTA: the yarn colours in order,
+// each over its segments on the substep's recorded-segment list (a few per
+// fruit), CTA barriers between the colours; segments of a colour share no
+// particle.  The fruit velocity changes are exact integer sums, so adding
+// them in this one CTA gives the same totals as summing per CTA; the CTA
+// applies them itself.
+__device__ void yarn_friction_sweep(Ctx& ctx) {
+    if (!ctx.fruit_cta) return;
+    const DeviceCloth& d = ctx.d;
     __shared__ unsigned long long s_sum[6u * NC_MAX_FRUITS];
-    // fruit velocities are frozen over the sweep: stage them once per CTA
     __shared__ float4 s_vw[NC_MAX_FRUITS];   // velocity xyz, inverse mass
     __shared__ float4 s_or[NC_MAX_FRUITS];   // spin xyz, radius
-    if (first) {
-        cta_sums_clear(s_sum, 6u * d.f_count);
-        for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
-            const NumiClothFruit& fr = d.fruits[f];
-            const float4 vg = __ldcg(reinterpret_cast<const float4*>(&fr.velocityAndGroundImpulse));
-            const float4 om = __ldcg(reinterpret_cast<const float4*>(&fr.angularVelocity));
-            s_vw[f] = make_float4(vg.x, vg.y, vg.z, __ldcg(&fr.positionAndInverseMass.w));
-            s_or[f] = make_float4(om.x, om.y, om.z, __ldcg(&fr.previousAndRadius.w));
+    cta_sums_clear(s_sum, 6u * d.f_count);
+    for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
+        const NumiClothFruit& fr = d.fruits[f];
+        const float4 vg = __ldcg(reinterpret_cast<const float4*>(&fr.velocityAndGroundImpulse));
+        const float4 om = __ldcg(reinterpret_cast<const float4*>(&fr.angularVelocity));
+        s_vw[f] = make_float4(vg.x, vg.y, vg.z, __ldcg(&fr.positionAndInverseMass.w));
+        s_or[f] = make_float4(om.x, om.y, om.z, __ldcg(&fr.previousAndRadius.w));
+    }
+    __syncthreads();
+    const uint32_t listed = min(__ldcg(d.yarn_list_n), d.d_count);
+    for (uint32_t b = 0; b < d.n_dist_batches; ++b) {
+        const Batch bt = d.dist_batches[b];
+        if (bt.yarn == 0u) continue;
+        for (uint32_t e = threadIdx.x; e < listed; e += blockDim.x) {
+            const uint32_t seg = __ldcg(d.yarn_list + e);
+            if (seg < bt.first || seg >= bt.first + bt.yarn) continue;
+            yarn_friction_segment(ctx, seg, s_vw, s_or, s_sum);
         }
         __syncthreads();
     }
-    for (Range r = item_range(ctx, bt.yarn); r.i < r.end; r.i += r.stride) {
-        const uint32_t seg = bt.first + r.i;
-        if (__ldcg(d.yarn_live + seg) != ctx.epoch) continue;
-        const uint2 ij = __ldg(d.d_ij + seg);
-        uint32_t st[NC_YARN_SLOTS];
-#pragma unroll
-        for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q)
-            st[q] = __float_as_uint(__ldcg(&d.yarn_slot_b[seg * NC_YARN_SLOTS + q].z));
-        const float4 pa = px(ctx, ij.x);
-        const float4 pb = px(ctx, ij.y);
-        float4 va = pv(ctx, ij.x);
-        float4 vb = pv(ctx, ij.y);
-        // Live records of this segment, visited in ascending fruit order.
-        const uint32_t live = ctx.epoch & 0x3ffffffu;
-        uint32_t fruit_of[NC_YARN_SLOTS];
-        uint32_t nlive = 0;
-#pragma unroll
-        for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q) {
-            fruit_of[q] = ((st[q] >> 6) == live) ? (st[q] & 63u) : 0xffffffffu;
-            nlive += fruit_of[q] != 0xffffffffu ? 1u : 0u;
-        }
-        for (uint32_t visit = 0; visit < nlive; ++visit) {
-            uint32_t slot = 0;
-            uint32_t f = 0xffffffffu;
-#pragma unroll
-            for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q)
-                if (fruit_of[q] < f) {
-                    f = fruit_of[q];
-                    slot = q;
-                }
-#pragma unroll
-            for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q)
-                if (q == slot) fruit_of[q] = 0xffffffffu;
-            const float4 sa = __ldcg(&d.yarn_slot_a[seg * NC_YARN_SLOTS + slot]);
-            const float4 sb = __ldcg(&d.yarn_slot_b[seg * NC_YARN_SLOTS + slot]);
-            const float ni = sa.w;
-            const V3 wn{sa.x, sa.y, sa.z};
-            if (ni <= 0.0f || lsq(wn) < 1.0e-20f) continue;
-            FruitState fr;
-            {
-                const float4 vw = s_vw[f];
-                const float4 orr = s_or[f];
-                fr.v = V3{vw.x, vw.y, vw.z};
-                fr.w = vw.w;
-                fr.omega = V3{orr.x, orr.y, orr.z};
-                fr.radius = orr.w;
-            }
-            const V3 normal = normalized3(wn);
-            float wt[2] = {sb.x / ni, sb.y / ni};
-            const float sum = wt[0] + wt[1];
-            if (sum <= 1.0e-12f) continue;
-            wt[0] = wt[0] / sum;
-            wt[1] = wt[1] / sum;
-            const V3 yv = (V3{0.0f, 0.0f, 0.0f} + xyz(va) * wt[0]) + xyz(vb) * wt[1];
-            const V3 off = normal * -fr.radius;
-            const V3 bcv = fr.v + cross3(fr.omega, off);
-            const V3 rel = bcv - yv;
-            const V3 tv = rel - normal * dot3(rel, normal);
-            const float slip = len3(tv);
-            if (slip < 1.0e-10f) continue;
-            const V3 t = vdiv(tv, slip);
-            const float inv_i = inverse_inertia(fr.w, fr.radius);
-            float den = fr.w + inv_i * lsq(cross3(off, t));
-            V3 resp[2];
-            const float4* pp[2] = {&pa, &pb};
-            for (int s = 0; s < 2; ++s) {
-                resp[s] = t * pp[s]->w;
-                if (c.ground && pp[s]->z <= c.radius + 1.0e-6f && resp[s].z < 0.0f) resp[s].z = 0.0f;
-                den = den + dot3(t, resp[s]) * wt[s] * wt[s];
-            }
-            if (den <= 0.0f) continue;
-            const float limit = c.mu_fruit_yarn * ni;
-            const float ti = fminf(slip / den, limit);
-            if (ti <= 0.0f) continue;
-            const V3 imp = t * -ti;
-            const V3 dv = imp * fr.w;
-            const V3 dw = cross3(off, imp) * inv_i;
-            cta_sums_add(s_sum + 6u * f + 0u, dv.x);
-            cta_sums_add(s_sum + 6u * f + 1u, dv.y);
-            cta_sums_add(s_sum + 6u * f + 2u, dv.z);
-            cta_sums_add(s_sum + 6u * f + 3u, dw.x);
-            cta_sums_add(s_sum + 6u * f + 4u, dw.y);
-            cta_sums_add(s_sum + 6u * f + 5u, dw.z);
-            const V3 na = xyz(va) + resp[0] * (ti * wt[0]);
-            const V3 nb = xyz(vb) + resp[1] * (ti * wt[1]);
-            va = with_xyz(va, na);
-            vb = with_xyz(vb, nb);
-        }
-        pv_set(ctx, ij.x, va);
-        pv_set(ctx, ij.y, vb);
+    for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
+        NumiClothFruit& fr = d.fruits[f];
+        unsigned long long sm[6];
+        for (int k = 0; k < 6; ++k) sm[k] = s_sum[6u * f + k];
+        const numi_float4 v = fr.velocityAndGroundImpulse;
+        const numi_float4 w = fr.angularVelocity;
+        fr.velocityAndGroundImpulse =
+            nf4<numi_float4>(v.x + from_fixed(sm[0]), v.y + from_fixed(sm[1]), v.z + from_fixed(sm[2]), v.w);
+        fr.angularVelocity = nf4<numi_float4>(w.x + from_fixed(sm[3]), w.y + from_fixed(sm[4]), w.z + from_fixed(sm[5]), w.w);
     }
-    if (last) cta_sums_flush(s_sum, acc, 6u * d.f_count);
+    __syncthreads();
 }
 
 // ---------------------------------------------------------- release ----
@@ -1552,20 +1565,7 @@ __device__ __forceinline__ bool substep(Ctx& ctx, bool last) {
         edge_friction(ctx);   // yarn/yarn self friction (tools/cloth_bag.cpp:3995-4090)
         NC_SYNC(ctx);
     }
-    if (s.frictions && d.f_count > 0u) {
-        uint32_t first = NC_MAX_BATCHES, last = 0;
-        for (uint32_t b = 0; b < d.n_dist_batches; ++b)
-            if (d.dist_batches[b].yarn != 0u) {
-                first = min(first, b);
-                last = b;
-            }
-        for (uint32_t b = first; b <= last && b < d.n_dist_batches; ++b) {
-            if (d.dist_batches[b].yarn == 0u) continue;
-            yarn_friction_batch(ctx, d.dist_batches[b], b == first, b == last);
-            NC_SYNC(ctx);
-        }
-        fruit_flush_velocity(ctx);
-    }
+    if (s.frictions && d.f_count > 0u) yarn_friction_sweep(ctx);   // fruit CTA, no grid barrier
     fruit_tail(ctx, last);
     NC_SYNC(ctx);
     if (ctx.rank == 0 && threadIdx.x == 0) {
