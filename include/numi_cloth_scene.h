@@ -104,6 +104,29 @@ int numi_cloth_scene_view(const numi_cloth_scene_t* scene, NumiClothScene* out);
  * bend colours, pair colours, yarn segments, bottom centre. */
 int numi_cloth_scene_counts(const numi_cloth_scene_t* scene, uint32_t out[15]);
 
+/* Render triangles (3 indices each; the bag's are the reference's
+ * renderTriangles, tools/cloth_bag.cpp:812-839; the square's two per quad).
+ * Copies at most capacity triangles into out (may be NULL); returns the
+ * triangle count. */
+uint32_t numi_cloth_scene_triangles(const numi_cloth_scene_t* scene, uint32_t* out, uint32_t capacity);
+
+/* The bag's grip handle: the authored top-ring particle 0 in FP64, lifted
+ * for the spin scenario (tools/cloth_bag.cpp:475-527, :1476-1480). */
+int numi_cloth_bag_handle_base(int scenario, double out[3]);
+
+/* Scripted grip target of the spin and pickup scenarios at time t (s)
+ * (spinGripTarget, pickupGripTarget, tools/cloth_bag.cpp:1476-1502). */
+int numi_cloth_bag_grip_target(int scenario, double time, double out[3]);
+
+/* Per-substep Configs of the grounded, spin and pickup scenarios for
+ * substeps first..first+count-1 (recorded runs use
+ * numi_cloth_trajectory_configs): the grip target of the end of each
+ * substep with identity orientation (updateGrip, tools/cloth_bag.cpp:1621-1627);
+ * grounded copies base.  targets (count x 3, may be NULL) receives the FP64
+ * grip targets. */
+int numi_cloth_bag_scenario_configs(int scenario, const NumiClothConfig* base, uint64_t first_substep,
+                                    uint32_t count, double timestep, NumiClothConfig* out, double* targets);
+
 /* Rest positions in FP64 (the values the FP32 records were rounded from). */
 int numi_cloth_scene_rest_fp64(const numi_cloth_scene_t* scene, double* out_xyz);
 

@@ -199,6 +199,7 @@ struct numi_cloth_scene {
     uint32_t dist_colours = 0, knot_colours = 0, bend_colours = 0, pair_colours = 0;
     uint32_t yarn_segments = 0;
     uint32_t bottom_center = 0;
+    std::vector<uint32_t> triangles;   // render triangles, 3 indices each
 };
 
 namespace {
@@ -604,6 +605,24 @@ numi_cloth_scene_t* numi_cloth_scene_bag(const NumiClothMaterial* material, int 
         for (uint32_t ring = 0; ring < kAround; ++ring) s->rim.push_back(node(kLevels - 1u, ring));
         add_local_topology(s, pos.size());
         s->bottom_center = bottom_index((kBottomGrid - 1u) / 2u, (kBottomGrid - 1u) / 2u);
+        // render triangles (tools/cloth_bag.cpp:812-839): the wall quads, then
+        // the bottom grid with alternating diagonals
+        for (uint32_t level = 0; level + 1u < kLevels; ++level)
+            for (uint32_t ring = 0; ring < kAround; ++ring) {
+                const uint32_t next = (ring + 1u) % kAround;
+                const uint32_t a = node(level, ring), b = node(level, next), c = node(level + 1u, ring),
+                               d = node(level + 1u, next);
+                s->triangles.insert(s->triangles.end(), {a, b, c, b, d, c});
+            }
+        for (uint32_t row = 0; row + 1u < kBottomGrid; ++row)
+            for (uint32_t col = 0; col + 1u < kBottomGrid; ++col) {
+                const uint32_t a = bottom_index(row, col), b = bottom_index(row, col + 1u),
+                               c = bottom_index(row + 1u, col), d = bottom_index(row + 1u, col + 1u);
+                if ((row + col) % 2u == 0u)
+                    s->triangles.insert(s->triangles.end(), {a, c, b, b, c, d});
+                else
+                    s->triangles.insert(s->triangles.end(), {a, d, b, a, c, d});
+            }
         base_config(s, m, timestep, scenario != NUMI_CLOTH_SCENARIO_SPIN);
         NumiClothConfig& c = s->config;
         c.gripTargetAndActive = f4(base.x, base.y, base.z, s->grips.empty() ? 0.0 : 1.0);
@@ -700,6 +719,11 @@ numi_cloth_scene_t* numi_cloth_scene_square(const NumiClothSquareSpec* spec, con
         }
         add_pairs(s);
         s->grid_width = side;
+        for (uint32_t i = 0; i + 1u < side; ++i)
+            for (uint32_t j = 0; j + 1u < side; ++j) {
+                const uint32_t a = id(i, j), b = id(i, j + 1u), c = id(i + 1u, j), d = id(i + 1u, j + 1u);
+                s->triangles.insert(s->triangles.end(), {a, b, c, b, d, c});
+            }
         base_config(s, m, spec->timestep, spec->groundEnabled != 0u);
         NumiClothConfig& c = s->config;
         c.gripTargetAndActive = f4(base.x, base.y, base.z, s->grips.empty() ? 0.0 : 1.0);
@@ -752,6 +776,76 @@ int numi_cloth_scene_counts(const numi_cloth_scene_t* s, uint32_t out[15]) {
                             s->yarn_segments,
                             s->bottom_center};
     std::memcpy(out, v, sizeof(v));
+    return NUMI_CLOTH_OK;
+}
+
+uint32_t numi_cloth_scene_triangles(const numi_cloth_scene_t* s, uint32_t* out, uint32_t capacity) {
+    if (!s) return 0;
+    const uint32_t count = static_cast<uint32_t>(s->triangles.size() / 3u);
+    if (out) std::memcpy(out, s->triangles.data(), 3u * std::min(count, capacity) * sizeof(uint32_t));
+    return count;
+}
+
+int numi_cloth_bag_handle_base(int scenario, double out[3]) {
+    if (!out || scenario < NUMI_CLOTH_SCENARIO_GROUNDED || scenario > NUMI_CLOTH_SCENARIO_RECORDED)
+        return NUMI_CLOTH_EINVAL;
+    D3 p = wall_position(kLevels - 1u, 0u);
+    if (scenario == NUMI_CLOTH_SCENARIO_SPIN) p.z += kAirborneLift;
+    out[0] = p.x;
+    out[1] = p.y;
+    out[2] = p.z;
+    return NUMI_CLOTH_OK;
+}
+
+// The scripted grip motions of the spin and pickup scenarios
+// (spinGripTarget, pickupGripTarget, tools/cloth_bag.cpp:1476-1502).
+int numi_cloth_bag_grip_target(int scenario, double time, double out[3]) {
+    if (!out) return NUMI_CLOTH_EINVAL;
+    D3 base = wall_position(kLevels - 1u, 0u);
+    if (scenario == NUMI_CLOTH_SCENARIO_SPIN) {
+        base.z += kAirborneLift;
+        const double radius = 0.28, angular_speed = 4.8, ramp = 0.18;
+        const double angle = angular_speed * (time - ramp * (1.0 - std::exp(-time / ramp)));
+        out[0] = base.x + radius * (std::cos(angle) - 1.0);
+        out[1] = base.y + radius * std::sin(angle);
+        out[2] = base.z + 0.035 * std::sin(0.5 * angle);
+        return NUMI_CLOTH_OK;
+    }
+    if (scenario == NUMI_CLOTH_SCENARIO_PICKUP) {
+        const double lift = smooth(time / 0.80);
+        const double snap = smooth((time - 1.00) / 0.23);
+        const double recovery = smooth((time - 1.45) / 0.50);
+        out[0] = base.x + -0.10 * snap;
+        out[1] = base.y + 0.04 * std::sin(kPi * snap);
+        out[2] = base.z + (1.25 * lift - 0.85 * snap + 0.75 * recovery);
+        return NUMI_CLOTH_OK;
+    }
+    return NUMI_CLOTH_EINVAL;
+}
+
+int numi_cloth_bag_scenario_configs(int scenario, const NumiClothConfig* base, uint64_t first_substep,
+                                    uint32_t count, double timestep, NumiClothConfig* out, double* targets) {
+    if (!base || !out || !(timestep > 0.0)) return NUMI_CLOTH_EINVAL;
+    if (scenario != NUMI_CLOTH_SCENARIO_GROUNDED && scenario != NUMI_CLOTH_SCENARIO_SPIN &&
+        scenario != NUMI_CLOTH_SCENARIO_PICKUP)
+        return NUMI_CLOTH_EINVAL;
+    for (uint32_t k = 0; k < count; ++k) {
+        out[k] = *base;
+        double g[3] = {0.0, 0.0, 0.0};
+        if (scenario != NUMI_CLOTH_SCENARIO_GROUNDED) {
+            // the grip moves to its pose at the end of the substep
+            // (tools/cloth_bag.cpp:4776-4786)
+            const double time = static_cast<double>(first_substep + k + 1u) * timestep;
+            numi_cloth_bag_grip_target(scenario, time, g);
+            out[k].gripTargetAndActive = f4(g[0], g[1], g[2], 1.0);
+            out[k].gripOrientation = f4(0.0, 0.0, 0.0, 1.0);
+        }
+        if (targets) {
+            targets[3u * k + 0u] = g[0];
+            targets[3u * k + 1u] = g[1];
+            targets[3u * k + 2u] = g[2];
+        }
+    }
     return NUMI_CLOTH_OK;
 }
 

@@ -136,6 +136,15 @@ def load_library() -> ctypes.CDLL:
             i32,
             [vp, vp, ctypes.POINTER(ctypes.c_double), ctypes.c_uint64, u32, ctypes.c_double, vp],
         ),
+        "numi_cloth_scene_triangles": (u32, [vp, vp, u32]),
+        "numi_cloth_bag_handle_base": (i32, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
+        "numi_cloth_bag_grip_target": (i32, [ctypes.c_int, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]),
+        "numi_cloth_bag_scenario_configs": (
+            i32, [ctypes.c_int, vp, ctypes.c_uint64, u32, ctypes.c_double, vp, vp]),
+        "numi_cloth_state_hash": (ctypes.c_uint64, [ctypes.POINTER(abi.HashState)]),
+        "numi_cloth_write_obj": (i32, [ctypes.c_char_p, ctypes.POINTER(abi.ObjState)]),
+        "numi_cloth_replay": (i32, [ctypes.POINTER(abi.ReplayOptions), ctypes.POINTER(abi.ReplayResult),
+                                    ctypes.c_char_p, ctypes.c_size_t]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -234,12 +243,15 @@ def _scene_from_handle(h) -> SceneArrays:
 
         rest64 = np.zeros(3 * n, np.float64)
         lib.numi_cloth_scene_rest_fp64(h, rest64.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        ntri = lib.numi_cloth_scene_triangles(h, None, 0)
+        triangles = np.zeros((ntri, 3), np.uint32)
+        lib.numi_cloth_scene_triangles(h, triangles.ctypes.data, ntri)
         local_off = grab(view.localOffsets, np.dtype("<u4"), n + 1) if view.localOffsets else None
         local_idx = (
             grab(view.localIndices, np.dtype("<u4"), int(local_off[-1])) if local_off is not None else None
         )
         cfg = grab(view.config, CONFIG, 1)
-        return SceneArrays(
+        arrays = SceneArrays(
             config=cfg,
             particles=grab(view.particles, PARTICLE, n),
             rest=grab(view.restPositions, np.dtype("<f4"), 4 * n).reshape(n, 4),
@@ -264,6 +276,8 @@ def _scene_from_handle(h) -> SceneArrays:
                 "yarn_segments": int(counts[13]),
             },
         )
+        arrays.extra["triangles"] = triangles
+        return arrays
     finally:
         lib.numi_cloth_scene_destroy(h)
 
@@ -288,6 +302,67 @@ def bag_scene(
     s.extra["material"] = m
     del c
     return s
+
+
+def bag_scenario_configs(scene: SceneArrays, first_substep: int, count: int, dt: float):
+    """Configs of the grounded, spin and pickup scenarios for substeps
+    first..first+count-1, and their FP64 grip targets [count, 3]."""
+    out = np.zeros(count, CONFIG)
+    targets = np.zeros((count, 3), np.float64)
+    rc = load_library().numi_cloth_bag_scenario_configs(
+        SCENARIOS[scene.extra["scenario"]], _ptr(scene.config), first_substep, count, dt, _ptr(out), _ptr(targets))
+    if rc != 0:
+        raise ClothError("scenario has no scripted grip (recorded runs use GripTrajectory.configs)")
+    return out, targets
+
+
+def state_hash(particle_state: np.ndarray, fruit_state: np.ndarray, grip_target, grip_active: bool,
+               generation: int = 1, grip_particles=None, grip_offsets=None, patch_selections: int = 0) -> int:
+    """The reference's hashResult over an FP64 state: particle_state [n, 6]
+    (position, velocity), fruit_state [f, 13] (position, velocity, angular
+    velocity, orientation w x y z)."""
+    ps = np.ascontiguousarray(particle_state, np.float64)
+    fs = np.ascontiguousarray(fruit_state, np.float64)
+    hs = abi.HashState()
+    hs.particles, hs.fruits = len(ps), len(fs)
+    hs.particleState = ps.ctypes.data
+    hs.fruitState = fs.ctypes.data if len(fs) else None
+    hs.gripTarget = (ctypes.c_double * 3)(*grip_target)
+    hs.gripActive = 1 if grip_active else 0
+    hs.generation = generation
+    hs.patchSelections = patch_selections
+    gp = np.ascontiguousarray(grip_particles if grip_particles is not None else np.zeros(0), np.uint32)
+    go = np.ascontiguousarray(grip_offsets if grip_offsets is not None else np.zeros((0, 3)), np.float64)
+    hs.grips = len(gp)
+    hs.gripParticle = gp.ctypes.data if len(gp) else None
+    hs.gripOffset = go.ctypes.data if len(go) else None
+    return int(load_library().numi_cloth_state_hash(ctypes.byref(hs)))
+
+
+def replay(scenario: str, steps: int, substeps: int = 48, frame_dt: float = 1.0 / 60.0, schedule: Schedule | None = None,
+           replays: int = 1, material: str | None = None, trajectory: str | None = None,
+           dump_frames: str | None = None, dump_every: int = 0, dump_obj: str | None = None) -> dict:
+    """numi_cloth_replay: a produce-bag scenario frame after frame on the GPU."""
+    o = abi.ReplayOptions()
+    o.scenario = SCENARIOS[scenario]
+    o.steps, o.substeps, o.replays, o.frameTimestep = steps, substeps, replays, frame_dt
+    o.material = material.encode() if material else None
+    o.gripTrajectory = trajectory.encode() if trajectory else None
+    o.dumpObj = dump_obj.encode() if dump_obj else None
+    o.dumpFrames = dump_frames.encode() if dump_frames else None
+    o.dumpEvery = dump_every
+    o.schedule = schedule if schedule is not None else Schedule.make()
+    r = abi.ReplayResult()
+    err = ctypes.create_string_buffer(512)
+    rc = load_library().numi_cloth_replay(ctypes.byref(o), ctypes.byref(r), err, 512)
+    if rc != 0:
+        raise ClothError(err.value.decode() or f"replay failed ({rc})")
+    return {"hash": int(r.hash), "replay_hash": int(r.replayHash), "deterministic": bool(r.deterministic),
+            "failure": int(r.failure), "particles": r.particles, "fruits": r.fruits,
+            "render_triangles": r.renderTriangles, "generation": r.generation,
+            "residuals": list(r.residuals), "self_contacts": int(r.selfContacts),
+            "edge_contacts": (int(r.edgeContacts[0]), int(r.edgeContacts[1])),
+            "masks": (int(r.masks[0]), int(r.masks[1])), "seconds": r.seconds}
 
 
 def _bag_handle_base(scenario: str):

@@ -239,3 +239,56 @@ class DeviceState(ctypes.Structure):
 NOALLOC_MAX_PARTICLES = 4096
 NOALLOC_MAX_DISTANCES = 8192
 NOALLOC_MAX_SUBSTEPS = 256
+
+
+class HashState(ctypes.Structure):
+    """NumiClothHashState (include/numi_cloth_replay.h)."""
+
+    _fields_ = [
+        ("particles", ctypes.c_uint32), ("fruits", ctypes.c_uint32), ("grips", ctypes.c_uint32),
+        ("gripActive", ctypes.c_uint32),
+        ("particleState", ctypes.c_void_p), ("fruitState", ctypes.c_void_p),
+        ("gripTarget", ctypes.c_double * 3),
+        ("generation", ctypes.c_uint32), ("patchSelections", ctypes.c_uint32),
+        ("gripParticle", ctypes.c_void_p), ("gripOffset", ctypes.c_void_p),
+    ]
+
+
+class ObjState(ctypes.Structure):
+    """NumiClothObjState (include/numi_cloth_replay.h)."""
+
+    _fields_ = [
+        ("particles", ctypes.c_uint32), ("triangles", ctypes.c_uint32),
+        ("positions", ctypes.c_void_p), ("triangleIndices", ctypes.c_void_p),
+        ("scenario", ctypes.c_int), ("gripActive", ctypes.c_uint32),
+        ("gripTarget", ctypes.c_double * 3), ("gripOrientationWxyz", ctypes.c_double * 4),
+        ("patchCenter", ctypes.c_uint32), ("fruits", ctypes.c_uint32),
+        ("fruitState", ctypes.c_void_p), ("fruitAppearance", ctypes.c_void_p),
+    ]
+
+
+class ReplayOptions(ctypes.Structure):
+    """NumiClothReplayOptions (include/numi_cloth_replay.h)."""
+
+    _fields_ = [
+        ("scenario", ctypes.c_int), ("steps", ctypes.c_uint32), ("substeps", ctypes.c_uint32),
+        ("replays", ctypes.c_uint32), ("frameTimestep", ctypes.c_double),
+        ("material", ctypes.c_char_p), ("gripTrajectory", ctypes.c_char_p),
+        ("dumpObj", ctypes.c_char_p), ("dumpFrames", ctypes.c_char_p),
+        ("dumpEvery", ctypes.c_uint32), ("pad", ctypes.c_uint32),
+        ("schedule", Schedule),
+    ]
+
+
+class ReplayResult(ctypes.Structure):
+    """NumiClothReplayResult (include/numi_cloth_replay.h)."""
+
+    _fields_ = [
+        ("hash", ctypes.c_uint64), ("replayHash", ctypes.c_uint64),
+        ("deterministic", ctypes.c_uint32), ("failure", ctypes.c_uint32),
+        ("particles", ctypes.c_uint32), ("fruits", ctypes.c_uint32),
+        ("renderTriangles", ctypes.c_uint32), ("generation", ctypes.c_uint32),
+        ("residuals", ctypes.c_double * 4),
+        ("selfContacts", ctypes.c_ulonglong), ("edgeContacts", ctypes.c_ulonglong * 2),
+        ("masks", ctypes.c_uint32 * 2), ("seconds", ctypes.c_double),
+    ]

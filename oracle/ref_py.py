@@ -39,6 +39,8 @@ def lib():
         L.ref_apply_material.restype = ctypes.c_int
         L.ref_apply_material.argtypes = [ctypes.c_char_p]
         L.ref_reset_material.argtypes = []
+        L.ref_render_triangles.restype = u32
+        L.ref_render_triangles.argtypes = [ctypes.c_int, vp]
         _LIB = L
     return _LIB
 
@@ -67,6 +69,13 @@ def scene(scenario: str) -> op.OracleScene:
     lib().ref_scene_export(SCENARIOS[scenario], _p(P), _p(D), _p(K), _p(B), _p(G), _p(F), _p(PR), _p(lo), _p(li),
                            _p(cuff), _p(rim), ctypes.byref(prm))
     return op.OracleScene(P, D, K, B, G, F, PR, prm, cuff, rim, lo, li)
+
+
+def render_triangles(scenario) -> np.ndarray:
+    n = lib().ref_render_triangles(SCENARIOS[scenario], None)
+    out = np.zeros((n, 3), np.uint32)
+    lib().ref_render_triangles(SCENARIOS[scenario], _p(out))
+    return out
 
 
 def simulate_hash(scenario, steps, frame_dt, substeps, iterations, trajectory=None) -> int:

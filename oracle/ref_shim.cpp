@@ -110,6 +110,19 @@ int ref_scene_counts(int scenario, uint32_t out[8]) {
     return 0;
 }
 
+// The reference's render triangles (3 indices each) into out when not
+// NULL; returns their count.
+uint32_t ref_render_triangles(int scenario, uint32_t* out) {
+    const ClothModel c = makeCloth(scenario_of(scenario));
+    if (out)
+        for (size_t t = 0; t < c.renderTriangles.size(); ++t) {
+            out[3 * t] = c.renderTriangles[t].first;
+            out[3 * t + 1] = c.renderTriangles[t].second;
+            out[3 * t + 2] = c.renderTriangles[t].third;
+        }
+    return static_cast<uint32_t>(c.renderTriangles.size());
+}
+
 // The reference scene in construction order (makeCloth / makeBalls).
 int ref_scene_export(int scenario, OracleParticle* P, OracleDistance* D, OracleKnot* K, OracleBend* B,
                      OracleGrip* G, OracleFruit* F, OraclePair* PR, uint32_t* local_off, uint32_t* local_idx,

@@ -8,11 +8,13 @@ Run in a checkout next to the reference sources (default /root/reference):
 It builds oracle/_ref (oracle/ref.mk), then writes into tests/golden/:
   reference_fixtures/   the reference's own calibration fixtures (grip
                         trajectories v1-v3, material artifacts), copied as data
-  ref_<case>.npz        reference scene (construction order, FP64), the grip
+  ref_<case>.npz        reference scene (construction order, FP64), its render
+                        triangles, the grip
                         pose of every substep, and the reference's final
                         particle/fruit state after the reference substep loop,
                         without (final_*) and with (full_*) the primitive
                         (edge/edge) self-collision family
+  ref_spin.obj          the reference executable's OBJ of the spin case's final state
   ref_probes.txt        stdout of the reference executable's analytic probes
   ref_hashes.json       reference simulate() state hashes (full substep) and
                         the shim loop's hash of the same runs
@@ -41,6 +43,7 @@ CASES = {
     "patch_regrab_v3": ("recorded", "reference_fixtures/synthetic-patch-regrab.csv", 1, 1.0 / 120.0, 24, 2),
     "regrab_v2": ("recorded", "reference_fixtures/synthetic-regrab.csv", 1, 1.0 / 120.0, 24, 2),
     "rotation_v1": ("recorded", "reference_fixtures/synthetic-rotation.csv", 1, 1.0 / 120.0, 12, 2),
+    "pickup": ("pickup", None, 1, 1.0 / 120.0, 6, 2),
 }
 
 PROBES = ["--strain-probe", "--cloth-ground-friction-probe", "--rolling-probe", "--aerodynamics-probe",
@@ -86,8 +89,14 @@ def main():
             masks=np.array([run["released_mask"], run["candidate_mask"]], np.uint64),
             full_particles=full["particles"], full_fruits=full["fruits"],
             full_masks=np.array([full["released_mask"], full["candidate_mask"]], np.uint64),
-            meta=np.array([steps, subs, its], np.uint32))
+            meta=np.array([steps, subs, its], np.uint32), triangles=rp.render_triangles(scenario))
         print(name, hashes[name])
+    # one OBJ frame written by the reference executable (dumpOBJ) after the
+    # spin case's run
+    a = CASES["spin"]
+    subprocess.run([rp.BINARY, "--scenario", "spin", "--steps", str(a[2]), "--timestep", repr(a[3]), "--substeps",
+                    str(a[4]), "--iterations", str(a[5]), "--dump-obj", os.path.join(HERE, "ref_spin.obj")],
+                   check=True, capture_output=True)
     with open(os.path.join(HERE, "ref_hashes.json"), "w") as f:
         json.dump(hashes, f, indent=1, sort_keys=True)
     lines = []

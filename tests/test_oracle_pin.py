@@ -17,7 +17,7 @@ import pytest
 import oracle_py as op
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-CASES = ["recorded_lift", "grounded", "spin", "patch_regrab_v3", "regrab_v2", "rotation_v1"]
+CASES = ["recorded_lift", "grounded", "spin", "patch_regrab_v3", "regrab_v2", "rotation_v1", "pickup"]
 
 
 def load_case(name):

@@ -1,0 +1,185 @@
+"""Replay harness of the produce-bag scenarios (the reference CLI's run,
+tools/cloth_bag.cpp:5504-5760): scripted grip motions, render triangles, the
+state hash (hashResult) and the OBJ writer (dumpOBJ) pinned to the reference,
+and the GPU harness checked against the oracle through that hash.
+"""
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import numi_cloth as nc
+import oracle_py as op
+from helpers import FULL, ROOT
+from test_oracle_pin import GOLDEN, load_case, reference_schedule
+
+SCENARIO_CASES = ["grounded", "spin", "pickup", "recorded_lift"]
+
+
+def _fp64_final_state(name):
+    """The oracle's serial FP64 run of a golden case with every family on:
+    the reference's final state, bit for bit."""
+    z, scene = load_case(name)
+    steps, subs, its = (int(v) for v in z["meta"])
+    o = op.Oracle(scene, 64)
+    sched = reference_schedule(its, 0 if name == "grounded" else 1)
+    sched.primitive_self = 1
+    for s in range(steps):
+        assert o.step(z["substeps"][s * subs:(s + 1) * subs], sched) == 0
+    return z, o.read()
+
+
+def _hash_of(st, last_sub):
+    p, f = st["particles"], st["fruits"]
+    ps = np.concatenate([p["x"], p["v"]], axis=1)
+    q = f["q"]   # xyzw
+    fs = np.concatenate([f["x"], f["v"], f["omega"], q[:, 3:4], q[:, 0:3]], axis=1)
+    g = st["grips"]
+    gen = int(last_sub["grip_gen"])
+    selected = 1 if (gen > 1 and int(last_sub["grip_select"]) == 1) else 0
+    return nc.state_hash(ps, fs, last_sub["grip_target"], bool(last_sub["grip_active"]), gen,
+                         g["particle"], g["offset"], selected)
+
+
+@pytest.mark.parametrize("name", SCENARIO_CASES)
+def test_render_triangles_equal_reference(name):
+    z = np.load(os.path.join(GOLDEN, f"ref_{name}.npz"))
+    scenario = json.load(open(os.path.join(GOLDEN, "ref_hashes.json")))[name]["args"]["scenario"]
+    ours = nc.bag_scene(scenario=scenario).extra["triangles"]
+    assert np.array_equal(ours, z["triangles"])
+
+
+@pytest.mark.parametrize("name", ["spin", "pickup"])
+def test_scripted_grip_targets_equal_reference(name):
+    """spinGripTarget / pickupGripTarget at the end of every substep, FP64,
+    against the poses the reference loop used."""
+    z = np.load(os.path.join(GOLDEN, f"ref_{name}.npz"))
+    steps, subs, _ = (int(v) for v in z["meta"])
+    args = json.load(open(os.path.join(GOLDEN, "ref_hashes.json")))[name]["args"]
+    dt = args["frame_dt"] / subs
+    scene = nc.bag_scene(scenario=name, timestep=dt)
+    cfg, targets = nc.bag_scenario_configs(scene, 0, steps * subs, dt)
+    ref = z["substeps"]
+    assert np.array_equal(targets, ref["grip_target"])
+    assert np.all(ref["grip_active"] == 1) and np.all(cfg["gripTargetAndActive"][:, 3] == 1.0)
+    assert np.array_equal(cfg["gripTargetAndActive"][:, :3], ref["grip_target"].astype(np.float32))
+    assert np.all(cfg["gripOrientation"] == np.array([0, 0, 0, 1], np.float32))
+
+
+def test_handle_base_equals_scene():
+    """The library's grip handle (numi_cloth_bag_handle_base) is the FP64
+    authored top-ring particle the scene's handle_base restates."""
+    import ctypes
+
+    for scenario in ("grounded", "spin", "pickup", "recorded"):
+        out = (ctypes.c_double * 3)()
+        assert nc.load_library().numi_cloth_bag_handle_base(nc.SCENARIOS[scenario], out) == 0
+        assert tuple(out) == nc.bag_scene(scenario=scenario).handle_base
+
+
+@pytest.mark.parametrize("name", ["recorded_lift", "grounded", "spin", "pickup", "patch_regrab_v3", "regrab_v2",
+                                  "rotation_v1"])
+def test_state_hash_equals_reference_simulate(name):
+    """hashResult restated, applied to the reference's final state (the
+    oracle's serial FP64 run), gives the reference simulate() hash."""
+    z, st = _fp64_final_state(name)
+    want = int(json.load(open(os.path.join(GOLDEN, "ref_hashes.json")))[name]["simulate"], 16)
+    assert _hash_of(st, z["substeps"][-1]) == want
+
+
+def test_obj_writer_equals_reference(tmp_path):
+    """dumpOBJ restated: the reference's final state of the spin case written
+    by our writer is the reference executable's file, byte for byte."""
+    import ctypes
+
+    z, st = _fp64_final_state("spin")
+    last = z["substeps"][-1]
+    p, f = st["particles"], st["fruits"]
+    xyz = np.ascontiguousarray(p["x"], np.float64)
+    tris = np.ascontiguousarray(z["triangles"], np.uint32)
+    q = f["q"]
+    fr = np.ascontiguousarray(np.concatenate([f["x"], f["radius"][:, None], q[:, 3:4], q[:, 0:3], f["omega"]],
+                                             axis=1), np.float64)
+    app = np.ascontiguousarray(f["appearance"], np.uint32)
+    s = nc.abi.ObjState()
+    s.particles, s.triangles = len(xyz), len(tris)
+    s.positions, s.triangleIndices = xyz.ctypes.data, tris.ctypes.data
+    s.scenario = nc.SCENARIOS["spin"]
+    s.gripActive = int(last["grip_active"])
+    s.gripTarget = (ctypes.c_double * 3)(*last["grip_target"])
+    gq = last["grip_q"]
+    s.gripOrientationWxyz = (ctypes.c_double * 4)(gq[3], gq[0], gq[1], gq[2])
+    s.patchCenter = 0
+    s.fruits = len(fr)
+    s.fruitState, s.fruitAppearance = fr.ctypes.data, app.ctypes.data
+    path = tmp_path / "spin.obj"
+    assert nc.load_library().numi_cloth_write_obj(str(path).encode(), ctypes.byref(s)) == 0
+    assert path.read_bytes() == open(os.path.join(GOLDEN, "ref_spin.obj"), "rb").read()
+
+
+def test_replay_rejects_bad_controls():
+    with pytest.raises(nc.ClothError, match="recorded scenario requires exactly one grip trajectory"):
+        nc.replay("recorded", steps=1)
+    with pytest.raises(nc.ClothError, match="simulation controls must be positive"):
+        nc.replay("spin", steps=0)
+
+
+# ----------------------------------------------------------------- GPU ----
+
+def _oracle_hash_fp32(scenario, steps, substeps, frame_dt, sched):
+    """The FP32 oracle's run of the scenario in the kernels' order, hashed as
+    the harness hashes the GPU state."""
+    dt = frame_dt / substeps
+    scene = nc.bag_scene(scenario=scenario, timestep=dt)
+    o = op.Oracle(op.from_abi(scene), 32)
+    osched = op.schedule_from_abi(sched, op.BATCHED)
+    target = np.zeros(3)
+    for s in range(steps):
+        cfg, targets = nc.bag_scenario_configs(scene, s * substeps, substeps, dt)
+        assert o.step(op.substeps_from_configs(cfg), osched) == 0
+        target = targets[-1]
+    st = o.read()
+    p, f = st["particles"], st["fruits"]
+    ps = np.concatenate([p["x"], p["v"]], axis=1)
+    q = f["q"]
+    fs = np.concatenate([f["x"], f["v"], f["omega"], q[:, 3:4], q[:, 0:3]], axis=1)
+    return nc.state_hash(ps, fs, target, scenario != "grounded", 1)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("scenario", ["spin", "pickup"])
+def test_gpu_replay_matches_oracle_and_replays(scenario):
+    sched = nc.Schedule.make(**dict(FULL, primitiveSelf=1, release=1))
+    r = nc.replay(scenario, steps=2, substeps=24, frame_dt=1.0 / 60.0, schedule=sched, replays=2)
+    assert r["failure"] == 0
+    assert r["deterministic"] and r["hash"] == r["replay_hash"]
+    assert r["hash"] == _oracle_hash_fp32(scenario, 2, 24, 1.0 / 60.0, sched)
+
+
+@pytest.mark.gpu
+def test_gpu_replay_recorded_frames(tmp_path):
+    sched = nc.Schedule.make(**dict(FULL, primitiveSelf=1, release=1))
+    traj = os.path.join(GOLDEN, "lift-v1.csv")
+    prefix = str(tmp_path / "lift")
+    r = nc.replay("recorded", steps=4, substeps=12, frame_dt=1.0 / 60.0, schedule=sched, trajectory=traj,
+                  dump_frames=prefix, dump_obj=str(tmp_path / "final.obj"))
+    assert r["failure"] == 0
+    for completed in (0, 1, 2, 3, 4):   # the quarters of 4 frames
+        lines = open(f"{prefix}-{completed}.obj").read().splitlines()
+        assert lines[0] == "# Numi Solver explicit-yarn cloth bag reference"
+        assert lines[1] == "# vertices 1465 render_triangles 2880"
+        assert sum(1 for l in lines if l.startswith("v ")) == 1465
+        assert sum(1 for l in lines if l.startswith("f ")) == 2880
+        assert sum(1 for l in lines if l.startswith("# ball ")) == 12
+    assert open(tmp_path / "final.obj").read() == open(f"{prefix}-4.obj").read()
+
+
+@pytest.mark.gpu
+def test_gpu_replay_command_line():
+    exe = os.path.join(ROOT, "numi-solver_b200", "numi_cloth", "numi-cloth-replay")
+    out = subprocess.run([exe, "--scenario", "pickup", "--steps", "1", "--substeps", "12", "--replays", "2"],
+                         capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    assert "deterministic=true" in out.stdout and "scenario=pickup" in out.stdout
