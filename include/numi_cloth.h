@@ -259,6 +259,12 @@ int numi_cloth_restore(numi_cloth_t* handle, uint32_t slot);
  * particles are resident in (distributed) shared memory. */
 int numi_cloth_launch_info(numi_cloth_t* handle, uint32_t out[6]);
 
+/* Pass counters: out[0] barriers of the last substep, out[1] the most
+ * reconciliation passes and out[2] the most certificate passes one substep
+ * took since create (the reference's max_contact_reconciliation_passes and
+ * max_primitive_certificate_passes, tools/cloth_bag.cpp:5838-5841). */
+int numi_cloth_pass_counts(numi_cloth_t* handle, uint32_t out[3]);
+
 /* Per-phase device timestamps of the last step (profiling aid).  Enabled
  * when the handle was created with NUMI_CLOTH_TRACE=<substeps> in the
  * environment; out receives substeps x slots (slots must be 128) globaltimer

@@ -86,6 +86,8 @@ typedef struct NumiClothReplayResult {
     unsigned long long selfContacts;
     unsigned long long edgeContacts[2];
     uint32_t masks[2];            /* released fruits, mouth candidates */
+    uint32_t reconcileMax;        /* most reconciliation passes of a substep */
+    uint32_t certificateMax;      /* most certificate passes of a substep */
     double seconds;               /* wall time of the first run's frames */
 } NumiClothReplayResult;
 

@@ -227,7 +227,7 @@ cudaError_t launch(numi_cloth* h, uint32_t substeps, const Schedule& s, uint32_t
     Schedule sc = s;
     sc.substeps = substeps;
     void* args[] = {&d, &sc};
-    const bool edge = sc.primitive_self != 0u && d.edge_head != nullptr;
+    const bool edge = sc.primitive_self != 0u && d.edge_count != nullptr;
     if (d.trace != nullptr && substeps > h->trace_capacity) d.trace = nullptr;
     if (d.trace == nullptr) d.trace_cta = nullptr;
     cudaError_t e = cudaMemsetAsync(h->d.bar_count, 0, 32 * sizeof(unsigned long long), h->stream);
@@ -306,25 +306,27 @@ int prepare_self_grid(numi_cloth* h, bool self_collision, uint32_t substeps) {
     return NUMI_CLOTH_OK;
 }
 
-// Edge/edge buffers of a cloth, allocated on first use: a segment grid of
-// about two buckets per yarn segment, room for 32 listed pairs and 16
-// candidate pairs per segment.  The grid cell is four times the cover sphere
-// of a median yarn segment stretched by half (larger spheres go to the
-// list).  The bucket heads are cleared when the 23-bit substep part of their
-// tags wraps within the next `substeps`.
+// Edge/edge buffers of a cloth, allocated on first use: a build grid of
+// about four buckets per yarn segment with room for 27 cells per segment, 32
+// listed pairs and 16 candidate pairs per segment.  The build cell is a
+// median yarn segment plus the yarn diameter and skin (three diameters), so
+// that a typical segment's grown box spans at most two cells a side.
 int prepare_edge_grid(numi_cloth* h, bool primitive, uint32_t substeps, float radius) {
+    (void)substeps;
     DeviceCloth& d = h->d;
-    if (primitive && d.edge_head == nullptr && d.y_count > 0u) {
+    if (primitive && d.edge_count == nullptr && d.y_count > 0u) {
         uint32_t buckets = 1024u;
-        while (buckets < 2u * d.y_count) buckets <<= 1;
+        while (buckets < 4u * d.y_count) buckets <<= 1;
         const uint32_t cap = std::max(1024u, 16u * d.y_count);
         const uint32_t list_cap = std::max(2048u, 32u * d.y_count);
+        const uint32_t ctas = std::max<uint32_t>(h->grid, 1u);
         DeviceCloth e = d;
-        e.edge_head = h->buf.alloc<unsigned long long>(buckets);
-        e.edge_slot = h->buf.alloc<HashSlot>(static_cast<size_t>(buckets) * NC_HASH_CAP);
-        e.edge_list_head = h->buf.alloc<unsigned long long>(1);
-        e.edge_list = h->buf.alloc<HashSlot>(d.y_count);
-        e.edge_flag = h->buf.alloc<uint32_t>(d.y_count);
+        e.edge_count = h->buf.alloc<uint32_t>(buckets);
+        e.edge_offs = h->buf.alloc<uint32_t>(buckets);
+        e.edge_chunk_total = h->buf.alloc<uint32_t>(ctas);
+        e.edge_entries = h->buf.alloc<uint4>(static_cast<size_t>(27u) * d.y_count);
+        e.edge_giant = h->buf.alloc<uint32_t>(d.y_count);
+        e.edge_bbox = h->buf.alloc<float4>(2u * d.y_count);
         e.edge_pairs = h->buf.alloc<uint2>(list_cap);
         e.edge_xb = h->buf.alloc<float4>(d.n);
         e.edge_pb = h->buf.alloc<float4>(d.n);
@@ -336,31 +338,28 @@ int prepare_edge_grid(numi_cloth* h, bool primitive, uint32_t substeps, float ra
         e.edge_order = h->buf.alloc<unsigned long long>(cap);
         e.edge_sorted = h->buf.alloc<unsigned long long>(cap);
         e.edge_new = h->buf.alloc<EdgeRecord>(cap);
+        e.edge_lv = h->buf.alloc<uint32_t>(cap);
+        e.edge_level = h->buf.alloc<uint32_t>(d.n);
+        e.edge_qbox_raw = h->buf.alloc<float>(6u * d.y_count);
         e.edge_rec = h->buf.alloc<EdgeRecord>(cap);
         e.edge_ctl = h->buf.alloc<uint32_t>(8);
         e.edge_stats = h->buf.alloc<unsigned long long>(2);
-        e.edge_red = h->buf.alloc<double>(2u * std::max<uint32_t>(h->grid, 1u));
-        if (!e.edge_head || !e.edge_slot || !e.edge_list_head || !e.edge_list || !e.edge_flag || !e.edge_pairs ||
-            !e.edge_xb || !e.edge_pb || !e.edge_built_radius || !e.edge_sph || !e.edge_x0 || !e.edge_path ||
-            !e.edge_cand || !e.edge_order || !e.edge_sorted || !e.edge_new || !e.edge_rec || !e.edge_ctl ||
-            !e.edge_stats || !e.edge_red)
+        e.edge_red = h->buf.alloc<double>(3u * ctas);
+        if (!e.edge_count || !e.edge_offs || !e.edge_chunk_total || !e.edge_entries || !e.edge_giant ||
+            !e.edge_pairs || !e.edge_xb || !e.edge_pb || !e.edge_built_radius || !e.edge_sph || !e.edge_x0 ||
+            !e.edge_path || !e.edge_cand || !e.edge_order || !e.edge_sorted || !e.edge_new || !e.edge_rec ||
+            !e.edge_ctl || !e.edge_stats || !e.edge_red || !e.edge_lv || !e.edge_level || !e.edge_qbox_raw || !e.edge_bbox)
             return NUMI_CLOTH_ENOMEM;
         e.edge_mask = buckets - 1u;
         e.edge_cap = cap;
         e.edge_list_cap = list_cap;
         d = e;
     }
-    if (d.edge_head != nullptr) {
-        d.edge_cell = 4.0f * (0.75f * h->yarn_rest_median + 2.0f * radius);
+    if (d.edge_count != nullptr) {
+        d.edge_cell = h->yarn_rest_median + 3.0f * (2.0f * radius);
         if (const char* v = std::getenv("NUMI_CLOTH_EDGE_CELL")) {
-            const float cell = std::strtof(v, nullptr);   // test hook: force the grid or the list path
+            const float cell = std::strtof(v, nullptr);   // test hook: force long segments or crowded cells
             if (cell > 0.0f) d.edge_cell = cell;
-        }
-        if (((h->epoch + substeps) >> 23) != (h->epoch >> 23)) {
-            if (cudaMemsetAsync(d.edge_head, 0, (static_cast<size_t>(d.edge_mask) + 1u) * sizeof(unsigned long long),
-                                h->stream) != cudaSuccess ||
-                cudaMemsetAsync(d.edge_list_head, 0, sizeof(unsigned long long), h->stream) != cudaSuccess)
-                return NUMI_CLOTH_ECUDA;
         }
     }
     return NUMI_CLOTH_OK;
@@ -999,6 +998,19 @@ int numi_cloth_trace_cta(numi_cloth_t* h, unsigned long long* out, uint32_t subs
     return NUMI_CLOTH_OK;
 }
 
+int numi_cloth_pass_counts(numi_cloth_t* h, uint32_t out[3]) {
+    if (h == nullptr || out == nullptr) return NUMI_CLOTH_EINVAL;
+    cudaSetDevice(h->device);
+    uint32_t stats[4] = {0, 0, 0, 0};
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess ||
+        cudaMemcpy(stats, h->d.stats, sizeof(stats), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return NUMI_CLOTH_ECUDA;
+    out[0] = stats[0];
+    out[1] = stats[1];
+    out[2] = stats[2];
+    return NUMI_CLOTH_OK;
+}
+
 int numi_cloth_launch_info(numi_cloth_t* h, uint32_t out[6]) {
     if (h == nullptr || out == nullptr) return NUMI_CLOTH_EINVAL;
     cudaSetDevice(h->device);
@@ -1311,7 +1323,7 @@ int batch_prepare(numi_cloth_batch* b, const NumiClothConfig* configs, uint32_t 
     for (size_t k = 0; k < b->cloths.size(); ++k) {
         numi_cloth* h = b->cloths[k];
         void* before = h->d.hash_head;
-        void* edge_before = h->d.edge_head;
+        void* edge_before = h->d.edge_count;
         const float cell_before = h->d.edge_cell;
         h->epoch = b->epoch_host;
         int rc = prepare_self_grid(h, sched.selfCollision != 0u, substeps);
@@ -1319,7 +1331,7 @@ int batch_prepare(numi_cloth_batch* b, const NumiClothConfig* configs, uint32_t 
             rc = prepare_edge_grid(h, sched.primitiveSelf != 0u, substeps,
                                    configs[k * substeps].clothMaterial.x);
         if (rc != NUMI_CLOTH_OK) return rc;
-        if (h->d.hash_head != before || h->d.edge_head != edge_before || h->d.edge_cell != cell_before)
+        if (h->d.hash_head != before || h->d.edge_count != edge_before || h->d.edge_cell != cell_before)
             b->layout_valid = false;
         if (h->stream != b->stream && h->stream != nullptr && cudaStreamSynchronize(h->stream) != cudaSuccess)
             return NUMI_CLOTH_ECUDA;
@@ -1566,8 +1578,6 @@ int numi_cloth_batch_replay(numi_cloth_batch_t* b) {
         }
         if (h->d.hash_head != nullptr && ((b->epoch_host + b->graph_substeps) >> 26) != (b->epoch_host >> 26))
             return NUMI_CLOTH_ESTATE;   // tag wrap: capture again after a plain step
-        if (h->d.edge_head != nullptr && ((b->epoch_host + b->graph_substeps) >> 23) != (b->epoch_host >> 23))
-            return NUMI_CLOTH_ESTATE;
     }
     const cudaError_t e = cudaGraphLaunch(b->exec, b->stream);
     batch_advance(b, b->graph_substeps);

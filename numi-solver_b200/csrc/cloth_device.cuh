@@ -153,12 +153,11 @@ struct DeviceCloth {
     unsigned long long* self_stats;
     // edge/edge yarn self-collision.  Yarn segments: the distances that are
     // not shear diagonals, in array order.  Buffers (allocated on first use):
-    //   pair list: every non-local segment pair (first < second) whose
-    //     present or swept spheres were within the skin when it was built,
-    //     the positions of the build, and for the build a hashed grid of
-    //     segment cover spheres (heads as the point grid's, pass tag = 23 bits
-    //     of the substep counter << 9 | pass) with a list for spheres too
-    //     large for a cell or met in a full bucket;
+    //   pair list: every non-local segment pair (first < second) within the
+    //     yarn diameter plus the skin at its build, the positions of the
+    //     build, and for the build a hashed cell grid sorted by counting
+    //     (per-bucket counts and offsets, the cells' entries: segment, lower
+    //     cell corner key, spans) with a list of segments too long for it;
     //   pass: the pass-start positions and spheres, each particle's path
     //     length, the candidates (first, second, distance bound bits, ordered
     //     flag), the keys (first << 32 | second) of the ordered pairs and
@@ -170,31 +169,36 @@ struct DeviceCloth {
     float edge_cell;
     uint32_t edge_cap;            // candidates, ordered pairs, records
     uint32_t edge_list_cap;       // pairs on the list
-    unsigned long long* edge_head;
-    HashSlot* edge_slot;          // [buckets * NC_HASH_CAP]
-    unsigned long long* edge_list_head;
-    HashSlot* edge_list;          // [y_count]
-    uint32_t* edge_flag;          // [y_count] 1: the segment's cover sphere is in the list
+    uint32_t* edge_count;         // [buckets]
+    uint32_t* edge_offs;          // [buckets], within the bucket's scan chunk
+    uint32_t* edge_chunk_total;   // [CTAs] entries of each CTA's chunk of buckets
+    uint4* edge_entries;          // [27 * y_count]
+    uint32_t* edge_giant;         // [y_count] segments the grid does not hold
+    float4* edge_bbox;            // [2 * y_count] grown boxes of the build
     uint2* edge_pairs;            // [edge_list_cap]
     float4* edge_xb;              // [n] positions at the build
     float4* edge_pb;              // [n] substep-start positions at the build
     float* edge_built_radius;     // yarn radius of the build
     float4* edge_x0;              // [n]
     float4* edge_sph;             // [y_count] pass spheres (centre, radius)
+    float* edge_qbox_raw;         // [6 * y_count] a first segment's tree-query box of the pass
     float* edge_path;             // [n]
     uint4* edge_cand;             // [edge_cap]
     unsigned long long* edge_order;    // [edge_cap]
     unsigned long long* edge_sorted;   // [edge_cap]
     EdgeRecord* edge_new;         // [edge_cap]
+    uint32_t* edge_lv;            // [edge_cap] wavefront level of each ordered pair (+ first / moved bits)
+    uint32_t* edge_level;         // [n] last wavefront level of each particle (zero between passes)
     EdgeRecord* edge_rec;         // [edge_cap]
     // [0] candidates, [1] ordered pairs, [2] violations found (only grows),
     // [3] records of the substep, [4] records of the pass, [5] pairs on the
-    // list, [6] 1 once the list is built
+    // list, [6] 1 once the list is built, [7] long segments of the build
     uint32_t* edge_ctl;
     // [0] edge/edge contacts resolved, [1] self-friction contacts
     unsigned long long* edge_stats;
     // [0, CTAs) deepest non-local pair of the last measure, [CTAs, 2 CTAs)
-    // largest displacement since the build
+    // largest displacement since the build, [2 CTAs, 3 CTAs) largest motion
+    // over the substep
     double* edge_red;
     // adjoint tape (one-CTA launches only): positions at the start of every
     // substep and after every barrier, [substep][tape_slots][n], and

@@ -40,7 +40,7 @@ namespace {   // internal linkage: the edge kernels' unit includes these too
 #define NC_EDGE_MARGIN 0.125f
 #define NC_EDGE_ROUNDS 64u
 // Skin of the pair list, in yarn diameters.
-#define NC_EDGE_SKIN 1.0f
+#define NC_EDGE_SKIN 2.0f
 
 __device__ __forceinline__ float clamp01f(float v) {
     const float a = v < 0.0f ? 0.0f : v;
@@ -157,10 +157,6 @@ __device__ __forceinline__ bool edge_local(const DeviceCloth& d, uint2 a, uint2 
     return local_pair(d, a.x, b.x) || local_pair(d, a.x, b.y) || local_pair(d, a.y, b.x) || local_pair(d, a.y, b.y);
 }
 
-// Pass tag of the segment grid: 23 bits of the substep counter and the
-// pass within the substep (the host clears the heads when they wrap).
-__device__ __forceinline__ uint32_t edge_tag(const Ctx& ctx) { return ((ctx.epoch & 0x7fffffu) << 9) | (ctx.edge_pass & 511u); }
-
 __device__ __forceinline__ unsigned long long edge_key(uint32_t i, uint32_t j) {
     return (static_cast<unsigned long long>(i) << 32) | j;
 }
@@ -273,33 +269,27 @@ __device__ bool edge_present(EdgeQuad& q, float radius, float dt, EdgeRecord& re
     return true;
 }
 
-// Cover sphere of a segment for the pair list: centred on the segment's
-// midpoint, large enough to hold both its present and its swept sphere,
-// plus half the skin.
-__device__ __forceinline__ float4 edge_cover(V3 a, V3 b, V3 ap, V3 bp, float ex, float skin) {
-    const float4 ps = edge_sphere(a, b, ap, bp, false, ex);
-    const float4 ss = edge_sphere(a, b, ap, bp, true, ex);
-    const float r = fmaxf(ps.w, len3(xyz(ss) - xyz(ps)) + ss.w) + 0.5f * skin;
-    return make_float4(ps.x, ps.y, ps.z, r);
-}
-
 __device__ __forceinline__ float edge_skin(const Ctx& ctx) { return NC_EDGE_SKIN * (2.0f * ctx.c.radius); }
 
 // Phase 1: snapshot the pass-start positions, clear the path lengths, write
-// every segment's pass sphere and this CTA's largest displacement (of x and
-// of the substep-start positions) since the pair list was built.
+// every segment's pass sphere, and this CTA's largest displacement since the
+// pair list was built (of x and of the substep-start positions) and largest
+// motion over the substep so far (x - substep start).
 __device__ void edge_begin(Ctx& ctx, bool swept) {
     const DeviceCloth& d = ctx.d;
     const float ex = 0.5f * (2.0f * ctx.c.radius);
-    float moved = 0.0f;
+    float moved = 0.0f, motion = 0.0f;
     for (Range r = particle_range(ctx); r.i < r.end; r.i += r.stride) {
         const float4 p = px(ctx, r.i);
+        const V3 prev = xyz(ld(d.xp + r.i));
         d.edge_x0[r.i] = p;
         d.edge_path[r.i] = 0.0f;
-        const V3 dx = xyz(p) - xyz(ld(d.edge_xb + r.i));
-        const V3 dp = xyz(ld(d.xp + r.i)) - xyz(ld(d.edge_pb + r.i));
-        moved = fmaxf(moved, fmaxf(len3(dx), len3(dp)));
-        if (!(len3(dx) == len3(dx))) moved = INFINITY;   // NaN: rebuild, and the bound checks fail later
+        const float dx = len3(xyz(p) - xyz(ld(d.edge_xb + r.i)));
+        const float dp = len3(prev - xyz(ld(d.edge_pb + r.i)));
+        const float dm = len3(xyz(p) - prev);
+        moved = fmaxf(moved, fmaxf(dx, dp));
+        motion = fmaxf(motion, dm);
+        if (!(dx == dx && dp == dp && dm == dm)) moved = INFINITY;   // NaN: rebuild; the bound checks fail later
     }
     for (Range r = item_range(ctx, d.y_count); r.i < r.end; r.i += r.stride) {
         const uint2 ab = __ldg(d.y_ij + r.i);
@@ -308,78 +298,118 @@ __device__ void edge_begin(Ctx& ctx, bool swept) {
     }
     double (*s_r)[NC_BLOCK_MAX] = nc_red_smem;
     s_r[0][threadIdx.x] = static_cast<double>(moved);
+    s_r[1][threadIdx.x] = static_cast<double>(motion);
     __syncthreads();
     for (uint32_t st = blockDim.x / 2u; st > 0u; st >>= 1u) {
-        if (threadIdx.x < st) s_r[0][threadIdx.x] = fmax(s_r[0][threadIdx.x], s_r[0][threadIdx.x + st]);
+        if (threadIdx.x < st) {
+            s_r[0][threadIdx.x] = fmax(s_r[0][threadIdx.x], s_r[0][threadIdx.x + st]);
+            s_r[1][threadIdx.x] = fmax(s_r[1][threadIdx.x], s_r[1][threadIdx.x + st]);
+        }
         __syncthreads();
     }
-    if (threadIdx.x == 0) d.edge_red[ctx.ranks + ctx.rank] = s_r[0][0];
+    if (threadIdx.x == 0) {
+        d.edge_red[ctx.ranks + ctx.rank] = s_r[0][0];
+        d.edge_red[2u * ctx.ranks + ctx.rank] = s_r[1][0];
+    }
     __syncthreads();
     if (ctx.rank == 0 && threadIdx.x == 0) {
         d.edge_ctl[0] = 0u;   // candidates
         d.edge_ctl[1] = 0u;   // ordered pairs
         d.edge_ctl[4] = 0u;   // records of the pass
+        d.edge_ctl[7] = 0u;   // segments too long for the build grid
         if (swept) d.edge_ctl[3] = 0u;   // records of the substep
     }
 }
 
-// The pair list holds every non-local pair whose present or swept spheres
-// were within the skin of each other when it was built.  A sphere's centre
-// moves at most as far as its points and its radius changes at most twice
-// that, so while every position moved less than a sixth of the skin since
-// the build, every pair whose spheres overlap now is on the list.
+// The pair list holds every non-local pair whose segments were within the
+// yarn diameter plus the skin of each other at the build, at the build's
+// positions or at its substep-start positions.  Every position has moved at
+// most D since (D: the larger of the two displacements), and every endpoint
+// at most M over the substep so far, so an unlisted pair is at least
+// diameter + skin - 2D apart now, and its swept bound (half the start and end
+// distances less the motion) is at least diameter + skin - 2D - M.  While
+// 2D + M + the ordering margin stays below the skin, no unlisted pair can be
+// a candidate, and no pair closer than the diameter is unlisted.
 __device__ bool edge_list_valid(const Ctx& ctx) {
     const DeviceCloth& d = ctx.d;
     if (__ldcg(d.edge_ctl + 6) == 0u || __ldcg(d.edge_built_radius) != ctx.c.radius) return false;
-    double moved = 0.0;
-    for (uint32_t r = 0; r < ctx.ranks; ++r) moved = fmax(moved, __ldcg(d.edge_red + ctx.ranks + r));
-    return 6.0 * moved + 1.0e-6 < static_cast<double>(edge_skin(ctx));
+    double moved = 0.0, motion = 0.0;
+    for (uint32_t r = 0; r < ctx.ranks; ++r) {
+        moved = fmax(moved, __ldcg(d.edge_red + ctx.ranks + r));
+        motion = fmax(motion, __ldcg(d.edge_red + 2u * ctx.ranks + r));
+    }
+    const double target = 2.0 * static_cast<double>(ctx.c.radius);
+    return 2.0 * moved + motion + NC_EDGE_MARGIN * target + 1.0e-6 < static_cast<double>(edge_skin(ctx));
 }
 
-// Rebuild, step 1: put every segment's cover sphere into the grid (or the
-// list) and remember the positions of the build.
-__device__ void edge_build_insert(Ctx& ctx) {
+// Build-grid cells of a segment: its current and substep-start endpoints'
+// box grown by half of (diameter + skin), so that two segments within
+// diameter + skin of each other share a cell.  A span of 0 marks a segment
+// the grid does not hold (more than 27 cells, or not finite).
+struct EdgeCells {
+    int lo[3];
+    int span[3];
+};
+__device__ __forceinline__ EdgeCells edge_cells(V3 a, V3 b, V3 ap, V3 bp, float h, float inv_cell) {
+    const float lo[3] = {fminf(fminf(a.x, b.x), fminf(ap.x, bp.x)) - h, fminf(fminf(a.y, b.y), fminf(ap.y, bp.y)) - h,
+                         fminf(fminf(a.z, b.z), fminf(ap.z, bp.z)) - h};
+    const float hi[3] = {fmaxf(fmaxf(a.x, b.x), fmaxf(ap.x, bp.x)) + h, fmaxf(fmaxf(a.y, b.y), fmaxf(ap.y, bp.y)) + h,
+                         fmaxf(fmaxf(a.z, b.z), fmaxf(ap.z, bp.z)) + h};
+    EdgeCells c;
+    bool ok = true;
+    for (int k = 0; k < 3; ++k) {
+        const float l = floorf(lo[k] * inv_cell), u = floorf(hi[k] * inv_cell);
+        ok = ok && l >= -1048576.0f && u <= 1048575.0f && u - l <= 2.0f;   // finite, biased key, at most 3 cells
+        c.lo[k] = ok ? static_cast<int>(l) : 0;
+        c.span[k] = ok ? static_cast<int>(u - l) + 1 : 0;
+    }
+    if (!ok)
+        for (int k = 0; k < 3; ++k) c.span[k] = 0;
+    return c;
+}
+__device__ __forceinline__ unsigned long long edge_cell_key(int x, int y, int z) {
+    return (static_cast<unsigned long long>(x + (1 << 20)) & 0x1fffffull) |
+           ((static_cast<unsigned long long>(y + (1 << 20)) & 0x1fffffull) << 21) |
+           ((static_cast<unsigned long long>(z + (1 << 20)) & 0x1fffffull) << 42);
+}
+
+// Exclusive-scan chunk of the buckets handled by this CTA.
+__device__ __forceinline__ uint32_t edge_chunk(const Ctx& ctx) {
+    const uint32_t buckets = ctx.d.edge_mask + 1u;
+    return (buckets + ctx.ranks - 1u) / ctx.ranks;
+}
+
+// Rebuild, step 1: remember the build's positions and count every
+// segment's cells into its bucket (cells hash as the point grid's); a
+// segment the grid does not hold goes to the long-segment list.
+__device__ void edge_build_count(Ctx& ctx) {
     const DeviceCloth& d = ctx.d;
-    const float ex = 0.5f * (2.0f * ctx.c.radius);
-    const float skin = edge_skin(ctx);
+    const float h = 0.5f * (2.0f * ctx.c.radius + edge_skin(ctx));
     const float inv_cell = 1.0f / d.edge_cell;
-    const float grid_radius = 0.25f * d.edge_cell;
-    const unsigned long long tag = edge_tag(ctx);
     for (Range r = particle_range(ctx); r.i < r.end; r.i += r.stride) {
         d.edge_xb[r.i] = ld(d.edge_x0 + r.i);
         d.edge_pb[r.i] = ld(d.xp + r.i);
     }
     for (Range r = item_range(ctx, d.y_count); r.i < r.end; r.i += r.stride) {
-        const uint32_t k = r.i;
-        const uint2 ab = __ldg(d.y_ij + k);
-        const float4 sph = edge_cover(xyz(ld(d.edge_x0 + ab.x)), xyz(ld(d.edge_x0 + ab.y)), xyz(ld(d.xp + ab.x)),
-                                      xyz(ld(d.xp + ab.y)), ex, skin);
-        bool listed = !(sph.w <= grid_radius);
-        HashSlot* e = nullptr;
-        if (!listed) {
-            const uint32_t bucket = cell_bucket(static_cast<int>(floorf(sph.x * inv_cell)),
-                                                static_cast<int>(floorf(sph.y * inv_cell)),
-                                                static_cast<int>(floorf(sph.z * inv_cell)), d.edge_mask);
-            unsigned long long* head = d.edge_head + bucket;
-            atomicMax(head, tag << 32);
-            const uint32_t slot = static_cast<uint32_t>(atomicAdd(head, 1ull));
-            if (slot < NC_HASH_CAP)
-                e = d.edge_slot + bucket * NC_HASH_CAP + slot;
-            else
-                listed = true;
+        const uint2 ab = __ldg(d.y_ij + r.i);
+        const V3 a = xyz(ld(d.edge_x0 + ab.x)), b = xyz(ld(d.edge_x0 + ab.y)), ap = xyz(ld(d.xp + ab.x)),
+                 bp = xyz(ld(d.xp + ab.y));
+        // the grown box, for the pair search's first test
+        d.edge_bbox[2u * r.i] = make_float4(fminf(fminf(a.x, b.x), fminf(ap.x, bp.x)) - h,
+                                            fminf(fminf(a.y, b.y), fminf(ap.y, bp.y)) - h,
+                                            fminf(fminf(a.z, b.z), fminf(ap.z, bp.z)) - h, 0.0f);
+        d.edge_bbox[2u * r.i + 1u] = make_float4(fmaxf(fmaxf(a.x, b.x), fmaxf(ap.x, bp.x)) + h,
+                                                 fmaxf(fmaxf(a.y, b.y), fmaxf(ap.y, bp.y)) + h,
+                                                 fmaxf(fmaxf(a.z, b.z), fmaxf(ap.z, bp.z)) + h, 0.0f);
+        const EdgeCells c = edge_cells(a, b, ap, bp, h, inv_cell);
+        if (c.span[0] == 0) {
+            d.edge_giant[atomicAdd(d.edge_ctl + 7, 1u)] = r.i;
+            continue;
         }
-        if (listed) {
-            atomicMax(d.edge_list_head, tag << 32);
-            const uint32_t o = static_cast<uint32_t>(atomicAdd(d.edge_list_head, 1ull));
-            if (o >= d.y_count) {   // cannot happen: at most one entry per segment
-                fail(d, NUMI_CLOTH_FAILURE_RANGE);
-                continue;
-            }
-            e = d.edge_list + o;
-        }
-        e->pos = sph;
-        e->meta = make_uint4(k, 0u, 0u, 0u);
-        d.edge_flag[k] = listed ? 1u : 0u;
+        for (int z = 0; z < c.span[2]; ++z)
+            for (int y = 0; y < c.span[1]; ++y)
+                for (int x = 0; x < c.span[0]; ++x)
+                    atomicAdd(d.edge_count + cell_bucket(c.lo[0] + x, c.lo[1] + y, c.lo[2] + z, d.edge_mask), 1u);
     }
     if (ctx.rank == 0 && threadIdx.x == 0) {
         d.edge_ctl[5] = 0u;   // pairs on the list
@@ -387,36 +417,106 @@ __device__ void edge_build_insert(Ctx& ctx) {
     }
 }
 
-// Rebuild, step 2: every pair of overlapping cover spheres (a < b) once.
-// Grid segments query the 2 x 2 x 2 cells on their centre's side (a cell
-// is at least twice the largest distance between the centres of two
-// overlapping grid spheres) and scan the list; list segments scan only the
-// list.  A pair of grid segments is met by its lower index, a grid/list
-// pair by the grid segment, a pair of list segments by its lower index.
-__device__ void edge_build_pairs(Ctx& ctx) {
+// Rebuild, step 2: exclusive scan of the bucket counts.  Each CTA scans its
+// chunk of buckets into edge_offs (chunk-local) and publishes the chunk's
+// total; the counts are zeroed to serve as fill cursors.
+__device__ void edge_build_scan(Ctx& ctx) {
     const DeviceCloth& d = ctx.d;
-    const float ex = 0.5f * (2.0f * ctx.c.radius);
-    const float skin = edge_skin(ctx);
+    __shared__ uint32_t s_part[NC_BLOCK_MAX];
+    const uint32_t buckets = d.edge_mask + 1u;
+    const uint32_t chunk = edge_chunk(ctx);
+    const uint32_t first = min(ctx.rank * chunk, buckets), end = min(first + chunk, buckets);
+    const uint32_t per = (end - first + blockDim.x - 1u) / blockDim.x;
+    const uint32_t lo = min(first + threadIdx.x * per, end), hi = min(lo + per, end);
+    uint32_t sum = 0;
+    for (uint32_t b = lo; b < hi; ++b) sum += __ldcg(d.edge_count + b);
+    s_part[threadIdx.x] = sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {   // the CTA's thread totals, in order
+        uint32_t run = 0;
+        for (uint32_t t = 0; t < blockDim.x; ++t) {
+            const uint32_t v = s_part[t];
+            s_part[t] = run;
+            run += v;
+        }
+        d.edge_chunk_total[ctx.rank] = run;
+    }
+    __syncthreads();
+    uint32_t run = s_part[threadIdx.x];
+    for (uint32_t b = lo; b < hi; ++b) {
+        const uint32_t v = __ldcg(d.edge_count + b);
+        d.edge_offs[b] = run;
+        d.edge_count[b] = 0u;
+        run += v;
+    }
+}
+
+// The start of every CTA's chunk: exclusive prefix of the chunk totals.
+__device__ __forceinline__ void edge_chunk_starts(const Ctx& ctx, uint32_t* s_start) {
+    if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (uint32_t r = 0; r < ctx.ranks; ++r) {
+            s_start[r] = run;
+            run += __ldcg(ctx.d.edge_chunk_total + r);
+        }
+    }
+    __syncthreads();
+}
+
+// Rebuild, step 3: every segment's cells into the sorted entry array
+// (segment, lower cell corner key, spans).
+__device__ void edge_build_scatter(Ctx& ctx, uint32_t* s_start) {
+    const DeviceCloth& d = ctx.d;
+    const float h = 0.5f * (2.0f * ctx.c.radius + edge_skin(ctx));
     const float inv_cell = 1.0f / d.edge_cell;
-    const uint32_t tag = edge_tag(ctx);
-    const unsigned long long lh = __ldcg(d.edge_list_head);
-    const uint32_t listed_count = static_cast<uint32_t>(lh >> 32) == tag ? min(static_cast<uint32_t>(lh), d.y_count) : 0u;
-    // the exact test of the build: present or swept spheres within the skin
+    const uint32_t chunk = edge_chunk(ctx);
+    edge_chunk_starts(ctx, s_start);
+    for (Range r = item_range(ctx, d.y_count); r.i < r.end; r.i += r.stride) {
+        const uint2 ab = __ldg(d.y_ij + r.i);
+        const EdgeCells c = edge_cells(xyz(ld(d.edge_x0 + ab.x)), xyz(ld(d.edge_x0 + ab.y)), xyz(ld(d.xp + ab.x)),
+                                       xyz(ld(d.xp + ab.y)), h, inv_cell);
+        if (c.span[0] == 0) continue;
+        const unsigned long long key = edge_cell_key(c.lo[0], c.lo[1], c.lo[2]);
+        const uint4 entry = make_uint4(r.i, static_cast<uint32_t>(key), static_cast<uint32_t>(key >> 32),
+                                       static_cast<uint32_t>((c.span[0] - 1) | ((c.span[1] - 1) << 2) |
+                                                             ((c.span[2] - 1) << 4)));
+        for (int z = 0; z < c.span[2]; ++z)
+            for (int y = 0; y < c.span[1]; ++y)
+                for (int x = 0; x < c.span[0]; ++x) {
+                    const uint32_t b = cell_bucket(c.lo[0] + x, c.lo[1] + y, c.lo[2] + z, d.edge_mask);
+                    const uint32_t at = s_start[b / chunk] + __ldcg(d.edge_offs + b) + atomicAdd(d.edge_count + b, 1u);
+                    d.edge_entries[at] = entry;
+                }
+    }
+}
+
+// Rebuild, step 4: the pairs.  A segment visits its cells; an entry of a
+// later segment is a pair when the visited cell lies in that segment's
+// range and is the lowest cell of the two ranges' overlap, so that every
+// pair is met once.  Long segments: every held segment scans their list,
+// and they pair among themselves by index.  A pair is listed when it is
+// not local and its segments are within diameter + skin at the build's
+// positions or at its substep-start positions.
+__device__ void edge_build_pairs(Ctx& ctx, const uint32_t* s_start) {
+    const DeviceCloth& d = ctx.d;
+    const float target = 2.0f * ctx.c.radius;
+    const float reach = target + edge_skin(ctx);
+    const float h = 0.5f * reach;
+    const float inv_cell = 1.0f / d.edge_cell;
+    const uint32_t chunk = edge_chunk(ctx);
+    const uint32_t giants = min(__ldcg(d.edge_ctl + 7), d.y_count);
+    // the positions and entries are not written in this phase: the reads
+    // may go through L1 after a grid barrier (a gpu-scope acquire), not
+    // after the cluster barrier (cluster scope)
+    const bool l1 = d.cluster_barrier == 0u;
+    auto rd = [l1](const float4* p) { return xyz(l1 ? __ldca(p) : __ldcg(p)); };
     auto keep = [&](uint32_t a, uint32_t b) {
         const uint2 sa = __ldg(d.y_ij + a), sb = __ldg(d.y_ij + b);
-        if (edge_local(d, sa, sb)) return;
-        const V3 xa0 = xyz(ld(d.edge_x0 + sa.x)), xa1 = xyz(ld(d.edge_x0 + sa.y));
-        const V3 xb0 = xyz(ld(d.edge_x0 + sb.x)), xb1 = xyz(ld(d.edge_x0 + sb.y));
-        const V3 pa0 = xyz(ld(d.xp + sa.x)), pa1 = xyz(ld(d.xp + sa.y));
-        const V3 pb0 = xyz(ld(d.xp + sb.x)), pb1 = xyz(ld(d.xp + sb.y));
-        bool near = false;
-        for (int v = 0; v < 2 && !near; ++v) {
-            const float4 s1 = edge_sphere(xa0, xa1, pa0, pa1, v == 1, ex);
-            const float4 s2 = edge_sphere(xb0, xb1, pb0, pb1, v == 1, ex);
-            const float r = s1.w + s2.w + skin;
-            near = lsq(xyz(s1) - xyz(s2)) <= r * r;
-        }
-        if (!near) return;
+        const bool near =
+            segment_distance(rd(d.edge_x0 + sa.x), rd(d.edge_x0 + sa.y), rd(d.edge_x0 + sb.x), rd(d.edge_x0 + sb.y)) <=
+                reach ||
+            segment_distance(rd(d.xp + sa.x), rd(d.xp + sa.y), rd(d.xp + sb.x), rd(d.xp + sb.y)) <= reach;
+        if (!near || edge_local(d, sa, sb)) return;
         const uint32_t k = atomicAdd(d.edge_ctl + 5, 1u);
         if (k >= d.edge_list_cap) {
             fail(d, NUMI_CLOTH_FAILURE_RANGE);
@@ -424,87 +524,101 @@ __device__ void edge_build_pairs(Ctx& ctx) {
         }
         d.edge_pairs[k] = make_uint2(a, b);
     };
+    auto rd4 = [l1](const float4* p) { return l1 ? __ldca(p) : __ldcg(p); };
     for (Range r = item_range(ctx, d.y_count); r.i < r.end; r.i += r.stride) {
         const uint32_t i = r.i;
-        const uint2 ai = __ldg(d.y_ij + i);
-        const float4 si = edge_cover(xyz(ld(d.edge_x0 + ai.x)), xyz(ld(d.edge_x0 + ai.y)), xyz(ld(d.xp + ai.x)),
-                                     xyz(ld(d.xp + ai.y)), ex, skin);
-        const bool listed = __ldcg(d.edge_flag + i) != 0u;
-        if (!listed) {
-            int base[3], step[3];
-            float gap2[3];
-            const float coord[3] = {si.x * inv_cell, si.y * inv_cell, si.z * inv_cell};
-            for (int k = 0; k < 3; ++k) {
-                const float c0 = floorf(coord[k]);
-                const float frac = coord[k] - c0;
-                base[k] = static_cast<int>(c0);
-                step[k] = frac < 0.5f ? -1 : 1;
-                const float gap = frac < 0.5f ? frac : 1.0f - frac;
-                gap2[k] = gap * gap;
-            }
-            // neighbour cells farther than this sphere's reach (its radius
-            // plus the largest grid radius, a quarter cell) hold no partner;
-            // the margin covers the rounding of the cell coordinates
-            const float reach = si.w * inv_cell + 0.25f + 1.0e-3f +
-                                2.4e-7f * fmaxf(fabsf(coord[0]), fmaxf(fabsf(coord[1]), fabsf(coord[2])));
-            const float reach2 = reach * reach;
-            uint32_t bk[8];
-            bool near[8];
-            for (uint32_t q = 0; q < 8u; ++q) {
-                bk[q] = cell_bucket(base[0] + ((q & 1u) ? step[0] : 0), base[1] + ((q & 2u) ? step[1] : 0),
-                                    base[2] + ((q & 4u) ? step[2] : 0), d.edge_mask);
-                const float g2 =
-                    ((q & 1u) ? gap2[0] : 0.0f) + ((q & 2u) ? gap2[1] : 0.0f) + ((q & 4u) ? gap2[2] : 0.0f);
-                bool repeat = false;
-                for (uint32_t e = 0; e < q; ++e) repeat = repeat || (near[e] && bk[e] == bk[q]);
-                near[q] = (q == 0u || g2 < reach2) && !repeat;
-            }
-            for (uint32_t q = 0; q < 8u; ++q) {
-                if (!near[q]) continue;
-                const unsigned long long hd = __ldcg(d.edge_head + bk[q]);
-                if (static_cast<uint32_t>(hd >> 32) != tag) continue;
-                const uint32_t cnt = min(static_cast<uint32_t>(hd), NC_HASH_CAP);
-                for (uint32_t k = 0; k < cnt; ++k) {
-                    const HashSlot* e = d.edge_slot + bk[q] * NC_HASH_CAP + k;
-                    const uint32_t j = __ldcg(&e->meta.x);
-                    if (j <= i || !spheres_overlap(si, __ldcg(&e->pos))) continue;
-                    keep(i, j);
-                }
-            }
+        const uint2 ab = __ldg(d.y_ij + i);
+        const EdgeCells c = edge_cells(xyz(ld(d.edge_x0 + ab.x)), xyz(ld(d.edge_x0 + ab.y)), xyz(ld(d.xp + ab.x)),
+                                       xyz(ld(d.xp + ab.y)), h, inv_cell);
+        const float4 blo = rd4(d.edge_bbox + 2u * i), bhi = rd4(d.edge_bbox + 2u * i + 1u);
+        if (c.span[0] != 0) {
+            for (int z = 0; z < c.span[2]; ++z)
+                for (int y = 0; y < c.span[1]; ++y)
+                    for (int x = 0; x < c.span[0]; ++x) {
+                        const int cx = c.lo[0] + x, cy = c.lo[1] + y, cz = c.lo[2] + z;
+                        const uint32_t b = cell_bucket(cx, cy, cz, d.edge_mask);
+                        const uint32_t start = s_start[b / chunk] + (l1 ? __ldca(d.edge_offs + b) : __ldcg(d.edge_offs + b));
+                        const uint32_t count = l1 ? __ldca(d.edge_count + b) : __ldcg(d.edge_count + b);
+                        for (uint32_t e0 = start; e0 < start + count; e0 += 8u) {
+                          uint4 ens[8];
+#pragma unroll
+                          for (uint32_t q = 0; q < 8u; ++q) {   // issue the group's loads together
+                              const uint32_t e = min(e0 + q, start + count - 1u);
+                              ens[q] = l1 ? __ldca(d.edge_entries + e) : __ldcg(d.edge_entries + e);
+                          }
+#pragma unroll
+                          for (uint32_t q = 0; q < 8u; ++q) {
+                            if (e0 + q >= start + count) break;
+                            const uint4 en = ens[q];
+                            if (en.x <= i) continue;
+                            const unsigned long long key = static_cast<unsigned long long>(en.y) |
+                                                           (static_cast<unsigned long long>(en.z) << 32);
+                            const int jx = static_cast<int>(key & 0x1fffffull) - (1 << 20);
+                            const int jy = static_cast<int>((key >> 21) & 0x1fffffull) - (1 << 20);
+                            const int jz = static_cast<int>((key >> 42) & 0x1fffffull) - (1 << 20);
+                            const int sx = static_cast<int>(en.w & 3u) + 1, sy = static_cast<int>((en.w >> 2) & 3u) + 1,
+                                      sz = static_cast<int>((en.w >> 4) & 3u) + 1;
+                            // the visited cell in the other range, and the lowest common cell
+                            if (cx < jx || cx >= jx + sx || cy < jy || cy >= jy + sy || cz < jz || cz >= jz + sz)
+                                continue;
+                            if (cx != max(c.lo[0], jx) || cy != max(c.lo[1], jy) || cz != max(c.lo[2], jz)) continue;
+                            const float4 olo = rd4(d.edge_bbox + 2u * en.x), ohi = rd4(d.edge_bbox + 2u * en.x + 1u);
+                            if (olo.x > bhi.x || ohi.x < blo.x || olo.y > bhi.y || ohi.y < blo.y || olo.z > bhi.z ||
+                                ohi.z < blo.z)
+                                continue;   // the grown boxes do not meet: farther apart than diameter + skin
+                            keep(i, en.x);
+                          }
+                        }
+                    }
         }
-        for (uint32_t o = 0; o < listed_count; ++o) {
-            const uint32_t j = __ldcg(&d.edge_list[o].meta.x);
-            if (j == i || (listed && j < i)) continue;
-            if (!spheres_overlap(si, __ldcg(&d.edge_list[o].pos))) continue;
-            if (j > i)
-                keep(i, j);
-            else
-                keep(j, i);
+        for (uint32_t g = 0; g < giants; ++g) {
+            const uint32_t j = __ldcg(d.edge_giant + g);
+            if (j == i || (c.span[0] == 0 && j < i)) continue;
+            keep(min(i, j), max(i, j));
         }
     }
 }
 
-// Phases 1 and the rebuild when it is due.  Returns false when a barrier
-// gave up.
-__device__ __forceinline__ bool edge_prepare(Ctx& ctx, bool swept) {
+// Phase 1 and, when due, the rebuild of the pair list.  Returns false
+// when a barrier gave up; rebuilt tells the candidates phase to clear the
+// build counts.
+__device__ __forceinline__ bool edge_prepare(Ctx& ctx, bool swept, bool& rebuilt) {
+    __shared__ uint32_t s_start[1024];
     edge_begin(ctx, swept);
     NC_SYNC(ctx);
-    if (!edge_list_valid(ctx)) {
-        edge_build_insert(ctx);
+    rebuilt = !edge_list_valid(ctx);
+    if (rebuilt) {
+        if (ctx.ranks > 1024u) {   // the chunk starts live in shared memory
+            fail(ctx.d, NUMI_CLOTH_FAILURE_RANGE);
+            rebuilt = false;
+            return true;
+        }
+        edge_build_count(ctx);
         NC_SYNC(ctx);
-        edge_build_pairs(ctx);
+        edge_build_scan(ctx);
+        NC_SYNC(ctx);
+        edge_build_scatter(ctx, s_start);
+        NC_SYNC(ctx);
+        edge_build_pairs(ctx, s_start);
         NC_SYNC(ctx);
         if (ctx.rank == 0 && threadIdx.x == 0) ctx.d.edge_ctl[6] = 1u;   // the list is built
     }
     return true;
 }
 
+// The build counts serve as fill cursors and ranges until the pairs are
+// listed; clear them for the next build.
+__device__ __forceinline__ void edge_clear_counts(const Ctx& ctx) {
+    for (uint32_t b = ctx.tid; b <= ctx.d.edge_mask; b += ctx.nthreads) ctx.d.edge_count[b] = 0u;
+}
+
 // Phase 2: the pairs of the list whose pass spheres overlap (the
 // reference's sphere filter) are the candidates, each with a lower bound
 // (less the rounding slack) on every distance its solve could see; those
 // within the margin of contact are ordered.
-__device__ void edge_candidates(Ctx& ctx, bool swept) {
+__device__ void edge_candidates(Ctx& ctx, bool swept, bool rebuilt) {
     const DeviceCloth& d = ctx.d;
+    if (rebuilt) edge_clear_counts(ctx);
     const float target = 2.0f * ctx.c.radius;
     const float thr = (swept ? target + 1.0e-9f : target) + NC_EDGE_MARGIN * target;
     const uint32_t listed = min(__ldcg(d.edge_ctl + 5), d.edge_list_cap);
@@ -543,7 +657,11 @@ __device__ void edge_candidates(Ctx& ctx, bool swept) {
 }
 
 // Phase 3 (CTA 0): sort the ordered pairs, undo the previous round, then
-// resolve them one after another on thread 0.
+// resolve them in the reference's order as wavefronts: a pair's level is one
+// more than the last level of any of its four particles, so pairs of one
+// level share no particle and every pair runs after all earlier pairs it
+// shares a particle with, which is all the serial order requires.  The first
+// segment's box of the tree test is taken at its first pair.
 __device__ void edge_resolve(Ctx& ctx, bool swept, bool redo) {
     if (ctx.rank != 0) return;
     const DeviceCloth& d = ctx.d;
@@ -556,59 +674,102 @@ __device__ void edge_resolve(Ctx& ctx, bool swept, bool redo) {
         d.edge_sorted[rank] = key;
     }
     __syncthreads();
-    if (threadIdx.x != 0) return;
-    const float ex = 0.5f * (2.0f * ctx.c.radius);
-    if (redo) {
-        // back to the pass-start positions of every particle the last round moved
-        const uint32_t done = d.edge_ctl[4];
-        for (uint32_t r = 0; r < done; ++r) {
-            const uint2 sa = __ldg(d.y_ij + d.edge_new[r].i), sb = __ldg(d.y_ij + d.edge_new[r].j);
+    __shared__ uint32_t s_top;
+    if (threadIdx.x == 0) {
+        if (redo) {
+            // back to the pass-start positions of every particle the last round moved
+            const uint32_t done = d.edge_ctl[4];
+            for (uint32_t r = 0; r < done; ++r) {
+                const uint2 sa = __ldg(d.y_ij + d.edge_new[r].i), sb = __ldg(d.y_ij + d.edge_new[r].j);
+                const uint32_t id[4] = {sa.x, sa.y, sb.x, sb.y};
+                for (int e = 0; e < 4; ++e) {
+                    px_set(ctx, id[e], ld(d.edge_x0 + id[e]));
+                    d.edge_path[id[e]] = 0.0f;
+                }
+            }
+            d.edge_ctl[4] = 0u;
+        }
+        uint32_t top = 0;
+        for (uint32_t k = 0; k < count; ++k) {
+            const unsigned long long key = d.edge_sorted[k];
+            const uint32_t i = static_cast<uint32_t>(key >> 32);
+            const uint2 sa = __ldg(d.y_ij + i), sb = __ldg(d.y_ij + static_cast<uint32_t>(key));
             const uint32_t id[4] = {sa.x, sa.y, sb.x, sb.y};
+            uint32_t lv = 0;
+            for (int e = 0; e < 4; ++e) lv = max(lv, d.edge_level[id[e]]);
+            ++lv;
+            for (int e = 0; e < 4; ++e) d.edge_level[id[e]] = lv;
+            const bool first = k == 0u || static_cast<uint32_t>(d.edge_sorted[k - 1u] >> 32) != i;
+            d.edge_lv[k] = lv | (first ? 0x80000000u : 0u);
+            top = max(top, lv);
+        }
+        for (uint32_t k = 0; k < count; ++k) {   // leave the level marks zero for the next pass
+            const unsigned long long key = d.edge_sorted[k];
+            const uint2 sa = __ldg(d.y_ij + static_cast<uint32_t>(key >> 32)),
+                        sb = __ldg(d.y_ij + static_cast<uint32_t>(key));
+            d.edge_level[sa.x] = d.edge_level[sa.y] = d.edge_level[sb.x] = d.edge_level[sb.y] = 0u;
+        }
+        s_top = top;
+    }
+    __syncthreads();
+    const uint32_t top = s_top;
+    const float ex = 0.5f * (2.0f * ctx.c.radius);
+    for (uint32_t level = 1; level <= top; ++level) {
+        for (uint32_t k = threadIdx.x; k < count; k += blockDim.x) {
+            const uint32_t tagged = d.edge_lv[k];
+            if ((tagged & 0x3fffffffu) != level) continue;
+            const unsigned long long key = d.edge_sorted[k];
+            const uint32_t i = static_cast<uint32_t>(key >> 32), j = static_cast<uint32_t>(key);
+            const uint2 sa = __ldg(d.y_ij + i), sb = __ldg(d.y_ij + j);
+            EdgeQuad q;
+            q.id[0] = sa.x;
+            q.id[1] = sa.y;
+            q.id[2] = sb.x;
+            q.id[3] = sb.y;
             for (int e = 0; e < 4; ++e) {
-                px_set(ctx, id[e], ld(d.edge_x0 + id[e]));
-                d.edge_path[id[e]] = 0.0f;
+                q.x[e] = px(ctx, q.id[e]);
+                q.p[e] = xyz(ld(d.xp + q.id[e]));
+            }
+            // the reference's tree query: the first segment's box when its
+            // turn comes (before any of its own pairs), against the second
+            // segment's pass-start box
+            EdgeBox qi;
+            if (tagged & 0x80000000u) {
+                qi = edge_box(xyz(q.x[0]), xyz(q.x[1]), q.p[0], q.p[1], swept, ex);
+                float* qb = d.edge_qbox_raw + 6u * i;
+                qb[0] = qi.lo.x; qb[1] = qi.lo.y; qb[2] = qi.lo.z;
+                qb[3] = qi.hi.x; qb[4] = qi.hi.y; qb[5] = qi.hi.z;
+            } else {
+                const float* qb = d.edge_qbox_raw + 6u * i;   // written at a lower level
+                qi.lo = V3{qb[0], qb[1], qb[2]};
+                qi.hi = V3{qb[3], qb[4], qb[5]};
+            }
+            const EdgeBox bj =
+                edge_box(xyz(ld(d.edge_x0 + sb.x)), xyz(ld(d.edge_x0 + sb.y)), q.p[2], q.p[3], swept, ex);
+            EdgeRecord rec{};
+            rec.i = i;
+            rec.j = j;
+            bool moved = false;
+            if (boxes_overlap(bj, qi))
+                moved = swept ? edge_swept(q, ctx.c.radius, ctx.c.dt, rec) : edge_present(q, ctx.c.radius, ctx.c.dt, rec);
+            if (moved) {
+                for (int e = 0; e < 4; ++e) {
+                    const float4 before = px(ctx, q.id[e]);
+                    d.edge_path[q.id[e]] = d.edge_path[q.id[e]] + len3(xyz(q.x[e]) - xyz(before));
+                    px_set(ctx, q.id[e], q.x[e]);
+                }
+                d.edge_new[k] = rec;
+                d.edge_lv[k] = tagged | 0x40000000u;
             }
         }
-        d.edge_ctl[4] = 0u;
+        __syncthreads();
     }
-    uint32_t done = 0;
-    uint32_t first = 0xffffffffu;
-    EdgeBox qi{};
-    for (uint32_t k = 0; k < count; ++k) {
-        const unsigned long long key = d.edge_sorted[k];
-        const uint32_t i = static_cast<uint32_t>(key >> 32), j = static_cast<uint32_t>(key);
-        const uint2 sa = __ldg(d.y_ij + i), sb = __ldg(d.y_ij + j);
-        EdgeQuad q;
-        q.id[0] = sa.x;
-        q.id[1] = sa.y;
-        q.id[2] = sb.x;
-        q.id[3] = sb.y;
-        for (int e = 0; e < 4; ++e) {
-            q.x[e] = px(ctx, q.id[e]);
-            q.p[e] = xyz(ld(d.xp + q.id[e]));
-        }
-        // the reference's tree query: the first segment's box when its turn
-        // comes (before any of its own pairs), against the second segment's
-        // pass-start box
-        if (i != first) {
-            first = i;
-            qi = edge_box(xyz(q.x[0]), xyz(q.x[1]), q.p[0], q.p[1], swept, ex);
-        }
-        const EdgeBox bj = edge_box(xyz(ld(d.edge_x0 + sb.x)), xyz(ld(d.edge_x0 + sb.y)), q.p[2], q.p[3], swept, ex);
-        if (!boxes_overlap(bj, qi)) continue;
-        EdgeRecord rec{};
-        rec.i = i;
-        rec.j = j;
-        const bool moved = swept ? edge_swept(q, ctx.c.radius, ctx.c.dt, rec) : edge_present(q, ctx.c.radius, ctx.c.dt, rec);
-        if (!moved) continue;
-        for (int e = 0; e < 4; ++e) {
-            const float4 before = px(ctx, q.id[e]);
-            d.edge_path[q.id[e]] = d.edge_path[q.id[e]] + len3(xyz(q.x[e]) - xyz(before));
-            px_set(ctx, q.id[e], q.x[e]);
-        }
-        if (done < d.edge_cap) d.edge_new[done++] = rec;
+    if (threadIdx.x == 0) {   // the records of the pairs that moved, in key order
+        uint32_t done = 0;
+        for (uint32_t k = 0; k < count; ++k)
+            if (d.edge_lv[k] & 0x40000000u) d.edge_new[done++] = d.edge_new[k];
+        d.edge_ctl[4] = done;
     }
-    d.edge_ctl[4] = done;
 }
 
 // Phase 4: every candidate outside the ordered set must have stayed clear
@@ -686,8 +847,9 @@ __device__ void edge_commit(const Ctx& ctx) {
 // gave up.
 __device__ __forceinline__ bool edge_sweep(Ctx& ctx, bool swept) {
     const DeviceCloth& d = ctx.d;
-    if (!edge_prepare(ctx, swept)) return false;
-    edge_candidates(ctx, swept);
+    bool rebuilt = false;
+    if (!edge_prepare(ctx, swept, rebuilt)) return false;
+    edge_candidates(ctx, swept, rebuilt);
     NC_SYNC(ctx);
     uint32_t seen = __ldcg(d.edge_ctl + 2);
     for (uint32_t round = 0;; ++round) {
@@ -704,7 +866,6 @@ __device__ __forceinline__ bool edge_sweep(Ctx& ctx, bool swept) {
         }
     }
     edge_commit(ctx);
-    ++ctx.edge_pass;
     return true;
 }
 
@@ -714,8 +875,9 @@ __device__ __forceinline__ bool edge_sweep(Ctx& ctx, bool swept) {
 // filters (and is on the pair list), so the maximum over the listed pairs
 // whose present spheres overlap (and 0) is the reference's value.  Writes
 // this CTA's maximum to edge_red[rank].
-__device__ void edge_deepest(Ctx& ctx) {
+__device__ void edge_deepest(Ctx& ctx, bool rebuilt) {
     const DeviceCloth& d = ctx.d;
+    if (rebuilt) edge_clear_counts(ctx);
     const float target = 2.0f * ctx.c.radius;
     float pen = 0.0f;
     const uint32_t listed = min(__ldcg(d.edge_ctl + 5), d.edge_list_cap);
@@ -741,9 +903,9 @@ __device__ void edge_deepest(Ctx& ctx) {
 // Certificate measure: pass spheres (and the list, when due), then the
 // deepest pair.
 __device__ __forceinline__ bool edge_measure(Ctx& ctx) {
-    if (!edge_prepare(ctx, false)) return false;
-    edge_deepest(ctx);
-    ++ctx.edge_pass;
+    bool rebuilt = false;
+    if (!edge_prepare(ctx, false, rebuilt)) return false;
+    edge_deepest(ctx, rebuilt);
     return true;
 }
 

@@ -1453,7 +1453,7 @@ __device__ __forceinline__ bool substep(Ctx& ctx, bool last) {
         air_apply_advance(ctx, force, att);
         NC_SYNC(ctx);
     }
-    const bool prim = kEdge && s.primitive_self && d.edge_head != nullptr;
+    const bool prim = kEdge && s.primitive_self && d.edge_count != nullptr;
     if (prim && !edge_sweep(ctx, true)) return false;   // swept edge/edge (tools/cloth_bag.cpp:4921)
     if (s.swept_fruit_yarn && d.f_count > 0u) {
         uint32_t first = NC_MAX_BATCHES, last = 0;
@@ -1640,7 +1640,6 @@ __device__ __forceinline__ void run_frame(const DeviceCloth& src, const Schedule
         ctx.c = nc::load_cfg(d.cfg + s.cfg_offset + sub);
         ctx.epoch = epoch_base + sub;
         ctx.barriers = 0;
-        ctx.edge_pass = 0;
         if (d.tape != nullptr && ranks == 1u) {
             // adjoint tape: state at the start of the substep
             float4* slot = d.tape + static_cast<size_t>(sub) * d.tape_slots * d.n;

@@ -151,7 +151,6 @@ struct Ctx {
     uint32_t shift;           // log2 of the particles each CTA owns
     float4* xs;               // this CTA's positions in shared memory
     float4* vs;               // this CTA's velocities in shared memory
-    uint32_t edge_pass;       // edge/edge grid passes so far in this substep
 };
 
 __device__ __forceinline__ float4* resident_ptr(const Ctx& c, float4* local_base, uint32_t i) {

@@ -268,6 +268,10 @@ struct Run {
             numi_cloth_self_contacts(h, &r->selfContacts, &pen);
             numi_cloth_edge_contacts(h, r->edgeContacts);
             numi_cloth_release_masks(h, r->masks);
+            uint32_t passes[3] = {0, 0, 0};
+            numi_cloth_pass_counts(h, passes);
+            r->reconcileMax = passes[1];
+            r->certificateMax = passes[2];
             r->generation = generation;
         }
         numi_cloth_destroy(h);

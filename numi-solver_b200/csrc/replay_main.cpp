@@ -94,8 +94,9 @@ int main(int argc, char** argv) {
                 r.deterministic ? "true" : "false", r.failure, r.seconds);
     std::printf("strain_violation=%.9e ground_penetration=%.9e fruit_yarn_penetration=%.9e self_penetration=%.9e "
                 "self_contacts=%llu edge_edge_contacts=%llu self_friction_contacts=%llu released_mask=%u "
-                "mouth_candidate_mask=%u attachment_generation=%u\n",
+                "mouth_candidate_mask=%u attachment_generation=%u max_contact_reconciliation_passes=%u "
+                "max_primitive_certificate_passes=%u\n",
                 r.residuals[0], r.residuals[1], r.residuals[2], r.residuals[3], r.selfContacts, r.edgeContacts[0],
-                r.edgeContacts[1], r.masks[0], r.masks[1], r.generation);
+                r.edgeContacts[1], r.masks[0], r.masks[1], r.generation, r.reconcileMax, r.certificateMax);
     return r.failure == 0u ? 0 : 1;
 }

@@ -362,7 +362,8 @@ def replay(scenario: str, steps: int, substeps: int = 48, frame_dt: float = 1.0 
             "render_triangles": r.renderTriangles, "generation": r.generation,
             "residuals": list(r.residuals), "self_contacts": int(r.selfContacts),
             "edge_contacts": (int(r.edgeContacts[0]), int(r.edgeContacts[1])),
-            "masks": (int(r.masks[0]), int(r.masks[1])), "seconds": r.seconds}
+            "masks": (int(r.masks[0]), int(r.masks[1])), "reconcile_max": int(r.reconcileMax),
+            "certificate_max": int(r.certificateMax), "seconds": r.seconds}
 
 
 def _bag_handle_base(scenario: str):

@@ -290,5 +290,6 @@ class ReplayResult(ctypes.Structure):
         ("renderTriangles", ctypes.c_uint32), ("generation", ctypes.c_uint32),
         ("residuals", ctypes.c_double * 4),
         ("selfContacts", ctypes.c_ulonglong), ("edgeContacts", ctypes.c_ulonglong * 2),
-        ("masks", ctypes.c_uint32 * 2), ("seconds", ctypes.c_double),
+        ("masks", ctypes.c_uint32 * 2), ("reconcileMax", ctypes.c_uint32), ("certificateMax", ctypes.c_uint32),
+        ("seconds", ctypes.c_double),
     ]

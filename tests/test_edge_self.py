@@ -158,9 +158,9 @@ def test_gpu_bag_per_substep_fp64():
 @pytest.mark.gpu
 @pytest.mark.parametrize("cell", ["0.001", "10"])
 def test_gpu_bag_list_paths(cell):
-    """A tiny cell puts every cover sphere on the list; a huge one fills the
-    buckets so that most spill to it.  The pair list, and so the result, is
-    the same."""
+    """A tiny build cell makes every segment too long for the grid (all on
+    the long-segment list); a huge one puts every segment in one cell.  The
+    pair list, and so the result, is the same."""
     scene, cfg = _bag()
     s = _sched()
     g = _gpu(scene, cfg[:12], s, env={"NUMI_CLOTH_EDGE_CELL": cell})
