@@ -338,6 +338,7 @@ int prepare_edge_grid(numi_cloth* h, bool primitive, uint32_t substeps, float ra
         e.edge_order = h->buf.alloc<unsigned long long>(cap);
         e.edge_sorted = h->buf.alloc<unsigned long long>(cap);
         e.edge_new = h->buf.alloc<EdgeRecord>(cap);
+        e.edge_done = h->buf.alloc<uint32_t>(cap);
         e.edge_lv = h->buf.alloc<uint32_t>(cap);
         e.edge_level = h->buf.alloc<uint32_t>(d.n);
         e.edge_qbox_raw = h->buf.alloc<float>(6u * d.y_count);
@@ -347,7 +348,7 @@ int prepare_edge_grid(numi_cloth* h, bool primitive, uint32_t substeps, float ra
         e.edge_red = h->buf.alloc<double>(3u * ctas);
         if (!e.edge_count || !e.edge_offs || !e.edge_chunk_total || !e.edge_entries || !e.edge_giant ||
             !e.edge_pairs || !e.edge_xb || !e.edge_pb || !e.edge_built_radius || !e.edge_sph || !e.edge_x0 ||
-            !e.edge_path || !e.edge_cand || !e.edge_order || !e.edge_sorted || !e.edge_new || !e.edge_rec ||
+            !e.edge_path || !e.edge_cand || !e.edge_order || !e.edge_sorted || !e.edge_new || !e.edge_done || !e.edge_rec ||
             !e.edge_ctl || !e.edge_stats || !e.edge_red || !e.edge_lv || !e.edge_level || !e.edge_qbox_raw || !e.edge_bbox)
             return NUMI_CLOTH_ENOMEM;
         e.edge_mask = buckets - 1u;

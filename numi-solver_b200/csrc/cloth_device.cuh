@@ -186,7 +186,8 @@ struct DeviceCloth {
     uint4* edge_cand;             // [edge_cap]
     unsigned long long* edge_order;    // [edge_cap]
     unsigned long long* edge_sorted;   // [edge_cap]
-    EdgeRecord* edge_new;         // [edge_cap]
+    EdgeRecord* edge_new;         // [edge_cap] records of the pass's ordered pairs, by sorted index
+    uint32_t* edge_done;          // [edge_cap] sorted indices of the pairs that moved, ascending
     uint32_t* edge_lv;            // [edge_cap] wavefront level of each ordered pair (+ first / moved bits)
     uint32_t* edge_level;         // [n] last wavefront level of each particle (zero between passes)
     EdgeRecord* edge_rec;         // [edge_cap]

@@ -269,6 +269,18 @@ __device__ bool edge_present(EdgeQuad& q, float radius, float dt, EdgeRecord& re
     return true;
 }
 
+// A slot of an append counter: one atomic add for the lanes of a warp that
+// append together, each lane getting the next slot in lane order.
+__device__ __forceinline__ uint32_t warp_append(uint32_t* counter) {
+    const unsigned m = __activemask();
+    const uint32_t lane = threadIdx.x & 31u;
+    const int leader = __ffs(m) - 1;
+    uint32_t base = 0;
+    if (lane == static_cast<uint32_t>(leader)) base = atomicAdd(counter, static_cast<uint32_t>(__popc(m)));
+    base = __shfl_sync(m, base, leader);
+    return base + static_cast<uint32_t>(__popc(m & ((1u << lane) - 1u)));
+}
+
 __device__ __forceinline__ float edge_skin(const Ctx& ctx) { return NC_EDGE_SKIN * (2.0f * ctx.c.radius); }
 
 // Phase 1: snapshot the pass-start positions, clear the path lengths, write
@@ -490,13 +502,14 @@ __device__ void edge_build_scatter(Ctx& ctx, uint32_t* s_start) {
     }
 }
 
-// Rebuild, step 4: the pairs.  A segment visits its cells; an entry of a
-// later segment is a pair when the visited cell lies in that segment's
-// range and is the lowest cell of the two ranges' overlap, so that every
-// pair is met once.  Long segments: every held segment scans their list,
-// and they pair among themselves by index.  A pair is listed when it is
-// not local and its segments are within diameter + skin at the build's
-// positions or at its substep-start positions.
+// Rebuild, step 4: the pairs, one warp per segment.  The warp visits the
+// segment's cells and its lanes take the cell's entries side by side; an
+// entry of a later segment is a pair when the visited cell lies in that
+// segment's range and is the lowest cell of the two ranges' overlap, so
+// that every pair is met once.  Long segments: every held segment scans
+// their list, and they pair among themselves by index.  A pair is listed
+// when it is not local and its segments are within diameter + skin at the
+// build's positions or at its substep-start positions.
 __device__ void edge_build_pairs(Ctx& ctx, const uint32_t* s_start) {
     const DeviceCloth& d = ctx.d;
     const float target = 2.0f * ctx.c.radius;
@@ -505,51 +518,55 @@ __device__ void edge_build_pairs(Ctx& ctx, const uint32_t* s_start) {
     const float inv_cell = 1.0f / d.edge_cell;
     const uint32_t chunk = edge_chunk(ctx);
     const uint32_t giants = min(__ldcg(d.edge_ctl + 7), d.y_count);
+    const uint32_t lane = threadIdx.x & 31u;
     // the positions and entries are not written in this phase: the reads
     // may go through L1 after a grid barrier (a gpu-scope acquire), not
     // after the cluster barrier (cluster scope)
     const bool l1 = d.cluster_barrier == 0u;
-    auto rd = [l1](const float4* p) { return xyz(l1 ? __ldca(p) : __ldcg(p)); };
+    auto rd = [l1](const float4* p) { return l1 ? __ldca(p) : __ldcg(p); };
+    auto rdu = [l1](const uint32_t* p) { return l1 ? __ldca(p) : __ldcg(p); };
     auto keep = [&](uint32_t a, uint32_t b) {
         const uint2 sa = __ldg(d.y_ij + a), sb = __ldg(d.y_ij + b);
-        const bool near =
-            segment_distance(rd(d.edge_x0 + sa.x), rd(d.edge_x0 + sa.y), rd(d.edge_x0 + sb.x), rd(d.edge_x0 + sb.y)) <=
-                reach ||
-            segment_distance(rd(d.xp + sa.x), rd(d.xp + sa.y), rd(d.xp + sb.x), rd(d.xp + sb.y)) <= reach;
+        const bool near = segment_distance(xyz(rd(d.edge_x0 + sa.x)), xyz(rd(d.edge_x0 + sa.y)),
+                                           xyz(rd(d.edge_x0 + sb.x)), xyz(rd(d.edge_x0 + sb.y))) <= reach ||
+                          segment_distance(xyz(rd(d.xp + sa.x)), xyz(rd(d.xp + sa.y)), xyz(rd(d.xp + sb.x)),
+                                           xyz(rd(d.xp + sb.y))) <= reach;
         if (!near || edge_local(d, sa, sb)) return;
-        const uint32_t k = atomicAdd(d.edge_ctl + 5, 1u);
+        const uint32_t k = warp_append(d.edge_ctl + 5);
         if (k >= d.edge_list_cap) {
             fail(d, NUMI_CLOTH_FAILURE_RANGE);
             return;
         }
         d.edge_pairs[k] = make_uint2(a, b);
     };
-    auto rd4 = [l1](const float4* p) { return l1 ? __ldca(p) : __ldcg(p); };
-    for (Range r = item_range(ctx, d.y_count); r.i < r.end; r.i += r.stride) {
-        const uint32_t i = r.i;
+    // warps over the segments, as item_range spreads threads
+    const uint32_t warps = blockDim.x >> 5;
+    uint32_t i, end, stride;
+    if (ctx.resident) {
+        i = static_cast<uint32_t>(static_cast<unsigned long long>(d.y_count) * ctx.rank / ctx.ranks) +
+            (threadIdx.x >> 5);
+        end = static_cast<uint32_t>(static_cast<unsigned long long>(d.y_count) * (ctx.rank + 1u) / ctx.ranks);
+        stride = warps;
+    } else {
+        i = ctx.tid >> 5;
+        end = d.y_count;
+        stride = ctx.nthreads >> 5;
+    }
+    for (; i < end; i += stride) {   // warp-uniform from here on
         const uint2 ab = __ldg(d.y_ij + i);
         const EdgeCells c = edge_cells(xyz(ld(d.edge_x0 + ab.x)), xyz(ld(d.edge_x0 + ab.y)), xyz(ld(d.xp + ab.x)),
                                        xyz(ld(d.xp + ab.y)), h, inv_cell);
-        const float4 blo = rd4(d.edge_bbox + 2u * i), bhi = rd4(d.edge_bbox + 2u * i + 1u);
+        const float4 blo = rd(d.edge_bbox + 2u * i), bhi = rd(d.edge_bbox + 2u * i + 1u);
         if (c.span[0] != 0) {
             for (int z = 0; z < c.span[2]; ++z)
                 for (int y = 0; y < c.span[1]; ++y)
                     for (int x = 0; x < c.span[0]; ++x) {
                         const int cx = c.lo[0] + x, cy = c.lo[1] + y, cz = c.lo[2] + z;
                         const uint32_t b = cell_bucket(cx, cy, cz, d.edge_mask);
-                        const uint32_t start = s_start[b / chunk] + (l1 ? __ldca(d.edge_offs + b) : __ldcg(d.edge_offs + b));
-                        const uint32_t count = l1 ? __ldca(d.edge_count + b) : __ldcg(d.edge_count + b);
-                        for (uint32_t e0 = start; e0 < start + count; e0 += 8u) {
-                          uint4 ens[8];
-#pragma unroll
-                          for (uint32_t q = 0; q < 8u; ++q) {   // issue the group's loads together
-                              const uint32_t e = min(e0 + q, start + count - 1u);
-                              ens[q] = l1 ? __ldca(d.edge_entries + e) : __ldcg(d.edge_entries + e);
-                          }
-#pragma unroll
-                          for (uint32_t q = 0; q < 8u; ++q) {
-                            if (e0 + q >= start + count) break;
-                            const uint4 en = ens[q];
+                        const uint32_t start = s_start[b / chunk] + rdu(d.edge_offs + b);
+                        const uint32_t stop = start + rdu(d.edge_count + b);
+                        for (uint32_t e = start + lane; e < stop; e += 32u) {
+                            const uint4 en = l1 ? __ldca(d.edge_entries + e) : __ldcg(d.edge_entries + e);
                             if (en.x <= i) continue;
                             const unsigned long long key = static_cast<unsigned long long>(en.y) |
                                                            (static_cast<unsigned long long>(en.z) << 32);
@@ -562,16 +579,15 @@ __device__ void edge_build_pairs(Ctx& ctx, const uint32_t* s_start) {
                             if (cx < jx || cx >= jx + sx || cy < jy || cy >= jy + sy || cz < jz || cz >= jz + sz)
                                 continue;
                             if (cx != max(c.lo[0], jx) || cy != max(c.lo[1], jy) || cz != max(c.lo[2], jz)) continue;
-                            const float4 olo = rd4(d.edge_bbox + 2u * en.x), ohi = rd4(d.edge_bbox + 2u * en.x + 1u);
+                            const float4 olo = rd(d.edge_bbox + 2u * en.x), ohi = rd(d.edge_bbox + 2u * en.x + 1u);
                             if (olo.x > bhi.x || ohi.x < blo.x || olo.y > bhi.y || ohi.y < blo.y || olo.z > bhi.z ||
                                 ohi.z < blo.z)
                                 continue;   // the grown boxes do not meet: farther apart than diameter + skin
                             keep(i, en.x);
-                          }
                         }
                     }
         }
-        for (uint32_t g = 0; g < giants; ++g) {
+        for (uint32_t g = lane; g < giants; g += 32u) {
             const uint32_t j = __ldcg(d.edge_giant + g);
             if (j == i || (c.span[0] == 0 && j < i)) continue;
             keep(min(i, j), max(i, j));
@@ -645,14 +661,14 @@ __device__ void edge_candidates(Ctx& ctx, bool swept, bool rebuilt) {
         }
         // rounding of the distances, the paths and the solve's own distance
         bound = bound - (1.0e-6f + 1.0e-6f * big);
-        const uint32_t k = atomicAdd(d.edge_ctl + 0, 1u);
+        const uint32_t k = warp_append(d.edge_ctl + 0);
         if (k >= d.edge_cap) {
             fail(d, NUMI_CLOTH_FAILURE_RANGE);
             continue;
         }
         const bool ordered = !(bound >= thr);
         d.edge_cand[k] = make_uint4(a, b, __float_as_uint(bound), ordered ? 1u : 0u);
-        if (ordered) d.edge_order[atomicAdd(d.edge_ctl + 1, 1u)] = edge_key(a, b);
+        if (ordered) d.edge_order[warp_append(d.edge_ctl + 1)] = edge_key(a, b);
     }
 }
 
@@ -661,62 +677,127 @@ __device__ void edge_candidates(Ctx& ctx, bool swept, bool rebuilt) {
 // more than the last level of any of its four particles, so pairs of one
 // level share no particle and every pair runs after all earlier pairs it
 // shares a particle with, which is all the serial order requires.  The first
-// segment's box of the tree test is taken at its first pair.
+// segment's box of the tree test is taken at its first pair.  Up to
+// NC_EDGE_STAGED ordered pairs the sort and the levels run in shared memory
+// (each pair finds, in parallel, the last earlier pair of each of its
+// particles; one thread then chains the levels); more go through global
+// memory with a per-particle level array.
+#define NC_EDGE_STAGED 256u
 __device__ void edge_resolve(Ctx& ctx, bool swept, bool redo) {
     if (ctx.rank != 0) return;
     const DeviceCloth& d = ctx.d;
     const uint32_t count = min(__ldcg(d.edge_ctl + 1), d.edge_cap);
-    // rank sort: the keys are distinct
-    for (uint32_t k = threadIdx.x; k < count; k += blockDim.x) {
-        const unsigned long long key = __ldcg(d.edge_order + k);
-        uint32_t rank = 0;
-        for (uint32_t m = 0; m < count; ++m) rank += __ldcg(d.edge_order + m) < key ? 1u : 0u;
-        d.edge_sorted[rank] = key;
-    }
-    __syncthreads();
-    __shared__ uint32_t s_top;
-    if (threadIdx.x == 0) {
-        if (redo) {
-            // back to the pass-start positions of every particle the last round moved
-            const uint32_t done = d.edge_ctl[4];
-            for (uint32_t r = 0; r < done; ++r) {
-                const uint2 sa = __ldg(d.y_ij + d.edge_new[r].i), sb = __ldg(d.y_ij + d.edge_new[r].j);
-                const uint32_t id[4] = {sa.x, sa.y, sb.x, sb.y};
-                for (int e = 0; e < 4; ++e) {
-                    px_set(ctx, id[e], ld(d.edge_x0 + id[e]));
-                    d.edge_path[id[e]] = 0.0f;
-                }
-            }
-            d.edge_ctl[4] = 0u;
-        }
-        uint32_t top = 0;
-        for (uint32_t k = 0; k < count; ++k) {
-            const unsigned long long key = d.edge_sorted[k];
-            const uint32_t i = static_cast<uint32_t>(key >> 32);
-            const uint2 sa = __ldg(d.y_ij + i), sb = __ldg(d.y_ij + static_cast<uint32_t>(key));
+    const bool staged = count <= NC_EDGE_STAGED;
+    // the reduction scratch holds the staged arrays
+    static_assert(NC_EDGE_STAGED * (8u + 8u + 16u + 8u + 4u) <= sizeof(nc_red_smem), "staged arrays exceed the scratch");
+    unsigned char* scratch = reinterpret_cast<unsigned char*>(&nc_red_smem[0][0]);
+    unsigned long long* s_key = reinterpret_cast<unsigned long long*>(scratch);
+    unsigned long long* s_sorted = s_key + NC_EDGE_STAGED;
+    uint4* s_id = reinterpret_cast<uint4*>(s_sorted + NC_EDGE_STAGED);
+    uint2* s_pred = reinterpret_cast<uint2*>(s_id + NC_EDGE_STAGED);   // 16-bit pair indices, 0xffff: none
+    uint32_t* s_lv = reinterpret_cast<uint32_t*>(s_pred + NC_EDGE_STAGED);
+    if (redo) {
+        // back to the pass-start positions of every particle the last round
+        // moved (particles shared by records get the same values)
+        const uint32_t done = __ldcg(d.edge_ctl + 4);
+        for (uint32_t r = threadIdx.x; r < done; r += blockDim.x) {
+            const EdgeRecord& rec = d.edge_new[__ldcg(d.edge_done + r)];
+            const uint2 sa = __ldg(d.y_ij + rec.i), sb = __ldg(d.y_ij + rec.j);
             const uint32_t id[4] = {sa.x, sa.y, sb.x, sb.y};
-            uint32_t lv = 0;
-            for (int e = 0; e < 4; ++e) lv = max(lv, d.edge_level[id[e]]);
-            ++lv;
-            for (int e = 0; e < 4; ++e) d.edge_level[id[e]] = lv;
-            const bool first = k == 0u || static_cast<uint32_t>(d.edge_sorted[k - 1u] >> 32) != i;
-            d.edge_lv[k] = lv | (first ? 0x80000000u : 0u);
-            top = max(top, lv);
+            for (int e = 0; e < 4; ++e) {
+                px_set(ctx, id[e], ld(d.edge_x0 + id[e]));
+                d.edge_path[id[e]] = 0.0f;
+            }
         }
-        for (uint32_t k = 0; k < count; ++k) {   // leave the level marks zero for the next pass
-            const unsigned long long key = d.edge_sorted[k];
+    }
+    __shared__ uint32_t s_top;
+    if (staged) {
+        for (uint32_t k = threadIdx.x; k < count; k += blockDim.x) s_key[k] = __ldcg(d.edge_order + k);
+        __syncthreads();
+        // rank sort: the keys are distinct
+        for (uint32_t k = threadIdx.x; k < count; k += blockDim.x) {
+            const unsigned long long key = s_key[k];
+            uint32_t rank = 0;
+            for (uint32_t m = 0; m < count; ++m) rank += s_key[m] < key ? 1u : 0u;
+            s_sorted[rank] = key;
+            d.edge_sorted[rank] = key;
             const uint2 sa = __ldg(d.y_ij + static_cast<uint32_t>(key >> 32)),
                         sb = __ldg(d.y_ij + static_cast<uint32_t>(key));
-            d.edge_level[sa.x] = d.edge_level[sa.y] = d.edge_level[sb.x] = d.edge_level[sb.y] = 0u;
+            s_id[rank] = make_uint4(sa.x, sa.y, sb.x, sb.y);
         }
-        s_top = top;
+        __syncthreads();
+        // the last earlier pair of each particle
+        for (uint32_t k = threadIdx.x; k < count; k += blockDim.x) {
+            const uint4 me = s_id[k];
+            const uint32_t id[4] = {me.x, me.y, me.z, me.w};
+            uint32_t pred[4] = {0xffffu, 0xffffu, 0xffffu, 0xffffu};
+            uint32_t open = 4u;
+            for (uint32_t m = k; m-- > 0u && open > 0u;) {
+                const uint4 o = s_id[m];
+                for (int e = 0; e < 4; ++e)
+                    if (pred[e] == 0xffffu && (o.x == id[e] || o.y == id[e] || o.z == id[e] || o.w == id[e])) {
+                        pred[e] = m;
+                        --open;
+                    }
+            }
+            s_pred[k] = make_uint2(pred[0] | (pred[1] << 16), pred[2] | (pred[3] << 16));
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t top = 0;
+            for (uint32_t k = 0; k < count; ++k) {
+                const uint2 pr = s_pred[k];
+                const uint32_t pk[4] = {pr.x & 0xffffu, pr.x >> 16, pr.y & 0xffffu, pr.y >> 16};
+                uint32_t lv = 0;
+                for (int e = 0; e < 4; ++e)
+                    if (pk[e] != 0xffffu) lv = max(lv, s_lv[pk[e]] & 0x3fffffffu);
+                ++lv;
+                const bool first = k == 0u || (s_sorted[k - 1u] >> 32) != (s_sorted[k] >> 32);
+                s_lv[k] = lv | (first ? 0x80000000u : 0u);
+                top = max(top, lv);
+            }
+            s_top = top;
+        }
+    } else {
+        // rank sort: the keys are distinct
+        for (uint32_t k = threadIdx.x; k < count; k += blockDim.x) {
+            const unsigned long long key = __ldcg(d.edge_order + k);
+            uint32_t rank = 0;
+            for (uint32_t m = 0; m < count; ++m) rank += __ldcg(d.edge_order + m) < key ? 1u : 0u;
+            d.edge_sorted[rank] = key;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t top = 0;
+            for (uint32_t k = 0; k < count; ++k) {
+                const unsigned long long key = d.edge_sorted[k];
+                const uint32_t i = static_cast<uint32_t>(key >> 32);
+                const uint2 sa = __ldg(d.y_ij + i), sb = __ldg(d.y_ij + static_cast<uint32_t>(key));
+                const uint32_t id[4] = {sa.x, sa.y, sb.x, sb.y};
+                uint32_t lv = 0;
+                for (int e = 0; e < 4; ++e) lv = max(lv, d.edge_level[id[e]]);
+                ++lv;
+                for (int e = 0; e < 4; ++e) d.edge_level[id[e]] = lv;
+                const bool first = k == 0u || static_cast<uint32_t>(d.edge_sorted[k - 1u] >> 32) != i;
+                d.edge_lv[k] = lv | (first ? 0x80000000u : 0u);
+                top = max(top, lv);
+            }
+            for (uint32_t k = 0; k < count; ++k) {   // leave the level marks zero for the next pass
+                const unsigned long long key = d.edge_sorted[k];
+                const uint2 sa = __ldg(d.y_ij + static_cast<uint32_t>(key >> 32)),
+                            sb = __ldg(d.y_ij + static_cast<uint32_t>(key));
+                d.edge_level[sa.x] = d.edge_level[sa.y] = d.edge_level[sb.x] = d.edge_level[sb.y] = 0u;
+            }
+            s_top = top;
+        }
     }
     __syncthreads();
+    uint32_t* lvp = staged ? s_lv : d.edge_lv;
     const uint32_t top = s_top;
     const float ex = 0.5f * (2.0f * ctx.c.radius);
     for (uint32_t level = 1; level <= top; ++level) {
         for (uint32_t k = threadIdx.x; k < count; k += blockDim.x) {
-            const uint32_t tagged = d.edge_lv[k];
+            const uint32_t tagged = lvp[k];
             if ((tagged & 0x3fffffffu) != level) continue;
             const unsigned long long key = d.edge_sorted[k];
             const uint32_t i = static_cast<uint32_t>(key >> 32), j = static_cast<uint32_t>(key);
@@ -759,15 +840,15 @@ __device__ void edge_resolve(Ctx& ctx, bool swept, bool redo) {
                     px_set(ctx, q.id[e], q.x[e]);
                 }
                 d.edge_new[k] = rec;
-                d.edge_lv[k] = tagged | 0x40000000u;
+                lvp[k] = tagged | 0x40000000u;
             }
         }
         __syncthreads();
     }
-    if (threadIdx.x == 0) {   // the records of the pairs that moved, in key order
+    if (threadIdx.x == 0) {   // the pairs that moved, in key order
         uint32_t done = 0;
         for (uint32_t k = 0; k < count; ++k)
-            if (d.edge_lv[k] & 0x40000000u) d.edge_new[done++] = d.edge_new[k];
+            if (lvp[k] & 0x40000000u) d.edge_done[done++] = k;
         d.edge_ctl[4] = done;
     }
 }
@@ -804,7 +885,7 @@ __device__ void edge_commit(const Ctx& ctx) {
     auto key = [](const EdgeRecord& r) { return edge_key(r.i, r.j); };
     uint32_t inserts = 0;
     for (uint32_t k = 0, r = 0; k < fresh; ++k) {
-        const EdgeRecord& n = d.edge_new[k];
+        const EdgeRecord& n = d.edge_new[d.edge_done[k]];
         while (r < have && key(d.edge_rec[r]) < key(n)) ++r;
         if (r < have && key(d.edge_rec[r]) == key(n)) {
             EdgeRecord& o = d.edge_rec[r];
@@ -825,7 +906,7 @@ __device__ void edge_commit(const Ctx& ctx) {
     // new keys, merged in from the back
     int w = static_cast<int>(have + inserts) - 1, p = static_cast<int>(have) - 1;
     for (int k = static_cast<int>(fresh) - 1; k >= 0 && inserts > 0u; --k) {
-        const EdgeRecord& n = d.edge_new[k];
+        const EdgeRecord& n = d.edge_new[d.edge_done[k]];
         while (p >= 0 && key(d.edge_rec[p]) > key(n)) d.edge_rec[w--] = d.edge_rec[p--];
         if (p >= 0 && key(d.edge_rec[p]) == key(n)) continue;
         EdgeRecord o{};

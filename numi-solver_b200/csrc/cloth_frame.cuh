@@ -11,7 +11,7 @@ namespace {   // internal linkage: the edge kernels' unit includes these too
 // FP64 scratch of the CTA-wide reductions (air-load chunk sums, the air
 // attenuation, the residual maxima).  They run in different phases and each
 // ends with a CTA barrier, so they share one array.
-__shared__ double nc_red_smem[3][NC_BLOCK_MAX];
+__shared__ __align__(16) double nc_red_smem[3][NC_BLOCK_MAX];
 
 // Grid-wide barrier with a bounded wait.  Arrival is a release-add of 1 to
 // a counter the host zeroes before each launch; barrier number s of the
