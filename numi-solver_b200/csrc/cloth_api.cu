@@ -98,6 +98,10 @@ struct numi_cloth {
     uint32_t trace_capacity = 0;   // substeps the trace buffer holds
     uint32_t last_substeps = 0;
     float yarn_rest_median = 0.0f;   // median yarn segment rest length
+    bool neighbours = false;         // neighbour-sync tables built for the cooperative grid
+    // host copies for the edge/edge local lists, built with the edge buffers
+    std::vector<uint2> host_yarn;
+    std::vector<uint32_t> host_local_off, host_local_idx;
     Snapshot snaps[kSnapshotSlots];
     // dynamic state regions copied by snapshot/restore
     struct Region {
@@ -220,6 +224,106 @@ int make_batches(const Rec* recs, uint32_t count, uint32_t n_targets, ColourFn c
     return NUMI_CLOTH_OK;
 }
 
+// Neighbour syncs of the cooperative grid.  CTA r takes, in every colour
+// batch, the items whose lowest particle lies in its equal share
+// [r n / R, (r + 1) n / R) of the particle range; its neighbours are the
+// CTAs whose items share a particle with its own in any colour (reads
+// included: a bend's middle particle).  Built when every batch lists its
+// items in ascending lowest particle (a share is then one index range) and
+// no CTA has more than NC_NBR_MAX neighbours; otherwise every colour ends
+// with the grid barrier.
+bool prepare_neighbours(numi_cloth* h, const NumiClothScene* scene) {
+    DeviceCloth& d = h->d;
+    const uint32_t R = h->grid, n = d.n;
+    const uint32_t slots = d.n_dist_batches + d.n_knot_batches + d.n_bend_batches;
+    uint32_t want = 1;
+    env_u32("NUMI_CLOTH_NEIGHBOUR_SYNC", want);
+    if (want == 0u || R < 2u || h->cluster != 0u || d.resident != 0u || n == 0u || slots == 0u ||
+        slots > 3u * NC_MAX_BATCHES)
+        return false;
+    auto cta_of = [&](uint32_t p) { return static_cast<uint32_t>(static_cast<uint64_t>(p) * R / n); };
+    std::vector<uint2> range(static_cast<size_t>(R) * slots);
+    std::vector<std::vector<uint32_t>> touch(n);   // CTAs touching each particle
+    std::vector<uint32_t> cta;
+    auto batch = [&](uint32_t slot, const Batch& bt, auto parts) {
+        cta.assign(bt.count, 0u);
+        uint32_t prev = 0;
+        for (uint32_t k = 0; k < bt.count; ++k) {
+            uint32_t p[4];
+            const int np = parts(bt.first + k, p);
+            uint32_t lowest = p[0];
+            for (int e = 1; e < np; ++e) lowest = std::min(lowest, p[e]);
+            if (lowest < prev) return false;
+            prev = lowest;
+            cta[k] = cta_of(lowest);
+            for (int e = 0; e < np; ++e) {
+                std::vector<uint32_t>& t = touch[p[e]];
+                if (std::find(t.begin(), t.end(), cta[k]) == t.end()) t.push_back(cta[k]);
+            }
+        }
+        for (uint32_t r = 0, k = 0; r < R; ++r) {
+            const uint32_t start = k;
+            while (k < bt.count && cta[k] == r) ++k;
+            range[static_cast<size_t>(r) * slots + slot] = make_uint2(start, k);   // within the batch
+        }
+        return true;
+    };
+    bool ok = true;
+    for (uint32_t b = 0; ok && b < d.n_dist_batches; ++b)
+        ok = batch(b, d.dist_batches[b], [&](uint32_t i, uint32_t* p) {
+            p[0] = scene->distances[i].particlesAndColor.x;
+            p[1] = scene->distances[i].particlesAndColor.y;
+            return 2;
+        });
+    for (uint32_t b = 0; ok && b < d.n_knot_batches; ++b)
+        ok = batch(d.n_dist_batches + b, d.knot_batches[b], [&](uint32_t i, uint32_t* p) {
+            const NumiClothKnot& r = scene->knots[i];
+            p[0] = r.particles.x;
+            p[1] = r.particles.y;
+            p[2] = r.particles.z;
+            p[3] = r.particles.w;
+            return 4;
+        });
+    for (uint32_t b = 0; ok && b < d.n_bend_batches; ++b)
+        ok = batch(d.n_dist_batches + d.n_knot_batches + b, d.bend_batches[b], [&](uint32_t i, uint32_t* p) {
+            p[0] = scene->bends[i].particlesAndColor.x;
+            p[1] = scene->bends[i].particlesAndColor.y;
+            p[2] = scene->bends[i].particlesAndColor.z;
+            return 3;
+        });
+    if (!ok) return false;
+    std::vector<std::vector<uint32_t>> nbr(R);
+    for (const std::vector<uint32_t>& t : touch)
+        for (uint32_t c : t)
+            for (uint32_t o : t)
+                if (o != c && std::find(nbr[c].begin(), nbr[c].end(), o) == nbr[c].end()) {
+                    if (nbr[c].size() >= NC_NBR_MAX) return false;
+                    nbr[c].push_back(o);
+                }
+    std::vector<uint32_t> off(R + 1u, 0u), idx;
+    for (uint32_t r = 0; r < R; ++r) {
+        std::sort(nbr[r].begin(), nbr[r].end());
+        idx.insert(idx.end(), nbr[r].begin(), nbr[r].end());
+        off[r + 1u] = static_cast<uint32_t>(idx.size());
+    }
+    uint2* d_range = h->buf.alloc<uint2>(range.size());
+    uint32_t* d_off = h->buf.alloc<uint32_t>(off.size());
+    uint32_t* d_idx = h->buf.alloc<uint32_t>(std::max<size_t>(idx.size(), 1));
+    unsigned int* d_flag = h->buf.alloc<unsigned int>(R);
+    if (!d_range || !d_off || !d_idx || !d_flag) return false;
+    if (cudaMemcpy(d_range, range.data(), range.size() * sizeof(uint2), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(d_off, off.data(), off.size() * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess ||
+        (!idx.empty() &&
+         cudaMemcpy(d_idx, idx.data(), idx.size() * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess))
+        return false;
+    d.colour_slots = slots;
+    d.colour_range = d_range;
+    d.nbr_off = d_off;
+    d.nbr_idx = d_idx;
+    d.nbr_flag = d_flag;
+    return true;
+}
+
 cudaError_t launch(numi_cloth* h, uint32_t substeps, const Schedule& s, uint32_t cfg_offset = 0) {
     DeviceCloth d = h->d;
     d.cfg = h->d_cfg + cfg_offset;
@@ -252,6 +356,13 @@ cudaError_t launch(numi_cloth* h, uint32_t substeps, const Schedule& s, uint32_t
     } else if (h->grid == 1) {
         e = cudaLaunchKernel(frame_fn(edge), dim3(1), dim3(h->block), args, smem, h->stream);
     } else {
+        // neighbour syncs between colours (the kernel without the edge/edge
+        // phases; its flags start at zero in every launch)
+        if (h->neighbours && !edge) {
+            d.nbr_on = 1u;
+            e = cudaMemsetAsync(d.nbr_flag, 0, h->grid * sizeof(unsigned int), h->stream);
+            if (e != cudaSuccess) return e;
+        }
         e = cudaLaunchCooperativeKernel(frame_fn(edge), dim3(h->grid), dim3(h->block), args, smem, h->stream);
     }
     if (e == cudaSuccess) ++h->launches;
@@ -311,6 +422,75 @@ int prepare_self_grid(numi_cloth* h, bool self_collision, uint32_t substeps) {
 // listed pairs and 16 candidate pairs per segment.  The build cell is a
 // median yarn segment plus the yarn diameter and skin (three diameters), so
 // that a typical segment's grown box spans at most two cells a side.
+// Every yarn segment's local segments of higher index, ascending: the pairs
+// the edge/edge family skips (edgePairLocal, tools/cloth_bag.cpp:2740-2749:
+// some endpoint of one is local to some endpoint of the other, by the 2-hop
+// topology list or, on a row-major grid cloth, the 5 x 5 block).
+bool build_local_lists(const numi_cloth* h, std::vector<uint32_t>& off, std::vector<uint32_t>& idx) {
+    const DeviceCloth& d = h->d;
+    const std::vector<uint2>& y = h->host_yarn;
+    const bool csr = !h->host_local_off.empty();
+    auto local = [&](uint32_t a, uint32_t b) {
+        if (csr) {
+            const uint32_t* lo = h->host_local_idx.data() + h->host_local_off[a];
+            const uint32_t* hi = h->host_local_idx.data() + h->host_local_off[a + 1u];
+            return std::binary_search(lo, hi, b);
+        }
+        if (d.grid_width == 0u) return a == b;
+        const int ra = static_cast<int>(a / d.grid_width), ca = static_cast<int>(a % d.grid_width);
+        const int rb = static_cast<int>(b / d.grid_width), cb = static_cast<int>(b % d.grid_width);
+        return std::abs(ra - rb) <= 2 && std::abs(ca - cb) <= 2;
+    };
+    // segments at each particle
+    std::vector<uint32_t> at_off(d.n + 1u, 0u), at(2u * y.size());
+    for (const uint2& s : y) {
+        ++at_off[s.x + 1u];
+        ++at_off[s.y + 1u];
+    }
+    for (uint32_t p = 0; p < d.n; ++p) at_off[p + 1u] += at_off[p];
+    std::vector<uint32_t> fill(at_off.begin(), at_off.end() - 1);
+    for (uint32_t k = 0; k < y.size(); ++k) {
+        at[fill[y[k].x]++] = k;
+        at[fill[y[k].y]++] = k;
+    }
+    // the particles an endpoint can be local to
+    std::vector<uint32_t> near;
+    auto gather = [&](uint32_t a) {
+        near.push_back(a);
+        if (csr) {
+            near.insert(near.end(), h->host_local_idx.begin() + h->host_local_off[a],
+                        h->host_local_idx.begin() + h->host_local_off[a + 1u]);
+        } else if (d.grid_width != 0u) {
+            const int w = static_cast<int>(d.grid_width), rows = static_cast<int>((d.n + d.grid_width - 1u) / d.grid_width);
+            const int ra = static_cast<int>(a / d.grid_width), ca = static_cast<int>(a % d.grid_width);
+            for (int r = std::max(ra - 2, 0); r <= std::min(ra + 2, rows - 1); ++r)
+                for (int c = std::max(ca - 2, 0); c <= std::min(ca + 2, w - 1); ++c) {
+                    const uint32_t q = static_cast<uint32_t>(r * w + c);
+                    if (q < d.n) near.push_back(q);
+                }
+        }
+    };
+    off.assign(y.size() + 1u, 0u);
+    idx.clear();
+    std::vector<uint32_t> cand;
+    for (uint32_t i = 0; i < y.size(); ++i) {
+        near.clear();
+        gather(y[i].x);
+        gather(y[i].y);
+        cand.clear();
+        for (uint32_t q : near)
+            for (uint32_t k = at_off[q]; k < at_off[q + 1u]; ++k)
+                if (at[k] > i) cand.push_back(at[k]);
+        std::sort(cand.begin(), cand.end());
+        cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+        for (uint32_t j : cand)
+            if (local(y[i].x, y[j].x) || local(y[i].x, y[j].y) || local(y[i].y, y[j].x) || local(y[i].y, y[j].y))
+                idx.push_back(j);
+        off[i + 1u] = static_cast<uint32_t>(idx.size());
+    }
+    return true;
+}
+
 int prepare_edge_grid(numi_cloth* h, bool primitive, uint32_t substeps, float radius) {
     (void)substeps;
     DeviceCloth& d = h->d;
@@ -327,6 +507,18 @@ int prepare_edge_grid(numi_cloth* h, bool primitive, uint32_t substeps, float ra
         e.edge_entries = h->buf.alloc<uint4>(static_cast<size_t>(27u) * d.y_count);
         e.edge_giant = h->buf.alloc<uint32_t>(d.y_count);
         e.edge_bbox = h->buf.alloc<float4>(2u * d.y_count);
+        std::vector<uint32_t> loc_off, loc_idx;
+        build_local_lists(h, loc_off, loc_idx);
+        uint32_t* d_loc_off = h->buf.alloc<uint32_t>(loc_off.size());
+        uint32_t* d_loc_idx = h->buf.alloc<uint32_t>(std::max<size_t>(loc_idx.size(), 1));
+        if (d_loc_off != nullptr && d_loc_idx != nullptr &&
+            (cudaMemcpy(d_loc_off, loc_off.data(), loc_off.size() * sizeof(uint32_t), cudaMemcpyHostToDevice) !=
+                 cudaSuccess ||
+             (!loc_idx.empty() && cudaMemcpy(d_loc_idx, loc_idx.data(), loc_idx.size() * sizeof(uint32_t),
+                                             cudaMemcpyHostToDevice) != cudaSuccess)))
+            d_loc_off = nullptr;
+        e.edge_loc_off = d_loc_off;
+        e.edge_loc_idx = d_loc_idx;
         e.edge_pairs = h->buf.alloc<uint2>(list_cap);
         e.edge_xb = h->buf.alloc<float4>(d.n);
         e.edge_pb = h->buf.alloc<float4>(d.n);
@@ -349,7 +541,8 @@ int prepare_edge_grid(numi_cloth* h, bool primitive, uint32_t substeps, float ra
         if (!e.edge_count || !e.edge_offs || !e.edge_chunk_total || !e.edge_entries || !e.edge_giant ||
             !e.edge_pairs || !e.edge_xb || !e.edge_pb || !e.edge_built_radius || !e.edge_sph || !e.edge_x0 ||
             !e.edge_path || !e.edge_cand || !e.edge_order || !e.edge_sorted || !e.edge_new || !e.edge_done || !e.edge_rec ||
-            !e.edge_ctl || !e.edge_stats || !e.edge_red || !e.edge_lv || !e.edge_level || !e.edge_qbox_raw || !e.edge_bbox)
+            !e.edge_ctl || !e.edge_stats || !e.edge_red || !e.edge_lv || !e.edge_level || !e.edge_qbox_raw || !e.edge_bbox ||
+            !e.edge_loc_off || !e.edge_loc_idx)
             return NUMI_CLOTH_ENOMEM;
         e.edge_mask = buckets - 1u;
         e.edge_cap = cap;
@@ -697,6 +890,7 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
         d.y_ij = y_ij;
         d.y_count = static_cast<uint32_t>(hy.size());
         up(y_ij, hy.data(), hy.size() * sizeof(uint2));
+        h->host_yarn = hy;
     }
     up(d_mat, hdm.data(), D * sizeof(float4));
     up(d.d_lambda, hdl.data(), D * sizeof(float));
@@ -722,6 +916,8 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
         }
         up(off, scene->localOffsets, (n + 1u) * sizeof(uint32_t));
         up(idx, scene->localIndices, entries * sizeof(uint32_t));
+        h->host_local_off.assign(scene->localOffsets, scene->localOffsets + n + 1u);
+        h->host_local_idx.assign(scene->localIndices, scene->localIndices + entries);
         d.local_off = off;
         d.local_idx = idx;
     }
@@ -729,6 +925,7 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
         delete h;
         return NUMI_CLOTH_ECUDA;
     }
+    h->neighbours = prepare_neighbours(h, scene);
     h->dynamic = {{d.x, n * sizeof(float4)},
                   {d.xp, n * sizeof(float4)},
                   {d.v, n * sizeof(float4)},

@@ -124,6 +124,19 @@ struct DeviceCloth {
     // 1: the grid is one thread-block cluster and phases are separated by
     // the hardware cluster barrier instead of the global-memory barrier
     uint32_t cluster_barrier;
+    // Neighbour syncs between constraint colours (cooperative grid, particles
+    // in global memory): CTA r solves items [start, end) of colour batch b,
+    // colour_range[r * colour_slots + b], an equal share of the particle
+    // index range in every colour, and between two colours waits only for
+    // the CTAs whose items share a particle with its own in any colour
+    // (nbr_idx[nbr_off[r] .. nbr_off[r + 1]]).  nbr_flag[r] counts the
+    // colours CTA r has finished in the launch (zeroed before every launch).
+    uint32_t nbr_on;
+    uint32_t colour_slots;         // distance + knot + bend batches
+    const uint2* colour_range;     // [grid * colour_slots]
+    const uint32_t* nbr_off;       // [grid + 1]
+    const uint32_t* nbr_idx;
+    unsigned int* nbr_flag;        // [grid]
     // resident mode: 1 when particle positions and velocities live in the
     // (distributed) shared memory of the grid's CTAs for the whole launch;
     // CTA r owns particles [r << resident_shift, (r + 1) << resident_shift)
@@ -175,6 +188,8 @@ struct DeviceCloth {
     uint4* edge_entries;          // [27 * y_count]
     uint32_t* edge_giant;         // [y_count] segments the grid does not hold
     float4* edge_bbox;            // [2 * y_count] grown boxes of the build
+    const uint32_t* edge_loc_off; // [y_count + 1] CSR of every segment's local segments of higher index
+    const uint32_t* edge_loc_idx; //   (ascending)
     uint2* edge_pairs;            // [edge_list_cap]
     float4* edge_xb;              // [n] positions at the build
     float4* edge_pb;              // [n] substep-start positions at the build

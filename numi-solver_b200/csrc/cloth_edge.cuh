@@ -152,9 +152,19 @@ __device__ __forceinline__ bool spheres_overlap(float4 a, float4 b) {
     return lsq(xyz(a) - xyz(b)) <= r * r;
 }
 
-// edgePairLocal (tools/cloth_bag.cpp:2740-2749).
-__device__ __forceinline__ bool edge_local(const DeviceCloth& d, uint2 a, uint2 b) {
-    return local_pair(d, a.x, b.x) || local_pair(d, a.x, b.y) || local_pair(d, a.y, b.x) || local_pair(d, a.y, b.y);
+// Segments a < b local to each other (edgePairLocal,
+// tools/cloth_bag.cpp:2740-2749: any endpoint pair is local): b on a's list
+// of local segments of higher index (ascending), built on the host.
+__device__ __forceinline__ bool seg_local(const DeviceCloth& d, uint32_t a, uint32_t b) {
+    uint32_t lo = __ldg(d.edge_loc_off + a), hi = __ldg(d.edge_loc_off + a + 1u);
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        const uint32_t v = __ldg(d.edge_loc_idx + mid);
+        if (v == b) return true;
+        if (v < b) lo = mid + 1u;
+        else hi = mid;
+    }
+    return false;
 }
 
 __device__ __forceinline__ unsigned long long edge_key(uint32_t i, uint32_t j) {
@@ -508,8 +518,9 @@ __device__ void edge_build_scatter(Ctx& ctx, uint32_t* s_start) {
 // segment's range and is the lowest cell of the two ranges' overlap, so
 // that every pair is met once.  Long segments: every held segment scans
 // their list, and they pair among themselves by index.  A pair is listed
-// when it is not local and its segments are within diameter + skin at the
-// build's positions or at its substep-start positions.
+// when it is not local (the segment's local list, held in the warp's
+// registers) and its segments are within diameter + skin at the build's
+// positions or at its substep-start positions.
 __device__ void edge_build_pairs(Ctx& ctx, const uint32_t* s_start) {
     const DeviceCloth& d = ctx.d;
     const float target = 2.0f * ctx.c.radius;
@@ -525,13 +536,13 @@ __device__ void edge_build_pairs(Ctx& ctx, const uint32_t* s_start) {
     const bool l1 = d.cluster_barrier == 0u;
     auto rd = [l1](const float4* p) { return l1 ? __ldca(p) : __ldcg(p); };
     auto rdu = [l1](const uint32_t* p) { return l1 ? __ldca(p) : __ldcg(p); };
-    auto keep = [&](uint32_t a, uint32_t b) {
+    auto keep_far = [&](uint32_t a, uint32_t b) {   // a non-local pair: the distance test
         const uint2 sa = __ldg(d.y_ij + a), sb = __ldg(d.y_ij + b);
         const bool near = segment_distance(xyz(rd(d.edge_x0 + sa.x)), xyz(rd(d.edge_x0 + sa.y)),
                                            xyz(rd(d.edge_x0 + sb.x)), xyz(rd(d.edge_x0 + sb.y))) <= reach ||
                           segment_distance(xyz(rd(d.xp + sa.x)), xyz(rd(d.xp + sa.y)), xyz(rd(d.xp + sb.x)),
                                            xyz(rd(d.xp + sb.y))) <= reach;
-        if (!near || edge_local(d, sa, sb)) return;
+        if (!near) return;
         const uint32_t k = warp_append(d.edge_ctl + 5);
         if (k >= d.edge_list_cap) {
             fail(d, NUMI_CLOTH_FAILURE_RANGE);
@@ -557,6 +568,10 @@ __device__ void edge_build_pairs(Ctx& ctx, const uint32_t* s_start) {
         const EdgeCells c = edge_cells(xyz(ld(d.edge_x0 + ab.x)), xyz(ld(d.edge_x0 + ab.y)), xyz(ld(d.xp + ab.x)),
                                        xyz(ld(d.xp + ab.y)), h, inv_cell);
         const float4 blo = rd(d.edge_bbox + 2u * i), bhi = rd(d.edge_bbox + 2u * i + 1u);
+        // the segment's local list: up to 64 entries in two registers per lane
+        const uint32_t llo = __ldg(d.edge_loc_off + i), llen = __ldg(d.edge_loc_off + i + 1u) - llo;
+        const uint32_t la = lane < llen ? __ldg(d.edge_loc_idx + llo + lane) : 0xffffffffu;
+        const uint32_t lb = lane + 32u < llen ? __ldg(d.edge_loc_idx + llo + 32u + lane) : 0xffffffffu;
         if (c.span[0] != 0) {
             for (int z = 0; z < c.span[2]; ++z)
                 for (int y = 0; y < c.span[1]; ++y)
@@ -565,32 +580,50 @@ __device__ void edge_build_pairs(Ctx& ctx, const uint32_t* s_start) {
                         const uint32_t b = cell_bucket(cx, cy, cz, d.edge_mask);
                         const uint32_t start = s_start[b / chunk] + rdu(d.edge_offs + b);
                         const uint32_t stop = start + rdu(d.edge_count + b);
-                        for (uint32_t e = start + lane; e < stop; e += 32u) {
-                            const uint4 en = l1 ? __ldca(d.edge_entries + e) : __ldcg(d.edge_entries + e);
-                            if (en.x <= i) continue;
-                            const unsigned long long key = static_cast<unsigned long long>(en.y) |
-                                                           (static_cast<unsigned long long>(en.z) << 32);
-                            const int jx = static_cast<int>(key & 0x1fffffull) - (1 << 20);
-                            const int jy = static_cast<int>((key >> 21) & 0x1fffffull) - (1 << 20);
-                            const int jz = static_cast<int>((key >> 42) & 0x1fffffull) - (1 << 20);
-                            const int sx = static_cast<int>(en.w & 3u) + 1, sy = static_cast<int>((en.w >> 2) & 3u) + 1,
-                                      sz = static_cast<int>((en.w >> 4) & 3u) + 1;
-                            // the visited cell in the other range, and the lowest common cell
-                            if (cx < jx || cx >= jx + sx || cy < jy || cy >= jy + sy || cz < jz || cz >= jz + sz)
-                                continue;
-                            if (cx != max(c.lo[0], jx) || cy != max(c.lo[1], jy) || cz != max(c.lo[2], jz)) continue;
-                            const float4 olo = rd(d.edge_bbox + 2u * en.x), ohi = rd(d.edge_bbox + 2u * en.x + 1u);
-                            if (olo.x > bhi.x || ohi.x < blo.x || olo.y > bhi.y || ohi.y < blo.y || olo.z > bhi.z ||
-                                ohi.z < blo.z)
-                                continue;   // the grown boxes do not meet: farther apart than diameter + skin
-                            keep(i, en.x);
+                        for (uint32_t base = start; base < stop; base += 32u) {
+                            const uint32_t e = base + lane;
+                            bool cand = e < stop;
+                            uint32_t j = 0;
+                            if (cand) {
+                                const uint4 en = l1 ? __ldca(d.edge_entries + e) : __ldcg(d.edge_entries + e);
+                                j = en.x;
+                                const unsigned long long key = static_cast<unsigned long long>(en.y) |
+                                                               (static_cast<unsigned long long>(en.z) << 32);
+                                const int jx = static_cast<int>(key & 0x1fffffull) - (1 << 20);
+                                const int jy = static_cast<int>((key >> 21) & 0x1fffffull) - (1 << 20);
+                                const int jz = static_cast<int>((key >> 42) & 0x1fffffull) - (1 << 20);
+                                const int sx = static_cast<int>(en.w & 3u) + 1,
+                                          sy = static_cast<int>((en.w >> 2) & 3u) + 1,
+                                          sz = static_cast<int>((en.w >> 4) & 3u) + 1;
+                                // a later segment; the visited cell in its range and the
+                                // lowest common cell
+                                cand = j > i && cx >= jx && cx < jx + sx && cy >= jy && cy < jy + sy && cz >= jz &&
+                                       cz < jz + sz && cx == max(c.lo[0], jx) && cy == max(c.lo[1], jy) &&
+                                       cz == max(c.lo[2], jz);
+                                if (cand) {   // the grown boxes meet: not farther apart than diameter + skin
+                                    const float4 olo = rd(d.edge_bbox + 2u * j), ohi = rd(d.edge_bbox + 2u * j + 1u);
+                                    cand = !(olo.x > bhi.x || ohi.x < blo.x || olo.y > bhi.y || ohi.y < blo.y ||
+                                             olo.z > bhi.z || ohi.z < blo.z);
+                                }
+                            }
+                            if (!__any_sync(0xffffffffu, cand)) continue;
+                            bool local = false;
+                            if (llen > 64u) {
+                                local = cand && seg_local(d, i, j);
+                            } else {
+                                for (uint32_t t = 0; t < min(llen, 32u); ++t)
+                                    local |= __shfl_sync(0xffffffffu, la, t) == j;
+                                for (uint32_t t = 32u; t < llen; ++t)
+                                    local |= __shfl_sync(0xffffffffu, lb, t - 32u) == j;
+                            }
+                            if (cand && !local) keep_far(i, j);
                         }
                     }
         }
         for (uint32_t g = lane; g < giants; g += 32u) {
             const uint32_t j = __ldcg(d.edge_giant + g);
             if (j == i || (c.span[0] == 0 && j < i)) continue;
-            keep(min(i, j), max(i, j));
+            if (!seg_local(d, min(i, j), max(i, j))) keep_far(min(i, j), max(i, j));
         }
     }
 }

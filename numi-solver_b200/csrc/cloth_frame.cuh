@@ -84,6 +84,76 @@ __device__ bool grid_sync(Ctx& ctx) {
 #define NC_SYNC(ctx) \
     do { if (!grid_sync(ctx)) return false; } while (0)
 
+// This CTA's item ranges of the colour batches and its neighbour CTAs,
+// staged at the start of a launch that runs neighbour syncs.
+#define NC_NBR_MAX 64u
+__shared__ uint2 nc_colour_range[3u * NC_MAX_BATCHES];
+__shared__ uint32_t nc_nbr[NC_NBR_MAX];
+__shared__ uint32_t nc_nbr_count;
+
+__device__ __forceinline__ void neighbour_stage(const Ctx& ctx) {
+    const DeviceCloth& d = ctx.d;
+    if (!d.nbr_on) return;
+    for (uint32_t b = threadIdx.x; b < d.colour_slots; b += blockDim.x)
+        nc_colour_range[b] = d.colour_range[static_cast<size_t>(ctx.rank) * d.colour_slots + b];
+    const uint32_t lo = d.nbr_off[ctx.rank], hi = d.nbr_off[ctx.rank + 1u];
+    for (uint32_t k = threadIdx.x; k < hi - lo; k += blockDim.x) nc_nbr[k] = d.nbr_idx[lo + k];
+    if (threadIdx.x == 0) nc_nbr_count = hi - lo;
+    __syncthreads();
+}
+
+// Items of colour batch `slot` (count items) that this thread solves: the
+// CTA's share when neighbour syncs run, else the grid-stride range.
+__device__ __forceinline__ Range colour_items(const Ctx& ctx, uint32_t slot, uint32_t count) {
+    if (ctx.d.nbr_on) {
+        const uint2 r = nc_colour_range[slot];
+        return Range{r.x + threadIdx.x, min(r.y, count), blockDim.x};
+    }
+    return item_range(ctx, count);
+}
+
+// Barrier between two constraint colours.  With neighbour syncs the CTA
+// publishes the colours it has finished (a release store after the CTA
+// barrier) and waits until each neighbour has finished as many (acquire):
+// every CTA that touches one of its particles in any colour is then done
+// with the previous colour, and none can be more than one colour ahead, so
+// the colour order of every particle is the grid barrier's.  Bounded as the
+// grid barrier.
+__device__ bool colour_sync(Ctx& ctx) {
+    const DeviceCloth& d = ctx.d;
+    if (!d.nbr_on) return grid_sync(ctx);
+    ++ctx.barriers;
+    const unsigned target = ++ctx.nseq;
+    __syncthreads();
+    if (threadIdx.x == 0) st_release(d.nbr_flag + ctx.rank, target);
+    int ab = 0;
+    if (threadIdx.x < nc_nbr_count) {
+        const unsigned* f = d.nbr_flag + nc_nbr[threadIdx.x];
+        unsigned spins = 0u;
+        while (ld_relaxed(f) < target) {
+            ++spins;
+            if ((spins & 63u) == 0u && ld_acquire(d.abort_flag) != 0u) {
+                ab = 1;
+                break;
+            }
+            if (spins > NC_BARRIER_SPIN_LIMIT) {
+                atomicOr(d.failure, NUMI_CLOTH_FAILURE_TIMEOUT);
+                atomicExch(d.abort_flag, 1u);
+                ab = 1;
+                break;
+            }
+        }
+        if (!ab) (void)ld_acquire(f);
+    }
+    const int any = __syncthreads_or(ab);
+    if (d.trace && ctx.rank == 0 && threadIdx.x == 0 && ctx.barriers <= NC_TRACE_SLOTS)
+        d.trace[static_cast<size_t>(ctx.sub) * NC_TRACE_SLOTS + ctx.barriers - 1u] = globaltimer();
+    return any == 0;
+}
+
+#define NC_CSYNC(ctx, colour_next) \
+    do { if (!((colour_next) ? colour_sync(ctx) : grid_sync(ctx))) return false; } while (0)
+
 // Apply (and clear) the fixed-point fruit displacement sums.  Fruit CTA.
 __device__ void fruit_flush(Ctx& ctx) {
     if (!ctx.fruit_pending) return;
@@ -950,9 +1020,12 @@ __device__ bool strain_sweeps(Ctx& ctx) {
                 const Batch bt = d.dist_batches[b];
                 if (bt.limited == 0u) continue;
                 fruit_flush(ctx);
-                for (Range r = item_range(ctx, bt.limited); r.i < r.end; r.i += r.stride)
+                for (Range r = colour_items(ctx, b, bt.limited); r.i < r.end; r.i += r.stride)
                     limit_strain(ctx, bt.first + r.i);
-                NC_SYNC(ctx);
+                // a colour follows: a later limited batch, or the next sweep
+                bool more = sw + 1u < ctx.s.strain_sweeps;
+                for (uint32_t c = b + 1u; c < d.n_dist_batches && !more; ++c) more = d.dist_batches[c].limited != 0u;
+                NC_CSYNC(ctx, more);
             }
         }
     }
@@ -1478,18 +1551,29 @@ __device__ __forceinline__ bool substep(Ctx& ctx, bool last) {
                 NC_SYNC(ctx);
             }
         } else {
+            // a colour follows while batches of this sweep remain
+            const bool bends_follow = (it & 1u) == 0u && d.n_bend_batches > 0u;
             for (uint32_t b = 0; b < d.n_dist_batches; ++b) {
                 const Batch bt = d.dist_batches[b];
                 fruit_flush(ctx);
-                for (Range r = item_range(ctx, bt.count); r.i < r.end; r.i += r.stride)
+                for (Range r = colour_items(ctx, b, bt.count); r.i < r.end; r.i += r.stride)
                     solve_distance(ctx, bt.first + r.i, dt2);
-                NC_SYNC(ctx);
+                NC_CSYNC(ctx, b + 1u < d.n_dist_batches || d.n_knot_batches > 0u || bends_follow);
+            }
+            for (uint32_t b = 0; b < d.n_knot_batches; ++b) {
+                const Batch bt = d.knot_batches[b];
+                for (Range r = colour_items(ctx, d.n_dist_batches + b, bt.count); r.i < r.end; r.i += r.stride)
+                    solve_knot(ctx, bt.first + r.i, dt2);
+                NC_CSYNC(ctx, b + 1u < d.n_knot_batches || bends_follow);
             }
         }
-        for (uint32_t b = 0; b < d.n_knot_batches; ++b) {
-            const Batch bt = d.knot_batches[b];
-            for (Range r = item_range(ctx, bt.count); r.i < r.end; r.i += r.stride) solve_knot(ctx, bt.first + r.i, dt2);
-            NC_SYNC(ctx);
+        if constexpr (kIlp) {
+            for (uint32_t b = 0; b < d.n_knot_batches; ++b) {
+                const Batch bt = d.knot_batches[b];
+                for (Range r = item_range(ctx, bt.count); r.i < r.end; r.i += r.stride)
+                    solve_knot(ctx, bt.first + r.i, dt2);
+                NC_SYNC(ctx);
+            }
         }
         if ((it & 1u) == 0u) {
             if constexpr (kIlp) {
@@ -1499,11 +1583,12 @@ __device__ __forceinline__ bool substep(Ctx& ctx, bool last) {
                     NC_SYNC(ctx);
                 }
             } else {
+                const uint32_t slot0 = d.n_dist_batches + d.n_knot_batches;
                 for (uint32_t b = 0; b < d.n_bend_batches; ++b) {
                     const Batch bt = d.bend_batches[b];
-                    for (Range r = item_range(ctx, bt.count); r.i < r.end; r.i += r.stride)
+                    for (Range r = colour_items(ctx, slot0 + b, bt.count); r.i < r.end; r.i += r.stride)
                         solve_bend(ctx, bt.first + r.i, dt2, ctx.c.radius, ctx.c.ground);
-                    NC_SYNC(ctx);
+                    NC_CSYNC(ctx, b + 1u < d.n_bend_batches);
                 }
             }
         }
@@ -1608,6 +1693,7 @@ __device__ __forceinline__ void run_frame(const DeviceCloth& src, const Schedule
     ctx.grip_cta = rank == 0u;
     ctx.fruit_pending = false;
     ctx.seq = 0;
+    ctx.nseq = 0;
     ctx.resident = d.resident != 0u;
     ctx.rank = rank;
     ctx.ranks = ranks;
@@ -1628,6 +1714,7 @@ __device__ __forceinline__ void run_frame(const DeviceCloth& src, const Schedule
         else
             __syncthreads();
     }
+    nc::neighbour_stage(ctx);
     if (ctx.fruit_cta) {
         for (uint32_t k = threadIdx.x; k < d.p_count; k += blockDim.x)
             fruit_shared.ab[k] =

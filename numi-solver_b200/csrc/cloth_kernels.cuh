@@ -55,6 +55,11 @@ __device__ __forceinline__ float from_fixed(unsigned long long v) {
     return static_cast<float>(static_cast<double>(static_cast<long long>(v)) * (1.0 / NC_FIXED_SCALE));
 }
 
+__device__ __forceinline__ unsigned ld_relaxed(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
 __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
     unsigned long long v;
     asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
@@ -144,6 +149,7 @@ struct Ctx {
     uint32_t epoch;
     uint32_t sub;
     unsigned long long seq;   // barriers passed in this launch
+    unsigned nseq;            // colour syncs passed in this launch
     FruitShared* fs;          // fruit-CTA shared state (valid in the fruit CTA)
     bool resident;
     uint32_t rank;            // cluster rank (resident) or 0

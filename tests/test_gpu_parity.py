@@ -136,6 +136,26 @@ def test_resident_equals_global(side, ranks):
     _check_bitexact(res, o)
 
 
+@pytest.mark.parametrize("side,grid", [(96, 0), (64, 37)])
+def test_neighbour_syncs_equal_grid_barriers(side, grid):
+    """Colours separated by neighbour syncs (each CTA waits only for the
+    CTAs that share a particle with it) give the grid barrier's bits, and
+    the oracle's."""
+    scene = small_square(side=side, fruits=12)
+    cfg = nc.substep_configs(scene, 24)
+    s = nc.Schedule.make(**dict(FULL, strainSweeps=2, selfCollision=1))
+    env = {"NUMI_CLOTH_RESIDENT": "0"}
+    if grid:
+        env["NUMI_CLOTH_GRID"] = str(grid)
+    nbr = run_gpu(scene, cfg, s, env=env)
+    bar = run_gpu(scene, cfg, s, env=dict(env, NUMI_CLOTH_NEIGHBOUR_SYNC="0"))
+    assert nbr["info"]["grid"] > 1 and nbr["failure"] == 0 and bar["failure"] == 0
+    assert np.array_equal(nbr["particles"], bar["particles"])
+    assert np.array_equal(nbr["fruits"], bar["fruits"])
+    assert np.array_equal(nbr["distances"], bar["distances"])
+    _check_bitexact(nbr, run_oracle(scene, cfg, s, bits=32))
+
+
 def test_two_runs_bit_identical():
     scene = small_square(side=40, fruits=10)
     cfg = nc.substep_configs(scene, 24)
