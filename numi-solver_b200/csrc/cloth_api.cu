@@ -504,7 +504,7 @@ int prepare_edge_grid(numi_cloth* h, bool primitive, uint32_t substeps, float ra
         e.edge_count = h->buf.alloc<uint32_t>(buckets);
         e.edge_offs = h->buf.alloc<uint32_t>(buckets);
         e.edge_chunk_total = h->buf.alloc<uint32_t>(ctas);
-        e.edge_entries = h->buf.alloc<uint4>(static_cast<size_t>(27u) * d.y_count);
+        e.edge_entries = h->buf.alloc<float4>(static_cast<size_t>(54u) * d.y_count);
         e.edge_giant = h->buf.alloc<uint32_t>(d.y_count);
         e.edge_bbox = h->buf.alloc<float4>(2u * d.y_count);
         std::vector<uint32_t> loc_off, loc_idx;

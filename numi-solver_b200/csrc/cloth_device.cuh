@@ -185,7 +185,7 @@ struct DeviceCloth {
     uint32_t* edge_count;         // [buckets]
     uint32_t* edge_offs;          // [buckets], within the bucket's scan chunk
     uint32_t* edge_chunk_total;   // [CTAs] entries of each CTA's chunk of buckets
-    uint4* edge_entries;          // [27 * y_count]
+    float4* edge_entries;         // [2 * 27 * y_count] grown box per entry, segment index in the first w
     uint32_t* edge_giant;         // [y_count] segments the grid does not hold
     float4* edge_bbox;            // [2 * y_count] grown boxes of the build
     const uint32_t* edge_loc_off; // [y_count + 1] CSR of every segment's local segments of higher index

@@ -389,11 +389,6 @@ __device__ __forceinline__ EdgeCells edge_cells(V3 a, V3 b, V3 ap, V3 bp, float 
         for (int k = 0; k < 3; ++k) c.span[k] = 0;
     return c;
 }
-__device__ __forceinline__ unsigned long long edge_cell_key(int x, int y, int z) {
-    return (static_cast<unsigned long long>(x + (1 << 20)) & 0x1fffffull) |
-           ((static_cast<unsigned long long>(y + (1 << 20)) & 0x1fffffull) << 21) |
-           ((static_cast<unsigned long long>(z + (1 << 20)) & 0x1fffffull) << 42);
-}
 
 // Exclusive-scan chunk of the buckets handled by this CTA.
 __device__ __forceinline__ uint32_t edge_chunk(const Ctx& ctx) {
@@ -485,8 +480,9 @@ __device__ __forceinline__ void edge_chunk_starts(const Ctx& ctx, uint32_t* s_st
     __syncthreads();
 }
 
-// Rebuild, step 3: every segment's cells into the sorted entry array
-// (segment, lower cell corner key, spans).
+// Rebuild, step 3: every segment's cells into the sorted entry array; an
+// entry is the segment's grown box (its cells follow from the box) with
+// the segment index in the lower corner's w.
 __device__ void edge_build_scatter(Ctx& ctx, uint32_t* s_start) {
     const DeviceCloth& d = ctx.d;
     const float h = 0.5f * (2.0f * ctx.c.radius + edge_skin(ctx));
@@ -498,16 +494,16 @@ __device__ void edge_build_scatter(Ctx& ctx, uint32_t* s_start) {
         const EdgeCells c = edge_cells(xyz(ld(d.edge_x0 + ab.x)), xyz(ld(d.edge_x0 + ab.y)), xyz(ld(d.xp + ab.x)),
                                        xyz(ld(d.xp + ab.y)), h, inv_cell);
         if (c.span[0] == 0) continue;
-        const unsigned long long key = edge_cell_key(c.lo[0], c.lo[1], c.lo[2]);
-        const uint4 entry = make_uint4(r.i, static_cast<uint32_t>(key), static_cast<uint32_t>(key >> 32),
-                                       static_cast<uint32_t>((c.span[0] - 1) | ((c.span[1] - 1) << 2) |
-                                                             ((c.span[2] - 1) << 4)));
+        float4 lo = __ldcg(d.edge_bbox + 2u * r.i);
+        const float4 hi = __ldcg(d.edge_bbox + 2u * r.i + 1u);
+        lo.w = __uint_as_float(r.i);
         for (int z = 0; z < c.span[2]; ++z)
             for (int y = 0; y < c.span[1]; ++y)
                 for (int x = 0; x < c.span[0]; ++x) {
                     const uint32_t b = cell_bucket(c.lo[0] + x, c.lo[1] + y, c.lo[2] + z, d.edge_mask);
                     const uint32_t at = s_start[b / chunk] + __ldcg(d.edge_offs + b) + atomicAdd(d.edge_count + b, 1u);
-                    d.edge_entries[at] = entry;
+                    d.edge_entries[2u * at] = lo;
+                    d.edge_entries[2u * at + 1u] = hi;
                 }
     }
 }
@@ -550,6 +546,21 @@ __device__ void edge_build_pairs(Ctx& ctx, const uint32_t* s_start) {
         }
         d.edge_pairs[k] = make_uint2(a, b);
     };
+    // Non-local candidates queue up per warp (in the reduction scratch) and
+    // take the distance test 32 at a time, one per lane, instead of one or
+    // two lanes at a time as they turn up.
+    static_assert(2u * NC_BLOCK_MAX * sizeof(uint2) <= sizeof(nc_red_smem), "pair queues exceed the scratch");
+    uint2* queue = reinterpret_cast<uint2*>(&nc_red_smem[0][0]) + 64u * (threadIdx.x >> 5);
+    uint32_t queued = 0;   // warp-uniform
+    auto flush = [&]() {
+        __syncwarp();
+        for (uint32_t k = lane; k < queued; k += 32u) {
+            const uint2 pr = queue[k];
+            keep_far(pr.x, pr.y);
+        }
+        __syncwarp();
+        queued = 0;
+    };
     // warps over the segments, as item_range spreads threads
     const uint32_t warps = blockDim.x >> 5;
     uint32_t i, end, stride;
@@ -573,52 +584,59 @@ __device__ void edge_build_pairs(Ctx& ctx, const uint32_t* s_start) {
         const uint32_t la = lane < llen ? __ldg(d.edge_loc_idx + llo + lane) : 0xffffffffu;
         const uint32_t lb = lane + 32u < llen ? __ldg(d.edge_loc_idx + llo + 32u + lane) : 0xffffffffu;
         if (c.span[0] != 0) {
-            for (int z = 0; z < c.span[2]; ++z)
-                for (int y = 0; y < c.span[1]; ++y)
-                    for (int x = 0; x < c.span[0]; ++x) {
-                        const int cx = c.lo[0] + x, cy = c.lo[1] + y, cz = c.lo[2] + z;
-                        const uint32_t b = cell_bucket(cx, cy, cz, d.edge_mask);
-                        const uint32_t start = s_start[b / chunk] + rdu(d.edge_offs + b);
-                        const uint32_t stop = start + rdu(d.edge_count + b);
-                        for (uint32_t base = start; base < stop; base += 32u) {
-                            const uint32_t e = base + lane;
-                            bool cand = e < stop;
-                            uint32_t j = 0;
-                            if (cand) {
-                                const uint4 en = l1 ? __ldca(d.edge_entries + e) : __ldcg(d.edge_entries + e);
-                                j = en.x;
-                                const unsigned long long key = static_cast<unsigned long long>(en.y) |
-                                                               (static_cast<unsigned long long>(en.z) << 32);
-                                const int jx = static_cast<int>(key & 0x1fffffull) - (1 << 20);
-                                const int jy = static_cast<int>((key >> 21) & 0x1fffffull) - (1 << 20);
-                                const int jz = static_cast<int>((key >> 42) & 0x1fffffull) - (1 << 20);
-                                const int sx = static_cast<int>(en.w & 3u) + 1,
-                                          sy = static_cast<int>((en.w >> 2) & 3u) + 1,
-                                          sz = static_cast<int>((en.w >> 4) & 3u) + 1;
-                                // a later segment; the visited cell in its range and the
-                                // lowest common cell
-                                cand = j > i && cx >= jx && cx < jx + sx && cy >= jy && cy < jy + sy && cz >= jz &&
-                                       cz < jz + sz && cx == max(c.lo[0], jx) && cy == max(c.lo[1], jy) &&
-                                       cz == max(c.lo[2], jz);
-                                if (cand) {   // the grown boxes meet: not farther apart than diameter + skin
-                                    const float4 olo = rd(d.edge_bbox + 2u * j), ohi = rd(d.edge_bbox + 2u * j + 1u);
-                                    cand = !(olo.x > bhi.x || ohi.x < blo.x || olo.y > bhi.y || ohi.y < blo.y ||
-                                             olo.z > bhi.z || ohi.z < blo.z);
-                                }
-                            }
-                            if (!__any_sync(0xffffffffu, cand)) continue;
-                            bool local = false;
-                            if (llen > 64u) {
-                                local = cand && seg_local(d, i, j);
-                            } else {
-                                for (uint32_t t = 0; t < min(llen, 32u); ++t)
-                                    local |= __shfl_sync(0xffffffffu, la, t) == j;
-                                for (uint32_t t = 32u; t < llen; ++t)
-                                    local |= __shfl_sync(0xffffffffu, lb, t - 32u) == j;
-                            }
-                            if (cand && !local) keep_far(i, j);
-                        }
+            // the segment's cells, one per lane: bucket range and cell
+            const uint32_t cells = static_cast<uint32_t>(c.span[0] * c.span[1] * c.span[2]);
+            uint32_t my_start = 0, my_stop = 0;
+            if (lane < cells) {
+                const int x = static_cast<int>(lane) % c.span[0], y = (static_cast<int>(lane) / c.span[0]) % c.span[1],
+                          z = static_cast<int>(lane) / (c.span[0] * c.span[1]);
+                const uint32_t b = cell_bucket(c.lo[0] + x, c.lo[1] + y, c.lo[2] + z, d.edge_mask);
+                my_start = s_start[b / chunk] + rdu(d.edge_offs + b);
+                my_stop = my_start + rdu(d.edge_count + b);
+            }
+            for (uint32_t t = 0; t < cells; ++t) {
+                const int cx = c.lo[0] + static_cast<int>(t) % c.span[0];
+                const int cy = c.lo[1] + (static_cast<int>(t) / c.span[0]) % c.span[1];
+                const int cz = c.lo[2] + static_cast<int>(t) / (c.span[0] * c.span[1]);
+                const uint32_t start = __shfl_sync(0xffffffffu, my_start, t);
+                const uint32_t stop = __shfl_sync(0xffffffffu, my_stop, t);
+                for (uint32_t base = start; base < stop; base += 32u) {
+                    const uint32_t e = base + lane;
+                    bool cand = e < stop;
+                    uint32_t j = 0;
+                    if (cand) {
+                        const float4 olo = rd(d.edge_entries + 2u * e), ohi = rd(d.edge_entries + 2u * e + 1u);
+                        j = __float_as_uint(olo.w);
+                        // the other segment's cells, as edge_cells finds them from the same box
+                        const int jx = static_cast<int>(floorf(olo.x * inv_cell)),
+                                  jy = static_cast<int>(floorf(olo.y * inv_cell)),
+                                  jz = static_cast<int>(floorf(olo.z * inv_cell));
+                        const int ux = static_cast<int>(floorf(ohi.x * inv_cell)),
+                                  uy = static_cast<int>(floorf(ohi.y * inv_cell)),
+                                  uz = static_cast<int>(floorf(ohi.z * inv_cell));
+                        // a later segment; the visited cell in its range and the lowest
+                        // common cell; the grown boxes meet (not farther apart than
+                        // diameter + skin)
+                        cand = j > i && cx >= jx && cx <= ux && cy >= jy && cy <= uy && cz >= jz && cz <= uz &&
+                               cx == max(c.lo[0], jx) && cy == max(c.lo[1], jy) && cz == max(c.lo[2], jz) &&
+                               !(olo.x > bhi.x || ohi.x < blo.x || olo.y > bhi.y || ohi.y < blo.y || olo.z > bhi.z ||
+                                 ohi.z < blo.z);
                     }
+                    if (!__any_sync(0xffffffffu, cand)) continue;
+                    bool local = false;
+                    if (llen > 64u) {
+                        local = cand && seg_local(d, i, j);
+                    } else {
+                        for (uint32_t q = 0; q < min(llen, 32u); ++q) local |= __shfl_sync(0xffffffffu, la, q) == j;
+                        for (uint32_t q = 32u; q < llen; ++q) local |= __shfl_sync(0xffffffffu, lb, q - 32u) == j;
+                    }
+                    const bool push = cand && !local;
+                    const unsigned m = __ballot_sync(0xffffffffu, push);
+                    if (push) queue[queued + __popc(m & ((1u << lane) - 1u))] = make_uint2(i, j);
+                    queued += static_cast<uint32_t>(__popc(m));
+                    if (queued >= 32u) flush();
+                }
+            }
         }
         for (uint32_t g = lane; g < giants; g += 32u) {
             const uint32_t j = __ldcg(d.edge_giant + g);
@@ -626,6 +644,7 @@ __device__ void edge_build_pairs(Ctx& ctx, const uint32_t* s_start) {
             if (!seg_local(d, min(i, j), max(i, j))) keep_far(min(i, j), max(i, j));
         }
     }
+    flush();
 }
 
 // Phase 1 and, when due, the rebuild of the pair list.  Returns false
