@@ -471,7 +471,8 @@ def run_ours(args):
                        "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}",
                        "grid": info["grid"], "block": info["block"],
                        "barriers_per_substep": info["barriers_per_substep"], "cluster": info["cluster"],
-                       "particles_resident_in_smem": info["resident"]},
+                       "particles_resident_in_smem": info["resident"],
+                       "neighbour_syncs": info["neighbour_syncs"]},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                          "peak_source": peaks["source"], "algorithmic_bytes_per_substep": ab},

@@ -255,8 +255,10 @@ int numi_cloth_snapshot(numi_cloth_t* handle, uint32_t slot);
 int numi_cloth_restore(numi_cloth_t* handle, uint32_t slot);
 
 /* Launch geometry of the last step: grid CTAs, threads per CTA, barriers
- * per substep, kernel launches, cluster size (0: no cluster), and 1 when the
- * particles are resident in (distributed) shared memory. */
+ * per substep, kernel launches, cluster size (0: no cluster), and flags:
+ * bit 0 when the particles are resident in (distributed) shared memory,
+ * bit 1 when constraint colours are separated by neighbour syncs instead of
+ * the grid barrier. */
 int numi_cloth_launch_info(numi_cloth_t* handle, uint32_t out[6]);
 
 /* Pass counters: out[0] barriers of the last substep, out[1] the most

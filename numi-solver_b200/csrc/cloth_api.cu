@@ -99,6 +99,7 @@ struct numi_cloth {
     uint32_t last_substeps = 0;
     float yarn_rest_median = 0.0f;   // median yarn segment rest length
     bool neighbours = false;         // neighbour-sync tables built for the cooperative grid
+    size_t nbr_smem = 0;             // dynamic shared memory of a frame launch with them
     // host copies for the edge/edge local lists, built with the edge buffers
     std::vector<uint2> host_yarn;
     std::vector<uint32_t> host_local_off, host_local_idx;
@@ -226,12 +227,14 @@ int make_batches(const Rec* recs, uint32_t count, uint32_t n_targets, ColourFn c
 
 // Neighbour syncs of the cooperative grid.  CTA r takes, in every colour
 // batch, the items whose lowest particle lies in its equal share
-// [r n / R, (r + 1) n / R) of the particle range; its neighbours are the
+// [r n / R, (r + 1) n / R) of the particle range (a list of batch-relative
+// indices per colour, staged in its shared memory); its neighbours are the
 // CTAs whose items share a particle with its own in any colour (reads
-// included: a bend's middle particle).  Built when every batch lists its
-// items in ascending lowest particle (a share is then one index range) and
-// no CTA has more than NC_NBR_MAX neighbours; otherwise every colour ends
-// with the grid barrier.
+// included: a bend's middle particle).  Built when no CTA has more than
+// NC_NBR_MAX neighbours, its lists fit NC_NBR_WORDS words, and the grid
+// stays co-resident with them; otherwise every colour ends with the grid
+// barrier.  NUMI_CLOTH_NEIGHBOUR_SYNC=0 keeps the grid barrier.
+#define NC_NBR_WORDS 4096u
 bool prepare_neighbours(numi_cloth* h, const NumiClothScene* scene) {
     DeviceCloth& d = h->d;
     const uint32_t R = h->grid, n = d.n;
@@ -242,41 +245,31 @@ bool prepare_neighbours(numi_cloth* h, const NumiClothScene* scene) {
         slots > 3u * NC_MAX_BATCHES)
         return false;
     auto cta_of = [&](uint32_t p) { return static_cast<uint32_t>(static_cast<uint64_t>(p) * R / n); };
-    std::vector<uint2> range(static_cast<size_t>(R) * slots);
+    // lists[r][slot]: CTA r's items of the colour, ascending
+    std::vector<std::vector<std::vector<uint32_t>>> lists(R, std::vector<std::vector<uint32_t>>(slots));
     std::vector<std::vector<uint32_t>> touch(n);   // CTAs touching each particle
-    std::vector<uint32_t> cta;
     auto batch = [&](uint32_t slot, const Batch& bt, auto parts) {
-        cta.assign(bt.count, 0u);
-        uint32_t prev = 0;
         for (uint32_t k = 0; k < bt.count; ++k) {
             uint32_t p[4];
             const int np = parts(bt.first + k, p);
             uint32_t lowest = p[0];
             for (int e = 1; e < np; ++e) lowest = std::min(lowest, p[e]);
-            if (lowest < prev) return false;
-            prev = lowest;
-            cta[k] = cta_of(lowest);
+            const uint32_t c = cta_of(lowest);
+            lists[c][slot].push_back(k);
             for (int e = 0; e < np; ++e) {
                 std::vector<uint32_t>& t = touch[p[e]];
-                if (std::find(t.begin(), t.end(), cta[k]) == t.end()) t.push_back(cta[k]);
+                if (std::find(t.begin(), t.end(), c) == t.end()) t.push_back(c);
             }
         }
-        for (uint32_t r = 0, k = 0; r < R; ++r) {
-            const uint32_t start = k;
-            while (k < bt.count && cta[k] == r) ++k;
-            range[static_cast<size_t>(r) * slots + slot] = make_uint2(start, k);   // within the batch
-        }
-        return true;
     };
-    bool ok = true;
-    for (uint32_t b = 0; ok && b < d.n_dist_batches; ++b)
-        ok = batch(b, d.dist_batches[b], [&](uint32_t i, uint32_t* p) {
+    for (uint32_t b = 0; b < d.n_dist_batches; ++b)
+        batch(b, d.dist_batches[b], [&](uint32_t i, uint32_t* p) {
             p[0] = scene->distances[i].particlesAndColor.x;
             p[1] = scene->distances[i].particlesAndColor.y;
             return 2;
         });
-    for (uint32_t b = 0; ok && b < d.n_knot_batches; ++b)
-        ok = batch(d.n_dist_batches + b, d.knot_batches[b], [&](uint32_t i, uint32_t* p) {
+    for (uint32_t b = 0; b < d.n_knot_batches; ++b)
+        batch(d.n_dist_batches + b, d.knot_batches[b], [&](uint32_t i, uint32_t* p) {
             const NumiClothKnot& r = scene->knots[i];
             p[0] = r.particles.x;
             p[1] = r.particles.y;
@@ -284,14 +277,13 @@ bool prepare_neighbours(numi_cloth* h, const NumiClothScene* scene) {
             p[3] = r.particles.w;
             return 4;
         });
-    for (uint32_t b = 0; ok && b < d.n_bend_batches; ++b)
-        ok = batch(d.n_dist_batches + d.n_knot_batches + b, d.bend_batches[b], [&](uint32_t i, uint32_t* p) {
+    for (uint32_t b = 0; b < d.n_bend_batches; ++b)
+        batch(d.n_dist_batches + d.n_knot_batches + b, d.bend_batches[b], [&](uint32_t i, uint32_t* p) {
             p[0] = scene->bends[i].particlesAndColor.x;
             p[1] = scene->bends[i].particlesAndColor.y;
             p[2] = scene->bends[i].particlesAndColor.z;
             return 3;
         });
-    if (!ok) return false;
     std::vector<std::vector<uint32_t>> nbr(R);
     for (const std::vector<uint32_t>& t : touch)
         for (uint32_t c : t)
@@ -300,27 +292,54 @@ bool prepare_neighbours(numi_cloth* h, const NumiClothScene* scene) {
                     if (nbr[c].size() >= NC_NBR_MAX) return false;
                     nbr[c].push_back(o);
                 }
-    std::vector<uint32_t> off(R + 1u, 0u), idx;
+    std::vector<uint32_t> off(R + 1u, 0u), idx, block(R + 1u, 0u), items;
+    uint32_t widest = 0;
     for (uint32_t r = 0; r < R; ++r) {
         std::sort(nbr[r].begin(), nbr[r].end());
         idx.insert(idx.end(), nbr[r].begin(), nbr[r].end());
         off[r + 1u] = static_cast<uint32_t>(idx.size());
+        // the CTA's block: slot offsets, then the items
+        uint32_t at = 0;
+        for (uint32_t b = 0; b < slots; ++b) {
+            items.push_back(at);
+            at += static_cast<uint32_t>(lists[r][b].size());
+        }
+        items.push_back(at);
+        for (uint32_t b = 0; b < slots; ++b) items.insert(items.end(), lists[r][b].begin(), lists[r][b].end());
+        block[r + 1u] = static_cast<uint32_t>(items.size());
+        widest = std::max(widest, block[r + 1u] - block[r]);
     }
-    uint2* d_range = h->buf.alloc<uint2>(range.size());
+    if (widest > NC_NBR_WORDS) return false;
+    const size_t smem = nc_resident_offset() + static_cast<size_t>(widest) * sizeof(uint32_t);
+    int per_sm = 0;
+    if (raise_frame_smem(smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, frame_fn(false), static_cast<int>(h->block), smem) !=
+            cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+    if (static_cast<uint64_t>(per_sm) * static_cast<uint64_t>(sms) < R) return false;   // must stay co-resident
+    uint32_t* d_block = h->buf.alloc<uint32_t>(block.size());
+    uint32_t* d_items = h->buf.alloc<uint32_t>(items.size());
     uint32_t* d_off = h->buf.alloc<uint32_t>(off.size());
     uint32_t* d_idx = h->buf.alloc<uint32_t>(std::max<size_t>(idx.size(), 1));
-    unsigned int* d_flag = h->buf.alloc<unsigned int>(R);
-    if (!d_range || !d_off || !d_idx || !d_flag) return false;
-    if (cudaMemcpy(d_range, range.data(), range.size() * sizeof(uint2), cudaMemcpyHostToDevice) != cudaSuccess ||
+    unsigned int* d_flag = h->buf.alloc<unsigned int>(static_cast<size_t>(NC_NBR_FLAG_STRIDE) * R);
+    if (!d_block || !d_items || !d_off || !d_idx || !d_flag) return false;
+    if (cudaMemcpy(d_block, block.data(), block.size() * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(d_items, items.data(), items.size() * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(d_off, off.data(), off.size() * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess ||
         (!idx.empty() &&
          cudaMemcpy(d_idx, idx.data(), idx.size() * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess))
         return false;
     d.colour_slots = slots;
-    d.colour_range = d_range;
+    d.nbr_block = d_block;
+    d.nbr_items = d_items;
     d.nbr_off = d_off;
     d.nbr_idx = d_idx;
     d.nbr_flag = d_flag;
+    h->nbr_smem = smem;
     return true;
 }
 
@@ -360,10 +379,11 @@ cudaError_t launch(numi_cloth* h, uint32_t substeps, const Schedule& s, uint32_t
         // phases; its flags start at zero in every launch)
         if (h->neighbours && !edge) {
             d.nbr_on = 1u;
-            e = cudaMemsetAsync(d.nbr_flag, 0, h->grid * sizeof(unsigned int), h->stream);
+            e = cudaMemsetAsync(d.nbr_flag, 0, NC_NBR_FLAG_STRIDE * h->grid * sizeof(unsigned int), h->stream);
             if (e != cudaSuccess) return e;
         }
-        e = cudaLaunchCooperativeKernel(frame_fn(edge), dim3(h->grid), dim3(h->block), args, smem, h->stream);
+        e = cudaLaunchCooperativeKernel(frame_fn(edge), dim3(h->grid), dim3(h->block), args,
+                                        d.nbr_on ? h->nbr_smem : smem, h->stream);
     }
     if (e == cudaSuccess) ++h->launches;
     return e;
@@ -1221,7 +1241,7 @@ int numi_cloth_launch_info(numi_cloth_t* h, uint32_t out[6]) {
     out[2] = stats[0];
     out[3] = h->launches;
     out[4] = h->cluster;
-    out[5] = h->d.resident;
+    out[5] = h->d.resident | (h->neighbours ? 2u : 0u);
     return NUMI_CLOTH_OK;
 }
 

@@ -125,18 +125,21 @@ struct DeviceCloth {
     // the hardware cluster barrier instead of the global-memory barrier
     uint32_t cluster_barrier;
     // Neighbour syncs between constraint colours (cooperative grid, particles
-    // in global memory): CTA r solves items [start, end) of colour batch b,
-    // colour_range[r * colour_slots + b], an equal share of the particle
-    // index range in every colour, and between two colours waits only for
-    // the CTAs whose items share a particle with its own in any colour
-    // (nbr_idx[nbr_off[r] .. nbr_off[r + 1]]).  nbr_flag[r] counts the
-    // colours CTA r has finished in the launch (zeroed before every launch).
+    // in global memory): CTA r solves, in every colour, the items whose
+    // lowest particle lies in its equal share of the particle range (its
+    // list: nbr_items[nbr_block[r] .. nbr_block[r + 1]], colour_slots + 1
+    // offsets then batch-relative item indices), and between two colours
+    // waits only for the CTAs whose items share a particle with its own in
+    // any colour (nbr_idx[nbr_off[r] .. nbr_off[r + 1]]).
+    // nbr_flag[32 r] counts the colours CTA r has finished in the launch
+    // (zeroed before every launch).
     uint32_t nbr_on;
     uint32_t colour_slots;         // distance + knot + bend batches
-    const uint2* colour_range;     // [grid * colour_slots]
+    const uint32_t* nbr_block;     // [grid + 1]
+    const uint32_t* nbr_items;
     const uint32_t* nbr_off;       // [grid + 1]
     const uint32_t* nbr_idx;
-    unsigned int* nbr_flag;        // [grid]
+    unsigned int* nbr_flag;        // [32 * grid]
     // resident mode: 1 when particle positions and velocities live in the
     // (distributed) shared memory of the grid's CTAs for the whole launch;
     // CTA r owns particles [r << resident_shift, (r + 1) << resident_shift)

@@ -5,6 +5,13 @@
 
 #include "cloth_kernels.cuh"
 
+// Dynamic shared memory of a frame: the cloth descriptor, the fruit CTA's
+// state, then either (resident mode) the CTA's particle positions and
+// velocities or (neighbour syncs) the CTA's colour item lists.
+__host__ __device__ constexpr size_t nc_round256(size_t b) { return (b + 255u) & ~size_t(255u); }
+__host__ __device__ constexpr size_t nc_fruit_offset() { return nc_round256(sizeof(DeviceCloth)); }
+__host__ __device__ constexpr size_t nc_resident_offset() { return nc_round256(nc_fruit_offset() + sizeof(FruitShared)); }
+
 namespace nc {
 namespace {   // internal linkage: the edge kernels' unit includes these too
 
@@ -84,32 +91,45 @@ __device__ bool grid_sync(Ctx& ctx) {
 #define NC_SYNC(ctx) \
     do { if (!grid_sync(ctx)) return false; } while (0)
 
-// This CTA's item ranges of the colour batches and its neighbour CTAs,
-// staged at the start of a launch that runs neighbour syncs.
+// Neighbour syncs: this CTA's neighbour CTAs (static shared memory) and its
+// colour item lists (dynamic shared memory after the fruit state: the
+// colour_slots + 1 list offsets, then the batch-relative item indices),
+// staged at the start of a launch.  Each CTA's finished-colour count has
+// its own 128-byte line.
 #define NC_NBR_MAX 64u
-__shared__ uint2 nc_colour_range[3u * NC_MAX_BATCHES];
+#define NC_NBR_FLAG_STRIDE 32u
 __shared__ uint32_t nc_nbr[NC_NBR_MAX];
 __shared__ uint32_t nc_nbr_count;
+extern __shared__ __align__(16) unsigned char nc_frame_smem[];
+
+__device__ __forceinline__ uint32_t* colour_lists() {
+    return reinterpret_cast<uint32_t*>(nc_frame_smem + nc_resident_offset());
+}
 
 __device__ __forceinline__ void neighbour_stage(const Ctx& ctx) {
     const DeviceCloth& d = ctx.d;
     if (!d.nbr_on) return;
-    for (uint32_t b = threadIdx.x; b < d.colour_slots; b += blockDim.x)
-        nc_colour_range[b] = d.colour_range[static_cast<size_t>(ctx.rank) * d.colour_slots + b];
     const uint32_t lo = d.nbr_off[ctx.rank], hi = d.nbr_off[ctx.rank + 1u];
     for (uint32_t k = threadIdx.x; k < hi - lo; k += blockDim.x) nc_nbr[k] = d.nbr_idx[lo + k];
     if (threadIdx.x == 0) nc_nbr_count = hi - lo;
+    const uint32_t w0 = d.nbr_block[ctx.rank], w1 = d.nbr_block[ctx.rank + 1u];
+    uint32_t* lists = colour_lists();
+    for (uint32_t k = threadIdx.x; k < w1 - w0; k += blockDim.x) lists[k] = d.nbr_items[w0 + k];
     __syncthreads();
 }
 
-// Items of colour batch `slot` (count items) that this thread solves: the
-// CTA's share when neighbour syncs run, else the grid-stride range.
+// Positions of colour batch `slot` that this thread takes: in the CTA's
+// list when neighbour syncs run, else the grid-stride range of the batch
+// (count items).  colour_item maps a position to the batch-relative item.
 __device__ __forceinline__ Range colour_items(const Ctx& ctx, uint32_t slot, uint32_t count) {
     if (ctx.d.nbr_on) {
-        const uint2 r = nc_colour_range[slot];
-        return Range{r.x + threadIdx.x, min(r.y, count), blockDim.x};
+        const uint32_t* lists = colour_lists();
+        return Range{lists[slot] + threadIdx.x, lists[slot + 1u], blockDim.x};
     }
     return item_range(ctx, count);
+}
+__device__ __forceinline__ uint32_t colour_item(const Ctx& ctx, uint32_t pos) {
+    return ctx.d.nbr_on ? colour_lists()[ctx.d.colour_slots + 1u + pos] : pos;
 }
 
 // Barrier between two constraint colours.  With neighbour syncs the CTA
@@ -125,10 +145,10 @@ __device__ bool colour_sync(Ctx& ctx) {
     ++ctx.barriers;
     const unsigned target = ++ctx.nseq;
     __syncthreads();
-    if (threadIdx.x == 0) st_release(d.nbr_flag + ctx.rank, target);
+    if (threadIdx.x == 0) st_release(d.nbr_flag + NC_NBR_FLAG_STRIDE * ctx.rank, target);
     int ab = 0;
     if (threadIdx.x < nc_nbr_count) {
-        const unsigned* f = d.nbr_flag + nc_nbr[threadIdx.x];
+        const unsigned* f = d.nbr_flag + NC_NBR_FLAG_STRIDE * nc_nbr[threadIdx.x];
         unsigned spins = 0u;
         while (ld_relaxed(f) < target) {
             ++spins;
@@ -1020,8 +1040,10 @@ __device__ bool strain_sweeps(Ctx& ctx) {
                 const Batch bt = d.dist_batches[b];
                 if (bt.limited == 0u) continue;
                 fruit_flush(ctx);
-                for (Range r = colour_items(ctx, b, bt.limited); r.i < r.end; r.i += r.stride)
-                    limit_strain(ctx, bt.first + r.i);
+                for (Range r = colour_items(ctx, b, bt.limited); r.i < r.end; r.i += r.stride) {
+                    const uint32_t k = colour_item(ctx, r.i);
+                    if (k < bt.limited) limit_strain(ctx, bt.first + k);
+                }
                 // a colour follows: a later limited batch, or the next sweep
                 bool more = sw + 1u < ctx.s.strain_sweeps;
                 for (uint32_t c = b + 1u; c < d.n_dist_batches && !more; ++c) more = d.dist_batches[c].limited != 0u;
@@ -1557,13 +1579,13 @@ __device__ __forceinline__ bool substep(Ctx& ctx, bool last) {
                 const Batch bt = d.dist_batches[b];
                 fruit_flush(ctx);
                 for (Range r = colour_items(ctx, b, bt.count); r.i < r.end; r.i += r.stride)
-                    solve_distance(ctx, bt.first + r.i, dt2);
+                    solve_distance(ctx, bt.first + colour_item(ctx, r.i), dt2);
                 NC_CSYNC(ctx, b + 1u < d.n_dist_batches || d.n_knot_batches > 0u || bends_follow);
             }
             for (uint32_t b = 0; b < d.n_knot_batches; ++b) {
                 const Batch bt = d.knot_batches[b];
                 for (Range r = colour_items(ctx, d.n_dist_batches + b, bt.count); r.i < r.end; r.i += r.stride)
-                    solve_knot(ctx, bt.first + r.i, dt2);
+                    solve_knot(ctx, bt.first + colour_item(ctx, r.i), dt2);
                 NC_CSYNC(ctx, b + 1u < d.n_knot_batches || bends_follow);
             }
         }
@@ -1587,7 +1609,7 @@ __device__ __forceinline__ bool substep(Ctx& ctx, bool last) {
                 for (uint32_t b = 0; b < d.n_bend_batches; ++b) {
                     const Batch bt = d.bend_batches[b];
                     for (Range r = colour_items(ctx, slot0 + b, bt.count); r.i < r.end; r.i += r.stride)
-                        solve_bend(ctx, bt.first + r.i, dt2, ctx.c.radius, ctx.c.ground);
+                        solve_bend(ctx, bt.first + colour_item(ctx, r.i), dt2, ctx.c.radius, ctx.c.ground);
                     NC_CSYNC(ctx, b + 1u < d.n_bend_batches);
                 }
             }
@@ -1663,11 +1685,6 @@ __device__ __forceinline__ bool substep(Ctx& ctx, bool last) {
 }  // namespace
 }  // namespace nc
 
-// Dynamic shared memory of a frame: the cloth descriptor, the fruit CTA's
-// state, then (resident mode) the CTA's particle positions and velocities.
-__host__ __device__ constexpr size_t nc_round256(size_t b) { return (b + 255u) & ~size_t(255u); }
-__host__ __device__ constexpr size_t nc_fruit_offset() { return nc_round256(sizeof(DeviceCloth)); }
-__host__ __device__ constexpr size_t nc_resident_offset() { return nc_round256(nc_fruit_offset() + sizeof(FruitShared)); }
 
 // One cloth's frame on `ranks` CTAs (this one is `rank`): all substeps of
 // the launch's Configs, particles optionally resident in (distributed)

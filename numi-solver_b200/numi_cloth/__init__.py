@@ -593,7 +593,7 @@ class ClothSolver:
         out = (ctypes.c_uint32 * 6)()
         self._check(self.lib.numi_cloth_launch_info(self._h, out))
         return {"grid": out[0], "block": out[1], "barriers_per_substep": out[2], "launches": out[3],
-                "cluster": out[4], "resident": bool(out[5])}
+                "cluster": out[4], "resident": bool(out[5] & 1), "neighbour_syncs": bool(out[5] & 2)}
 
     def trace(self, substeps: int) -> np.ndarray:
         """Per-barrier globaltimer stamps (ns) of the last step, [substeps, 128]."""

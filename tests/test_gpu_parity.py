@@ -150,6 +150,7 @@ def test_neighbour_syncs_equal_grid_barriers(side, grid):
     nbr = run_gpu(scene, cfg, s, env=env)
     bar = run_gpu(scene, cfg, s, env=dict(env, NUMI_CLOTH_NEIGHBOUR_SYNC="0"))
     assert nbr["info"]["grid"] > 1 and nbr["failure"] == 0 and bar["failure"] == 0
+    assert nbr["info"]["neighbour_syncs"] and not bar["info"]["neighbour_syncs"]
     assert np.array_equal(nbr["particles"], bar["particles"])
     assert np.array_equal(nbr["fruits"], bar["fruits"])
     assert np.array_equal(nbr["distances"], bar["distances"])
