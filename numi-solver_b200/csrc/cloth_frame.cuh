@@ -1211,15 +1211,30 @@ __device__ void phase_finalize(Ctx& ctx) {
 // Fruit/yarn Coulomb friction (tools/cloth_bag.cpp:3178-3270) of one
 // recorded segment, with fruit velocities frozen over the sweep; the fruit
 // velocity changes go into the CTA's fixed-point sums.
-__device__ __forceinline__ void yarn_friction_segment(const Ctx& ctx, uint32_t seg, const float4* s_vw,
+// A recorded segment's endpoints and slot states: what the friction of the
+// segment reads that no yarn colour of the sweep changes.
+struct FrictionSeg {
+    uint32_t seg;
+    uint2 ij;
+    uint32_t st[NC_YARN_SLOTS];
+};
+__device__ __forceinline__ FrictionSeg friction_seg(const DeviceCloth& d, uint32_t seg) {
+    FrictionSeg fs;
+    fs.seg = seg;
+    fs.ij = __ldg(d.d_ij + seg);
+#pragma unroll
+    for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q)
+        fs.st[q] = __float_as_uint(__ldcg(&d.yarn_slot_b[seg * NC_YARN_SLOTS + q].z));
+    return fs;
+}
+
+__device__ __forceinline__ void yarn_friction_segment(const Ctx& ctx, const FrictionSeg& fseg, const float4* s_vw,
                                                       const float4* s_or, unsigned long long* s_sum) {
     const DeviceCloth& d = ctx.d;
     const SubCfg& c = ctx.c;
-    const uint2 ij = __ldg(d.d_ij + seg);
-    uint32_t st[NC_YARN_SLOTS];
-#pragma unroll
-    for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q)
-        st[q] = __float_as_uint(__ldcg(&d.yarn_slot_b[seg * NC_YARN_SLOTS + q].z));
+    const uint32_t seg = fseg.seg;
+    const uint2 ij = fseg.ij;
+    const uint32_t* st = fseg.st;
     const float4 pa = px(ctx, ij.x);
     const float4 pb = px(ctx, ij.y);
     float4 va = pv(ctx, ij.x);
@@ -1326,13 +1341,20 @@ __device__ void yarn_friction_sweep(Ctx& ctx) {
     }
     __syncthreads();
     const uint32_t listed = min(__ldcg(d.yarn_list_n), d.d_count);
+    // this thread's first listed segment, loaded once for all colours (the
+    // colours then wait only on their particle loads); further ones (more
+    // segments listed than threads) are loaded in their colour
+    FrictionSeg mine{};
+    if (threadIdx.x < listed) mine = friction_seg(d, __ldcg(d.yarn_list + threadIdx.x));
     for (uint32_t b = 0; b < d.n_dist_batches; ++b) {
         const Batch bt = d.dist_batches[b];
         if (bt.yarn == 0u) continue;
-        for (uint32_t e = threadIdx.x; e < listed; e += blockDim.x) {
+        if (threadIdx.x < listed && mine.seg >= bt.first && mine.seg < bt.first + bt.yarn)
+            yarn_friction_segment(ctx, mine, s_vw, s_or, s_sum);
+        for (uint32_t e = threadIdx.x + blockDim.x; e < listed; e += blockDim.x) {
             const uint32_t seg = __ldcg(d.yarn_list + e);
             if (seg < bt.first || seg >= bt.first + bt.yarn) continue;
-            yarn_friction_segment(ctx, seg, s_vw, s_or, s_sum);
+            yarn_friction_segment(ctx, friction_seg(d, seg), s_vw, s_or, s_sum);
         }
         __syncthreads();
     }
