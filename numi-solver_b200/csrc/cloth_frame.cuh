@@ -530,7 +530,7 @@ struct SegRecords {
 // colour stages them in shared memory for all colours, the CTA's
 // displacement sums accumulate over the sweep, and the last colour adds
 // them to the global sums.
-__device__ void yarn_contact_batch(Ctx& ctx, const Batch& bt, bool first, bool last) {
+__device__ void yarn_contact_batch(Ctx& ctx, uint32_t slot, const Batch& bt, bool first, bool last) {
     const DeviceCloth& d = ctx.d;
     const SubCfg& c = ctx.c;
     __shared__ float4 s_fruit[NC_MAX_FRUITS];   // xyz position, w radius
@@ -549,10 +549,14 @@ __device__ void yarn_contact_batch(Ctx& ctx, const Batch& bt, bool first, bool l
     unsigned long long* acc = reinterpret_cast<unsigned long long*>(d.fruit_partial);
     const uint32_t nf = d.f_count;
     const uint32_t lane = threadIdx.x & 31u;
-    const Range rg = item_range(ctx, bt.yarn);
+    // the colour's items of this CTA (its yarn segments lead its list) or
+    // the grid-stride range, a warp at a time
+    const Range rg = colour_items(ctx, slot, bt.yarn);
     for (uint32_t base = rg.i - lane; base < rg.end; base += rg.stride) {
-        const uint32_t k = base + lane;
-        const bool valid = k < rg.end;
+        const uint32_t pos = base + lane;
+        const uint32_t k = pos < rg.end ? colour_item(ctx, pos) : bt.yarn;
+        const bool valid = k < bt.yarn;
+        if (!__any_sync(0xffffffffu, valid)) break;
         const uint32_t seg = bt.first + (valid ? k : 0u);
         uint2 ij = make_uint2(0u, 0u);
         float4 pa = make_float4(0, 0, 0, 0), pb = pa;
@@ -757,8 +761,8 @@ __device__ bool yarn_sweep(Ctx& ctx) {
     for (uint32_t b = first; b <= last && b < ctx.d.n_dist_batches; ++b) {
         const Batch bt = ctx.d.dist_batches[b];
         if (bt.yarn == 0u) continue;
-        yarn_contact_batch(ctx, bt, b == first, b == last);
-        NC_SYNC(ctx);
+        yarn_contact_batch(ctx, b, bt, b == first, b == last);
+        NC_CSYNC(ctx, b != last);   // colour to colour: neighbour sync
     }
     ctx.fruit_pending = true;
     return true;
