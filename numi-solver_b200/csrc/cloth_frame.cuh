@@ -204,7 +204,10 @@ __device__ void phase_begin(Ctx& ctx) {
     const DeviceCloth& d = ctx.d;
     const SubCfg& c = ctx.c;
     if (ctx.grip_cta) {
-        grip_attach(ctx);
+        // on one CTA the attach reads the positions before this CTA
+        // predicts them; on more it ran at the end of the previous substep
+        // (or before the launch's first), where every position is final
+        if (ctx.ranks == 1u) grip_attach(ctx);
         __syncthreads();
         for (uint32_t g = threadIdx.x; g < d.g_count; g += blockDim.x) {
             d.grips[g].lambda.x = 0.0f;
@@ -1700,6 +1703,11 @@ __device__ __forceinline__ bool substep(Ctx& ctx, bool last) {
     }
     if (s.frictions && d.f_count > 0u) yarn_friction_sweep(ctx);   // fruit CTA, no grid barrier
     fruit_tail(ctx, last);
+    if (ctx.ranks > 1u && ctx.grip_cta && !last) {   // the next substep's grip attach
+        Ctx next = ctx;
+        next.c = nc::load_cfg(d.cfg + s.cfg_offset + ctx.sub + 1u);
+        grip_attach(next);
+    }
     NC_SYNC(ctx);
     if (ctx.rank == 0 && threadIdx.x == 0) {
         d.stats[1] = max(d.stats[1], passes);
@@ -1765,6 +1773,15 @@ __device__ __forceinline__ void run_frame(const DeviceCloth& src, const Schedule
         __syncthreads();
     }
     const uint32_t epoch_base = s.epoch_ptr != nullptr ? *s.epoch_ptr : d.epoch_base;
+    if (ranks > 1u && s.substeps > 0u) {
+        // the first substep's grip attach, before any CTA predicts (later
+        // substeps attach at the end of the one before)
+        ctx.sub = 0;
+        ctx.c = nc::load_cfg(d.cfg + s.cfg_offset);
+        ctx.barriers = 0;
+        if (ctx.grip_cta) nc::grip_attach(ctx);
+        if (!nc::grid_sync(ctx)) return;
+    }
     for (uint32_t sub = 0; sub < s.substeps; ++sub) {
         ctx.sub = sub;
         ctx.c = nc::load_cfg(d.cfg + s.cfg_offset + sub);

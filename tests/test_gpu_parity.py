@@ -157,6 +157,47 @@ def test_neighbour_syncs_equal_grid_barriers(side, grid):
     _check_bitexact(nbr, run_oracle(scene, cfg, s, bits=32))
 
 
+def test_bag_neighbour_syncs_bitexact():
+    """The produce bag (knots, bends, 12 fruits, grips, self contact) on a
+    cooperative grid with neighbour syncs between its colours gives the
+    one-CTA run's bits and the oracle's."""
+    dt = 1.0 / 5760.0
+    scene = nc.bag_scene(scenario="recorded", timestep=dt)
+    cfg = bag_frame_configs(scene, 0, 24, dt)
+    s = nc.Schedule.make(**dict(FULL, selfCollision=1))
+    many = run_gpu(scene, cfg, s, env={"NUMI_CLOTH_GRID": "6", "NUMI_CLOTH_RESIDENT": "0"})
+    one = run_gpu(scene, cfg, s)
+    assert many["info"]["grid"] == 6 and many["info"]["neighbour_syncs"]
+    assert many["failure"] == 0 and one["failure"] == 0
+    assert np.array_equal(many["particles"], one["particles"])
+    assert np.array_equal(many["fruits"], one["fruits"])
+    _check_bitexact(many, run_oracle(scene, cfg, s, bits=32))
+
+
+def test_patch_regrab_multi_cta_bitexact():
+    """The reference's patch-regrab fixture (three grip generations, each
+    re-attaching to the cuff particles nearest the grip target) on one CTA
+    and on a cooperative grid: the attach reads the positions the previous
+    substep left, on every launch shape, and the result is the oracle's."""
+    import os
+
+    traj = nc.GripTrajectory(os.path.join(os.path.dirname(__file__), "golden", "reference_fixtures",
+                                          "synthetic-patch-regrab.csv"))
+    assert traj.select_nearest
+    dt = (1.0 / 120.0) / 24
+    scene = nc.bag_scene(scenario="recorded", timestep=dt, select_nearest=True)
+    cfg = traj.configs(scene.config, scene.handle_base, 0, 24, dt)
+    s = nc.Schedule.make(**FULL)
+    one = run_gpu(scene, cfg, s)
+    many = run_gpu(scene, cfg, s, env={"NUMI_CLOTH_GRID": "6", "NUMI_CLOTH_RESIDENT": "0"})
+    assert many["info"]["grid"] == 6 and one["failure"] == 0 and many["failure"] == 0
+    assert np.array_equal(one["grips"], many["grips"])
+    assert np.array_equal(one["particles"], many["particles"])
+    o = run_oracle(scene, cfg, s, bits=32)
+    _check_bitexact(many, o)
+    _check_bitexact(one, o)
+
+
 def test_two_runs_bit_identical():
     scene = small_square(side=40, fruits=10)
     cfg = nc.substep_configs(scene, 24)
