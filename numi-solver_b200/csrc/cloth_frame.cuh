@@ -580,17 +580,25 @@ __device__ void yarn_contact_batch(Ctx& ctx, uint32_t slot, const Batch& bt, boo
             whi.y = fmaxf(whi.y, __shfl_xor_sync(0xffffffffu, whi.y, o));
             whi.z = fmaxf(whi.z, __shfl_xor_sync(0xffffffffu, whi.z, o));
         }
-        unsigned long long mask = 0ull;
+        // fruits near the warp's box, and (wide) near it grown by a margin:
+        // while a segment's box stays within half the margin of the warp's
+        // box, every fruit near it is on the wide mask
+        const float margin = 8.0f * c.radius;
+        unsigned long long mask = 0ull, wide = 0ull;
         for (uint32_t f0 = 0; f0 < nf; f0 += 32u) {
             const uint32_t f = f0 + lane;
-            bool near = false;
+            bool near = false, near_wide = false;
             if (f < nf) {
                 const float4 fs = s_fruit[f];
                 const float target = fs.w + c.radius;
                 near = !(fs.x < wlo.x - target || fs.x > whi.x + target || fs.y < wlo.y - target ||
                          fs.y > whi.y + target || fs.z < wlo.z - target || fs.z > whi.z + target);
+                const float reach = target + margin;
+                near_wide = !(fs.x < wlo.x - reach || fs.x > whi.x + reach || fs.y < wlo.y - reach ||
+                              fs.y > whi.y + reach || fs.z < wlo.z - reach || fs.z > whi.z + reach);
             }
             mask |= static_cast<unsigned long long>(__ballot_sync(0xffffffffu, near)) << f0;
+            wide |= static_cast<unsigned long long>(__ballot_sync(0xffffffffu, near_wide)) << f0;
         }
         if (!valid || mask == 0ull) continue;
         // this segment's own candidates among the warp's: the box test the
@@ -630,11 +638,20 @@ __device__ void yarn_contact_batch(Ctx& ctx, uint32_t slot, const Batch& bt, boo
             V3 delta{0.0f, 0.0f, 0.0f};
             const float lam = yarn_correction(pa, pb, w0, w1, s_fw[f], n, corr, c.ground, c.radius, delta);
             // the segment moved: its candidates are the later fruits near its
-            // new box
+            // new box (those on the wide mask while the box stays within half
+            // the margin of the warp's box, else any fruit)
             changed = true;
             mask = 0ull;
-            for (uint32_t g = f + 1u; g < nf; ++g)
+            const float half = 0.5f * margin;
+            const bool inside = fminf(pa.x, pb.x) >= wlo.x - half && fmaxf(pa.x, pb.x) <= whi.x + half &&
+                                fminf(pa.y, pb.y) >= wlo.y - half && fmaxf(pa.y, pb.y) <= whi.y + half &&
+                                fminf(pa.z, pb.z) >= wlo.z - half && fmaxf(pa.z, pb.z) <= whi.z + half;
+            unsigned long long pool = inside ? wide : (nf >= 64u ? ~0ull : (1ull << nf) - 1ull);
+            pool &= f + 1u < 64u ? (~0ull << (f + 1u)) : 0ull;
+            for (; pool != 0ull; pool &= pool - 1ull) {
+                const uint32_t g = static_cast<uint32_t>(__ffsll(static_cast<long long>(pool)) - 1);
                 if (fruit_near_segment(s_fruit[g], pa, pb, c.radius)) mask |= 1ull << g;
+            }
             cta_sums_add(s_sum + 3u * f + 0u, delta.x);
             cta_sums_add(s_sum + 3u * f + 1u, delta.y);
             cta_sums_add(s_sum + 3u * f + 2u, delta.z);
