@@ -1010,9 +1010,16 @@ __device__ void self_solve(Ctx& ctx, uint32_t it) {
             px_set(ctx, a, make_float4(p.x + dx, p.y + dy, p.z + dz, p.w));
         }
     }
-    if (contacts != 0ull) {
+    // one atomic pair per warp (an integer sum and the maximum of
+    // non-negative floats as integers: the order does not matter)
+    unsigned pen_bits = __float_as_uint(max_pen);
+    for (int o = 16; o > 0; o >>= 1) {
+        contacts += __shfl_xor_sync(0xffffffffu, contacts, o);
+        pen_bits = max(pen_bits, __shfl_xor_sync(0xffffffffu, pen_bits, o));
+    }
+    if ((threadIdx.x & 31u) == 0u && contacts != 0ull) {
         atomicAdd(d.self_stats, contacts);
-        atomicMax(d.self_stats + 1, static_cast<unsigned long long>(__float_as_uint(max_pen)));
+        atomicMax(d.self_stats + 1, static_cast<unsigned long long>(pen_bits));
     }
 }
 
