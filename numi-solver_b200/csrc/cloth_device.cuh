@@ -35,10 +35,10 @@ struct Batch {
     uint32_t yarn;       // leading records that are yarn segments
 };
 
-// One particle in the self-contact grid: one 32-byte sector.
-struct __align__(32) HashSlot {
-    float4 pos;     // start-of-pass position xyz, inverse mass
-    uint4 meta;     // particle index, 0, 0, 0
+// One particle in the self-contact grid: its start-of-pass position and,
+// in w, its index (bits); two slots per 32-byte sector.
+struct __align__(16) HashSlot {
+    float4 pos;
 };
 
 // One edge/edge pair record of a substep (SelfEdgeEdgeContactImpulse,

@@ -865,8 +865,7 @@ __device__ void self_insert(Ctx& ctx, uint32_t it) {
             }
             e = d.hash_over + o;
         }
-        e->pos = p;
-        e->meta = make_uint4(i, 0u, 0u, 0u);
+        e->pos = make_float4(p.x, p.y, p.z, __uint_as_float(i));
     }
 }
 
@@ -950,21 +949,20 @@ __device__ void self_solve(Ctx& ctx, uint32_t it) {
                 slot[j] = bq * NC_HASH_CAP + (t - pq);
             }
             float4 e[NC_SELF_BATCH];
-            uint32_t bidx[NC_SELF_BATCH];
 #pragma unroll
-            for (uint32_t j = 0; j < NC_SELF_BATCH; ++j) {
+            for (uint32_t j = 0; j < NC_SELF_BATCH; ++j)
                 e[j] = l1 ? __ldca(&d.hash[slot[j]].pos) : __ldcg(&d.hash[slot[j]].pos);
-                bidx[j] = l1 ? __ldca(&d.hash[slot[j]].meta.x) : __ldcg(&d.hash[slot[j]].meta.x);
-            }
 #pragma unroll
             for (uint32_t j = 0; j < NC_SELF_BATCH; ++j) {
                 if (t0 + j >= total) continue;
-                const uint32_t b = bidx[j];
+                const uint32_t b = __float_as_uint(e[j].w);
                 if (b == a) continue;
                 const V3 diff = xyz(e[j]) - xyz(p);
                 const float L = len3(diff);
                 if (L >= target || L < 1.0e-12f) continue;
-                const float den = p.w + e[j].w;
+                // the partner's inverse mass (fixed; the corrections of this
+                // pass rewrite only positions)
+                const float den = p.w + px(ctx, b).w;
                 if (den <= 0.0f) continue;
                 if (local_pair(d, a, b)) continue;
                 const V3 corr = diff * ((target - L) / (L * den));
@@ -984,12 +982,12 @@ __device__ void self_solve(Ctx& ctx, uint32_t it) {
             const uint32_t over = static_cast<uint32_t>(oh >> 32) == tag ? min(static_cast<uint32_t>(oh), d.n) : 0u;
             for (uint32_t o = 0; o < over; ++o) {
                 const float4 e = __ldcg(&d.hash_over[o].pos);
-                const uint32_t b = __ldcg(&d.hash_over[o].meta.x);
+                const uint32_t b = __float_as_uint(e.w);
                 if (b == a) continue;
                 const V3 diff = xyz(e) - xyz(p);
                 const float L = len3(diff);
                 if (L >= target || L < 1.0e-12f) continue;
-                const float den = p.w + e.w;
+                const float den = p.w + px(ctx, b).w;
                 if (den <= 0.0f) continue;
                 if (local_pair(d, a, b)) continue;
                 const V3 corr = diff * ((target - L) / (L * den));
