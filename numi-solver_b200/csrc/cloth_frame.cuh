@@ -907,14 +907,10 @@ __device__ void self_solve(Ctx& ctx, uint32_t it) {
         for (uint32_t q = 0; q < 8u; ++q)
             bk[q] = cell_bucket(base[0] + ((q & 1u) ? step[0] : 0), base[1] + ((q & 2u) ? step[1] : 0),
                                 base[2] + ((q & 4u) ? step[2] : 0), d.hash_mask);
-#pragma unroll
-        for (uint32_t q = 0; q < 8u; ++q) hd[q] = l1 ? __ldca(d.hash_head + bk[q]) : __ldcg(d.hash_head + bk[q]);
-        // candidates per bucket (a bucket met twice counts once)
-        uint32_t pre[9];
-        pre[0] = 0u;
         // A neighbour cell farther than the contact distance (half a cell)
         // cannot hold a contact.  The margin covers the rounding of the cell
         // coordinates: 1e-3 cells plus a few ulps of the largest coordinate.
+        // Only the heads of near cells are read.
         const float slack =
             0.5f + 1.0e-3f + 2.4e-7f * fmaxf(fabsf(coord[0]), fmaxf(fabsf(coord[1]), fabsf(coord[2])));
         const float reach2 = slack * slack;
@@ -923,6 +919,13 @@ __device__ void self_solve(Ctx& ctx, uint32_t it) {
         for (uint32_t q = 0; q < 8u; ++q) {
             const float g2 = ((q & 1u) ? gap2[0] : 0.0f) + ((q & 2u) ? gap2[1] : 0.0f) + ((q & 4u) ? gap2[2] : 0.0f);
             near[q] = q == 0u || g2 < reach2;
+            hd[q] = !near[q] ? 0ull : l1 ? __ldca(d.hash_head + bk[q]) : __ldcg(d.hash_head + bk[q]);
+        }
+        // candidates per bucket (a bucket met twice counts once)
+        uint32_t pre[9];
+        pre[0] = 0u;
+#pragma unroll
+        for (uint32_t q = 0; q < 8u; ++q) {
             bool repeat = false;
 #pragma unroll
             for (uint32_t e = 0; e < q; ++e) repeat = repeat || (near[e] && bk[e] == bk[q]);
