@@ -1363,6 +1363,13 @@ __device__ void yarn_friction_sweep(Ctx& ctx) {
     __shared__ unsigned long long s_sum[6u * NC_MAX_FRUITS];
     __shared__ float4 s_vw[NC_MAX_FRUITS];   // velocity xyz, inverse mass
     __shared__ float4 s_or[NC_MAX_FRUITS];   // spin xyz, radius
+    // this thread's first listed segment, loaded once for all colours (the
+    // colours then wait only on their particle loads; the loads overlap the
+    // fruit staging); further ones (more segments listed than threads) are
+    // loaded in their colour
+    const uint32_t listed = min(__ldcg(d.yarn_list_n), d.d_count);
+    FrictionSeg mine{};
+    if (threadIdx.x < listed) mine = friction_seg(d, __ldcg(d.yarn_list + threadIdx.x));
     cta_sums_clear(s_sum, 6u * d.f_count);
     for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
         const NumiClothFruit& fr = d.fruits[f];
@@ -1372,12 +1379,6 @@ __device__ void yarn_friction_sweep(Ctx& ctx) {
         s_or[f] = make_float4(om.x, om.y, om.z, __ldcg(&fr.previousAndRadius.w));
     }
     __syncthreads();
-    const uint32_t listed = min(__ldcg(d.yarn_list_n), d.d_count);
-    // this thread's first listed segment, loaded once for all colours (the
-    // colours then wait only on their particle loads); further ones (more
-    // segments listed than threads) are loaded in their colour
-    FrictionSeg mine{};
-    if (threadIdx.x < listed) mine = friction_seg(d, __ldcg(d.yarn_list + threadIdx.x));
     for (uint32_t b = 0; b < d.n_dist_batches; ++b) {
         const Batch bt = d.dist_batches[b];
         if (bt.yarn == 0u) continue;
@@ -1390,15 +1391,14 @@ __device__ void yarn_friction_sweep(Ctx& ctx) {
         }
         __syncthreads();
     }
+    // the fruits' velocities and spins with the friction sums, handed to the
+    // fruit tail in shared memory (the fruit CTA's own fruit state)
     for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
-        NumiClothFruit& fr = d.fruits[f];
         unsigned long long sm[6];
         for (int k = 0; k < 6; ++k) sm[k] = s_sum[6u * f + k];
-        const numi_float4 v = fr.velocityAndGroundImpulse;
-        const numi_float4 w = fr.angularVelocity;
-        fr.velocityAndGroundImpulse =
-            nf4<numi_float4>(v.x + from_fixed(sm[0]), v.y + from_fixed(sm[1]), v.z + from_fixed(sm[2]), v.w);
-        fr.angularVelocity = nf4<numi_float4>(w.x + from_fixed(sm[3]), w.y + from_fixed(sm[4]), w.z + from_fixed(sm[5]), w.w);
+        const float4 v = s_vw[f], w = s_or[f];
+        ctx.fs->v[f] = make_float4(v.x + from_fixed(sm[0]), v.y + from_fixed(sm[1]), v.z + from_fixed(sm[2]), v.w);
+        ctx.fs->o[f] = make_float4(w.x + from_fixed(sm[3]), w.y + from_fixed(sm[4]), w.z + from_fixed(sm[5]), w.w);
     }
     __syncthreads();
 }
@@ -1526,12 +1526,14 @@ __device__ void release_masks(Ctx& ctx) {
 // then ground friction, rolling resistance and orientation per fruit; the
 // pair impulses of a launch's last substep are published to global memory
 // for readback.
-__device__ void fruit_tail(Ctx& ctx, bool last) {
+__device__ void fruit_tail(Ctx& ctx, bool last, bool staged) {
     if (!ctx.fruit_cta) return;
     const DeviceCloth& d = ctx.d;
     const SubCfg& c = ctx.c;
     FruitShared& fs = *ctx.fs;
-    for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
+    // velocities and spins: staged by the fruit/yarn friction sweep, else
+    // from the fruit records
+    for (uint32_t f = threadIdx.x; f < d.f_count && !staged; f += blockDim.x) {
         const NumiClothFruit& fr = d.fruits[f];
         fs.v[f] = make_float4(fr.velocityAndGroundImpulse.x, fr.velocityAndGroundImpulse.y,
                               fr.velocityAndGroundImpulse.z, fr.positionAndInverseMass.w);
@@ -1726,8 +1728,9 @@ __device__ __forceinline__ bool substep(Ctx& ctx, bool last) {
         edge_friction(ctx);   // yarn/yarn self friction (tools/cloth_bag.cpp:3995-4090)
         NC_SYNC(ctx);
     }
-    if (s.frictions && d.f_count > 0u) yarn_friction_sweep(ctx);   // fruit CTA, no grid barrier
-    fruit_tail(ctx, last);
+    const bool friction_sweep = s.frictions && d.f_count > 0u;
+    if (friction_sweep) yarn_friction_sweep(ctx);   // fruit CTA, no grid barrier
+    fruit_tail(ctx, last, friction_sweep);
     if (ctx.ranks > 1u && ctx.grip_cta && !last) {   // the next substep's grip attach
         Ctx next = ctx;
         next.c = nc::load_cfg(d.cfg + s.cfg_offset + ctx.sub + 1u);
