@@ -142,3 +142,49 @@ class Calibration:
         final, _, _, rough = self.evaluate(logc, damp)
         history.append(final.copy())
         return {"logc": logc, "damping": damp, "loss": final, "history": np.array(history), "nonsmooth": rough}
+
+
+def adjoint_observations(solver: ClothSolver, configs: np.ndarray, schedule: Schedule, observables,
+                         parameters=None, split: str = "calibration", trial: str = "trial", measured=None,
+                         sigma: float = 1.0, checkpoint_every: int = 8) -> tuple[list[str], str]:
+    """Rows of the calibration qualifier's observation CSV
+    (numi_cloth.qualify; tools/cloth_calibration.cpp:213-297) for one trial,
+    with the `dlog_` sensitivity columns made by the adjoint instead of
+    central finite differences.
+
+    observables: (name, particle, axis) triples, each the particle's axis
+    coordinate at the end of the rollout; parameters: (name, [compliance
+    group indices]) pairs, default one per compliance group, each the log
+    scale of the groups' compliances.  baseline is the forward value, measured
+    the given values (default: the baseline), sigma the given one.  The
+    solver state is left as it was.  Returns (parameter names, CSV text).
+
+    One reverse sweep per observable: the rollout loss is the squared
+    distance of the tracked particle to a target, and with the target half a
+    unit below the forward position along the axis, d loss / d theta is
+    exactly d coordinate / d theta."""
+    configs = np.ascontiguousarray(configs)
+    groups = solver.compliance_groups()
+    if parameters is None:
+        parameters = [(f"{fam}_{value:.6g}", [g]) for g, (fam, value) in enumerate(groups)]
+    n = len(configs)
+    slot = 1
+    solver.snapshot(slot)
+    solver.step(configs, schedule)
+    x = solver.particles()["positionAndInverseMass"][:, :3].astype(np.float64)
+    solver.restore(slot)
+    rows = []
+    for k, (name, particle, axis) in enumerate(observables):
+        target = x[particle].copy()
+        target[axis] -= 0.5
+        r = solver.rollout_grad(configs, schedule, np.array([particle], np.uint32), target.reshape(1, 1, 3), n,
+                                checkpoint_every)
+        solver.restore(slot)
+        sens = [float(sum(r["grads"][g] for g in gs)) for _, gs in parameters]
+        base = float(x[particle, axis])
+        meas = base if measured is None else float(measured[k])
+        rows.append(",".join([trial, split, name, repr(meas), repr(float(sigma)), repr(base)] +
+                             [repr(v) for v in sens]))
+    names = [p for p, _ in parameters]
+    header = "trial_id,split,observable,measured,sigma,baseline" + "".join(f",dlog_{p}" for p in names)
+    return names, header + "\n" + "\n".join(rows) + "\n"

@@ -2,6 +2,7 @@
 # Builds, from the reference sources where they lie, into oracle/_ref/:
 #   cloth_bag      the reference FP64 CPU cloth executable (tools/cloth_bag.cpp)
 #   libref_shim.so the same source behind the C API of ref_shim.cpp
+#   cloth_calibration the reference calibration qualifier (tools/cloth_calibration.cpp)
 # Nothing here is copied into the repository; _ref/ is git-ignored.
 REFERENCE ?= /root/reference
 CXX ?= g++
@@ -9,9 +10,13 @@ HERE := $(abspath $(dir $(lastword $(MAKEFILE_LIST))))
 OUT := $(HERE)/_ref
 FLAGS := -std=c++23 -O3 -I$(REFERENCE)/include -I$(REFERENCE)
 
-all: $(OUT)/cloth_bag $(OUT)/libref_shim.so
+all: $(OUT)/cloth_bag $(OUT)/libref_shim.so $(OUT)/cloth_calibration
 
 $(OUT)/cloth_bag: $(REFERENCE)/tools/cloth_bag.cpp
+	@mkdir -p $(OUT)
+	$(CXX) $(FLAGS) $< -o $@
+
+$(OUT)/cloth_calibration: $(REFERENCE)/tools/cloth_calibration.cpp
 	@mkdir -p $(OUT)
 	$(CXX) $(FLAGS) $< -o $@
 
