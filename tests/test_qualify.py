@@ -144,3 +144,21 @@ def test_adjoint_fed_qualification(tmp_path):
     assert text.startswith("schema=numi.cloth.material.v1\n")
     for n, b, d in zip(names, base, truth):
         assert f"{n}=" in text
+
+
+def test_material_artifact_loads(tmp_path):
+    """The qualified full-contract artifact (19 parameters, the reference
+    runtime check's case) loads through the library's material reader, as
+    the reference feeds it back to its simulator."""
+    import numi_cloth as nc
+
+    text = CASES["full_contract"]["material"]
+    path = tmp_path / "material.txt"
+    path.write_text(text)
+    m = nc.load_material(str(path))
+    values = dict(l.split("=", 1) for l in text.strip().split("\n")[3:])
+    assert len(values) == 19
+    for name, v in values.items():
+        head, *rest = name.split("_")
+        field = head + "".join(w[:1].upper() + w[1:] for w in rest)   # the record's field name
+        assert abs(getattr(m, field) - float(v)) <= 1e-12 * max(1.0, abs(float(v))), name
