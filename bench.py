@@ -313,6 +313,65 @@ def calibration_leg(nc, torch, stream, candidates: int, steps: int, plain_sample
             "note": "fruit contact and cloth/ground friction are not differentiated; their events are counted"}
 
 
+BAG_SCHEDULE = dict(iterations=1, strainSweeps=3, reconcilePasses=8, finalPasses=2, certificatePasses=128,
+                    earlyExit=1, selfCollision=1, aerodynamics=1, sweptGround=1, sweptFruitYarn=1, frictions=1,
+                    release=1)
+
+
+def bag_leg(nc, torch, stream, frames: int, ref_frames: int) -> dict:
+    """The produce bag (1,465 particles, 12 fruits) on the recorded lift under
+    the reference's full schedule (strain sweeps, reconciliation, final and
+    certificate passes, swept contact, air, frictions, release), 48 substeps
+    of 1/2880 s per frame, one launch per frame: frames 1..frames after one
+    warm-up frame, with the edge/edge yarn self-collision family on and off.
+    The CPU baseline runs the compiled reference executable (built from
+    tools/cloth_bag.cpp into oracle/_ref) on the first ref_frames frames of
+    the same run, one core."""
+    import subprocess
+    import time
+
+    dt = 1.0 / 2880.0
+    scene = nc.bag_scene(scenario="recorded", timestep=dt)
+    lift = os.path.join(ROOT, "tests", "golden", "lift-v1.csv")
+    traj = nc.GripTrajectory(lift)
+    cfgs = [traj.configs(scene.config, scene.handle_base, f * SUBSTEPS, SUBSTEPS, dt) for f in range(frames + 1)]
+    out = {"metric": "ms per bag frame (reference full schedule, 48 substeps)", "frames": frames,
+           "schedule": BAG_SCHEDULE}
+    for key, prim in (("ms_per_frame", 1), ("ms_per_frame_no_edge", 0)):
+        sv = nc.ClothSolver(scene)
+        sv.set_stream(stream.cuda_stream)
+        sched = nc.Schedule.make(**dict(BAG_SCHEDULE, primitiveSelf=prim))
+        sv.step(cfgs[0], sched)
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for f in range(1, frames + 1):
+            sv.step(cfgs[f], sched)
+        b.record(stream)
+        b.synchronize()
+        out[key] = a.elapsed_time(b) / frames
+        out["failure" if prim else "failure_no_edge"] = nc.failure_names(sv.failure())
+        if prim:
+            out["edge_contacts"] = sv.edge_contacts()
+        sv.close()
+    exe = os.path.join(ROOT, "oracle", "_ref", "cloth_bag")
+    if ref_frames > 0 and os.path.exists(exe):
+        t = time.perf_counter()
+        # the executable runs the frames twice (its determinism replay)
+        p = subprocess.run([exe, "--scenario", "recorded", "--grip-trajectory", lift, "--steps", str(ref_frames),
+                            "--substeps", str(SUBSTEPS), "--iterations", "1", "--replays", "2",
+                            "--timestep", repr(1.0 / 60.0)], capture_output=True, text=True)
+        seconds = time.perf_counter() - t
+        if p.returncode == 0:
+            out["cpu_baseline"] = {"value": 1000.0 * seconds / (2 * ref_frames), "unit": "ms per frame",
+                                   "cores": 1, "kind": "reference",
+                                   "sample": f"frames 0..{ref_frames - 1} of the same run twice (the "
+                                             f"executable's determinism replay), compiled reference executable, "
+                                             f"{seconds:.1f} s wall including start-up"}
+    return out
+
+
 def dist_info():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -452,6 +511,10 @@ def run_ours(args):
     if world == 1 and not args.no_calibration:
         calibration = calibration_leg(nc, torch, stream, args.calib_candidates, args.calib_steps, 4)
 
+    bag = None
+    if world == 1 and not args.no_bag:
+        bag = bag_leg(nc, torch, stream, args.bag_frames, 0 if args.no_cpu else args.bag_frames + 1)
+
     cpu = None
     if rank == 0 and not args.no_cpu:
         r = cpu_sample(args.cpu_seconds, 1)
@@ -481,6 +544,7 @@ def run_ours(args):
                     "d2h_bytes_per_step": int(d2h)},
             "batched": batched,
             "calibration": calibration,
+            "bag": bag,
             "gpu_launches": args.steps,
             "clocks": clocks.summary(),
             "failure": nc.failure_names(fail),
@@ -509,6 +573,8 @@ def main():
     ap.add_argument("--no-calibration", action="store_true")
     ap.add_argument("--calib-candidates", type=int, default=256)
     ap.add_argument("--calib-steps", type=int, default=50)
+    ap.add_argument("--no-bag", action="store_true")
+    ap.add_argument("--bag-frames", type=int, default=10)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
