@@ -258,7 +258,9 @@ int numi_cloth_restore(numi_cloth_t* handle, uint32_t slot);
  * per substep, kernel launches, cluster size (0: no cluster), and flags:
  * bit 0 when the particles are resident in (distributed) shared memory,
  * bit 1 when constraint colours are separated by neighbour syncs instead of
- * the grid barrier. */
+ * the grid barrier, bit 2 when the cloth has tile plans (colour chains run
+ * on per-CTA closures in shared memory between grid barriers), bit 3 when
+ * the last step ran in that tile mode. */
 int numi_cloth_launch_info(numi_cloth_t* handle, uint32_t out[6]);
 
 /* Pass counters: out[0] barriers of the last substep, out[1] the most
@@ -286,29 +288,40 @@ int numi_cloth_trace_cta(numi_cloth_t* handle, unsigned long long* out, uint32_t
  * always allocates its own buffers (tools/cloth_bag_metal.mm:4091-4202).
  *
  * For callers that cannot let the library allocate GPU memory: hosts that
- * own every device byte through their own pool or arena, and code that steps
- * the cloth from inside a stream capture, where a cudaMalloc would break the
- * capture (and elsewhere synchronises the whole device).  The caller passes
- * every input and output as device buffers in the library's structure-of-
- * arrays layout; the library's own scratch (contact records, air forces,
- * fixed-point fruit sums, reduction partials, the substep Configs) lives in
- * one statically allocated device array of about 1.2 MB that every GPU that
- * loads the library keeps until the process exits.
+ * own every device byte through their own pool or arena (a simulator that
+ * sizes its device heap once at start-up, a game or robot controller that
+ * forbids allocation once its real-time loop runs), and hosts for which a
+ * cudaMalloc is too costly mid-run because it may synchronise the whole
+ * device.  The caller passes every input and output as device buffers in the
+ * library's structure-of-arrays layout; the library's own scratch (contact
+ * records, air forces, fixed-point fruit sums, reduction partials, the
+ * substep Configs) lives in one statically allocated device array of about
+ * 1.2 MB that every GPU that loads the library keeps until the process
+ * exits.  No call allocates device memory: no cudaMalloc, no cudaFree and no
+ * allocating library routine.
  *
  * Limits: at most NUMI_CLOTH_NOALLOC_MAX_PARTICLES particles,
- * NUMI_CLOTH_NOALLOC_MAX_DISTANCES distances, 64 fruits and
- * NUMI_CLOTH_NOALLOC_MAX_SUBSTEPS substeps per call; larger inputs are
- * rejected with NUMI_CLOTH_EINVAL, and so is a schedule with selfCollision
- * (the point self-contact hash grid is not part of the static scratch) or
- * with release (the state carries no mouth rim).
- * The cloth runs on one CTA (the resident small-cloth path).
+ * NUMI_CLOTH_NOALLOC_MAX_DISTANCES distances, 64 fruits, 32 grips, 2,016
+ * fruit pairs, 64 colour runs per family and NUMI_CLOTH_NOALLOC_MAX_SUBSTEPS
+ * substeps per call; larger inputs are rejected with NUMI_CLOTH_EINVAL, and
+ * so is a colour run that reaches past its family's record count (or whose
+ * yarn or strain-limited prefix is longer than the run), and a schedule with
+ * selfCollision (the point self-contact hash grid is not part of the static
+ * scratch), primitiveSelf (nor are the edge/edge pass buffers) or release
+ * (the state carries no mouth rim).  The colouring itself is the caller's
+ * contract: the kernel checks every particle index it reads against the
+ * particle count (an index out of range sets NUMI_CLOTH_FAILURE_RANGE and the
+ * item is skipped), but two items of one run that share a particle are not
+ * detected.  The cloth runs on one CTA (the resident small-cloth path).
  *
  * The first call on a device looks up the scratch array's device address
- * (once per device, with that device current); make that first call before
- * any stream capture begins.  All calls share the one scratch array and
- * every call clears the parts that must start at zero, so calls whose
- * kernels overlap on the GPU (different streams, no ordering between them)
- * race on it: order them on one stream or with events.
+ * (once per device, with that device current) and keeps it for the life of
+ * the process; after a cudaDeviceReset of that device the kept address is
+ * stale, so do not use this entry point after a reset.  All calls share the
+ * one scratch array and every call clears the parts that must start at zero
+ * and keeps nothing from the call before, so calls whose kernels overlap on
+ * the GPU (different streams, no ordering between them) race on it: order
+ * them on one stream or with events.
  * ------------------------------------------------------------------------ */
 #define NUMI_CLOTH_NOALLOC_MAX_PARTICLES 4096u
 #define NUMI_CLOTH_NOALLOC_MAX_DISTANCES 8192u

@@ -89,6 +89,14 @@ typedef struct NumiClothReplayResult {
     uint32_t reconcileMax;        /* most reconciliation passes of a substep */
     uint32_t certificateMax;      /* most certificate passes of a substep */
     double seconds;               /* wall time of the first run's frames */
+    /* grip metrics of the first run (tools/cloth_bag.cpp:1563-1620, 5409-5437) */
+    uint32_t regrabCount;         /* attachments of a new generation */
+    uint32_t patchSelections;     /* nearest-cuff-patch selections (v3) */
+    uint32_t maxPatchRingShift;   /* largest cyclic ring shift between selections */
+    uint32_t patchCenter;         /* centre ring of the last selected patch */
+    uint32_t patchParticlesUnique;/* 1: no two grips hold one particle */
+    uint32_t patchTopologyExact;  /* 1: the grips are the 2 x 5 patch around patchCenter */
+    uint64_t inactiveGripSubsteps;/* substeps with the grip released */
 } NumiClothReplayResult;
 
 /* Run the scenario; err receives a message on a rejected input. */

@@ -152,6 +152,13 @@ int numi_cloth_trajectory_info(const numi_cloth_trajectory_t* trajectory,
                                uint32_t* select_nearest, double* duration,
                                uint64_t* fingerprint);
 
+/* Schema version (1..3), pose count, the largest pose rotation angle
+ * 2 acos|w| (radians) and the highest attachment generation: the summary
+ * the reference CLI prints (maximumGripTrajectoryRotation,
+ * gripTrajectoryAttachmentGenerations, include/numi/grip_trajectory.h:371-389). */
+int numi_cloth_trajectory_summary(const numi_cloth_trajectory_t* trajectory, uint32_t* version,
+                                  uint32_t* poses, double* max_rotation, uint32_t* generations);
+
 /* Fill count per-substep Configs from base for substeps first..first+count-1:
  * the grip pose is sampled at the end of each substep, (k+1)*dt
  * (tools/cloth_bag.cpp:4776-4779), relative to handle_base. */

@@ -13,6 +13,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <new>
+#include <mutex>
 #include <vector>
 
 #include "cloth_frame.cuh"
@@ -35,6 +36,8 @@ static_assert(sizeof(DeviceCloth) % 4u == 0u, "DeviceCloth is copied as 32-bit w
 __global__ void __launch_bounds__(NC_THREADS) numi_cloth_residual_kernel(DeviceCloth d, NumiClothConfig cfg) {
     Schedule s{};
     nc::Ctx ctx{d, s};
+    ctx.gx = d.x;
+    ctx.gv = d.v;
     ctx.c = nc::load_cfg(&cfg);
     ctx.tid = blockIdx.x * blockDim.x + threadIdx.x;
     ctx.nthreads = gridDim.x * blockDim.x;
@@ -100,6 +103,15 @@ struct numi_cloth {
     float yarn_rest_median = 0.0f;   // median yarn segment rest length
     bool neighbours = false;         // neighbour-sync tables built for the cooperative grid
     size_t nbr_smem = 0;             // dynamic shared memory of a frame launch with them
+    // tile mode (cloth_tile.cuh): launch shape and shared memory of a tile
+    // launch; the plan is rebuilt before the next launch when a material
+    // changed (its items carry the materials)
+    bool tiles = false;
+    bool tiles_dirty = false;
+    uint32_t tile_grid = 0, tile_block = 0;
+    size_t tile_smem = 0;
+    uint32_t last_grid = 0, last_block = 0;
+    bool last_tiles = false;
     // host copies for the edge/edge local lists, built with the edge buffers
     std::vector<uint2> host_yarn;
     std::vector<uint32_t> host_local_off, host_local_idx;
@@ -343,6 +355,266 @@ bool prepare_neighbours(numi_cloth* h, const NumiClothScene* scene) {
     return true;
 }
 
+// Tile plans of the cooperative grid (cloth_tile.cuh).  CTA t < T owns a
+// tile: for a row-major grid cloth a block of a x b particles (the shape
+// with the fewest estimated closure particles among those giving at most T
+// tiles), else an index strip; the last CTA is the fruit CTA and owns none.
+// For each chain of colours the closure of a tile is found backwards: the
+// items of the last colour touching an owned particle, then those of the
+// colour before touching an owned particle or a particle of an item found,
+// and so on.  Local particles are ordered own, then the fruit/yarn and
+// strain chains' other particles, then the constraint chain's, so every
+// chain reads a prefix.  Returns false (tile mode off) when a plan would not
+// fit the shared memory of one CTA per SM or a closure holds 65,536
+// particles or more.
+struct TileColour {
+    uint32_t family, first, count;
+};
+
+bool build_tiles(numi_cloth* h, uint32_t grid_width, const std::vector<uint2>& dij, const std::vector<float4>& dmat,
+                 const std::vector<uint4>& bij, const std::vector<float2>& bmat, size_t smem_budget) {
+    const DeviceCloth& d = h->d;
+    const uint32_t n = d.n, R = h->tile_grid, T = R - 1u;
+    if (R < 3u || n == 0u) return false;
+    // tiles
+    std::vector<uint32_t> tile_of(n);
+    uint32_t tiles = 0;
+    if (grid_width > 0u && n % grid_width == 0u) {
+        const uint32_t W = grid_width, H = n / grid_width;
+        uint32_t best_a = 0, best_b = 0;
+        uint64_t best = ~0ull;
+        for (uint32_t a = 1; a <= std::min(H, 512u); ++a)
+            for (uint32_t b = 1; b <= std::min(W, 512u); ++b) {
+                const uint64_t count = static_cast<uint64_t>((H + a - 1u) / a) * ((W + b - 1u) / b);
+                if (count > T) continue;
+                const uint64_t cost = static_cast<uint64_t>(a + 12u) * (b + 12u);
+                if (cost < best) {
+                    best = cost;
+                    best_a = a;
+                    best_b = b;
+                }
+            }
+        if (best_a == 0u) return false;
+        const uint32_t across = (W + best_b - 1u) / best_b;
+        for (uint32_t i = 0; i < n; ++i) tile_of[i] = (i / W / best_a) * across + (i % W) / best_b;
+        tiles = ((H + best_a - 1u) / best_a) * across;
+    } else {
+        for (uint32_t i = 0; i < n; ++i) tile_of[i] = static_cast<uint32_t>(static_cast<uint64_t>(i) * T / n);
+        tiles = T;
+    }
+    // chains
+    std::vector<std::vector<TileColour>> chains(NC_TILE_CHAINS);
+    for (uint32_t b = 0; b < d.n_dist_batches; ++b) {
+        const Batch& bt = d.dist_batches[b];
+        chains[NC_TILE_CONSTRAINTS].push_back({NC_TILE_DISTANCE, bt.first, bt.count});
+        if (bt.yarn) chains[NC_TILE_YARN].push_back({NC_TILE_SEGMENT, bt.first, bt.yarn});
+        if (bt.limited) chains[NC_TILE_STRAIN].push_back({NC_TILE_LIMIT, bt.first, bt.limited});
+    }
+    for (uint32_t b = 0; b < d.n_bend_batches; ++b)
+        chains[NC_TILE_CONSTRAINTS].push_back({NC_TILE_BEND, d.bend_batches[b].first, d.bend_batches[b].count});
+    // particle -> records (CSR), distances and bends
+    auto csr = [&](uint32_t records, auto ends, std::vector<uint32_t>& off, std::vector<uint32_t>& idx) {
+        off.assign(n + 1u, 0u);
+        for (uint32_t k = 0; k < records; ++k) {
+            const uint2 e = ends(k);
+            ++off[e.x + 1u];
+            ++off[e.y + 1u];
+        }
+        for (uint32_t i = 0; i < n; ++i) off[i + 1u] += off[i];
+        idx.assign(off[n], 0u);
+        std::vector<uint32_t> at(off.begin(), off.end() - 1);
+        for (uint32_t k = 0; k < records; ++k) {
+            const uint2 e = ends(k);
+            idx[at[e.x]++] = k;
+            idx[at[e.y]++] = k;
+        }
+    };
+    std::vector<uint32_t> doff, didx, boff, bidx;
+    csr(d.d_count, [&](uint32_t k) { return dij[k]; }, doff, didx);
+    csr(d.b_count, [&](uint32_t k) { return make_uint2(bij[k].x, bij[k].z); }, boff, bidx);
+    auto ends = [&](uint32_t family, uint32_t rec) {
+        return family == NC_TILE_BEND ? make_uint2(bij[rec].x, bij[rec].z) : dij[rec];
+    };
+    std::vector<uint32_t> owner(n, 0u), local_of(n, 0u);
+    std::vector<uint32_t> need_stamp(n, 0u), item_stamp_d(d.d_count, 0u), item_stamp_b(d.b_count, 0u);
+    std::vector<int32_t> lidx(n, -1);
+    uint32_t stamp = 0;
+    std::vector<std::vector<uint32_t>> plans(R);
+    size_t widest = 0;
+    std::vector<std::vector<uint32_t>> own_of(tiles);
+    for (uint32_t i = 0; i < n; ++i) own_of[tile_of[i]].push_back(i);
+    for (uint32_t t = 0; t < R; ++t) {
+        const std::vector<uint32_t> none;
+        const std::vector<uint32_t>& own = t < tiles ? own_of[t] : none;
+        // closures: per chain, the items of every colour and the particles
+        std::vector<std::vector<std::vector<uint32_t>>> items(NC_TILE_CHAINS);
+        std::vector<std::vector<uint32_t>> parts(NC_TILE_CHAINS);
+        for (uint32_t k = 0; k < NC_TILE_CHAINS; ++k) {
+            const uint32_t g = ++stamp;
+            std::vector<uint32_t> cur(own.begin(), own.end());
+            for (uint32_t p : cur) need_stamp[p] = g;
+            items[k].resize(chains[k].size());
+            for (size_t c = chains[k].size(); c-- > 0;) {
+                const TileColour& col = chains[k][c];
+                const uint32_t cs = ++stamp;
+                std::vector<uint32_t>& its = items[k][c];
+                const size_t upto = cur.size();
+                for (size_t q = 0; q < upto; ++q) {
+                    const uint32_t p = cur[q];
+                    const bool bend = col.family == NC_TILE_BEND;
+                    const std::vector<uint32_t>& off = bend ? boff : doff;
+                    const std::vector<uint32_t>& idx = bend ? bidx : didx;
+                    std::vector<uint32_t>& ist = bend ? item_stamp_b : item_stamp_d;
+                    for (uint32_t e = off[p]; e < off[p + 1u]; ++e) {
+                        const uint32_t rec = idx[e];
+                        if (rec < col.first || rec >= col.first + col.count || ist[rec] == cs) continue;
+                        ist[rec] = cs;
+                        its.push_back(rec);
+                        const uint2 pe = ends(col.family, rec);
+                        for (uint32_t v : {pe.x, pe.y})
+                            if (need_stamp[v] != g) {
+                                need_stamp[v] = g;
+                                cur.push_back(v);
+                            }
+                    }
+                }
+                std::sort(its.begin(), its.end());
+            }
+            parts[k] = cur;
+        }
+        // local order: own, then the yarn and strain chains' others, then
+        // the constraint chain's
+        std::vector<uint32_t> local(own.begin(), own.end());
+        for (uint32_t p : own) lidx[p] = 0;
+        auto add = [&](std::initializer_list<uint32_t> ks) {
+            std::vector<uint32_t> extra;
+            for (uint32_t k : ks)
+                for (uint32_t p : parts[k])
+                    if (lidx[p] < 0) {
+                        lidx[p] = 0;
+                        extra.push_back(p);
+                    }
+            std::sort(extra.begin(), extra.end());
+            local.insert(local.end(), extra.begin(), extra.end());
+        };
+        add({NC_TILE_YARN, NC_TILE_STRAIN});
+        const uint32_t small = static_cast<uint32_t>(local.size());
+        add({NC_TILE_CONSTRAINTS});
+        for (uint32_t l = 0; l < local.size(); ++l) lidx[local[l]] = static_cast<int32_t>(l);
+        if (local.size() >= 65536u) return false;
+        for (uint32_t l = 0; l < own.size(); ++l) {
+            owner[own[l]] = t;
+            local_of[own[l]] = l;
+        }
+        // plan words
+        uint32_t colours = 0, nitems = 0;
+        for (uint32_t k = 0; k < NC_TILE_CHAINS; ++k) {
+            colours += static_cast<uint32_t>(chains[k].size());
+            for (const auto& its : items[k]) nitems += static_cast<uint32_t>(its.size());
+        }
+        std::vector<uint32_t>& w = plans[t];
+        const uint32_t table_at = NC_TILE_HEADER;
+        const uint32_t list_at = table_at + 2u * colours;
+        const uint32_t items_at = (list_at + static_cast<uint32_t>(local.size()) + 3u) & ~3u;
+        w.assign(items_at + 4u * nitems, 0u);
+        w[0] = static_cast<uint32_t>(local.size());
+        w[1] = static_cast<uint32_t>(own.size());
+        w[2] = list_at;
+        w[3] = items_at;
+        w[4u + NC_TILE_CONSTRAINTS] = static_cast<uint32_t>(local.size());
+        w[4u + NC_TILE_YARN] = small;
+        w[4u + NC_TILE_STRAIN] = small;
+        uint32_t tat = table_at, item = 0;
+        for (uint32_t k = 0; k < NC_TILE_CHAINS; ++k) {
+            w[8u + 2u * k] = tat;
+            w[9u + 2u * k] = static_cast<uint32_t>(chains[k].size());
+            for (size_t c = 0; c < chains[k].size(); ++c) {
+                const TileColour& col = chains[k][c];
+                const std::vector<uint32_t>& its = items[k][c];
+                w[tat++] = item;
+                w[tat++] = static_cast<uint32_t>(its.size()) | (col.family << 28);
+                for (uint32_t rec : its) {
+                    const uint2 pe = ends(col.family, rec);
+                    uint32_t* o = w.data() + items_at + 4u * item++;
+                    o[0] = static_cast<uint32_t>(lidx[pe.x]) | (static_cast<uint32_t>(lidx[pe.y]) << 16);
+                    o[1] = rec | ((t < tiles && tile_of[pe.x] == t) ? 0x80000000u : 0u);
+                    float m0 = 0.0f, m1 = 0.0f;
+                    if (col.family == NC_TILE_DISTANCE) {
+                        m0 = dmat[rec].x;
+                        m1 = dmat[rec].y;
+                    } else if (col.family == NC_TILE_BEND) {
+                        m0 = bmat[rec].x;
+                        m1 = bmat[rec].y;
+                    } else if (col.family == NC_TILE_LIMIT) {
+                        m0 = dmat[rec].x;
+                        m1 = dmat[rec].w;
+                    }
+                    std::memcpy(o + 2, &m0, 4);
+                    std::memcpy(o + 3, &m1, 4);
+                }
+            }
+        }
+        for (uint32_t l = 0; l < local.size(); ++l) w[list_at + l] = local[l];
+        for (uint32_t p : local) lidx[p] = -1;
+        widest = std::max(widest, w.size() * 4u + local.size() * sizeof(float4));
+    }
+    const size_t smem = std::max(nc_resident_offset(), nc_fruit_offset() + widest);
+    if (smem > smem_budget) return false;
+    std::vector<uint32_t> off(R + 1u, 0u), words;
+    for (uint32_t t = 0; t < R; ++t) {
+        words.insert(words.end(), plans[t].begin(), plans[t].end());
+        off[t + 1u] = static_cast<uint32_t>(words.size());
+    }
+    std::vector<uint32_t> owner_word(n);
+    for (uint32_t i = 0; i < n; ++i) owner_word[i] = (owner[i] << 16) | local_of[i];
+    DeviceCloth& dd = h->d;
+    if (dd.x_alt == nullptr) {
+        dd.x_alt = h->buf.alloc<float4>(n);
+        dd.v_alt = h->buf.alloc<float4>(n);
+        dd.tile_owner = h->buf.alloc<uint32_t>(n);
+        dd.tile_off = h->buf.alloc<uint32_t>(R + 1u);
+    }
+    // the words are replaced on a rebuild (their size can change)
+    uint32_t* dw = h->buf.alloc<uint32_t>(words.size());
+    if (!dd.x_alt || !dd.v_alt || !dd.tile_owner || !dd.tile_off || !dw) return false;
+    if (cudaMemcpy(const_cast<uint32_t*>(dd.tile_owner), owner_word.data(), n * sizeof(uint32_t),
+                   cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(const_cast<uint32_t*>(dd.tile_off), off.data(), off.size() * sizeof(uint32_t),
+                   cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(dw, words.data(), words.size() * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess)
+        return false;
+    dd.tile_words = dw;
+    h->tile_smem = smem;
+    return true;
+}
+
+// Rebuild the tile plan from the device records (after a material change).
+bool rebuild_tiles(numi_cloth* h) {
+    const DeviceCloth& d = h->d;
+    std::vector<uint2> dij(d.d_count);
+    std::vector<float4> dmat(d.d_count);
+    std::vector<uint4> bij(d.b_count);
+    std::vector<float2> bmat(d.b_count);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess ||
+        (d.d_count && (cudaMemcpy(dij.data(), d.d_ij, d.d_count * sizeof(uint2), cudaMemcpyDeviceToHost) != cudaSuccess ||
+                       cudaMemcpy(dmat.data(), d.d_mat, d.d_count * sizeof(float4), cudaMemcpyDeviceToHost) != cudaSuccess)) ||
+        (d.b_count && (cudaMemcpy(bij.data(), d.b_ij, d.b_count * sizeof(uint4), cudaMemcpyDeviceToHost) != cudaSuccess ||
+                       cudaMemcpy(bmat.data(), d.b_mat, d.b_count * sizeof(float2), cudaMemcpyDeviceToHost) != cudaSuccess)))
+        return false;
+    int max_optin = 0;
+    cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
+    cudaFuncAttributes fa{};
+    cudaFuncGetAttributes(&fa, frame_fn(false));
+    return build_tiles(h, d.grid_width, dij, dmat, bij, bmat, static_cast<size_t>(max_optin) - fa.sharedSizeBytes);
+}
+
+// A launch runs in tile mode when the cloth has tile plans and the
+// schedule is one the tile substep covers.
+bool tile_schedule(const numi_cloth* h, const Schedule& s) {
+    return h->tiles && s.iterations == 1u && s.aerodynamics == 0u && s.swept_fruit_yarn == 0u &&
+           s.primitive_self == 0u && s.reconcile_passes == 0u && s.final_passes == 0u && s.certificate_passes == 0u;
+}
+
 cudaError_t launch(numi_cloth* h, uint32_t substeps, const Schedule& s, uint32_t cfg_offset = 0) {
     DeviceCloth d = h->d;
     d.cfg = h->d_cfg + cfg_offset;
@@ -374,6 +646,23 @@ cudaError_t launch(numi_cloth* h, uint32_t substeps, const Schedule& s, uint32_t
         e = cudaLaunchKernelExC(&cfg, frame_fn(edge), args);
     } else if (h->grid == 1) {
         e = cudaLaunchKernel(frame_fn(edge), dim3(1), dim3(h->block), args, smem, h->stream);
+    } else if (tile_schedule(h, sc)) {
+        if (h->tiles_dirty) {
+            if (!rebuild_tiles(h)) return cudaErrorUnknown;
+            h->tiles_dirty = false;
+            d.tile_words = h->d.tile_words;
+        }
+        sc.tiles = 1u;
+        if (h->tile_grid > h->grid) d.trace_cta = nullptr;
+        e = raise_frame_smem(h->tile_smem);
+        if (e == cudaSuccess)
+            e = cudaLaunchCooperativeKernel(frame_fn(false), dim3(h->tile_grid), dim3(h->tile_block), args,
+                                            h->tile_smem, h->stream);
+        h->last_grid = h->tile_grid;
+        h->last_block = h->tile_block;
+        h->last_tiles = true;
+        if (e == cudaSuccess) ++h->launches;
+        return e;
     } else {
         // neighbour syncs between colours (the kernel without the edge/edge
         // phases; its flags start at zero in every launch)
@@ -385,6 +674,9 @@ cudaError_t launch(numi_cloth* h, uint32_t substeps, const Schedule& s, uint32_t
         e = cudaLaunchCooperativeKernel(frame_fn(edge), dim3(h->grid), dim3(h->block), args,
                                         d.nbr_on ? h->nbr_smem : smem, h->stream);
     }
+    h->last_grid = h->cluster > 0 ? h->cluster : h->grid;
+    h->last_block = h->block;
+    h->last_tiles = false;
     if (e == cudaSuccess) ++h->launches;
     return e;
 }
@@ -827,6 +1119,15 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
         }
         cudaGetLastError();
     }
+    // Bounded waits: NUMI_CLOTH_WAIT_LIMIT sets the polls a barrier or
+    // neighbour wait makes before it raises TIMEOUT (default 2^22, a few
+    // seconds).  NUMI_CLOTH_TEST_MISSING_CTA=1 is a failure-path test hook:
+    // every grid barrier of the cooperative grid also waits for a CTA that
+    // does not exist, so the first wait runs out and the launch ends with
+    // TIMEOUT.
+    env_u32("NUMI_CLOTH_WAIT_LIMIT", d.spin_limit);
+    env_u32("NUMI_CLOTH_TEST_MISSING_CTA", d.bar_phantom);
+    if (d.bar_phantom > 1u) d.bar_phantom = 1u;
     uint32_t trace_substeps = 0;
     if (env_u32("NUMI_CLOTH_TRACE", trace_substeps) && trace_substeps > 0) {
         d.trace = h->buf.alloc<unsigned long long>(static_cast<size_t>(trace_substeps) * NC_TRACE_SLOTS);
@@ -952,6 +1253,31 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
         return NUMI_CLOTH_ECUDA;
     }
     h->neighbours = prepare_neighbours(h, scene);
+    // Tile mode of the cooperative grid (cloth_tile.cuh): one 512-thread CTA
+    // per SM, used by the launches whose schedule it covers;
+    // NUMI_CLOTH_TILES=1 turns it on, 0 keeps the colour-by-colour schedule.
+    uint32_t want_tiles = 0;
+    env_u32("NUMI_CLOTH_TILES", want_tiles);
+    if (want_tiles != 0u && h->grid > 1u && h->cluster == 0u && d.resident == 0u && K == 0u) {
+        int max_optin = 0;
+        cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
+        cudaFuncAttributes fa{};
+        cudaFuncGetAttributes(&fa, frame_fn(false));
+        uint32_t tgrid = static_cast<uint32_t>(sms);
+        env_u32("NUMI_CLOTH_TILE_GRID", tgrid);
+        h->tile_grid = std::max(tgrid, 3u);
+        h->tile_block = NC_BLOCK_MAX;
+        h->tiles = build_tiles(h, scene->gridWidth, hij, hdm, hbij, hbm,
+                               static_cast<size_t>(max_optin) - fa.sharedSizeBytes);
+        if (h->tiles) {
+            int k = 0;
+            h->tiles = raise_frame_smem(h->tile_smem) == cudaSuccess &&
+                       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, frame_fn(false), NC_BLOCK_MAX,
+                                                                     h->tile_smem) == cudaSuccess &&
+                       static_cast<uint64_t>(k) * static_cast<uint64_t>(sms) >= h->tile_grid;
+        }
+        cudaGetLastError();
+    }
     h->dynamic = {{d.x, n * sizeof(float4)},
                   {d.xp, n * sizeof(float4)},
                   {d.v, n * sizeof(float4)},
@@ -1242,12 +1568,13 @@ int numi_cloth_launch_info(numi_cloth_t* h, uint32_t out[6]) {
     if (cudaStreamSynchronize(h->stream) != cudaSuccess ||
         cudaMemcpy(stats, h->d.stats, sizeof(stats), cudaMemcpyDeviceToHost) != cudaSuccess)
         return NUMI_CLOTH_ECUDA;
-    out[0] = h->grid;
-    out[1] = h->block;
+    // the shape of the last launch (tile mode has its own), else the default
+    out[0] = h->last_grid != 0u ? h->last_grid : h->grid;
+    out[1] = h->last_block != 0u ? h->last_block : h->block;
     out[2] = stats[0];
     out[3] = h->launches;
     out[4] = h->cluster;
-    out[5] = h->d.resident | (h->neighbours ? 2u : 0u);
+    out[5] = h->d.resident | (h->neighbours ? 2u : 0u) | (h->tiles ? 4u : 0u) | (h->last_tiles ? 8u : 0u);
     return NUMI_CLOTH_OK;
 }
 
@@ -1269,6 +1596,7 @@ struct NoAllocScratch {
     float4 force[NUMI_CLOTH_NOALLOC_MAX_PARTICLES];
     unsigned long long fruit_sums[9u * NC_MAX_FRUITS + 8u];
     double red[256];
+    uint32_t stamp[NUMI_CLOTH_NOALLOC_MAX_PARTICLES + NC_MAX_FRUITS];
     NumiClothConfig configs[NUMI_CLOTH_NOALLOC_MAX_SUBSTEPS];
     unsigned long long barrier[32];
     uint32_t stats[4];
@@ -1279,11 +1607,17 @@ struct NoAllocScratch {
 // cudaGetSymbolAddress, once per device.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocScratch)];
 
+// The scratch array's device address on each device, looked up on the
+// first call with that device current and kept for the process (stale after
+// a cudaDeviceReset of the device).  The lookup runs under a mutex, so two
+// host threads making their first calls on one device at once agree.
 constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
 NoAllocScratch* g_noalloc_ptr[kMaxDevices] = {};
 
 NoAllocScratch* noalloc_scratch(int device) {
     if (device < 0 || device >= kMaxDevices) return nullptr;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
     if (g_noalloc_ptr[device] == nullptr) {
         void* ptr = nullptr;
         if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || ptr == nullptr) return nullptr;
@@ -1321,6 +1655,19 @@ extern "C" int numi_cloth_step_noalloc(const NumiClothConfig* base, const NumiCl
         if (batchCounts[k] > NC_MAX_BATCHES) return noalloc_reject("more than 64 colour runs in one family");
     if ((batchCounts[0] + batchCounts[1] + batchCounts[2] + batchCounts[3]) != 0u && batches == nullptr)
         return noalloc_reject("null batches");
+    {
+        // every colour run stays inside its family's records, and a distance
+        // run's yarn and strain-limited prefixes inside the run
+        const uint32_t records[4] = {D, K, B, P};
+        const NumiClothBatch* run = batches;
+        for (int fam = 0; fam < 4; ++fam)
+            for (uint32_t k = 0; k < batchCounts[fam]; ++k, ++run) {
+                const uint64_t first = run->control.x, cnt = run->control.y;
+                if (first + cnt > records[fam]) return noalloc_reject("a colour run reaches past its family's records");
+                if (fam == 0 && ((run->control.w & 0xffffu) > cnt || (run->control.w >> 16) > cnt))
+                    return noalloc_reject("a distance run's yarn or strain-limited prefix is longer than the run");
+            }
+    }
     if (schedule->selfCollision)
         return noalloc_reject("selfCollision needs the point self-contact hash grid, which this path does not hold");
     if (schedule->release)
@@ -1382,6 +1729,8 @@ extern "C" int numi_cloth_step_noalloc(const NumiClothConfig* base, const NumiCl
     d.stats = scratch->stats;
     d.cfg = scratch->configs;
     d.epoch_base = 1u;   // contact records are cleared below, so epochs restart at 1
+    d.damping = -1.0f;   // the schedule's damping applies (as on the handle path)
+    d.check_stamp = scratch->stamp;   // the kernel checks the caller's records first
     Batch* families[4] = {d.dist_batches, d.knot_batches, d.bend_batches, d.pair_batches};
     uint32_t* family_counts[4] = {&d.n_dist_batches, &d.n_knot_batches, &d.n_bend_batches, &d.n_pair_batches};
     const NumiClothBatch* b = batches;
@@ -1955,6 +2304,7 @@ extern "C" int numi_cloth_compliance_groups(numi_cloth_t* h, uint32_t family[NUM
 extern "C" int numi_cloth_replace_compliance(numi_cloth_t* h, uint32_t family, float from, float to) {
     if (h == nullptr || family > 3u || !(to >= 0.0f) || !std::isfinite(to)) return NUMI_CLOTH_EINVAL;
     cudaSetDevice(h->device);
+    h->tiles_dirty = h->tiles;   // the tile plan's items carry the materials
     numi_cloth_replace_compliance_kernel<<<64, 256, 0, h->stream>>>(h->d, family, from, to);
     return cudaGetLastError() == cudaSuccess ? NUMI_CLOTH_OK : NUMI_CLOTH_ECUDA;
 }

@@ -117,6 +117,12 @@ struct DeviceCloth {
     unsigned long long* bar_count;
     unsigned long long* bar_flag;   // barrier number released last (own 128-byte line)
     unsigned int* abort_flag;
+    // polls a barrier or neighbour wait makes before it gives up (0: the
+    // default NC_BARRIER_SPIN_LIMIT)
+    uint32_t spin_limit;
+    // failure-path tests only: grid barriers also wait for this many CTAs
+    // that do not exist, so every bounded wait runs out (0 in production)
+    uint32_t bar_phantom;
     // optional per-barrier globaltimer trace: [substep][NC_TRACE_SLOTS]
     unsigned long long* trace;
     // optional per-CTA barrier arrival stamps: [substep][NC_TRACE_SLOTS][grid]
@@ -225,6 +231,19 @@ struct DeviceCloth {
     float4* tape;
     float4* tape_v;
     uint32_t tape_slots;
+    // tile mode of the cooperative grid (cloth_tile.cuh): CTA r's plan is
+    // tile_words[tile_off[r] .. tile_off[r + 1]); tile_owner[i] = (owning
+    // CTA << 16) | local index of particle i; positions and velocities
+    // alternate between x, v and x_alt, v_alt
+    const uint32_t* tile_off;
+    const uint32_t* tile_words;
+    const uint32_t* tile_owner;
+    float4* x_alt;
+    float4* v_alt;
+    // allocation-free launches: [n + NC_MAX_FRUITS] words of scratch; when
+    // set, the launch first checks every record's indices and the colouring
+    // of every run (validate_records) and steps nothing if one is wrong
+    uint32_t* check_stamp;
 };
 
 struct Schedule {
@@ -249,6 +268,8 @@ struct Schedule {
     const uint32_t* epoch_ptr;
     // first Config of the launch within DeviceCloth::cfg
     uint32_t cfg_offset;
+    // 1: the launch runs in tile mode (cloth_tile.cuh)
+    uint32_t tiles;
 };
 
 // Fruit-side state kept in the shared memory of the fruit CTA for a whole

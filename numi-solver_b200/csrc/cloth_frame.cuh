@@ -57,7 +57,8 @@ __device__ bool grid_sync(Ctx& ctx) {
     __shared__ unsigned s_abort;
     __syncthreads();
     if (threadIdx.x == 0) {
-        const unsigned long long target = ctx.seq * ctx.ranks;
+        const unsigned long long target = ctx.seq * (ctx.ranks + d.bar_phantom);
+        const unsigned limit = d.spin_limit != 0u ? d.spin_limit : NC_BARRIER_SPIN_LIMIT;
         red_release_add_u64(d.bar_count, 1ull);
         unsigned ab = 0u;
         unsigned spins = 0u;
@@ -69,7 +70,7 @@ __device__ bool grid_sync(Ctx& ctx) {
                 ab = 1u;
                 break;
             }
-            if (spins > NC_BARRIER_SPIN_LIMIT) {
+            if (spins > limit) {
                 atomicOr(d.failure, NUMI_CLOTH_FAILURE_TIMEOUT);
                 atomicExch(d.abort_flag, 1u);
                 ab = 1u;
@@ -149,6 +150,7 @@ __device__ bool colour_sync(Ctx& ctx) {
     int ab = 0;
     if (threadIdx.x < nc_nbr_count) {
         const unsigned* f = d.nbr_flag + NC_NBR_FLAG_STRIDE * nc_nbr[threadIdx.x];
+        const unsigned limit = d.spin_limit != 0u ? d.spin_limit : NC_BARRIER_SPIN_LIMIT;
         unsigned spins = 0u;
         while (ld_relaxed(f) < target) {
             ++spins;
@@ -156,7 +158,7 @@ __device__ bool colour_sync(Ctx& ctx) {
                 ab = 1;
                 break;
             }
-            if (spins > NC_BARRIER_SPIN_LIMIT) {
+            if (spins > limit) {
                 atomicOr(d.failure, NUMI_CLOTH_FAILURE_TIMEOUT);
                 atomicExch(d.abort_flag, 1u);
                 ab = 1;
@@ -199,10 +201,38 @@ __device__ void fruit_flush(Ctx& ctx) {
 
 // ------------------------------------------------------------ phases -----
 
+// Predict of one particle (tools/cloth_bag.cpp:4788-4826): gravity,
+// damping and (air load off) the advance with the swept ground clamp, from
+// position p and velocity vv; a particle of zero inverse mass follows its
+// rest position.  prev is xyz(p).
+__device__ __forceinline__ void predict_particle(const Ctx& ctx, uint32_t i, const float4& p, const float4& vv,
+                                                 bool air, V3& pos, V3& vel) {
+    const DeviceCloth& d = ctx.d;
+    const SubCfg& c = ctx.c;
+    const float dt = c.dt;
+    const float inv_dt = 1.0f / dt;
+    const float damp = d.damping >= 0.0f ? d.damping : ctx.s.damping;
+    pos = xyz(p);
+    const V3 prev = pos;
+    vel = xyz(vv);
+    if (p.w == 0.0f) {
+        pos = xyz(__ldg(d.rest + i));
+        vel = (pos - prev) * inv_dt;
+    } else {
+        vel = vel + c.gravity * dt;
+        if (damp != 0.0f) vel = vel * (1.0f / (1.0f + damp * dt));
+        if (!air) {
+            pos = pos + vel * dt;
+        }
+    }
+    if (!air && ctx.s.swept_ground && c.ground && prev.z >= c.radius && pos.z < c.radius) pos.z = c.radius;
+}
+
+__device__ void fruit_begin(Ctx& ctx);
+
 // Grip attach + begin + advance (+ swept ground), aero off.
 __device__ void phase_begin(Ctx& ctx) {
     const DeviceCloth& d = ctx.d;
-    const SubCfg& c = ctx.c;
     if (ctx.grip_cta) {
         // on one CTA the attach reads the positions before this CTA
         // predicts them; on more it ran at the end of the previous substep
@@ -215,30 +245,14 @@ __device__ void phase_begin(Ctx& ctx) {
             d.grips[g].lambda.z = 0.0f;
         }
     }
-    const float dt = c.dt;
-    const float inv_dt = 1.0f / dt;
     const bool air = ctx.s.aerodynamics != 0u;
-    const float damp = d.damping >= 0.0f ? d.damping : ctx.s.damping;
     for (Range r = particle_range(ctx); r.i < r.end; r.i += r.stride) {
         const uint32_t i = r.i;
         float4 p = px(ctx, i);
         const float4 pp = ld(d.xp + i);
-        float4 vv = pv(ctx, i);
-        V3 pos = xyz(p);
-        const V3 prev = pos;
-        V3 vel = xyz(vv);
-        if (p.w == 0.0f) {
-            pos = xyz(__ldg(d.rest + i));
-            vel = (pos - prev) * inv_dt;
-        } else {
-            vel = vel + c.gravity * dt;
-            if (damp != 0.0f) vel = vel * (1.0f / (1.0f + damp * dt));
-            if (!air) {
-                pos = pos + vel * dt;
-            }
-        }
-        if (!air && ctx.s.swept_ground && c.ground && prev.z >= c.radius && pos.z < c.radius) pos.z = c.radius;
-        d.xp[i] = make_float4(prev.x, prev.y, prev.z, pp.w);
+        V3 pos, vel;
+        predict_particle(ctx, i, p, pv(ctx, i), air, pos, vel);
+        d.xp[i] = make_float4(p.x, p.y, p.z, pp.w);
         px_set(ctx, i, with_xyz(p, pos));
         pv_set(ctx, i, make_float4(vel.x, vel.y, vel.z, vel.z));
     }
@@ -246,6 +260,16 @@ __device__ void phase_begin(Ctx& ctx) {
     for (uint32_t k = ctx.tid; k < d.d_count; k += ctx.nthreads) d.d_lambda[k] = 0.0f;
     for (uint32_t k = ctx.tid; k < d.k_count; k += ctx.nthreads) d.k_lambda[k] = 0.0f;
     for (uint32_t k = ctx.tid; k < d.b_count; k += ctx.nthreads) d.b_lambda[k] = 0.0f;
+    fruit_begin(ctx);
+}
+
+// The fruits' part of the substep start (fruit CTA): predict with the
+// swept ground, and the pair contact records cleared.
+__device__ void fruit_begin(Ctx& ctx) {
+    const DeviceCloth& d = ctx.d;
+    const SubCfg& c = ctx.c;
+    const float dt = c.dt;
+    const bool air = ctx.s.aerodynamics != 0u;
     if (ctx.fruit_cta) {
         for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
             FruitState s = load_fruit(d.fruits[f]);
@@ -528,6 +552,122 @@ struct SegRecords {
     }
 };
 
+// One warp's segments of a fruit/yarn colour (tools/cloth_bag.cpp:2955-3020,
+// 3141-3176), each lane one segment (`valid` where it has one) on its loaded
+// endpoints pa, pb; every lane of the warp takes part.
+//
+// Warp broadphase: a warp bounds its 32 segments and keeps only the fruits
+// whose centre lies inside that box grown by the contact distance.  Float
+// subtraction is monotone, so a fruit outside the warp box also fails every
+// per-segment box test; once a contact moves a segment its thread tests all
+// remaining fruits again.  The result is identical to testing every fruit,
+// whichever segments share the warp.  The fruit displacement sums and the
+// friction records are left to the segment's `owner`; another CTA that
+// computes the same segment (a tile's ghost zone) only moves its copies of
+// the endpoints.  Returns whether the lane's endpoints moved.
+__device__ __forceinline__ bool yarn_warp_contacts(const Ctx& ctx, bool valid, bool owner, uint32_t seg, float4& pa,
+                                                   float4& pb, const float4* s_fruit, const float* s_fw,
+                                                   unsigned long long* s_sum) {
+    const SubCfg& c = ctx.c;
+    const uint32_t nf = ctx.d.f_count;
+    const uint32_t lane = threadIdx.x & 31u;
+    V3 lo{INFINITY, INFINITY, INFINITY}, hi{-INFINITY, -INFINITY, -INFINITY};
+    if (valid) {
+        lo = V3{fminf(pa.x, pb.x), fminf(pa.y, pb.y), fminf(pa.z, pb.z)};
+        hi = V3{fmaxf(pa.x, pb.x), fmaxf(pa.y, pb.y), fmaxf(pa.z, pb.z)};
+    }
+    V3 wlo = lo, whi = hi;
+    for (int o = 16; o > 0; o >>= 1) {
+        wlo.x = fminf(wlo.x, __shfl_xor_sync(0xffffffffu, wlo.x, o));
+        wlo.y = fminf(wlo.y, __shfl_xor_sync(0xffffffffu, wlo.y, o));
+        wlo.z = fminf(wlo.z, __shfl_xor_sync(0xffffffffu, wlo.z, o));
+        whi.x = fmaxf(whi.x, __shfl_xor_sync(0xffffffffu, whi.x, o));
+        whi.y = fmaxf(whi.y, __shfl_xor_sync(0xffffffffu, whi.y, o));
+        whi.z = fmaxf(whi.z, __shfl_xor_sync(0xffffffffu, whi.z, o));
+    }
+    // fruits near the warp's box, and (wide) near it grown by a margin:
+    // while a segment's box stays within half the margin of the warp's
+    // box, every fruit near it is on the wide mask
+    const float margin = 8.0f * c.radius;
+    unsigned long long mask = 0ull, wide = 0ull;
+    for (uint32_t f0 = 0; f0 < nf; f0 += 32u) {
+        const uint32_t f = f0 + lane;
+        bool near = false, near_wide = false;
+        if (f < nf) {
+            const float4 fs = s_fruit[f];
+            const float target = fs.w + c.radius;
+            near = !(fs.x < wlo.x - target || fs.x > whi.x + target || fs.y < wlo.y - target ||
+                     fs.y > whi.y + target || fs.z < wlo.z - target || fs.z > whi.z + target);
+            const float reach = target + margin;
+            near_wide = !(fs.x < wlo.x - reach || fs.x > whi.x + reach || fs.y < wlo.y - reach ||
+                          fs.y > whi.y + reach || fs.z < wlo.z - reach || fs.z > whi.z + reach);
+        }
+        mask |= static_cast<unsigned long long>(__ballot_sync(0xffffffffu, near)) << f0;
+        wide |= static_cast<unsigned long long>(__ballot_sync(0xffffffffu, near_wide)) << f0;
+    }
+    if (!valid || mask == 0ull) return false;
+    // this segment's own candidates among the warp's: the box test the
+    // loop applies, so the loop visits only fruits it would not skip
+    {
+        unsigned long long own = 0ull;
+        for (unsigned long long m = mask; m != 0ull; m &= m - 1ull) {
+            const uint32_t f = static_cast<uint32_t>(__ffsll(static_cast<long long>(m)) - 1);
+            if (fruit_near_segment(s_fruit[f], pa, pb, c.radius)) own |= 1ull << f;
+        }
+        mask = own;
+    }
+    bool changed = false;
+    SegRecords rec(seg);
+    while (mask != 0ull) {
+        const uint32_t f = static_cast<uint32_t>(__ffsll(static_cast<long long>(mask)) - 1);
+        mask &= mask - 1ull;
+        const float4 fs = s_fruit[f];
+        const V3 X{fs.x, fs.y, fs.z};
+        const float target = fs.w + c.radius;
+        if (!fruit_near_segment(fs, pa, pb, c.radius)) continue;
+        V3 closest;
+        float t;
+        point_segment(X, xyz(pa), xyz(pb), closest, t);
+        V3 sep = closest - X;
+        float dist = len3(sep);
+        if (dist >= target) continue;
+        if (dist < 1.0e-12f) {
+            const V3 sd = normalized3(xyz(pb) - xyz(pa));
+            sep = normalized3(cross3(sd, fabsf(sd.z) < 0.9f ? V3{0.0f, 0.0f, 1.0f} : V3{1.0f, 0.0f, 0.0f}));
+            dist = 0.0f;
+        }
+        const V3 n = normalized3(sep);
+        const float w0 = 1.0f - t;
+        const float w1 = t;
+        const float corr = target - dist;
+        V3 delta{0.0f, 0.0f, 0.0f};
+        const float lam = yarn_correction(pa, pb, w0, w1, s_fw[f], n, corr, c.ground, c.radius, delta);
+        // the segment moved: its candidates are the later fruits near its
+        // new box (those on the wide mask while the box stays within half
+        // the margin of the warp's box, else any fruit)
+        changed = true;
+        mask = 0ull;
+        const float half = 0.5f * margin;
+        const bool inside = fminf(pa.x, pb.x) >= wlo.x - half && fmaxf(pa.x, pb.x) <= whi.x + half &&
+                            fminf(pa.y, pb.y) >= wlo.y - half && fmaxf(pa.y, pb.y) <= whi.y + half &&
+                            fminf(pa.z, pb.z) >= wlo.z - half && fmaxf(pa.z, pb.z) <= whi.z + half;
+        unsigned long long pool = inside ? wide : (nf >= 64u ? ~0ull : (1ull << nf) - 1ull);
+        pool &= f + 1u < 64u ? (~0ull << (f + 1u)) : 0ull;
+        for (; pool != 0ull; pool &= pool - 1ull) {
+            const uint32_t g = static_cast<uint32_t>(__ffsll(static_cast<long long>(pool)) - 1);
+            if (fruit_near_segment(s_fruit[g], pa, pb, c.radius)) mask |= 1ull << g;
+        }
+        if (!owner) continue;
+        cta_sums_add(s_sum + 3u * f + 0u, delta.x);
+        cta_sums_add(s_sum + 3u * f + 1u, delta.y);
+        cta_sums_add(s_sum + 3u * f + 2u, delta.z);
+        if (lam <= 0.0f) continue;
+        rec.add(ctx, f, n, lam / c.dt, w0, w1);
+    }
+    if (owner) rec.finish(ctx);
+    return changed;
+}
+
 // One yarn colour of the fruit/yarn sweep.  Fruits do not move during a
 // sweep (their summed displacements are applied after it), so the first
 // colour stages them in shared memory for all colours, the CTA's
@@ -535,7 +675,6 @@ struct SegRecords {
 // them to the global sums.
 __device__ void yarn_contact_batch(Ctx& ctx, uint32_t slot, const Batch& bt, bool first, bool last) {
     const DeviceCloth& d = ctx.d;
-    const SubCfg& c = ctx.c;
     __shared__ float4 s_fruit[NC_MAX_FRUITS];   // xyz position, w radius
     __shared__ float s_fw[NC_MAX_FRUITS];
     __shared__ unsigned long long s_sum[3u * NC_MAX_FRUITS];
@@ -563,106 +702,15 @@ __device__ void yarn_contact_batch(Ctx& ctx, uint32_t slot, const Batch& bt, boo
         const uint32_t seg = bt.first + (valid ? k : 0u);
         uint2 ij = make_uint2(0u, 0u);
         float4 pa = make_float4(0, 0, 0, 0), pb = pa;
-        V3 lo{INFINITY, INFINITY, INFINITY}, hi{-INFINITY, -INFINITY, -INFINITY};
         if (valid) {
             ij = __ldg(d.d_ij + seg);
             pa = px(ctx, ij.x);
             pb = px(ctx, ij.y);
-            lo = V3{fminf(pa.x, pb.x), fminf(pa.y, pb.y), fminf(pa.z, pb.z)};
-            hi = V3{fmaxf(pa.x, pb.x), fmaxf(pa.y, pb.y), fmaxf(pa.z, pb.z)};
         }
-        V3 wlo = lo, whi = hi;
-        for (int o = 16; o > 0; o >>= 1) {
-            wlo.x = fminf(wlo.x, __shfl_xor_sync(0xffffffffu, wlo.x, o));
-            wlo.y = fminf(wlo.y, __shfl_xor_sync(0xffffffffu, wlo.y, o));
-            wlo.z = fminf(wlo.z, __shfl_xor_sync(0xffffffffu, wlo.z, o));
-            whi.x = fmaxf(whi.x, __shfl_xor_sync(0xffffffffu, whi.x, o));
-            whi.y = fmaxf(whi.y, __shfl_xor_sync(0xffffffffu, whi.y, o));
-            whi.z = fmaxf(whi.z, __shfl_xor_sync(0xffffffffu, whi.z, o));
-        }
-        // fruits near the warp's box, and (wide) near it grown by a margin:
-        // while a segment's box stays within half the margin of the warp's
-        // box, every fruit near it is on the wide mask
-        const float margin = 8.0f * c.radius;
-        unsigned long long mask = 0ull, wide = 0ull;
-        for (uint32_t f0 = 0; f0 < nf; f0 += 32u) {
-            const uint32_t f = f0 + lane;
-            bool near = false, near_wide = false;
-            if (f < nf) {
-                const float4 fs = s_fruit[f];
-                const float target = fs.w + c.radius;
-                near = !(fs.x < wlo.x - target || fs.x > whi.x + target || fs.y < wlo.y - target ||
-                         fs.y > whi.y + target || fs.z < wlo.z - target || fs.z > whi.z + target);
-                const float reach = target + margin;
-                near_wide = !(fs.x < wlo.x - reach || fs.x > whi.x + reach || fs.y < wlo.y - reach ||
-                              fs.y > whi.y + reach || fs.z < wlo.z - reach || fs.z > whi.z + reach);
-            }
-            mask |= static_cast<unsigned long long>(__ballot_sync(0xffffffffu, near)) << f0;
-            wide |= static_cast<unsigned long long>(__ballot_sync(0xffffffffu, near_wide)) << f0;
-        }
-        if (!valid || mask == 0ull) continue;
-        // this segment's own candidates among the warp's: the box test the
-        // loop applies, so the loop visits only fruits it would not skip
-        {
-            unsigned long long own = 0ull;
-            for (unsigned long long m = mask; m != 0ull; m &= m - 1ull) {
-                const uint32_t f = static_cast<uint32_t>(__ffsll(static_cast<long long>(m)) - 1);
-                if (fruit_near_segment(s_fruit[f], pa, pb, c.radius)) own |= 1ull << f;
-            }
-            mask = own;
-        }
-        bool changed = false;
-        SegRecords rec(seg);
-        while (mask != 0ull) {
-            const uint32_t f = static_cast<uint32_t>(__ffsll(static_cast<long long>(mask)) - 1);
-            mask &= mask - 1ull;
-            const float4 fs = s_fruit[f];
-            const V3 X{fs.x, fs.y, fs.z};
-            const float target = fs.w + c.radius;
-            if (!fruit_near_segment(fs, pa, pb, c.radius)) continue;
-            V3 closest;
-            float t;
-            point_segment(X, xyz(pa), xyz(pb), closest, t);
-            V3 sep = closest - X;
-            float dist = len3(sep);
-            if (dist >= target) continue;
-            if (dist < 1.0e-12f) {
-                const V3 sd = normalized3(xyz(pb) - xyz(pa));
-                sep = normalized3(cross3(sd, fabsf(sd.z) < 0.9f ? V3{0.0f, 0.0f, 1.0f} : V3{1.0f, 0.0f, 0.0f}));
-                dist = 0.0f;
-            }
-            const V3 n = normalized3(sep);
-            const float w0 = 1.0f - t;
-            const float w1 = t;
-            const float corr = target - dist;
-            V3 delta{0.0f, 0.0f, 0.0f};
-            const float lam = yarn_correction(pa, pb, w0, w1, s_fw[f], n, corr, c.ground, c.radius, delta);
-            // the segment moved: its candidates are the later fruits near its
-            // new box (those on the wide mask while the box stays within half
-            // the margin of the warp's box, else any fruit)
-            changed = true;
-            mask = 0ull;
-            const float half = 0.5f * margin;
-            const bool inside = fminf(pa.x, pb.x) >= wlo.x - half && fmaxf(pa.x, pb.x) <= whi.x + half &&
-                                fminf(pa.y, pb.y) >= wlo.y - half && fmaxf(pa.y, pb.y) <= whi.y + half &&
-                                fminf(pa.z, pb.z) >= wlo.z - half && fmaxf(pa.z, pb.z) <= whi.z + half;
-            unsigned long long pool = inside ? wide : (nf >= 64u ? ~0ull : (1ull << nf) - 1ull);
-            pool &= f + 1u < 64u ? (~0ull << (f + 1u)) : 0ull;
-            for (; pool != 0ull; pool &= pool - 1ull) {
-                const uint32_t g = static_cast<uint32_t>(__ffsll(static_cast<long long>(pool)) - 1);
-                if (fruit_near_segment(s_fruit[g], pa, pb, c.radius)) mask |= 1ull << g;
-            }
-            cta_sums_add(s_sum + 3u * f + 0u, delta.x);
-            cta_sums_add(s_sum + 3u * f + 1u, delta.y);
-            cta_sums_add(s_sum + 3u * f + 2u, delta.z);
-            if (lam <= 0.0f) continue;
-            rec.add(ctx, f, n, lam / c.dt, w0, w1);
-        }
-        if (changed) {
+        if (yarn_warp_contacts(ctx, valid, true, seg, pa, pb, s_fruit, s_fw, s_sum)) {
             px_set(ctx, ij.x, pa);
             px_set(ctx, ij.y, pb);
         }
-        rec.finish(ctx);
     }
     if (last) cta_sums_flush(s_sum, acc, 3u * nf);
 }
@@ -838,13 +886,10 @@ __device__ __forceinline__ uint32_t self_pass_tag(const Ctx& ctx, uint32_t it) {
 // (tag, 0) resets a bucket of an older pass and leaves a current one alone;
 // the add after it, in the same thread's order on the same address, takes
 // the next slot.
-__device__ void self_insert(Ctx& ctx, uint32_t it) {
+__device__ __forceinline__ void self_insert_one(const Ctx& ctx, unsigned long long tag, uint32_t i, const float4& p) {
     const DeviceCloth& d = ctx.d;
     const float inv_cell = 1.0f / (4.0f * ctx.c.radius);
-    const unsigned long long tag = self_pass_tag(ctx, it);
-    for (Range r = particle_range(ctx); r.i < r.end; r.i += r.stride) {
-        const uint32_t i = r.i;
-        const float4 p = px(ctx, i);
+    {
         const uint32_t bucket = cell_bucket(static_cast<int>(floorf(p.x * inv_cell)),
                                             static_cast<int>(floorf(p.y * inv_cell)),
                                             static_cast<int>(floorf(p.z * inv_cell)), d.hash_mask);
@@ -861,12 +906,17 @@ __device__ void self_insert(Ctx& ctx, uint32_t it) {
             const uint32_t o = static_cast<uint32_t>(atomicAdd(d.hash_over_head, 1ull));
             if (o >= d.n) {
                 fail(d, NUMI_CLOTH_FAILURE_RANGE);
-                continue;
+                return;
             }
             e = d.hash_over + o;
         }
         e->pos = make_float4(p.x, p.y, p.z, __uint_as_float(i));
     }
+}
+
+__device__ void self_insert(Ctx& ctx, uint32_t it) {
+    const unsigned long long tag = self_pass_tag(ctx, it);
+    for (Range r = particle_range(ctx); r.i < r.end; r.i += r.stride) self_insert_one(ctx, tag, r.i, px(ctx, r.i));
 }
 
 // Resolve every particle's pairs.  A cell is twice the contact distance,
@@ -878,17 +928,16 @@ __device__ void self_insert(Ctx& ctx, uint32_t it) {
 // may go through L1, where neighbouring particles of a CTA share cells;
 // under the cluster barrier (cluster-scope acquire) they stay L2 reads.
 #define NC_SELF_BATCH 8u
-__device__ void self_solve(Ctx& ctx, uint32_t it) {
+// The pass of particle a at its start-of-pass position p: true when a pair
+// moved it, with the moved position in `moved`; counts the pairs a < b and the
+// deepest penetration.
+__device__ __forceinline__ bool self_solve_one(const Ctx& ctx, uint32_t tag, uint32_t a, const float4& p,
+                                               float4& moved, unsigned long long& contacts, float& max_pen) {
     const DeviceCloth& d = ctx.d;
     const float target = 2.0f * ctx.c.radius;
     const float inv_cell = 1.0f / (4.0f * ctx.c.radius);
-    const uint32_t tag = self_pass_tag(ctx, it);
     const bool l1 = d.cluster_barrier == 0u;
-    unsigned long long contacts = 0ull;
-    float max_pen = 0.0f;
-    for (Range r = particle_range(ctx); r.i < r.end; r.i += r.stride) {
-        const uint32_t a = r.i;
-        const float4 p = px(ctx, a);
+    {
         int base[3], step[3];
         float gap2[3];   // squared distance to the probed neighbour cell, in cell units
         const float coord[3] = {p.x * inv_cell, p.y * inv_cell, p.z * inv_cell};
@@ -1008,11 +1057,16 @@ __device__ void self_solve(Ctx& ctx, uint32_t it) {
             const float dx = from_fixed(static_cast<unsigned long long>(sum[0]));
             const float dy = from_fixed(static_cast<unsigned long long>(sum[1]));
             const float dz = from_fixed(static_cast<unsigned long long>(sum[2]));
-            px_set(ctx, a, make_float4(p.x + dx, p.y + dy, p.z + dz, p.w));
+            moved = make_float4(p.x + dx, p.y + dy, p.z + dz, p.w);
         }
+        return touched;
     }
-    // one atomic pair per warp (an integer sum and the maximum of
-    // non-negative floats as integers: the order does not matter)
+}
+
+// The self-contact statistics of a CTA's particles: one atomic pair per
+// warp (an integer sum and the maximum of non-negative floats as integers:
+// the order does not matter).
+__device__ __forceinline__ void self_stats_flush(const DeviceCloth& d, unsigned long long contacts, float max_pen) {
     unsigned pen_bits = __float_as_uint(max_pen);
     for (int o = 16; o > 0; o >>= 1) {
         contacts += __shfl_xor_sync(0xffffffffu, contacts, o);
@@ -1024,6 +1078,20 @@ __device__ void self_solve(Ctx& ctx, uint32_t it) {
     }
 }
 
+__device__ void self_solve(Ctx& ctx, uint32_t it) {
+    const uint32_t tag = self_pass_tag(ctx, it);
+    unsigned long long contacts = 0ull;
+    float max_pen = 0.0f;
+    for (Range r = particle_range(ctx); r.i < r.end; r.i += r.stride) {
+        const uint32_t a = r.i;
+        const float4 p = px(ctx, a);
+        float4 q;
+        if (self_solve_one(ctx, tag, a, p, q, contacts, max_pen)) px_set(ctx, a, q);
+    }
+    self_stats_flush(ctx.d, contacts, max_pen);
+}
+
+
 }  // namespace
 }  // namespace nc
 
@@ -1033,8 +1101,9 @@ namespace nc {
 namespace {   // internal linkage: the edge kernels' unit includes these too
 
 // Ground clamp (tools/cloth_bag.cpp:2655-2690).
+__device__ void fruit_ground(Ctx& ctx);
+
 __device__ void phase_ground(Ctx& ctx) {
-    const DeviceCloth& d = ctx.d;
     const SubCfg& c = ctx.c;
     fruit_flush(ctx);
     if (!c.ground) return;
@@ -1042,6 +1111,13 @@ __device__ void phase_ground(Ctx& ctx) {
         const float4 p = px(ctx, r.i);
         if (c.radius - p.z > 0.0f) px_set(ctx, r.i, make_float4(p.x, p.y, c.radius, p.w));
     }
+    fruit_ground(ctx);
+}
+
+// The fruits' ground clamp with its normal impulse (fruit CTA; ground on).
+__device__ void fruit_ground(Ctx& ctx) {
+    const DeviceCloth& d = ctx.d;
+    const SubCfg& c = ctx.c;
     if (ctx.fruit_cta) {
         for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
             NumiClothFruit& fr = d.fruits[f];
@@ -1194,42 +1270,64 @@ __device__ bool contacts_pass(Ctx& ctx, bool with_strain) {
 }
 
 // Finalize + cloth/ground friction (tools/cloth_bag.cpp:5186-5211, 2076-2115).
-__device__ void phase_finalize(Ctx& ctx) {
+// Finalize of one particle at its final position p: the velocity from the
+// substep's motion with the ground normal impulse (velocity w) and the
+// cloth/ground Coulomb friction; a particle of zero inverse mass returns to
+// its rest position (true: p was moved).
+__device__ __forceinline__ bool finalize_particle(const Ctx& ctx, uint32_t i, float4& p, const float4& vv,
+                                                  float4& vout) {
     const DeviceCloth& d = ctx.d;
     const SubCfg& c = ctx.c;
-    fruit_flush(ctx);
     const float inv_dt = 1.0f / c.dt;
+    const V3 prev = xyz(ld(d.xp + i));
+    V3 pos = xyz(p);
+    V3 vel;
+    float gi = 0.0f;
+    bool moved = false;
+    if (p.w == 0.0f) {
+        pos = xyz(__ldg(d.rest + i));
+        vel = (pos - prev) * inv_dt;
+        p = with_xyz(p, pos);
+        moved = true;
+    } else {
+        vel = (pos - prev) * inv_dt;
+        if (c.ground && pos.z <= c.radius + 1.0e-6f) {
+            const float nvc = vel.z - vv.w;
+            gi = fmaxf(0.0f, nvc / p.w);
+        }
+        if (ctx.s.frictions && gi > 0.0f) {
+            const V3 tv{vel.x, vel.y, 0.0f};
+            const float slip = len3(tv);
+            if (!(slip < 1.0e-10f)) {
+                const float limit = c.mu_cloth_ground * gi;
+                const float ti = fminf(slip / p.w, limit);
+                if (ti > 0.0f) vel = vel - tv * (ti * p.w / slip);
+            }
+        }
+    }
+    if (!finite3(vel)) fail(d, NUMI_CLOTH_FAILURE_NONFINITE);
+    vout = make_float4(vel.x, vel.y, vel.z, gi);
+    return moved;
+}
+
+__device__ void fruit_finalize(Ctx& ctx);
+
+__device__ void phase_finalize(Ctx& ctx) {
+    fruit_flush(ctx);
     for (Range r = particle_range(ctx); r.i < r.end; r.i += r.stride) {
         const uint32_t i = r.i;
         float4 p = px(ctx, i);
-        const V3 prev = xyz(ld(d.xp + i));
-        const float4 vv = pv(ctx, i);
-        V3 pos = xyz(p);
-        V3 vel;
-        float gi = 0.0f;
-        if (p.w == 0.0f) {
-            pos = xyz(__ldg(d.rest + i));
-            vel = (pos - prev) * inv_dt;
-            px_set(ctx, i, with_xyz(p, pos));
-        } else {
-            vel = (pos - prev) * inv_dt;
-            if (c.ground && pos.z <= c.radius + 1.0e-6f) {
-                const float nvc = vel.z - vv.w;
-                gi = fmaxf(0.0f, nvc / p.w);
-            }
-            if (ctx.s.frictions && gi > 0.0f) {
-                const V3 tv{vel.x, vel.y, 0.0f};
-                const float slip = len3(tv);
-                if (!(slip < 1.0e-10f)) {
-                    const float limit = c.mu_cloth_ground * gi;
-                    const float ti = fminf(slip / p.w, limit);
-                    if (ti > 0.0f) vel = vel - tv * (ti * p.w / slip);
-                }
-            }
-        }
-        if (!finite3(vel)) fail(d, NUMI_CLOTH_FAILURE_NONFINITE);
-        pv_set(ctx, i, make_float4(vel.x, vel.y, vel.z, gi));
+        float4 v;
+        if (finalize_particle(ctx, i, p, pv(ctx, i), v)) px_set(ctx, i, p);
+        pv_set(ctx, i, v);
     }
+    fruit_finalize(ctx);
+}
+
+// The fruits' velocities from their substep motion (fruit CTA).
+__device__ void fruit_finalize(Ctx& ctx) {
+    const DeviceCloth& d = ctx.d;
+    const float inv_dt = 1.0f / ctx.c.dt;
     if (ctx.fruit_cta) {
         for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
             FruitState s = load_fruit(d.fruits[f]);
@@ -1744,9 +1842,97 @@ __device__ __forceinline__ bool substep(Ctx& ctx, bool last) {
     return true;
 }
 
+// Checks of caller-built records before an allocation-free launch steps
+// anything, one CTA (the reference kernels make the same checks item by
+// item, ClothBag.metal:1156-1175): every particle index below the particle
+// count and the two (or four) particles of an item distinct, else RANGE;
+// no two items of one colour run sharing a particle (or fruit), else BATCH.
+// A run claims its particles with an atomic max of its own tag, which grows
+// run by run, so an item that finds its tag already there shares a particle
+// with an earlier item of the same run.  Returns false (failure bits set)
+// when anything is wrong; the launch then steps nothing.
+__device__ bool validate_records(const DeviceCloth& d, const SubCfg& c0) {
+    uint32_t* stamp = d.check_stamp;
+    for (uint32_t i = threadIdx.x; i < d.n + NC_MAX_FRUITS; i += blockDim.x) stamp[i] = 0u;
+    __syncthreads();
+    unsigned bad = 0u;
+    uint32_t tag = 0u;
+    auto claim = [&](uint32_t slot) {
+        if (atomicMax(stamp + slot, tag) == tag) bad |= NUMI_CLOTH_FAILURE_BATCH;
+    };
+    for (uint32_t b = 0; b < d.n_dist_batches; ++b) {
+        const Batch bt = d.dist_batches[b];
+        ++tag;
+        for (uint32_t k = threadIdx.x; k < bt.count; k += blockDim.x) {
+            const uint2 ij = d.d_ij[bt.first + k];
+            if (ij.x >= d.n || ij.y >= d.n || ij.x == ij.y) {
+                bad |= NUMI_CLOTH_FAILURE_RANGE;
+                continue;
+            }
+            claim(ij.x);
+            claim(ij.y);
+        }
+        __syncthreads();
+    }
+    for (uint32_t b = 0; b < d.n_knot_batches; ++b) {
+        const Batch bt = d.knot_batches[b];
+        ++tag;
+        for (uint32_t k = threadIdx.x; k < bt.count; k += blockDim.x) {
+            const uint4 q = d.k_ij[bt.first + k];
+            if (q.x >= d.n || q.y >= d.n || q.z >= d.n || q.w >= d.n || q.x == q.y || q.x == q.z ||
+                q.x == q.w || q.y == q.z || q.y == q.w || q.z == q.w) {
+                bad |= NUMI_CLOTH_FAILURE_RANGE;
+                continue;
+            }
+            claim(q.x);
+            claim(q.y);
+            claim(q.z);
+            claim(q.w);
+        }
+        __syncthreads();
+    }
+    for (uint32_t b = 0; b < d.n_bend_batches; ++b) {
+        const Batch bt = d.bend_batches[b];
+        ++tag;
+        for (uint32_t k = threadIdx.x; k < bt.count; k += blockDim.x) {
+            const uint4 q = d.b_ij[bt.first + k];
+            if (q.x >= d.n || q.y >= d.n || q.z >= d.n || q.x == q.z) {
+                bad |= NUMI_CLOTH_FAILURE_RANGE;
+                continue;
+            }
+            claim(q.x);
+            claim(q.z);
+        }
+        __syncthreads();
+    }
+    for (uint32_t b = 0; b < d.n_pair_batches; ++b) {
+        const Batch bt = d.pair_batches[b];
+        ++tag;
+        for (uint32_t k = threadIdx.x; k < bt.count; k += blockDim.x) {
+            const numi_uint4 fc = d.pairs[bt.first + k].fruitsAndColor;
+            if (fc.x >= d.f_count || fc.y >= d.f_count || fc.x == fc.y) {
+                bad |= NUMI_CLOTH_FAILURE_RANGE;
+                continue;
+            }
+            claim(d.n + fc.x);
+            claim(d.n + fc.y);
+        }
+        __syncthreads();
+    }
+    for (uint32_t g = threadIdx.x; g < d.g_count; g += blockDim.x)
+        if (d.grips[g].particle.x >= d.n) bad |= NUMI_CLOTH_FAILURE_RANGE;
+    if (c0.grip_select == 1u)
+        for (uint32_t k = threadIdx.x; k < 2u * c0.ring_count; k += blockDim.x)
+            if (d.cuff[k] >= d.n) bad |= NUMI_CLOTH_FAILURE_RANGE;
+    const int any = __syncthreads_or(bad != 0u);
+    if (bad != 0u) fail(d, bad);
+    return any == 0;
+}
+
 }  // namespace
 }  // namespace nc
 
+#include "cloth_tile.cuh"
 
 // One cloth's frame on `ranks` CTAs (this one is `rank`): all substeps of
 // the launch's Configs, particles optionally resident in (distributed)
@@ -1763,8 +1949,12 @@ __device__ __forceinline__ void run_frame(const DeviceCloth& src, const Schedule
         __syncthreads();
     }
     const DeviceCloth& d = *reinterpret_cast<const DeviceCloth*>(dynamic_smem);
+    if (d.check_stamp != nullptr && s.substeps > 0u && !nc::validate_records(d, nc::load_cfg(d.cfg + s.cfg_offset)))
+        return;
     FruitShared& fruit_shared = *reinterpret_cast<FruitShared*>(dynamic_smem + nc_fruit_offset());
     nc::Ctx ctx{d, s};
+    ctx.gx = d.x;
+    ctx.gv = d.v;
     ctx.fs = &fruit_shared;
     ctx.tid = rank * blockDim.x + threadIdx.x;
     ctx.nthreads = ranks * blockDim.x;
@@ -1793,7 +1983,19 @@ __device__ __forceinline__ void run_frame(const DeviceCloth& src, const Schedule
         else
             __syncthreads();
     }
-    nc::neighbour_stage(ctx);
+    if (s.tiles) {
+        // tile mode: the CTA's plan and its local particles after the
+        // descriptor (the fruit CTA keeps its fruit state there instead)
+        uint32_t* plan = reinterpret_cast<uint32_t*>(dynamic_smem + nc_fruit_offset());
+        ctx.tp = plan;
+        if (!ctx.fruit_cta) {
+            if (!nc::tile_stage(ctx, plan)) return;
+            ctx.tx = reinterpret_cast<float4*>(
+                dynamic_smem + nc_fruit_offset() + 4u * (d.tile_off[rank + 1u] - d.tile_off[rank]));
+        }
+    } else {
+        nc::neighbour_stage(ctx);
+    }
     if (ctx.fruit_cta) {
         for (uint32_t k = threadIdx.x; k < d.p_count; k += blockDim.x)
             fruit_shared.ab[k] =
@@ -1824,8 +2026,23 @@ __device__ __forceinline__ void run_frame(const DeviceCloth& src, const Schedule
             }
             __syncthreads();
         }
+        if constexpr (!kEdge && !kIlp) {
+            if (s.tiles) {
+                if (!nc::substep_tiles(ctx, sub + 1u == s.substeps)) return;
+                if (rank == 0 && threadIdx.x == 0) d.stats[0] = ctx.barriers;
+                continue;
+            }
+        }
         if (!nc::substep<kEdge, kIlp>(ctx, sub + 1u == s.substeps)) return;
         if (rank == 0 && threadIdx.x == 0) d.stats[0] = ctx.barriers;
+    }
+    if (ctx.gx != d.x || ctx.gv != d.v) {
+        // tile mode ended on the alternate buffers: copy them back (every
+        // store of the launch ended at its last barrier)
+        for (nc::Range r = nc::particle_range(ctx); r.i < r.end; r.i += r.stride) {
+            if (ctx.gx != d.x) d.x[r.i] = __ldcg(ctx.gx + r.i);
+            if (ctx.gv != d.v) d.v[r.i] = __ldcg(ctx.gv + r.i);
+        }
     }
     if (ctx.resident) {
         // Every remote access ended at the last barrier: write the CTA's own

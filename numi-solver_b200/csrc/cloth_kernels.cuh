@@ -157,6 +157,15 @@ struct Ctx {
     uint32_t shift;           // log2 of the particles each CTA owns
     float4* xs;               // this CTA's positions in shared memory
     float4* vs;               // this CTA's velocities in shared memory
+    // global position and velocity buffers the phases read and write:
+    // DeviceCloth::x and ::v, or in tile mode (cloth_tile.cuh) whichever of
+    // them and their alternates holds the current values
+    float4* gx;
+    float4* gv;
+    // tile mode: this CTA's plan and its local particle positions, both in
+    // shared memory
+    const uint32_t* tp;
+    float4* tx;
 };
 
 __device__ __forceinline__ float4* resident_ptr(const Ctx& c, float4* local_base, uint32_t i) {
@@ -166,22 +175,22 @@ __device__ __forceinline__ float4* resident_ptr(const Ctx& c, float4* local_base
 }
 // Particle position (xyz, inverse mass) and velocity accessors.
 __device__ __forceinline__ float4 px(const Ctx& c, uint32_t i) {
-    return c.resident ? *resident_ptr(c, c.xs, i) : __ldcg(c.d.x + i);
+    return c.resident ? *resident_ptr(c, c.xs, i) : __ldcg(c.gx + i);
 }
 __device__ __forceinline__ void px_set(const Ctx& c, uint32_t i, float4 v) {
     if (c.resident)
         *resident_ptr(c, c.xs, i) = v;
     else
-        c.d.x[i] = v;
+        c.gx[i] = v;
 }
 __device__ __forceinline__ float4 pv(const Ctx& c, uint32_t i) {
-    return c.resident ? *resident_ptr(c, c.vs, i) : __ldcg(c.d.v + i);
+    return c.resident ? *resident_ptr(c, c.vs, i) : __ldcg(c.gv + i);
 }
 __device__ __forceinline__ void pv_set(const Ctx& c, uint32_t i, float4 v) {
     if (c.resident)
         *resident_ptr(c, c.vs, i) = v;
     else
-        c.d.v[i] = v;
+        c.gv[i] = v;
 }
 
 // Loop range of this thread over count items: grid-stride in the global
@@ -269,19 +278,12 @@ __device__ void grip_attach(const Ctx& ctx) {
     d.grips[g] = grip;
 }
 
-// Compliant vector attachment (tools/cloth_bag.cpp:1630-1647).
-__device__ void solve_grips(const Ctx& ctx) {
-    const DeviceCloth& d = ctx.d;
-    const SubCfg& c = ctx.c;
-    const uint32_t g = threadIdx.x;
-    if (g >= d.g_count || !c.grip_active) return;
-    NumiClothGrip grip = d.grips[g];
-    if (grip.particle.y != c.grip_gen) return;
-    const uint32_t i = grip.particle.x;
-    float4 p = px(ctx, i);
+// Compliant vector attachment (tools/cloth_bag.cpp:1630-1647) on a loaded
+// particle and grip record; false when it changes nothing.
+__device__ __forceinline__ bool grip_core(const DeviceCloth& d, const SubCfg& c, NumiClothGrip& grip, float4& p) {
     const float alpha = grip.targetOffsetAndCompliance.w / (c.dt * c.dt);
     const float den = p.w + alpha;
-    if (den <= 0.0f) return;
+    if (den <= 0.0f) return false;
     const V3 offset{grip.targetOffsetAndCompliance.x, grip.targetOffsetAndCompliance.y,
                     grip.targetOffsetAndCompliance.z};
     const V3 target = c.grip_target + rotate_q(c.grip_q, offset);
@@ -291,10 +293,24 @@ __device__ void solve_grips(const Ctx& ctx) {
     const V3 nl = lambda + dl;
     const V3 np = xyz(p) + dl * p.w;
     if (!finite3(np)) fail(d, NUMI_CLOTH_FAILURE_NONFINITE);
-    px_set(ctx, i, with_xyz(p, np));
+    p = with_xyz(p, np);
     grip.lambda.x = nl.x;
     grip.lambda.y = nl.y;
     grip.lambda.z = nl.z;
+    return true;
+}
+
+__device__ void solve_grips(const Ctx& ctx) {
+    const DeviceCloth& d = ctx.d;
+    const SubCfg& c = ctx.c;
+    const uint32_t g = threadIdx.x;
+    if (g >= d.g_count || !c.grip_active) return;
+    NumiClothGrip grip = d.grips[g];
+    if (grip.particle.y != c.grip_gen) return;
+    const uint32_t i = grip.particle.x;
+    float4 p = px(ctx, i);
+    if (!grip_core(d, c, grip, p)) return;
+    px_set(ctx, i, p);
     d.grips[g] = grip;
 }
 

@@ -128,6 +128,9 @@ struct Run {
         bool grip_active = false;
         double grip_q[4] = {1.0, 0.0, 0.0, 0.0};   // wxyz
         uint32_t generation = 1u, selections = 0u, patch_center = 0u;
+        // the reference's grip metrics (tools/cloth_bag.cpp:1563-1620)
+        uint32_t regrabs = 0u, ring_shift = 0u;
+        uint64_t inactive = 0u;
         if (o.scenario != NUMI_CLOTH_SCENARIO_GROUNDED) {
             std::copy(handle, handle + 3, grip);
             grip_active = true;
@@ -184,6 +187,10 @@ struct Run {
         uint32_t failure = 0;
         for (uint32_t step = 0; step < o.steps && failure == 0u; ++step) {
             const uint64_t first = static_cast<uint64_t>(step) * o.substeps;
+            // substeps of this frame that attach a new grip generation: the
+            // frame is stepped in launches that end after each of them, so
+            // the selected patch centre of every re-grab can be read
+            std::vector<uint32_t> cuts;
             if (o.scenario == NUMI_CLOTH_SCENARIO_RECORDED) {
                 rc = numi_cloth_trajectory_configs(traj, view.config, handle, first, o.substeps, dt, cfg.data());
                 // the grip state updateGrip keeps, substep by substep
@@ -198,9 +205,14 @@ struct Run {
                     grip_q[2] = pose.orientation[1];
                     grip_q[3] = pose.orientation[2];
                     if (pose.active && pose.generation != generation) {
-                        if (select_nearest) ++selections;
+                        if (select_nearest) {
+                            ++selections;
+                            cuts.push_back(k + 1u);
+                        }
+                        ++regrabs;
                         generation = pose.generation;
                     }
+                    if (!pose.active) ++inactive;
                 }
             } else {
                 rc = numi_cloth_bag_scenario_configs(o.scenario, view.config, first, o.substeps, dt, cfg.data(),
@@ -208,19 +220,36 @@ struct Run {
                 if (o.scenario != NUMI_CLOTH_SCENARIO_GROUNDED)
                     std::copy(targets.end() - 3, targets.end(), grip);
             }
-            if (rc == NUMI_CLOTH_OK) rc = numi_cloth_step(h, cfg.data(), o.substeps, &o.schedule);
+            // the attach substeps end launches of their own (at most one
+            // attach per launch), then the frame's remainder
+            const size_t attaches = cuts.size();
+            if (cuts.empty() || cuts.back() != o.substeps) cuts.push_back(o.substeps);
+            uint32_t done = 0;
+            for (size_t c = 0; c < cuts.size() && rc == NUMI_CLOTH_OK && failure == 0u; ++c) {
+                const uint32_t end = cuts[c];
+                rc = numi_cloth_step(h, cfg.data() + done, end - done, &o.schedule);
+                if (rc != NUMI_CLOTH_OK) break;
+                failure = numi_cloth_failure(h);
+                if (c < attaches && g > 0u && failure == 0u) {
+                    // the nearest-patch centre this re-grab selected
+                    // (cyclicRingDistance, tools/cloth_bag.cpp:462-468)
+                    numi_cloth_read_grips(h, G.data(), g);
+                    const uint32_t centre = G[0].particle.w;
+                    const uint32_t direct = centre > patch_center ? centre - patch_center : patch_center - centre;
+                    const uint32_t around = view.config->gripControl.z;
+                    ring_shift = std::max(ring_shift, std::min(direct, around - direct));
+                    patch_center = centre;
+                }
+                done = end;
+            }
             if (rc != NUMI_CLOTH_OK) break;
-            failure = numi_cloth_failure(h);
             dump(step + 1u);
         }
         const double seconds =
             std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         if (write && o.dumpObj != nullptr) write_frame(o.dumpObj);
         read();
-        if (g && select_nearest && selections > 0u) {
-            // the patch centre ring: the middle grip of the upper row
-            patch_center = G[2].particle.x % 48u;
-        }
+
         std::vector<double> xv(6u * n), fs(13u * f), off(3u * g);
         std::vector<uint32_t> gp(g);
         for (uint32_t i = 0; i < n; ++i) {
@@ -273,6 +302,25 @@ struct Run {
             r->reconcileMax = passes[1];
             r->certificateMax = passes[2];
             r->generation = generation;
+            r->regrabCount = regrabs;
+            r->inactiveGripSubsteps = inactive;
+            r->patchSelections = selections;
+            r->maxPatchRingShift = ring_shift;
+            r->patchCenter = patch_center;
+            // gripParticlesUnique and gripPatchTopologyExact
+            // (tools/cloth_bag.cpp:5409-5437) on the final grips
+            bool unique = true;
+            for (uint32_t a = 0; a < g; ++a)
+                for (uint32_t b = a + 1u; b < g; ++b) unique = unique && G[a].particle.x != G[b].particle.x;
+            const uint32_t rings = view.config->gripControl.z;
+            bool exact = g == 10u && view.cuffParticles != nullptr && rings >= 5u;
+            for (uint32_t row = 0; exact && row < 2u; ++row)
+                for (uint32_t slot = 0; slot < 5u; ++slot) {
+                    const uint32_t ring = (patch_center + rings + slot - 2u) % rings;
+                    exact = exact && G[row * 5u + slot].particle.x == view.cuffParticles[row * rings + ring];
+                }
+            r->patchParticlesUnique = unique ? 1u : 0u;
+            r->patchTopologyExact = exact ? 1u : 0u;
         }
         numi_cloth_destroy(h);
         numi_cloth_scene_destroy(scene);

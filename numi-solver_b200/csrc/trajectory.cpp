@@ -90,6 +90,7 @@ void set_err(char* err, size_t size, const std::string& msg) {
 struct numi_cloth_trajectory {
     std::vector<Pose> poses;
     bool select_nearest = false;
+    uint32_t version = 0;   // schema v1..v3
     uint64_t fingerprint = 0;
 };
 
@@ -129,6 +130,7 @@ numi_cloth_trajectory_t* numi_cloth_trajectory_load(const char* path, char* err,
                         throw std::runtime_error("grip trajectory schema mismatch");
                     reactivate = line != "schema=numi.grip.trajectory.v1";
                     t->select_nearest = line == "schema=numi.grip.trajectory.v3";
+                    t->version = static_cast<uint32_t>(line.back() - '0');
                     schema = true;
                     continue;
                 }
@@ -236,6 +238,25 @@ int numi_cloth_trajectory_info(const numi_cloth_trajectory_t* t, uint32_t* selec
     if (select_nearest) *select_nearest = t->select_nearest ? 1u : 0u;
     if (duration) *duration = t->poses.back().t;
     if (fingerprint) *fingerprint = t->fingerprint;
+    return NUMI_CLOTH_OK;
+}
+
+// maximumGripTrajectoryRotation and gripTrajectoryAttachmentGenerations
+// (include/numi/grip_trajectory.h:371-389): the largest rotation angle
+// 2 acos|w| of any pose, and the highest attachment generation.
+int numi_cloth_trajectory_summary(const numi_cloth_trajectory_t* t, uint32_t* version, uint32_t* poses,
+                                  double* max_rotation, uint32_t* generations) {
+    if (!t) return NUMI_CLOTH_EINVAL;
+    double rot = 0.0;
+    uint32_t gen = 0u;
+    for (const Pose& p : t->poses) {
+        rot = std::max(rot, 2.0 * std::acos(std::clamp(std::abs(p.q[3]), 0.0, 1.0)));
+        gen = std::max(gen, p.generation);
+    }
+    if (version) *version = t->version;
+    if (poses) *poses = static_cast<uint32_t>(t->poses.size());
+    if (max_rotation) *max_rotation = rot;
+    if (generations) *generations = gen;
     return NUMI_CLOTH_OK;
 }
 

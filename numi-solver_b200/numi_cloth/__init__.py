@@ -363,7 +363,12 @@ def replay(scenario: str, steps: int, substeps: int = 48, frame_dt: float = 1.0 
             "residuals": list(r.residuals), "self_contacts": int(r.selfContacts),
             "edge_contacts": (int(r.edgeContacts[0]), int(r.edgeContacts[1])),
             "masks": (int(r.masks[0]), int(r.masks[1])), "reconcile_max": int(r.reconcileMax),
-            "certificate_max": int(r.certificateMax), "seconds": r.seconds}
+            "certificate_max": int(r.certificateMax), "seconds": r.seconds,
+            "regrab_count": int(r.regrabCount), "patch_selections": int(r.patchSelections),
+            "max_patch_ring_shift": int(r.maxPatchRingShift), "patch_center": int(r.patchCenter),
+            "patch_particles_unique": bool(r.patchParticlesUnique),
+            "patch_topology_exact": bool(r.patchTopologyExact),
+            "inactive_grip_substeps": int(r.inactiveGripSubsteps)}
 
 
 def _bag_handle_base(scenario: str):
@@ -593,7 +598,8 @@ class ClothSolver:
         out = (ctypes.c_uint32 * 6)()
         self._check(self.lib.numi_cloth_launch_info(self._h, out))
         return {"grid": out[0], "block": out[1], "barriers_per_substep": out[2], "launches": out[3],
-                "cluster": out[4], "resident": bool(out[5] & 1), "neighbour_syncs": bool(out[5] & 2)}
+                "cluster": out[4], "resident": bool(out[5] & 1), "neighbour_syncs": bool(out[5] & 2),
+                "tiles": bool(out[5] & 4), "last_tiles": bool(out[5] & 8)}
 
     def trace(self, substeps: int) -> np.ndarray:
         """Per-barrier globaltimer stamps (ns) of the last step, [substeps, 128]."""

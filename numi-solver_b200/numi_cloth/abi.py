@@ -292,4 +292,8 @@ class ReplayResult(ctypes.Structure):
         ("selfContacts", ctypes.c_ulonglong), ("edgeContacts", ctypes.c_ulonglong * 2),
         ("masks", ctypes.c_uint32 * 2), ("reconcileMax", ctypes.c_uint32), ("certificateMax", ctypes.c_uint32),
         ("seconds", ctypes.c_double),
+        ("regrabCount", ctypes.c_uint32), ("patchSelections", ctypes.c_uint32),
+        ("maxPatchRingShift", ctypes.c_uint32), ("patchCenter", ctypes.c_uint32),
+        ("patchParticlesUnique", ctypes.c_uint32), ("patchTopologyExact", ctypes.c_uint32),
+        ("inactiveGripSubsteps", ctypes.c_uint64),
     ]

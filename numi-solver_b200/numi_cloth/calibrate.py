@@ -129,16 +129,21 @@ class Calibration:
         return r["loss"], g, r["damping"], r["nonsmooth"]
 
     def fit(self, logc0: np.ndarray, damping0: np.ndarray, steps: int, lr: float = 0.1, lr_damping: float = 0.005,
-            damping_max: float = 1.0) -> dict:
+            damping_max: float = 1.0, frozen=None) -> dict:
+        """Adam on every candidate's log-compliances and damping; `frozen`
+        (one flag per parameter, damping last) keeps those at their start."""
         logc, damp = logc0.astype(np.float64).copy(), damping0.astype(np.float64).copy()
         opt_c, opt_d = Adam(logc.shape, lr), Adam(damp.shape, lr_damping)
+        hold = np.zeros(logc.shape[1] + 1, bool) if frozen is None else np.asarray(frozen, bool)
         history = []
         loss = None
         for _ in range(steps):
             loss, g, gd, rough = self.evaluate(logc, damp)
             history.append(loss.copy())
+            g = np.where(hold[None, :-1], 0.0, g)
             logc = opt_c.step(logc, g)
-            damp = np.clip(opt_d.step(damp, gd), 0.0, damping_max)
+            if not hold[-1]:
+                damp = np.clip(opt_d.step(damp, gd), 0.0, damping_max)
         final, _, _, rough = self.evaluate(logc, damp)
         history.append(final.copy())
         return {"logc": logc, "damping": damp, "loss": final, "history": np.array(history), "nonsmooth": rough}
@@ -188,3 +193,90 @@ def adjoint_observations(solver: ClothSolver, configs: np.ndarray, schedule: Sch
     names = [p for p, _ in parameters]
     header = "trial_id,split,observable,measured,sigma,baseline" + "".join(f",dlog_{p}" for p in names)
     return names, header + "\n" + "\n".join(rows) + "\n"
+
+
+def tracked_trajectory(scene, configs: np.ndarray, schedule: Schedule, tracked, loss_every: int, values,
+                       damping: float, base_values, params=BAG_PARAMS, stream: int | None = None) -> np.ndarray:
+    """Positions of the tracked particles after every loss_every substeps
+    (the observations of the fit), forward only, for compliances `values`
+    (one per parameter) and `damping`."""
+    sv = ClothSolver(scene)
+    try:
+        if stream is not None:
+            sv.set_stream(stream)
+        current = np.asarray(base_values, np.float32).copy()
+        for p, (fam, _) in enumerate(params):
+            new = np.float32(values[p])
+            if new == current[p]:
+                continue
+            # never step onto another parameter's value of the family (their
+            # records would merge)
+            others = [current[q] for q, (f, _) in enumerate(params) if f == fam and q != p]
+            while new in others:
+                new = np.nextafter(new, np.float32(np.inf))
+            sv.replace_compliance(fam, float(current[p]), float(new))
+            current[p] = new
+        sv.set_damping(float(damping))
+        out = []
+        for k in range(len(configs) // loss_every):
+            sv.step(configs[k * loss_every:(k + 1) * loss_every], schedule)
+            out.append(sv.particles()["positionAndInverseMass"][np.asarray(tracked), :3].astype(np.float64))
+        return np.stack(out)
+    finally:
+        sv.close()
+
+
+def sensitivities(scene, configs: np.ndarray, schedule: Schedule, tracked, loss_every: int, log_values,
+                  damping: float, base_values, params=BAG_PARAMS, step: float = 0.1, damping_step: float = 0.002,
+                  stream: int | None = None) -> np.ndarray:
+    """Central-difference Jacobian of the flattened observations with
+    respect to each log-compliance (step in log) and the damping (last
+    column), at the given parameters, from forward runs."""
+    cols = []
+    for p in range(len(params) + 1):
+        run = []
+        for sign in (1.0, -1.0):
+            lv = np.array(log_values, np.float64)
+            dmp = damping
+            if p < len(params):
+                lv[p] += sign * step
+            else:
+                dmp = max(0.0, damping + sign * damping_step)
+            run.append(tracked_trajectory(scene, configs, schedule, tracked, loss_every, np.exp(lv), dmp,
+                                          base_values, params, stream).ravel())
+        h = 2.0 * step if p < len(params) else (max(0.0, damping + damping_step) - max(0.0, damping - damping_step))
+        cols.append((run[0] - run[1]) / h)
+    return np.stack(cols, axis=1)
+
+
+def identifiable(jacobian: np.ndarray, sigma: float, max_condition: float = 1.0e4, min_norm: float = 1.0):
+    """Which parameters the observations can determine, by the calibration
+    qualifier's tests (tools/cloth_calibration.cpp:301-393, numi_cloth.qualify):
+    each kept parameter moves the observations by at least `min_norm` noise
+    units (sigma, metres) per unit of its parameter, and the Gram matrix of
+    the kept column-normalised sensitivities has full rank and a condition
+    number (square root of the eigenvalue ratio, Jacobi eigenvalues) at most
+    `max_condition`; of several sets that pass, the largest with the lowest
+    condition.  Returns (keep flags, condition number of the kept set)."""
+    from itertools import combinations
+
+    from .qualify import jacobi_eigenvalues
+
+    design = np.asarray(jacobian, np.float64) / sigma
+    norms = np.sqrt((design * design).sum(axis=0))
+    able = [j for j in range(design.shape[1]) if norms[j] >= min_norm]
+    for size in range(len(able), 0, -1):
+        best = None
+        for keep in combinations(able, size):
+            cols = design[:, list(keep)] / norms[list(keep)]
+            eig = jacobi_eigenvalues((cols.T @ cols).tolist())
+            if eig[0] <= 0.0:
+                continue
+            cond = float(np.sqrt(eig[-1] / eig[0]))
+            if cond <= max_condition and (best is None or cond < best[1]):
+                best = (keep, cond)
+        if best is not None:
+            flags = np.zeros(design.shape[1], bool)
+            flags[list(best[0])] = True
+            return flags, best[1]
+    return np.zeros(design.shape[1], bool), float("inf")

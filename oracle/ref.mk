@@ -4,7 +4,9 @@
 #   libref_shim.so the same source behind the C API of ref_shim.cpp
 #   cloth_calibration the reference calibration qualifier (tools/cloth_calibration.cpp)
 # Nothing here is copied into the repository; _ref/ is git-ignored.
-REFERENCE ?= /root/reference
+# the reference checkout: NUMI_CLOTH_REFERENCE, default /root/reference
+NUMI_CLOTH_REFERENCE ?= /root/reference
+REFERENCE ?= $(NUMI_CLOTH_REFERENCE)
 CXX ?= g++
 HERE := $(abspath $(dir $(lastword $(MAKEFILE_LIST))))
 OUT := $(HERE)/_ref

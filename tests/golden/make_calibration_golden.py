@@ -18,7 +18,7 @@ import tempfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = "/root/reference"
+REF = os.environ.get("NUMI_CLOTH_REFERENCE", "/root/reference")
 OUT = os.path.join(HERE, "calibration")
 TOOL = os.path.join(ROOT, "oracle", "_ref", "cloth_calibration")
 

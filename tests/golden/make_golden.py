@@ -53,7 +53,7 @@ PROBES = ["--strain-probe", "--cloth-ground-friction-probe", "--rolling-probe", 
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("NUMI_CLOTH_REFERENCE", "/root/reference"))
     args = ap.parse_args()
     subprocess.run(["make", "-s", "-f", "ref.mk", f"REFERENCE={args.reference}"], cwd=os.path.join(ROOT, "oracle"),
                    check=True)

@@ -111,12 +111,14 @@ def oracle_state_to_abi(scene, st):
     return P, F
 
 
-def per_substep_errors(scene, configs, sched):
+def per_substep_errors(scene, configs, sched, mode=op.BATCHED):
     """Max particle / fruit position error of one GPU substep started from
-    the FP64 trajectory's state (rounded to FP32), for every substep."""
+    the FP64 trajectory's state (rounded to FP32), for every substep.  mode:
+    the FP64 oracle's order, BATCHED (the kernels' order) or SERIAL (the
+    reference's order)."""
     o = op.Oracle(op.from_abi(scene), 64)
     subs = op.substeps_from_configs(configs)
-    osched = op.schedule_from_abi(sched, op.BATCHED)
+    osched = op.schedule_from_abi(sched, mode)
     s = nc.ClothSolver(scene)
     errs, ferrs = [], []
     try:

@@ -179,7 +179,11 @@ def test_gpu_replay_recorded_frames(tmp_path):
 @pytest.mark.gpu
 def test_gpu_replay_command_line():
     exe = os.path.join(ROOT, "numi-solver_b200", "numi_cloth", "numi-cloth-replay")
-    out = subprocess.run([exe, "--scenario", "pickup", "--steps", "1", "--substeps", "12", "--replays", "2"],
+    out = subprocess.run([exe, "--scenario", "pickup", "--steps", "1", "--substeps", "12", "--iterations", "1",
+                          "--replays", "2", "--timestep", repr(1.0 / 60.0)],
                          capture_output=True, text=True, timeout=300)
-    assert out.returncode == 0, out.stderr
+    # one frame releases no fruit, so the pickup outcome gate fails: exit 1,
+    # as the reference's acceptance would (tools/cloth_bag.cpp:5454-5455)
+    assert out.returncode == 1, out.stderr
     assert "deterministic=true" in out.stdout and "scenario=pickup" in out.stdout
+    assert "result=FAIL" in out.stdout

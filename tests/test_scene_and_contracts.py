@@ -212,7 +212,7 @@ def test_record_sizes_match_reference_abi():
 def test_reference_header_offsets(tmp_path):
     """Byte layout identical to the reference ABI header (compiled check,
     where the reference sources are present)."""
-    ref = "/root/reference/include"
+    ref = os.path.join(os.environ.get("NUMI_CLOTH_REFERENCE", "/root/reference"), "include")
     if not os.path.isdir(ref):
         pytest.skip("reference headers not present")
     src = tmp_path / "abi_check.cpp"

@@ -1,14 +1,15 @@
 """The allocation-free entry point, numi_cloth_step_noalloc.
 
 Some callers cannot let a library allocate GPU memory: hosts that own every
-device byte through their own pool, and code that steps the cloth inside a
-stream capture, where a cudaMalloc would break the capture.  For them the
-library steps caller-owned device buffers and keeps its own scratch in one
-statically allocated device array.  This test owns the buffers (allocated
-through torch), calls the entry point twice in a row through the C ABI and
-requires the same bits as the ordinary handle-based path after each call.
-It runs alone or after the other tests: every call clears the shared
-scratch it needs zeroed.
+device byte through their own pool or arena, sized once at start-up, and
+real-time loops where a cudaMalloc (which may synchronise the whole device)
+is not allowed once they run.  For them the library steps caller-owned device
+buffers and keeps its own scratch in one statically allocated device array.
+This test owns the buffers (allocated through torch), calls the entry point
+twice in a row through the C ABI and requires the same bits as the ordinary
+handle-based path after each call, with the schedule's damping off and on.
+It runs alone or after the other tests: every call clears the shared scratch
+it needs zeroed.
 """
 import numpy as np
 import pytest
@@ -65,7 +66,8 @@ def _host(t, dtype, shape):
     return t.cpu().numpy().view(dtype).reshape(shape)
 
 
-def test_noalloc_matches_handle_path_two_calls():
+@pytest.mark.parametrize("damping", [0.0, 0.8])
+def test_noalloc_matches_handle_path_two_calls(damping):
     torch = pytest.importorskip("torch")
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
@@ -73,15 +75,22 @@ def test_noalloc_matches_handle_path_two_calls():
     torch.zeros(1, device="cuda")
     dt = 1.0 / 5760.0
     scene = nc.bag_scene(scenario="recorded", timestep=dt)
-    sched = nc.Schedule.make(**FULL)
+    sched = nc.Schedule.make(**dict(FULL, damping=damping))
     frames = [bag_frame_configs(scene, 0, 48, dt), bag_frame_configs(scene, 48, 48, dt)]
 
     ref = nc.ClothSolver(scene)
     st, bufs = _device_state(torch, scene)
     batches, counts = nc.colour_runs(scene)
     stream = torch.cuda.current_stream()
+    undamped = None
+    if damping != 0.0:
+        # the same call without damping ends elsewhere: the damping is used
+        flat = nc.ClothSolver(scene)
+        flat.step(frames[0], nc.Schedule.make(**FULL))
+        undamped = flat.particles()["positionAndInverseMass"].copy()
+        flat.close()
     try:
-        for cfg in frames:
+        for k, cfg in enumerate(frames):
             ref.step(cfg, sched)
             assert ref.failure() == 0
             rc = nc.step_noalloc(scene, st, batches, counts, cfg, sched, stream.cuda_stream)
@@ -91,15 +100,37 @@ def test_noalloc_matches_handle_path_two_calls():
             rp = ref.particles()
             rf = ref.fruits()
             n = scene.n
-            assert np.array_equal(_host(bufs["positions"], np.float32, (n, 4)), rp["positionAndInverseMass"])
+            got = _host(bufs["positions"], np.float32, (n, 4))
+            assert np.array_equal(got, rp["positionAndInverseMass"])
             assert np.array_equal(_host(bufs["velocities"], np.float32, (n, 4)), rp["velocity"])
             assert np.array_equal(_host(bufs["previous"], np.float32, (n, 4)), rp["previousAndMass"])
             got_f = _host(bufs["fruits"], nc.abi.FRUIT, (len(scene.fruits),))
             assert np.array_equal(got_f.view(np.uint8), rf.view(np.uint8))
             lam = _host(bufs["distanceLambda"], np.float32, (len(scene.distances),))
             assert np.array_equal(lam, ref.distances()["material"][:, 2])
+            if k == 0 and undamped is not None:
+                assert not np.array_equal(got, undamped)
     finally:
         ref.close()
+
+
+def test_noalloc_rejects_run_past_records():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    torch.cuda.set_device(0)
+    torch.zeros(1, device="cuda")
+    scene = nc.square_scene(side=12, fruitCount=1)
+    st, bufs = _device_state(torch, scene)
+    batches, counts = nc.colour_runs(scene)
+    bad = batches.copy()
+    bad[0, 1] = len(scene.distances) + 1   # the first distance run (first, count, colour, prefixes) reaches past D
+    rc = nc.step_noalloc(scene, st, bad, counts, nc.substep_configs(scene, 1), nc.Schedule.make())
+    assert rc == -1
+    bad = batches.copy()
+    bad[0, 3] = (int(bad[0, 1]) + 1) << 16   # strain-limited prefix longer than the run
+    rc = nc.step_noalloc(scene, st, bad, counts, nc.substep_configs(scene, 1), nc.Schedule.make())
+    assert rc == -1
 
 
 def test_noalloc_rejects_oversize():
