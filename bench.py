@@ -373,6 +373,125 @@ def calibration_leg(nc, torch, stream, candidates: int, steps: int, plain_sample
             "note": "fruit contact and cloth/ground friction are not differentiated; their events are counted"}
 
 
+# The differentiable rollout: a 64 x 64 cloth at 4 mm, one corner on a
+# seeded 6-DoF grip trajectory (translation at most 5 cm, rotation at most
+# 15 degrees), ground and 4 spheres, 96 substeps (two 60 Hz frames), the loss
+# over 32 seeded tracked particles against a target trajectory made at
+# log-compliances shifted by N(0, 0.3) (by the forward here, by the FP64
+# oracle in the tests).  The cloth hangs
+# 12 cm above the ground and the spheres start 3-8 cm above it, as in the
+# benchmark cloth; soft enough compliances that the constraint violations
+# stay well above the FP32 position resolution.
+CONFIG3_SUBSTEPS, CONFIG3_LOSS_EVERY, CONFIG3_TRACKED = 96, 12, 32
+CONFIG3_SCHED = dict(iterations=1, strainSweeps=1, reconcilePasses=0, finalPasses=0, certificatePasses=0,
+                     earlyExit=0, aerodynamics=0, sweptGround=1, frictions=1, damping=0.5)
+
+
+def config3_scene(stretch=2e-5, shear=5e-5, bend=2e-4):
+    import numi_cloth as nc
+
+    return nc.square_scene(side=64, spacing=0.004, height=0.12, gripCorners=1, fruitCount=4,
+                           fruitRadiusMin=0.02, fruitRadiusMax=0.05, fruitHeightMin=0.15, fruitHeightMax=0.20,
+                           stretchCompliance=stretch, shearCompliance=shear, bendCompliance=bend,
+                           timestep=1.0 / 2880.0, seed=20260310)
+
+
+def config3_configs(scene, seed: int = 303):
+    """Per-substep Configs of the seeded 6-DoF grip: a smooth translation
+    of at most 5 cm and a rotation about a seeded axis of at most 15 degrees,
+    both starting at rest."""
+    import numpy as np
+
+    import numi_cloth as nc
+
+    rng = np.random.default_rng(seed)
+    n = CONFIG3_SUBSTEPS
+    cfg = nc.substep_configs(scene, n)
+    s = np.arange(1, n + 1) / n
+    ramp = 0.5 - 0.5 * np.cos(np.pi * s)
+    direction = rng.normal(size=3)
+    direction /= np.linalg.norm(direction)
+    amplitude = rng.uniform(0.02, 0.05)
+    wobble = rng.uniform(0.0, 0.01, size=3)
+    trans = direction[None, :] * (amplitude * ramp)[:, None] + wobble[None, :] * np.sin(2.0 * np.pi * s)[:, None]
+    trans *= np.minimum(1.0, 0.05 / np.maximum(np.linalg.norm(trans, axis=1), 1e-12))[:, None]
+    axis = rng.normal(size=3)
+    axis /= np.linalg.norm(axis)
+    angle = np.radians(rng.uniform(8.0, 15.0)) * ramp
+    base = cfg["gripTargetAndActive"][:, :3].astype(np.float64)
+    cfg["gripTargetAndActive"][:, :3] = (base + trans).astype(np.float32)
+    q = np.concatenate([axis[None, :] * np.sin(angle / 2)[:, None], np.cos(angle / 2)[:, None]], axis=1)
+    cfg["gripOrientation"] = q.astype(np.float32)
+    return cfg
+
+
+def rollout_leg(nc, torch, stream, reps: int, candidates: int) -> dict:
+    """The differentiable rollout (config3_scene / config3_configs): forward
+    + adjoint gradients (compliance groups, damping, every substep's grip
+    pose) of one cloth per numi_cloth_rollout_grad call, timed over `reps`
+    calls, and of `candidates` copies in one batched call
+    (numi_cloth_batch_rollout_grad).  The target trajectory comes from the
+    forward at log-compliances shifted by N(0, 0.3)."""
+    import numpy as np
+
+    scene = config3_scene()
+    cfg = config3_configs(scene)
+    sched = nc.Schedule.make(**CONFIG3_SCHED)
+    rng = np.random.default_rng(3)
+    tracked = np.sort(rng.choice(scene.n, CONFIG3_TRACKED, replace=False)).astype(np.uint32)
+    shift = np.exp(rng.normal(0.0, 0.3, size=3))
+    sv = nc.ClothSolver(config3_scene(2e-5 * shift[0], 5e-5 * shift[1], 2e-4 * shift[2]))
+    sv.set_stream(stream.cuda_stream)
+    targets = []
+    for k in range(CONFIG3_SUBSTEPS // CONFIG3_LOSS_EVERY):
+        sv.step(cfg[k * CONFIG3_LOSS_EVERY:(k + 1) * CONFIG3_LOSS_EVERY], sched)
+        targets.append(sv.particles()["positionAndInverseMass"][tracked, :3].astype(np.float64))
+    sv.close()
+    targets = np.stack(targets)
+    sv = nc.ClothSolver(scene)
+    sv.set_stream(stream.cuda_stream)
+    sv.snapshot(0)
+    r = sv.rollout_grad(cfg, sched, tracked, targets, CONFIG3_LOSS_EVERY, checkpoint_every=8)
+    times = []
+    for _ in range(reps):
+        sv.restore(0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sv.rollout_grad(cfg, sched, tracked, targets, CONFIG3_LOSS_EVERY, checkpoint_every=8)
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+    sv.close()
+    solvers = [nc.ClothSolver(scene) for _ in range(candidates)]
+    batch = nc.ClothBatch(solvers)
+    batch.set_stream(stream.cuda_stream)
+    for s in solvers:
+        s.set_stream(stream.cuda_stream)
+        s.snapshot(0)
+    allcfg = np.stack([cfg] * candidates)
+    alltg = np.stack([targets] * candidates)
+    batch.rollout_grad(allcfg, sched, tracked, alltg, CONFIG3_LOSS_EVERY, checkpoint_every=8)
+    for s in solvers:
+        s.restore(0)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    rb = batch.rollout_grad(allcfg, sched, tracked, alltg, CONFIG3_LOSS_EVERY, checkpoint_every=8)
+    torch.cuda.synchronize()
+    batched_s = time.perf_counter() - t0
+    batch.close()
+    for s in solvers:
+        s.close()
+    single = 1.0 / statistics.median(times)
+    return {"metric": "gradients/s (64x64 cloth, 96-substep forward + adjoint)", "value": single,
+            "unit": "gradients/s", "reps": reps, "ms_per_gradient": 1000.0 / single,
+            "batched_value": candidates / batched_s, "batched_candidates": candidates,
+            "speedup_batched": candidates / batched_s / single, "loss": float(r["loss"]),
+            "nonsmooth_events": int(r["nonsmooth"]), "nonsmooth_events_batched": int(rb["nonsmooth"].sum()),
+            "groups": [f"{f} {v:.3g}" for f, v in r["groups"]], "schedule": CONFIG3_SCHED,
+            "gradients": ["log-compliance per group", "damping", "grip pose per substep (6)"],
+            "workload": "64x64 cloth (4,096 particles, 4 mm), 1 gripped corner on a seeded 6-DoF trajectory, "
+                        "ground, 4 spheres, 96 substeps at 1/2880 s, 32 tracked particles, checkpoints every 8"}
+
+
 BAG_SCHEDULE = dict(iterations=1, strainSweeps=3, reconcilePasses=8, finalPasses=2, certificatePasses=128,
                     earlyExit=1, selfCollision=1, aerodynamics=1, sweptGround=1, sweptFruitYarn=1, frictions=1,
                     release=1)
@@ -571,6 +690,10 @@ def run_ours(args):
     if world == 1 and not args.no_calibration:
         calibration = calibration_leg(nc, torch, stream, args.calib_candidates, args.calib_steps, 32)
 
+    rollout = None
+    if world == 1 and not args.no_rollout:
+        rollout = rollout_leg(nc, torch, stream, 20, 64)
+
     bag = None
     if world == 1 and not args.no_bag:
         bag = bag_leg(nc, torch, stream, args.bag_frames, 0 if args.no_cpu else args.bag_frames + 1)
@@ -604,6 +727,7 @@ def run_ours(args):
                     "d2h_bytes_per_step": int(d2h)},
             "batched": batched,
             "calibration": calibration,
+            "rollout": rollout,
             "bag": bag,
             "gpu_launches": args.steps,
             "clocks": clocks.summary(),
@@ -634,6 +758,7 @@ def main():
     ap.add_argument("--calib-candidates", type=int, default=256)
     ap.add_argument("--calib-steps", type=int, default=50)
     ap.add_argument("--no-bag", action="store_true")
+    ap.add_argument("--no-rollout", action="store_true")
     ap.add_argument("--bag-frames", type=int, default=10)
     args = ap.parse_args()
     if args.impl == "reference":

@@ -558,7 +558,8 @@ bool build_tiles(numi_cloth* h, uint32_t grid_width, const std::vector<uint2>& d
         for (uint32_t p : local) lidx[p] = -1;
         widest = std::max(widest, w.size() * 4u + local.size() * sizeof(float4));
     }
-    const size_t smem = std::max(nc_resident_offset(), nc_fruit_offset() + widest);
+    // the fruit CTA holds its fruit state and the staged friction sweep
+    const size_t smem = std::max(nc_resident_offset() + sizeof(FrictionStage), nc_fruit_offset() + widest);
     if (smem > smem_budget) return false;
     std::vector<uint32_t> off(R + 1u, 0u), words;
     for (uint32_t t = 0; t < R; ++t) {

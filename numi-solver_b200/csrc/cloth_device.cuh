@@ -27,6 +27,7 @@
 #define NC_MAX_PAIRS 2016u
 #define NC_TRACE_SLOTS 128u
 #define NC_HASH_CAP 8u      /* particles one self-contact bucket holds */
+#define NC_FRICTION_STAGE 128u   /* recorded segments the staged friction sweep holds */
 
 struct Batch {
     uint32_t first;
@@ -284,4 +285,21 @@ struct FruitShared {
     float4 v[NC_MAX_FRUITS];               // velocity xyz, inverse mass
     float4 o[NC_MAX_FRUITS];               // spin xyz, radius
     unsigned long long loaded;             // pair colours with an impulse this substep
+};
+
+// The fruit/yarn friction sweep's recorded segments, staged by the fruit CTA
+// in tile mode (friction_stage, after FruitShared in its shared memory):
+// segment, slot tags and records, endpoint particles, for every endpoint
+// the first endpoint slot with the same particle, endpoint positions and
+// velocities.
+struct FrictionStage {
+    uint32_t count;                        // staged segments (NC_FRICTION_STAGE + 1: too many)
+    uint32_t seg[NC_FRICTION_STAGE];
+    uint32_t tag[NC_FRICTION_STAGE][NC_YARN_SLOTS];
+    uint32_t pid[2 * NC_FRICTION_STAGE];
+    unsigned short rep[2 * NC_FRICTION_STAGE];
+    float4 x[2 * NC_FRICTION_STAGE];
+    float4 v[2 * NC_FRICTION_STAGE];
+    float4 ra[NC_FRICTION_STAGE][NC_YARN_SLOTS];
+    float4 rb[NC_FRICTION_STAGE][NC_YARN_SLOTS];
 };

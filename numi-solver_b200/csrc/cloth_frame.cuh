@@ -1358,17 +1358,13 @@ __device__ __forceinline__ FrictionSeg friction_seg(const DeviceCloth& d, uint32
     return fs;
 }
 
-__device__ __forceinline__ void yarn_friction_segment(const Ctx& ctx, const FrictionSeg& fseg, const float4* s_vw,
-                                                      const float4* s_or, unsigned long long* s_sum) {
-    const DeviceCloth& d = ctx.d;
+// The friction of one segment on its loaded endpoints: positions pa, pb,
+// velocities va, vb (updated), slot tags st and the slots' records ra, rb
+// (only the live ones are read).
+__device__ __forceinline__ void yarn_friction_core(const Ctx& ctx, const float4& pa, const float4& pb, float4& va,
+                                                   float4& vb, const uint32_t* st, const float4* ra, const float4* rb,
+                                                   const float4* s_vw, const float4* s_or, unsigned long long* s_sum) {
     const SubCfg& c = ctx.c;
-    const uint32_t seg = fseg.seg;
-    const uint2 ij = fseg.ij;
-    const uint32_t* st = fseg.st;
-    const float4 pa = px(ctx, ij.x);
-    const float4 pb = px(ctx, ij.y);
-    float4 va = pv(ctx, ij.x);
-    float4 vb = pv(ctx, ij.y);
     // Live records of this segment, visited in ascending fruit order.
     const uint32_t live = ctx.epoch & 0x3ffffffu;
     uint32_t fruit_of[NC_YARN_SLOTS];
@@ -1390,8 +1386,13 @@ __device__ __forceinline__ void yarn_friction_segment(const Ctx& ctx, const Fric
 #pragma unroll
         for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q)
             if (q == slot) fruit_of[q] = 0xffffffffu;
-        const float4 sa = __ldcg(&d.yarn_slot_a[seg * NC_YARN_SLOTS + slot]);
-        const float4 sb = __ldcg(&d.yarn_slot_b[seg * NC_YARN_SLOTS + slot]);
+        float4 sa = ra[0], sb = rb[0];
+#pragma unroll
+        for (uint32_t q = 1; q < NC_YARN_SLOTS; ++q)
+            if (q == slot) {
+                sa = ra[q];
+                sb = rb[q];
+            }
         const float ni = sa.w;
         const V3 wn{sa.x, sa.y, sa.z};
         if (ni <= 0.0f || lsq(wn) < 1.0e-20f) continue;
@@ -1445,8 +1446,80 @@ __device__ __forceinline__ void yarn_friction_segment(const Ctx& ctx, const Fric
         va = with_xyz(va, na);
         vb = with_xyz(vb, nb);
     }
+}
+
+
+// The slot records of a segment's live slots (the others zero).
+__device__ __forceinline__ void friction_records(const Ctx& ctx, uint32_t seg, const uint32_t* st, float4* ra,
+                                                 float4* rb) {
+    const DeviceCloth& d = ctx.d;
+    const uint32_t live = ctx.epoch & 0x3ffffffu;
+#pragma unroll
+    for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q) {
+        const bool on = (st[q] >> 6) == live;
+        ra[q] = on ? __ldcg(&d.yarn_slot_a[seg * NC_YARN_SLOTS + q]) : make_float4(0, 0, 0, 0);
+        rb[q] = on ? __ldcg(&d.yarn_slot_b[seg * NC_YARN_SLOTS + q]) : make_float4(0, 0, 0, 0);
+    }
+}
+
+__device__ __forceinline__ void yarn_friction_segment(const Ctx& ctx, const FrictionSeg& fseg, const float4* s_vw,
+                                                      const float4* s_or, unsigned long long* s_sum) {
+    const uint2 ij = fseg.ij;
+    const float4 pa = px(ctx, ij.x);
+    const float4 pb = px(ctx, ij.y);
+    float4 va = pv(ctx, ij.x);
+    float4 vb = pv(ctx, ij.y);
+    float4 ra[NC_YARN_SLOTS], rb[NC_YARN_SLOTS];
+    friction_records(ctx, fseg.seg, fseg.st, ra, rb);
+    yarn_friction_core(ctx, pa, pb, va, vb, fseg.st, ra, rb, s_vw, s_or, s_sum);
     pv_set(ctx, ij.x, va);
     pv_set(ctx, ij.y, vb);
+}
+
+// Fruit state of the fruit/yarn friction sweep (fruit CTA): the fixed-point
+// velocity and spin sums, the staged velocities and spins.
+__shared__ unsigned long long nc_fric_sum[6u * NC_MAX_FRUITS];
+__shared__ float4 nc_fric_vw[NC_MAX_FRUITS];
+__shared__ float4 nc_fric_or[NC_MAX_FRUITS];
+
+// Stage the substep's recorded segments for the friction sweep (fruit CTA,
+// tile mode): what the sweep reads that no later phase changes, read as
+// soon as the fruit/yarn sweep has ended: segment, endpoints, slot tags and
+// the live slots' records, and for every endpoint the first endpoint of the
+// list with the same particle (where a later colour must see an earlier
+// colour's velocity change).  More segments than NC_FRICTION_STAGE are not
+// staged (the sweep reads them from global memory).
+__device__ void friction_stage(const Ctx& ctx) {
+    if (!ctx.fruit_cta || ctx.fst == nullptr) return;
+    const DeviceCloth& d = ctx.d;
+    FrictionStage& fs = *ctx.fst;
+    const uint32_t listed = min(__ldcg(d.yarn_list_n), d.d_count);
+    const uint32_t n = listed <= NC_FRICTION_STAGE ? listed : NC_FRICTION_STAGE + 1u;
+    if (threadIdx.x == 0) fs.count = n;
+    if (n <= NC_FRICTION_STAGE) {
+        for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) {
+            const uint32_t seg = __ldcg(d.yarn_list + k);
+            const uint2 ij = __ldg(d.d_ij + seg);
+            fs.seg[k] = seg;
+            fs.pid[2u * k] = ij.x;
+            fs.pid[2u * k + 1u] = ij.y;
+#pragma unroll
+            for (uint32_t q = 0; q < NC_YARN_SLOTS; ++q)
+                fs.tag[k][q] = __float_as_uint(__ldcg(&d.yarn_slot_b[seg * NC_YARN_SLOTS + q].z));
+            friction_records(ctx, seg, fs.tag[k], fs.ra[k], fs.rb[k]);
+        }
+        __syncthreads();
+        for (uint32_t e = threadIdx.x; e < 2u * n; e += blockDim.x) {
+            uint32_t r = e;
+            for (uint32_t o = 0; o < e; ++o)
+                if (fs.pid[o] == fs.pid[e]) {
+                    r = o;
+                    break;
+                }
+            fs.rep[e] = static_cast<unsigned short>(r);
+        }
+    }
+    __syncthreads();
 }
 
 // The fruit/yarn friction sweep on the fruit CTA: the yarn colours in order,
@@ -1455,12 +1528,11 @@ __device__ __forceinline__ void yarn_friction_segment(const Ctx& ctx, const Fric
 // particle.  The fruit velocity changes are exact integer sums, so adding
 // them in this one CTA gives the same totals as summing per CTA; the CTA
 // applies them itself.
-__device__ void yarn_friction_sweep(Ctx& ctx) {
-    if (!ctx.fruit_cta) return;
+__device__ void yarn_friction_sweep_global(Ctx& ctx) {
     const DeviceCloth& d = ctx.d;
-    __shared__ unsigned long long s_sum[6u * NC_MAX_FRUITS];
-    __shared__ float4 s_vw[NC_MAX_FRUITS];   // velocity xyz, inverse mass
-    __shared__ float4 s_or[NC_MAX_FRUITS];   // spin xyz, radius
+    unsigned long long* s_sum = nc_fric_sum;
+    float4* s_vw = nc_fric_vw;   // velocity xyz, inverse mass
+    float4* s_or = nc_fric_or;   // spin xyz, radius
     // this thread's first listed segment, loaded once for all colours (the
     // colours then wait only on their particle loads; the loads overlap the
     // fruit staging); further ones (more segments listed than threads) are
@@ -1494,6 +1566,63 @@ __device__ void yarn_friction_sweep(Ctx& ctx) {
     for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
         unsigned long long sm[6];
         for (int k = 0; k < 6; ++k) sm[k] = s_sum[6u * f + k];
+        const float4 v = s_vw[f], w = s_or[f];
+        ctx.fs->v[f] = make_float4(v.x + from_fixed(sm[0]), v.y + from_fixed(sm[1]), v.z + from_fixed(sm[2]), v.w);
+        ctx.fs->o[f] = make_float4(w.x + from_fixed(sm[3]), w.y + from_fixed(sm[4]), w.z + from_fixed(sm[5]), w.w);
+    }
+    __syncthreads();
+}
+
+// The sweep on staged segments (friction_stage, tile mode): the endpoints
+// are loaded once, the colours run in shared memory, the velocities are
+// stored once; unstaged, the sweep over global memory.
+__device__ void yarn_friction_sweep(Ctx& ctx) {
+    if (!ctx.fruit_cta) return;
+    if (ctx.fst == nullptr || ctx.fst->count > NC_FRICTION_STAGE) {
+        yarn_friction_sweep_global(ctx);
+        return;
+    }
+    const DeviceCloth& d = ctx.d;
+    FrictionStage& fs = *ctx.fst;
+    unsigned long long* s_sum = nc_fric_sum;
+    float4* s_vw = nc_fric_vw;
+    float4* s_or = nc_fric_or;
+    const uint32_t n = fs.count;
+    cta_sums_clear(s_sum, 6u * d.f_count);
+    for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
+        const NumiClothFruit& fr = d.fruits[f];
+        const float4 vg = __ldcg(reinterpret_cast<const float4*>(&fr.velocityAndGroundImpulse));
+        const float4 om = __ldcg(reinterpret_cast<const float4*>(&fr.angularVelocity));
+        s_vw[f] = make_float4(vg.x, vg.y, vg.z, __ldcg(&fr.positionAndInverseMass.w));
+        s_or[f] = make_float4(om.x, om.y, om.z, __ldcg(&fr.previousAndRadius.w));
+    }
+    for (uint32_t e = threadIdx.x; e < 2u * n; e += blockDim.x)
+        if (fs.rep[e] == e) {
+            fs.x[e] = px(ctx, fs.pid[e]);
+            fs.v[e] = pv(ctx, fs.pid[e]);
+        }
+    __syncthreads();
+    for (uint32_t b = 0; b < d.n_dist_batches; ++b) {
+        const Batch bt = d.dist_batches[b];
+        if (bt.yarn == 0u) continue;
+        for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) {
+            const uint32_t seg = fs.seg[k];
+            if (seg < bt.first || seg >= bt.first + bt.yarn) continue;
+            const uint32_t ea = fs.rep[2u * k], eb = fs.rep[2u * k + 1u];
+            float4 va = fs.v[ea], vb = fs.v[eb];
+            yarn_friction_core(ctx, fs.x[ea], fs.x[eb], va, vb, fs.tag[k], fs.ra[k], fs.rb[k], s_vw, s_or, s_sum);
+            fs.v[ea] = va;
+            fs.v[eb] = vb;
+        }
+        __syncthreads();
+    }
+    for (uint32_t e = threadIdx.x; e < 2u * n; e += blockDim.x)
+        if (fs.rep[e] == e) pv_set(ctx, fs.pid[e], fs.v[e]);
+    // the fruits' velocities and spins with the friction sums, handed to the
+    // fruit tail in shared memory (the fruit CTA's own fruit state)
+    for (uint32_t f = threadIdx.x; f < d.f_count; f += blockDim.x) {
+        unsigned long long sm[6];
+        for (int q = 0; q < 6; ++q) sm[q] = s_sum[6u * f + q];
         const float4 v = s_vw[f], w = s_or[f];
         ctx.fs->v[f] = make_float4(v.x + from_fixed(sm[0]), v.y + from_fixed(sm[1]), v.z + from_fixed(sm[2]), v.w);
         ctx.fs->o[f] = make_float4(w.x + from_fixed(sm[3]), w.y + from_fixed(sm[4]), w.z + from_fixed(sm[5]), w.w);
@@ -1988,6 +2117,7 @@ __device__ __forceinline__ void run_frame(const DeviceCloth& src, const Schedule
         // descriptor (the fruit CTA keeps its fruit state there instead)
         uint32_t* plan = reinterpret_cast<uint32_t*>(dynamic_smem + nc_fruit_offset());
         ctx.tp = plan;
+        if (ctx.fruit_cta) ctx.fst = reinterpret_cast<FrictionStage*>(dynamic_smem + nc_resident_offset());
         if (!ctx.fruit_cta) {
             if (!nc::tile_stage(ctx, plan)) return;
             ctx.tx = reinterpret_cast<float4*>(

@@ -166,6 +166,7 @@ struct Ctx {
     // shared memory
     const uint32_t* tp;
     float4* tx;
+    FrictionStage* fst;       // tile mode, fruit CTA: the staged friction sweep
 };
 
 __device__ __forceinline__ float4* resident_ptr(const Ctx& c, float4* local_base, uint32_t i) {

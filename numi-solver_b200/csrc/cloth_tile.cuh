@@ -369,6 +369,9 @@ __device__ bool substep_tiles(Ctx& ctx, bool last) {
                 fruit_flush(ctx);
                 if (ctx.c.ground) fruit_ground(ctx);
                 fruit_finalize(ctx);
+                // the friction sweep's recorded segments, while the tiles
+                // run the strain colours
+                if (s.frictions && fruits) friction_stage(ctx);
             }
         } else {
             tile_load(ctx, NC_TILE_STRAIN);

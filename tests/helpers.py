@@ -140,3 +140,31 @@ def per_substep_errors(scene, configs, sched, mode=op.BATCHED):
     finally:
         s.close()
     return np.array(errs), np.array(ferrs) if ferrs else np.zeros(1)
+
+
+# ---------------------------------------------------------------- config 3
+# The differentiable rollout's scene and grip trajectory are the benchmark's
+# (bench.py); the target trajectory here comes from the FP64 oracle.
+from bench import (CONFIG3_LOSS_EVERY, CONFIG3_SCHED, CONFIG3_SUBSTEPS, CONFIG3_TRACKED,  # noqa: E402
+                   config3_configs, config3_scene)
+
+
+def config3_targets(scene: nc.SceneArrays, cfg: np.ndarray, seed: int = 3):
+    """32 seeded tracked particles and their target trajectory: the FP64
+    oracle (reference order) at log-compliances shifted by N(0, 0.3)."""
+    rng = np.random.default_rng(seed)
+    tracked = np.sort(rng.choice(scene.n, CONFIG3_TRACKED, replace=False)).astype(np.uint32)
+    shift = np.exp(rng.normal(0.0, 0.3, size=3))
+    osc = op.from_abi(scene)
+    kinds = osc.distances["kind"]
+    osc.distances["compliance"][kinds != 3] *= shift[0]
+    osc.distances["compliance"][kinds == 3] *= shift[1]
+    osc.bends["compliance"] *= shift[2]
+    o = op.Oracle(osc, 64)
+    subs = op.substeps_from_configs(cfg)
+    osched = op.schedule_from_abi(nc.Schedule.make(**CONFIG3_SCHED), op.SERIAL)
+    out = []
+    for k in range(CONFIG3_SUBSTEPS // CONFIG3_LOSS_EVERY):
+        o.step(subs[k * CONFIG3_LOSS_EVERY:(k + 1) * CONFIG3_LOSS_EVERY], osched)
+        out.append(o.read()["particles"]["x"][tracked].copy())
+    return tracked, np.stack(out), o.stats()
