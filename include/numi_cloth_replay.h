@@ -85,7 +85,7 @@ typedef struct NumiClothReplayResult {
     double residuals[4];          /* numi_cloth_residuals */
     unsigned long long selfContacts;
     unsigned long long edgeContacts[2];
-    uint32_t masks[2];            /* released fruits, mouth candidates */
+    uint32_t masks[2];            /* mouth candidates, released fruits (numi_cloth_release_masks) */
     uint32_t reconcileMax;        /* most reconciliation passes of a substep */
     uint32_t certificateMax;      /* most certificate passes of a substep */
     double seconds;               /* wall time of the first run's frames */

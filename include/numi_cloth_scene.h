@@ -81,7 +81,8 @@ typedef struct NumiClothSquareSpec {
     double strainLimit;        /* max relative extension of warp/weft */
     double gripCompliance;     /* m/N; corner attachments */
     uint32_t gripCorners;      /* 0, 1 (corner 0) or 2 (corners 0 and side-1) */
-    uint32_t fruitCount;       /* spheres */
+    uint32_t fruitCount;       /* spheres (<= 64), seeded, none overlapping another;
+                                  the builder returns NULL when 4096 draws find no room */
     double fruitRadiusMin, fruitRadiusMax, fruitMass;
     double fruitHeightMin, fruitHeightMax;   /* height of the sphere bottom */
     double thickness;          /* yarn radius r; self contact distance 2r */

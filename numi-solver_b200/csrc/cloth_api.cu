@@ -50,6 +50,7 @@ namespace {
 
 constexpr uint32_t kSnapshotSlots = 8;
 constexpr uint32_t kResidentChunk = 4096;   // particles a CTA holds in resident mode
+constexpr uint32_t kResidentClusterChunk = 256;   // default chunk of a small resident cloth
 
 struct Snapshot {
     bool valid = false;
@@ -629,7 +630,22 @@ cudaError_t launch(numi_cloth* h, uint32_t substeps, const Schedule& s, uint32_t
     cudaError_t e = cudaMemsetAsync(h->d.bar_count, 0, 32 * sizeof(unsigned long long), h->stream);
     if (e != cudaSuccess) return e;
     h->last_substeps = substeps;
-    const size_t smem = h->smem;
+    size_t smem = h->smem;
+    if (edge) {
+        // the edge/edge phases' box-tree sort keys after the launch's own
+        // shared memory, where the device has room
+        int max_optin = 0;
+        cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
+        cudaFuncAttributes fe{};
+        cudaFuncGetAttributes(&fe, frame_fn(true));
+        const size_t at = nc_round256(smem);
+        if (at + NC_EDGE_TREE_KEY_BYTES + fe.sharedSizeBytes <= static_cast<size_t>(max_optin) &&
+            raise_smem(frame_fn(true), at + NC_EDGE_TREE_KEY_BYTES) == cudaSuccess) {
+            sc.tree_keys = static_cast<uint32_t>(at);
+            smem = at + NC_EDGE_TREE_KEY_BYTES;
+        }
+        cudaGetLastError();
+    }
     if (h->cluster > 0) {
         cudaLaunchConfig_t cfg{};
         cfg.gridDim = dim3(h->cluster);
@@ -847,6 +863,8 @@ int prepare_edge_grid(numi_cloth* h, bool primitive, uint32_t substeps, float ra
         e.edge_lv = h->buf.alloc<uint32_t>(cap);
         e.edge_level = h->buf.alloc<uint32_t>(d.n);
         e.edge_qbox_raw = h->buf.alloc<float>(6u * d.y_count);
+        e.edge_tree = h->buf.alloc<uint32_t>(2u * d.y_count);
+        e.edge_centre = h->buf.alloc<float4>(d.y_count);
         e.edge_rec = h->buf.alloc<EdgeRecord>(cap);
         e.edge_ctl = h->buf.alloc<uint32_t>(8);
         e.edge_stats = h->buf.alloc<unsigned long long>(2);
@@ -855,6 +873,7 @@ int prepare_edge_grid(numi_cloth* h, bool primitive, uint32_t substeps, float ra
             !e.edge_pairs || !e.edge_xb || !e.edge_pb || !e.edge_built_radius || !e.edge_sph || !e.edge_x0 ||
             !e.edge_path || !e.edge_cand || !e.edge_order || !e.edge_sorted || !e.edge_new || !e.edge_done || !e.edge_rec ||
             !e.edge_ctl || !e.edge_stats || !e.edge_red || !e.edge_lv || !e.edge_level || !e.edge_qbox_raw || !e.edge_bbox ||
+            !e.edge_tree || !e.edge_centre ||
             !e.edge_loc_off || !e.edge_loc_idx)
             return NUMI_CLOTH_ENOMEM;
         e.edge_mask = buckets - 1u;
@@ -1056,9 +1075,18 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
     uint32_t want_resident = 1;
     env_u32("NUMI_CLOTH_RESIDENT", want_resident);
     const uint32_t resident_limit = want_resident >= 2u ? 16u * kResidentChunk : kResidentChunk;
-    if (want_resident != 0u && forced == 0 && n > 0u && n <= resident_limit) {
+    // Particles each CTA of a resident cluster holds: a cloth of up to
+    // 4096 particles runs on a cluster of ceil(n / 256) CTAs (up to 16),
+    // which measured 1.3-1.5x faster on the 1,400-particle bag than one CTA
+    // holding it all (more threads per colour batch, the same bits); with
+    // NUMI_CLOTH_RESIDENT=2 each CTA holds 4096.  NUMI_CLOTH_RESIDENT_CHUNK
+    // (a power of two, 64 to 4096) overrides it.
+    uint32_t chunk = want_resident >= 2u ? kResidentChunk : kResidentClusterChunk;
+    env_u32("NUMI_CLOTH_RESIDENT_CHUNK", chunk);
+    if (chunk < 64u || chunk > kResidentChunk || (chunk & (chunk - 1u)) != 0u) chunk = kResidentChunk;
+    if (want_resident != 0u && forced == 0 && n > 0u && n <= resident_limit && (n + chunk - 1u) / chunk <= 16u) {
         uint32_t shift = 4u;
-        while ((1u << shift) < std::min(n, kResidentChunk)) ++shift;
+        while ((1u << shift) < std::min(n, chunk)) ++shift;
         const uint32_t ranks = (n + (1u << shift) - 1u) >> shift;
         const size_t smem = nc_resident_offset() + 2u * (static_cast<size_t>(1u) << shift) * sizeof(float4);
         int max_optin = 0;
@@ -1256,8 +1284,8 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
     h->neighbours = prepare_neighbours(h, scene);
     // Tile mode of the cooperative grid (cloth_tile.cuh): one 512-thread CTA
     // per SM, used by the launches whose schedule it covers;
-    // NUMI_CLOTH_TILES=1 turns it on, 0 keeps the colour-by-colour schedule.
-    uint32_t want_tiles = 0;
+    // on by default; NUMI_CLOTH_TILES=0 keeps the colour-by-colour schedule.
+    uint32_t want_tiles = 1;
     env_u32("NUMI_CLOTH_TILES", want_tiles);
     if (want_tiles != 0u && h->grid > 1u && h->cluster == 0u && d.resident == 0u && K == 0u) {
         int max_optin = 0;
@@ -1829,12 +1857,15 @@ int batch_shape(numi_cloth_batch* b, uint32_t chunk, uint32_t block) {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
     int per_sm = 1 << 30;
     for (bool edge : {false, true}) {
+        // the edge/edge kernel also holds the box tree's sort keys
+        const size_t bytes = edge ? nc_round256(smem) + NC_EDGE_TREE_KEY_BYTES : smem;
         cudaFuncAttributes fa{};
         if (cudaFuncGetAttributes(&fa, batch_fn(edge)) != cudaSuccess) return NUMI_CLOTH_ECUDA;
-        if (smem + fa.sharedSizeBytes > static_cast<size_t>(optin)) return NUMI_CLOTH_EINVAL;
-        if (raise_smem(batch_fn(edge), smem) != cudaSuccess) return NUMI_CLOTH_ECUDA;
+        if (bytes + fa.sharedSizeBytes > static_cast<size_t>(optin)) return NUMI_CLOTH_EINVAL;
+        if (raise_smem(batch_fn(edge), bytes) != cudaSuccess) return NUMI_CLOTH_ECUDA;
+        if (edge) continue;   // launched without co-residence
         int k = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, batch_fn(edge), static_cast<int>(block), smem) !=
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, batch_fn(edge), static_cast<int>(block), bytes) !=
             cudaSuccess)
             return NUMI_CLOTH_EINVAL;
         per_sm = std::min(per_sm, k);
@@ -1925,7 +1956,12 @@ cudaError_t batch_launch(numi_cloth_batch* b, const NumiClothConfig* configs, ui
     unsigned int* queue = b->queue;
     const DeviceCloth* cloths = b->d_cloths;
     void* args[] = {&cloths, const_cast<uint32_t*>(&count), &sc, &queue};
-    e = cudaLaunchKernel(batch_fn(sc.primitive_self != 0u), dim3(b->ctas), dim3(b->block), args, b->smem, b->stream);
+    size_t smem = b->smem;
+    if (sc.primitive_self != 0u) {   // the box tree's sort keys (batch_shape checked the room)
+        sc.tree_keys = static_cast<uint32_t>(nc_round256(smem));
+        smem = nc_round256(smem) + NC_EDGE_TREE_KEY_BYTES;
+    }
+    e = cudaLaunchKernel(batch_fn(sc.primitive_self != 0u), dim3(b->ctas), dim3(b->block), args, smem, b->stream);
     if (e != cudaSuccess) return e;
     numi_cloth_epoch_kernel<<<1, 1, 0, b->stream>>>(b->epoch, substeps);
     return cudaGetLastError();

@@ -207,6 +207,9 @@ struct DeviceCloth {
     float4* edge_x0;              // [n]
     float4* edge_sph;             // [y_count] pass spheres (centre, radius)
     float* edge_qbox_raw;         // [6 * y_count] a first segment's tree-query box of the pass
+    uint32_t* edge_tree;          // [2 * y_count] the pass's box-tree leaf order: position -> segment,
+                                  //   then segment -> position (edge_tree_order)
+    float4* edge_centre;          // [y_count] centres of the pass-start boxes of the tree
     float* edge_path;             // [n]
     uint4* edge_cand;             // [edge_cap]
     unsigned long long* edge_order;    // [edge_cap]
@@ -271,6 +274,9 @@ struct Schedule {
     uint32_t cfg_offset;
     // 1: the launch runs in tile mode (cloth_tile.cuh)
     uint32_t tiles;
+    // edge/edge launches: byte offset in dynamic shared memory of the box
+    // tree's sort keys (edge_tree_order), 0 when the launch has none
+    uint32_t tree_keys;
 };
 
 // Fruit-side state kept in the shared memory of the fruit CTA for a whole

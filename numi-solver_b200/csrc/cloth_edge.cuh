@@ -724,6 +724,156 @@ __device__ void edge_candidates(Ctx& ctx, bool swept, bool rebuilt) {
     }
 }
 
+// The leaf order of the reference's box tree over the pass-start segment
+// boxes (makeCollisionBVH / buildCollisionBVHNode,
+// tools/cloth_bag.cpp:3780-3842), in which a segment meets its candidates
+// (gatherCollisionCandidates :3844-3878 visits the left subtree first, so
+// the candidates come in ascending tree position).  A node of more than 8
+// primitives orders them by box centre along the longest axis of its
+// centres (ties by index) and splits them at the middle; the node ranges
+// follow from the count alone, so the tree is built level by level: the
+// centre bounds of every splitting node (a warp each), then one bitonic sort
+// of (node, centre, index) keys in shared memory orders every node of the
+// level at once.  CTA 0, all threads; at most NC_EDGE_TREE_MAX segments.
+// Leaves edge_tree[p] = segment at position p, edge_tree[m + s] = position
+// of segment s.
+#define NC_EDGE_TREE_MAX 4096u
+#define NC_EDGE_TREE_KEY_BYTES (NC_EDGE_TREE_MAX * 8u)
+__shared__ unsigned char nc_edge_tree_axis[NC_EDGE_TREE_MAX / 8u];
+
+// The node of position p (or of index j, a path of `level` left/right bits)
+// at depth `level`; false past a leaf.
+__device__ __forceinline__ bool tree_node_of_path(uint32_t m, uint32_t level, uint32_t j, uint32_t& b, uint32_t& e) {
+    b = 0u;
+    e = m;
+    for (uint32_t l = 0; l < level; ++l) {
+        if (e - b <= 8u) return false;
+        const uint32_t mid = b + (e - b) / 2u;
+        if ((j >> (level - 1u - l)) & 1u)
+            b = mid;
+        else
+            e = mid;
+    }
+    return true;
+}
+__device__ __forceinline__ uint32_t tree_path_of_position(uint32_t m, uint32_t level, uint32_t p, uint32_t& b,
+                                                          uint32_t& e) {
+    b = 0u;
+    e = m;
+    uint32_t j = 0u;
+    for (uint32_t l = 0; l < level && e - b > 8u; ++l) {
+        const uint32_t mid = b + (e - b) / 2u;
+        j <<= 1;
+        if (p >= mid) {
+            b = mid;
+            j |= 1u;
+        } else {
+            e = mid;
+        }
+    }
+    return j;
+}
+// Float bits in an order of unsigned integers (zeros of either sign equal).
+__device__ __forceinline__ uint32_t ordered_bits(float v) {
+    if (v == 0.0f) v = 0.0f;
+    const uint32_t u = __float_as_uint(v);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+__device__ void edge_tree_order(const Ctx& ctx, bool swept) {
+    const DeviceCloth& d = ctx.d;
+    // the sort keys, in the launch's dynamic shared memory
+    unsigned long long* nc_edge_tree_keys = reinterpret_cast<unsigned long long*>(nc_frame_smem + ctx.s.tree_keys);
+    const uint32_t m = d.y_count;
+    const float ex = 0.5f * (2.0f * ctx.c.radius);
+    uint32_t* ord = d.edge_tree;
+    for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
+        const uint2 ab = __ldg(d.y_ij + k);
+        const EdgeBox bx = edge_box(xyz(ld(d.edge_x0 + ab.x)), xyz(ld(d.edge_x0 + ab.y)), xyz(ld(d.xp + ab.x)),
+                                    xyz(ld(d.xp + ab.y)), swept, ex);
+        d.edge_centre[k] = make_float4(0.5f * (bx.lo.x + bx.hi.x), 0.5f * (bx.lo.y + bx.hi.y),
+                                       0.5f * (bx.lo.z + bx.hi.z), 0.0f);
+        ord[k] = k;
+    }
+    uint32_t size = 4096u;
+    while (size / 2u >= m && size > 2u) size /= 2u;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u, warps = blockDim.x >> 5;
+    __syncthreads();
+    for (uint32_t level = 0; level < 32u; ++level) {
+        // centre bounds and axis of every node of the level that splits
+        const uint32_t nodes = 1u << level;
+        bool any = false;
+        for (uint32_t j = warp; j < nodes && j < NC_EDGE_TREE_MAX / 8u; j += warps) {
+            uint32_t b, e;
+            if (!tree_node_of_path(m, level, j, b, e) || e - b <= 8u) continue;
+            V3 lo{INFINITY, INFINITY, INFINITY}, hi{-INFINITY, -INFINITY, -INFINITY};
+            for (uint32_t p = b + lane; p < e; p += 32u) {
+                const float4 c = __ldcg(d.edge_centre + __ldcg(ord + p));
+                lo = V3{fminf(lo.x, c.x), fminf(lo.y, c.y), fminf(lo.z, c.z)};
+                hi = V3{fmaxf(hi.x, c.x), fmaxf(hi.y, c.y), fmaxf(hi.z, c.z)};
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                lo.x = fminf(lo.x, __shfl_xor_sync(0xffffffffu, lo.x, o));
+                lo.y = fminf(lo.y, __shfl_xor_sync(0xffffffffu, lo.y, o));
+                lo.z = fminf(lo.z, __shfl_xor_sync(0xffffffffu, lo.z, o));
+                hi.x = fmaxf(hi.x, __shfl_xor_sync(0xffffffffu, hi.x, o));
+                hi.y = fmaxf(hi.y, __shfl_xor_sync(0xffffffffu, hi.y, o));
+                hi.z = fmaxf(hi.z, __shfl_xor_sync(0xffffffffu, hi.z, o));
+            }
+            const V3 ext = hi - lo;
+            if (lane == 0)
+                nc_edge_tree_axis[j] = static_cast<unsigned char>(
+                    ext.y > ext.x ? (ext.z > ext.y ? 2u : 1u) : (ext.z > ext.x ? 2u : 0u));
+            any = true;
+        }
+        if (!__syncthreads_or(any)) break;
+        // keys: (node start, centre along the node's axis, segment); a
+        // position in a leaf keeps its place (its offset in the leaf)
+        for (uint32_t p = threadIdx.x; p < size; p += blockDim.x) {
+            unsigned long long key = ~0ull;
+            if (p < m) {
+                uint32_t b, e;
+                const uint32_t j = tree_path_of_position(m, level, p, b, e);
+                const uint32_t s = __ldcg(ord + p);
+                if (e - b <= 8u) {
+                    key = (static_cast<unsigned long long>(b) << 52) | (p - b);
+                } else {
+                    const float4 c = __ldcg(d.edge_centre + s);
+                    const uint32_t axis = nc_edge_tree_axis[j];
+                    const float v = axis == 0u ? c.x : (axis == 1u ? c.y : c.z);
+                    key = (static_cast<unsigned long long>(b) << 52) |
+                          (static_cast<unsigned long long>(ordered_bits(v)) << 12) | s;
+                }
+            }
+            nc_edge_tree_keys[p] = key;
+        }
+        __syncthreads();
+        for (uint32_t k = 2u; k <= size; k <<= 1) {
+            for (uint32_t jj = k >> 1; jj > 0u; jj >>= 1) {
+                for (uint32_t i = threadIdx.x; i < size; i += blockDim.x) {
+                    const uint32_t ixj = i ^ jj;
+                    if (ixj > i) {
+                        const unsigned long long a = nc_edge_tree_keys[i], c = nc_edge_tree_keys[ixj];
+                        if ((a > c) == ((i & k) == 0u)) {
+                            nc_edge_tree_keys[i] = c;
+                            nc_edge_tree_keys[ixj] = a;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        for (uint32_t p = threadIdx.x; p < m; p += blockDim.x) {
+            uint32_t b, e;
+            tree_path_of_position(m, level, p, b, e);
+            if (e - b > 8u) ord[p] = static_cast<uint32_t>(nc_edge_tree_keys[p] & 0xfffu);
+        }
+        __syncthreads();
+    }
+    for (uint32_t p = threadIdx.x; p < m; p += blockDim.x) ord[m + __ldcg(ord + p)] = p;
+    __syncthreads();
+}
+
 // Phase 3 (CTA 0): sort the ordered pairs, undo the previous round, then
 // resolve them in the reference's order as wavefronts: a pair's level is one
 // more than the last level of any of its four particles, so pairs of one
@@ -763,18 +913,34 @@ __device__ void edge_resolve(Ctx& ctx, bool swept, bool redo) {
         }
     }
     __shared__ uint32_t s_top;
+    // A segment with several ordered pairs meets them in the tree's leaf
+    // order (edge_tree_order), else the first segments' order is all that
+    // matters: pairs are sorted by (first, tree position of the second).
+    bool mine = false;
+    for (uint32_t k = threadIdx.x; k < count && !mine; k += blockDim.x) {
+        const uint32_t first = static_cast<uint32_t>(__ldcg(d.edge_order + k) >> 32);
+        for (uint32_t m = 0; m < count && !mine; ++m)
+            mine = m != k && static_cast<uint32_t>(__ldcg(d.edge_order + m) >> 32) == first;
+    }
+    const bool tree = __syncthreads_or(mine) != 0 && d.y_count <= NC_EDGE_TREE_MAX && ctx.s.tree_keys != 0u;
+    if (tree) edge_tree_order(ctx, swept);
+    const uint32_t* tpos = d.edge_tree + d.y_count;
+    auto sort_key = [&](unsigned long long key) {
+        return tree ? ((key & 0xffffffff00000000ull) | __ldcg(tpos + static_cast<uint32_t>(key))) : key;
+    };
     if (staged) {
-        for (uint32_t k = threadIdx.x; k < count; k += blockDim.x) s_key[k] = __ldcg(d.edge_order + k);
+        for (uint32_t k = threadIdx.x; k < count; k += blockDim.x) s_key[k] = sort_key(__ldcg(d.edge_order + k));
         __syncthreads();
         // rank sort: the keys are distinct
         for (uint32_t k = threadIdx.x; k < count; k += blockDim.x) {
             const unsigned long long key = s_key[k];
             uint32_t rank = 0;
             for (uint32_t m = 0; m < count; ++m) rank += s_key[m] < key ? 1u : 0u;
-            s_sorted[rank] = key;
-            d.edge_sorted[rank] = key;
-            const uint2 sa = __ldg(d.y_ij + static_cast<uint32_t>(key >> 32)),
-                        sb = __ldg(d.y_ij + static_cast<uint32_t>(key));
+            const unsigned long long orig = __ldcg(d.edge_order + k);
+            s_sorted[rank] = orig;
+            d.edge_sorted[rank] = orig;
+            const uint2 sa = __ldg(d.y_ij + static_cast<uint32_t>(orig >> 32)),
+                        sb = __ldg(d.y_ij + static_cast<uint32_t>(orig));
             s_id[rank] = make_uint4(sa.x, sa.y, sb.x, sb.y);
         }
         __syncthreads();
@@ -813,10 +979,11 @@ __device__ void edge_resolve(Ctx& ctx, bool swept, bool redo) {
     } else {
         // rank sort: the keys are distinct
         for (uint32_t k = threadIdx.x; k < count; k += blockDim.x) {
-            const unsigned long long key = __ldcg(d.edge_order + k);
+            const unsigned long long orig = __ldcg(d.edge_order + k);
+            const unsigned long long key = sort_key(orig);
             uint32_t rank = 0;
-            for (uint32_t m = 0; m < count; ++m) rank += __ldcg(d.edge_order + m) < key ? 1u : 0u;
-            d.edge_sorted[rank] = key;
+            for (uint32_t m = 0; m < count; ++m) rank += sort_key(__ldcg(d.edge_order + m)) < key ? 1u : 0u;
+            d.edge_sorted[rank] = orig;
         }
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -901,6 +1068,19 @@ __device__ void edge_resolve(Ctx& ctx, bool swept, bool redo) {
         uint32_t done = 0;
         for (uint32_t k = 0; k < count; ++k)
             if (lvp[k] & 0x40000000u) d.edge_done[done++] = k;
+        if (tree) {
+            // in tree order within a first segment: back to key order
+            for (uint32_t a = 1; a < done; ++a) {
+                const uint32_t v = d.edge_done[a];
+                const unsigned long long kv = d.edge_sorted[v];
+                uint32_t b = a;
+                while (b > 0u && d.edge_sorted[d.edge_done[b - 1u]] > kv) {
+                    d.edge_done[b] = d.edge_done[b - 1u];
+                    --b;
+                }
+                d.edge_done[b] = v;
+            }
+        }
         d.edge_ctl[4] = done;
     }
 }

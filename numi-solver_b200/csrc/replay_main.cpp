@@ -129,7 +129,7 @@ int main(int argc, char** argv) {
                 "selected_patch_center_ring=%u patch_particles_unique=%s patch_topology_exact=%s "
                 "attachment_generation=%u failure=%u deterministic=%s state_hash=0x%llx replay_hash=0x%llx\n",
                 r.residuals[0], r.residuals[1], r.residuals[2], r.residuals[3], r.selfContacts, r.edgeContacts[0],
-                r.edgeContacts[1], r.masks[0], r.masks[1], r.reconcileMax, r.certificateMax, r.regrabCount,
+                r.edgeContacts[1], r.masks[1], r.masks[0], r.reconcileMax, r.certificateMax, r.regrabCount,
                 static_cast<unsigned long long>(r.inactiveGripSubsteps), r.patchSelections, r.maxPatchRingShift,
                 r.patchCenter, r.patchParticlesUnique ? "true" : "false", r.patchTopologyExact ? "true" : "false",
                 r.generation, r.failure, deterministic ? "true" : "false", static_cast<unsigned long long>(r.hash),
@@ -141,7 +141,7 @@ int main(int argc, char** argv) {
     // the pickup outcome and the spatial patch checks
     const bool patch_ok = r.patchSelections == 0u ||
                           (r.patchSelections == r.regrabCount && r.patchParticlesUnique && r.patchTopologyExact);
-    const bool pickup_ok = o.scenario != NUMI_CLOTH_SCENARIO_PICKUP || __builtin_popcount(r.masks[0]) >= 2;
+    const bool pickup_ok = o.scenario != NUMI_CLOTH_SCENARIO_PICKUP || __builtin_popcount(r.masks[1]) >= 2;
     const bool pass = r.failure == 0u && deterministic && patch_ok && pickup_ok && r.residuals[0] < 2.0e-6 &&
                       r.residuals[1] < 2.0e-6 && r.residuals[2] < 2.0e-6;
     std::printf("result=%s\n", pass ? "PASS" : "FAIL");

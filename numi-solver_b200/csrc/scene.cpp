@@ -708,14 +708,37 @@ numi_cloth_scene_t* numi_cloth_scene_square(const NumiClothSquareSpec* spec, con
                 s->grips.push_back(g);
             }
         }
+        // Seeded spheres, each redrawn (up to kSphereDraws times) until it
+        // overlaps no earlier sphere, so the scene starts without fruit/fruit
+        // penetration.
+        constexpr uint32_t kSphereDraws = 4096;
         uint64_t rng = spec->seed;
+        std::vector<D3> centres;
+        std::vector<double> radii;
         for (uint32_t k = 0; k < spec->fruitCount; ++k) {
-            const double x = -half + 2.0 * half * uniform01(rng);
-            const double y = -half + 2.0 * half * uniform01(rng);
-            const double bottom = spec->fruitHeightMin + (spec->fruitHeightMax - spec->fruitHeightMin) * uniform01(rng);
-            const double r = spec->fruitRadiusMin + (spec->fruitRadiusMax - spec->fruitRadiusMin) * uniform01(rng);
-            const double z = bottom + r;
-            s->fruits.push_back(make_fruit(D3{x, y, z}, r, spec->fruitMass, k & 3u));
+            D3 c{};
+            double r = 0.0;
+            bool clear = false;
+            for (uint32_t draw = 0; draw < kSphereDraws && !clear; ++draw) {
+                const double x = -half + 2.0 * half * uniform01(rng);
+                const double y = -half + 2.0 * half * uniform01(rng);
+                const double bottom =
+                    spec->fruitHeightMin + (spec->fruitHeightMax - spec->fruitHeightMin) * uniform01(rng);
+                r = spec->fruitRadiusMin + (spec->fruitRadiusMax - spec->fruitRadiusMin) * uniform01(rng);
+                c = D3{x, y, bottom + r};
+                clear = true;
+                for (size_t j = 0; j < centres.size() && clear; ++j) {
+                    const double dx = c.x - centres[j].x, dy = c.y - centres[j].y, dz = c.z - centres[j].z;
+                    clear = dx * dx + dy * dy + dz * dz >= (r + radii[j]) * (r + radii[j]);
+                }
+            }
+            if (!clear) {
+                delete s;
+                return nullptr;   // no room for the requested spheres
+            }
+            centres.push_back(c);
+            radii.push_back(r);
+            s->fruits.push_back(make_fruit(c, r, spec->fruitMass, k & 3u));
         }
         add_pairs(s);
         s->grid_width = side;

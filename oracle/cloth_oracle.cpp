@@ -1552,9 +1552,10 @@ struct Sim {
 
     // The kernels' order (restates solvePrimitiveSelfCollision,
     // tools/cloth_bag.cpp:3880-3993): the same Gauss-Seidel sweep with the
-    // same pass-start spheres and current query boxes, but the candidates
-    // of a segment in ascending index order instead of the tree's leaf order.
-    R edge_batched(bool swept, R dt) { return edge_serial(swept, dt, true); }
+    // same pass-start spheres, current query boxes and tree leaf order; a
+    // cloth of more than 4,096 yarn segments (the kernels' tree limit) takes
+    // a segment's candidates in ascending index order instead.
+    R edge_batched(bool swept, R dt) { return edge_serial(swept, dt, ya.size() > 4096u); }
     // applyClothSelfFriction is already in key order, which the kernels keep.
     void edge_friction_batched(R mu) { edge_friction_serial(mu); }
 
@@ -2063,6 +2064,24 @@ void write_state(Sim<R>& s, const OracleParticle* ps, const OracleFruit* fs) {
         }
 }
 
+// The grips' attachment state (particle, generation, patch ring, offset,
+// multiplier, capture distance and error), as a reference run left it.
+template <class R>
+void write_grips(Sim<R>& s, const OracleGrip* gs) {
+    for (size_t k = 0; k < s.grips.size(); ++k) {
+        const OracleGrip& o = gs[k];
+        auto& g = s.grips[k];
+        g.particle = o.particle;
+        g.gen = o.gen;
+        g.ring = o.ring;
+        g.offset = {R(o.offset[0]), R(o.offset[1]), R(o.offset[2])};
+        g.compliance = R(o.compliance);
+        g.lambda = {R(o.lambda[0]), R(o.lambda[1]), R(o.lambda[2])};
+        g.capture = R(o.capture);
+        g.error = R(o.error);
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -2123,6 +2142,15 @@ void oracle_write(void* p, const OracleParticle* ps, const OracleFruit* fs) {
         write_state(*h->f, ps, fs);
     else
         write_state(*h->d, ps, fs);
+}
+
+void oracle_write_grips(void* p, const OracleGrip* gs) {
+    auto* h = static_cast<Handle*>(p);
+    if (!h || !gs) return;
+    if (h->f)
+        write_grips(*h->f, gs);
+    else
+        write_grips(*h->d, gs);
 }
 
 void oracle_residuals(void* p, double out[4]) {

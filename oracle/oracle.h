@@ -133,6 +133,7 @@ void oracle_read(void* h, OracleParticle* particles, OracleDistance* distances, 
                  OracleFruit* fruits, OraclePair* pairs);
 /* Overwrite particle and fruit state. */
 void oracle_write(void* h, const OracleParticle* particles, const OracleFruit* fruits);
+void oracle_write_grips(void* h, const OracleGrip* grips);
 /* FP64 residuals of the current state: strain, ground, fruit/yarn, self. */
 void oracle_residuals(void* h, double out[4]);
 /* Release masks (mouth candidates, released) and counters:

@@ -122,6 +122,7 @@ def lib() -> ctypes.CDLL:
         L.oracle_step.argtypes = [vp, vp, ctypes.c_uint32, ctypes.POINTER(OSchedule)]
         L.oracle_read.argtypes = [vp, vp, vp, vp, vp, vp]
         L.oracle_write.argtypes = [vp, vp, vp]
+        L.oracle_write_grips.argtypes = [vp, vp]
         L.oracle_residuals.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
         L.oracle_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64)]
         L.oracle_self_pass.restype = ctypes.c_double
@@ -318,8 +319,10 @@ class Oracle:
         lib().oracle_read(self._h, _p(P), _p(D), _p(G), _p(F), _p(PR))
         return {"particles": P, "distances": D, "grips": G, "fruits": F, "pairs": PR}
 
-    def write(self, particles=None, fruits=None):
+    def write(self, particles=None, fruits=None, grips=None):
         lib().oracle_write(self._h, _p(particles), _p(fruits))
+        if grips is not None and len(grips):
+            lib().oracle_write_grips(self._h, _p(np.ascontiguousarray(grips, GRIP)))
 
     def residuals(self) -> np.ndarray:
         out = (ctypes.c_double * 4)()

@@ -8,7 +8,7 @@ z = height, warp / weft distances with the strain limit, both shear
 diagonals, skip-one bends, first-fit colouring (64-bit masks, record order)
 with the yarn and shear colour spaces apart and each colour's yarn segments
 first, two gripped corners, seeded spheres (SplitMix64; Steele, Lea and
-Flood 2014), every value rounded once to FP32 as the ABI records are and
+Flood 2014) redrawn until each overlaps no earlier one, every value rounded once to FP32 as the ABI records are and
 widened back, so the oracle runs the same workload as the GPU.  The
 authored material values are the reference's defaults
 (include/numi/cloth_material.h:15-60).
@@ -28,6 +28,7 @@ FRUIT_PAIR_FRICTION = 0.30
 ROLLING_RESISTANCE = 0.015
 AERO = (1.10, 0.010, 0.47, 0.010)   # yarn crossflow, yarn skin, fruit drag, fruit rotational drag
 MASK64 = (1 << 64) - 1
+SPHERE_DRAWS = 4096   # draws per sphere before the builder gives up
 
 
 def _f32(v):
@@ -128,19 +129,28 @@ def build(side: int = 256, spacing: float = 0.004, height: float = 0.5, particle
         G[g]["gen"] = 1
         G[g]["offset"] = _f32(pos[i] - pos[0])
         G[g]["compliance"] = _f32(grip_compliance)
-    # seeded spheres
+    # seeded spheres, each redrawn until it overlaps no earlier sphere
     F = np.zeros(fruit_count, op.FRUIT)
     state = seed
+    placed = []
     for k in range(fruit_count):
-        state, u = _uniform01(state)
-        x = -half + 2.0 * half * u
-        state, u = _uniform01(state)
-        y = -half + 2.0 * half * u
-        state, u = _uniform01(state)
-        bottom = fruit_height[0] + (fruit_height[1] - fruit_height[0]) * u
-        state, u = _uniform01(state)
-        r = fruit_radius[0] + (fruit_radius[1] - fruit_radius[0]) * u
-        F[k]["x"] = _f32([x, y, bottom + r])
+        for _ in range(SPHERE_DRAWS):
+            state, u = _uniform01(state)
+            x = -half + 2.0 * half * u
+            state, u = _uniform01(state)
+            y = -half + 2.0 * half * u
+            state, u = _uniform01(state)
+            bottom = fruit_height[0] + (fruit_height[1] - fruit_height[0]) * u
+            state, u = _uniform01(state)
+            r = fruit_radius[0] + (fruit_radius[1] - fruit_radius[0]) * u
+            z = bottom + r
+            if all((x - a) * (x - a) + (y - b) * (y - b) + (z - c) * (z - c) >= (r + q) * (r + q)
+                   for a, b, c, q in placed):
+                break
+        else:
+            raise ValueError("no room for the requested spheres")
+        placed.append((x, y, z, r))
+        F[k]["x"] = _f32([x, y, z])
         F[k]["prev"] = F[k]["x"]
         F[k]["w"] = _f32(1.0 / fruit_mass)
         F[k]["radius"] = _f32(r)

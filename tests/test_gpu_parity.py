@@ -77,7 +77,9 @@ def test_bag_frame_bitexact_and_fp64():
     cfg = bag_frame_configs(scene, 0, 48, dt)
     s = nc.Schedule.make(**FULL)
     g = run_gpu(scene, cfg, s)
-    assert g["info"]["grid"] == 1   # resident single-CTA path
+    # resident cluster path: 256 particles in the shared memory of each CTA
+    n = len(scene.particles)
+    assert g["info"]["resident"] and g["info"]["grid"] == (n + 255) // 256 == g["info"]["cluster"]
     o32 = run_oracle(scene, cfg, s, bits=32)
     _check_bitexact(g, o32)
     o64 = run_oracle(scene, cfg, s, bits=64)
@@ -116,15 +118,19 @@ def test_cluster_equals_cooperative_grid():
     _check_bitexact(clus, o)
 
 
-@pytest.mark.parametrize("side,ranks", [(40, 1), (96, 3), (128, 4)])
-def test_resident_equals_global(side, ranks):
+@pytest.mark.parametrize("side,ranks,chunk", [(40, 1, "4096"), (40, 7, None), (60, 15, "256"), (96, 3, None),
+                                              (128, 4, None)])
+def test_resident_equals_global(side, ranks, chunk):
     """Particles resident in the shared memory of one CTA or spread over a
     cluster's distributed shared memory give the same bits as particles in
     global memory, and as the oracle."""
     scene = small_square(side=side, fruits=12)
     cfg = nc.substep_configs(scene, 12)
     s = nc.Schedule.make(**FULL)
-    res = run_gpu(scene, cfg, s, env={"NUMI_CLOTH_RESIDENT": "1" if ranks == 1 else "2"})
+    env = {"NUMI_CLOTH_RESIDENT": "1" if side * side <= 4096 else "2"}
+    if chunk:
+        env["NUMI_CLOTH_RESIDENT_CHUNK"] = chunk
+    res = run_gpu(scene, cfg, s, env=env)
     glob = run_gpu(scene, cfg, s, env={"NUMI_CLOTH_RESIDENT": "0"})
     assert res["info"]["resident"] and res["info"]["grid"] == ranks
     assert not glob["info"]["resident"]
