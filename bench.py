@@ -370,30 +370,48 @@ def calibration_leg(nc, torch, stream, candidates: int, steps: int, plain_sample
             "error_units": "log-compliance for compliances, absolute for damping",
             "best_loss": float(out["loss"][best]), "initial_best_loss": float(out["history"][0].min()),
             "nonsmooth_events_best": int(out["nonsmooth"][best]),
-            "note": "fruit contact and cloth/ground friction are not differentiated; their events are counted"}
+            "note": "fruit/yarn contact and its friction are not differentiated; their events are counted"}
 
 
-# The differentiable rollout: a 64 x 64 cloth at 4 mm, one corner on a
-# seeded 6-DoF grip trajectory (translation at most 5 cm, rotation at most
-# 15 degrees), ground and 4 spheres, 96 substeps (two 60 Hz frames), the loss
-# over 32 seeded tracked particles against a target trajectory made at
-# log-compliances shifted by N(0, 0.3) (by the forward here, by the FP64
-# oracle in the tests).  The cloth hangs
-# 12 cm above the ground and the spheres start 3-8 cm above it, as in the
-# benchmark cloth; soft enough compliances that the constraint violations
-# stay well above the FP32 position resolution.
+# The differentiable rollout: a 64 x 64 cloth at 4 mm, a 3 x 3 patch at one
+# corner held by compliant grips on a seeded 6-DoF trajectory (translation at
+# most 5 cm, rotation at most 15 degrees), ground and 4 spheres, 96 substeps
+# (two 60 Hz frames), the loss over 32 seeded tracked particles against a
+# target trajectory made at log-compliances shifted by N(0, 0.3) (by the
+# forward here, by the FP64 oracle in the tests).  The cloth hangs 12 cm
+# above the ground and the spheres start 3-8 cm above it.  The compliances
+# are soft enough that the loss residuals (about 1 mm) stay three orders
+# above the FP32 trajectory's own error against FP64 (about 1 um), which
+# bounds how closely FP32 gradients can match FP64 finite differences.
 CONFIG3_SUBSTEPS, CONFIG3_LOSS_EVERY, CONFIG3_TRACKED = 96, 12, 32
 CONFIG3_SCHED = dict(iterations=1, strainSweeps=1, reconcilePasses=0, finalPasses=0, certificatePasses=0,
                      earlyExit=0, aerodynamics=0, sweptGround=1, frictions=1, damping=0.5)
+CONFIG3_COMPLIANCE = (1.0e-3, 2.0e-3, 1.0e-2)   # stretch, shear, bend (m/N)
+CONFIG3_GRIP_PATCH = 3                          # gripped corner patch side (particles)
 
 
-def config3_scene(stretch=2e-5, shear=5e-5, bend=2e-4):
+def config3_scene(stretch=CONFIG3_COMPLIANCE[0], shear=CONFIG3_COMPLIANCE[1], bend=CONFIG3_COMPLIANCE[2]):
+    import numpy as np
+
     import numi_cloth as nc
 
-    return nc.square_scene(side=64, spacing=0.004, height=0.12, gripCorners=1, fruitCount=4,
-                           fruitRadiusMin=0.02, fruitRadiusMax=0.05, fruitHeightMin=0.15, fruitHeightMax=0.20,
-                           stretchCompliance=stretch, shearCompliance=shear, bendCompliance=bend,
-                           timestep=1.0 / 2880.0, seed=20260310)
+    side = 64
+    scene = nc.square_scene(side=side, spacing=0.004, height=0.12, gripCorners=1, fruitCount=4,
+                            fruitRadiusMin=0.02, fruitRadiusMax=0.05, fruitHeightMin=0.15, fruitHeightMax=0.20,
+                            stretchCompliance=stretch, shearCompliance=shear, bendCompliance=bend,
+                            timestep=1.0 / 2880.0, seed=20260310)
+    # one grip per particle of the corner patch, offsets from the corner
+    # (the grip target's origin), all with the corner grip's compliance
+    corner = scene.grips[0]
+    pos = scene.particles["positionAndInverseMass"][:, :3].astype(np.float64)
+    ids = [i * side + j for i in range(CONFIG3_GRIP_PATCH) for j in range(CONFIG3_GRIP_PATCH)]
+    grips = np.zeros(len(ids), scene.grips.dtype)
+    for g, i in enumerate(ids):
+        off = pos[i] - pos[0]
+        grips[g]["particle"] = (i, corner["particle"][1], 0, 0)
+        grips[g]["targetOffsetAndCompliance"] = (off[0], off[1], off[2], corner["targetOffsetAndCompliance"][3])
+    scene.grips = grips
+    return scene
 
 
 def config3_configs(scene, seed: int = 303):
@@ -440,7 +458,7 @@ def rollout_leg(nc, torch, stream, reps: int, candidates: int) -> dict:
     rng = np.random.default_rng(3)
     tracked = np.sort(rng.choice(scene.n, CONFIG3_TRACKED, replace=False)).astype(np.uint32)
     shift = np.exp(rng.normal(0.0, 0.3, size=3))
-    sv = nc.ClothSolver(config3_scene(2e-5 * shift[0], 5e-5 * shift[1], 2e-4 * shift[2]))
+    sv = nc.ClothSolver(config3_scene(*(c * f for c, f in zip(CONFIG3_COMPLIANCE, shift))))
     sv.set_stream(stream.cuda_stream)
     targets = []
     for k in range(CONFIG3_SUBSTEPS // CONFIG3_LOSS_EVERY):

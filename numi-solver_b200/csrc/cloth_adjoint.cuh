@@ -11,13 +11,16 @@
 // derivatives are evaluated in FP64 at the FP32 state, and adjoints and
 // parameter gradients are accumulated in FP64.
 //
-// Differentiated: predict with gravity and damping, XPBD distance / shear /
-// knot / bend projections (one iteration, so lambda starts at zero), compliant
-// grips, the ground clamp, unilateral strain limits, finalize.  The other
-// phases (fruit pairs, fruit/yarn contact and friction, cloth/ground
-// friction, swept ground, bend ground active sets) are non-smooth; where one
-// of them changes the cloth it is counted in `nonsmooth` and passed through
-// as the identity.
+// Differentiated: predict with gravity and damping, the swept ground clamp,
+// XPBD distance / shear / knot / bend projections (one iteration, so lambda
+// starts at zero), the bend's ground active set, step fraction and ground
+// clamp, compliant grips, the ground clamp, unilateral strain limits,
+// finalize with cloth/ground Coulomb friction (sticking and sliding).  Each
+// is piecewise smooth: the pieces the forward took are recomputed in FP32
+// and differentiated exactly.  Fruit/yarn contact and its friction move
+// the cloth through the fruits' rigid-body state, which the adjoint does not
+// carry; where they change the cloth the event is counted in `nonsmooth` and
+// passed through as the identity.
 #pragma once
 
 #include "cloth_kernels.cuh"
@@ -50,6 +53,7 @@ struct AdjointArgs {
     uint32_t substeps;               // substeps of the segment
     uint32_t first_substep;          // rollout index of the segment's first substep
     float damping;                   // the schedule's (or the cloth's) damping
+    uint32_t frictions;              // the schedule's frictions switch
     const uint32_t* tracked;         // [n_tracked]
     uint32_t n_tracked;
     const double* targets;           // [losses][n_tracked][3]
@@ -153,6 +157,106 @@ __device__ __forceinline__ void knot_dual(const DV p[4], const double w[4], Dual
     }
 }
 
+// Branches the forward bend projection took (nc::bend_core): active[s]
+// when the ground holds particle s's normal motion; frac_src the particle
+// whose ground distance limits the step (-1: none, fraction 1), frac_zero
+// when that distance is zero; clamp[s] when the new position is lifted back
+// to the ground.
+struct BendBranches {
+    bool active[2];
+    int frac_src;
+    bool frac_zero;
+    bool clamp[2];
+};
+
+// The forward's FP32 decisions for one bend with lambda from zero; false
+// when the forward leaves the pair unchanged.
+__device__ __forceinline__ bool bend_branches(const float4& p0, const float4& p2, const float2& m, float dt2,
+                                              float radius, bool ground, BendBranches& b) {
+    const float4 p[2] = {p0, p2};
+    const V3 diff = xyz(p2) - xyz(p0);
+    const float chord = len3(diff);
+    if (chord < 1.0e-12f) return false;
+    const float value = chord - m.x;
+    const V3 dir = vdiv(diff, chord);
+    const V3 g[2] = {dir * -1.0f, dir};
+    const float alpha = m.y / dt2;
+    float free_den = alpha;
+    free_den = free_den + p[0].w * lsq(g[0]);
+    free_den = free_den + p[1].w * lsq(g[1]);
+    if (free_den < 1.0e-16f) return false;
+    const float lam = 0.0f;
+    const float numerator = -value - alpha * lam;
+    const float free_dl = numerator / free_den;
+    float den = alpha;
+    for (int s = 0; s < 2; ++s) {
+        b.active[s] = ground && p[s].z <= radius + 1.0e-9f && g[s].z * free_dl < 0.0f;
+        den = den + p[s].w * (lsq(g[s]) - (b.active[s] ? g[s].z * g[s].z : 0.0f));
+    }
+    if (den < 1.0e-16f) return false;
+    const float dl = numerator / den;
+    float fraction = 1.0f;
+    b.frac_src = -1;
+    b.frac_zero = false;
+    if (ground) {
+        for (int s = 0; s < 2; ++s) {
+            if (b.active[s]) continue;
+            const float vc = g[s].z * p[s].w * dl;
+            if (vc >= 0.0f) continue;
+            const float cand = fmaxf(0.0f, p[s].z - radius) / -vc;
+            if (cand < fraction) {
+                fraction = cand;
+                b.frac_src = s;
+                b.frac_zero = !(p[s].z - radius > 0.0f);
+            }
+        }
+    }
+    const float applied = dl * fraction;
+    for (int s = 0; s < 2; ++s) {
+        V3 corr = g[s] * (p[s].w * applied);
+        if (b.active[s]) corr.z = 0.0f;
+        const V3 np = xyz(p[s]) + corr;
+        b.clamp[s] = ground && np.z < radius;
+    }
+    return true;
+}
+
+// The bend projection on dual numbers along the forward's branches:
+// positions p[2] (the pair's ends), inverse masses w[2], compliance alpha
+// (over dt^2); writes out[2].
+__device__ __forceinline__ void bend_dual(const DV p[2], const double w[2], Dual alpha, double rest, double radius,
+                                          const BendBranches& b, DV out[2]) {
+    const Dual zero{0.0, 0.0};
+    const Dual one{1.0, 0.0};
+    const DV diff = p[1] - p[0];
+    const Dual chord = dsqrt(ddot(diff, diff));
+    const Dual value = chord - Dual{rest, 0.0};
+    const DV dir = diff * (one / chord);
+    const DV g[2] = {DV{zero, zero, zero} - dir, dir};
+    const Dual numerator = zero - value;
+    Dual den = alpha;
+    for (int s = 0; s < 2; ++s)
+        den = den + Dual{w[s], 0.0} * (ddot(g[s], g[s]) - (b.active[s] ? g[s].z * g[s].z : zero));
+    const Dual dl = numerator / den;
+    Dual fraction = one;
+    if (b.frac_src >= 0) {
+        const int s = b.frac_src;
+        if (b.frac_zero) {
+            fraction = zero;
+        } else {
+            const Dual vc = g[s].z * Dual{w[s], 0.0} * dl;
+            fraction = (p[s].z - Dual{radius, 0.0}) / (zero - vc);
+        }
+    }
+    const Dual applied = dl * fraction;
+    for (int s = 0; s < 2; ++s) {
+        const Dual k = Dual{w[s], 0.0} * applied;
+        DV np{p[s].x + g[s].x * k, p[s].y + g[s].y * k, p[s].z + (b.active[s] ? zero : g[s].z * k)};
+        if (b.clamp[s]) np.z = Dual{radius, 0.0};
+        out[s] = np;
+    }
+}
+
 }  // namespace adj
 
 __device__ __forceinline__ void adjoint_segment(const AdjointArgs& A) {
@@ -201,8 +305,17 @@ __device__ __forceinline__ void adjoint_segment(const AdjointArgs& A) {
                     if (pre[i].x != post[i].x || pre[i].y != post[i].y || pre[i].z != post[i].z) ++rough;
                 break;
             case ADJ_FINAL: {
-                // v_end = (x - x_start) / dt; cloth/ground friction of a
-                // particle resting on the ground is not differentiated
+                // v_end = (x - x_start) / dt, then the cloth/ground Coulomb
+                // friction of a grounded particle (nc::finalize_particle):
+                // with normal impulse gi = (v_end.z - v_pred.z) / w, sticking
+                // (|v_t| / w <= mu gi) zeroes the tangential velocity and
+                // sliding removes mu (v_end.z - v_pred.z) along the slip.
+                // The adjoint of the predicted normal velocity goes to
+                // gprev.w for the predict step.
+                const float4* xs = T;
+                const float4* vs = A.tape_v + static_cast<size_t>(si) * n;
+                const float inv_dt = 1.0f / dt;
+                const float mu = cf.clothMaterial.z;
                 for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
                     if (pre[i].w == 0.0f) {
                         A.gx[i] = make_double4(0, 0, 0, 0);
@@ -210,10 +323,41 @@ __device__ __forceinline__ void adjoint_segment(const AdjointArgs& A) {
                         A.gprev[i] = make_double4(0, 0, 0, 0);
                         continue;
                     }
-                    if (ground && pre[i].z <= radius + 1.0e-6f) ++rough;
-                    const D3v gvv = d3(A.gv[i]);
+                    D3v gvv = d3(A.gv[i]);
+                    double gvpz = 0.0;
+                    if (ground && A.frictions != 0u && pre[i].z <= radius + 1.0e-6f) {
+                        // the forward's decisions, in FP32
+                        const float w = pre[i].w;
+                        const V3 vel = (xyz(pre[i]) - xyz(xs[i])) * inv_dt;
+                        float vpz = vs[i].z + cf.gravityAndTimestep.z * dt;
+                        if (A.damping != 0.0f) vpz = vpz * (1.0f / (1.0f + A.damping * dt));
+                        const float gi = fmaxf(0.0f, (vel.z - vpz) / w);
+                        const V3 tv{vel.x, vel.y, 0.0f};
+                        const float slip = len3(tv);
+                        if (gi > 0.0f && !(slip < 1.0e-10f) && fminf(slip / w, mu * gi) > 0.0f) {
+                            if (slip / w <= mu * gi) {
+                                gvv.x = 0.0;   // sticking
+                                gvv.y = 0.0;
+                            } else {
+                                // sliding: v_t' = v_t - phi v_t / |v_t|, phi = mu (v.z - v_pred.z)
+                                const D3v vd = muld(subd(d4f(pre[i]), d4f(xs[i])), 1.0 / dtd);
+                                double vpd = static_cast<double>(vs[i].z) + static_cast<double>(cf.gravityAndTimestep.z) * dtd;
+                                if (A.damping != 0.0f) vpd /= 1.0 + static_cast<double>(A.damping) * dtd;
+                                const double sl = sqrt(vd.x * vd.x + vd.y * vd.y);
+                                const double nx = vd.x / sl, ny = vd.y / sl;
+                                const double phi = static_cast<double>(mu) * (vd.z - vpd);
+                                const double gn = gvv.x * nx + gvv.y * ny;
+                                const double gtx = gvv.x - phi / sl * (gvv.x - nx * gn);
+                                const double gty = gvv.y - phi / sl * (gvv.y - ny * gn);
+                                const double gphi = -gn;
+                                gvv = D3v{gtx, gty, gvv.z + static_cast<double>(mu) * gphi};
+                                gvpz = -static_cast<double>(mu) * gphi;
+                            }
+                        }
+                    }
                     put(A.gx, i, addd(d3(A.gx[i]), muld(gvv, 1.0 / dtd)));
-                    put(A.gprev, i, muld(gvv, -1.0 / dtd));
+                    const D3v gp = muld(gvv, -1.0 / dtd);
+                    A.gprev[i] = make_double4(gp.x, gp.y, gp.z, gvpz);
                     A.gv[i] = make_double4(0, 0, 0, 0);
                 }
                 break;
@@ -310,34 +454,45 @@ __device__ __forceinline__ void adjoint_segment(const AdjointArgs& A) {
                     const uint4 q = d.b_ij[k];
                     const float2 m = d.b_mat[k];
                     const float4 p0 = pre[q.x], p2 = pre[q.z];
-                    const V3 diff = xyz(p2) - xyz(p0);
-                    const float chord = len3(diff);
-                    if (chord < 1.0e-12f) continue;
-                    const float value = chord - m.x;
-                    const V3 dir = vdiv(diff, chord);
-                    const float alpha = m.y / dt2;
-                    float free_den = alpha;
-                    free_den = free_den + p0.w * lsq(dir * -1.0f);
-                    free_den = free_den + p2.w * lsq(dir);
-                    if (free_den < 1.0e-16f) continue;
-                    const float free_dl = -value / free_den;
-                    const bool act0 = ground && p0.z <= radius + 1.0e-9f && -dir.z * free_dl < 0.0f;
-                    const bool act2 = ground && p2.z <= radius + 1.0e-9f && dir.z * free_dl < 0.0f;
-                    if (act0 || act2) {
-                        ++rough;   // ground active set: not differentiated
+                    BendBranches br;
+                    if (!bend_branches(p0, p2, m, dt2, radius, ground, br)) continue;
+                    const double alphad = static_cast<double>(m.y) / (dtd * dtd);
+                    if (!br.active[0] && !br.active[1] && br.frac_src < 0 && !br.clamp[0] && !br.clamp[1]) {
+                        // clear of the ground: the distance form
+                        const double galpha =
+                            distance_vjp(A.gx, q.x, q.z, p0, p2, static_cast<double>(m.x), alphad);
+                        acc[A.b_group[k]] += galpha * alphad;
                         continue;
                     }
-                    if (ground) {
-                        const float vc0 = -dir.z * p0.w * free_dl, vc2 = dir.z * p2.w * free_dl;
-                        if ((vc0 < 0.0f && fmaxf(0.0f, p0.z - radius) < -vc0) ||
-                            (vc2 < 0.0f && fmaxf(0.0f, p2.z - radius) < -vc2))
-                            ++rough;   // fraction clamp: not differentiated
-                        if (p0.z + (-dir.z) * (p0.w * free_dl) < radius || p2.z + dir.z * (p2.w * free_dl) < radius)
-                            ++rough;   // clamped to the ground after the bend: not differentiated
+                    // on the ground: VJP by forward mode along the forward's
+                    // branches, one tangent per input (6 coordinates, alpha)
+                    const uint32_t idx[2] = {q.x, q.z};
+                    const float4 pp[2] = {p0, p2};
+                    double u[6];
+                    for (int e = 0; e < 2; ++e) {
+                        const double4 ge = A.gx[idx[e]];
+                        u[3 * e] = ge.x;
+                        u[3 * e + 1] = ge.y;
+                        u[3 * e + 2] = ge.z;
                     }
-                    const double alphad = static_cast<double>(m.y) / (dtd * dtd);
-                    const double galpha = distance_vjp(A.gx, q.x, q.z, p0, p2, static_cast<double>(m.x), alphad);
-                    acc[A.b_group[k]] += galpha * alphad;
+                    const double w[2] = {p0.w, p2.w};
+                    double gin[7];
+                    for (int dir = 0; dir < 7; ++dir) {
+                        DV pd[2];
+                        for (int e = 0; e < 2; ++e)
+                            pd[e] = DV{Dual{pp[e].x, dir == 3 * e ? 1.0 : 0.0}, Dual{pp[e].y, dir == 3 * e + 1 ? 1.0 : 0.0},
+                                       Dual{pp[e].z, dir == 3 * e + 2 ? 1.0 : 0.0}};
+                        DV out[2];
+                        bend_dual(pd, w, Dual{alphad, dir == 6 ? 1.0 : 0.0}, static_cast<double>(m.x),
+                                  static_cast<double>(radius), br, out);
+                        double acc_dir = 0.0;
+                        for (int e = 0; e < 2; ++e)
+                            acc_dir += u[3 * e] * out[e].x.d + u[3 * e + 1] * out[e].y.d + u[3 * e + 2] * out[e].z.d;
+                        gin[dir] = acc_dir;
+                    }
+                    for (int e = 0; e < 2; ++e)
+                        A.gx[idx[e]] = make_double4(gin[3 * e], gin[3 * e + 1], gin[3 * e + 2], 0.0);
+                    acc[A.b_group[k]] += gin[6] * alphad;
                 }
                 break;
             }
@@ -408,11 +563,11 @@ __device__ __forceinline__ void adjoint_segment(const AdjointArgs& A) {
                         continue;
                     }
                     D3v gpos = d3(A.gx[i]);
-                    if (ground && pre[i].z >= radius && post[i].z == radius) {
-                        ++rough;   // swept ground clamp: not differentiated
-                        gpos.z = 0.0;
-                    }
-                    const D3v gvp = muld(gpos, dtd);
+                    // swept ground clamp: the predicted z is set to the radius
+                    if (ground && pre[i].z >= radius && post[i].z == radius) gpos.z = 0.0;
+                    // v' feeds x' and, through friction, the finalize step
+                    D3v gvp = muld(gpos, dtd);
+                    gvp.z += A.gprev[i].w;
                     const D3v v0 = addd(D3v{vs[i].x, vs[i].y, vs[i].z}, muld(grav, dtd));
                     acc[damp_slot] += dotd(gvp, v0) * dk;
                     put(A.gv, i, muld(gvp, kf));

@@ -2499,6 +2499,7 @@ extern "C" int numi_cloth_rollout_grad(numi_cloth_t* h, const NumiClothConfig* c
         A.substeps = count;
         A.first_substep = first;
         A.damping = damping;
+        A.frictions = s.frictions;
         A.tracked = d_tracked;
         A.n_tracked = n_tracked;
         A.targets = d_targets;
@@ -2663,6 +2664,7 @@ extern "C" int numi_cloth_batch_rollout_grad(numi_cloth_batch_t* b, const NumiCl
         A.phases = ph;
         A.slots = slots;
         A.damping = h->d.damping >= 0.0f ? h->d.damping : s.damping;
+        A.frictions = s.frictions;
         A.tracked = d_tracked;
         A.n_tracked = n_tracked;
         A.targets = d_targets + static_cast<size_t>(k) * losses * n_tracked * 3u;

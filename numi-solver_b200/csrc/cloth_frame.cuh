@@ -885,33 +885,56 @@ __device__ __forceinline__ uint32_t self_pass_tag(const Ctx& ctx, uint32_t it) {
 // host clears the heads when the substep counter wraps), so a max with
 // (tag, 0) resets a bucket of an older pass and leaves a current one alone;
 // the add after it, in the same thread's order on the same address, takes
-// the next slot.
+// the next slots.  The slots are claimed warp by warp: the lanes that hash
+// to one bucket (neighbouring particles mostly share cells) form a group
+// (match), its first lane claims as many slots as the group has lanes with
+// one atomic, and each lane takes the claimed base plus its rank in the
+// group (a segmented prefix count over the warp); lanes whose slots fall
+// past the bucket's capacity claim overflow entries the same way (ballot
+// and prefix count).  The slot order does not change any result: a query
+// sums its corrections in fixed point.
 __device__ __forceinline__ void self_insert_one(const Ctx& ctx, unsigned long long tag, uint32_t i, const float4& p) {
     const DeviceCloth& d = ctx.d;
     const float inv_cell = 1.0f / (4.0f * ctx.c.radius);
-    {
-        const uint32_t bucket = cell_bucket(static_cast<int>(floorf(p.x * inv_cell)),
-                                            static_cast<int>(floorf(p.y * inv_cell)),
-                                            static_cast<int>(floorf(p.z * inv_cell)), d.hash_mask);
+    const uint32_t bucket = cell_bucket(static_cast<int>(floorf(p.x * inv_cell)),
+                                        static_cast<int>(floorf(p.y * inv_cell)),
+                                        static_cast<int>(floorf(p.z * inv_cell)), d.hash_mask);
+    const unsigned active = __activemask();
+    const uint32_t lane = threadIdx.x & 31u;
+    const unsigned below = (1u << lane) - 1u;
+    const unsigned peers = __match_any_sync(active, bucket);
+    const int leader = __ffs(static_cast<int>(peers)) - 1;
+    unsigned long long base = 0ull;
+    if (static_cast<int>(lane) == leader) {
         unsigned long long* head = d.hash_head + bucket;
         atomicMax(head, tag << 32);
-        const uint32_t slot = static_cast<uint32_t>(atomicAdd(head, 1ull));
-        HashSlot* e;
-        if (slot < NC_HASH_CAP) {
-            e = d.hash + bucket * NC_HASH_CAP + slot;
-        } else {
-            // a full bucket (a crumpled cloth packs many particles into a
-            // cell): the particle goes to the overflow list every query scans
-            atomicMax(d.hash_over_head, tag << 32);
-            const uint32_t o = static_cast<uint32_t>(atomicAdd(d.hash_over_head, 1ull));
-            if (o >= d.n) {
-                fail(d, NUMI_CLOTH_FAILURE_RANGE);
-                return;
-            }
-            e = d.hash_over + o;
-        }
-        e->pos = make_float4(p.x, p.y, p.z, __uint_as_float(i));
+        base = atomicAdd(head, static_cast<unsigned long long>(__popc(peers)));
     }
+    base = __shfl_sync(peers, base, leader);
+    const uint32_t slot = static_cast<uint32_t>(base) + static_cast<uint32_t>(__popc(peers & below));
+    const bool over = slot >= NC_HASH_CAP;
+    const unsigned overs = __ballot_sync(active, over);
+    HashSlot* e;
+    if (!over) {
+        e = d.hash + bucket * NC_HASH_CAP + slot;
+    } else {
+        // a full bucket (a crumpled cloth packs many particles into a
+        // cell): the particle goes to the overflow list every query scans
+        const int first = __ffs(static_cast<int>(overs)) - 1;
+        unsigned long long obase = 0ull;
+        if (static_cast<int>(lane) == first) {
+            atomicMax(d.hash_over_head, tag << 32);
+            obase = atomicAdd(d.hash_over_head, static_cast<unsigned long long>(__popc(overs)));
+        }
+        obase = __shfl_sync(overs, obase, first);
+        const uint32_t o = static_cast<uint32_t>(obase) + static_cast<uint32_t>(__popc(overs & below));
+        if (o >= d.n) {
+            fail(d, NUMI_CLOTH_FAILURE_RANGE);
+            return;
+        }
+        e = d.hash_over + o;
+    }
+    e->pos = make_float4(p.x, p.y, p.z, __uint_as_float(i));
 }
 
 __device__ void self_insert(Ctx& ctx, uint32_t it) {
@@ -2061,6 +2084,7 @@ __device__ bool validate_records(const DeviceCloth& d, const SubCfg& c0) {
 }  // namespace
 }  // namespace nc
 
+#include "cloth_bulk.cuh"
 #include "cloth_tile.cuh"
 
 // One cloth's frame on `ranks` CTAs (this one is `rank`): all substeps of
@@ -2098,19 +2122,21 @@ __device__ __forceinline__ void run_frame(const DeviceCloth& src, const Schedule
     ctx.shift = d.resident_shift;
     uint32_t own_first = 0, own_end = 0;
     if (ctx.resident) {
-        // Stage this CTA's particles into shared memory for the whole launch.
+        // Stage this CTA's particles into shared memory for the whole launch
+        // (bulk copies of its slices of x and v).
         ctx.xs = reinterpret_cast<float4*>(dynamic_smem + nc_resident_offset());
         ctx.vs = ctx.xs + (1u << ctx.shift);
-        own_first = ctx.rank << ctx.shift;
+        own_first = min(ctx.rank << ctx.shift, d.n);
         own_end = min(own_first + (1u << ctx.shift), d.n);
-        for (uint32_t i = own_first + threadIdx.x; i < own_end; i += blockDim.x) {
-            ctx.xs[i - own_first] = __ldcg(d.x + i);
-            ctx.vs[i - own_first] = __ldcg(d.v + i);
-        }
+        const uint32_t bytes = (own_end - own_first) * static_cast<uint32_t>(sizeof(float4));
+        const nc::BulkJob jobs[2] = {{ctx.xs, d.x + own_first, bytes}, {ctx.vs, d.v + own_first, bytes}};
+        const bool staged = nc::bulk_load(d, jobs, 2u);
+        // a cluster's CTAs all pass its barrier; a copy that timed out has
+        // raised TIMEOUT and the abort flag for the host
         if (ranks > 1u)
             cooperative_groups::this_cluster().sync();
-        else
-            __syncthreads();
+        else if (!staged)
+            return;
     }
     if (s.tiles) {
         // tile mode: the CTA's plan and its local particles after the
@@ -2176,11 +2202,10 @@ __device__ __forceinline__ void run_frame(const DeviceCloth& src, const Schedule
     }
     if (ctx.resident) {
         // Every remote access ended at the last barrier: write the CTA's own
-        // particles back.
-        for (uint32_t i = own_first + threadIdx.x; i < own_end; i += blockDim.x) {
-            d.x[i] = ctx.xs[i - own_first];
-            d.v[i] = ctx.vs[i - own_first];
-        }
+        // particles back (bulk copies).
+        const uint32_t bytes = (own_end - own_first) * static_cast<uint32_t>(sizeof(float4));
+        const nc::BulkJob jobs[2] = {{ctx.xs, d.x + own_first, bytes}, {ctx.vs, d.v + own_first, bytes}};
+        nc::bulk_store(jobs, 2u);
     }
 }
 

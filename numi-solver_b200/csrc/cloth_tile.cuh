@@ -60,52 +60,13 @@ namespace {
 #define NC_TILE_BEND 1u
 #define NC_TILE_LIMIT 2u
 #define NC_TILE_SEGMENT 3u
-#define NC_TILE_COPY_CHUNK 32768u   /* bytes per bulk copy of the plan */
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-// Stage this CTA's plan into shared memory: bulk copies (cp.async.bulk,
-// global to shared, completion counted on an mbarrier), no multicast, from
-// this GPU's own memory.  The wait is bounded: past the limit the CTA raises
-// TIMEOUT and the abort flag and returns false after a second bounded wait
-// for its copies.
+// Stage this CTA's plan into shared memory: one bulk load (nc::bulk_load,
+// bounded wait).
 __device__ bool tile_stage(const Ctx& ctx, uint32_t* plan) {
     const DeviceCloth& d = ctx.d;
-    __shared__ __align__(8) unsigned long long s_bar;
     const uint32_t w0 = d.tile_off[ctx.rank], w1 = d.tile_off[ctx.rank + 1u];
-    const uint32_t bytes = (w1 - w0) * 4u;
-    const uint32_t bar = smem_addr(&s_bar);
-    if (threadIdx.x == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-        const char* src = reinterpret_cast<const char*>(d.tile_words + w0);
-        for (uint32_t at = 0; at < bytes; at += NC_TILE_COPY_CHUNK) {
-            const uint32_t len = min(NC_TILE_COPY_CHUNK, bytes - at);
-            asm volatile(
-                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                    smem_addr(reinterpret_cast<char*>(plan) + at)),
-                "l"(src + at), "r"(len), "r"(bar)
-                : "memory");
-        }
-    }
-    __syncthreads();
-    // every thread waits for the copies (phase 0 of the barrier)
-    const unsigned limit = d.spin_limit != 0u ? d.spin_limit : NC_BARRIER_SPIN_LIMIT;
-    uint32_t done = 0u;
-    for (unsigned spin = 0; spin <= 2u * limit && !done; ++spin) {
-        asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
-                     : "=r"(done)
-                     : "r"(bar)
-                     : "memory");
-        if (!done && spin == limit && threadIdx.x == 0) {
-            atomicOr(d.failure, NUMI_CLOTH_FAILURE_TIMEOUT);
-            atomicExch(d.abort_flag, 1u);
-        }
-    }
-    return __syncthreads_and(done != 0u) != 0;
+    const BulkJob job{plan, d.tile_words + w0, (w1 - w0) * 4u};
+    return bulk_load(d, &job, 1u);
 }
 
 __device__ __forceinline__ const uint32_t* tile_list(const Ctx& ctx) { return ctx.tp + ctx.tp[2]; }

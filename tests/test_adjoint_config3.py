@@ -1,9 +1,15 @@
 """The differentiable rollout at its stated size: a 64 x 64 cloth (4,096
-particles, 4 mm) with one corner on a seeded 6-DoF grip trajectory
+particles, 4 mm) with a 3 x 3 corner patch on a seeded 6-DoF grip trajectory
 (translation at most 5 cm, rotation at most 15 degrees), ground and 4
 spheres, 96 substeps at 1/2880 s, checkpoints every 8 substeps, the loss over
 32 seeded tracked particles against a target trajectory made at
 log-compliances shifted by N(0, 0.3) (tests/helpers.py config3_*).
+
+The adjoint differentiates the FP32 trajectory the GPU ran.  That trajectory
+is within about 1.3e-6 m of the FP64 one, and the loss residuals are about
+1e-3 m; the gradient error that this alone causes, estimated on the CPU from
+the FP32 and FP64 oracles and FP64 Jacobians, is about 1e-4 (material and
+damping) and 3e-4 (grip pose) norm-wise, inside the 1e-3 bar.
 
 The adjoint's gradients with respect to the compliance groups (stretch,
 shear, bend, grip), the damping and the grip pose are compared with
