@@ -437,6 +437,10 @@ int numi_cloth_batch_step(numi_cloth_batch_t* batch, const NumiClothConfig* conf
  * many particles keep them in shared memory; 0 = none), out[1] threads per
  * CTA, out[2] CTAs of the persistent launch. */
 int numi_cloth_batch_shape(numi_cloth_batch_t* batch, uint32_t out[3]);
+/* A shape whose resident chunk leaves no shared memory for the edge/edge
+ * family's box-tree sort keys (32 KB) serves only schedules with
+ * primitiveSelf = 0: a step or capture with primitiveSelf on returns EINVAL
+ * on it, and the tuner skips it for such schedules. */
 int numi_cloth_batch_set_shape(numi_cloth_batch_t* batch, uint32_t resident_chunk, uint32_t threads);
 
 /* Autotuner: times one step of every candidate shape (resident chunk 0,

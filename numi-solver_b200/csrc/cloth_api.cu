@@ -863,7 +863,7 @@ int prepare_edge_grid(numi_cloth* h, bool primitive, uint32_t substeps, float ra
         e.edge_lv = h->buf.alloc<uint32_t>(cap);
         e.edge_level = h->buf.alloc<uint32_t>(d.n);
         e.edge_qbox_raw = h->buf.alloc<float>(6u * d.y_count);
-        e.edge_tree = h->buf.alloc<uint32_t>(2u * d.y_count);
+        e.edge_tree = h->buf.alloc<uint32_t>(static_cast<size_t>(NC_EDGE_TREE_WORDS) * d.y_count);
         e.edge_centre = h->buf.alloc<float4>(d.y_count);
         e.edge_rec = h->buf.alloc<EdgeRecord>(cap);
         e.edge_ctl = h->buf.alloc<uint32_t>(8);
@@ -1832,6 +1832,7 @@ struct numi_cloth_batch {
     uint32_t epoch_host = 1;
     uint32_t block = NC_THREADS;
     uint32_t chunk = 0;                // resident particle chunk (0: none)
+    bool edge_room = true;             // the shape leaves room for the box tree's sort keys
     uint32_t ctas = 0;
     size_t smem = 0;
     cudaGraph_t graph = nullptr;
@@ -1856,14 +1857,22 @@ int batch_shape(numi_cloth_batch* b, uint32_t chunk, uint32_t block) {
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
     int per_sm = 1 << 30;
+    bool edge_room = false;
     for (bool edge : {false, true}) {
-        // the edge/edge kernel also holds the box tree's sort keys
+        // the edge/edge kernel also holds the box tree's sort keys; a shape
+        // without room for them serves only schedules without that family
         const size_t bytes = edge ? nc_round256(smem) + NC_EDGE_TREE_KEY_BYTES : smem;
         cudaFuncAttributes fa{};
         if (cudaFuncGetAttributes(&fa, batch_fn(edge)) != cudaSuccess) return NUMI_CLOTH_ECUDA;
-        if (bytes + fa.sharedSizeBytes > static_cast<size_t>(optin)) return NUMI_CLOTH_EINVAL;
+        if (bytes + fa.sharedSizeBytes > static_cast<size_t>(optin)) {
+            if (edge) continue;
+            return NUMI_CLOTH_EINVAL;
+        }
         if (raise_smem(batch_fn(edge), bytes) != cudaSuccess) return NUMI_CLOTH_ECUDA;
-        if (edge) continue;   // launched without co-residence
+        if (edge) {
+            edge_room = true;
+            continue;   // launched without co-residence
+        }
         int k = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, batch_fn(edge), static_cast<int>(block), bytes) !=
             cudaSuccess)
@@ -1871,6 +1880,7 @@ int batch_shape(numi_cloth_batch* b, uint32_t chunk, uint32_t block) {
         per_sm = std::min(per_sm, k);
     }
     if (per_sm < 1) return NUMI_CLOTH_EINVAL;
+    b->edge_room = edge_room;
     b->chunk = chunk;
     b->block = block;
     b->smem = smem;
@@ -1906,6 +1916,7 @@ int batch_layout(numi_cloth_batch* b, uint32_t substeps) {
 
 // Validate and stage one launch: Configs, self-contact grids, descriptors.
 int batch_prepare(numi_cloth_batch* b, const NumiClothConfig* configs, uint32_t substeps, const NumiClothSchedule& sched) {
+    if (sched.primitiveSelf != 0u && !b->edge_room) return NUMI_CLOTH_EINVAL;   // set a smaller shape first
     const uint32_t count = static_cast<uint32_t>(b->cloths.size());
     for (uint32_t k = 0; k < count; ++k) {
         numi_cloth* h = b->cloths[k];
@@ -2108,6 +2119,7 @@ int numi_cloth_batch_tune(numi_cloth_batch_t* b, const NumiClothConfig* configs,
         if (chunk > 0u && chunk / 2u >= largest) continue;   // same as a smaller chunk
         for (uint32_t block : blocks) {
             if (batch_shape(b, chunk, block) != NUMI_CLOTH_OK) continue;
+            if (schedule->primitiveSelf != 0u && !b->edge_room) continue;
             rc = batch_prepare(b, configs, substeps, *schedule);
             if (rc != NUMI_CLOTH_OK) break;
             cudaEventRecord(t0, b->stream);

@@ -207,8 +207,8 @@ struct DeviceCloth {
     float4* edge_x0;              // [n]
     float4* edge_sph;             // [y_count] pass spheres (centre, radius)
     float* edge_qbox_raw;         // [6 * y_count] a first segment's tree-query box of the pass
-    uint32_t* edge_tree;          // [2 * y_count] the pass's box-tree leaf order: position -> segment,
-                                  //   then segment -> position (edge_tree_order)
+    uint32_t* edge_tree;          // [10 * y_count] the pass's box-tree leaf order: position -> segment,
+                                  //   then segment -> position, then the build's scratch (edge_tree_order)
     float4* edge_centre;          // [y_count] centres of the pass-start boxes of the tree
     float* edge_path;             // [n]
     uint4* edge_cand;             // [edge_cap]

@@ -731,15 +731,21 @@ __device__ void edge_candidates(Ctx& ctx, bool swept, bool rebuilt) {
 // the candidates come in ascending tree position).  A node of more than 8
 // primitives orders them by box centre along the longest axis of its
 // centres (ties by index) and splits them at the middle; the node ranges
-// follow from the count alone, so the tree is built level by level: the
-// centre bounds of every splitting node (a warp each), then one bitonic sort
-// of (node, centre, index) keys in shared memory orders every node of the
-// level at once.  CTA 0, all threads; at most NC_EDGE_TREE_MAX segments.
-// Leaves edge_tree[p] = segment at position p, edge_tree[m + s] = position
-// of segment s.
+// follow from the count alone, so the tree is built level by level.  The
+// segments are sorted once along each axis (x, y, z lists); every level
+// then keeps each node's members in one range of all three lists, each in
+// its own axis order: a splitting node sends the first half of its axis
+// list to the left child, and a stable partition (one CTA-wide prefix count
+// per list) moves every list's members to their child, in order.  A leaf's
+// order is its parent's axis list.  CTA 0, all threads; at most
+// NC_EDGE_TREE_MAX segments.  edge_tree: [m] segment at each leaf position,
+// [m] position of each segment, then the build's scratch (two sets of the
+// three lists, the side of each segment, the parent axis of each position).
 #define NC_EDGE_TREE_MAX 4096u
 #define NC_EDGE_TREE_KEY_BYTES (NC_EDGE_TREE_MAX * 8u)
+#define NC_EDGE_TREE_WORDS 10u   /* edge_tree words per segment */
 __shared__ unsigned char nc_edge_tree_axis[NC_EDGE_TREE_MAX / 8u];
+__shared__ uint32_t nc_edge_scan[32];
 
 // The node of position p (or of index j, a path of `level` left/right bits)
 // at depth `level`; false past a leaf.
@@ -780,26 +786,154 @@ __device__ __forceinline__ uint32_t ordered_bits(float v) {
     return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
 }
 
+// Ascending bitonic sort of E * blockDim.x keys in shared memory.  Each
+// thread holds E consecutive keys in registers: compare distances below E
+// stay in the thread, distances below 32 E go between the lanes of a warp
+// (shuffles), and only the longer ones pass through shared memory between
+// CTA barriers.
+template <int E>
+__device__ void block_sort_keys(unsigned long long* keys) {
+    const uint32_t t = threadIdx.x;
+    const uint32_t n = static_cast<uint32_t>(E) * blockDim.x;
+    unsigned long long v[E];
+#pragma unroll
+    for (int r = 0; r < E; ++r) v[r] = keys[t * E + r];
+    for (uint32_t k = 2u; k <= n; k <<= 1) {
+        for (uint32_t jj = k >> 1; jj >= static_cast<uint32_t>(E); jj >>= 1) {
+            if (jj < 32u * E) {
+                const uint32_t lm = jj / E;
+#pragma unroll
+                for (int r = 0; r < E; ++r) {
+                    const uint32_t i = t * E + r;
+                    const unsigned long long o = __shfl_xor_sync(0xffffffffu, v[r], lm);
+                    const bool keep_min = ((i & jj) == 0u) == ((i & k) == 0u);
+                    v[r] = keep_min ? (o < v[r] ? o : v[r]) : (o > v[r] ? o : v[r]);
+                }
+            } else {
+                __syncthreads();
+#pragma unroll
+                for (int r = 0; r < E; ++r) keys[t * E + r] = v[r];
+                __syncthreads();
+#pragma unroll
+                for (int r = 0; r < E; ++r) {
+                    const uint32_t i = t * E + r;
+                    const unsigned long long o = keys[i ^ jj];
+                    const bool keep_min = ((i & jj) == 0u) == ((i & k) == 0u);
+                    v[r] = keep_min ? (o < v[r] ? o : v[r]) : (o > v[r] ? o : v[r]);
+                }
+            }
+        }
+#pragma unroll
+        for (int q = E / 2; q >= 1; q >>= 1) {
+            if (static_cast<uint32_t>(q) < k) {
+#pragma unroll
+                for (int r = 0; r < E; ++r) {
+                    const int pr = r ^ q;
+                    if (pr > r) {
+                        const bool asc = ((t * E + r) & k) == 0u;
+                        const unsigned long long a = v[r], b = v[pr];
+                        const bool swap = asc ? (a > b) : (a < b);
+                        v[r] = swap ? b : a;
+                        v[pr] = swap ? a : b;
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < E; ++r) keys[t * E + r] = v[r];
+    __syncthreads();
+}
+
+// Sort the first n keys (n a power of two, blockDim.x <= n <= 16 blockDim.x).
+__device__ void block_sort(unsigned long long* keys, uint32_t n) {
+    switch (n / blockDim.x) {
+    case 1u: block_sort_keys<1>(keys); break;
+    case 2u: block_sort_keys<2>(keys); break;
+    case 4u: block_sort_keys<4>(keys); break;
+    case 8u: block_sort_keys<8>(keys); break;
+    default: block_sort_keys<16>(keys); break;
+    }
+}
+
+// Exclusive prefix sums of flags[0..m) (0 or 1) into out[0..m) (shared
+// memory), every thread a contiguous run.
+__device__ void block_prefix(const uint32_t* flags, uint32_t* out, uint32_t m) {
+    const uint32_t per = (m + blockDim.x - 1u) / blockDim.x;
+    const uint32_t lo = min(threadIdx.x * per, m), hi = min(lo + per, m);
+    uint32_t sum = 0u;
+    for (uint32_t p = lo; p < hi; ++p) sum += flags[p];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t incl = sum;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= static_cast<uint32_t>(o)) incl += y;
+    }
+    if (lane == 31u) nc_edge_scan[warp] = incl;
+    __syncthreads();
+    if (warp == 0u) {
+        const uint32_t warps = blockDim.x >> 5;
+        uint32_t w = lane < warps ? nc_edge_scan[lane] : 0u;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= static_cast<uint32_t>(o)) w += y;
+        }
+        if (lane < warps) nc_edge_scan[lane] = w;
+    }
+    __syncthreads();
+    uint32_t run = (warp > 0u ? nc_edge_scan[warp - 1u] : 0u) + incl - sum;
+    for (uint32_t p = lo; p < hi; ++p) {
+        out[p] = run;
+        run += flags[p];
+    }
+    __syncthreads();
+}
+
 __device__ void edge_tree_order(const Ctx& ctx, bool swept) {
     const DeviceCloth& d = ctx.d;
-    // the sort keys, in the launch's dynamic shared memory
-    unsigned long long* nc_edge_tree_keys = reinterpret_cast<unsigned long long*>(nc_frame_smem + ctx.s.tree_keys);
+    // the sort keys and prefix sums, in the launch's dynamic shared memory
+    unsigned long long* keys = reinterpret_cast<unsigned long long*>(nc_frame_smem + ctx.s.tree_keys);
+    uint32_t* prefix = reinterpret_cast<uint32_t*>(keys);
     const uint32_t m = d.y_count;
     const float ex = 0.5f * (2.0f * ctx.c.radius);
     uint32_t* ord = d.edge_tree;
+    uint32_t* lists = d.edge_tree + 2u * m;   // [2][3][m]
+    uint32_t* right = lists + 6u * m;         // per segment: goes to the right child
+    uint32_t* leaf_axis = right + m;          // per position: axis of its deepest split
     for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
         const uint2 ab = __ldg(d.y_ij + k);
         const EdgeBox bx = edge_box(xyz(ld(d.edge_x0 + ab.x)), xyz(ld(d.edge_x0 + ab.y)), xyz(ld(d.xp + ab.x)),
                                     xyz(ld(d.xp + ab.y)), swept, ex);
         d.edge_centre[k] = make_float4(0.5f * (bx.lo.x + bx.hi.x), 0.5f * (bx.lo.y + bx.hi.y),
                                        0.5f * (bx.lo.z + bx.hi.z), 0.0f);
-        ord[k] = k;
+        leaf_axis[k] = 3u;
     }
-    uint32_t size = 4096u;
-    while (size / 2u >= m && size > 2u) size /= 2u;
-    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u, warps = blockDim.x >> 5;
+    uint32_t size = blockDim.x;
+    while (size < m) size <<= 1;
     __syncthreads();
+    // the three axis lists: (centre, index) order
+    for (uint32_t a = 0; a < 3u; ++a) {
+        for (uint32_t p = threadIdx.x; p < size; p += blockDim.x) {
+            unsigned long long key = ~0ull;
+            if (p < m) {
+                const float4 c = __ldcg(d.edge_centre + p);
+                const float v = a == 0u ? c.x : (a == 1u ? c.y : c.z);
+                key = (static_cast<unsigned long long>(ordered_bits(v)) << 12) | p;
+            }
+            keys[p] = key;
+        }
+        __syncthreads();
+        block_sort(keys, size);
+        for (uint32_t p = threadIdx.x; p < m; p += blockDim.x)
+            lists[a * m + p] = static_cast<uint32_t>(keys[p] & 0xfffull);
+        __syncthreads();
+    }
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u, warps = blockDim.x >> 5;
+    uint32_t cur = 0u;
     for (uint32_t level = 0; level < 32u; ++level) {
+        const uint32_t* L = lists + cur * 3u * m;
+        uint32_t* N = lists + (cur ^ 1u) * 3u * m;
         // centre bounds and axis of every node of the level that splits
         const uint32_t nodes = 1u << level;
         bool any = false;
@@ -808,7 +942,7 @@ __device__ void edge_tree_order(const Ctx& ctx, bool swept) {
             if (!tree_node_of_path(m, level, j, b, e) || e - b <= 8u) continue;
             V3 lo{INFINITY, INFINITY, INFINITY}, hi{-INFINITY, -INFINITY, -INFINITY};
             for (uint32_t p = b + lane; p < e; p += 32u) {
-                const float4 c = __ldcg(d.edge_centre + __ldcg(ord + p));
+                const float4 c = __ldcg(d.edge_centre + __ldcg(L + p));
                 lo = V3{fminf(lo.x, c.x), fminf(lo.y, c.y), fminf(lo.z, c.z)};
                 hi = V3{fmaxf(hi.x, c.x), fmaxf(hi.y, c.y), fmaxf(hi.z, c.z)};
             }
@@ -827,49 +961,45 @@ __device__ void edge_tree_order(const Ctx& ctx, bool swept) {
             any = true;
         }
         if (!__syncthreads_or(any)) break;
-        // keys: (node start, centre along the node's axis, segment); a
-        // position in a leaf keeps its place (its offset in the leaf)
-        for (uint32_t p = threadIdx.x; p < size; p += blockDim.x) {
-            unsigned long long key = ~0ull;
-            if (p < m) {
-                uint32_t b, e;
-                const uint32_t j = tree_path_of_position(m, level, p, b, e);
-                const uint32_t s = __ldcg(ord + p);
-                if (e - b <= 8u) {
-                    key = (static_cast<unsigned long long>(b) << 52) | (p - b);
-                } else {
-                    const float4 c = __ldcg(d.edge_centre + s);
-                    const uint32_t axis = nc_edge_tree_axis[j];
-                    const float v = axis == 0u ? c.x : (axis == 1u ? c.y : c.z);
-                    key = (static_cast<unsigned long long>(b) << 52) |
-                          (static_cast<unsigned long long>(ordered_bits(v)) << 12) | s;
-                }
-            }
-            nc_edge_tree_keys[p] = key;
-        }
-        __syncthreads();
-        for (uint32_t k = 2u; k <= size; k <<= 1) {
-            for (uint32_t jj = k >> 1; jj > 0u; jj >>= 1) {
-                for (uint32_t i = threadIdx.x; i < size; i += blockDim.x) {
-                    const uint32_t ixj = i ^ jj;
-                    if (ixj > i) {
-                        const unsigned long long a = nc_edge_tree_keys[i], c = nc_edge_tree_keys[ixj];
-                        if ((a > c) == ((i & k) == 0u)) {
-                            nc_edge_tree_keys[i] = c;
-                            nc_edge_tree_keys[ixj] = a;
-                        }
-                    }
-                }
-                __syncthreads();
-            }
-        }
+        // sides: the second half of a splitting node's axis list goes right
         for (uint32_t p = threadIdx.x; p < m; p += blockDim.x) {
             uint32_t b, e;
-            tree_path_of_position(m, level, p, b, e);
-            if (e - b > 8u) ord[p] = static_cast<uint32_t>(nc_edge_tree_keys[p] & 0xfffu);
+            const uint32_t j = tree_path_of_position(m, level, p, b, e);
+            if (e - b <= 8u) {
+                right[__ldcg(L + p)] = 0u;
+                continue;
+            }
+            const uint32_t a = nc_edge_tree_axis[j];
+            right[__ldcg(L + a * m + p)] = p - b >= (e - b) / 2u ? 1u : 0u;
+            leaf_axis[p] = a;
         }
         __syncthreads();
+        // every list: stable partition of each splitting node's range
+        for (uint32_t a = 0; a < 3u; ++a) {
+            for (uint32_t p = threadIdx.x; p < m; p += blockDim.x) prefix[m + p] = __ldcg(right + __ldcg(L + a * m + p));
+            __syncthreads();
+            block_prefix(prefix + m, prefix, m);
+            for (uint32_t p = threadIdx.x; p < m; p += blockDim.x) {
+                uint32_t b, e;
+                tree_path_of_position(m, level, p, b, e);
+                const uint32_t s = __ldcg(L + a * m + p);
+                uint32_t to = p;
+                if (e - b > 8u) {
+                    const uint32_t rights = prefix[p] - prefix[b];
+                    to = prefix[m + p] != 0u ? b + (e - b) / 2u + rights : p - rights;
+                }
+                N[a * m + to] = s;
+            }
+            __syncthreads();
+        }
+        cur ^= 1u;
     }
+    const uint32_t* L = lists + cur * 3u * m;
+    for (uint32_t p = threadIdx.x; p < m; p += blockDim.x) {
+        const uint32_t a = __ldcg(leaf_axis + p);
+        ord[p] = a < 3u ? __ldcg(L + a * m + p) : p;
+    }
+    __syncthreads();
     for (uint32_t p = threadIdx.x; p < m; p += blockDim.x) ord[m + __ldcg(ord + p)] = p;
     __syncthreads();
 }
