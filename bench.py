@@ -411,6 +411,7 @@ def config3_scene(stretch=CONFIG3_COMPLIANCE[0], shear=CONFIG3_COMPLIANCE[1], be
         grips[g]["particle"] = (i, corner["particle"][1], 0, 0)
         grips[g]["targetOffsetAndCompliance"] = (off[0], off[1], off[2], corner["targetOffsetAndCompliance"][3])
     scene.grips = grips
+    scene.config["control"][0, 3] = len(grips)   # the Config's grip count
     return scene
 
 
@@ -660,9 +661,16 @@ def run_ours(args):
     value = world * SUBSTEPS * args.steps / (total_ms / 1000.0)
 
     # e2e through the public API with host buffers: upload state, one frame,
-    # download state; wall clock around the synchronous calls.
-    host_p = solver.particles()
-    host_f = solver.fruits()
+    # download state; wall clock around the synchronous calls.  The state
+    # lives in pinned host memory, read back in place.
+    def pinned(like):
+        buf = torch.empty(like.nbytes, dtype=torch.uint8, pin_memory=True).numpy().view(like.dtype)
+        buf[:] = like
+        return buf
+
+    host_p = pinned(solver.particles())
+    host_f = pinned(solver.fruits())
+    host_cfg = pinned(cfg)
     e2e_times = []
     for k in range(0 if args.no_e2e else args.warmup + args.steps):
         flush.fill_(1.0)
@@ -670,9 +678,9 @@ def run_ours(args):
         t0 = time.perf_counter()
         solver.write_particles(host_p)
         solver.write_fruits(host_f)
-        solver.step(cfg, sched)
-        host_p = solver.particles()
-        host_f = solver.fruits()
+        solver.step(host_cfg, sched)
+        solver.particles(out=host_p)
+        solver.fruits(out=host_f)
         dt = time.perf_counter() - t0
         if k >= args.warmup:
             e2e_times.append(dt)

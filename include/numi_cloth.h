@@ -211,14 +211,18 @@ int numi_cloth_set_stream(numi_cloth_t* handle, void* stream);
  * grip generation, timestep and gravity may change between substeps.  The
  * last substep of the call runs the certificate loop.  Asynchronous on the
  * handle's stream; returns NUMI_CLOTH_OK or a negative code.  Read the
- * failure word with numi_cloth_failure. */
+ * failure word with numi_cloth_failure.  The Configs are copied on the
+ * stream: pageable ones may be reused on return, pinned ones only after the
+ * stream has passed the step. */
 int numi_cloth_step(numi_cloth_t* handle, const NumiClothConfig* configs,
                     uint32_t count, const NumiClothSchedule* schedule);
 
 /* Synchronise the stream and return the accumulated failure word. */
 uint32_t numi_cloth_failure(numi_cloth_t* handle);
 
-/* Host copies of the state (synchronous). */
+/* Host copies of the state (synchronous).  Particle records travel as one
+ * copy through a device staging buffer, transposed to and from the state
+ * arrays on the device; pinned host buffers copy fastest. */
 int numi_cloth_read_particles(numi_cloth_t* handle, NumiClothParticle* out, uint32_t count);
 int numi_cloth_write_particles(numi_cloth_t* handle, const NumiClothParticle* in, uint32_t count);
 int numi_cloth_read_fruits(numi_cloth_t* handle, NumiClothFruit* out, uint32_t count);
@@ -279,8 +283,9 @@ int numi_cloth_pass_counts(numi_cloth_t* handle, uint32_t out[3]);
 int numi_cloth_trace(numi_cloth_t* handle, unsigned long long* out,
                      uint32_t substeps, uint32_t slots);
 
-/* Per-CTA barrier arrival stamps of the last step, [substeps][128][grid CTAs]
- * (ns), when the handle was also created with NUMI_CLOTH_TRACE_CTA=1. */
+/* Per-CTA barrier arrival stamps of the last step, [substeps][128][CTAs of
+ * that launch] (ns; numi_cloth_launch_info's grid), when the handle was also
+ * created with NUMI_CLOTH_TRACE_CTA=1. */
 int numi_cloth_trace_cta(numi_cloth_t* handle, unsigned long long* out, uint32_t substeps);
 
 /* ---------------------------------------------------------------------------

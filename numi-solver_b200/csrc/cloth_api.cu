@@ -123,6 +123,9 @@ struct numi_cloth {
         size_t bytes;
     };
     std::vector<Region> dynamic;
+    // device staging of particle records for the host copies (one transfer
+    // each way, transposed to and from the state arrays on the device)
+    NumiClothParticle* io = nullptr;
 };
 
 namespace {
@@ -1389,38 +1392,63 @@ uint32_t numi_cloth_failure(numi_cloth_t* h) {
     return f | h->host_failure;
 }
 
+// Particle records <-> the state arrays (x, previous, v), one thread per
+// particle: coalesced 16-byte loads and stores on both sides.
+__global__ void numi_cloth_unpack_particles_kernel(const NumiClothParticle* in, float4* x, float4* xp, float4* v,
+                                                   uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4* r = reinterpret_cast<const float4*>(in + i);
+        x[i] = __ldcs(r);
+        xp[i] = __ldcs(r + 1);
+        v[i] = __ldcs(r + 2);
+    }
+}
+
+__global__ void numi_cloth_pack_particles_kernel(const float4* x, const float4* xp, const float4* v,
+                                                 NumiClothParticle* out, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4* r = reinterpret_cast<float4*>(out + i);
+        __stcs(r, x[i]);
+        __stcs(r + 1, xp[i]);
+        __stcs(r + 2, v[i]);
+    }
+}
+
+static_assert(sizeof(NumiClothParticle) == 3u * sizeof(float4), "particle record: three float4 words");
+
+// The handle's staging buffer for particle records, allocated on first use.
+static NumiClothParticle* particle_io(numi_cloth_t* h) {
+    if (h->io == nullptr) h->io = h->buf.alloc<NumiClothParticle>(h->d.n);
+    return h->io;
+}
+
 int numi_cloth_read_particles(numi_cloth_t* h, NumiClothParticle* out, uint32_t count) {
     if (h == nullptr || out == nullptr || count != h->d.n) return NUMI_CLOTH_EINVAL;
     cudaSetDevice(h->device);
-    std::vector<float4> x(count), xp(count), v(count);
-    if (cudaStreamSynchronize(h->stream) != cudaSuccess ||
-        cudaMemcpy(x.data(), h->d.x, count * sizeof(float4), cudaMemcpyDeviceToHost) != cudaSuccess ||
-        cudaMemcpy(xp.data(), h->d.xp, count * sizeof(float4), cudaMemcpyDeviceToHost) != cudaSuccess ||
-        cudaMemcpy(v.data(), h->d.v, count * sizeof(float4), cudaMemcpyDeviceToHost) != cudaSuccess)
+    NumiClothParticle* io = particle_io(h);
+    if (io == nullptr) return NUMI_CLOTH_ECUDA;
+    const uint32_t blocks = std::min<uint32_t>((count + 255u) / 256u, 1184u);
+    numi_cloth_pack_particles_kernel<<<blocks, 256, 0, h->stream>>>(h->d.x, h->d.xp, h->d.v, io, count);
+    if (cudaGetLastError() != cudaSuccess ||
+        cudaMemcpyAsync(out, io, count * sizeof(NumiClothParticle), cudaMemcpyDeviceToHost, h->stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(h->stream) != cudaSuccess)
         return NUMI_CLOTH_ECUDA;
-    for (uint32_t i = 0; i < count; ++i) {
-        out[i].positionAndInverseMass = {x[i].x, x[i].y, x[i].z, x[i].w};
-        out[i].previousAndMass = {xp[i].x, xp[i].y, xp[i].z, xp[i].w};
-        out[i].velocity = {v[i].x, v[i].y, v[i].z, v[i].w};
-    }
     return NUMI_CLOTH_OK;
 }
 
 int numi_cloth_write_particles(numi_cloth_t* h, const NumiClothParticle* in, uint32_t count) {
     if (h == nullptr || in == nullptr || count != h->d.n) return NUMI_CLOTH_EINVAL;
     cudaSetDevice(h->device);
-    std::vector<float4> x(count), xp(count), v(count);
-    for (uint32_t i = 0; i < count; ++i) {
-        const NumiClothParticle& p = in[i];
-        x[i] = make_float4(p.positionAndInverseMass.x, p.positionAndInverseMass.y, p.positionAndInverseMass.z,
-                           p.positionAndInverseMass.w);
-        xp[i] = make_float4(p.previousAndMass.x, p.previousAndMass.y, p.previousAndMass.z, p.previousAndMass.w);
-        v[i] = make_float4(p.velocity.x, p.velocity.y, p.velocity.z, p.velocity.w);
-    }
-    if (cudaStreamSynchronize(h->stream) != cudaSuccess ||
-        cudaMemcpy(h->d.x, x.data(), count * sizeof(float4), cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(h->d.xp, xp.data(), count * sizeof(float4), cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(h->d.v, v.data(), count * sizeof(float4), cudaMemcpyHostToDevice) != cudaSuccess)
+    NumiClothParticle* io = particle_io(h);
+    if (io == nullptr) return NUMI_CLOTH_ECUDA;
+    const uint32_t blocks = std::min<uint32_t>((count + 255u) / 256u, 1184u);
+    if (cudaMemcpyAsync(io, in, count * sizeof(NumiClothParticle), cudaMemcpyHostToDevice, h->stream) !=
+        cudaSuccess)
+        return NUMI_CLOTH_ECUDA;
+    numi_cloth_unpack_particles_kernel<<<blocks, 256, 0, h->stream>>>(io, h->d.x, h->d.xp, h->d.v, count);
+    // synchronous: the caller may reuse its buffer on return
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(h->stream) != cudaSuccess)
         return NUMI_CLOTH_ECUDA;
     return NUMI_CLOTH_OK;
 }
@@ -1569,9 +1597,12 @@ int numi_cloth_trace_cta(numi_cloth_t* h, unsigned long long* out, uint32_t subs
     if (h == nullptr || out == nullptr) return NUMI_CLOTH_EINVAL;
     if (h->d.trace_cta == nullptr || substeps > h->trace_capacity) return NUMI_CLOTH_ESTATE;
     cudaSetDevice(h->device);
+    // the last launch's CTAs (a tile launch may use fewer than the grid)
+    const uint32_t grid = h->last_grid != 0u ? h->last_grid : h->grid;
+    if (grid > h->grid) return NUMI_CLOTH_ESTATE;   // not traced per CTA
     if (cudaStreamSynchronize(h->stream) != cudaSuccess ||
         cudaMemcpy(out, h->d.trace_cta,
-                   static_cast<size_t>(substeps) * NC_TRACE_SLOTS * h->grid * sizeof(unsigned long long),
+                   static_cast<size_t>(substeps) * NC_TRACE_SLOTS * grid * sizeof(unsigned long long),
                    cudaMemcpyDeviceToHost) != cudaSuccess)
         return NUMI_CLOTH_ECUDA;
     return NUMI_CLOTH_OK;

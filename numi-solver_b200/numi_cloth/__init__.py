@@ -535,8 +535,13 @@ class ClothSolver:
     def failure(self) -> int:
         return int(self.lib.numi_cloth_failure(self._h))
 
-    def particles(self) -> np.ndarray:
-        out = np.zeros(self.n, PARTICLE)
+    def particles(self, out: np.ndarray | None = None) -> np.ndarray:
+        """The particle records; `out` (PARTICLE[n], contiguous, e.g. over
+        pinned host memory) receives them when given."""
+        if out is None:
+            out = np.zeros(self.n, PARTICLE)
+        elif out.dtype != PARTICLE or len(out) != self.n or not out.flags["C_CONTIGUOUS"]:
+            raise ClothError("particles(out=): a contiguous PARTICLE array of the cloth's size")
         self._check(self.lib.numi_cloth_read_particles(self._h, _ptr(out), self.n))
         return out
 
@@ -544,8 +549,12 @@ class ClothSolver:
         p = np.ascontiguousarray(p, PARTICLE)
         self._check(self.lib.numi_cloth_write_particles(self._h, _ptr(p), len(p)))
 
-    def fruits(self) -> np.ndarray:
-        out = np.zeros(len(self.scene.fruits), FRUIT)
+    def fruits(self, out: np.ndarray | None = None) -> np.ndarray:
+        """The fruit records; `out` (FRUIT[f], contiguous) receives them when given."""
+        if out is None:
+            out = np.zeros(len(self.scene.fruits), FRUIT)
+        elif out.dtype != FRUIT or len(out) != len(self.scene.fruits) or not out.flags["C_CONTIGUOUS"]:
+            raise ClothError("fruits(out=): a contiguous FRUIT array of the cloth's fruit count")
         self._check(self.lib.numi_cloth_read_fruits(self._h, _ptr(out), len(out)))
         return out
 
