@@ -34,7 +34,9 @@
 //      each);
 //   4. fruit CTA: fruit/yarn friction, fruit frictions, orientation,
 //      release; CTA 0: the next substep's grip attach;
-// with one grid barrier after each, instead of one per colour.
+// with one grid barrier after each, instead of one per colour; the one
+// after phase 4 only where the next substep needs it (friction on listed
+// segments, a grip re-attach, the launch's last substep).
 //
 // Plan of one CTA (host-built, 16-byte aligned words, staged into shared
 // memory once per launch with a bulk copy):
@@ -344,8 +346,23 @@ __device__ bool substep_tiles(Ctx& ctx, bool last) {
         ctx.gx = x_next;
         NC_SYNC(ctx);
     }
-    // 4. frictions on the fruit CTA, the next substep's grip attach
+    // 4. frictions on the fruit CTA, the next substep's grip attach.  The
+    // next substep's first phase reads nothing this phase writes unless the
+    // friction sweep has listed segments (it changes their particles'
+    // velocities) or the grips re-attach: otherwise no CTA waits here, and
+    // the fruit CTA's tail overlaps the tiles' next predict and constraint
+    // chain (the fruit CTA's own next phase follows its tail; the barrier
+    // after that phase joins every CTA).  Every CTA takes the decision from
+    // the configs and the list count, which no CTA changes before every CTA
+    // has read it (the next substep's reset of the count runs only past
+    // this barrier when the count is not zero).
     const bool friction_sweep = s.frictions && d.f_count > 0u;
+    bool hold = last;
+    if (!last) {
+        const SubCfg next = nc::load_cfg(d.cfg + s.cfg_offset + ctx.sub + 1u);
+        const bool attach = next.grip_active && (!ctx.c.grip_active || next.grip_gen != ctx.c.grip_gen);
+        hold = attach || (friction_sweep && __ldcg(d.yarn_list_n) != 0u);
+    }
     if (friction_sweep) yarn_friction_sweep(ctx);
     fruit_tail(ctx, last, friction_sweep);
     if (ctx.grip_cta && !last) {
@@ -353,7 +370,7 @@ __device__ bool substep_tiles(Ctx& ctx, bool last) {
         next.c = nc::load_cfg(d.cfg + s.cfg_offset + ctx.sub + 1u);
         grip_attach(next);
     }
-    NC_SYNC(ctx);
+    if (hold) NC_SYNC(ctx);
     return true;
 }
 
