@@ -51,6 +51,7 @@ namespace {
 constexpr uint32_t kSnapshotSlots = 8;
 constexpr uint32_t kResidentChunk = 4096;   // particles a CTA holds in resident mode
 constexpr uint32_t kResidentClusterChunk = 256;   // default chunk of a small resident cloth
+constexpr uint32_t kBarrierWords = 48;   // barrier counter, abort, release and fruit flags: three 128-byte lines
 
 struct Snapshot {
     bool valid = false;
@@ -630,7 +631,7 @@ cudaError_t launch(numi_cloth* h, uint32_t substeps, const Schedule& s, uint32_t
     const bool edge = sc.primitive_self != 0u && d.edge_count != nullptr;
     if (d.trace != nullptr && substeps > h->trace_capacity) d.trace = nullptr;
     if (d.trace == nullptr) d.trace_cta = nullptr;
-    cudaError_t e = cudaMemsetAsync(h->d.bar_count, 0, 32 * sizeof(unsigned long long), h->stream);
+    cudaError_t e = cudaMemsetAsync(h->d.bar_count, 0, kBarrierWords * sizeof(unsigned long long), h->stream);
     if (e != cudaSuccess) return e;
     h->last_substeps = substeps;
     size_t smem = h->smem;
@@ -1029,9 +1030,10 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
     d.failure = h->buf.alloc<unsigned int>(1);
     // barrier counter (u64) and abort flag share one 16-byte block so one
     // memset resets both before a launch
-    d.bar_count = h->buf.alloc<unsigned long long>(32);
+    d.bar_count = h->buf.alloc<unsigned long long>(kBarrierWords);
     d.abort_flag = reinterpret_cast<unsigned int*>(d.bar_count + 1);
-    d.bar_flag = d.bar_count + 16;   // 128 bytes away from the arrival counter
+    d.bar_flag = d.bar_count + 16;     // 128 bytes away from the arrival counter
+    d.fruit_flag = d.bar_count + 32;   // and 128 more
     d.stats = h->buf.alloc<uint32_t>(4);
 
     // Launch geometry: one resident CTA for a small cloth, else a full

@@ -117,6 +117,7 @@ struct DeviceCloth {
     // the host before every launch) and a sticky abort flag
     unsigned long long* bar_count;
     unsigned long long* bar_flag;   // barrier number released last (own 128-byte line)
+    unsigned long long* fruit_flag; // tile mode: substeps whose fruit-CTA tail is done (own line)
     unsigned int* abort_flag;
     // polls a barrier or neighbour wait makes before it gives up (0: the
     // default NC_BARRIER_SPIN_LIMIT)

@@ -167,6 +167,8 @@ struct Ctx {
     const uint32_t* tp;
     float4* tx;
     FrictionStage* fst;       // tile mode, fruit CTA: the staged friction sweep
+    bool hold_tail;           // tile mode: a grid barrier follows the fruit-CTA tail
+    bool fruit_wait;          // tile mode: the next predict waits for the fruit-CTA tail
 };
 
 __device__ __forceinline__ float4* resident_ptr(const Ctx& c, float4* local_base, uint32_t i) {

@@ -34,9 +34,11 @@
 //      each);
 //   4. fruit CTA: fruit/yarn friction, fruit frictions, orientation,
 //      release; CTA 0: the next substep's grip attach;
-// with one grid barrier after each, instead of one per colour; the one
-// after phase 4 only where the next substep needs it (friction on listed
-// segments, a grip re-attach, the launch's last substep).
+// with one grid barrier after each, instead of one per colour; after
+// phase 4 only where the next substep needs one (a grip re-attach, the
+// launch's last substep, a friction list too long to stage): otherwise a
+// tile CTA whose next predict reads velocities the friction sweep rewrote
+// waits for the fruit CTA's flag, and the others go on.
 //
 // Plan of one CTA (host-built, 16-byte aligned words, staged into shared
 // memory once per launch with a bulk copy):
@@ -280,6 +282,73 @@ __device__ void tile_finalize(const Ctx& ctx) {
     }
 }
 
+// With the per-barrier trace on, a middle tile CTA stamps the end of each
+// step inside the phases into trace slots 64 and up (a CTA barrier first,
+// so the stamp follows the step's last thread).
+#define NC_TILE_MARK_SLOT 64u
+__device__ __forceinline__ void tile_mark(const Ctx& ctx, uint32_t k) {
+    const DeviceCloth& d = ctx.d;
+    if (d.trace == nullptr || ctx.rank != ctx.ranks / 2u) return;
+    __syncthreads();
+    if (threadIdx.x == 0 && NC_TILE_MARK_SLOT + k < NC_TRACE_SLOTS)
+        d.trace[static_cast<size_t>(ctx.sub) * NC_TRACE_SLOTS + NC_TILE_MARK_SLOT + k] = globaltimer();
+}
+
+// Whether the friction sweep's listed segments touch a particle this CTA
+// predicts in the next substep's first phase (chain 0's closure): their
+// velocities are the ones the sweep rewrites.  Tile CTAs, listed at most
+// NC_FRICTION_STAGE.
+__device__ bool tile_touches_listed(const Ctx& ctx, uint32_t listed) {
+    const DeviceCloth& d = ctx.d;
+    uint32_t* s_pid = reinterpret_cast<uint32_t*>(&nc_red_smem[0][0]);
+    static_assert(2u * NC_FRICTION_STAGE * sizeof(uint32_t) <= sizeof(nc_red_smem), "listed particles exceed the scratch");
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < listed; k += blockDim.x) {
+        const uint2 ij = __ldg(d.d_ij + __ldcg(d.yarn_list + k));
+        s_pid[2u * k] = ij.x;
+        s_pid[2u * k + 1u] = ij.y;
+    }
+    __syncthreads();
+    const uint32_t nl = ctx.tp[4u + NC_TILE_CONSTRAINTS];
+    const uint32_t* gi = tile_list(ctx);
+    bool hit = false;
+    for (uint32_t l = threadIdx.x; l < nl && !hit; l += blockDim.x) {
+        const uint32_t id = gi[l];
+        for (uint32_t e = 0; e < 2u * listed; ++e) hit = hit || s_pid[e] == id;
+    }
+    return __syncthreads_or(hit) != 0;
+}
+
+// Wait (bounded) until the fruit CTA has finished the tail of substep
+// `done` - 1 of this launch; false when the wait gave up or another CTA
+// aborted.
+__device__ bool tile_wait_fruit(const Ctx& ctx, unsigned long long done) {
+    const DeviceCloth& d = ctx.d;
+    __shared__ unsigned s_fruit_abort;
+    if (threadIdx.x == 0) {
+        const unsigned limit = d.spin_limit != 0u ? d.spin_limit : NC_BARRIER_SPIN_LIMIT;
+        unsigned ab = 0u;
+        unsigned spins = 0u;
+        while (ld_relaxed_u64(d.fruit_flag) < done) {
+            ++spins;
+            if ((spins & 63u) == 0u && ld_acquire(d.abort_flag) != 0u) {
+                ab = 1u;
+                break;
+            }
+            if (spins > limit) {
+                atomicOr(d.failure, NUMI_CLOTH_FAILURE_TIMEOUT);
+                atomicExch(d.abort_flag, 1u);
+                ab = 1u;
+                break;
+            }
+        }
+        if (!ab) (void)ld_acquire_u64(d.fruit_flag);
+        s_fruit_abort = ab;
+    }
+    __syncthreads();
+    return s_fruit_abort == 0u;
+}
+
 // One substep in tile mode (see the top of this file).
 __device__ bool substep_tiles(Ctx& ctx, bool last) {
     const DeviceCloth& d = ctx.d;
@@ -298,13 +367,23 @@ __device__ bool substep_tiles(Ctx& ctx, bool last) {
                 fruit_pair_sweep(d, *ctx.fs, ctx.c.dt);
             }
         } else {
+            // the previous substep's friction rewrote velocities this CTA
+            // predicts: wait for the fruit CTA's tail
+            if (ctx.fruit_wait && !tile_wait_fruit(ctx, ctx.sub)) return false;
+            ctx.fruit_wait = false;
+            tile_mark(ctx, 0u);
             tile_predict(ctx, v_next);
+            tile_mark(ctx, 1u);
             tile_chain(ctx, NC_TILE_CONSTRAINTS, dt2);
+            tile_mark(ctx, 2u);
             tile_grips(ctx);
             if (self && !fruits) tile_insert(ctx);
             tile_store(ctx, x_next);
+            tile_mark(ctx, 3u);
         }
-        if (ctx.tid == 0u) *d.yarn_list_n = 0u;
+        // the friction list restarts empty: here on a launch's first
+        // substep, at the end of the fruit CTA's tail on the others
+        if (ctx.tid == 0u && ctx.sub == 0u) *d.yarn_list_n = 0u;
         ctx.gx = x_next;
         ctx.gv = v_next;
         NC_SYNC(ctx);
@@ -313,16 +392,41 @@ __device__ bool substep_tiles(Ctx& ctx, bool last) {
     if (fruits) {
         float4* x_next = other_x(ctx);
         if (!ctx.fruit_cta) {
+            tile_mark(ctx, 4u);
             tile_load(ctx, NC_TILE_YARN);
+            tile_mark(ctx, 5u);
             tile_yarn(ctx);
+            tile_mark(ctx, 6u);
             if (self) tile_insert(ctx);
+            tile_mark(ctx, 7u);
             tile_store(ctx, x_next);
+            tile_mark(ctx, 8u);
         }
         ctx.gx = x_next;
         ctx.fruit_pending = true;
         NC_SYNC(ctx);
     }
-    // 3. self-contact solve + ground, strain sweeps, finalize
+    // 3. self-contact solve + ground, strain sweeps, finalize.  Every CTA
+    // decides here, alike, whether a grid barrier must follow the fruit
+    // CTA's tail (phase 4): the next substep's first phase reads nothing
+    // the tail writes except the velocities the friction sweep rewrites and
+    // the grips a re-attach rewrites.  Without a re-attach (or the launch's
+    // end, or a list too long to stage) there is no barrier: a tile CTA
+    // whose predict closure holds a listed segment's particle waits for the
+    // fruit CTA's flag before its next predict, the others go on.  The
+    // list and its count stay unchanged until the fruit CTA's tail resets
+    // them, after this phase's barrier.
+    const bool friction_sweep = s.frictions && d.f_count > 0u;
+    {
+        const uint32_t listed = friction_sweep ? min(__ldcg(d.yarn_list_n), d.d_count) : 0u;
+        bool attach = false;
+        if (!last) {
+            const SubCfg next = nc::load_cfg(d.cfg + s.cfg_offset + ctx.sub + 1u);
+            attach = next.grip_active && (!ctx.c.grip_active || next.grip_gen != ctx.c.grip_gen);
+        }
+        ctx.hold_tail = last || attach || listed > NC_FRICTION_STAGE;
+        if (!ctx.hold_tail && listed > 0u && !ctx.fruit_cta) ctx.fruit_wait = tile_touches_listed(ctx, listed);
+    }
     const uint32_t sweeps = max(s.strain_sweeps, 1u);
     for (uint32_t sw = 0; sw < sweeps; ++sw) {
         float4* x_next = other_x(ctx);
@@ -337,40 +441,43 @@ __device__ bool substep_tiles(Ctx& ctx, bool last) {
                 if (s.frictions && fruits) friction_stage(ctx);
             }
         } else {
+            tile_mark(ctx, 9u);
             tile_load(ctx, NC_TILE_STRAIN);
+            tile_mark(ctx, 10u);
             if (sw == 0u) tile_self_ground(ctx, self);
+            tile_mark(ctx, 11u);
             if (s.strain_sweeps > 0u) tile_chain(ctx, NC_TILE_STRAIN, dt2);
+            tile_mark(ctx, 12u);
             if (final_sweep) tile_finalize(ctx);
+            tile_mark(ctx, 13u);
             tile_store(ctx, x_next);
+            tile_mark(ctx, 14u);
         }
         ctx.gx = x_next;
         NC_SYNC(ctx);
     }
-    // 4. frictions on the fruit CTA, the next substep's grip attach.  The
-    // next substep's first phase reads nothing this phase writes unless the
-    // friction sweep has listed segments (it changes their particles'
-    // velocities) or the grips re-attach: otherwise no CTA waits here, and
-    // the fruit CTA's tail overlaps the tiles' next predict and constraint
-    // chain (the fruit CTA's own next phase follows its tail; the barrier
-    // after that phase joins every CTA).  Every CTA takes the decision from
-    // the configs and the list count, which no CTA changes before every CTA
-    // has read it (the next substep's reset of the count runs only past
-    // this barrier when the count is not zero).
-    const bool friction_sweep = s.frictions && d.f_count > 0u;
-    bool hold = last;
-    if (!last) {
-        const SubCfg next = nc::load_cfg(d.cfg + s.cfg_offset + ctx.sub + 1u);
-        const bool attach = next.grip_active && (!ctx.c.grip_active || next.grip_gen != ctx.c.grip_gen);
-        hold = attach || (friction_sweep && __ldcg(d.yarn_list_n) != 0u);
-    }
+    // 4. frictions on the fruit CTA, the next substep's grip attach (the
+    // barrier after it only where phase 3 decided so)
     if (friction_sweep) yarn_friction_sweep(ctx);
     fruit_tail(ctx, last, friction_sweep);
+    if (ctx.fruit_cta) {
+        // fruit_tail ended with a CTA barrier: the list is read
+        if (threadIdx.x == 0) {
+            *d.yarn_list_n = 0u;
+            asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(d.fruit_flag),
+                         "l"(static_cast<unsigned long long>(ctx.sub) + 1ull)
+                         : "memory");
+        }
+    }
     if (ctx.grip_cta && !last) {
         Ctx next = ctx;
         next.c = nc::load_cfg(d.cfg + s.cfg_offset + ctx.sub + 1u);
         grip_attach(next);
     }
-    if (hold) NC_SYNC(ctx);
+    if (ctx.hold_tail) {
+        ctx.fruit_wait = false;
+        NC_SYNC(ctx);
+    }
     return true;
 }
 
