@@ -951,139 +951,160 @@ __device__ void self_insert(Ctx& ctx, uint32_t it) {
 // may go through L1, where neighbouring particles of a CTA share cells;
 // under the cluster barrier (cluster-scope acquire) they stay L2 reads.
 #define NC_SELF_BATCH 8u
+// A particle's query: its buckets, the candidates each holds (prefix
+// counts, a bucket met twice counts once) and their total.
+struct SelfQuery {
+    uint32_t bk[8];
+    uint32_t pre[9];
+};
+
+// Buckets of the 2 x 2 x 2 cells on the particle's side of its cell centre
+// and the heads of those within reach, loaded together.
+__device__ __forceinline__ void self_heads(const Ctx& ctx, const float4& p, SelfQuery& q, unsigned long long hd[8],
+                                           bool near[8]) {
+    const DeviceCloth& d = ctx.d;
+    const float inv_cell = 1.0f / (4.0f * ctx.c.radius);
+    const bool l1 = d.cluster_barrier == 0u;
+    int base[3], step[3];
+    float gap2[3];   // squared distance to the probed neighbour cell, in cell units
+    const float coord[3] = {p.x * inv_cell, p.y * inv_cell, p.z * inv_cell};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float c0 = floorf(coord[k]);
+        const float frac = coord[k] - c0;
+        base[k] = static_cast<int>(c0);
+        step[k] = frac < 0.5f ? -1 : 1;
+        const float gap = frac < 0.5f ? frac : 1.0f - frac;
+        gap2[k] = gap * gap;
+    }
+#pragma unroll
+    for (uint32_t c = 0; c < 8u; ++c)
+        q.bk[c] = cell_bucket(base[0] + ((c & 1u) ? step[0] : 0), base[1] + ((c & 2u) ? step[1] : 0),
+                              base[2] + ((c & 4u) ? step[2] : 0), d.hash_mask);
+    // A neighbour cell farther than the contact distance (half a cell)
+    // cannot hold a contact.  The margin covers the rounding of the cell
+    // coordinates: 1e-3 cells plus a few ulps of the largest coordinate.
+    // Only the heads of near cells are read.
+    const float slack = 0.5f + 1.0e-3f + 2.4e-7f * fmaxf(fabsf(coord[0]), fmaxf(fabsf(coord[1]), fabsf(coord[2])));
+    const float reach2 = slack * slack;
+#pragma unroll
+    for (uint32_t c = 0; c < 8u; ++c) {
+        const float g2 = ((c & 1u) ? gap2[0] : 0.0f) + ((c & 2u) ? gap2[1] : 0.0f) + ((c & 4u) ? gap2[2] : 0.0f);
+        near[c] = c == 0u || g2 < reach2;
+        hd[c] = !near[c] ? 0ull : l1 ? __ldca(d.hash_head + q.bk[c]) : __ldcg(d.hash_head + q.bk[c]);
+    }
+}
+
+// Candidates per bucket of this pass (a bucket met twice counts once).
+__device__ __forceinline__ uint32_t self_counts(uint32_t tag, SelfQuery& q, const unsigned long long hd[8],
+                                                const bool near[8]) {
+    q.pre[0] = 0u;
+#pragma unroll
+    for (uint32_t c = 0; c < 8u; ++c) {
+        bool repeat = false;
+#pragma unroll
+        for (uint32_t e = 0; e < c; ++e) repeat = repeat || (near[e] && q.bk[e] == q.bk[c]);
+        const uint32_t cnt = (near[c] && !repeat && static_cast<uint32_t>(hd[c] >> 32) == tag)
+                                 ? min(static_cast<uint32_t>(hd[c]), NC_HASH_CAP)
+                                 : 0u;
+        q.pre[c + 1u] = q.pre[c] + cnt;
+    }
+    return q.pre[8];
+}
+
+// Slot of candidate t (past the end: the last one again).
+__device__ __forceinline__ uint32_t self_slot(const SelfQuery& q, uint32_t t, uint32_t total) {
+    t = min(t, total - 1u);
+    uint32_t bq = q.bk[0], pq = 0u;
+#pragma unroll
+    for (uint32_t k = 1; k < 8u; ++k)
+        if (t >= q.pre[k]) {
+            bq = q.bk[k];
+            pq = q.pre[k];
+        }
+    return bq * NC_HASH_CAP + (t - pq);
+}
+
+// One candidate entry e of particle a at its start-of-pass position p: the
+// reference pair correction (a's half), summed in fixed point.
+__device__ __forceinline__ void self_pair(const Ctx& ctx, uint32_t a, const float4& p, const float4& e,
+                                          long long sum[3], bool& touched, unsigned long long& contacts,
+                                          float& max_pen) {
+    const DeviceCloth& d = ctx.d;
+    const float target = 2.0f * ctx.c.radius;
+    const uint32_t b = __float_as_uint(e.w);
+    if (b == a) return;
+    const V3 diff = xyz(e) - xyz(p);
+    const float L = len3(diff);
+    if (L >= target || L < 1.0e-12f) return;
+    // the partner's inverse mass (fixed; the corrections of this pass
+    // rewrite only positions)
+    const float den = p.w + px(ctx, b).w;
+    if (den <= 0.0f) return;
+    if (local_pair(d, a, b)) return;
+    const V3 corr = diff * ((target - L) / (L * den));
+    sum[0] += to_fixed(-(corr.x * p.w));
+    sum[1] += to_fixed(-(corr.y * p.w));
+    sum[2] += to_fixed(-(corr.z * p.w));
+    touched = true;
+    if (a < b) {
+        ++contacts;
+        max_pen = fmaxf(max_pen, target - L);
+    }
+}
+
+// The overflow list (particles of full buckets), then the moved position.
+__device__ __forceinline__ bool self_finish(const Ctx& ctx, uint32_t tag, uint32_t a, const float4& p,
+                                            long long sum[3], bool touched, float4& moved,
+                                            unsigned long long& contacts, float& max_pen) {
+    const DeviceCloth& d = ctx.d;
+    const bool l1 = d.cluster_barrier == 0u;
+    const unsigned long long oh = l1 ? __ldca(d.hash_over_head) : __ldcg(d.hash_over_head);
+    const uint32_t over = static_cast<uint32_t>(oh >> 32) == tag ? min(static_cast<uint32_t>(oh), d.n) : 0u;
+    for (uint32_t o = 0; o < over; ++o) self_pair(ctx, a, p, __ldcg(&d.hash_over[o].pos), sum, touched, contacts, max_pen);
+    if (touched) {
+        const float dx = from_fixed(static_cast<unsigned long long>(sum[0]));
+        const float dy = from_fixed(static_cast<unsigned long long>(sum[1]));
+        const float dz = from_fixed(static_cast<unsigned long long>(sum[2]));
+        moved = make_float4(p.x + dx, p.y + dy, p.z + dz, p.w);
+    }
+    return touched;
+}
+
+// Resolve every particle's pairs.  A cell is twice the contact distance,
+// so the 2 x 2 x 2 cells on the particle's side of its own cell's centre
+// hold every particle closer than the contact distance.  The eight bucket
+// heads are read together, then the candidates in batches of eight, every
+// load of a batch issued before any is used.  The grid is read-only in this
+// phase and the grid barrier before it is a gpu-scope acquire, so the reads
+// may go through L1, where neighbouring particles of a CTA share cells;
+// under the cluster barrier (cluster-scope acquire) they stay L2 reads.
 // The pass of particle a at its start-of-pass position p: true when a pair
 // moved it, with the moved position in `moved`; counts the pairs a < b and the
 // deepest penetration.
 __device__ __forceinline__ bool self_solve_one(const Ctx& ctx, uint32_t tag, uint32_t a, const float4& p,
                                                float4& moved, unsigned long long& contacts, float& max_pen) {
     const DeviceCloth& d = ctx.d;
-    const float target = 2.0f * ctx.c.radius;
-    const float inv_cell = 1.0f / (4.0f * ctx.c.radius);
     const bool l1 = d.cluster_barrier == 0u;
-    {
-        int base[3], step[3];
-        float gap2[3];   // squared distance to the probed neighbour cell, in cell units
-        const float coord[3] = {p.x * inv_cell, p.y * inv_cell, p.z * inv_cell};
+    SelfQuery q;
+    unsigned long long hd[8];
+    bool near[8];
+    self_heads(ctx, p, q, hd, near);
+    const uint32_t total = self_counts(tag, q, hd, near);
+    long long sum[3] = {0, 0, 0};
+    bool touched = false;
+    for (uint32_t t0 = 0; t0 < total; t0 += NC_SELF_BATCH) {
+        float4 e[NC_SELF_BATCH];
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            const float c0 = floorf(coord[k]);
-            const float frac = coord[k] - c0;
-            base[k] = static_cast<int>(c0);
-            step[k] = frac < 0.5f ? -1 : 1;
-            const float gap = frac < 0.5f ? frac : 1.0f - frac;
-            gap2[k] = gap * gap;
+        for (uint32_t j = 0; j < NC_SELF_BATCH; ++j) {
+            const uint32_t slot = self_slot(q, t0 + j, total);
+            e[j] = l1 ? __ldca(&d.hash[slot].pos) : __ldcg(&d.hash[slot].pos);
         }
-        uint32_t bk[8];
-        unsigned long long hd[8];
 #pragma unroll
-        for (uint32_t q = 0; q < 8u; ++q)
-            bk[q] = cell_bucket(base[0] + ((q & 1u) ? step[0] : 0), base[1] + ((q & 2u) ? step[1] : 0),
-                                base[2] + ((q & 4u) ? step[2] : 0), d.hash_mask);
-        // A neighbour cell farther than the contact distance (half a cell)
-        // cannot hold a contact.  The margin covers the rounding of the cell
-        // coordinates: 1e-3 cells plus a few ulps of the largest coordinate.
-        // Only the heads of near cells are read.
-        const float slack =
-            0.5f + 1.0e-3f + 2.4e-7f * fmaxf(fabsf(coord[0]), fmaxf(fabsf(coord[1]), fabsf(coord[2])));
-        const float reach2 = slack * slack;
-        bool near[8];
-#pragma unroll
-        for (uint32_t q = 0; q < 8u; ++q) {
-            const float g2 = ((q & 1u) ? gap2[0] : 0.0f) + ((q & 2u) ? gap2[1] : 0.0f) + ((q & 4u) ? gap2[2] : 0.0f);
-            near[q] = q == 0u || g2 < reach2;
-            hd[q] = !near[q] ? 0ull : l1 ? __ldca(d.hash_head + bk[q]) : __ldcg(d.hash_head + bk[q]);
-        }
-        // candidates per bucket (a bucket met twice counts once)
-        uint32_t pre[9];
-        pre[0] = 0u;
-#pragma unroll
-        for (uint32_t q = 0; q < 8u; ++q) {
-            bool repeat = false;
-#pragma unroll
-            for (uint32_t e = 0; e < q; ++e) repeat = repeat || (near[e] && bk[e] == bk[q]);
-            const uint32_t cnt = (near[q] && !repeat && static_cast<uint32_t>(hd[q] >> 32) == tag)
-                                     ? min(static_cast<uint32_t>(hd[q]), NC_HASH_CAP)
-                                     : 0u;
-            pre[q + 1u] = pre[q] + cnt;
-        }
-        const uint32_t total = pre[8];
-        long long sum[3] = {0, 0, 0};
-        bool touched = false;
-        for (uint32_t t0 = 0; t0 < total; t0 += NC_SELF_BATCH) {
-            uint32_t slot[NC_SELF_BATCH];
-#pragma unroll
-            for (uint32_t j = 0; j < NC_SELF_BATCH; ++j) {
-                const uint32_t t = min(t0 + j, total - 1u);   // past the end: repeat the last
-                uint32_t bq = bk[0], pq = 0u;
-#pragma unroll
-                for (uint32_t k = 1; k < 8u; ++k)
-                    if (t >= pre[k]) {
-                        bq = bk[k];
-                        pq = pre[k];
-                    }
-                slot[j] = bq * NC_HASH_CAP + (t - pq);
-            }
-            float4 e[NC_SELF_BATCH];
-#pragma unroll
-            for (uint32_t j = 0; j < NC_SELF_BATCH; ++j)
-                e[j] = l1 ? __ldca(&d.hash[slot[j]].pos) : __ldcg(&d.hash[slot[j]].pos);
-#pragma unroll
-            for (uint32_t j = 0; j < NC_SELF_BATCH; ++j) {
-                if (t0 + j >= total) continue;
-                const uint32_t b = __float_as_uint(e[j].w);
-                if (b == a) continue;
-                const V3 diff = xyz(e[j]) - xyz(p);
-                const float L = len3(diff);
-                if (L >= target || L < 1.0e-12f) continue;
-                // the partner's inverse mass (fixed; the corrections of this
-                // pass rewrite only positions)
-                const float den = p.w + px(ctx, b).w;
-                if (den <= 0.0f) continue;
-                if (local_pair(d, a, b)) continue;
-                const V3 corr = diff * ((target - L) / (L * den));
-                sum[0] += to_fixed(-(corr.x * p.w));
-                sum[1] += to_fixed(-(corr.y * p.w));
-                sum[2] += to_fixed(-(corr.z * p.w));
-                touched = true;
-                if (a < b) {
-                    ++contacts;
-                    max_pen = fmaxf(max_pen, target - L);
-                }
-            }
-        }
-        // the overflow list (particles of full buckets)
-        {
-            const unsigned long long oh = l1 ? __ldca(d.hash_over_head) : __ldcg(d.hash_over_head);
-            const uint32_t over = static_cast<uint32_t>(oh >> 32) == tag ? min(static_cast<uint32_t>(oh), d.n) : 0u;
-            for (uint32_t o = 0; o < over; ++o) {
-                const float4 e = __ldcg(&d.hash_over[o].pos);
-                const uint32_t b = __float_as_uint(e.w);
-                if (b == a) continue;
-                const V3 diff = xyz(e) - xyz(p);
-                const float L = len3(diff);
-                if (L >= target || L < 1.0e-12f) continue;
-                const float den = p.w + px(ctx, b).w;
-                if (den <= 0.0f) continue;
-                if (local_pair(d, a, b)) continue;
-                const V3 corr = diff * ((target - L) / (L * den));
-                sum[0] += to_fixed(-(corr.x * p.w));
-                sum[1] += to_fixed(-(corr.y * p.w));
-                sum[2] += to_fixed(-(corr.z * p.w));
-                touched = true;
-                if (a < b) {
-                    ++contacts;
-                    max_pen = fmaxf(max_pen, target - L);
-                }
-            }
-        }
-        if (touched) {
-            const float dx = from_fixed(static_cast<unsigned long long>(sum[0]));
-            const float dy = from_fixed(static_cast<unsigned long long>(sum[1]));
-            const float dz = from_fixed(static_cast<unsigned long long>(sum[2]));
-            moved = make_float4(p.x + dx, p.y + dy, p.z + dz, p.w);
-        }
-        return touched;
+        for (uint32_t j = 0; j < NC_SELF_BATCH; ++j)
+            if (t0 + j < total) self_pair(ctx, a, p, e[j], sum, touched, contacts, max_pen);
     }
+    return self_finish(ctx, tag, a, p, sum, touched, moved, contacts, max_pen);
 }
 
 // The self-contact statistics of a CTA's particles: one atomic pair per
@@ -2148,6 +2169,7 @@ __device__ __forceinline__ void run_frame(const DeviceCloth& src, const Schedule
             if (!nc::tile_stage(ctx, plan)) return;
             ctx.tx = reinterpret_cast<float4*>(
                 dynamic_smem + nc_fruit_offset() + 4u * (d.tile_off[rank + 1u] - d.tile_off[rank]));
+            ctx.tile_box = nc::tile_closure_box(ctx);
         }
     } else {
         nc::neighbour_stage(ctx);

@@ -168,7 +168,8 @@ struct Ctx {
     float4* tx;
     FrictionStage* fst;       // tile mode, fruit CTA: the staged friction sweep
     bool hold_tail;           // tile mode: a grid barrier follows the fruit-CTA tail
-    bool fruit_wait;          // tile mode: the next predict waits for the fruit-CTA tail
+    bool fruit_wait;          // tile mode: the next predict waits for the fruit-CTA friction
+    uint4 tile_box;           // tile mode: rows and columns (grid cloth) or index range of chain 0's closure
 };
 
 __device__ __forceinline__ float4* resident_ptr(const Ctx& c, float4* local_base, uint32_t i) {

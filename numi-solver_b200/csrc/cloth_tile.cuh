@@ -294,34 +294,60 @@ __device__ __forceinline__ void tile_mark(const Ctx& ctx, uint32_t k) {
         d.trace[static_cast<size_t>(ctx.sub) * NC_TRACE_SLOTS + NC_TILE_MARK_SLOT + k] = globaltimer();
 }
 
-// Whether the friction sweep's listed segments touch a particle this CTA
-// predicts in the next substep's first phase (chain 0's closure): their
-// velocities are the ones the sweep rewrites.  Tile CTAs, listed at most
-// NC_FRICTION_STAGE.
-__device__ bool tile_touches_listed(const Ctx& ctx, uint32_t listed) {
-    const DeviceCloth& d = ctx.d;
-    uint32_t* s_pid = reinterpret_cast<uint32_t*>(&nc_red_smem[0][0]);
-    static_assert(2u * NC_FRICTION_STAGE * sizeof(uint32_t) <= sizeof(nc_red_smem), "listed particles exceed the scratch");
-    __syncthreads();
-    for (uint32_t k = threadIdx.x; k < listed; k += blockDim.x) {
-        const uint2 ij = __ldg(d.d_ij + __ldcg(d.yarn_list + k));
-        s_pid[2u * k] = ij.x;
-        s_pid[2u * k + 1u] = ij.y;
+// Row and column of a particle of a grid cloth (row-major), else (0, index).
+__device__ __forceinline__ uint2 tile_cell(const DeviceCloth& d, uint32_t i) {
+    return d.grid_width != 0u ? make_uint2(i / d.grid_width, i % d.grid_width) : make_uint2(0u, i);
+}
+
+// The bounding box, in rows and columns (or indices), of the particles this
+// CTA predicts in a substep's first phase (chain 0's closure); once per
+// launch.
+__device__ uint4 tile_closure_box(const Ctx& ctx) {
+    __shared__ uint32_t s_box[4];
+    if (threadIdx.x == 0) {
+        s_box[0] = s_box[2] = 0xffffffffu;
+        s_box[1] = s_box[3] = 0u;
     }
     __syncthreads();
     const uint32_t nl = ctx.tp[4u + NC_TILE_CONSTRAINTS];
     const uint32_t* gi = tile_list(ctx);
+    uint32_t r0 = 0xffffffffu, r1 = 0u, c0 = 0xffffffffu, c1 = 0u;
+    for (uint32_t l = threadIdx.x; l < nl; l += blockDim.x) {
+        const uint2 rc = tile_cell(ctx.d, gi[l]);
+        r0 = min(r0, rc.x);
+        r1 = max(r1, rc.x);
+        c0 = min(c0, rc.y);
+        c1 = max(c1, rc.y);
+    }
+    atomicMin(&s_box[0], r0);
+    atomicMax(&s_box[1], r1);
+    atomicMin(&s_box[2], c0);
+    atomicMax(&s_box[3], c1);
+    __syncthreads();
+    const uint4 box = make_uint4(s_box[0], s_box[1], s_box[2], s_box[3]);
+    __syncthreads();
+    return box;
+}
+
+// Whether a friction-listed segment may touch a particle this CTA predicts
+// in the next substep's first phase (its closure box: a superset), whose
+// velocity the friction sweep rewrites.  Tile CTAs.
+__device__ bool tile_touches_listed(const Ctx& ctx, uint32_t listed) {
+    const DeviceCloth& d = ctx.d;
+    const uint4 b = ctx.tile_box;
     bool hit = false;
-    for (uint32_t l = threadIdx.x; l < nl && !hit; l += blockDim.x) {
-        const uint32_t id = gi[l];
-        for (uint32_t e = 0; e < 2u * listed; ++e) hit = hit || s_pid[e] == id;
+    for (uint32_t k = threadIdx.x; k < listed; k += blockDim.x) {
+        const uint2 ij = __ldg(d.d_ij + __ldcg(d.yarn_list + k));
+        const uint2 p = tile_cell(d, ij.x), q = tile_cell(d, ij.y);
+        hit = hit || (p.x >= b.x && p.x <= b.y && p.y >= b.z && p.y <= b.w) ||
+              (q.x >= b.x && q.x <= b.y && q.y >= b.z && q.y <= b.w);
     }
     return __syncthreads_or(hit) != 0;
 }
 
-// Wait (bounded) until the fruit CTA has finished the tail of substep
-// `done` - 1 of this launch; false when the wait gave up or another CTA
-// aborted.
+// Wait (bounded) until the fruit CTA has finished the friction sweep of
+// substep `done` - 1 of this launch; false when the wait gave up or another
+// CTA aborted.
 __device__ bool tile_wait_fruit(const Ctx& ctx, unsigned long long done) {
     const DeviceCloth& d = ctx.d;
     __shared__ unsigned s_fruit_abort;
@@ -457,11 +483,12 @@ __device__ bool substep_tiles(Ctx& ctx, bool last) {
         NC_SYNC(ctx);
     }
     // 4. frictions on the fruit CTA, the next substep's grip attach (the
-    // barrier after it only where phase 3 decided so)
+    // barrier after it only where phase 3 decided so).  The fruit CTA
+    // releases its flag as soon as the friction sweep has written the
+    // velocities back: the rest of its tail touches only fruit state.
     if (friction_sweep) yarn_friction_sweep(ctx);
-    fruit_tail(ctx, last, friction_sweep);
     if (ctx.fruit_cta) {
-        // fruit_tail ended with a CTA barrier: the list is read
+        __syncthreads();   // the sweep's velocity stores and list reads are done
         if (threadIdx.x == 0) {
             *d.yarn_list_n = 0u;
             asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(d.fruit_flag),
@@ -469,6 +496,7 @@ __device__ bool substep_tiles(Ctx& ctx, bool last) {
                          : "memory");
         }
     }
+    fruit_tail(ctx, last, friction_sweep);
     if (ctx.grip_cta && !last) {
         Ctx next = ctx;
         next.c = nc::load_cfg(d.cfg + s.cfg_offset + ctx.sub + 1u);
