@@ -901,6 +901,9 @@ __device__ void edge_tree_order(const Ctx& ctx, bool swept) {
     uint32_t* lists = d.edge_tree + 2u * m;   // [2][3][m]
     uint32_t* right = lists + 6u * m;         // per segment: goes to the right child
     uint32_t* leaf_axis = right + m;          // per position: axis of its deepest split
+    // Every array here is written and read by this CTA alone between CTA
+    // barriers, which make the writes visible to its threads: plain loads,
+    // served from L1.
     for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
         const uint2 ab = __ldg(d.y_ij + k);
         const EdgeBox bx = edge_box(xyz(ld(d.edge_x0 + ab.x)), xyz(ld(d.edge_x0 + ab.y)), xyz(ld(d.xp + ab.x)),
@@ -917,7 +920,7 @@ __device__ void edge_tree_order(const Ctx& ctx, bool swept) {
         for (uint32_t p = threadIdx.x; p < size; p += blockDim.x) {
             unsigned long long key = ~0ull;
             if (p < m) {
-                const float4 c = __ldcg(d.edge_centre + p);
+                const float4 c = d.edge_centre[p];
                 const float v = a == 0u ? c.x : (a == 1u ? c.y : c.z);
                 key = (static_cast<unsigned long long>(ordered_bits(v)) << 12) | p;
             }
@@ -942,7 +945,7 @@ __device__ void edge_tree_order(const Ctx& ctx, bool swept) {
             if (!tree_node_of_path(m, level, j, b, e) || e - b <= 8u) continue;
             V3 lo{INFINITY, INFINITY, INFINITY}, hi{-INFINITY, -INFINITY, -INFINITY};
             for (uint32_t p = b + lane; p < e; p += 32u) {
-                const float4 c = __ldcg(d.edge_centre + __ldcg(L + p));
+                const float4 c = d.edge_centre[L[p]];
                 lo = V3{fminf(lo.x, c.x), fminf(lo.y, c.y), fminf(lo.z, c.z)};
                 hi = V3{fmaxf(hi.x, c.x), fmaxf(hi.y, c.y), fmaxf(hi.z, c.z)};
             }
@@ -966,23 +969,23 @@ __device__ void edge_tree_order(const Ctx& ctx, bool swept) {
             uint32_t b, e;
             const uint32_t j = tree_path_of_position(m, level, p, b, e);
             if (e - b <= 8u) {
-                right[__ldcg(L + p)] = 0u;
+                right[L[p]] = 0u;
                 continue;
             }
             const uint32_t a = nc_edge_tree_axis[j];
-            right[__ldcg(L + a * m + p)] = p - b >= (e - b) / 2u ? 1u : 0u;
+            right[L[a * m + p]] = p - b >= (e - b) / 2u ? 1u : 0u;
             leaf_axis[p] = a;
         }
         __syncthreads();
         // every list: stable partition of each splitting node's range
         for (uint32_t a = 0; a < 3u; ++a) {
-            for (uint32_t p = threadIdx.x; p < m; p += blockDim.x) prefix[m + p] = __ldcg(right + __ldcg(L + a * m + p));
+            for (uint32_t p = threadIdx.x; p < m; p += blockDim.x) prefix[m + p] = right[L[a * m + p]];
             __syncthreads();
             block_prefix(prefix + m, prefix, m);
             for (uint32_t p = threadIdx.x; p < m; p += blockDim.x) {
                 uint32_t b, e;
                 tree_path_of_position(m, level, p, b, e);
-                const uint32_t s = __ldcg(L + a * m + p);
+                const uint32_t s = L[a * m + p];
                 uint32_t to = p;
                 if (e - b > 8u) {
                     const uint32_t rights = prefix[p] - prefix[b];
@@ -996,11 +999,11 @@ __device__ void edge_tree_order(const Ctx& ctx, bool swept) {
     }
     const uint32_t* L = lists + cur * 3u * m;
     for (uint32_t p = threadIdx.x; p < m; p += blockDim.x) {
-        const uint32_t a = __ldcg(leaf_axis + p);
-        ord[p] = a < 3u ? __ldcg(L + a * m + p) : p;
+        const uint32_t a = leaf_axis[p];
+        ord[p] = a < 3u ? L[a * m + p] : p;
     }
     __syncthreads();
-    for (uint32_t p = threadIdx.x; p < m; p += blockDim.x) ord[m + __ldcg(ord + p)] = p;
+    for (uint32_t p = threadIdx.x; p < m; p += blockDim.x) ord[m + ord[p]] = p;
     __syncthreads();
 }
 
