@@ -1050,10 +1050,23 @@ __device__ void edge_resolve(Ctx& ctx, bool swept, bool redo) {
     // order (edge_tree_order), else the first segments' order is all that
     // matters: pairs are sorted by (first, tree position of the second).
     bool mine = false;
-    for (uint32_t k = threadIdx.x; k < count && !mine; k += blockDim.x) {
-        const uint32_t first = static_cast<uint32_t>(__ldcg(d.edge_order + k) >> 32);
-        for (uint32_t m = 0; m < count && !mine; ++m)
-            mine = m != k && static_cast<uint32_t>(__ldcg(d.edge_order + m) >> 32) == first;
+    if (staged) {
+        // the first segments in shared memory (the staged key array, filled
+        // again below), compared there
+        uint32_t* s_first = reinterpret_cast<uint32_t*>(s_key);
+        for (uint32_t k = threadIdx.x; k < count; k += blockDim.x)
+            s_first[k] = static_cast<uint32_t>(__ldcg(d.edge_order + k) >> 32);
+        __syncthreads();
+        for (uint32_t k = threadIdx.x; k < count && !mine; k += blockDim.x) {
+            const uint32_t first = s_first[k];
+            for (uint32_t m = 0; m < count && !mine; ++m) mine = m != k && s_first[m] == first;
+        }
+    } else {
+        for (uint32_t k = threadIdx.x; k < count && !mine; k += blockDim.x) {
+            const uint32_t first = static_cast<uint32_t>(__ldcg(d.edge_order + k) >> 32);
+            for (uint32_t m = 0; m < count && !mine; ++m)
+                mine = m != k && static_cast<uint32_t>(__ldcg(d.edge_order + m) >> 32) == first;
+        }
     }
     const bool tree = __syncthreads_or(mine) != 0 && d.y_count <= NC_EDGE_TREE_MAX && ctx.s.tree_keys != 0u;
     if (tree) edge_tree_order(ctx, swept);
@@ -1062,6 +1075,7 @@ __device__ void edge_resolve(Ctx& ctx, bool swept, bool redo) {
         return tree ? ((key & 0xffffffff00000000ull) | __ldcg(tpos + static_cast<uint32_t>(key))) : key;
     };
     if (staged) {
+        __syncthreads();   // the first-segment comparisons are done with the scratch
         for (uint32_t k = threadIdx.x; k < count; k += blockDim.x) s_key[k] = sort_key(__ldcg(d.edge_order + k));
         __syncthreads();
         // rank sort: the keys are distinct
