@@ -868,7 +868,7 @@ int prepare_edge_grid(numi_cloth* h, bool primitive, uint32_t substeps, float ra
         e.edge_level = h->buf.alloc<uint32_t>(d.n);
         e.edge_qbox_raw = h->buf.alloc<float>(6u * d.y_count);
         e.edge_tree = h->buf.alloc<uint32_t>(static_cast<size_t>(NC_EDGE_TREE_WORDS) * d.y_count);
-        e.edge_centre = h->buf.alloc<float4>(d.y_count);
+        e.edge_centre = h->buf.alloc<float4>(2u * static_cast<size_t>(d.y_count));   // centres, last build's
         e.edge_rec = h->buf.alloc<EdgeRecord>(cap);
         e.edge_ctl = h->buf.alloc<uint32_t>(8);
         e.edge_stats = h->buf.alloc<unsigned long long>(2);

@@ -208,9 +208,11 @@ struct DeviceCloth {
     float4* edge_x0;              // [n]
     float4* edge_sph;             // [y_count] pass spheres (centre, radius)
     float* edge_qbox_raw;         // [6 * y_count] a first segment's tree-query box of the pass
-    uint32_t* edge_tree;          // [10 * y_count] the pass's box-tree leaf order: position -> segment,
-                                  //   then segment -> position, then the build's scratch (edge_tree_order)
-    float4* edge_centre;          // [y_count] centres of the pass-start boxes of the tree
+    uint32_t* edge_tree;          // [14 * y_count] the pass's box-tree leaf order: position -> segment,
+                                  //   then segment -> position, the build's scratch and the last
+                                  //   build's axis orders (edge_tree_order)
+    float4* edge_centre;          // [2 * y_count] centres of the pass-start boxes of the tree, then
+                                  //   those of the last build
     float* edge_path;             // [n]
     uint4* edge_cand;             // [edge_cap]
     unsigned long long* edge_order;    // [edge_cap]

@@ -743,9 +743,10 @@ __device__ void edge_candidates(Ctx& ctx, bool swept, bool rebuilt) {
 // three lists, the side of each segment, the parent axis of each position).
 #define NC_EDGE_TREE_MAX 4096u
 #define NC_EDGE_TREE_KEY_BYTES (NC_EDGE_TREE_MAX * 8u)
-#define NC_EDGE_TREE_WORDS 10u   /* edge_tree words per segment */
+#define NC_EDGE_TREE_WORDS 14u   /* edge_tree words per segment (13, and one flag word) */
+#define NC_EDGE_TREE_WARM 8u     /* odd-even passes tried on the previous order before a full sort */
 __shared__ unsigned char nc_edge_tree_axis[NC_EDGE_TREE_MAX / 8u];
-__shared__ uint32_t nc_edge_scan[32];
+__shared__ uint32_t nc_edge_scan[3][32];
 
 // The node of position p (or of index j, a path of `level` left/right bits)
 // at depth `level`; false past a leaf.
@@ -857,79 +858,126 @@ __device__ void block_sort(unsigned long long* keys, uint32_t n) {
     }
 }
 
-// Exclusive prefix sums of flags[0..m) (0 or 1) into out[0..m) (shared
-// memory), every thread a contiguous run.
-__device__ void block_prefix(const uint32_t* flags, uint32_t* out, uint32_t m) {
+// Exclusive prefix counts, for each of the three lists L[a][0..m), of the
+// members that go right (right[segment] = 1), into pre[a][0..m) (shared
+// memory; counts below 65,536): every thread a contiguous run of each list.
+__device__ void tree_prefix3(const uint32_t* L, const uint32_t* right, unsigned short* pre, uint32_t m) {
     const uint32_t per = (m + blockDim.x - 1u) / blockDim.x;
     const uint32_t lo = min(threadIdx.x * per, m), hi = min(lo + per, m);
-    uint32_t sum = 0u;
-    for (uint32_t p = lo; p < hi; ++p) sum += flags[p];
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    uint32_t incl = sum;
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= static_cast<uint32_t>(o)) incl += y;
+    uint32_t sum[3], incl[3];
+#pragma unroll
+    for (uint32_t a = 0; a < 3u; ++a) {
+        sum[a] = 0u;
+        for (uint32_t p = lo; p < hi; ++p) sum[a] += right[L[a * m + p]];
+        incl[a] = sum[a];
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl[a], o);
+            if (lane >= static_cast<uint32_t>(o)) incl[a] += y;
+        }
+        if (lane == 31u) nc_edge_scan[a][warp] = incl[a];
     }
-    if (lane == 31u) nc_edge_scan[warp] = incl;
     __syncthreads();
-    if (warp == 0u) {
+    if (warp < 3u) {
         const uint32_t warps = blockDim.x >> 5;
-        uint32_t w = lane < warps ? nc_edge_scan[lane] : 0u;
+        uint32_t w = lane < warps ? nc_edge_scan[warp][lane] : 0u;
         for (int o = 1; o < 32; o <<= 1) {
             const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
             if (lane >= static_cast<uint32_t>(o)) w += y;
         }
-        if (lane < warps) nc_edge_scan[lane] = w;
+        if (lane < warps) nc_edge_scan[warp][lane] = w;
     }
     __syncthreads();
-    uint32_t run = (warp > 0u ? nc_edge_scan[warp - 1u] : 0u) + incl - sum;
-    for (uint32_t p = lo; p < hi; ++p) {
-        out[p] = run;
-        run += flags[p];
+#pragma unroll
+    for (uint32_t a = 0; a < 3u; ++a) {
+        uint32_t run = (warp > 0u ? nc_edge_scan[a][warp - 1u] : 0u) + incl[a] - sum[a];
+        for (uint32_t p = lo; p < hi; ++p) {
+            pre[a * m + p] = static_cast<unsigned short>(run);
+            run += right[L[a * m + p]];
+        }
     }
     __syncthreads();
 }
 
 __device__ void edge_tree_order(const Ctx& ctx, bool swept) {
     const DeviceCloth& d = ctx.d;
-    // the sort keys and prefix sums, in the launch's dynamic shared memory
+    // the sort keys, then the prefix counts, in the launch's dynamic shared
+    // memory
     unsigned long long* keys = reinterpret_cast<unsigned long long*>(nc_frame_smem + ctx.s.tree_keys);
-    uint32_t* prefix = reinterpret_cast<uint32_t*>(keys);
+    unsigned short* pre = reinterpret_cast<unsigned short*>(keys);
     const uint32_t m = d.y_count;
     const float ex = 0.5f * (2.0f * ctx.c.radius);
     uint32_t* ord = d.edge_tree;
     uint32_t* lists = d.edge_tree + 2u * m;   // [2][3][m]
     uint32_t* right = lists + 6u * m;         // per segment: goes to the right child
     uint32_t* leaf_axis = right + m;          // per position: axis of its deepest split
+    uint32_t* gsort = leaf_axis + m;          // [3][m] the last build's order along each axis
+    uint32_t* valid = gsort + 3u * m;         // 1 once a tree was built
+    float4* prev = d.edge_centre + m;         // the last build's centres
     // Every array here is written and read by this CTA alone between CTA
     // barriers, which make the writes visible to its threads: plain loads,
     // served from L1.
+    const bool warm = *valid != 0u;
+    bool changed = !warm;
     for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
         const uint2 ab = __ldg(d.y_ij + k);
         const EdgeBox bx = edge_box(xyz(ld(d.edge_x0 + ab.x)), xyz(ld(d.edge_x0 + ab.y)), xyz(ld(d.xp + ab.x)),
                                     xyz(ld(d.xp + ab.y)), swept, ex);
-        d.edge_centre[k] = make_float4(0.5f * (bx.lo.x + bx.hi.x), 0.5f * (bx.lo.y + bx.hi.y),
-                                       0.5f * (bx.lo.z + bx.hi.z), 0.0f);
+        const float4 c = make_float4(0.5f * (bx.lo.x + bx.hi.x), 0.5f * (bx.lo.y + bx.hi.y),
+                                     0.5f * (bx.lo.z + bx.hi.z), 0.0f);
+        d.edge_centre[k] = c;
+        if (warm) {
+            const float4 q = prev[k];
+            changed = changed || __float_as_uint(c.x) != __float_as_uint(q.x) ||
+                      __float_as_uint(c.y) != __float_as_uint(q.y) || __float_as_uint(c.z) != __float_as_uint(q.z);
+        }
         leaf_axis[k] = 3u;
     }
+    // the same centres as the last build: the same tree
+    if (!__syncthreads_or(changed)) return;
     uint32_t size = blockDim.x;
     while (size < m) size <<= 1;
-    __syncthreads();
-    // the three axis lists: (centre, index) order
+    // the three axis lists, (centre, index) order: from the last build's
+    // order, a few odd-even transposition passes while it is not sorted
+    // (the centres move little from pass to pass), else a full sort
     for (uint32_t a = 0; a < 3u; ++a) {
         for (uint32_t p = threadIdx.x; p < size; p += blockDim.x) {
             unsigned long long key = ~0ull;
             if (p < m) {
-                const float4 c = d.edge_centre[p];
+                const uint32_t sg = warm ? gsort[a * m + p] : p;
+                const float4 c = d.edge_centre[sg];
                 const float v = a == 0u ? c.x : (a == 1u ? c.y : c.z);
-                key = (static_cast<unsigned long long>(ordered_bits(v)) << 12) | p;
+                key = (static_cast<unsigned long long>(ordered_bits(v)) << 12) | sg;
             }
             keys[p] = key;
         }
         __syncthreads();
-        block_sort(keys, size);
-        for (uint32_t p = threadIdx.x; p < m; p += blockDim.x)
-            lists[a * m + p] = static_cast<uint32_t>(keys[p] & 0xfffull);
+        bool sorted = false;
+        for (uint32_t t = 0; warm && t <= NC_EDGE_TREE_WARM; ++t) {
+            bool out = false;
+            for (uint32_t p = threadIdx.x; p + 1u < m; p += blockDim.x) out = out || keys[p] > keys[p + 1u];
+            if (!__syncthreads_or(out)) {
+                sorted = true;
+                break;
+            }
+            if (t == NC_EDGE_TREE_WARM) break;
+            for (uint32_t phase = 0; phase < 2u; ++phase) {
+                for (uint32_t p = 2u * threadIdx.x + phase; p + 1u < m; p += 2u * blockDim.x) {
+                    const unsigned long long x = keys[p], y = keys[p + 1u];
+                    if (x > y) {
+                        keys[p] = y;
+                        keys[p + 1u] = x;
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        if (!sorted) block_sort(keys, size);
+        for (uint32_t p = threadIdx.x; p < m; p += blockDim.x) {
+            const uint32_t sg = static_cast<uint32_t>(keys[p] & 0xfffull);
+            lists[a * m + p] = sg;
+            gsort[a * m + p] = sg;
+        }
         __syncthreads();
     }
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u, warps = blockDim.x >> 5;
@@ -978,32 +1026,31 @@ __device__ void edge_tree_order(const Ctx& ctx, bool swept) {
         }
         __syncthreads();
         // every list: stable partition of each splitting node's range
-        for (uint32_t a = 0; a < 3u; ++a) {
-            for (uint32_t p = threadIdx.x; p < m; p += blockDim.x) prefix[m + p] = right[L[a * m + p]];
-            __syncthreads();
-            block_prefix(prefix + m, prefix, m);
-            for (uint32_t p = threadIdx.x; p < m; p += blockDim.x) {
-                uint32_t b, e;
-                tree_path_of_position(m, level, p, b, e);
-                const uint32_t s = L[a * m + p];
-                uint32_t to = p;
-                if (e - b > 8u) {
-                    const uint32_t rights = prefix[p] - prefix[b];
-                    to = prefix[m + p] != 0u ? b + (e - b) / 2u + rights : p - rights;
-                }
-                N[a * m + to] = s;
+        tree_prefix3(L, right, pre, m);
+        for (uint32_t q = threadIdx.x; q < 3u * m; q += blockDim.x) {
+            const uint32_t a = q / m, p = q - a * m;
+            uint32_t b, e;
+            tree_path_of_position(m, level, p, b, e);
+            const uint32_t sg = L[q];
+            uint32_t to = p;
+            if (e - b > 8u) {
+                const uint32_t rights = static_cast<uint32_t>(pre[q]) - static_cast<uint32_t>(pre[a * m + b]);
+                to = right[sg] != 0u ? b + (e - b) / 2u + rights : p - rights;
             }
-            __syncthreads();
+            N[a * m + to] = sg;
         }
+        __syncthreads();
         cur ^= 1u;
     }
     const uint32_t* L = lists + cur * 3u * m;
     for (uint32_t p = threadIdx.x; p < m; p += blockDim.x) {
         const uint32_t a = leaf_axis[p];
         ord[p] = a < 3u ? L[a * m + p] : p;
+        prev[p] = d.edge_centre[p];
     }
     __syncthreads();
     for (uint32_t p = threadIdx.x; p < m; p += blockDim.x) ord[m + ord[p]] = p;
+    if (threadIdx.x == 0) *valid = 1u;
     __syncthreads();
 }
 
