@@ -254,6 +254,19 @@ int numi_cloth_edge_contacts(numi_cloth_t* handle, unsigned long long out[2]);
  * every substep of a step whose schedule has release = 1. */
 int numi_cloth_release_masks(numi_cloth_t* handle, uint32_t out[2]);
 
+/* Launch-shape tuner of one cloth on the cooperative grid: times `count`
+ * substeps of `configs` under `schedule` for each colours-per-sync choice
+ * the cloth and schedule allow (one constraint colour between
+ * synchronisations, the colour-by-colour launch; or tile mode, whose CTAs
+ * run every constraint colour of a substep on their closures between two
+ * grid barriers, at the SM count, three quarters and half of it, in CTAs),
+ * keeps the fastest, and leaves the cloth's state as it was.  out: [0]
+ * constraint colours per synchronisation of the kept shape, [1] CTAs, [2]
+ * threads per CTA, [3] its time for the configs in us (0: nothing to
+ * choose).  ESTATE on a cloth whose failure word is set. */
+int numi_cloth_tune(numi_cloth_t* handle, const NumiClothConfig* configs, uint32_t count,
+                    const NumiClothSchedule* schedule, uint32_t out[4]);
+
 /* Device-side snapshot of the full dynamic state into slot (0..7), and back. */
 int numi_cloth_snapshot(numi_cloth_t* handle, uint32_t slot);
 int numi_cloth_restore(numi_cloth_t* handle, uint32_t slot);

@@ -49,6 +49,7 @@ __global__ void __launch_bounds__(NC_THREADS) numi_cloth_residual_kernel(DeviceC
 namespace {
 
 constexpr uint32_t kSnapshotSlots = 8;
+constexpr uint32_t kTuneSlot = kSnapshotSlots;   // snapshot slot of the launch-shape tuners
 constexpr uint32_t kResidentChunk = 4096;   // particles a CTA holds in resident mode
 constexpr uint32_t kResidentClusterChunk = 256;   // default chunk of a small resident cloth
 constexpr uint32_t kBarrierWords = 48;   // barrier counter, abort, release and fruit flags: three 128-byte lines
@@ -117,7 +118,7 @@ struct numi_cloth {
     // host copies for the edge/edge local lists, built with the edge buffers
     std::vector<uint2> host_yarn;
     std::vector<uint32_t> host_local_off, host_local_idx;
-    Snapshot snaps[kSnapshotSlots];
+    Snapshot snaps[kSnapshotSlots + 1u];   // the callers' slots, then the tuners' own
     // dynamic state regions copied by snapshot/restore
     struct Region {
         void* ptr;
@@ -1550,8 +1551,25 @@ int numi_cloth_release_masks(numi_cloth_t* h, uint32_t out[2]) {
     return NUMI_CLOTH_OK;
 }
 
+namespace {
+int snapshot_slot(numi_cloth_t* h, uint32_t slot);
+int restore_slot(numi_cloth_t* h, uint32_t slot);
+}  // namespace
+
 int numi_cloth_snapshot(numi_cloth_t* h, uint32_t slot) {
     if (h == nullptr || slot >= kSnapshotSlots) return NUMI_CLOTH_EINVAL;
+    return snapshot_slot(h, slot);
+}
+
+int numi_cloth_restore(numi_cloth_t* h, uint32_t slot) {
+    if (h == nullptr || slot >= kSnapshotSlots || !h->snaps[slot].valid) return NUMI_CLOTH_EINVAL;
+    return restore_slot(h, slot);
+}
+
+}  // extern "C"
+
+namespace {
+int snapshot_slot(numi_cloth_t* h, uint32_t slot) {
     cudaSetDevice(h->device);
     size_t total = 0;
     for (const auto& r : h->dynamic) total += (r.bytes + 255u) & ~size_t(255u);
@@ -1571,8 +1589,7 @@ int numi_cloth_snapshot(numi_cloth_t* h, uint32_t slot) {
     return NUMI_CLOTH_OK;
 }
 
-int numi_cloth_restore(numi_cloth_t* h, uint32_t slot) {
-    if (h == nullptr || slot >= kSnapshotSlots || !h->snaps[slot].valid) return NUMI_CLOTH_EINVAL;
+int restore_slot(numi_cloth_t* h, uint32_t slot) {
     cudaSetDevice(h->device);
     size_t off = 0;
     for (const auto& r : h->dynamic) {
@@ -1583,6 +1600,9 @@ int numi_cloth_restore(numi_cloth_t* h, uint32_t slot) {
     }
     return NUMI_CLOTH_OK;
 }
+}  // namespace
+
+extern "C" {
 
 int numi_cloth_trace(numi_cloth_t* h, unsigned long long* out, uint32_t substeps, uint32_t slots) {
     if (h == nullptr || out == nullptr || slots != NC_TRACE_SLOTS) return NUMI_CLOTH_EINVAL;
@@ -1622,6 +1642,130 @@ int numi_cloth_pass_counts(numi_cloth_t* h, uint32_t out[3]) {
     out[2] = stats[2];
     return NUMI_CLOTH_OK;
 }
+
+}  // extern "C"
+
+namespace {
+
+// Tile plans for a tile launch of `grid` CTAs, and whether the device holds
+// that grid co-resident with their shared memory.
+bool configure_tiles(numi_cloth* h, uint32_t grid) {
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+    h->tile_grid = grid;
+    h->tiles = rebuild_tiles(h);
+    h->tiles_dirty = false;
+    if (h->tiles) {
+        int k = 0;
+        h->tiles = raise_frame_smem(h->tile_smem) == cudaSuccess &&
+                   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, frame_fn(false), NC_BLOCK_MAX, h->tile_smem) ==
+                       cudaSuccess &&
+                   static_cast<uint64_t>(k) * static_cast<uint64_t>(sms) >= h->tile_grid;
+    }
+    cudaGetLastError();
+    return h->tiles;
+}
+
+}  // namespace
+
+extern "C" int numi_cloth_tune(numi_cloth_t* h, const NumiClothConfig* configs, uint32_t count,
+                               const NumiClothSchedule* schedule, uint32_t out[4]) {
+    if (h == nullptr || configs == nullptr || schedule == nullptr || count == 0 || out == nullptr)
+        return NUMI_CLOTH_EINVAL;
+    if (h->poisoned) return NUMI_CLOTH_ESTATE;
+    cudaSetDevice(h->device);
+    if (numi_cloth_failure(h) != 0u) return NUMI_CLOTH_ESTATE;   // a failed cloth is not timed
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+    const Schedule sched = device_schedule(*schedule);
+    const uint32_t colours = h->d.n_dist_batches + h->d.n_bend_batches;
+    // the candidates: one colour per synchronisation (the colour-by-colour
+    // launch), and tile mode at three CTA counts
+    struct Shape {
+        bool tiles;
+        uint32_t grid;
+    };
+    std::vector<Shape> shapes;
+    const bool had_tiles = h->tiles;
+    const uint32_t had_grid = h->tile_grid;
+    const bool tile_capable = h->tile_block != 0u && h->grid > 1u && h->cluster == 0u && h->d.resident == 0u;
+    if (h->grid > 1u) shapes.push_back({false, h->grid});
+    if (tile_capable) {
+        h->tiles = true;   // tile_schedule asks only whether the schedule is covered
+        const bool covered = tile_schedule(h, sched);
+        h->tiles = had_tiles;
+        if (covered)
+            for (uint32_t g : {static_cast<uint32_t>(sms), static_cast<uint32_t>(3 * sms / 4), static_cast<uint32_t>(sms / 2)})
+                shapes.push_back({true, std::max(g, 3u)});
+    }
+    auto report = [&](float us) {
+        out[0] = h->tiles ? colours : 1u;
+        out[1] = h->tiles ? h->tile_grid : h->grid;
+        out[2] = h->tiles ? h->tile_block : h->block;
+        out[3] = static_cast<uint32_t>(us);
+    };
+    if (shapes.size() < 2u) {
+        report(0.0f);
+        return NUMI_CLOTH_OK;
+    }
+    int rc = snapshot_slot(h, kTuneSlot);
+    if (rc != NUMI_CLOTH_OK) return rc;
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    float best_ms = INFINITY;
+    size_t best = shapes.size();
+    for (size_t k = 0; k < shapes.size() && rc == NUMI_CLOTH_OK; ++k) {
+        if (shapes[k].tiles) {
+            if (!configure_tiles(h, shapes[k].grid)) continue;
+        } else {
+            h->tiles = false;
+        }
+        float ms = 0.0f;
+        for (int rep = 0; rep < 2 && rc == NUMI_CLOTH_OK; ++rep) {   // a warm-up run, then the timed one
+            rc = restore_slot(h, kTuneSlot);
+            if (rc == NUMI_CLOTH_OK) cudaEventRecord(t0, h->stream);
+            if (rc == NUMI_CLOTH_OK) rc = numi_cloth_step(h, configs, count, schedule);
+            if (rc == NUMI_CLOTH_OK) {
+                cudaEventRecord(t1, h->stream);
+                if (cudaEventSynchronize(t1) != cudaSuccess) rc = NUMI_CLOTH_ECUDA;
+            }
+        }
+        if (rc != NUMI_CLOTH_OK) break;
+        cudaEventElapsedTime(&ms, t0, t1);
+        if (numi_cloth_failure(h) != 0u || h->host_failure != 0u) {
+            // this shape failed (the caller's state comes back below)
+            cudaMemsetAsync(h->d.failure, 0, sizeof(uint32_t), h->stream);
+            h->host_failure = 0u;
+            continue;
+        }
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = k;
+        }
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    // keep the fastest shape (else the one the cloth had) and its state
+    if (best < shapes.size() && shapes[best].tiles) {
+        if (!configure_tiles(h, shapes[best].grid)) best = shapes.size();
+    } else if (best < shapes.size()) {
+        h->tiles = false;
+    }
+    if (best == shapes.size()) {
+        if (had_tiles)
+            configure_tiles(h, had_grid);
+        else
+            h->tiles = false;
+    }
+    const int rrc = restore_slot(h, kTuneSlot);
+    if (rc == NUMI_CLOTH_OK) rc = rrc;
+    if (rc == NUMI_CLOTH_OK && cudaStreamSynchronize(h->stream) != cudaSuccess) rc = NUMI_CLOTH_ECUDA;
+    report(best < shapes.size() ? 1000.0f * best_ms : 0.0f);
+    return rc;
+}
+
+extern "C" {
 
 int numi_cloth_launch_info(numi_cloth_t* h, uint32_t out[6]) {
     if (h == nullptr || out == nullptr) return NUMI_CLOTH_EINVAL;
@@ -2132,9 +2276,9 @@ int numi_cloth_batch_tune(numi_cloth_batch_t* b, const NumiClothConfig* configs,
     batch_drop_graph(b);
     uint32_t largest = 0;
     for (numi_cloth* h : b->cloths) largest = std::max(largest, h->d.n);
-    const uint32_t slot = kSnapshotSlots - 1u;
+    const uint32_t slot = kTuneSlot;
     for (numi_cloth* h : b->cloths) {
-        const int rc = numi_cloth_snapshot(h, slot);
+        const int rc = snapshot_slot(h, slot);
         if (rc != NUMI_CLOTH_OK) return rc;
         if (h->stream && cudaStreamSynchronize(h->stream) != cudaSuccess) return NUMI_CLOTH_ECUDA;
     }
@@ -2170,7 +2314,7 @@ int numi_cloth_batch_tune(numi_cloth_batch_t* b, const NumiClothConfig* configs,
                 best_chunk = chunk;
                 best_block = block;
             }
-            for (numi_cloth* h : b->cloths) numi_cloth_restore(h, slot);
+            for (numi_cloth* h : b->cloths) restore_slot(h, slot);
             if (cudaDeviceSynchronize() != cudaSuccess) {
                 rc = NUMI_CLOTH_ECUDA;
                 break;

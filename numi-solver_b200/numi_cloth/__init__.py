@@ -91,6 +91,7 @@ def load_library() -> ctypes.CDLL:
         "numi_cloth_snapshot": (i32, [vp, u32]),
         "numi_cloth_restore": (i32, [vp, u32]),
         "numi_cloth_launch_info": (i32, [vp, ctypes.POINTER(u32)]),
+        "numi_cloth_tune": (i32, [vp, vp, u32, vp, ctypes.POINTER(u32)]),
         "numi_cloth_self_contacts": (i32, [vp, ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(ctypes.c_double)]),
         "numi_cloth_edge_contacts": (i32, [vp, ctypes.POINTER(ctypes.c_ulonglong)]),
         "numi_cloth_set_damping": (i32, [vp, ctypes.c_float]),
@@ -602,6 +603,15 @@ class ClothSolver:
         out = (ctypes.c_ulonglong * 2)()
         self._check(self.lib.numi_cloth_edge_contacts(self._h, out))
         return int(out[0]), int(out[1])
+
+    def tune(self, configs: np.ndarray, schedule: Schedule) -> dict:
+        """numi_cloth_tune: time the colours-per-sync choices (the
+        colour-by-colour launch, tile mode at three CTA counts) on these
+        substeps, keep the fastest; the state is left as it was."""
+        configs = np.ascontiguousarray(configs, CONFIG)
+        out = (ctypes.c_uint32 * 4)()
+        self._check(self.lib.numi_cloth_tune(self._h, configs.ctypes.data, len(configs), ctypes.byref(schedule), out))
+        return {"colours_per_sync": out[0], "ctas": out[1], "threads": out[2], "us": out[3]}
 
     def launch_info(self) -> dict:
         out = (ctypes.c_uint32 * 6)()

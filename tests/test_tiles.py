@@ -128,3 +128,27 @@ def test_non_tile_schedule_on_tiled_cloth():
     assert not outs[0][1]["last_tiles"] and outs[0][2]["last_tiles"]
     assert outs[0][3] == 0 and outs[1][3] == 0
     assert np.array_equal(outs[0][0].view(np.uint8), outs[1][0].view(np.uint8))
+
+
+def test_tune_keeps_state_and_bits():
+    """numi_cloth_tune times the colour-by-colour launch and tile mode at
+    three CTA counts, keeps the fastest and leaves the state as it was: a
+    tuned handle steps to the same bits as an untuned one."""
+    scene = small_square(side=96, fruits=6)
+    cfg = nc.substep_configs(scene, 12)
+    s = nc.Schedule.make(**BENCH_LIKE)
+    tuned = make_solver(scene)
+    before = tuned.particles()
+    r = tuned.tune(cfg, s)
+    print("tune:", r)
+    assert np.array_equal(tuned.particles().view(np.uint8), before.view(np.uint8))
+    assert tuned.failure() == 0
+    colours = r["colours_per_sync"]
+    assert colours == 1 or colours > 1 and r["threads"] == 512
+    tuned.step(cfg, s)
+    plain = make_solver(scene)
+    plain.step(cfg, s)
+    assert np.array_equal(tuned.particles().view(np.uint8), plain.particles().view(np.uint8))
+    assert tuned.launch_info()["last_tiles"] == (colours > 1)
+    tuned.close()
+    plain.close()
