@@ -630,6 +630,9 @@ def run_ours(args):
     solver.set_stream(stream.cuda_stream)
     cfg = nc.substep_configs(scene, SUBSTEPS)
     sched = nc.Schedule.make(**BENCH_SCHEDULE)
+    # launch shape from the tuner: colours per synchronisation (1, or every
+    # constraint colour in tile mode) and CTAs; the state is left as it was
+    tuned = solver.tune(cfg, sched)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
     def barrier():
@@ -747,7 +750,9 @@ def run_ours(args):
                        "grid": info["grid"], "block": info["block"],
                        "barriers_per_substep": info["barriers_per_substep"], "cluster": info["cluster"],
                        "particles_resident_in_smem": info["resident"],
-                       "neighbour_syncs": info["neighbour_syncs"]},
+                       "neighbour_syncs": info["neighbour_syncs"], "tiles": info["last_tiles"],
+                       "tuned": {"colours_per_sync": tuned["colours_per_sync"], "ctas": tuned["ctas"],
+                                 "threads": tuned["threads"]}},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                          "peak_source": peaks["source"], "algorithmic_bytes_per_substep": ab},
