@@ -1300,6 +1300,11 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
         cudaFuncGetAttributes(&fa, frame_fn(false));
         uint32_t tgrid = static_cast<uint32_t>(sms);
         env_u32("NUMI_CLOTH_TILE_GRID", tgrid);
+        // NUMI_CLOTH_TILE_SPLIT=0 resolves self contact inside the strain
+        // closures (no extra barrier, every closure repeats its ghosts'
+        // queries); the default has the owners resolve it first
+        d.tile_split_self = 1u;
+        env_u32("NUMI_CLOTH_TILE_SPLIT", d.tile_split_self);
         h->tile_grid = std::max(tgrid, 3u);
         h->tile_block = NC_BLOCK_MAX;
         h->tiles = build_tiles(h, scene->gridWidth, hij, hdm, hbij, hbm,

@@ -118,6 +118,7 @@ struct DeviceCloth {
     unsigned long long* bar_count;
     unsigned long long* bar_flag;   // barrier number released last (own 128-byte line)
     unsigned long long* fruit_flag; // tile mode: substeps whose fruit-CTA tail is done (own line)
+    uint32_t tile_split_self;       // tile mode: owners resolve self contact before the strain chains
     unsigned int* abort_flag;
     // polls a barrier or neighbour wait makes before it gives up (0: the
     // default NC_BARRIER_SPIN_LIMIT)

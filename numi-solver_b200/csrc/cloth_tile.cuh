@@ -88,6 +88,14 @@ __device__ __forceinline__ void tile_load(const Ctx& ctx, uint32_t chain) {
     __syncthreads();
 }
 
+// The owned particles (the list's first) from the current position buffer.
+__device__ __forceinline__ void tile_load_owned(const Ctx& ctx) {
+    const uint32_t own = ctx.tp[1];
+    const uint32_t* gi = tile_list(ctx);
+    for (uint32_t l = threadIdx.x; l < own; l += blockDim.x) ctx.tx[l] = __ldcg(ctx.gx + gi[l]);
+    __syncthreads();
+}
+
 // Owned particles to the other position buffer.
 __device__ __forceinline__ void tile_store(const Ctx& ctx, float4* out) {
     const uint32_t own = ctx.tp[1];
@@ -242,12 +250,11 @@ __device__ __forceinline__ void tile_insert(const Ctx& ctx) {
     for (uint32_t l = threadIdx.x; l < own; l += blockDim.x) self_insert_one(ctx, tag, gi[l], ctx.tx[l]);
 }
 
-// Self-contact solve and ground clamp of the strain chain's particles
-// (each a function of its start-of-pass position and the grid), counted
-// for the owned ones.
-__device__ void tile_self_ground(const Ctx& ctx, bool self) {
+// Self-contact solve and ground clamp of the first nl local particles (the
+// strain chain's closure, or the owned ones; each a function of its
+// start-of-pass position and the grid), counted for the owned ones.
+__device__ void tile_self_ground(const Ctx& ctx, bool self, uint32_t nl) {
     const SubCfg& c = ctx.c;
-    const uint32_t nl = ctx.tp[4u + NC_TILE_STRAIN];
     const uint32_t own = ctx.tp[1];
     const uint32_t* gi = tile_list(ctx);
     const uint32_t tag = self_pass_tag(ctx, 0u);
@@ -453,12 +460,35 @@ __device__ bool substep_tiles(Ctx& ctx, bool last) {
         ctx.hold_tail = last || attach || listed > NC_FRICTION_STAGE;
         if (!ctx.hold_tail && listed > 0u && !ctx.fruit_cta) ctx.fruit_wait = tile_touches_listed(ctx, listed);
     }
+    // With split self contact the owners first resolve their own particles'
+    // self contact and ground clamp and publish them (one more grid
+    // barrier), so each query runs once instead of in every closure that
+    // holds the particle; the strain chains then load resolved positions.
+    const bool split = self && d.tile_split_self != 0u;
+    if (split) {
+        float4* x_next = other_x(ctx);
+        if (ctx.fruit_cta) {
+            fruit_flush(ctx);
+            if (ctx.c.ground) fruit_ground(ctx);
+            fruit_finalize(ctx);
+            if (s.frictions && fruits) friction_stage(ctx);
+        } else {
+            tile_mark(ctx, 9u);
+            tile_load_owned(ctx);
+            tile_mark(ctx, 10u);
+            tile_self_ground(ctx, true, ctx.tp[1]);
+            tile_mark(ctx, 11u);
+            tile_store(ctx, x_next);
+        }
+        ctx.gx = x_next;
+        NC_SYNC(ctx);
+    }
     const uint32_t sweeps = max(s.strain_sweeps, 1u);
     for (uint32_t sw = 0; sw < sweeps; ++sw) {
         float4* x_next = other_x(ctx);
         const bool final_sweep = sw + 1u == sweeps;
         if (ctx.fruit_cta) {
-            if (sw == 0u) {
+            if (sw == 0u && !split) {
                 fruit_flush(ctx);
                 if (ctx.c.ground) fruit_ground(ctx);
                 fruit_finalize(ctx);
@@ -467,10 +497,10 @@ __device__ bool substep_tiles(Ctx& ctx, bool last) {
                 if (s.frictions && fruits) friction_stage(ctx);
             }
         } else {
-            tile_mark(ctx, 9u);
+            if (!split) tile_mark(ctx, 9u);
             tile_load(ctx, NC_TILE_STRAIN);
-            tile_mark(ctx, 10u);
-            if (sw == 0u) tile_self_ground(ctx, self);
+            if (!split) tile_mark(ctx, 10u);
+            if (sw == 0u && !split) tile_self_ground(ctx, self, ctx.tp[4u + NC_TILE_STRAIN]);
             tile_mark(ctx, 11u);
             if (s.strain_sweeps > 0u) tile_chain(ctx, NC_TILE_STRAIN, dt2);
             tile_mark(ctx, 12u);

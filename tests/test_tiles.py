@@ -37,11 +37,18 @@ def _same(a, b):
     assert a["self_contacts"] == b["self_contacts"]
 
 
-@pytest.mark.parametrize("variant", ["bench", "sweeps2-damped", "no-self", "no-strain", "no-fruits",
-                                     "many-fruits"])
+@pytest.mark.parametrize("variant", ["bench", "bench-unsplit", "sweeps2-damped", "sweeps2-unsplit", "no-self",
+                                     "no-strain", "no-fruits", "many-fruits"])
 def test_tiles_equal_colour_schedule_and_oracle(variant):
+    """Tile mode against the colour-by-colour launch and the oracle; the
+    -unsplit variants resolve self contact inside the strain closures
+    (NUMI_CLOTH_TILE_SPLIT=0) instead of by the owners first."""
     sched = dict(BENCH_LIKE)
     kw = dict(side=96, fruits=12)
+    env = dict(TILES, NUMI_CLOTH_TILE_SPLIT="0") if variant.endswith("-unsplit") else TILES
+    variant = variant.replace("-unsplit", "")
+    if variant == "sweeps2":
+        variant = "sweeps2-damped"
     if variant == "sweeps2-damped":
         sched.update(strainSweeps=2, damping=0.3)
     elif variant == "no-self":
@@ -55,7 +62,8 @@ def test_tiles_equal_colour_schedule_and_oracle(variant):
     scene = small_square(**kw)
     cfg = nc.substep_configs(scene, 24)
     s = nc.Schedule.make(**sched)
-    tiled, plain = _both(scene, cfg, s)
+    tiled = run_gpu(scene, cfg, s, env=env)
+    plain = run_gpu(scene, cfg, s, env=COLOURS)
     assert tiled["info"]["last_tiles"], tiled["info"]
     assert not plain["info"]["last_tiles"]
     assert tiled["failure"] == 0 and plain["failure"] == 0, nc.failure_names(tiled["failure"] | plain["failure"])
