@@ -241,6 +241,14 @@ int numi_cloth_residuals(numi_cloth_t* handle, double out[4]);
  * step ran with selfCollision. */
 int numi_cloth_self_contacts(numi_cloth_t* handle, unsigned long long* contacts, double* max_penetration);
 
+/* How the point self-contact passes since create kept the reference's
+ * Gauss-Seidel order: out[0] passes whose phase A listed coupled pairs (the
+ * ordered pass ran), out[1] pairs listed over those passes, out[2]
+ * ordered-pass rounds, out[3] passes resolved by the serial fallback.  No
+ * counterpart in the reference, whose pass is serial.  Zero until a step ran
+ * with selfCollision. */
+int numi_cloth_self_order_stats(numi_cloth_t* handle, unsigned long long out[4]);
+
 /* Edge/edge yarn self-collision counters since create: out[0] edge/edge
  * solves that moved particles (the reference's edgeEdgeSelfContacts plus
  * sweptEdgeEdgeSelfContacts), out[1] yarn/yarn self-friction contacts
@@ -277,7 +285,9 @@ int numi_cloth_restore(numi_cloth_t* handle, uint32_t slot);
  * bit 1 when constraint colours are separated by neighbour syncs instead of
  * the grid barrier, bit 2 when the cloth has tile plans (colour chains run
  * on per-CTA closures in shared memory between grid barriers), bit 3 when
- * the last step ran in that tile mode. */
+ * the last step ran in that tile mode, bit 4 when point self contact keeps
+ * the reference's Gauss-Seidel order (NUMI_CLOTH_SELF_ORDER=reference at
+ * create; else the batched order). */
 int numi_cloth_launch_info(numi_cloth_t* handle, uint32_t out[6]);
 
 /* Pass counters: out[0] barriers of the last substep, out[1] the most

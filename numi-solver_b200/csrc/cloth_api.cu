@@ -96,6 +96,7 @@ struct numi_cloth {
     uint32_t epoch = 1;
     uint32_t host_failure = 0;
     bool poisoned = false;
+    bool self_exact = false;   // point self contact in the reference's order (NUMI_CLOTH_SELF_ORDER=reference)
     uint32_t grid = 1;
     uint32_t block = NC_THREADS;
     uint32_t cluster = 0;   // > 0: the grid is one cluster of this many CTAs
@@ -137,7 +138,12 @@ namespace {
 // ever raise it, so that creating one cloth never breaks another's launch.
 // The frame and batch kernels come in two builds: without and with the
 // edge/edge yarn self-collision phases (primitiveSelf).
-const void* frame_fn(bool edge) {
+// A third pair resolves point self contact in the reference's Gauss-Seidel
+// order (NUMI_CLOTH_SELF_ORDER=reference at create).
+const void* frame_fn(bool edge, bool exact = false) {
+    if (exact)
+        return edge ? reinterpret_cast<const void*>(numi_cloth_frame_edge_exact_kernel)
+                    : reinterpret_cast<const void*>(numi_cloth_frame_exact_kernel);
     return edge ? reinterpret_cast<const void*>(numi_cloth_frame_edge_kernel)
                 : reinterpret_cast<const void*>(numi_cloth_frame_kernel);
 }
@@ -154,21 +160,26 @@ cudaError_t raise_smem(const void* fn, size_t bytes) {
     return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
 }
 cudaError_t raise_frame_smem(size_t bytes) {
-    cudaError_t e = raise_smem(frame_fn(false), bytes);
-    return e == cudaSuccess ? raise_smem(frame_fn(true), bytes) : e;
+    cudaError_t e = cudaSuccess;
+    for (bool exact : {false, true})
+        for (bool edge : {false, true})
+            if (e == cudaSuccess) e = raise_smem(frame_fn(edge, exact), bytes);
+    return e;
 }
 void allow_large_clusters() {
-    for (bool edge : {false, true})
-        cudaFuncSetAttribute(frame_fn(edge), cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    for (bool exact : {false, true})
+        for (bool edge : {false, true})
+            cudaFuncSetAttribute(frame_fn(edge, exact), cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
 }
-// Clusters of cfg's shape that both frame kernels can place at once.
+// Clusters of cfg's shape that every frame kernel can place at once.
 int frame_clusters(const cudaLaunchConfig_t& cfg) {
     int lo = 1 << 30;
-    for (bool edge : {false, true}) {
-        int clusters = 0;
-        if (cudaOccupancyMaxActiveClusters(&clusters, frame_fn(edge), &cfg) != cudaSuccess) return 0;
-        lo = std::min(lo, clusters);
-    }
+    for (bool exact : {false, true})
+        for (bool edge : {false, true}) {
+            int clusters = 0;
+            if (cudaOccupancyMaxActiveClusters(&clusters, frame_fn(edge, exact), &cfg) != cudaSuccess) return 0;
+            lo = std::min(lo, clusters);
+        }
     return lo;
 }
 
@@ -665,9 +676,9 @@ cudaError_t launch(numi_cloth* h, uint32_t substeps, const Schedule& s, uint32_t
         cfg.attrs = &attr;
         cfg.numAttrs = 1;
         d.cluster_barrier = 1u;
-        e = cudaLaunchKernelExC(&cfg, frame_fn(edge), args);
+        e = cudaLaunchKernelExC(&cfg, frame_fn(edge, h->self_exact), args);
     } else if (h->grid == 1) {
-        e = cudaLaunchKernel(frame_fn(edge), dim3(1), dim3(h->block), args, smem, h->stream);
+        e = cudaLaunchKernel(frame_fn(edge, h->self_exact), dim3(1), dim3(h->block), args, smem, h->stream);
     } else if (tile_schedule(h, sc)) {
         if (h->tiles_dirty) {
             if (!rebuild_tiles(h)) return cudaErrorUnknown;
@@ -678,7 +689,7 @@ cudaError_t launch(numi_cloth* h, uint32_t substeps, const Schedule& s, uint32_t
         if (h->tile_grid > h->grid) d.trace_cta = nullptr;
         e = raise_frame_smem(h->tile_smem);
         if (e == cudaSuccess)
-            e = cudaLaunchCooperativeKernel(frame_fn(false), dim3(h->tile_grid), dim3(h->tile_block), args,
+            e = cudaLaunchCooperativeKernel(frame_fn(false, h->self_exact), dim3(h->tile_grid), dim3(h->tile_block), args,
                                             h->tile_smem, h->stream);
         h->last_grid = h->tile_grid;
         h->last_block = h->tile_block;
@@ -693,7 +704,7 @@ cudaError_t launch(numi_cloth* h, uint32_t substeps, const Schedule& s, uint32_t
             e = cudaMemsetAsync(d.nbr_flag, 0, NC_NBR_FLAG_STRIDE * h->grid * sizeof(unsigned int), h->stream);
             if (e != cudaSuccess) return e;
         }
-        e = cudaLaunchCooperativeKernel(frame_fn(edge), dim3(h->grid), dim3(h->block), args,
+        e = cudaLaunchCooperativeKernel(frame_fn(edge, h->self_exact), dim3(h->grid), dim3(h->block), args,
                                         d.nbr_on ? h->nbr_smem : smem, h->stream);
     }
     h->last_grid = h->cluster > 0 ? h->cluster : h->grid;
@@ -734,18 +745,43 @@ int prepare_self_grid(numi_cloth* h, bool self_collision, uint32_t substeps) {
         d.hash_over_head = h->buf.alloc<unsigned long long>(1);
         d.hash_over = h->buf.alloc<HashSlot>(h->d.n);
         d.hash = h->buf.alloc<HashSlot>(static_cast<size_t>(buckets) * NC_HASH_CAP);
-        d.self_stats = h->buf.alloc<unsigned long long>(2);
+        d.self_stats = h->buf.alloc<unsigned long long>(8);
+        // the ordered pass's list: room for three pairs per particle (a
+        // power of two, at least 4,096); scratch of three words per listed
+        // pair (sort keys, or the wavefront form's keys, predecessors and
+        // waves) plus one turn's partners
+        uint32_t list_cap = 4096u;
+        while (list_cap < 3u * h->d.n) list_cap <<= 1;
+        bool order_ok = true;
+        if (h->self_exact) {
+            d.self_list = h->buf.alloc<float4>(2u * static_cast<size_t>(list_cap));
+            d.self_list_head = h->buf.alloc<unsigned long long>(1);
+            d.self_pass_stats = h->buf.alloc<unsigned long long>(2);
+            d.self_keys = h->buf.alloc<unsigned long long>(3u * static_cast<size_t>(list_cap) + NC_SELF_GROUP);
+            d.self_mark = h->buf.alloc<unsigned long long>(h->d.n);
+            d.self_x0 = h->buf.alloc<float4>(h->d.n);
+            d.self_disp = h->buf.alloc<float>(h->d.n);
+            order_ok = d.self_list != nullptr && d.self_list_head != nullptr && d.self_pass_stats != nullptr &&
+                       d.self_keys != nullptr && d.self_mark != nullptr && d.self_x0 != nullptr &&
+                       d.self_disp != nullptr;
+        }
         if (d.hash_head == nullptr || d.hash == nullptr || d.self_stats == nullptr || d.hash_over_head == nullptr ||
-            d.hash_over == nullptr) {
+            d.hash_over == nullptr || !order_ok) {
             d.hash_head = nullptr;
             return NUMI_CLOTH_ENOMEM;
         }
+        d.self_list_cap = list_cap;
+        d.self_key_cap = list_cap;
         d.hash_mask = buckets - 1u;
     }
     if (h->d.hash_head != nullptr && ((h->epoch + substeps) >> 26) != (h->epoch >> 26)) {
         if (cudaMemsetAsync(h->d.hash_head, 0, (static_cast<size_t>(h->d.hash_mask) + 1u) * sizeof(unsigned long long),
                             h->stream) != cudaSuccess ||
-            cudaMemsetAsync(h->d.hash_over_head, 0, sizeof(unsigned long long), h->stream) != cudaSuccess)
+            cudaMemsetAsync(h->d.hash_over_head, 0, sizeof(unsigned long long), h->stream) != cudaSuccess ||
+            (h->self_exact &&
+             (cudaMemsetAsync(h->d.self_list_head, 0, sizeof(unsigned long long), h->stream) != cudaSuccess ||
+              cudaMemsetAsync(h->d.self_mark, 0, static_cast<size_t>(h->d.n) * sizeof(unsigned long long),
+                              h->stream) != cudaSuccess)))
             return NUMI_CLOTH_ECUDA;
     }
     return NUMI_CLOTH_OK;
@@ -1037,6 +1073,11 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
     d.fruit_flag = d.bar_count + 32;   // and 128 more
     d.stats = h->buf.alloc<uint32_t>(4);
 
+    // Point self contact in the reference's Gauss-Seidel order
+    // (NUMI_CLOTH_SELF_ORDER=reference): the frame kernels of
+    // cloth_self_order_kernels.cu; else the batched (Jacobi) order.
+    if (const char* order = std::getenv("NUMI_CLOTH_SELF_ORDER")) h->self_exact = std::strcmp(order, "reference") == 0;
+
     // Launch geometry: one resident CTA for a small cloth, else a full
     // cooperative grid (as many CTAs as can be co-resident).
     int sms = 0;
@@ -1052,7 +1093,8 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
     h->block = block;
     for (bool edge : {false, true}) {
         int k = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, frame_fn(edge), static_cast<int>(block), nc_resident_offset());
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, frame_fn(edge, h->self_exact), static_cast<int>(block),
+                                                      nc_resident_offset());
         per_sm = edge ? std::min(per_sm, k) : k;
     }
     uint32_t work = std::max({n, D, K, B});
@@ -1300,11 +1342,6 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
         cudaFuncGetAttributes(&fa, frame_fn(false));
         uint32_t tgrid = static_cast<uint32_t>(sms);
         env_u32("NUMI_CLOTH_TILE_GRID", tgrid);
-        // NUMI_CLOTH_TILE_SPLIT=0 resolves self contact inside the strain
-        // closures (no extra barrier, every closure repeats its ghosts'
-        // queries); the default has the owners resolve it first
-        d.tile_split_self = 1u;
-        env_u32("NUMI_CLOTH_TILE_SPLIT", d.tile_split_self);
         h->tile_grid = std::max(tgrid, 3u);
         h->tile_block = NC_BLOCK_MAX;
         h->tiles = build_tiles(h, scene->gridWidth, hij, hdm, hbij, hbm,
@@ -1532,6 +1569,17 @@ int numi_cloth_self_contacts(numi_cloth_t* h, unsigned long long* contacts, doub
     const uint32_t bits = static_cast<uint32_t>(st[1]);
     std::memcpy(&pen, &bits, sizeof(pen));
     *max_penetration = pen;
+    return NUMI_CLOTH_OK;
+}
+
+int numi_cloth_self_order_stats(numi_cloth_t* h, unsigned long long out[4]) {
+    if (h == nullptr || out == nullptr) return NUMI_CLOTH_EINVAL;
+    for (int k = 0; k < 4; ++k) out[k] = 0ull;
+    if (h->d.self_stats == nullptr) return NUMI_CLOTH_OK;
+    cudaSetDevice(h->device);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess ||
+        cudaMemcpy(out, h->d.self_stats + 2, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return NUMI_CLOTH_ECUDA;
     return NUMI_CLOTH_OK;
 }
 
@@ -1785,7 +1833,8 @@ int numi_cloth_launch_info(numi_cloth_t* h, uint32_t out[6]) {
     out[2] = stats[0];
     out[3] = h->launches;
     out[4] = h->cluster;
-    out[5] = h->d.resident | (h->neighbours ? 2u : 0u) | (h->tiles ? 4u : 0u) | (h->last_tiles ? 8u : 0u);
+    out[5] = h->d.resident | (h->neighbours ? 2u : 0u) | (h->tiles ? 4u : 0u) | (h->last_tiles ? 8u : 0u) |
+             (h->self_exact ? 16u : 0u);
     return NUMI_CLOTH_OK;
 }
 

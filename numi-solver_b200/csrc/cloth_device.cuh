@@ -118,7 +118,6 @@ struct DeviceCloth {
     unsigned long long* bar_count;
     unsigned long long* bar_flag;   // barrier number released last (own 128-byte line)
     unsigned long long* fruit_flag; // tile mode: substeps whose fruit-CTA tail is done (own line)
-    uint32_t tile_split_self;       // tile mode: owners resolve self contact before the strain chains
     unsigned int* abort_flag;
     // polls a barrier or neighbour wait makes before it gives up (0: the
     // default NC_BARRIER_SPIN_LIMIT)
@@ -176,6 +175,21 @@ struct DeviceCloth {
     // [0] self contacts (a < b pairs resolved), [1] max self penetration
     // (float bits; non-negative so unsigned max orders them)
     unsigned long long* self_stats;
+    // point self contact in the reference order: pairs phase A lists for the
+    // ordered pass (two entries each: start position, index | known bit),
+    // the list head (tag << 32 | entries), this pass's statistics, sort keys
+    // (self_key_cap, then room for one particle's turn), and per particle
+    // the ordered pass's marks (tag << 32 | bits), start positions and
+    // largest displacements
+    float4* self_list;
+    unsigned long long* self_list_head;
+    uint32_t self_list_cap;
+    unsigned long long* self_pass_stats;
+    unsigned long long* self_keys;
+    uint32_t self_key_cap;
+    unsigned long long* self_mark;
+    float4* self_x0;
+    float* self_disp;
     // edge/edge yarn self-collision.  Yarn segments: the distances that are
     // not shear diagonals, in array order.  Buffers (allocated on first use):
     //   pair list: every non-local segment pair (first < second) within the

@@ -1025,6 +1025,15 @@ __device__ __forceinline__ uint32_t self_slot(const SelfQuery& q, uint32_t t, ui
     return bq * NC_HASH_CAP + (t - pq);
 }
 
+// ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// Point self contact in the batched order (the default): every non-local
+// pair closer than 2r at the start of the pass, each particle's
+// corrections from all its pairs summed in fixed point and applied once.
+// Where every particle has at most one partner this makes the reference's
+// moves (tools/cloth_bag.cpp:4249-4315); the reference-order form below
+// keeps its Gauss-Seidel order everywhere.
+// ---------------------------------------------------------------------------
 // One candidate entry e of particle a at its start-of-pass position p: the
 // reference pair correction (a's half), summed in fixed point.
 __device__ __forceinline__ void self_pair(const Ctx& ctx, uint32_t a, const float4& p, const float4& e,
@@ -1133,6 +1142,738 @@ __device__ void self_solve(Ctx& ctx, uint32_t it) {
         if (self_solve_one(ctx, tag, a, p, q, contacts, max_pen)) px_set(ctx, a, q);
     }
     self_stats_flush(ctx.d, contacts, max_pen);
+}
+
+// Point self contact in the reference's Gauss-Seidel order
+// (solveSelfCollision, tools/cloth_bag.cpp:4249-4315).
+//
+// The reference visits the particles in index order.  Particle a, from its
+// position at its turn, resolves every non-local b > a whose start-of-pass
+// cell (edge = the contact distance 2r) is one of the 27 around a's cell,
+// cell by cell (z, then y, then x, each from -1) and by index within a
+// cell, each pair on the current positions.  The kernel makes the same
+// moves in parallel:
+//  * phase A, every particle at its start-of-pass position: a particle that
+//    touches nobody (no non-local particle closer than 2r) is no mover.  A
+//    mover whose only particle within 4r is its one contact partner, and
+//    whose partner's only particle within 4r is the mover itself, is one
+//    side of an isolated pair: each side computes the reference correction
+//    from the two start positions and applies its own half.  Every other
+//    mover lists its pairs with all particles within 4r (it is coupled).
+//  * the ordered pass, on one CTA and only where something was listed:
+//    the listed particles go back to their start positions and the listed
+//    pairs run serially in the reference's order.
+// Why that is the reference's result: a pair nobody listed either starts
+// 4r or more apart, or joins two particles that touch nobody.  The first
+// kind can act only if its particles move by 2r together, the second only
+// if one of them moves at all.  An isolated pair moves each of its
+// particles by at most r (a deeper pair is listed instead); the ordered
+// pass checks every listed particle's largest displacement against r and,
+// for a listed particle that touched nobody at the start but moved, lists
+// its own 4r neighbourhood and starts over.  Where a listed particle moves
+// farther, the list overflows or a particle has too many listed partners,
+// the ordered pass runs the reference loop itself on one thread over the
+// whole cloth (exact, slow, and met only where layers interpenetrate by
+// more than half the contact distance).
+// ---------------------------------------------------------------------------
+#define NC_SELF_LISTED 1ull
+#define NC_SELF_KNOWN 2ull     // the particle's whole 4r neighbourhood is listed
+#define NC_SELF_SIMPLE 4ull    // one side of an isolated pair (phase A)
+#define NC_SELF_ROUNDS 8u      // ordered-pass rounds before the fallback
+#define NC_SELF_GROUP 512u     // listed partners of one particle in one turn
+#define NC_SELF_KNOWN_BIT 0x80000000u
+#define NC_SELF_WAVE_MAX 8192u   // pairs in contact the wavefront form orders
+
+// Reference cell of a position (edge = the contact distance; the
+// reference's floor(position * inverseCell)).
+__device__ __forceinline__ int3 self_ref_cell(V3 p, float inv) {
+    return make_int3(static_cast<int>(floorf(p.x * inv)), static_cast<int>(floorf(p.y * inv)),
+                     static_cast<int>(floorf(p.z * inv)));
+}
+// Rank of cell b among the 27 around cell a in the reference's visit order
+// (dz, then dy, then dx, each from -1), or -1 outside them.
+__device__ __forceinline__ int self_visit_rank(int3 a, int3 b) {
+    const int dx = b.x - a.x, dy = b.y - a.y, dz = b.z - a.z;
+    if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1) return -1;
+    return (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
+}
+
+// Every grid entry of this pass within one grid cell (4r) of p: the buckets
+// of the 27 cells around p's cell that reach within a cell of p, then the
+// overflow list.  Two cells that share a bucket repeat its entries; callers
+// either tolerate repeats (a repeat only makes a particle look coupled) or
+// remove them.
+template <class F>
+__device__ __forceinline__ void self_scan_cell(const Ctx& ctx, uint32_t tag, const float4& p, F&& visit) {
+    const DeviceCloth& d = ctx.d;
+    const float inv_cell = 1.0f / (4.0f * ctx.c.radius);
+    const float coord[3] = {p.x * inv_cell, p.y * inv_cell, p.z * inv_cell};
+    int base[3];
+    float lo2[3], hi2[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float c0 = floorf(coord[k]);
+        base[k] = static_cast<int>(c0);
+        const float f = coord[k] - c0;
+        lo2[k] = f * f;
+        hi2[k] = (1.0f - f) * (1.0f - f);
+    }
+    const float slack = 1.0f + 1.0e-3f + 2.4e-7f * fmaxf(fabsf(coord[0]), fmaxf(fabsf(coord[1]), fabsf(coord[2])));
+    const float reach2 = slack * slack;
+    for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx) {
+                const float g2 = (dx < 0 ? lo2[0] : dx > 0 ? hi2[0] : 0.0f) +
+                                 (dy < 0 ? lo2[1] : dy > 0 ? hi2[1] : 0.0f) +
+                                 (dz < 0 ? lo2[2] : dz > 0 ? hi2[2] : 0.0f);
+                if (g2 >= reach2) continue;
+                const uint32_t bk = cell_bucket(base[0] + dx, base[1] + dy, base[2] + dz, d.hash_mask);
+                const unsigned long long hd = __ldcg(d.hash_head + bk);
+                if (static_cast<uint32_t>(hd >> 32) != tag) continue;
+                const uint32_t cnt = min(static_cast<uint32_t>(hd), NC_HASH_CAP);
+                for (uint32_t s = 0; s < cnt; ++s) visit(__ldcg(&d.hash[bk * NC_HASH_CAP + s].pos));
+            }
+    const unsigned long long oh = __ldcg(d.hash_over_head);
+    const uint32_t over = static_cast<uint32_t>(oh >> 32) == tag ? min(static_cast<uint32_t>(oh), d.n) : 0u;
+    for (uint32_t o = 0; o < over; ++o) visit(__ldcg(&d.hash_over[o].pos));
+}
+
+// A pair the pass can resolve: another particle, not local, not both
+// fixed (w: the inverse masses).
+__device__ __forceinline__ bool self_partner(const DeviceCloth& d, uint32_t a, uint32_t b, float wa, float wb) {
+    return b != a && wa + wb > 0.0f && !local_pair(d, min(a, b), max(a, b));
+}
+
+// Entries within 4r of particle a (start position p, w = its inverse mass)
+// that it may pair with, counted up to two.
+__device__ __noinline__ uint32_t self_count_near(const Ctx& ctx, uint32_t tag, uint32_t a, const float4& p) {
+    const float reach = 4.0f * ctx.c.radius;
+    uint32_t n = 0u;
+    self_scan_cell(ctx, tag, p, [&](const float4& e) {
+        const uint32_t b = __float_as_uint(e.w);
+        if (n >= 2u || b == a || len3(xyz(e) - xyz(p)) >= reach) return;
+        if (self_partner(ctx.d, a, b, p.w, px(ctx, b).w)) ++n;
+    });
+    return n;
+}
+
+// List particle a's pairs with every particle within 4r (a's start position
+// p; a's entry carries the known bit).  False where the list is full.
+__device__ __noinline__ bool self_list_near(const Ctx& ctx, uint32_t tag, uint32_t a, const float4& p) {
+    const DeviceCloth& d = ctx.d;
+    const float reach = 4.0f * ctx.c.radius;
+    bool room = true;
+    self_scan_cell(ctx, tag, p, [&](const float4& e) {
+        const uint32_t b = __float_as_uint(e.w);
+        if (b == a || len3(xyz(e) - xyz(p)) >= reach || !self_partner(d, a, b, p.w, px(ctx, b).w)) return;
+        atomicMax(d.self_list_head, static_cast<unsigned long long>(tag) << 32);
+        const uint32_t k = static_cast<uint32_t>(atomicAdd(d.self_list_head, 1ull));
+        if (k >= d.self_list_cap) {
+            room = false;
+            return;
+        }
+        const float4 ea = make_float4(p.x, p.y, p.z, __uint_as_float(a | NC_SELF_KNOWN_BIT));
+        const float4 eb = make_float4(e.x, e.y, e.z, __uint_as_float(b));
+        d.self_list[2u * k] = a < b ? ea : eb;
+        d.self_list[2u * k + 1u] = a < b ? eb : ea;
+    });
+    return room;
+}
+
+// Phase A of a mover a (start position p) with `touches` contact partners,
+// the last one `partner` (start position and inverse mass pe): the isolated
+// pair's move, or the coupled particle's listing.  Out of line: only movers
+// run it.
+__device__ __noinline__ bool self_mover(const Ctx& ctx, uint32_t tag, uint32_t a, const float4& p, uint32_t touches,
+                                        uint32_t partner, const float4& pe, float4& moved,
+                                        unsigned long long& contacts, float& max_pen) {
+    const DeviceCloth& d = ctx.d;
+    const float target = 2.0f * ctx.c.radius;
+    if (touches == 1u && self_count_near(ctx, tag, a, p) == 1u && self_count_near(ctx, tag, partner, pe) == 1u) {
+        // isolated pair: the reference's correction with f < s
+        const bool first = a < partner;
+        const float4 xf = first ? p : pe, xs = first ? pe : p;
+        const float inv_ref = 1.0f / target;
+        const bool visited = self_visit_rank(self_ref_cell(xyz(xf), inv_ref), self_ref_cell(xyz(xs), inv_ref)) >= 0;
+        const V3 diff = xyz(xs) - xyz(xf);
+        const float L = len3(diff);
+        if (!visited || L < 1.0e-12f) {
+            d.self_mark[a] = (static_cast<unsigned long long>(tag) << 32) | NC_SELF_SIMPLE;
+            return false;   // a pair the reference skips, and nothing else moves either side
+        }
+        const float den = xf.w + xs.w;
+        const V3 corr = diff * ((target - L) / (L * den));
+        const V3 cf = corr * xf.w, cs = corr * xs.w;
+        const float lim = 0.5f * target * (1.0f - 1.0e-4f);
+        if (len3(cf) <= lim && len3(cs) <= lim) {
+            d.self_mark[a] = (static_cast<unsigned long long>(tag) << 32) | NC_SELF_SIMPLE;
+            moved = with_xyz(p, first ? xyz(p) - cf : xyz(p) + cs);
+            if (first) {
+                ++contacts;
+                max_pen = fmaxf(max_pen, target - L);
+            }
+            return true;
+        }
+    }
+    (void)self_list_near(ctx, tag, a, p);   // a full list sends the ordered pass to the fallback
+    return false;
+}
+
+
+// Phase A of particle a at its start-of-pass position p: true when its
+// isolated pair moved it, with the moved position in `moved`; counts that
+// pair (on its first particle) and its penetration.  A coupled particle is
+// listed and left where it is.
+__device__ __forceinline__ bool self_exact_one(const Ctx& ctx, uint32_t tag, uint32_t a, const float4& p,
+                                               float4& moved, unsigned long long& contacts, float& max_pen) {
+    const DeviceCloth& d = ctx.d;
+    const bool l1 = d.cluster_barrier == 0u;
+    const float target = 2.0f * ctx.c.radius;
+    SelfQuery q;
+    unsigned long long hd[8];
+    bool near[8];
+    self_heads(ctx, p, q, hd, near);
+    const uint32_t total = self_counts(tag, q, hd, near);
+    uint32_t touches = 0u, partner = 0u;
+    float4 pe = p;
+    auto touch = [&](const float4& e) {
+        const uint32_t b = __float_as_uint(e.w);
+        if (b == a || len3(xyz(e) - xyz(p)) >= target) return;
+        const float wb = px(ctx, b).w;
+        if (!self_partner(d, a, b, p.w, wb)) return;
+        ++touches;
+        partner = b;
+        pe = make_float4(e.x, e.y, e.z, wb);
+    };
+    for (uint32_t t0 = 0; t0 < total; t0 += NC_SELF_BATCH) {
+        float4 e[NC_SELF_BATCH];
+#pragma unroll
+        for (uint32_t j = 0; j < NC_SELF_BATCH; ++j) {
+            const uint32_t slot = self_slot(q, t0 + j, total);
+            e[j] = l1 ? __ldca(&d.hash[slot].pos) : __ldcg(&d.hash[slot].pos);
+        }
+#pragma unroll
+        for (uint32_t j = 0; j < NC_SELF_BATCH; ++j)
+            if (t0 + j < total) touch(e[j]);
+    }
+    {
+        const unsigned long long oh = l1 ? __ldca(d.hash_over_head) : __ldcg(d.hash_over_head);
+        const uint32_t over = static_cast<uint32_t>(oh >> 32) == tag ? min(static_cast<uint32_t>(oh), d.n) : 0u;
+        for (uint32_t o = 0; o < over; ++o) touch(__ldcg(&d.hash_over[o].pos));
+    }
+    if (touches == 0u) return false;
+    return self_mover(ctx, tag, a, p, touches, partner, pe, moved, contacts, max_pen);
+}
+
+// This pass's contact statistics of phase A: one atomic pair per warp (an
+// integer sum and the maximum of non-negative floats as integers).
+__device__ __forceinline__ void self_pass_flush(const DeviceCloth& d, unsigned long long contacts, float max_pen) {
+    unsigned pen_bits = __float_as_uint(max_pen);
+    for (int o = 16; o > 0; o >>= 1) {
+        contacts += __shfl_xor_sync(0xffffffffu, contacts, o);
+        pen_bits = max(pen_bits, __shfl_xor_sync(0xffffffffu, pen_bits, o));
+    }
+    if ((threadIdx.x & 31u) == 0u && contacts != 0ull) {
+        atomicAdd(d.self_pass_stats, contacts);
+        atomicMax(d.self_pass_stats + 1, static_cast<unsigned long long>(pen_bits));
+    }
+}
+
+__device__ void self_solve_exact(Ctx& ctx, uint32_t it) {
+    const uint32_t tag = self_pass_tag(ctx, it);
+    unsigned long long contacts = 0ull;
+    float max_pen = 0.0f;
+    for (Range r = particle_range(ctx); r.i < r.end; r.i += r.stride) {
+        const uint32_t a = r.i;
+        const float4 p = px(ctx, a);
+        float4 q;
+        if (self_exact_one(ctx, tag, a, p, q, contacts, max_pen)) px_set(ctx, a, q);
+    }
+    self_pass_flush(ctx.d, contacts, max_pen);
+}
+
+// The pass's statistics into the cloth's (one thread, after the pass).
+__device__ __forceinline__ void self_fold(const DeviceCloth& d) {
+    const unsigned long long c = __ldcg(d.self_pass_stats);
+    const unsigned long long pen = __ldcg(d.self_pass_stats + 1);
+    if (c != 0ull) {
+        d.self_stats[0] += c;
+        d.self_stats[1] = max(d.self_stats[1], pen);
+    }
+    d.self_pass_stats[0] = 0ull;
+    d.self_pass_stats[1] = 0ull;
+}
+
+// The reference pair body (first f < second s) on the current positions;
+// with `x0` set, also the largest displacement of each side from its start
+// position.  True where it acted, with its penetration.
+__device__ __forceinline__ bool self_gs_pair(const Ctx& ctx, uint32_t f, uint32_t s, float target, bool track,
+                                             float& pen) {
+    const DeviceCloth& d = ctx.d;
+    const float4 xf = px(ctx, f), xs = px(ctx, s);
+    const V3 diff = xyz(xs) - xyz(xf);
+    const float L = len3(diff);
+    if (L >= target || L < 1.0e-12f) return false;
+    const float den = xf.w + xs.w;
+    if (den <= 0.0f) return false;
+    const V3 corr = diff * ((target - L) / (L * den));
+    const V3 nf = xyz(xf) - corr * xf.w, ns = xyz(xs) + corr * xs.w;
+    px_set(ctx, f, with_xyz(xf, nf));
+    px_set(ctx, s, with_xyz(xs, ns));
+    if (track) {
+        d.self_disp[f] = fmaxf(d.self_disp[f], len3(nf - xyz(d.self_x0[f])));
+        d.self_disp[s] = fmaxf(d.self_disp[s], len3(ns - xyz(d.self_x0[s])));
+    }
+    pen = target - L;
+    return true;
+}
+
+// Sort n keys (a power of two) ascending, the calling CTA together.
+__device__ void self_bitonic(unsigned long long* keys, uint32_t n) {
+    for (uint32_t size = 2u; size <= n; size <<= 1)
+        for (uint32_t stride = size >> 1; stride > 0u; stride >>= 1) {
+            for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+                const uint32_t j = i ^ stride;
+                if (j <= i) continue;
+                const unsigned long long ki = keys[i], kj = keys[j];
+                const bool up = (i & size) == 0u;
+                if ((ki > kj) == up) {
+                    keys[i] = kj;
+                    keys[j] = ki;
+                }
+            }
+            __syncthreads();
+        }
+}
+
+// Insertion sort of a short run of keys (one thread).
+__device__ __forceinline__ void self_sort_run(unsigned long long* k, uint32_t n) {
+    for (uint32_t i = 1; i < n; ++i) {
+        const unsigned long long v = k[i];
+        uint32_t j = i;
+        while (j > 0u && k[j - 1u] > v) {
+            k[j] = k[j - 1u];
+            --j;
+        }
+        k[j] = v;
+    }
+}
+
+// The reference loop itself, one thread, every particle from its
+// start-of-pass position (its grid entry): the exact fallback.  False where
+// a particle has more than NC_SELF_GROUP candidates in its 27 cells.
+__device__ __noinline__ bool self_serial_all(const Ctx& ctx, uint32_t tag, unsigned long long& contacts, float& max_pen) {
+    const DeviceCloth& d = ctx.d;
+    const float target = 2.0f * ctx.c.radius;
+    const float inv_ref = 1.0f / target;
+    unsigned long long* run = d.self_keys + 3u * d.self_key_cap;
+    const unsigned long long oh = __ldcg(d.hash_over_head);
+    const uint32_t over = static_cast<uint32_t>(oh >> 32) == tag ? min(static_cast<uint32_t>(oh), d.n) : 0u;
+    auto floor_half = [](int v) { return v >= 0 ? v / 2 : -((1 - v) / 2); };
+    for (uint32_t a = 0; a < d.n; ++a) {
+        const int3 tc = self_ref_cell(xyz(px(ctx, a)), inv_ref);
+        uint32_t n = 0u;
+        bool room = true;
+        auto take = [&](const float4& e) {
+            const uint32_t b = __float_as_uint(e.w);
+            if (b <= a || local_pair(d, a, b)) return;
+            const int rank = self_visit_rank(tc, self_ref_cell(xyz(e), inv_ref));
+            if (rank < 0) return;
+            if (n >= NC_SELF_GROUP) {
+                room = false;
+                return;
+            }
+            run[n++] = (static_cast<unsigned long long>(rank) << 32) | b;
+        };
+        // grid cells (edge 4r) that hold the reference cells tc - 1 .. tc + 1:
+        // a grid coordinate is exactly half the reference one (1/(4r) is
+        // 1/(2r) halved, so the products differ by an exact factor of two)
+        const int gx0 = floor_half(tc.x - 1), gx1 = floor_half(tc.x + 1);
+        const int gy0 = floor_half(tc.y - 1), gy1 = floor_half(tc.y + 1);
+        const int gz0 = floor_half(tc.z - 1), gz1 = floor_half(tc.z + 1);
+        for (int gz = gz0; gz <= gz1; ++gz)
+            for (int gy = gy0; gy <= gy1; ++gy)
+                for (int gx = gx0; gx <= gx1; ++gx) {
+                    const uint32_t bk = cell_bucket(gx, gy, gz, d.hash_mask);
+                    const unsigned long long hd = __ldcg(d.hash_head + bk);
+                    if (static_cast<uint32_t>(hd >> 32) != tag) continue;
+                    const uint32_t cnt = min(static_cast<uint32_t>(hd), NC_HASH_CAP);
+                    for (uint32_t s = 0; s < cnt; ++s) take(__ldcg(&d.hash[bk * NC_HASH_CAP + s].pos));
+                }
+        for (uint32_t o = 0; o < over; ++o) take(__ldcg(&d.hash_over[o].pos));
+        if (!room) return false;
+        self_sort_run(run, n);
+        for (uint32_t k = 0; k < n; ++k) {
+            if (k > 0u && run[k] == run[k - 1u]) continue;   // a bucket met twice
+            float pen;
+            if (self_gs_pair(ctx, a, static_cast<uint32_t>(run[k]), target, false, pen)) {
+                ++contacts;
+                max_pen = fmaxf(max_pen, pen);
+            }
+        }
+    }
+    return true;
+}
+
+// The ordered pass's fast form (the calling CTA, all its threads): the
+// listed pairs in contact at the start of the pass are ordered by the
+// reference's key (first particle, rank of the second's cell around the
+// first's, second particle) and run as wavefronts: a pair runs once the
+// pairs before it in that order that share a particle have run, so each
+// pair sees the positions the serial pass gives it.  The listed pairs that
+// start apart run nowhere; they are proved idle afterwards (their start
+// distance less both particles' largest displacements stays at least the
+// contact distance), as are the visit cells (every first particle's cell at
+// its turn is its start cell).  False where a proof fails or the pairs do
+// not fit the scratch: the caller then restores the start positions and
+// runs the pairs serially.  Scratch (d.self_keys, u64 words): keys [0, K),
+// predecessors [K, 2K) (via the first particle << 32 | via the second,
+// 0xffffffff none), wavefront [2K, 3K) (bit 63: the first pair of its
+// first particle's turn; low bits 0 pending, t run in wave t; ~0 a repeat),
+// K = self_key_cap.  The predecessor search compares every pair with every
+// other; beyond NC_SELF_WAVE_MAX pairs the serial form runs instead.
+__device__ __noinline__ bool self_ordered_levels(const Ctx& ctx, uint32_t tag, uint32_t m,
+                                                 unsigned long long& contacts_out, float& pen_out) {
+    const DeviceCloth& d = ctx.d;
+    const float target = 2.0f * ctx.c.radius;
+    const float inv_ref = 1.0f / target;
+    const float lim = 0.5f * target * (1.0f - 1.0e-4f);
+    const uint32_t K = min(d.self_key_cap, NC_SELF_WAVE_MAX);
+    unsigned long long* key = d.self_keys;
+    unsigned long long* pred = d.self_keys + K;
+    unsigned long long* wave = d.self_keys + 2u * K;
+    constexpr uint32_t kNone = 0xffffffffu;
+    __shared__ uint32_t s_k, s_bad, s_left;
+    __shared__ unsigned long long s_contacts;
+    __shared__ unsigned s_pen_bits;
+    if (threadIdx.x == 0) {
+        s_k = 0u;
+        s_bad = 0u;
+        s_contacts = 0ull;
+        s_pen_bits = 0u;
+    }
+    // listed particles at their start positions, displacements cleared
+    for (uint32_t k = threadIdx.x; k < 2u * m; k += blockDim.x) {
+        const float4 en = __ldcg(d.self_list + k);
+        const uint32_t i = __float_as_uint(en.w) & ~NC_SELF_KNOWN_BIT;
+        d.self_x0[i] = make_float4(en.x, en.y, en.z, 0.0f);
+        d.self_disp[i] = 0.0f;
+        px_set(ctx, i, make_float4(en.x, en.y, en.z, px(ctx, i).w));
+    }
+    __syncthreads();
+    // the pairs in contact at the start, keyed in the reference's order
+    for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
+        const float4 ef = __ldcg(d.self_list + 2u * k), es = __ldcg(d.self_list + 2u * k + 1u);
+        const uint32_t f = __float_as_uint(ef.w) & ~NC_SELF_KNOWN_BIT, s = __float_as_uint(es.w) & ~NC_SELF_KNOWN_BIT;
+        const float L0 = len3(xyz(es) - xyz(ef));
+        if (L0 >= target || L0 < 1.0e-12f) continue;
+        const int rank = self_visit_rank(self_ref_cell(xyz(ef), inv_ref), self_ref_cell(xyz(es), inv_ref));
+        if (rank < 0 || s >= (1u << 27)) {
+            s_bad = 1u;   // a touching pair outside the visit cells: the serial form decides
+            continue;
+        }
+        const uint32_t slot = atomicAdd(&s_k, 1u);
+        if (slot < K) key[slot] = (static_cast<unsigned long long>(f) << 32) |
+                                  (static_cast<unsigned long long>(rank) << 27) | s;
+    }
+    __syncthreads();
+    const uint32_t n = s_k;
+    if (n > K || s_bad != 0u) return false;
+    // predecessors through each particle (the latest earlier pair that
+    // shares it; among equal keys the lowest slot), repeats, first pairs of
+    // a turn
+    for (uint32_t p = threadIdx.x; p < n; p += blockDim.x) {
+        const unsigned long long kp = key[p];
+        const uint32_t f = static_cast<uint32_t>(kp >> 32), s = static_cast<uint32_t>(kp) & ((1u << 27) - 1u);
+        unsigned long long bf = 0ull, bs = 0ull;
+        uint32_t pf = kNone, ps = kNone;
+        bool repeat = false;
+        for (uint32_t q = 0; q < n; ++q) {
+            const unsigned long long kq = key[q];
+            if (kq == kp) {
+                repeat = repeat || q < p;
+                continue;
+            }
+            if (kq > kp) continue;
+            const uint32_t fq = static_cast<uint32_t>(kq >> 32), sq = static_cast<uint32_t>(kq) & ((1u << 27) - 1u);
+            if ((fq == f || sq == f) && (pf == kNone || kq > bf)) {
+                bf = kq;
+                pf = q;
+            }
+            if ((fq == s || sq == s) && (ps == kNone || kq > bs)) {
+                bs = kq;
+                ps = q;
+            }
+        }
+        pred[p] = (static_cast<unsigned long long>(pf) << 32) | ps;
+        // first pair of f's turn: no earlier pair has f as its first particle
+        const bool first = pf == kNone || static_cast<uint32_t>(bf >> 32) != f;
+        wave[p] = repeat ? ~0ull : (first ? (1ull << 63) : 0ull);
+    }
+    if (threadIdx.x == 0) s_left = n;
+    // wavefronts: a pair runs in wave t once both predecessors ran in an
+    // earlier wave (every wave runs at least the earliest pending pair)
+    for (uint32_t t = 1u;; ++t) {
+        __syncthreads();   // the last wave's writes are visible
+        const bool go = s_left != 0u && s_bad == 0u && t <= n + 1u;
+        __syncthreads();   // everyone read the counters before any wave writes them
+        if (!go) break;
+        unsigned long long contacts = 0ull;
+        float pen_max = 0.0f;
+        uint32_t ran = 0u;
+        for (uint32_t p = threadIdx.x; p < n; p += blockDim.x) {
+            const unsigned long long w = wave[p];
+            if (w == ~0ull) {
+                if (t == 1u) ++ran;   // a repeat counts once, as done
+                continue;
+            }
+            if ((w & ~(1ull << 63)) != 0ull) continue;
+            const unsigned long long pp = pred[p];
+            const uint32_t pf = static_cast<uint32_t>(pp >> 32), ps = static_cast<uint32_t>(pp);
+            auto ready = [&](uint32_t q) {
+                if (q == kNone) return true;
+                const unsigned long long wq = wave[q] & ~(1ull << 63);
+                return wq != 0ull && wq < t;
+            };
+            if (!ready(pf) || !ready(ps)) continue;
+            const unsigned long long kp = key[p];
+            const uint32_t f = static_cast<uint32_t>(kp >> 32), s = static_cast<uint32_t>(kp) & ((1u << 27) - 1u);
+            if ((w >> 63) != 0ull) {
+                // f's turn starts: its cell must still be its start cell
+                const int3 tc = self_ref_cell(xyz(px(ctx, f)), inv_ref);
+                const int3 sc = self_ref_cell(xyz(d.self_x0[f]), inv_ref);
+                if (tc.x != sc.x || tc.y != sc.y || tc.z != sc.z) s_bad = 1u;
+            }
+            float pen;
+            if (self_gs_pair(ctx, f, s, target, true, pen)) {
+                ++contacts;
+                pen_max = fmaxf(pen_max, pen);
+            }
+            wave[p] = (w & (1ull << 63)) | t;
+            ++ran;
+        }
+        if (contacts != 0ull) {
+            atomicAdd(&s_contacts, contacts);
+            atomicMax(&s_pen_bits, __float_as_uint(pen_max));
+        }
+        if (ran != 0u) atomicSub(&s_left, ran);
+    }
+    if (threadIdx.x == 0 && s_left != 0u) s_bad = 1u;   // unreachable: the waves ran out
+    // the proofs: every listed pair that started apart stays apart, and no
+    // particle moved farther than the listing reach allows
+    for (uint32_t k = threadIdx.x; k < m && s_bad == 0u; k += blockDim.x) {
+        const float4 ef = __ldcg(d.self_list + 2u * k), es = __ldcg(d.self_list + 2u * k + 1u);
+        const uint32_t f = __float_as_uint(ef.w) & ~NC_SELF_KNOWN_BIT, s = __float_as_uint(es.w) & ~NC_SELF_KNOWN_BIT;
+        const float df = d.self_disp[f], ds = d.self_disp[s];
+        if (df > lim || ds > lim) s_bad = 1u;
+        const float L0 = len3(xyz(es) - xyz(ef));
+        if (L0 < 1.0e-12f) {
+            if (df + ds > 0.0f) s_bad = 1u;   // coincident at the start and moved: it may act
+        } else if (L0 >= target && L0 - (df + ds) <= target * (1.0f + 1.0e-5f)) {
+            s_bad = 1u;
+        }
+    }
+    __syncthreads();
+    contacts_out = s_contacts;
+    pen_out = __uint_as_float(s_pen_bits);
+    return s_bad == 0u;
+}
+
+// The ordered pass (the CTA that calls it, all its threads): the listed
+// pairs in the reference's order, the fallback where the checks fail, then
+// the ground clamp of the particles it moved and the pass statistics.
+__device__ __noinline__ void self_ordered(const Ctx& ctx, uint32_t tag, uint32_t listed) {
+    const DeviceCloth& d = ctx.d;
+    const SubCfg& c = ctx.c;
+    const float target = 2.0f * c.radius;
+    const float lim = 0.5f * target * (1.0f - 1.0e-4f);
+    const unsigned long long mark_tag = static_cast<unsigned long long>(tag) << 32;
+    __shared__ uint32_t s_state;   // 1: fallback, 2: the list grew
+    __shared__ unsigned long long s_contacts;
+    __shared__ float s_pen;
+    uint32_t m = listed;
+    bool fallback = m > d.self_list_cap;
+    uint32_t rounds = 0u;
+    unsigned long long fast_contacts = 0ull;
+    float fast_pen = 0.0f;
+    const bool fast = !fallback && self_ordered_levels(ctx, tag, m, fast_contacts, fast_pen);
+    for (uint32_t round = 0; !fallback && !fast; ++round) {
+        if (round == NC_SELF_ROUNDS) {
+            fallback = true;
+            break;
+        }
+        rounds = round + 1u;
+        // listed particles back at their start positions
+        for (uint32_t k = threadIdx.x; k < 2u * m; k += blockDim.x) {
+            const float4 en = __ldcg(d.self_list + k);
+            const uint32_t raw = __float_as_uint(en.w), i = raw & ~NC_SELF_KNOWN_BIT;
+            atomicMax(d.self_mark + i, mark_tag);
+            atomicOr(d.self_mark + i, NC_SELF_LISTED | ((raw & NC_SELF_KNOWN_BIT) ? NC_SELF_KNOWN : 0ull));
+            d.self_x0[i] = make_float4(en.x, en.y, en.z, 0.0f);
+            d.self_disp[i] = 0.0f;
+            px_set(ctx, i, make_float4(en.x, en.y, en.z, px(ctx, i).w));
+        }
+        uint32_t pow2 = 1u;
+        while (pow2 < m) pow2 <<= 1;
+        for (uint32_t k = threadIdx.x; k < pow2; k += blockDim.x) {
+            unsigned long long key = ~0ull;
+            if (k < m) {
+                const uint32_t f = __float_as_uint(__ldcg(&d.self_list[2u * k].w)) & ~NC_SELF_KNOWN_BIT;
+                const uint32_t s = __float_as_uint(__ldcg(&d.self_list[2u * k + 1u].w)) & ~NC_SELF_KNOWN_BIT;
+                key = (static_cast<unsigned long long>(f) << 32) | s;
+            }
+            d.self_keys[k] = key;
+        }
+        if (threadIdx.x == 0) s_state = 0u;
+        __syncthreads();
+        self_bitonic(d.self_keys, pow2);
+        // the listed pairs, first particle by first particle; a turn's pairs
+        // in the reference's cell order from the particle's position then
+        if (threadIdx.x == 0) {
+            const float inv_ref = 1.0f / target;
+            unsigned long long* run = d.self_keys + 3u * d.self_key_cap;
+            unsigned long long contacts = 0ull;
+            float pen_max = 0.0f;
+            for (uint32_t k = 0; k < m && s_state == 0u;) {
+                const uint32_t a = static_cast<uint32_t>(d.self_keys[k] >> 32);
+                const int3 tc = self_ref_cell(xyz(px(ctx, a)), inv_ref);
+                uint32_t n = 0u;
+                for (; k < m && static_cast<uint32_t>(d.self_keys[k] >> 32) == a; ++k) {
+                    if (k > 0u && d.self_keys[k] == d.self_keys[k - 1u]) continue;   // listed by both sides
+                    const uint32_t b = static_cast<uint32_t>(d.self_keys[k]);
+                    const int rank = self_visit_rank(tc, self_ref_cell(xyz(d.self_x0[b]), inv_ref));
+                    if (rank < 0) continue;
+                    if (n == NC_SELF_GROUP) {
+                        s_state = 1u;
+                        break;
+                    }
+                    run[n++] = (static_cast<unsigned long long>(rank) << 32) | b;
+                }
+                self_sort_run(run, n);
+                for (uint32_t j = 0; j < n; ++j) {
+                    float pen;
+                    if (self_gs_pair(ctx, a, static_cast<uint32_t>(run[j]), target, true, pen)) {
+                        ++contacts;
+                        pen_max = fmaxf(pen_max, pen);
+                    }
+                }
+            }
+            s_contacts = contacts;
+            s_pen = pen_max;
+        }
+        __syncthreads();
+        // the checks: every listed particle within r of its start; a moved
+        // particle whose neighbourhood is not listed yet lists it
+        for (uint32_t k = threadIdx.x; k < 2u * m; k += blockDim.x) {
+            const uint32_t i = __float_as_uint(__ldcg(&d.self_list[k].w)) & ~NC_SELF_KNOWN_BIT;
+            const float dsp = __ldcg(d.self_disp + i);
+            if (dsp > lim) {
+                atomicOr(&s_state, 1u);
+            } else if (dsp > 0.0f) {
+                const unsigned long long old = atomicOr(d.self_mark + i, NC_SELF_KNOWN);
+                if ((old & NC_SELF_KNOWN) == 0ull) {
+                    const float4 x0 = d.self_x0[i];
+                    bool simple_met = false;
+                    self_scan_cell(ctx, tag, x0, [&](const float4& e) {
+                        const uint32_t b = __float_as_uint(e.w);
+                        if (b == i || len3(xyz(e) - xyz(x0)) >= 2.0f * target) return;
+                        const unsigned long long mb = __ldcg(d.self_mark + b);
+                        if ((mb >> 32) == tag && (mb & NC_SELF_SIMPLE)) simple_met = true;
+                    });
+                    const float4 xi = make_float4(x0.x, x0.y, x0.z, px(ctx, i).w);
+                    if (simple_met || !self_list_near(ctx, tag, i, xi)) atomicOr(&s_state, 1u);
+                    atomicOr(&s_state, 2u);
+                }
+            }
+        }
+        __syncthreads();
+        const uint32_t state = s_state;
+        if (state & 1u) {
+            fallback = true;
+            break;
+        }
+        if ((state & 2u) == 0u) break;
+        const unsigned long long head = __ldcg(d.self_list_head);
+        m = static_cast<uint32_t>(head);
+        fallback = m > d.self_list_cap;
+        __syncthreads();
+    }
+    if (fallback) {
+        // every particle back at its start-of-pass position
+        for (uint32_t bk = threadIdx.x; bk <= d.hash_mask; bk += blockDim.x) {
+            const unsigned long long hd = __ldcg(d.hash_head + bk);
+            if (static_cast<uint32_t>(hd >> 32) != tag) continue;
+            const uint32_t cnt = min(static_cast<uint32_t>(hd), NC_HASH_CAP);
+            for (uint32_t s = 0; s < cnt; ++s) {
+                const float4 e = __ldcg(&d.hash[bk * NC_HASH_CAP + s].pos);
+                const uint32_t i = __float_as_uint(e.w);
+                px_set(ctx, i, make_float4(e.x, e.y, e.z, px(ctx, i).w));
+            }
+        }
+        {
+            const unsigned long long oh = __ldcg(d.hash_over_head);
+            const uint32_t over = static_cast<uint32_t>(oh >> 32) == tag ? min(static_cast<uint32_t>(oh), d.n) : 0u;
+            for (uint32_t o = threadIdx.x; o < over; o += blockDim.x) {
+                const float4 e = __ldcg(&d.hash_over[o].pos);
+                const uint32_t i = __float_as_uint(e.w);
+                px_set(ctx, i, make_float4(e.x, e.y, e.z, px(ctx, i).w));
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned long long contacts = 0ull;
+            float pen = 0.0f;
+            if (!self_serial_all(ctx, tag, contacts, pen)) fail(d, NUMI_CLOTH_FAILURE_RANGE);
+            // the pass's statistics are this loop's alone
+            d.self_pass_stats[0] = contacts;
+            d.self_pass_stats[1] = __float_as_uint(pen);
+        }
+        __syncthreads();
+        if (c.ground)
+            for (uint32_t i = threadIdx.x; i < d.n; i += blockDim.x) {
+                const float4 p = px(ctx, i);
+                if (c.radius - p.z > 0.0f) px_set(ctx, i, make_float4(p.x, p.y, c.radius, p.w));
+            }
+    } else {
+        if (c.ground)
+            for (uint32_t k = threadIdx.x; k < 2u * m; k += blockDim.x) {
+                const uint32_t i = __float_as_uint(__ldcg(&d.self_list[k].w)) & ~NC_SELF_KNOWN_BIT;
+                const float4 p = px(ctx, i);
+                if (c.radius - p.z > 0.0f) px_set(ctx, i, make_float4(p.x, p.y, c.radius, p.w));
+            }
+        const unsigned long long ordered_contacts = fast ? fast_contacts : s_contacts;
+        const float ordered_pen = fast ? fast_pen : s_pen;
+        if (threadIdx.x == 0 && ordered_contacts != 0ull) {
+            d.self_pass_stats[0] += ordered_contacts;
+            d.self_pass_stats[1] =
+                max(d.self_pass_stats[1], static_cast<unsigned long long>(__float_as_uint(ordered_pen)));
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        self_fold(d);
+        d.self_stats[2] += 1ull;
+        d.self_stats[3] += m;
+        d.self_stats[4] += rounds;
+        d.self_stats[5] += fallback ? 1ull : 0ull;
+    }
+}
+
+// After phase A and the barrier behind it, every CTA alike: the ordered
+// pass where phase A listed pairs (then one more barrier), else only the
+// statistics.
+__device__ bool self_settle(Ctx& ctx, uint32_t it) {
+    const DeviceCloth& d = ctx.d;
+    const uint32_t tag = self_pass_tag(ctx, it);
+    const unsigned long long head = __ldcg(d.self_list_head);
+    const uint32_t listed = static_cast<uint32_t>(head >> 32) == tag ? static_cast<uint32_t>(head) : 0u;
+    if (listed == 0u) {
+        if (ctx.grip_cta && threadIdx.x == 0) self_fold(d);
+        return true;
+    }
+    if (ctx.grip_cta) self_ordered(ctx, tag, listed);
+    NC_SYNC(ctx);
+    return true;
 }
 
 
@@ -1953,10 +2694,17 @@ __device__ __forceinline__ bool substep(Ctx& ctx, bool last) {
             fruit_flush(ctx);
             self_insert(ctx, it);
             NC_SYNC(ctx);
+#ifdef NC_SELF_ORDER_KERNELS
+            self_solve_exact(ctx, it);   // same particle ranges as the ground clamp below
+#else
             self_solve(ctx, it);   // same particle ranges as the ground clamp below
+#endif
         }
         phase_ground(ctx);
         NC_SYNC(ctx);
+#ifdef NC_SELF_ORDER_KERNELS
+        if (s.self_collision && d.hash_head != nullptr && !self_settle(ctx, it)) return false;
+#endif
     }
     // reconciliation (tools/cloth_bag.cpp:4975-5058)
     uint32_t passes = 0;
@@ -2238,6 +2986,12 @@ __device__ __forceinline__ void run_frame(const DeviceCloth& src, const Schedule
 __global__ void numi_cloth_frame_edge_kernel(DeviceCloth d, Schedule s);
 __global__ void numi_cloth_batch_edge_kernel(const DeviceCloth* cloths, uint32_t count, Schedule s,
                                              unsigned int* queue);
+// The frame kernels whose point self contact keeps the reference's
+// Gauss-Seidel order are likewise in cloth_self_order_kernels.cu: its
+// out-of-line ordered pass would otherwise cost the default kernels
+// registers in every phase.
+__global__ void numi_cloth_frame_exact_kernel(DeviceCloth d, Schedule s);
+__global__ void numi_cloth_frame_edge_exact_kernel(DeviceCloth d, Schedule s);
 
 // Many independent cloths in one persistent launch: every CTA takes the
 // next cloth from a device work queue (cloths ordered by work, largest
@@ -2256,11 +3010,11 @@ __global__ void numi_cloth_batch_edge_kernel(const DeviceCloth* cloths, uint32_t
 
 #ifndef NC_EDGE_KERNELS
 // One cloth on the whole grid (one CTA, a cooperative grid or a cluster).
-__global__ void __launch_bounds__(NC_BLOCK_MAX) numi_cloth_frame_kernel(DeviceCloth d, Schedule s) {
+__global__ void __launch_bounds__(NC_BLOCK_MAX, 1) numi_cloth_frame_kernel(DeviceCloth d, Schedule s) {
     extern __shared__ __align__(16) unsigned char nc_dynamic_smem[];
     run_frame<false, false>(d, s, blockIdx.x, gridDim.x, nc_dynamic_smem);
 }
-__global__ void __launch_bounds__(NC_BLOCK_MAX) numi_cloth_batch_kernel(const DeviceCloth* cloths, uint32_t count,
+__global__ void __launch_bounds__(NC_BLOCK_MAX, 1) numi_cloth_batch_kernel(const DeviceCloth* cloths, uint32_t count,
                                                                          Schedule s, unsigned int* queue) {
     NC_BATCH_BODY(false)
 }

@@ -28,7 +28,10 @@
 //   1. predict of the closure, distance and bend colours, grips (owner of
 //      the gripped particle); fruit CTA: fruit predict and fruit pairs;
 //   2. fruit/yarn colours, self-contact insert of the owned particles;
-//   3. self-contact solve and ground clamp of the closure, strain colours,
+//   3. with self contact: its phase A and the ground clamp of the owned
+//      particles, then (after the barrier, and only where phase A listed
+//      pairs) its ordered pass on CTA 0 and one more barrier; strain
+//      colours (without self contact the closure's ground clamp first),
 //      finalize and cloth/ground friction of the owned particles; fruit
 //      CTA: fruit sums, ground and finalize (more strain sweeps: one phase
 //      each);
@@ -250,28 +253,33 @@ __device__ __forceinline__ void tile_insert(const Ctx& ctx) {
     for (uint32_t l = threadIdx.x; l < own; l += blockDim.x) self_insert_one(ctx, tag, gi[l], ctx.tx[l]);
 }
 
-// Self-contact solve and ground clamp of the first nl local particles (the
-// strain chain's closure, or the owned ones; each a function of its
-// start-of-pass position and the grid), counted for the owned ones.
+// Self-contact phase A (the ordered pass follows the barrier) and the
+// ground clamp of the first nl local particles (the owned ones, or the
+// strain chain's closure where the ground clamp alone runs there).
 __device__ void tile_self_ground(const Ctx& ctx, bool self, uint32_t nl) {
     const SubCfg& c = ctx.c;
-    const uint32_t own = ctx.tp[1];
     const uint32_t* gi = tile_list(ctx);
     const uint32_t tag = self_pass_tag(ctx, 0u);
-    unsigned long long contacts = 0ull, ghost_contacts = 0ull;
-    float max_pen = 0.0f, ghost_pen = 0.0f;
+    unsigned long long contacts = 0ull;
+    float max_pen = 0.0f;
     for (uint32_t l = threadIdx.x; l < nl; l += blockDim.x) {
         float4 p = ctx.tx[l];
         if (self) {
             float4 q;
-            const bool mine = l < own;
-            if (self_solve_one(ctx, tag, gi[l], p, q, mine ? contacts : ghost_contacts, mine ? max_pen : ghost_pen))
-                p = q;
+#ifdef NC_SELF_ORDER_KERNELS
+            if (self_exact_one(ctx, tag, gi[l], p, q, contacts, max_pen)) p = q;
+#else
+            if (self_solve_one(ctx, tag, gi[l], p, q, contacts, max_pen)) p = q;
+#endif
         }
         if (c.ground && c.radius - p.z > 0.0f) p = make_float4(p.x, p.y, c.radius, p.w);
         ctx.tx[l] = p;
     }
+#ifdef NC_SELF_ORDER_KERNELS
+    if (self) self_pass_flush(ctx.d, contacts, max_pen);
+#else
     if (self) self_stats_flush(ctx.d, contacts, max_pen);
+#endif
     __syncthreads();
 }
 
@@ -460,11 +468,11 @@ __device__ bool substep_tiles(Ctx& ctx, bool last) {
         ctx.hold_tail = last || attach || listed > NC_FRICTION_STAGE;
         if (!ctx.hold_tail && listed > 0u && !ctx.fruit_cta) ctx.fruit_wait = tile_touches_listed(ctx, listed);
     }
-    // With split self contact the owners first resolve their own particles'
-    // self contact and ground clamp and publish them (one more grid
-    // barrier), so each query runs once instead of in every closure that
-    // holds the particle; the strain chains then load resolved positions.
-    const bool split = self && d.tile_split_self != 0u;
+    // With self contact the owners first resolve their own particles' self
+    // contact (phase A) and ground clamp and publish them (one more grid
+    // barrier), the ordered pass follows where phase A listed pairs, and the
+    // strain chains then load resolved positions.
+    const bool split = self;
     if (split) {
         float4* x_next = other_x(ctx);
         if (ctx.fruit_cta) {
@@ -482,6 +490,9 @@ __device__ bool substep_tiles(Ctx& ctx, bool last) {
         }
         ctx.gx = x_next;
         NC_SYNC(ctx);
+#ifdef NC_SELF_ORDER_KERNELS
+        if (!self_settle(ctx, 0u)) return false;
+#endif
     }
     const uint32_t sweeps = max(s.strain_sweeps, 1u);
     for (uint32_t sw = 0; sw < sweeps; ++sw) {
@@ -500,7 +511,7 @@ __device__ bool substep_tiles(Ctx& ctx, bool last) {
             if (!split) tile_mark(ctx, 9u);
             tile_load(ctx, NC_TILE_STRAIN);
             if (!split) tile_mark(ctx, 10u);
-            if (sw == 0u && !split) tile_self_ground(ctx, self, ctx.tp[4u + NC_TILE_STRAIN]);
+            if (sw == 0u && !split) tile_self_ground(ctx, false, ctx.tp[4u + NC_TILE_STRAIN]);
             tile_mark(ctx, 11u);
             if (s.strain_sweeps > 0u) tile_chain(ctx, NC_TILE_STRAIN, dt2);
             tile_mark(ctx, 12u);

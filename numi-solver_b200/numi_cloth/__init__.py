@@ -93,6 +93,7 @@ def load_library() -> ctypes.CDLL:
         "numi_cloth_launch_info": (i32, [vp, ctypes.POINTER(u32)]),
         "numi_cloth_tune": (i32, [vp, vp, u32, vp, ctypes.POINTER(u32)]),
         "numi_cloth_self_contacts": (i32, [vp, ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(ctypes.c_double)]),
+        "numi_cloth_self_order_stats": (i32, [vp, ctypes.POINTER(ctypes.c_ulonglong)]),
         "numi_cloth_edge_contacts": (i32, [vp, ctypes.POINTER(ctypes.c_ulonglong)]),
         "numi_cloth_set_damping": (i32, [vp, ctypes.c_float]),
         "numi_cloth_rollout_grad": (i32, [vp, vp, u32, ctypes.POINTER(Schedule), u32, vp, u32, vp, u32,
@@ -597,6 +598,15 @@ class ClothSolver:
         self._check(self.lib.numi_cloth_self_contacts(self._h, ctypes.byref(n), ctypes.byref(pen)))
         return int(n.value), float(pen.value)
 
+    def self_order_stats(self) -> dict:
+        """How the point self-contact passes kept the reference's order since
+        create: passes that ran the ordered pass, pairs listed, ordered-pass
+        rounds, passes resolved by the serial fallback."""
+        out = (ctypes.c_ulonglong * 4)()
+        self._check(self.lib.numi_cloth_self_order_stats(self._h, out))
+        return {"ordered_passes": int(out[0]), "listed_pairs": int(out[1]), "rounds": int(out[2]),
+                "fallbacks": int(out[3])}
+
     def edge_contacts(self) -> tuple[int, int]:
         """(edge/edge solves that moved particles, yarn/yarn self-friction
         contacts) since create."""
@@ -618,7 +628,7 @@ class ClothSolver:
         self._check(self.lib.numi_cloth_launch_info(self._h, out))
         return {"grid": out[0], "block": out[1], "barriers_per_substep": out[2], "launches": out[3],
                 "cluster": out[4], "resident": bool(out[5] & 1), "neighbour_syncs": bool(out[5] & 2),
-                "tiles": bool(out[5] & 4), "last_tiles": bool(out[5] & 8)}
+                "tiles": bool(out[5] & 4), "last_tiles": bool(out[5] & 8), "self_order_reference": bool(out[5] & 16)}
 
     def trace(self, substeps: int) -> np.ndarray:
         """Per-barrier globaltimer stamps (ns) of the last step, [substeps, 128]."""

@@ -1918,8 +1918,11 @@ struct Sim {
             solve_grips(sub, dt);
             pair_sweep(dt, serial);
             yarn_sweep(serial, ground_on, dt);
+            // point self contact: the kernels' batched pass, or (the
+            // reference-order kernels, and the serial order) the reference's
+            // Gauss-Seidel pass
             if (s.self_collision) {
-                if (serial)
+                if (serial || s.mode == ORACLE_BATCHED_SELF_REFERENCE)
                     self_serial();
                 else
                     self_batched();

@@ -11,7 +11,12 @@
  *                    hash-grid point self contact (tools/cloth_bag.cpp:4712-5310);
  *   ORACLE_BATCHED - the colour-batch schedule of the B200 kernels (colour
  *                    runs of the arrays; fruit/yarn with fruit positions
- *                    frozen over a sweep and summed; Jacobi self contact).
+ *                    frozen over a sweep and summed; batched point self
+ *                    contact: every pair at the start of the pass, sums
+ *                    applied once);
+ *   ORACLE_BATCHED_SELF_REFERENCE - the same with point self contact in the
+ *                    reference's Gauss-Seidel order (the kernels built with
+ *                    the ordered pass, NUMI_CLOTH_SELF_ORDER=reference).
  * and in two scalar types: 64 (the FP64 oracle) and 32 (float with the
  * kernels' exact evaluation order, fixed-point fruit sums and FP64 fixed-tree
  * air reductions, used to prove bit-identity of the GPU path).
@@ -121,7 +126,7 @@ typedef struct OracleScene {
     const OracleParams* params;
 } OracleScene;
 
-enum { ORACLE_BATCHED = 0, ORACLE_SERIAL = 1 };
+enum { ORACLE_BATCHED = 0, ORACLE_SERIAL = 1, ORACLE_BATCHED_SELF_REFERENCE = 2 };
 
 /* bits: 32 or 64.  Returns NULL on a malformed scene. */
 void* oracle_create(int bits, const OracleScene* scene);

@@ -99,7 +99,7 @@ class OScene(ctypes.Structure):
     ]
 
 
-BATCHED, SERIAL = 0, 1
+BATCHED, SERIAL, BATCHED_SELF_REFERENCE = 0, 1, 2
 _LIB = None
 
 
@@ -329,8 +329,10 @@ class Oracle:
         lib().oracle_residuals(self._h, out)
         return np.array(out[:])
 
-    def self_pass(self, serial: bool) -> float:
-        """One point self-contact pass on the current state."""
+    def self_pass(self, serial: bool = True) -> float:
+        """One point self-contact pass on the current state: the reference's
+        Gauss-Seidel order, or the kernels' batched order; its deepest
+        penetration."""
         return float(lib().oracle_self_pass(self._h, 1 if serial else 0))
 
     def stats(self) -> dict:

@@ -11,6 +11,10 @@ import oracle_py as op
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 
+# Point self contact in the reference's Gauss-Seidel order (the frame
+# kernels with the ordered pass), and its oracle order.
+SELF_REFERENCE = {"NUMI_CLOTH_SELF_ORDER": "reference"}
+
 # Schedules exercised by the parity tests.  "reference" is the reference
 # CPU substep (tools/cloth_bag.cpp:4891-5185) with a reduced certificate cap.
 FULL = dict(iterations=2, strainSweeps=3, reconcilePasses=3, finalPasses=2, certificatePasses=4, earlyExit=1,
@@ -111,15 +115,15 @@ def oracle_state_to_abi(scene, st):
     return P, F
 
 
-def per_substep_errors(scene, configs, sched, mode=op.BATCHED):
+def per_substep_errors(scene, configs, sched, mode=op.BATCHED, env=None):
     """Max particle / fruit position error of one GPU substep started from
     the FP64 trajectory's state (rounded to FP32), for every substep.  mode:
     the FP64 oracle's order, BATCHED (the kernels' order) or SERIAL (the
-    reference's order)."""
+    reference's order); env: launch-policy variables of the GPU solver."""
     o = op.Oracle(op.from_abi(scene), 64)
     subs = op.substeps_from_configs(configs)
     osched = op.schedule_from_abi(sched, mode)
-    s = nc.ClothSolver(scene)
+    s = make_solver(scene, env=env)
     errs, ferrs = [], []
     try:
         for k in range(len(configs)):

@@ -1,21 +1,29 @@
-"""Point/point self contact (tools/cloth_bag.cpp:4249-4315): the batched
-restatement in the oracle, and the GPU hash grid against it.
+"""Point/point self contact (tools/cloth_bag.cpp:4249-4315): the oracle's
+two pass orders, and the GPU hash grid against them.
 
-The batched order resolves every non-local pair closer than 2r against the
-positions at the start of the pass and applies each particle's summed
-corrections once.  Where every particle is in at most one pair the reference's
+The default kernels run the batched order: every non-local pair closer than
+2r at the start of the pass, each particle's summed corrections applied
+once.  Where every particle is in at most one pair the reference's
 Gauss-Seidel pass and the batched pass make the same moves, bit for bit in
-FP64; that pins the batched pair set and per-pair correction to the
-reference's serial pass, which is itself pinned to the compiled reference by
-the golden runs.
+FP64; where particles have several partners they differ (stated below).
+The kernels built with the ordered pass (NUMI_CLOTH_SELF_ORDER=reference)
+keep the reference's Gauss-Seidel order everywhere: phase A resolves
+isolated pairs in parallel, one CTA resolves the coupled particles'
+listed pairs in the reference's order (wavefronts, else serially), and a
+serial pass over the whole cloth backs both up; they are bit-identical to
+the FP32 oracle in that order.
 """
 import numpy as np
 import pytest
 
 import numi_cloth as nc
 import oracle_py as op
-from helpers import FULL, gpu_positions, run_gpu, run_oracle, small_square
+from helpers import (FULL, SELF_REFERENCE, gpu_positions, make_solver, per_substep_errors, run_gpu, run_oracle,
+                     small_square)
 
+
+POS_TOL_FP64 = 1.0e-5   # m: one FP32 substep vs the FP64 reference-order substep from the same state
+FIRST_DEEP_SUBSTEP_STATED = 2.0e-4   # m: the offset fold's first substep (1.05e-4 measured), stated
 
 def folded_square(side=24, gap=0.0015, fruits=0):
     """A square folded in half over its middle row: the upper layer lies
@@ -108,9 +116,10 @@ def test_multi_partner_contacts_batched_vs_serial_fp64():
     the reference's Gauss-Seidel pass differ: one FP64 pass and one FP64
     substep from the same state on the offset fold (987 contacts, up to
     four partners per particle) differ by 3.4e-4 m.  Stated, not within the
-    1e-5 m bar; on the benchmark scenes (the bag, the 256x256 cloth) every
-    particle has at most one partner and the orders agree
-    (tests/test_headline_parity.py, tests/test_gpu_parity.py)."""
+    1e-5 m bar; on the benchmark scenes (the bag, the 256x256 cloth's first
+    frame) every particle has at most one partner and the orders agree
+    (tests/test_headline_parity.py, tests/test_gpu_parity.py), and the
+    reference-order kernels remove the gap (tests below)."""
     scene = offset_folded_square()
     a, b = _oracle(scene, 64), _oracle(scene, 64)
     a.self_pass(serial=True)
@@ -176,3 +185,96 @@ def test_gpu_self_contact_full_buckets_use_the_overflow_list():
     assert g["failure"] == 0, nc.failure_names(g["failure"])
     assert np.array_equal(gpu_positions(g).astype(np.float64), o["particles"]["x"])
     assert g["self_contacts"][0] == o["stats"]["self_contacts"] > 100
+
+
+def test_offset_fold_fp64_orders_agree():
+    """One FP64 substep of the offset fold (every family on, point self
+    contact in both iterations) in the reference-order kernels' order and in
+    the reference's order: the same bits."""
+    scene = offset_folded_square()
+    cfg = nc.substep_configs(scene, 1)
+    sched = nc.Schedule.make(**dict(FULL, selfCollision=1))
+    subs = op.substeps_from_configs(cfg)
+    ser, bat = _oracle(scene, 64), _oracle(scene, 64)
+    ser.step(subs, op.schedule_from_abi(sched, op.SERIAL))
+    bat.step(subs, op.schedule_from_abi(sched, op.BATCHED_SELF_REFERENCE))
+    assert np.array_equal(ser.read()["particles"]["x"], bat.read()["particles"]["x"])
+    assert ser.stats()["self_contacts"] == bat.stats()["self_contacts"] > 900
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("launch", ["one-cta", "grid", "resident"])
+def test_gpu_multi_partner_fold_bitexact_fp32(launch):
+    """Reference-order kernels, up to four partners per particle: phase A
+    lists the coupled particles and the ordered pass resolves them in the
+    reference's order; the GPU gives the FP32 oracle's bits (the reference's
+    Gauss-Seidel pass in FP32) and the same contact count, on one CTA, a
+    cooperative grid and a resident cluster."""
+    scene = offset_folded_square()
+    cfg = nc.substep_configs(scene, 12)
+    s = nc.Schedule.make(**dict(FULL, selfCollision=1))
+    kw = {"one-cta": dict(grid=1, env=dict(SELF_REFERENCE, NUMI_CLOTH_RESIDENT="0")),
+          "grid": dict(grid=6, env=SELF_REFERENCE),
+          "resident": dict(env=dict(SELF_REFERENCE, NUMI_CLOTH_RESIDENT="1"))}[launch]
+    g = run_gpu(scene, cfg, s, **kw)
+    assert g["info"]["self_order_reference"]
+    o = run_oracle(scene, cfg, s, bits=32, mode=op.BATCHED_SELF_REFERENCE)
+    assert g["failure"] == 0, nc.failure_names(g["failure"])
+    gp = gpu_positions(g).astype(np.float64)
+    assert np.array_equal(gp, o["particles"]["x"]), f"max |dx| = {np.abs(gp - o['particles']['x']).max()}"
+    assert np.array_equal(g["particles"]["velocity"][:, :3].astype(np.float64), o["particles"]["v"])
+    assert g["self_contacts"][0] == o["stats"]["self_contacts"] > 900
+
+
+@pytest.mark.gpu
+def test_gpu_multi_partner_fold_per_substep_fp64():
+    """Reference-order kernels: every substep of the offset fold's first 12,
+    started from the FP64 reference-order state, against the FP64 reference.  The first substep
+    resolves 1 mm interpenetrations of about a thousand four-partner pairs;
+    there the FP32 substep (the GPU's, equal to the FP32 oracle's bit for
+    bit) departs from FP64 by about 1e-4 m, which is precision, not order:
+    the FP64 batched and reference orders agree bit for bit on it
+    (test_offset_fold_fp64_orders_agree).  The later substeps are within
+    1e-5 m (stated)."""
+    scene = offset_folded_square()
+    cfg = nc.substep_configs(scene, 12)
+    s = nc.Schedule.make(**dict(FULL, selfCollision=1))
+    errs, _ = per_substep_errors(scene, cfg, s, op.SERIAL, env=SELF_REFERENCE)
+    print(f"offset fold, per substep against the FP64 reference order: first {errs[0]:.3e} m, "
+          f"then max {errs[1:].max():.3e} m (median {np.median(errs[1:]):.3e})")
+    assert errs[0] <= FIRST_DEEP_SUBSTEP_STATED
+    assert errs[1:].max() <= POS_TOL_FP64
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["folded", "squeezed"])
+def test_gpu_reference_order_other_scenes(case):
+    """Reference-order kernels on the folded cloth (isolated pairs: phase A
+    alone) and on a cloth squeezed into a couple of cells (every particle
+    coupled, the overflow list in use: the serial fallback), bit-identical
+    to the FP32 oracle in that order, with its contact counts."""
+    if case == "folded":
+        scene = folded_square(fruits=4)
+        cfg = nc.substep_configs(scene, 12)
+    else:
+        scene = small_square(side=10, fruits=0)
+        pos = scene.particles["positionAndInverseMass"]
+        centre = pos[:, :3].mean(axis=0)
+        pos[:, 0] = centre[0] + (pos[:, 0] - centre[0]) * np.float32(0.05)
+        pos[:, 1] = centre[1] + (pos[:, 1] - centre[1]) * np.float32(0.05)
+        scene.particles["previousAndMass"][:, :3] = pos[:, :3]
+        cfg = nc.substep_configs(scene, 2)
+    s = nc.Schedule.make(**dict(FULL, selfCollision=1))
+    solver = make_solver(scene, env=SELF_REFERENCE)
+    solver.step(cfg, s)
+    fail = solver.failure()
+    gp = solver.particles()["positionAndInverseMass"][:, :3].astype(np.float64)
+    contacts = solver.self_contacts()[0]
+    order = solver.self_order_stats()
+    solver.close()
+    o = run_oracle(scene, cfg, s, bits=32, mode=op.BATCHED_SELF_REFERENCE)
+    assert fail == 0, nc.failure_names(fail)
+    assert np.array_equal(gp, o["particles"]["x"]), f"max |dx| = {np.abs(gp - o['particles']['x']).max()}"
+    assert contacts == o["stats"]["self_contacts"] > 0
+    print(f"{case}: {order}")
+    if case == "squeezed":
+        assert order["fallbacks"] > 0

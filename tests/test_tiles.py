@@ -10,7 +10,8 @@ import numpy as np
 import pytest
 
 import numi_cloth as nc
-from helpers import make_solver, run_gpu, run_oracle, small_square
+import oracle_py as op
+from helpers import SELF_REFERENCE, make_solver, run_gpu, run_oracle, small_square
 from test_gpu_parity import _check_bitexact
 
 pytestmark = pytest.mark.gpu
@@ -37,18 +38,17 @@ def _same(a, b):
     assert a["self_contacts"] == b["self_contacts"]
 
 
-@pytest.mark.parametrize("variant", ["bench", "bench-unsplit", "sweeps2-damped", "sweeps2-unsplit", "no-self",
-                                     "no-strain", "no-fruits", "many-fruits"])
+@pytest.mark.parametrize("variant", ["bench", "sweeps2-damped", "no-self", "no-strain", "no-fruits", "many-fruits",
+                                     "folded", "folded-reference-order"])
 def test_tiles_equal_colour_schedule_and_oracle(variant):
     """Tile mode against the colour-by-colour launch and the oracle; the
-    -unsplit variants resolve self contact inside the strain closures
-    (NUMI_CLOTH_TILE_SPLIT=0) instead of by the owners first."""
+    folded variants lay the upper half of the cloth over the lower one,
+    shifted half a spacing, so that point self contact has particles with
+    several partners (in the reference order phase A lists them and CTA 0
+    runs the ordered pass)."""
     sched = dict(BENCH_LIKE)
     kw = dict(side=96, fruits=12)
-    env = dict(TILES, NUMI_CLOTH_TILE_SPLIT="0") if variant.endswith("-unsplit") else TILES
-    variant = variant.replace("-unsplit", "")
-    if variant == "sweeps2":
-        variant = "sweeps2-damped"
+    env = TILES
     if variant == "sweeps2-damped":
         sched.update(strainSweeps=2, damping=0.3)
     elif variant == "no-self":
@@ -59,16 +59,29 @@ def test_tiles_equal_colour_schedule_and_oracle(variant):
         kw.update(fruits=0)
     elif variant == "many-fruits":
         kw.update(fruits=48, fruitRadiusMin=0.005, fruitRadiusMax=0.02)
-    scene = small_square(**kw)
+    plain_env = COLOURS
+    mode = op.BATCHED
+    if variant.startswith("folded"):
+        # a 48 x 48 fold (1,152 particles over 1,152, four partners each) on
+        # a forced cooperative grid of 16 CTAs
+        from test_self_contact import offset_folded_square
+        scene = offset_folded_square(side=48)
+        forced = {"NUMI_CLOTH_GRID": "16", "NUMI_CLOTH_TILE_GRID": "16", "NUMI_CLOTH_RESIDENT": "0"}
+        if variant.endswith("reference-order"):
+            forced.update(SELF_REFERENCE)
+            mode = op.BATCHED_SELF_REFERENCE
+        env, plain_env = dict(TILES, **forced), dict(COLOURS, **forced)
+    else:
+        scene = small_square(**kw)
     cfg = nc.substep_configs(scene, 24)
     s = nc.Schedule.make(**sched)
     tiled = run_gpu(scene, cfg, s, env=env)
-    plain = run_gpu(scene, cfg, s, env=COLOURS)
+    plain = run_gpu(scene, cfg, s, env=plain_env)
     assert tiled["info"]["last_tiles"], tiled["info"]
     assert not plain["info"]["last_tiles"]
     assert tiled["failure"] == 0 and plain["failure"] == 0, nc.failure_names(tiled["failure"] | plain["failure"])
     _same(tiled, plain)
-    _check_bitexact(tiled, run_oracle(scene, cfg, s, bits=32))
+    _check_bitexact(tiled, run_oracle(scene, cfg, s, bits=32, mode=mode))
 
 
 def test_tiles_across_launches_and_frames():
