@@ -309,6 +309,16 @@ __device__ __forceinline__ void tile_mark(const Ctx& ctx, uint32_t k) {
         d.trace[static_cast<size_t>(ctx.sub) * NC_TRACE_SLOTS + NC_TILE_MARK_SLOT + k] = globaltimer();
 }
 
+// The fruit CTA's own stamps (trace slots NC_FRUIT_MARK_SLOT and up).
+#define NC_FRUIT_MARK_SLOT 100u
+__device__ __forceinline__ void fruit_mark(const Ctx& ctx, uint32_t k) {
+    const DeviceCloth& d = ctx.d;
+    if (d.trace == nullptr || !ctx.fruit_cta) return;
+    __syncthreads();
+    if (threadIdx.x == 0 && NC_FRUIT_MARK_SLOT + k < NC_TRACE_SLOTS)
+        d.trace[static_cast<size_t>(ctx.sub) * NC_TRACE_SLOTS + NC_FRUIT_MARK_SLOT + k] = globaltimer();
+}
+
 // Row and column of a particle of a grid cloth (row-major), else (0, index).
 __device__ __forceinline__ uint2 tile_cell(const DeviceCloth& d, uint32_t i) {
     return d.grid_width != 0u ? make_uint2(i / d.grid_width, i % d.grid_width) : make_uint2(0u, i);
@@ -402,11 +412,14 @@ __device__ bool substep_tiles(Ctx& ctx, bool last) {
         float4* x_next = other_x(ctx);
         float4* v_next = other_v(ctx);
         if (ctx.fruit_cta) {
+            fruit_mark(ctx, 0u);
             fruit_begin(ctx);
+            fruit_mark(ctx, 1u);
             if (d.p_count > 0u) {
                 __syncthreads();
                 fruit_pair_sweep(d, *ctx.fs, ctx.c.dt);
             }
+            fruit_mark(ctx, 2u);
         } else {
             // the previous substep's friction rewrote velocities this CTA
             // predicts: wait for the fruit CTA's tail
@@ -476,10 +489,14 @@ __device__ bool substep_tiles(Ctx& ctx, bool last) {
     if (split) {
         float4* x_next = other_x(ctx);
         if (ctx.fruit_cta) {
+            fruit_mark(ctx, 3u);
             fruit_flush(ctx);
+            fruit_mark(ctx, 4u);
             if (ctx.c.ground) fruit_ground(ctx);
             fruit_finalize(ctx);
+            fruit_mark(ctx, 5u);
             if (s.frictions && fruits) friction_stage(ctx);
+            fruit_mark(ctx, 6u);
         } else {
             tile_mark(ctx, 9u);
             tile_load_owned(ctx);
@@ -527,7 +544,9 @@ __device__ bool substep_tiles(Ctx& ctx, bool last) {
     // barrier after it only where phase 3 decided so).  The fruit CTA
     // releases its flag as soon as the friction sweep has written the
     // velocities back: the rest of its tail touches only fruit state.
+    fruit_mark(ctx, 7u);
     if (friction_sweep) yarn_friction_sweep(ctx);
+    fruit_mark(ctx, 8u);
     if (ctx.fruit_cta) {
         __syncthreads();   // the sweep's velocity stores and list reads are done
         if (threadIdx.x == 0) {
@@ -538,6 +557,7 @@ __device__ bool substep_tiles(Ctx& ctx, bool last) {
         }
     }
     fruit_tail(ctx, last, friction_sweep);
+    fruit_mark(ctx, 9u);
     if (ctx.grip_cta && !last) {
         Ctx next = ctx;
         next.c = nc::load_cfg(d.cfg + s.cfg_offset + ctx.sub + 1u);
