@@ -1183,6 +1183,7 @@ __device__ void self_solve(Ctx& ctx, uint32_t it) {
 #define NC_SELF_GROUP 512u     // listed partners of one particle in one turn
 #define NC_SELF_KNOWN_BIT 0x80000000u
 #define NC_SELF_WAVE_MAX 8192u   // pairs in contact the wavefront form orders
+#define NC_SELF_BAND 0.01f       // listed pairs within this fraction of the contact distance join the wavefronts
 
 // Reference cell of a position (edge = the contact distance; the
 // reference's floor(position * inverseCell)).
@@ -1516,15 +1517,15 @@ __device__ __noinline__ bool self_serial_all(const Ctx& ctx, uint32_t tag, unsig
 }
 
 // The ordered pass's fast form (the calling CTA, all its threads): the
-// listed pairs in contact at the start of the pass are ordered by the
-// reference's key (first particle, rank of the second's cell around the
-// first's, second particle) and run as wavefronts: a pair runs once the
-// pairs before it in that order that share a particle have run, so each
-// pair sees the positions the serial pass gives it.  The listed pairs that
-// start apart run nowhere; they are proved idle afterwards (their start
-// distance less both particles' largest displacements stays at least the
-// contact distance), as are the visit cells (every first particle's cell at
-// its turn is its start cell).  False where a proof fails or the pairs do
+// listed pairs in contact at the start of the pass, or within NC_SELF_BAND
+// of it, are ordered by the reference's key (first particle, rank of the
+// second's cell around the first's, second particle) and run as wavefronts:
+// a pair runs once the pairs before it in that order that share a particle
+// have run, so each pair sees the positions the serial pass gives it (and
+// acts or not as there).  The listed pairs farther apart run nowhere; they
+// are proved idle afterwards (their start distance less both particles'
+// largest displacements stays above the contact distance), as are the visit
+// cells (every first particle's cell at its turn is its start cell).  False where a proof fails or the pairs do
 // not fit the scratch: the caller then restores the start positions and
 // runs the pairs serially.  Scratch (d.self_keys, u64 words): keys [0, K),
 // predecessors [K, 2K) (via the first particle << 32 | via the second,
@@ -1566,8 +1567,9 @@ __device__ __noinline__ bool self_ordered_levels(const Ctx& ctx, uint32_t tag, u
         const float4 ef = __ldcg(d.self_list + 2u * k), es = __ldcg(d.self_list + 2u * k + 1u);
         const uint32_t f = __float_as_uint(ef.w) & ~NC_SELF_KNOWN_BIT, s = __float_as_uint(es.w) & ~NC_SELF_KNOWN_BIT;
         const float L0 = len3(xyz(es) - xyz(ef));
-        if (L0 >= target || L0 < 1.0e-12f) continue;
+        if (L0 >= target * (1.0f + NC_SELF_BAND)) continue;
         const int rank = self_visit_rank(self_ref_cell(xyz(ef), inv_ref), self_ref_cell(xyz(es), inv_ref));
+        if (rank < 0 && L0 >= target) continue;   // never visited: the proof below covers it
         if (rank < 0 || s >= (1u << 27)) {
             s_bad = 1u;   // a touching pair outside the visit cells: the serial form decides
             continue;
@@ -1667,11 +1669,9 @@ __device__ __noinline__ bool self_ordered_levels(const Ctx& ctx, uint32_t tag, u
         const float df = d.self_disp[f], ds = d.self_disp[s];
         if (df > lim || ds > lim) s_bad = 1u;
         const float L0 = len3(xyz(es) - xyz(ef));
-        if (L0 < 1.0e-12f) {
-            if (df + ds > 0.0f) s_bad = 1u;   // coincident at the start and moved: it may act
-        } else if (L0 >= target && L0 - (df + ds) <= target * (1.0f + 1.0e-5f)) {
-            s_bad = 1u;
-        }
+        const int rank = self_visit_rank(self_ref_cell(xyz(ef), inv_ref), self_ref_cell(xyz(es), inv_ref));
+        if (rank >= 0 && L0 < target * (1.0f + NC_SELF_BAND)) continue;   // one of the wavefront pairs
+        if (L0 - (df + ds) <= target * (1.0f + 1.0e-5f)) s_bad = 1u;
     }
     __syncthreads();
     contacts_out = s_contacts;
