@@ -342,7 +342,7 @@ bool prepare_neighbours(numi_cloth* h, const NumiClothScene* scene) {
     const size_t smem = nc_resident_offset() + static_cast<size_t>(widest) * sizeof(uint32_t);
     int per_sm = 0;
     if (raise_frame_smem(smem) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, frame_fn(false), static_cast<int>(h->block), smem) !=
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, frame_fn(false, h->self_exact), static_cast<int>(h->block), smem) !=
             cudaSuccess) {
         cudaGetLastError();
         return false;
@@ -622,7 +622,7 @@ bool rebuild_tiles(numi_cloth* h) {
     int max_optin = 0;
     cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
     cudaFuncAttributes fa{};
-    cudaFuncGetAttributes(&fa, frame_fn(false));
+    cudaFuncGetAttributes(&fa, frame_fn(false, h->self_exact));
     return build_tiles(h, d.grid_width, dij, dmat, bij, bmat, static_cast<size_t>(max_optin) - fa.sharedSizeBytes);
 }
 
@@ -653,10 +653,10 @@ cudaError_t launch(numi_cloth* h, uint32_t substeps, const Schedule& s, uint32_t
         int max_optin = 0;
         cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
         cudaFuncAttributes fe{};
-        cudaFuncGetAttributes(&fe, frame_fn(true));
+        cudaFuncGetAttributes(&fe, frame_fn(true, h->self_exact));
         const size_t at = nc_round256(smem);
         if (at + NC_EDGE_TREE_KEY_BYTES + fe.sharedSizeBytes <= static_cast<size_t>(max_optin) &&
-            raise_smem(frame_fn(true), at + NC_EDGE_TREE_KEY_BYTES) == cudaSuccess) {
+            raise_smem(frame_fn(true, h->self_exact), at + NC_EDGE_TREE_KEY_BYTES) == cudaSuccess) {
             sc.tree_keys = static_cast<uint32_t>(at);
             smem = at + NC_EDGE_TREE_KEY_BYTES;
         }
@@ -1140,8 +1140,8 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
         int max_optin = 0;
         cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
         cudaFuncAttributes fa{}, fe{};
-        cudaFuncGetAttributes(&fa, frame_fn(false));
-        cudaFuncGetAttributes(&fe, frame_fn(true));
+        cudaFuncGetAttributes(&fa, frame_fn(false, h->self_exact));
+        cudaFuncGetAttributes(&fe, frame_fn(true, h->self_exact));
         bool ok = smem + std::max(fa.sharedSizeBytes, fe.sharedSizeBytes) <= static_cast<size_t>(max_optin) &&
                   raise_frame_smem(smem) == cudaSuccess;
         if (ok && ranks > 1u) {
@@ -1339,7 +1339,7 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
         int max_optin = 0;
         cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
         cudaFuncAttributes fa{};
-        cudaFuncGetAttributes(&fa, frame_fn(false));
+        cudaFuncGetAttributes(&fa, frame_fn(false, h->self_exact));
         uint32_t tgrid = static_cast<uint32_t>(sms);
         env_u32("NUMI_CLOTH_TILE_GRID", tgrid);
         h->tile_grid = std::max(tgrid, 3u);
@@ -1349,7 +1349,7 @@ int numi_cloth_create(const NumiClothScene* scene, numi_cloth_t** out) {
         if (h->tiles) {
             int k = 0;
             h->tiles = raise_frame_smem(h->tile_smem) == cudaSuccess &&
-                       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, frame_fn(false), NC_BLOCK_MAX,
+                       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, frame_fn(false, h->self_exact), NC_BLOCK_MAX,
                                                                      h->tile_smem) == cudaSuccess &&
                        static_cast<uint64_t>(k) * static_cast<uint64_t>(sms) >= h->tile_grid;
         }
@@ -1711,7 +1711,7 @@ bool configure_tiles(numi_cloth* h, uint32_t grid) {
     if (h->tiles) {
         int k = 0;
         h->tiles = raise_frame_smem(h->tile_smem) == cudaSuccess &&
-                   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, frame_fn(false), NC_BLOCK_MAX, h->tile_smem) ==
+                   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, frame_fn(false, h->self_exact), NC_BLOCK_MAX, h->tile_smem) ==
                        cudaSuccess &&
                    static_cast<uint64_t>(k) * static_cast<uint64_t>(sms) >= h->tile_grid;
     }

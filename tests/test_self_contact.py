@@ -278,3 +278,26 @@ def test_gpu_reference_order_other_scenes(case):
     print(f"{case}: {order}")
     if case == "squeezed":
         assert order["fallbacks"] > 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("edge", [0, 1], ids=["points", "with-edge-edge"])
+def test_gpu_reference_order_bag(edge):
+    """Reference-order kernels on the produce bag under the reference's own
+    schedule with the lift, one frame (with the edge/edge family: the
+    reference-order edge kernel): bit-identical to the FP32 oracle in that
+    order, with its contact counts."""
+    import bench
+    from helpers import bag_frame_configs
+    from test_gpu_parity import _check_bitexact
+
+    dt = 1.0 / 5760.0
+    scene = nc.bag_scene(scenario="recorded", timestep=dt)
+    cfg = bag_frame_configs(scene, 0, 48, dt)
+    s = nc.Schedule.make(**dict(bench.BAG_SCHEDULE, primitiveSelf=edge))
+    g = run_gpu(scene, cfg, s, env=SELF_REFERENCE)
+    o = run_oracle(scene, cfg, s, bits=32, mode=op.BATCHED_SELF_REFERENCE)
+    assert g["info"]["self_order_reference"]
+    assert g["failure"] == 0, nc.failure_names(g["failure"])
+    _check_bitexact(g, o)
+    assert g["self_contacts"][0] == o["stats"]["self_contacts"]
